@@ -1,0 +1,233 @@
+"""B200 batched Atari 2600 emulator core — Python binding of the C ABI.
+
+`BatchAtariGpu` mirrors the reference's Rust API (RPP1011/fast-atari-rs
+src/cuda_env.rs:99-191): construct from ROM bytes and an instance count, then
+reset / step / step_multi / set_sorted / download_states / num_envs.  All
+emulation runs in the sm_100a library (lib/libfast_atari.so, built by
+build.py); this module only marshals buffers.  There is no CPU fallback: if
+the library or a CUDA device is missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "lib" / "libfast_atari.so"
+
+FA_OK = 0
+FA_STATUS_ILLEGAL_OPCODE = 0x1
+FA_STATUS_VSYNC_BUDGET = 0x2
+FA_STATUS_NOT_RESET = 0x4
+FA_STATUS_HALT_MASK = 0x7
+FA_STATUS_CYCLE_CAP = 0x100
+
+SCHED_LANE, SCHED_PC, SCHED_LINE, SCHED_MATCH = 0, 1, 2, 3
+SCHED_NAMES = {"lane": SCHED_LANE, "pc": SCHED_PC, "line": SCHED_LINE, "match": SCHED_MATCH}
+
+# fa_state, include/fast_atari.h (the reference AtariStateGpu prefix + extension).
+STATE_DTYPE = np.dtype([
+    ("a", "u1"), ("x", "u1"), ("y", "u1"), ("sp", "u1"),
+    ("pc", "<u2"), ("status", "u1"), ("_pad0", "u1"),
+    ("ram", "u1", (128,)),
+    ("port_a_output", "u1"), ("port_a_ddr", "u1"), ("port_a_input", "u1"),
+    ("port_b_output", "u1"), ("port_b_ddr", "u1"), ("port_b_input", "u1"),
+    ("timer_value", "<u2"), ("timer_prescaler", "<u2"), ("timer_prescaler_select", "<u2"),
+    ("timer_underflow", "u1"), ("_pad1", "u1"), ("_pad2", "u1"), ("_pad3", "u1"),
+    ("tia_clock", "<u2"), ("tia_scanline", "<u2"),
+    ("tia_wsync", "u1"), ("tia_frame_complete", "u1"), ("tia_vsync", "u1"), ("tia_vblank", "u1"),
+    ("cxm0p", "u1"), ("cxm1p", "u1"), ("cxp0fb", "u1"), ("cxp1fb", "u1"),
+    ("cxm0fb", "u1"), ("cxm1fb", "u1"), ("cxblpf", "u1"), ("cxppmm", "u1"),
+    ("inpt4", "u1"), ("inpt5", "u1"), ("paddle0", "u1"), ("paddle1", "u1"),
+    ("paddle_counter", "<u2"), ("paddle_dumped", "u1"), ("_pad4", "u1"),
+    ("pos_p0", "<u2"), ("pos_p1", "<u2"), ("pos_m0", "<u2"), ("pos_m1", "<u2"), ("pos_bl", "<u2"),
+    ("hmp0", "u1"), ("hmp1", "u1"), ("hmm0", "u1"), ("hmm1", "u1"), ("hmbl", "u1"), ("_pad5", "u1"),
+    ("grp0", "u1"), ("grp1", "u1"), ("grp0_old", "u1"), ("grp1_old", "u1"),
+    ("enam0", "u1"), ("enam1", "u1"), ("enabl", "u1"), ("enabl_old", "u1"),
+    ("vdelp0", "u1"), ("vdelp1", "u1"), ("vdelbl", "u1"),
+    ("resmp0", "u1"), ("resmp1", "u1"), ("nusiz0", "u1"), ("nusiz1", "u1"),
+    ("colup0", "u1"), ("colup1", "u1"), ("colupf", "u1"), ("colubk", "u1"),
+    ("ctrlpf", "u1"), ("refp0", "u1"), ("refp1", "u1"),
+    ("pf0", "u1"), ("pf1", "u1"), ("pf2", "u1"),
+    ("bank", "u1"), ("scheme", "u1"), ("_pad_end", "u1", (2,)),
+    ("_pad_ext", "u1", (3,)),
+    ("cycles", "<u8"), ("frame_no", "<u4"), ("run_status", "<u4"),
+])
+assert STATE_DTYPE.itemsize == 240
+
+# Symbols declared in include/fast_atari.h, with ctypes signatures.
+_vp, _u8p, _sz, _i, _u32 = ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint8), ctypes.c_size_t, ctypes.c_int, ctypes.c_uint32
+_SIGS = {
+    "fa_last_error": (ctypes.c_char_p, []),
+    "fa_version": (ctypes.c_char_p, []),
+    "fa_device_count": (_i, []),
+    "fa_create": (_i, [_u8p, _sz, _sz, ctypes.POINTER(_vp)]),
+    "fa_destroy": (None, [_vp]),
+    "fa_num_envs": (_sz, [_vp]),
+    "fa_set_sorted": (_i, [_vp, _i]),
+    "fa_reset": (_i, [_vp, _u8p]),
+    "fa_step": (_i, [_vp, _u8p, _u8p]),
+    "fa_step_multi": (_i, [_vp, _u8p, _i, _u8p]),
+    "fa_step_multi_async": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "fa_synchronize": (_i, [_vp]),
+    "fa_get_states": (_i, [_vp, _vp]),
+    "fa_set_states": (_i, [_vp, _vp]),
+    "fa_get_ram": (_i, [_vp, _sz, _u8p]),
+    "fa_get_status": (_i, [_vp, ctypes.POINTER(_u32)]),
+    "fa_set_episode_frames": (_i, [_vp, _u32]),
+    "fa_set_frame_numbers": (_i, [_vp, ctypes.POINTER(_u32)]),
+    "fa_set_launch": (_i, [_vp, _i, _i, _i]),
+    "fa_get_launch": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "fa_last_instructions": (ctypes.c_ulonglong, [_vp]),
+    "fa_get_snapshot": (_i, [_vp, _vp]),
+    "fa_device_state": (_vp, [_vp, ctypes.POINTER(_u32)]),
+}
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+class FaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"fast_atari error {code}: {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """Load the in-tree CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: run build.py (no CPU fallback exists)")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != FA_OK:
+        raise FaError(rc, lib().fa_last_error().decode())
+
+
+def _u8(a: np.ndarray):
+    return a.ctypes.data_as(_u8p)
+
+
+def device_count() -> int:
+    return int(lib().fa_device_count())
+
+
+class BatchAtariGpu:
+    """n emulated consoles of one ROM, resident on the current CUDA device."""
+
+    def __init__(self, rom: bytes, n: int):
+        L = lib()
+        r = np.frombuffer(bytes(rom), dtype=np.uint8).copy()
+        h = _vp()
+        _check(L.fa_create(_u8(r), len(r), int(n), ctypes.byref(h)))
+        self._h = h
+        self.n = int(n)
+        self.rom = bytes(rom)
+        self._obs = np.zeros((self.n, 128), np.uint8)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().fa_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- the reference method set
+    def num_envs(self) -> int:
+        return int(lib().fa_num_envs(self._h))
+
+    def set_sorted(self, sorted_: bool) -> None:
+        _check(lib().fa_set_sorted(self._h, 1 if sorted_ else 0))
+
+    def reset(self) -> np.ndarray:
+        obs = np.zeros((self.n, 128), np.uint8)
+        _check(lib().fa_reset(self._h, _u8(obs)))
+        return obs
+
+    def step(self, actions, obs: bool = True) -> Optional[np.ndarray]:
+        a = np.ascontiguousarray(actions, dtype=np.uint8).reshape(-1)
+        if a.size != self.n:
+            raise ValueError(f"expected {self.n} actions, got {a.size}")
+        out = np.empty((self.n, 128), np.uint8) if obs else None
+        _check(lib().fa_step(self._h, _u8(a), _u8(out) if obs else None))
+        return out
+
+    def step_multi(self, actions, k: int, obs: bool = True) -> Optional[np.ndarray]:
+        a = np.ascontiguousarray(actions, dtype=np.uint8).reshape(-1)
+        if a.size != k * self.n:
+            raise ValueError(f"expected {k}*{self.n} actions, got {a.size}")
+        out = np.empty((self.n, 128), np.uint8) if obs else None
+        _check(lib().fa_step_multi(self._h, _u8(a), int(k), _u8(out) if obs else None))
+        return out
+
+    def download_states(self) -> np.ndarray:
+        s = np.zeros(self.n, STATE_DTYPE)
+        _check(lib().fa_get_states(self._h, s.ctypes.data))
+        return s
+
+    # ---- extensions
+    def upload_states(self, states: np.ndarray) -> None:
+        s = np.ascontiguousarray(states, dtype=STATE_DTYPE)
+        assert s.size == self.n
+        _check(lib().fa_set_states(self._h, s.ctypes.data))
+
+    def ram(self, idx: int) -> np.ndarray:
+        out = np.zeros(128, np.uint8)
+        _check(lib().fa_get_ram(self._h, int(idx), _u8(out)))
+        return out
+
+    def status(self) -> np.ndarray:
+        out = np.zeros(self.n, np.uint32)
+        _check(lib().fa_get_status(self._h, out.ctypes.data_as(ctypes.POINTER(_u32))))
+        return out
+
+    def snapshot(self) -> np.ndarray:
+        s = np.zeros(1, STATE_DTYPE)
+        _check(lib().fa_get_snapshot(self._h, s.ctypes.data))
+        return s[0]
+
+    def set_episode_frames(self, frames: int) -> None:
+        _check(lib().fa_set_episode_frames(self._h, int(frames)))
+
+    def set_frame_numbers(self, frame_no) -> None:
+        f = np.ascontiguousarray(frame_no, dtype=np.uint32)
+        assert f.size == self.n
+        _check(lib().fa_set_frame_numbers(self._h, f.ctypes.data_as(ctypes.POINTER(_u32))))
+
+    def set_launch(self, block: int = 128, sched="lane", persistent: bool = False) -> None:
+        s = SCHED_NAMES[sched] if isinstance(sched, str) else int(sched)
+        _check(lib().fa_set_launch(self._h, int(block), s, 1 if persistent else 0))
+
+    def get_launch(self):
+        b, s, p = _i(), _i(), _i()
+        _check(lib().fa_get_launch(self._h, ctypes.byref(b), ctypes.byref(s), ctypes.byref(p)))
+        return b.value, s.value, bool(p.value)
+
+    def last_instructions(self) -> int:
+        return int(lib().fa_last_instructions(self._h))
+
+    def step_multi_async(self, d_actions: int, k: int, d_obs: int = 0, stream: int = 0) -> None:
+        """Enqueue k frames from device actions (e.g. torch tensor data_ptr())."""
+        _check(lib().fa_step_multi_async(self._h, _vp(d_actions), int(k), _vp(d_obs or None),
+                                          _vp(stream or None)))
+
+    def synchronize(self) -> None:
+        _check(lib().fa_synchronize(self._h))

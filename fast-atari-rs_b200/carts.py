@@ -1,0 +1,607 @@
+"""Seeded synthetic Atari 2600 carts and action streams.
+
+The reference measures on Breakout.bin (examples/bench_cuda.rs:6), which is not
+available here; these carts stand in for it with the shapes of the benchmark
+configurations: a frame skeleton of 3 VSYNC, 37 VBLANK, 192 visible and 30
+overscan lines, visible lines running seeded basic blocks of legal 6502 ops
+that read SWCHA/INPT4/INPT0/INTIM and mix them into RAM, Fixed 2K/4K, F8, F6
+and F4 bank switching, WSYNC-terminated or DEX/BNE-timed lines, JSR/RTS and
+balanced stack traffic.
+
+Safety rules (so every cart runs forever without an illegal opcode):
+  * only forward branches inside a block; every block ends by falling into
+    its line terminator;
+  * RAM writes go to $82-$EF ($80/$81 belong to the skeleton, $F0-$FF to the
+    stack); TIA writes avoid VSYNC/VBLANK/WSYNC/RSYNC; indexed or indirect
+    writes are preceded by the loads that pin their effective address;
+  * on bank-switched carts no read can reach a hotspot except the skeleton's
+    trampoline, and every bank carries the same skeleton at the same address,
+    so execution continues in the new bank after a switch.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+MASK64 = (1 << 64) - 1
+
+# ----------------------------------------------------------------- RNG
+def splitmix64(x: int) -> int:
+    """SplitMix64 finaliser (Steele, Lea, Flood 2014)."""
+    x = (x + 0x9E3779B97F4A7C15) & MASK64
+    z = x
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK64
+    return z ^ (z >> 31)
+
+
+class Rng:
+    """Counter-based SplitMix64 stream; identical on every host."""
+
+    def __init__(self, seed: int):
+        self.state = splitmix64(seed & MASK64)
+
+    @classmethod
+    def from_state(cls, state: int) -> "Rng":
+        r = cls(0)
+        r.state = state & MASK64
+        return r
+
+    def next(self) -> int:
+        self.state = (self.state + 1) & MASK64
+        return splitmix64(self.state)
+
+    def below(self, n: int) -> int:
+        return self.next() % n
+
+    def range(self, lo: int, hi: int) -> int:      # inclusive
+        return lo + self.below(hi - lo + 1)
+
+    def chance(self, p: float) -> bool:
+        return (self.next() >> 11) * (1.0 / (1 << 53)) < p
+
+    def choice(self, seq):
+        return seq[self.below(len(seq))]
+
+
+def _splitmix64_np(x: np.ndarray) -> np.ndarray:
+    x = x + np.uint64(0x9E3779B97F4A7C15)
+    z = x
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def actions(seed: int, n: int, frames: int, frame0: int = 0, num_actions: int = 18) -> np.ndarray:
+    """int8 actions uniform over 18, frame-major [frames, n]: SplitMix64 of
+    (seed, frame, instance), so any sub-range can be regenerated exactly."""
+    with np.errstate(over="ignore"):
+        f = (np.arange(frame0, frame0 + frames, dtype=np.uint64)[:, None])
+        i = np.arange(n, dtype=np.uint64)[None, :]
+        key = (np.uint64(seed & MASK64) * np.uint64(0xD1B54A32D192ED03)
+               ^ f * np.uint64(0x9E3779B97F4A7C15) ^ i * np.uint64(0xC2B2AE3D27D4EB4F))
+        h = _splitmix64_np(key)
+    return (h % np.uint64(num_actions)).astype(np.uint8)
+
+
+# ------------------------------------------------------------ opcode table
+# (mnemonic, mode) -> opcode, for the 151 legal opcodes.
+_OPS: Dict[Tuple[str, str], int] = {}
+
+
+def _reg(mn, **modes):
+    for mode, op in modes.items():
+        _OPS[(mn, mode)] = op
+
+
+for _mn, _base in (("ORA", 0x00), ("AND", 0x20), ("EOR", 0x40), ("ADC", 0x60),
+                   ("LDA", 0xA0), ("CMP", 0xC0), ("SBC", 0xE0)):
+    _reg(_mn, indx=_base | 0x01, zp=_base | 0x05, imm=_base | 0x09, abs=_base | 0x0D,
+         indy=_base | 0x11, zpx=_base | 0x15, absy=_base | 0x19, absx=_base | 0x1D)
+_reg("STA", indx=0x81, zp=0x85, abs=0x8D, indy=0x91, zpx=0x95, absy=0x99, absx=0x9D)
+for _mn, _base in (("ASL", 0x00), ("ROL", 0x20), ("LSR", 0x40), ("ROR", 0x60)):
+    _reg(_mn, zp=_base | 0x06, acc=_base | 0x0A, abs=_base | 0x0E, zpx=_base | 0x16, absx=_base | 0x1E)
+_reg("DEC", zp=0xC6, abs=0xCE, zpx=0xD6, absx=0xDE)
+_reg("INC", zp=0xE6, abs=0xEE, zpx=0xF6, absx=0xFE)
+_reg("STX", zp=0x86, abs=0x8E, zpy=0x96)
+_reg("LDX", imm=0xA2, zp=0xA6, abs=0xAE, zpy=0xB6, absy=0xBE)
+_reg("STY", zp=0x84, abs=0x8C, zpx=0x94)
+_reg("LDY", imm=0xA0, zp=0xA4, abs=0xAC, zpx=0xB4, absx=0xBC)
+_reg("CPX", imm=0xE0, zp=0xE4, abs=0xEC)
+_reg("CPY", imm=0xC0, zp=0xC4, abs=0xCC)
+_reg("BIT", zp=0x24, abs=0x2C)
+_reg("JMP", abs=0x4C, ind=0x6C)
+_reg("JSR", abs=0x20)
+for _mn, _op in (("BPL", 0x10), ("BMI", 0x30), ("BVC", 0x50), ("BVS", 0x70),
+                 ("BCC", 0x90), ("BCS", 0xB0), ("BNE", 0xD0), ("BEQ", 0xF0)):
+    _reg(_mn, rel=_op)
+for _mn, _op in (("BRK", 0x00), ("RTI", 0x40), ("RTS", 0x60), ("PHP", 0x08), ("PLP", 0x28),
+                 ("PHA", 0x48), ("PLA", 0x68), ("CLC", 0x18), ("SEC", 0x38), ("CLI", 0x58),
+                 ("SEI", 0x78), ("CLV", 0xB8), ("CLD", 0xD8), ("SED", 0xF8), ("DEY", 0x88),
+                 ("TXA", 0x8A), ("TYA", 0x98), ("TXS", 0x9A), ("TAY", 0xA8), ("TAX", 0xAA),
+                 ("TSX", 0xBA), ("INY", 0xC8), ("DEX", 0xCA), ("INX", 0xE8), ("NOP", 0xEA)):
+    _reg(_mn, imp=_op)
+
+assert len(_OPS) == 151 and len(set(_OPS.values())) == 151
+OPCODES = dict(_OPS)
+LEGAL_OPCODES = sorted(_OPS.values())
+_SIZE = {"imp": 1, "acc": 1, "imm": 2, "zp": 2, "zpx": 2, "zpy": 2, "indx": 2, "indy": 2,
+         "rel": 2, "abs": 3, "absx": 3, "absy": 3, "ind": 3}
+
+READ_MN = {"LDA", "ADC", "AND", "CMP", "EOR", "ORA", "SBC", "LDX", "LDY", "CPX", "CPY", "BIT"}
+WRITE_MN = {"STA", "STX", "STY"}
+RMW_MN = {"ASL", "LSR", "ROL", "ROR", "INC", "DEC"}
+
+# Hardware registers used by the skeleton and the blocks.
+VSYNC, VBLANK, WSYNC = 0x00, 0x01, 0x02
+INPT0, INPT4 = 0x08, 0x0C
+SWCHA, SWACNT, SWCHB, INTIM, INSTAT = 0x280, 0x281, 0x282, 0x284, 0x285
+TIM1T, TIM8T, TIM64T, T1024T = 0x294, 0x295, 0x296, 0x297
+LINE_CTR, MIX = 0x80, 0x81
+RAM_W_LO, RAM_W_HI = 0x82, 0xEF                 # writable by blocks
+TIA_WRITABLE = [r for r in range(0x04, 0x2D)]    # not VSYNC/VBLANK/WSYNC/RSYNC
+TIA_READ_REGS = list(range(0x00, 0x0E))
+
+
+# ---------------------------------------------------------------- assembler
+@dataclass
+class Ins:
+    mn: str
+    mode: str
+    arg: object = None          # int, label name, or ("fwd", unit index) for block branches
+
+    def size(self) -> int:
+        return _SIZE[self.mode]
+
+
+class Asm:
+    """Two-pass assembler for one 4K bank image at origin $F000."""
+
+    def __init__(self, origin: int = 0xF000):
+        self.origin = origin
+        self.items: List[object] = []   # Ins | ("label", name) | ("org", addr) | ("bytes", b)
+
+    def label(self, name: str):
+        self.items.append(("label", name))
+
+    def org(self, addr: int):
+        self.items.append(("org", addr))
+
+    def raw(self, b: bytes):
+        self.items.append(("bytes", bytes(b)))
+
+    def ins(self, mn, mode="imp", arg=None):
+        assert (mn, mode) in _OPS, (mn, mode)
+        self.items.append(Ins(mn, mode, arg))
+
+    def assemble(self, size: int, labels_in: Optional[Dict[str, int]] = None):
+        labels: Dict[str, int] = dict(labels_in or {})
+        for _ in range(2):
+            pc = self.origin
+            for it in self.items:
+                if isinstance(it, Ins):
+                    pc += it.size()
+                elif it[0] == "label":
+                    labels[it[1]] = pc
+                elif it[0] == "org":
+                    assert it[1] >= pc, (hex(it[1]), hex(pc))
+                    pc = it[1]
+                else:
+                    pc += len(it[1])
+        img = bytearray(size)
+        pc = self.origin
+        end_limit = self.origin + size
+        for it in self.items:
+            if isinstance(it, Ins):
+                op = _OPS[(it.mn, it.mode)]
+                arg = it.arg
+                if isinstance(arg, str):
+                    arg = labels[arg]
+                if it.mode == "rel":
+                    off = arg - (pc + 2)
+                    assert -128 <= off <= 127, (it, off)
+                    enc = bytes([op, off & 0xFF])
+                elif it.size() == 1:
+                    enc = bytes([op])
+                elif it.size() == 2:
+                    assert 0 <= arg <= 0xFF, (it, arg)
+                    enc = bytes([op, arg])
+                else:
+                    assert 0 <= arg <= 0xFFFF, (it, arg)
+                    enc = bytes([op, arg & 0xFF, arg >> 8])
+                assert pc + len(enc) <= end_limit, "bank overflow"
+                img[(pc - self.origin) % size: (pc - self.origin) % size + len(enc)] = enc
+                pc += len(enc)
+            elif it[0] == "label":
+                pass
+            elif it[0] == "org":
+                pc = it[1]
+            else:
+                b = it[1]
+                img[(pc - self.origin) % size:(pc - self.origin) % size + len(b)] = b
+                pc += len(b)
+        return bytes(img), labels, pc
+
+
+# --------------------------------------------------------------- cart spec
+@dataclass
+class CartSpec:
+    """Parameters of one synthetic cart."""
+    name: str
+    rom_size: int                       # 2048, 4096, 8192, 16384, 32768
+    seed: int
+    wsync_density: float = 1.0          # fraction of visible lines ending in STA WSYNC
+    ops_min: int = 8
+    ops_max: int = 40
+    lines_per_group: int = 16           # distinct line blocks per bank; group loop runs 192/this times
+    subroutines: int = 0                # JSR targets per bank
+    stack_pairs: bool = True            # PHA/PLA, PHP/PLP balanced groups
+    bank_select: str = "cycle"          # "cycle": next bank each group; "data": bank from RAM bits
+
+    @property
+    def nbanks(self) -> int:
+        return max(1, self.rom_size // 4096)
+
+
+@dataclass
+class Cart:
+    spec: CartSpec
+    rom: bytes
+    labels: Dict[str, int] = field(default_factory=dict)
+
+
+class _BlockGen:
+    """Generates one visible-line block as a list of units (lists of Ins)."""
+
+    def __init__(self, rng: Rng, spec: CartSpec, bank: int, subs: List[str]):
+        self.r = rng
+        self.spec = spec
+        self.bank = bank
+        self.banked = spec.nbanks > 1
+        self.subs = subs
+        pool = []
+        for (mn, mode), op in _OPS.items():
+            if mn in ("BRK", "RTI", "RTS", "JMP", "TXS"):
+                continue
+            if mn == "JSR" and not subs:
+                continue
+            if mn in ("PHA", "PLA", "PHP", "PLP") and not spec.stack_pairs:
+                continue
+            pool.append((mn, mode))
+        self.pool = sorted(pool, key=lambda k: _OPS[k])
+
+    # -- operand helpers
+    def ram_w(self) -> int:
+        return self.r.range(RAM_W_LO, RAM_W_HI)
+
+    def ram_r(self) -> int:
+        return self.r.range(0x80, 0xFF)
+
+    def zp_read(self) -> int:
+        return self.ram_r() if self.r.chance(0.8) else self.r.choice(TIA_READ_REGS) | (0x40 if self.r.chance(0.2) else 0)
+
+    def tia_w(self) -> int:
+        return self.r.choice(TIA_WRITABLE) | (0x40 if self.r.chance(0.2) else 0)
+
+    def rom_addr(self, span: int = 0) -> int:
+        hi = 0xFEFF - span if self.banked else 0xFFFF - span
+        return self.r.range(0xF000, hi)
+
+    def abs_read(self) -> int:
+        k = self.r.below(6)
+        if k <= 1:
+            return self.rom_addr()
+        if k == 2:
+            return self.r.choice([0x0080, 0x0180]) + self.r.below(0x80)
+        if k == 3:
+            return self.r.choice([0x0480, 0x0880, 0x0C80]) + self.r.below(0x80)   # reads 0
+        if k == 4:
+            return self.r.choice([SWCHA, SWCHB, INTIM, INSTAT, SWACNT, 0x0283, 0x0380 | self.r.below(8)])
+        return self.r.choice(TIA_READ_REGS) | self.r.choice([0x000, 0x040, 0x100, 0x240])
+
+    def abs_write(self) -> int:
+        k = self.r.below(5)
+        if k <= 1:
+            return self.r.choice([0x0000, 0x0100, 0x0400, 0x0500, 0x0900]) + self.ram_w()
+        if k == 2:
+            return self.tia_w() | self.r.choice([0x000, 0x100])
+        if k == 3:
+            return self.r.choice([TIM1T, TIM8T, TIM64T, T1024T, SWACNT, 0x0280, 0x0282, 0x0283])
+        return self.rom_addr()          # writes to ROM space are ignored (non-hotspot)
+
+    def abs_rmw(self) -> int:
+        k = self.r.below(4)
+        if k <= 1:
+            return self.r.choice([0x0000, 0x0100]) + self.ram_w()
+        if k == 2:
+            return self.tia_w()
+        return self.rom_addr()
+
+    # -- units
+    def unit(self) -> List[Ins]:
+        mn, mode = self.r.choice(self.pool)
+        r = self.r
+        if mode in ("imp", "acc"):
+            if mn in ("PHA", "PHP", "PLA", "PLP"):
+                inner = [self.simple_unit() for _ in range(r.below(3))]
+                push = "PHA" if mn in ("PHA", "PLA") else "PHP"
+                pull = "PLA" if push == "PHA" else "PLP"
+                return [Ins(push, "imp")] + [i for u in inner for i in u] + [Ins(pull, "imp")]
+            return [Ins(mn, mode)]
+        if mode == "rel":
+            return [Ins(mn, "rel", ("fwd", r.range(1, 4)))]
+        if mn == "JSR":
+            return [Ins("JSR", "abs", r.choice(self.subs))]
+        return self.memory_unit(mn, mode)
+
+    def simple_unit(self) -> List[Ins]:
+        while True:
+            mn, mode = self.r.choice(self.pool)
+            if mode in ("rel",) or mn in ("JSR", "PHA", "PHP", "PLA", "PLP"):
+                continue
+            if mode in ("imp", "acc"):
+                return [Ins(mn, mode)]
+            return self.memory_unit(mn, mode)
+
+    def memory_unit(self, mn: str, mode: str) -> List[Ins]:
+        r = self.r
+        kind = "r" if mn in READ_MN else "w" if mn in WRITE_MN else "m"
+        if mode == "imm":
+            return [Ins(mn, "imm", r.below(256))]
+        if mode == "zp":
+            if kind == "r":
+                return [Ins(mn, "zp", self.zp_read())]
+            a = self.tia_w() if r.chance(0.15) else self.ram_w()
+            return [Ins(mn, "zp", a)]
+        if mode in ("zpx", "zpy"):
+            idx = "X" if mode == "zpx" else "Y"
+            if kind == "r":
+                return [Ins(mn, mode, self.ram_r())]
+            t, k = self.ram_w(), r.below(256)
+            return [Ins("LD" + idx, "imm", k), Ins(mn, mode, (t - k) & 0xFF)]
+        if mode == "abs":
+            a = self.abs_read() if kind == "r" else self.abs_write() if kind == "w" else self.abs_rmw()
+            return [Ins(mn, "abs", a)]
+        if mode in ("absx", "absy"):
+            idx = "X" if mode == "absx" else "Y"
+            if mn == "LDX":
+                idx = "Y"
+            if kind == "r":
+                base = r.choice([self.rom_addr(255), 0x0000 + r.below(0x100), 0x0280,
+                                 0x0080 + r.below(0x80)])
+                return [Ins(mn, mode, base)]
+            t, k = self.r.choice([0x0000, 0x0100]) + self.ram_w(), r.below(0x60)
+            return [Ins("LD" + idx, "imm", k), Ins(mn, mode, t - k)]
+        if mode == "indx":
+            if kind == "r" and not self.banked and r.chance(0.5):
+                return [Ins(mn, "indx", r.below(256))]
+            t = self.ptr_target(kind)
+            p, k = self.r.range(RAM_W_LO, RAM_W_HI - 1), r.below(256)
+            return [Ins("LDA", "imm", t & 0xFF), Ins("STA", "zp", p),
+                    Ins("LDA", "imm", t >> 8), Ins("STA", "zp", p + 1),
+                    Ins("LDX", "imm", k)] + ([Ins("TXA", "imp")] if mn == "STA" else []) + \
+                   [Ins(mn, "indx", (p - k) & 0xFF)]
+        if mode == "indy":
+            if kind == "r" and not self.banked and r.chance(0.5):
+                return [Ins(mn, "indy", self.ram_r())]
+            t = self.ptr_target(kind)
+            k = r.below(0x20)
+            base = t - k
+            p = self.r.range(RAM_W_LO, RAM_W_HI - 1)
+            return [Ins("LDA", "imm", base & 0xFF), Ins("STA", "zp", p),
+                    Ins("LDA", "imm", (base >> 8) & 0xFF), Ins("STA", "zp", p + 1),
+                    Ins("LDY", "imm", k)] + ([Ins("TYA", "imp")] if mn == "STA" else []) + \
+                   [Ins(mn, "indy", p)]
+        raise AssertionError((mn, mode))
+
+    def ptr_target(self, kind: str) -> int:
+        if kind == "r":
+            return self.r.choice([self.rom_addr(), 0x0080 + self.r.below(0x80), SWCHA, INTIM,
+                                  0x0480 + self.r.below(0x80), INPT4])
+        # a write target: RAM or one of its mirrors, never straddling a page
+        return self.r.choice([0x0000, 0x0100, 0x0400, 0x0D00]) + self.r.range(RAM_W_LO + 0x20, RAM_W_HI)
+
+    def mix_unit(self) -> List[Ins]:
+        src = self.r.choice([("abs", SWCHA), ("zp", INPT4), ("zp", INPT0), ("abs", INTIM), ("abs", SWCHB)])
+        op = self.r.choice(["EOR", "ADC", "ORA", "SBC", "AND"])
+        return [Ins("LDA", src[0], src[1]), Ins(op, "zp", self.ram_r()), Ins("STA", "zp", self.ram_w())]
+
+    def block(self) -> List[List[Ins]]:
+        target = self.r.range(self.spec.ops_min, self.spec.ops_max)
+        units: List[List[Ins]] = [self.mix_unit()]
+        n = 3
+        while n < target:
+            u = self.unit()
+            units.insert(self.r.below(len(units) + 1), u) if self.r.chance(0.2) else units.append(u)
+            n += len(u)
+        if self.r.chance(0.5):
+            units.append([Ins("LDA", "zp", self.ram_r()), Ins(self.r.choice(["BMI", "BPL", "BEQ", "BNE"]),
+                                                                 "rel", ("fwd", self.r.range(1, 3)))])
+            units.append(self.simple_unit())
+        return units
+
+
+def _emit_block(asm: Asm, units: List[List[Ins]], tag: str):
+    """Emit units; ("fwd", d) branch args become labels d units ahead (clamped
+    to the block end), so every branch is forward and lands on a unit start."""
+    nu = len(units)
+    for ui, u in enumerate(units):
+        asm.label(f"{tag}_u{ui}")
+        for ins in u:
+            if isinstance(ins.arg, tuple) and ins.arg[0] == "fwd":
+                dest = min(ui + ins.arg[1], nu)
+                asm.ins(ins.mn, "rel", f"{tag}_u{dest}")
+            else:
+                asm.ins(ins.mn, ins.mode, ins.arg)
+    asm.label(f"{tag}_u{nu}")
+
+
+def _wsync_lines(asm: Asm, n: int, tag: str):
+    asm.ins("LDX", "imm", n)
+    asm.label(tag)
+    asm.ins("STA", "zp", WSYNC)
+    asm.ins("DEX")
+    asm.ins("BNE", "rel", tag)
+
+
+def _hotspots(nbanks: int) -> List[int]:
+    first = {2: 0xFFF8, 4: 0xFFF6, 8: 0xFFF4}[nbanks]
+    return [first + b for b in range(nbanks)]
+
+
+def build_cart(spec: CartSpec) -> Cart:
+    """Assemble the cart.  All banks share the skeleton at identical
+    addresses; the line blocks and subroutines differ per bank.  Each bank is
+    generated twice from the same RNG state: once to measure its block
+    region, then with the region padded to the largest one."""
+    assert spec.rom_size in (2048, 4096, 8192, 16384, 32768)
+    assert 192 % spec.lines_per_group == 0
+    nb = spec.nbanks
+    bank_size = min(spec.rom_size, 4096)
+    groups = 192 // spec.lines_per_group
+    rng = Rng(spec.seed * 0x10001 + spec.rom_size)
+    # Per-line terminator choice is shared by all banks (same line structure).
+    term = [rng.chance(spec.wsync_density) for _ in range(spec.lines_per_group)]
+    for _attempt in range(16):
+        starts = [rng.next() for _ in range(nb)]
+        try:
+            ends = []
+            for b in range(nb):
+                asm = _bank_asm(spec, b, nb, Rng.from_state(starts[b]), term, groups, None)
+                ends.append(asm.assemble(bank_size)[1]["region_end"])
+            region_end = max(ends)
+            images, labels = [], {}
+            for b in range(nb):
+                asm = _bank_asm(spec, b, nb, Rng.from_state(starts[b]), term, groups, region_end)
+                img, labels, _ = asm.assemble(bank_size)
+                images.append(img)
+        except AssertionError:
+            continue
+        rom = b"".join(images)
+        assert len(rom) == spec.rom_size
+        return Cart(spec, rom, labels)
+    raise RuntimeError(f"cart {spec.name}: code does not fit in {bank_size} bytes")
+
+
+def _bank_asm(spec: CartSpec, b: int, nb: int, rng: Rng, term, groups: int,
+              region_end: Optional[int]) -> Asm:
+    bank_size = min(spec.rom_size, 4096)
+    asm = Asm(0xF000)
+    # --- reset: SEI; CLD; clear RAM $80-$FF; SP=$FF
+    asm.label("reset")
+    asm.ins("SEI"); asm.ins("CLD")
+    asm.ins("LDA", "imm", 0)
+    asm.ins("LDX", "imm", 0x7F)
+    asm.label("clr")
+    asm.ins("STA", "zpx", 0x80)
+    asm.ins("DEX")
+    asm.ins("BPL", "rel", "clr")
+    asm.ins("LDX", "imm", 0xFF)
+    asm.ins("TXS")
+    # --- frame: VSYNC (3 lines)
+    asm.label("frame")
+    asm.ins("LDA", "imm", 0x02)
+    asm.ins("STA", "zp", VSYNC)
+    asm.ins("STA", "zp", WSYNC); asm.ins("STA", "zp", WSYNC); asm.ins("STA", "zp", WSYNC)
+    asm.ins("LDA", "imm", 0x00)
+    asm.ins("STA", "zp", VSYNC)
+    # --- VBLANK (37 lines): dump paddles, set the interval timer
+    asm.ins("LDA", "imm", 0x82)
+    asm.ins("STA", "zp", VBLANK)
+    asm.ins("LDA", "imm", 43)
+    asm.ins("STA", "abs", TIM64T)
+    _wsync_lines(asm, 37, "vbl")
+    asm.ins("LDA", "imm", 0x00)
+    asm.ins("STA", "zp", VBLANK)
+    # --- visible: groups x lines_per_group lines
+    asm.ins("LDA", "imm", groups)
+    asm.ins("STA", "zp", LINE_CTR)
+    asm.label("vis_loop")
+    gen = _BlockGen(rng, spec, b, [f"sub{i}" for i in range(spec.subroutines)])
+    for j in range(spec.lines_per_group):
+        _emit_block(asm, gen.block(), f"b{j}")
+        if term[j]:
+            asm.ins("STA", "zp", WSYNC)
+        else:
+            asm.ins("LDX", "imm", 1 + rng.below(8))
+            asm.label(f"dly{j}")
+            asm.ins("DEX")
+            asm.ins("BNE", "rel", f"dly{j}")
+    asm.ins("JMP", "abs", "group_end")
+    asm.label("region_end")
+    if region_end is not None:
+        asm.org(region_end)
+    # --- group end: trampoline (same address in every bank), loop
+    asm.label("group_end")
+    if nb > 1:
+        hs = _hotspots(nb)
+        if spec.bank_select == "data":
+            asm.ins("LDA", "zp", 0x80 + 2 + (b * 7) % 0x6D)
+            asm.ins("LSR", "acc")
+            asm.ins("BCC", "rel", "tr_b")
+            asm.ins("BIT", "abs", hs[(b + 1) % nb])
+            asm.ins("JMP", "abs", "tr_done")
+            asm.label("tr_b")
+            asm.ins("BIT", "abs", hs[(b + nb - 1) % nb] if nb > 2 else hs[b])
+            asm.label("tr_done")
+        else:
+            asm.ins("BIT", "abs", hs[(b + 1) % nb])
+    asm.ins("DEC", "zp", LINE_CTR)
+    asm.ins("BEQ", "rel", "vis_done")
+    asm.ins("JMP", "abs", "vis_loop")
+    asm.label("vis_done")
+    # --- overscan (30 lines); mix INTIM into RAM
+    asm.ins("LDA", "imm", 0x02)
+    asm.ins("STA", "zp", VBLANK)
+    _wsync_lines(asm, 30, "ovs")
+    asm.ins("LDA", "abs", INTIM)
+    asm.ins("EOR", "zp", MIX)
+    asm.ins("STA", "zp", MIX)
+    asm.ins("JMP", "abs", "frame")
+    # --- subroutines (bank-specific)
+    for i in range(spec.subroutines):
+        asm.label(f"sub{i}")
+        sg = _BlockGen(rng, CartSpec(spec.name, spec.rom_size, 0, ops_min=4, ops_max=12,
+                                     stack_pairs=spec.stack_pairs), b, [])
+        units = sg.block()
+        _emit_block(asm, units, f"s{i}")
+        asm.ins("RTS")
+    # --- vectors
+    asm.org(0xF000 + bank_size - 4)
+    asm.raw(bytes([0x00, 0xF0, 0x00, 0xF0]))
+    return asm
+
+
+# ------------------------------------------------------- benchmark carts
+def plain_cart(seed: int = 1) -> Cart:
+    """4K Fixed, every visible line ends in STA WSYNC, 8-40 ops per block."""
+    return build_cart(CartSpec("plain_4k_fixed", 4096, seed, wsync_density=1.0,
+                               ops_min=8, ops_max=40))
+
+
+def divergence_cart(seed: int = 2) -> Cart:
+    """8K F8, no WSYNC in the visible kernel (DEX/BNE-timed lines), 20-60 ops,
+    JSR/RTS, PHA/PLA, data-dependent bank switch every 16 lines."""
+    return build_cart(CartSpec("divergence_8k_f8", 8192, seed, wsync_density=0.0,
+                               ops_min=20, ops_max=60, subroutines=4, bank_select="data"))
+
+
+def mixed_carts(seed: int = 3) -> List[Cart]:
+    """2K Fixed / 8K F8 / 16K F6 / 32K F4 with WSYNC density 100/50/10/0%."""
+    out = []
+    for i, (size, dens) in enumerate(((2048, 1.0), (8192, 0.5), (16384, 0.1), (32768, 0.0))):
+        out.append(build_cart(CartSpec(f"mixed_{size // 1024}k", size, seed + 17 * i,
+                                       wsync_density=dens, ops_min=8, ops_max=40,
+                                       subroutines=2 if size > 4096 else 0)))
+    return out
+
+
+MIXED_COUNTS = (100_000, 30_000, 5_000, 500)
+
+
+def scale_cart(seed: int = 4) -> Cart:
+    """32K F4, 0% WSYNC lines, bank switch every 8 lines."""
+    return build_cart(CartSpec("scale_32k_f4", 32768, seed, wsync_density=0.0,
+                               ops_min=8, ops_max=40, lines_per_group=8, subroutines=2))

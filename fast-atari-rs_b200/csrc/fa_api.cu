@@ -1,0 +1,558 @@
+// fa_api.cu — C ABI of the batched Atari core: the `BatchAtariGpu` handle.
+//
+// Mirrors src/cuda_env.rs:99-191 of the reference: a handle owns one ROM and
+// n instances resident in HBM; reset/step/step_multi/download_states act on
+// all of them.  Differences by design: state is structure-of-arrays, reset
+// runs on the device from one post-reset snapshot, the action and
+// observation buffers are preallocated (pinned on the host), and errors are
+// status codes rather than panics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/fast_atari.h"
+#include "fa_internal.h"
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+
+int fa_fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define FA_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fa_fail(FA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));       \
+    } while (0)
+
+extern "C" const char* fa_last_error(void) { return g_err.c_str(); }
+extern "C" const char* fa_version(void) { return "fast-atari-b200 0.1 (sm_100a)"; }
+
+extern "C" int fa_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return n;
+}
+
+// ------------------------------------------------------------------ packing
+static inline uint32_t b4(uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+    return (a & 0xFFu) | ((b & 0xFFu) << 8) | ((c & 0xFFu) << 16) | ((d & 0xFFu) << 24);
+}
+
+// Private bytes of one instance (RAM then the write-only TIA registers).
+static void priv_from_state(const fa_state& s, uint8_t* pb)
+{
+    memset(pb, 0, FA_PRIV_BYTES);
+    memcpy(pb, s.ram, 128);
+    const uint8_t cx[8] = { s.cxm0p, s.cxm1p, s.cxp0fb, s.cxp1fb, s.cxm0fb, s.cxm1fb, s.cxblpf, s.cxppmm };
+    memcpy(pb + PB_CX, cx, 8);
+    const uint16_t pos[5] = { s.pos_p0, s.pos_p1, s.pos_m0, s.pos_m1, s.pos_bl };
+    memcpy(pb + PB_POS, pos, 10);
+    const uint8_t hm[5] = { s.hmp0, s.hmp1, s.hmm0, s.hmm1, s.hmbl };
+    memcpy(pb + PB_HM, hm, 5);
+    pb[PB_GRP0] = s.grp0; pb[PB_GRP1] = s.grp1; pb[PB_GRP0_OLD] = s.grp0_old; pb[PB_GRP1_OLD] = s.grp1_old;
+    pb[PB_ENAM0] = !!s.enam0; pb[PB_ENAM1] = !!s.enam1; pb[PB_ENABL] = !!s.enabl; pb[PB_ENABL_OLD] = !!s.enabl_old;
+    pb[PB_VDELP0] = !!s.vdelp0; pb[PB_VDELP1] = !!s.vdelp1; pb[PB_VDELBL] = !!s.vdelbl;
+    pb[PB_RESMP0] = !!s.resmp0; pb[PB_RESMP1] = !!s.resmp1;
+    pb[PB_NUSIZ0] = s.nusiz0; pb[PB_NUSIZ1] = s.nusiz1;
+    pb[PB_COLUP0] = s.colup0; pb[PB_COLUP1] = s.colup1; pb[PB_COLUPF] = s.colupf; pb[PB_COLUBK] = s.colubk;
+    pb[PB_CTRLPF] = s.ctrlpf; pb[PB_REFP0] = !!s.refp0; pb[PB_REFP1] = !!s.refp1;
+    pb[PB_PF0] = s.pf0; pb[PB_PF1] = s.pf1; pb[PB_PF2] = s.pf2;
+}
+
+void fa_pack_column(const fa_state& s, uint32_t* col, size_t stride)
+{
+    uint8_t pb[FA_PRIV_BYTES];
+    priv_from_state(s, pb);
+    for (uint32_t w = 0; w < FA_PRIV_WORDS; w++) {
+        uint32_t v;
+        memcpy(&v, pb + 4 * w, 4);
+        col[w * stride] = v;
+    }
+    col[R_AXYS * stride] = b4(s.a, s.x, s.y, s.sp);
+    col[R_PC * stride] = (uint32_t)s.pc | ((uint32_t)s.status << 16) | ((uint32_t)s.bank << 24);
+    col[R_CYC_LO * stride] = (uint32_t)s.cycles;
+    col[R_CYC_HI * stride] = (uint32_t)(s.cycles >> 32);
+    col[R_PIA0 * stride] = b4(s.port_a_output, s.port_a_ddr, s.port_a_input, s.port_b_output);
+    col[R_PIA1 * stride] = b4(s.port_b_ddr, s.port_b_input, !!s.timer_underflow, !!s.paddle_dumped);
+    col[R_TIMER * stride] = (uint32_t)s.timer_value | ((uint32_t)s.timer_prescaler << 16);
+    col[R_SELPC * stride] = (uint32_t)s.timer_prescaler_select | ((uint32_t)s.paddle_counter << 16);
+    col[R_TIA0 * stride] = (uint32_t)s.tia_clock | ((uint32_t)s.tia_scanline << 16);
+    col[R_TIA1 * stride] = b4(!!s.tia_wsync, !!s.tia_frame_complete, s.tia_vsync, s.tia_vblank);
+    col[R_TIA2 * stride] = b4(!!s.inpt4, !!s.inpt5, s.paddle0, s.paddle1);
+    col[R_FRAME * stride] = s.frame_no;
+    col[R_STATUS * stride] = s.run_status;
+}
+
+void fa_unpack_column(const uint32_t* col, size_t stride, int scheme, fa_state& s)
+{
+    memset(&s, 0, sizeof(s));
+    uint8_t pb[FA_PRIV_BYTES];
+    for (uint32_t w = 0; w < FA_PRIV_WORDS; w++) {
+        uint32_t v = col[w * stride];
+        memcpy(pb + 4 * w, &v, 4);
+    }
+    memcpy(s.ram, pb, 128);
+    s.cxm0p = pb[PB_CX + 0]; s.cxm1p = pb[PB_CX + 1]; s.cxp0fb = pb[PB_CX + 2]; s.cxp1fb = pb[PB_CX + 3];
+    s.cxm0fb = pb[PB_CX + 4]; s.cxm1fb = pb[PB_CX + 5]; s.cxblpf = pb[PB_CX + 6]; s.cxppmm = pb[PB_CX + 7];
+    uint16_t pos[5];
+    memcpy(pos, pb + PB_POS, 10);
+    s.pos_p0 = pos[0]; s.pos_p1 = pos[1]; s.pos_m0 = pos[2]; s.pos_m1 = pos[3]; s.pos_bl = pos[4];
+    s.hmp0 = pb[PB_HM + 0]; s.hmp1 = pb[PB_HM + 1]; s.hmm0 = pb[PB_HM + 2]; s.hmm1 = pb[PB_HM + 3];
+    s.hmbl = pb[PB_HM + 4];
+    s.grp0 = pb[PB_GRP0]; s.grp1 = pb[PB_GRP1]; s.grp0_old = pb[PB_GRP0_OLD]; s.grp1_old = pb[PB_GRP1_OLD];
+    s.enam0 = pb[PB_ENAM0]; s.enam1 = pb[PB_ENAM1]; s.enabl = pb[PB_ENABL]; s.enabl_old = pb[PB_ENABL_OLD];
+    s.vdelp0 = pb[PB_VDELP0]; s.vdelp1 = pb[PB_VDELP1]; s.vdelbl = pb[PB_VDELBL];
+    s.resmp0 = pb[PB_RESMP0]; s.resmp1 = pb[PB_RESMP1];
+    s.nusiz0 = pb[PB_NUSIZ0]; s.nusiz1 = pb[PB_NUSIZ1];
+    s.colup0 = pb[PB_COLUP0]; s.colup1 = pb[PB_COLUP1]; s.colupf = pb[PB_COLUPF]; s.colubk = pb[PB_COLUBK];
+    s.ctrlpf = pb[PB_CTRLPF]; s.refp0 = pb[PB_REFP0]; s.refp1 = pb[PB_REFP1];
+    s.pf0 = pb[PB_PF0]; s.pf1 = pb[PB_PF1]; s.pf2 = pb[PB_PF2];
+    uint32_t w;
+    w = col[R_AXYS * stride]; s.a = w; s.x = w >> 8; s.y = w >> 16; s.sp = w >> 24;
+    w = col[R_PC * stride]; s.pc = (uint16_t)w; s.status = (uint8_t)(w >> 16); s.bank = (uint8_t)(w >> 24);
+    s.cycles = (uint64_t)col[R_CYC_LO * stride] | ((uint64_t)col[R_CYC_HI * stride] << 32);
+    w = col[R_PIA0 * stride]; s.port_a_output = w; s.port_a_ddr = w >> 8; s.port_a_input = w >> 16; s.port_b_output = w >> 24;
+    w = col[R_PIA1 * stride]; s.port_b_ddr = w; s.port_b_input = w >> 8; s.timer_underflow = w >> 16; s.paddle_dumped = w >> 24;
+    w = col[R_TIMER * stride]; s.timer_value = (uint16_t)w; s.timer_prescaler = (uint16_t)(w >> 16);
+    w = col[R_SELPC * stride]; s.timer_prescaler_select = (uint16_t)w; s.paddle_counter = (uint16_t)(w >> 16);
+    w = col[R_TIA0 * stride]; s.tia_clock = (uint16_t)w; s.tia_scanline = (uint16_t)(w >> 16);
+    w = col[R_TIA1 * stride]; s.tia_wsync = w; s.tia_frame_complete = w >> 8; s.tia_vsync = w >> 16; s.tia_vblank = w >> 24;
+    w = col[R_TIA2 * stride]; s.inpt4 = w; s.inpt5 = w >> 8; s.paddle0 = w >> 16; s.paddle1 = w >> 24;
+    s.frame_no = col[R_FRAME * stride];
+    s.run_status = col[R_STATUS * stride];
+    s.scheme = (uint8_t)scheme;
+}
+
+void fa_power_on_column(const uint8_t* img, uint32_t nbanks, int scheme, uint32_t* col)
+{
+    // HeadlessBus::new (src/atari.rs:410-430): power-on bank is the last one;
+    // Cpu::reset (src/cpu.rs:125-134) reads the vector at $FFFC/$FFFD.
+    fa_state s;
+    memset(&s, 0, sizeof(s));
+    const uint32_t bank = scheme == FA_SCHEME_FIXED ? 0u : nbanks - 1u;
+    s.bank = (uint8_t)bank;
+    s.pc = (uint16_t)(img[(bank << 12) | 0xFFC] | (img[(bank << 12) | 0xFFD] << 8));
+    s.sp = 0xFD;
+    s.port_a_input = 0xFF;                   // Pia::default, src/pia.rs:46-62
+    s.port_b_input = 0x3F;
+    s.timer_prescaler = 1;
+    s.timer_prescaler_select = 1;
+    s.inpt4 = 1;                             // HeadlessTia::default, src/headless_tia.rs:90-118
+    s.inpt5 = 1;
+    fa_pack_column(s, col, 1);
+}
+
+// ------------------------------------------------------------------ handle
+struct fa_handle {
+    int device = 0;
+    int sms = 148;
+    size_t n = 0;
+    uint32_t stride = 0;
+    int scheme = 0;
+    uint32_t nbanks = 1, hot_lo = 0x2000;
+    std::vector<uint8_t> image;        // host copy of the bank image
+    uint8_t* d_rom = nullptr;
+    uint32_t* d_state = nullptr;
+    uint32_t* d_snap = nullptr;        // post-reset column (FA_ROWS words)
+    bool have_snap = false;
+    uint8_t* d_actions = nullptr;
+    size_t actions_cap = 0;
+    uint8_t* d_obs = nullptr;
+    uint32_t* d_err = nullptr;         // [0] error word, [1] work-queue counter
+    unsigned long long* d_instr = nullptr;
+    uint8_t* h_actions = nullptr;      // pinned staging
+    size_t h_actions_cap = 0;
+    uint8_t* h_obs = nullptr;          // pinned, n*128
+    cudaStream_t stream = nullptr;
+    int block = 128;
+    int sched = FA_SCHED_LANE;
+    bool persistent = false;
+    uint32_t episode_frames = 0;
+    unsigned long long last_instr = 0;
+};
+
+static int rom_len_ok(size_t len)          // lengths HeadlessBus::new accepts (src/atari.rs:410-449)
+{
+    if (len == 0) return 0;
+    switch (fa_detect_scheme(len)) {
+    case FA_SCHEME_FIXED: return 1;
+    case FA_SCHEME_F8: return len >= 8192;
+    case FA_SCHEME_F6: return len >= 16384;
+    default: return len >= 32768;
+    }
+}
+
+// 4 KiB-per-bank image of a ROM: Fixed carts mirror into one 4K window
+// (HeadlessBus::load_bank, src/atari.rs:433-449); banked carts use their
+// first nbanks * 4 KiB.
+int fa_make_bank_image(const uint8_t* rom, size_t len, std::vector<uint8_t>& img, int& scheme)
+{
+    if (!rom || !rom_len_ok(len))
+        return fa_fail(FA_ERR_BAD_ROM, "ROM length %zu cannot be constructed (reference panics)", len);
+    scheme = fa_detect_scheme(len);
+    const uint32_t nb = fa_nbanks(scheme);
+    img.resize((size_t)nb * 4096);
+    if (scheme == FA_SCHEME_FIXED)
+        for (size_t i = 0; i < 4096; i++) img[i] = rom[i % len];
+    else
+        memcpy(img.data(), rom, img.size());
+    return FA_OK;
+}
+
+static void free_handle(fa_handle* h)
+{
+    if (!h) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->d_rom);
+    cudaFree(h->d_state);
+    cudaFree(h->d_snap);
+    cudaFree(h->d_actions);
+    cudaFree(h->d_obs);
+    cudaFree(h->d_err);
+    cudaFree(h->d_instr);
+    cudaFreeHost(h->h_actions);
+    cudaFreeHost(h->h_obs);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    cudaSetDevice(prev);
+    delete h;
+}
+
+#define CHECK_H(h)                                                                     \
+    do {                                                                               \
+        if (!(h)) return fa_fail(FA_ERR_INVALID, "null handle");                     \
+        cudaError_t e_ = cudaSetDevice((h)->device);                                   \
+        if (e_ != cudaSuccess) return fa_fail(FA_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" int fa_create(const uint8_t* rom, size_t rom_len, size_t n, fa_handle** out)
+{
+    if (!out) return fa_fail(FA_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (n == 0 || n > (size_t)0x7FFFFFFF) return fa_fail(FA_ERR_INVALID, "bad instance count %zu", n);
+    if (fa_device_count() < 1) return fa_fail(FA_ERR_NO_DEVICE, "no CUDA device visible");
+    fa_handle* h = new (std::nothrow) fa_handle();
+    if (!h) return fa_fail(FA_ERR_CAPACITY, "out of host memory");
+    int rc = fa_make_bank_image(rom, rom_len, h->image, h->scheme);
+    if (rc) { delete h; return rc; }
+    h->nbanks = fa_nbanks(h->scheme);
+    h->hot_lo = fa_hot_lo(h->scheme);
+    h->n = n;
+    h->stride = (uint32_t)((n + 31) & ~(size_t)31);
+    cudaGetDevice(&h->device);
+    cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
+    // Default launch shape: the plain per-frame form, 128 threads per CTA.
+    h->block = 128;
+    cudaError_t e = cudaSuccess;
+#define TRY(call) do { e = (call); if (e != cudaSuccess) { free_handle(h); \
+        return fa_fail(FA_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e)); } } while (0)
+    TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    TRY(cudaMalloc(&h->d_rom, h->image.size()));
+    TRY(cudaMemcpy(h->d_rom, h->image.data(), h->image.size(), cudaMemcpyHostToDevice));
+    const size_t state_words = (size_t)FA_ROWS * h->stride;
+    TRY(cudaMalloc(&h->d_state, state_words * 4));
+    TRY(cudaMemset(h->d_state, 0, state_words * 4));
+    TRY(cudaMalloc(&h->d_snap, FA_ROWS * 4));
+    TRY(cudaMalloc(&h->d_obs, n * 128));
+    TRY(cudaMalloc(&h->d_err, 2 * sizeof(uint32_t)));
+    TRY(cudaMemset(h->d_err, 0, 2 * sizeof(uint32_t)));
+    TRY(cudaMalloc(&h->d_instr, sizeof(unsigned long long)));
+    TRY(cudaMallocHost(&h->h_obs, n * 128));
+    // Every instance starts zeroed and marked not-reset (stepping it is a no-op).
+    {
+        std::vector<uint32_t> st(h->stride, FA_STATUS_NOT_RESET);
+        TRY(cudaMemcpy(h->d_state + (size_t)R_STATUS * h->stride, st.data(), h->stride * 4, cudaMemcpyHostToDevice));
+    }
+#undef TRY
+    *out = h;
+    return FA_OK;
+}
+
+extern "C" void fa_destroy(fa_handle* h) { free_handle(h); }
+
+extern "C" size_t fa_num_envs(const fa_handle* h) { return h ? h->n : 0; }
+
+extern "C" int fa_set_sorted(fa_handle* h, int sorted)
+{
+    if (!h) return fa_fail(FA_ERR_INVALID, "null handle");
+    h->sched = sorted ? FA_SCHED_MATCH : FA_SCHED_LANE;
+    return FA_OK;
+}
+
+static int ensure_actions(fa_handle* h, size_t bytes)
+{
+    if (bytes <= h->actions_cap) return FA_OK;
+    cudaFree(h->d_actions);
+    cudaFreeHost(h->h_actions);
+    h->d_actions = nullptr;
+    h->h_actions = nullptr;
+    h->actions_cap = h->h_actions_cap = 0;
+    FA_CUDA(cudaMalloc(&h->d_actions, bytes));
+    FA_CUDA(cudaMallocHost(&h->h_actions, bytes));
+    h->actions_cap = h->h_actions_cap = bytes;
+    return FA_OK;
+}
+
+static FaGroup make_group(fa_handle* h, const uint8_t* d_actions, uint32_t k, uint8_t* d_obs)
+{
+    FaGroup g;
+    memset(&g, 0, sizeof(g));
+    g.rom = h->d_rom;
+    g.snapshot = h->have_snap ? h->d_snap : nullptr;
+    g.state = h->d_state;
+    g.actions = d_actions;
+    g.obs = d_obs;
+    g.stride = h->stride;
+    g.n = (uint32_t)h->n;
+    g.act_stride = (uint32_t)h->n;
+    g.nbanks = h->nbanks;
+    g.hot_lo = h->hot_lo;
+    g.k = k;
+    g.episode_frames = h->episode_frames;
+    g.sched = (uint32_t)h->sched;
+    g.unit_begin = 0;
+    return g;
+}
+
+// Enqueue one launch over all instances of the handle.
+static int enqueue_run(fa_handle* h, const FaGroup& g, cudaStream_t s)
+{
+    FaLaunch L;
+    memset(&L, 0, sizeof(L));
+    L.g[0] = g;
+    L.ngroups = 1;
+    L.nunits = (uint32_t)((g.n + h->block - 1) / h->block);
+    L.rom_bytes_max = h->nbanks * 4096u;
+    L.err = h->d_err;
+    L.instr = h->d_instr;
+    if (h->persistent) {
+        L.queue = h->d_err + 1;
+        FA_CUDA(cudaMemsetAsync(L.queue, 0, sizeof(uint32_t), s));
+    }
+    FA_CUDA(fa_launch_run(L, h->block, h->persistent, h->sms, s));
+    return FA_OK;
+}
+
+static int finish(fa_handle* h)
+{
+    FA_CUDA(cudaStreamSynchronize(h->stream));
+    uint32_t err[2] = { 0, 0 };
+    FA_CUDA(cudaMemcpy(err, h->d_err, sizeof(err), cudaMemcpyDeviceToHost));
+    FA_CUDA(cudaMemcpy(&h->last_instr, h->d_instr, sizeof(h->last_instr), cudaMemcpyDeviceToHost));
+    if (err[0]) {
+        cudaMemset(h->d_err, 0, sizeof(uint32_t));
+        return fa_fail(FA_ERR_KERNEL, "device wait gave up (error word 0x%x)", err[0]);
+    }
+    return FA_OK;
+}
+
+extern "C" int fa_reset(fa_handle* h, uint8_t* obs_out)
+{
+    CHECK_H(h);
+    // HeadlessAtari::new + one run_frame without set_action
+    // (src/cuda_env.rs:134-139): one instance on the device, then broadcast.
+    uint32_t col[FA_ROWS];
+    fa_power_on_column(h->image.data(), h->nbanks, h->scheme, col);
+    FA_CUDA(cudaMemcpyAsync(h->d_snap, col, sizeof(col), cudaMemcpyHostToDevice, h->stream));
+    FaGroup g = make_group(h, nullptr, 1, nullptr);
+    g.state = h->d_snap;
+    g.stride = 1;
+    g.n = 1;
+    g.snapshot = nullptr;
+    g.episode_frames = 0;
+    g.sched = FA_SCHED_LANE;
+    FA_CUDA(cudaMemsetAsync(h->d_instr, 0, sizeof(unsigned long long), h->stream));
+    bool persistent = h->persistent;
+    h->persistent = false;
+    int rc = enqueue_run(h, g, h->stream);
+    h->persistent = persistent;
+    if (rc) return rc;
+    FA_CUDA(cudaMemcpyAsync(col, h->d_snap, sizeof(col), cudaMemcpyDeviceToHost, h->stream));
+    FA_CUDA(cudaStreamSynchronize(h->stream));
+    col[R_FRAME] = 0;                      // episode counter restarts at reset
+    FA_CUDA(cudaMemcpyAsync(h->d_snap, col, sizeof(col), cudaMemcpyHostToDevice, h->stream));
+    FA_CUDA(fa_launch_broadcast(h->d_state, h->stride, (uint32_t)h->n, h->d_snap, h->stream));
+    h->have_snap = true;
+    rc = finish(h);
+    if (rc) return rc;
+    if (obs_out) {
+        const uint8_t* ram = (const uint8_t*)col;
+        for (size_t i = 0; i < h->n; i++) memcpy(obs_out + i * 128, ram, 128);
+    }
+    return FA_OK;
+}
+
+static int step_host(fa_handle* h, const uint8_t* actions, int k, uint8_t* obs_out)
+{
+    CHECK_H(h);
+    if (!actions || k < 1) return fa_fail(FA_ERR_INVALID, "actions null or k < 1");
+    const size_t bytes = (size_t)k * h->n;
+    int rc = ensure_actions(h, bytes);
+    if (rc) return rc;
+    memcpy(h->h_actions, actions, bytes);
+    FA_CUDA(cudaMemcpyAsync(h->d_actions, h->h_actions, bytes, cudaMemcpyHostToDevice, h->stream));
+    FA_CUDA(cudaMemsetAsync(h->d_instr, 0, sizeof(unsigned long long), h->stream));
+    rc = enqueue_run(h, make_group(h, h->d_actions, (uint32_t)k, obs_out ? h->d_obs : nullptr), h->stream);
+    if (rc) return rc;
+    if (obs_out) FA_CUDA(cudaMemcpyAsync(h->h_obs, h->d_obs, h->n * 128, cudaMemcpyDeviceToHost, h->stream));
+    rc = finish(h);
+    if (rc) return rc;
+    if (obs_out) memcpy(obs_out, h->h_obs, h->n * 128);
+    return FA_OK;
+}
+
+extern "C" int fa_step(fa_handle* h, const uint8_t* actions, uint8_t* obs_out)
+{
+    return step_host(h, actions, 1, obs_out);
+}
+
+extern "C" int fa_step_multi(fa_handle* h, const uint8_t* actions, int k, uint8_t* obs_out)
+{
+    return step_host(h, actions, k, obs_out);
+}
+
+extern "C" int fa_step_multi_async(fa_handle* h, const uint8_t* d_actions, int k, uint8_t* d_obs, void* stream)
+{
+    CHECK_H(h);
+    if (!d_actions || k < 1) return fa_fail(FA_ERR_INVALID, "actions null or k < 1");
+    if (((uintptr_t)d_obs & 15u) != 0) return fa_fail(FA_ERR_INVALID, "d_obs must be 16-byte aligned");
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    return enqueue_run(h, make_group(h, d_actions, (uint32_t)k, d_obs), s);
+}
+
+extern "C" int fa_synchronize(fa_handle* h)
+{
+    CHECK_H(h);
+    FA_CUDA(cudaDeviceSynchronize());
+    return finish(h);
+}
+
+extern "C" int fa_get_states(fa_handle* h, fa_state* out)
+{
+    CHECK_H(h);
+    if (!out) return fa_fail(FA_ERR_INVALID, "out is null");
+    std::vector<uint32_t> buf((size_t)FA_ROWS * h->stride);
+    FA_CUDA(cudaStreamSynchronize(h->stream));
+    FA_CUDA(cudaMemcpy(buf.data(), h->d_state, buf.size() * 4, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < h->n; i++) fa_unpack_column(buf.data() + i, h->stride, h->scheme, out[i]);
+    return FA_OK;
+}
+
+extern "C" int fa_set_states(fa_handle* h, const fa_state* in)
+{
+    CHECK_H(h);
+    if (!in) return fa_fail(FA_ERR_INVALID, "in is null");
+    std::vector<uint32_t> buf((size_t)FA_ROWS * h->stride, 0);
+    for (size_t i = 0; i < h->n; i++) {
+        if (in[i].timer_prescaler_select == 0)
+            return fa_fail(FA_ERR_INVALID, "instance %zu: timer_prescaler_select 0 (reference divides by it)", i);
+        fa_state s = in[i];
+        if (s.bank >= h->nbanks) s.bank = (uint8_t)(h->nbanks - 1);
+        fa_pack_column(s, buf.data() + i, h->stride);
+    }
+    FA_CUDA(cudaStreamSynchronize(h->stream));
+    FA_CUDA(cudaMemcpy(h->d_state, buf.data(), buf.size() * 4, cudaMemcpyHostToDevice));
+    return FA_OK;
+}
+
+extern "C" int fa_get_ram(fa_handle* h, size_t idx, uint8_t* out128)
+{
+    CHECK_H(h);
+    if (!out128 || idx >= h->n) return fa_fail(FA_ERR_INVALID, "bad index %zu", idx);
+    FA_CUDA(cudaStreamSynchronize(h->stream));
+    uint32_t w[32];
+    FA_CUDA(cudaMemcpy2D(w, 4, h->d_state + idx, (size_t)h->stride * 4, 4, 32, cudaMemcpyDeviceToHost));
+    memcpy(out128, w, 128);
+    return FA_OK;
+}
+
+extern "C" int fa_get_status(fa_handle* h, uint32_t* out)
+{
+    CHECK_H(h);
+    if (!out) return fa_fail(FA_ERR_INVALID, "out is null");
+    FA_CUDA(cudaStreamSynchronize(h->stream));
+    FA_CUDA(cudaMemcpy(out, h->d_state + (size_t)R_STATUS * h->stride, h->n * 4, cudaMemcpyDeviceToHost));
+    return FA_OK;
+}
+
+extern "C" int fa_set_episode_frames(fa_handle* h, uint32_t episode_frames)
+{
+    if (!h) return fa_fail(FA_ERR_INVALID, "null handle");
+    h->episode_frames = episode_frames;
+    return FA_OK;
+}
+
+extern "C" int fa_set_frame_numbers(fa_handle* h, const uint32_t* frame_no)
+{
+    CHECK_H(h);
+    if (!frame_no) return fa_fail(FA_ERR_INVALID, "frame_no is null");
+    FA_CUDA(cudaStreamSynchronize(h->stream));
+    FA_CUDA(cudaMemcpy(h->d_state + (size_t)R_FRAME * h->stride, frame_no, h->n * 4, cudaMemcpyHostToDevice));
+    return FA_OK;
+}
+
+extern "C" int fa_set_launch(fa_handle* h, int block, int sched, int persistent)
+{
+    if (!h) return fa_fail(FA_ERR_INVALID, "null handle");
+    if (block != 64 && block != 128 && block != 256 && block != 512)
+        return fa_fail(FA_ERR_INVALID, "block must be 64, 128, 256 or 512");
+    if (sched < FA_SCHED_LANE || sched > FA_SCHED_MATCH) return fa_fail(FA_ERR_INVALID, "bad sched %d", sched);
+    h->block = block;
+    h->sched = sched;
+    h->persistent = persistent != 0;
+    return FA_OK;
+}
+
+extern "C" int fa_get_launch(const fa_handle* h, int* block, int* sched, int* persistent)
+{
+    if (!h) return fa_fail(FA_ERR_INVALID, "null handle");
+    if (block) *block = h->block;
+    if (sched) *sched = h->sched;
+    if (persistent) *persistent = h->persistent ? 1 : 0;
+    return FA_OK;
+}
+
+extern "C" unsigned long long fa_last_instructions(const fa_handle* h)
+{
+    return h ? h->last_instr : 0ull;
+}
+
+extern "C" int fa_get_snapshot(fa_handle* h, fa_state* out)
+{
+    CHECK_H(h);
+    if (!out) return fa_fail(FA_ERR_INVALID, "out is null");
+    if (!h->have_snap) return fa_fail(FA_ERR_INVALID, "no reset snapshot yet");
+    uint32_t col[FA_ROWS];
+    FA_CUDA(cudaStreamSynchronize(h->stream));
+    FA_CUDA(cudaMemcpy(col, h->d_snap, sizeof(col), cudaMemcpyDeviceToHost));
+    fa_unpack_column(col, 1, h->scheme, *out);
+    return FA_OK;
+}
+
+extern "C" void* fa_device_state(fa_handle* h, uint32_t* stride_words)
+{
+    if (!h) return nullptr;
+    if (stride_words) *stride_words = h->stride;
+    return h->d_state;
+}

@@ -1,0 +1,646 @@
+// fa_device.cuh — the per-thread Atari 2600 emulator for sm_100a.
+//
+// One thread emulates one console.  Its hot state lives in registers; its
+// 128-byte PIA RAM and the TIA registers that change only on a write live in
+// shared memory, interleaved by thread in 32-bit words (byte o of thread t is
+// at word (o/4)*BLOCK + t), so lanes touching any offsets hit bank t%32 and
+// never conflict.  ROM banks sit in shared memory, staged once per block.
+//
+// Semantics are those of the reference CPU emulator (RPP1011/fast-atari-rs):
+//   src/cpu.rs            6502 step, including every phantom access whose
+//                         side effect is visible on the Atari bus
+//   src/atari.rs:460-552  HeadlessBus read/write decode and bank hotspots
+//   src/atari.rs:584-614  run_frame / run_one_cycle
+//   src/headless_tia.rs   HeadlessTia
+//   src/pia.rs            Pia
+// The instruction decoder is organised by the 6502 opcode bit fields
+// (aaa bbb cc) instead of one 151-way switch: lanes executing different
+// opcodes that share an addressing mode or an ALU operation share code.
+#pragma once
+#include <stdint.h>
+
+#include "fa_layout.h"
+
+namespace fa {
+
+enum : uint32_t { F_C = 1, F_Z = 2, F_I = 4, F_D = 8, F_B = 16, F_U = 32, F_V = 64, F_N = 128 };
+
+// Action -> (SWCHA | INPT4<<8 | paddle0<<16), src/atari.rs:34-81,571-582.
+constexpr uint32_t act_word(int up, int down, int left, int right, int fire)
+{
+    return (0xFFu & ~(up ? 0x10u : 0u) & ~(down ? 0x20u : 0u) & ~(left ? 0x40u : 0u) & ~(right ? 0x80u : 0u))
+         | ((fire ? 0u : 1u) << 8) | ((left ? 200u : right ? 50u : 128u) << 16);
+}
+
+// Action::decode order (src/atari.rs:59-80): up, down, left, right, fire.
+__constant__ uint32_t c_action_table[18] = {
+    act_word(0, 0, 0, 0, 0), act_word(0, 0, 0, 0, 1), act_word(1, 0, 0, 0, 0), act_word(0, 0, 0, 1, 0),
+    act_word(0, 0, 1, 0, 0), act_word(0, 1, 0, 0, 0), act_word(1, 0, 0, 1, 0), act_word(1, 0, 1, 0, 0),
+    act_word(0, 1, 0, 1, 0), act_word(0, 1, 1, 0, 0), act_word(1, 0, 0, 0, 1), act_word(0, 0, 0, 1, 1),
+    act_word(0, 0, 1, 0, 1), act_word(0, 1, 0, 0, 1), act_word(1, 0, 0, 1, 1), act_word(1, 0, 1, 0, 1),
+    act_word(0, 1, 0, 1, 1), act_word(0, 1, 1, 0, 1),
+};
+
+template <int BLOCK>
+struct Emu {
+    // ---- placement
+    uint8_t* pv;             // private bytes of this thread (shared memory)
+    const uint8_t* rom;      // shared-memory ROM image, nbanks * 4 KiB
+    uint32_t hot_lo, nbanks;
+    // ---- CPU (src/cpu.rs:96-105)
+    uint32_t a, x, y, sp, p, pc, bank;
+    uint32_t cyc_lo, cyc_hi;
+    // ---- PIA (src/pia.rs:26-44)
+    uint32_t pa_out, pa_ddr, pa_in, pb_out, pb_ddr, pb_in;
+    uint32_t tv, ps, sel, uf;
+    // ---- TIA hot fields (src/headless_tia.rs:16-45)
+    uint32_t clock, scanline, wsync, fcomp, vsync, vblank;
+    uint32_t pcnt, pdump, inpt4, inpt5, pad0, pad1;
+    // ---- run bookkeeping
+    uint32_t frame_no, status, instr;
+
+    // ------------------------------------------------------------ private bytes
+    __device__ __forceinline__ uint32_t poff(uint32_t o) const { return (o & ~3u) * BLOCK + (o & 3u); }
+    __device__ __forceinline__ uint32_t ldp(uint32_t o) const { return pv[poff(o)]; }
+    __device__ __forceinline__ void stp(uint32_t o, uint32_t v) { pv[poff(o)] = (uint8_t)v; }
+    __device__ __forceinline__ uint32_t ldp16(uint32_t o) const { return *(const uint16_t*)(pv + poff(o)); }
+    __device__ __forceinline__ void stp16(uint32_t o, uint32_t v) { *(uint16_t*)(pv + poff(o)) = (uint16_t)v; }
+
+    // ------------------------------------------------------------ flags
+    __device__ __forceinline__ void nz(uint32_t v) { p = (p & ~(F_N | F_Z)) | (v & F_N) | (v ? 0u : F_Z); }
+    __device__ __forceinline__ void setc(bool c) { p = (p & ~F_C) | (c ? F_C : 0u); }
+
+    // ------------------------------------------------------------ bank switching
+    __device__ __forceinline__ void bsw(uint32_t a13)
+    {
+        uint32_t d = a13 - hot_lo;
+        if (d < nbanks) bank = d;
+    }
+
+    // ------------------------------------------------------------ TIA (headless_tia.rs)
+    __device__ __forceinline__ void end_scanline()                   // :183-198
+    {
+        clock = (clock - 228u) & 0xFFFFu;
+        scanline = (scanline + 1u) & 0xFFFFu;
+        wsync = 0;
+        if (!pdump && pcnt < 256u) pcnt++;
+        if (scanline >= 262u) { scanline = 0; fcomp = 1; }
+    }
+    __device__ __forceinline__ void tia_tick(uint32_t n)            // :153-158
+    {
+        clock = (clock + 3u * n) & 0xFFFFu;
+        if (clock >= 228u) end_scanline();
+    }
+    __device__ __forceinline__ uint32_t tia_skip()                   // :163-180
+    {
+        uint32_t rem = clock >= 228u ? 0u : 228u - clock;
+        uint32_t c = (rem + 2u) / 3u;
+        if (c) { clock = 228u; end_scanline(); }
+        return c;
+    }
+    __device__ uint32_t tia_read(uint32_t a) const                   // :205-223
+    {
+        uint32_t r = a & 0x0Fu;
+        if (r < 8u) return ldp(PB_CX + r);
+        switch (r) {
+        case 0x8: return pcnt >= pad0 ? 0x80u : 0u;
+        case 0x9: return pcnt >= pad1 ? 0x80u : 0u;
+        case 0xA: case 0xB: return 0x80u;
+        case 0xC: return inpt4 ? 0x80u : 0u;
+        case 0xD: return inpt5 ? 0x80u : 0u;
+        default: return 0u;
+        }
+    }
+    __device__ static __forceinline__ uint32_t mod160(int v)
+    {
+        int r = v % 160;
+        return (uint32_t)(r < 0 ? r + 160 : r);
+    }
+    __device__ void tia_write(uint32_t a, uint32_t v)                // :225-298
+    {
+        uint32_t r = a & 0x3Fu;
+        switch (r) {
+        case 0x00:
+            if (!(vsync & 2u) && (v & 2u)) { scanline = 0; fcomp = 1; }
+            vsync = v; break;
+        case 0x01:
+            if (v & 0x80u) { pcnt = 0; pdump = 1; } else if (pdump) pdump = 0;
+            vblank = v; break;
+        case 0x02: wsync = 1; break;
+        case 0x04: stp(PB_NUSIZ0, v); break;
+        case 0x05: stp(PB_NUSIZ1, v); break;
+        case 0x06: case 0x07: case 0x08: case 0x09: stp(PB_COLUP0 + (r - 0x06u), v); break;
+        case 0x0A: stp(PB_CTRLPF, v); break;
+        case 0x0B: stp(PB_REFP0, (v >> 3) & 1u); break;
+        case 0x0C: stp(PB_REFP1, (v >> 3) & 1u); break;
+        case 0x0D: case 0x0E: case 0x0F: stp(PB_PF0 + (r - 0x0Du), v); break;
+        case 0x10: case 0x11: case 0x12: case 0x13: case 0x14:
+            // RESPx: (clock as i16 - 68 + 5).rem_euclid(160)
+            stp16(PB_POS + 2u * (r - 0x10u), mod160((int16_t)(uint16_t)(clock - 63u)));
+            break;
+        case 0x1B: stp(PB_GRP0_OLD, ldp(PB_GRP0)); stp(PB_GRP0, v); break;
+        case 0x1C:
+            stp(PB_GRP1_OLD, ldp(PB_GRP1)); stp(PB_GRP1, v);
+            stp(PB_ENABL_OLD, ldp(PB_ENABL)); break;
+        case 0x1D: case 0x1E: case 0x1F: stp(PB_ENAM0 + (r - 0x1Du), (v >> 1) & 1u); break;
+        case 0x20: case 0x21: case 0x22: case 0x23: case 0x24: stp(PB_HM + (r - 0x20u), v); break;
+        case 0x25: case 0x26: case 0x27: stp(PB_VDELP0 + (r - 0x25u), v & 1u); break;
+        case 0x28: case 0x29: stp(PB_RESMP0 + (r - 0x28u), (v >> 1) & 1u); break;
+        case 0x2A:                                                      // HMOVE
+            for (uint32_t k = 0; k < 5u; k++) {
+                int off = ((int)(int8_t)(uint8_t)ldp(PB_HM + k)) >> 4;
+                int16_t d = (int16_t)(uint16_t)(ldp16(PB_POS + 2u * k) - (uint32_t)off);
+                stp16(PB_POS + 2u * k, mod160(d));
+            }
+            break;
+        case 0x2B: for (uint32_t k = 0; k < 5u; k++) stp(PB_HM + k, 0); break;
+        case 0x2C: for (uint32_t k = 0; k < 8u; k++) stp(PB_CX + k, 0); break;
+        default: break;
+        }
+    }
+
+    // ------------------------------------------------------------ PIA (pia.rs)
+    __device__ __forceinline__ void pia_tick(uint32_t n)             // :107-166
+    {
+        if (n == 0) return;
+        if (tv == 0 && uf) { tv = (0xFFu - (n - 1u)) & 0xFFu; return; }
+        uint32_t rem = n;
+        if (ps > 0) {
+            if (rem < ps) { ps -= rem; return; }
+            rem -= ps;
+            ps = 0;
+            if (tv == 0) {
+                uf = 1;
+                tv = rem ? ((0xFFu - (rem - 1u)) & 0xFFu) : 0xFFu;
+                return;
+            }
+            tv -= 1u;
+        }
+        if (rem == 0) { ps = sel; return; }
+        uint32_t full, left;
+        if ((sel & (sel - 1u)) == 0) {                    // 1, 8, 64, 1024
+            uint32_t sh = __ffs(sel) - 1u;
+            full = rem >> sh;
+            left = rem & (sel - 1u);
+        } else {
+            full = rem / sel;
+            left = rem % sel;
+        }
+        if (full >= tv) {
+            rem = (rem - ((tv * sel) & 0xFFFFu)) & 0xFFFFu;   // u16 arithmetic as in the reference
+            uf = 1;
+            tv = rem ? ((0xFFu - (rem - 1u)) & 0xFFu) : 0xFFu;
+        } else {
+            tv -= full;
+            ps = sel - left;
+        }
+    }
+    __device__ __forceinline__ uint32_t pia_read(uint32_t a)         // :169-199 (I/O half)
+    {
+        switch (a & 7u) {
+        case 0: return (pa_in & ~pa_ddr & 0xFFu) | (pa_out & pa_ddr);
+        case 1: return pa_ddr;
+        case 2: return (pb_in & ~pb_ddr & 0xFFu) | (pb_out & pb_ddr);
+        case 3: return pb_ddr;
+        case 4: uf = 0; return tv & 0xFFu;
+        case 5: return uf ? 0x80u : 0u;
+        default: return 0u;
+        }
+    }
+    __device__ __forceinline__ void pia_write(uint32_t a, uint32_t v) // :202-228 (I/O half)
+    {
+        if (a & 0x10u) {
+            tv = v; uf = 0;
+            sel = 1u << ((0xA630u >> (4u * (a & 3u))) & 0xFu);      // 1, 8, 64, 1024
+            ps = sel;
+            return;
+        }
+        switch (a & 3u) {
+        case 0: pa_out = v; break;
+        case 1: pa_ddr = v; break;
+        case 2: pb_out = v; break;
+        default: pb_ddr = v; break;
+        }
+    }
+
+    // ------------------------------------------------------------ bus (atari.rs:497-552)
+    __device__ __forceinline__ uint32_t read_low(uint32_t a)         // a < 0x1000
+    {
+        if (a & 0x80u) {
+            if ((a & 0x280u) == 0x280u) return pia_read(a);
+            if (a < 0x200u) return ldp(a & 0x7Fu);
+            return 0u;            // other RAM mirrors read the never-written flat array
+        }
+        return tia_read(a);
+    }
+    __device__ __forceinline__ uint32_t read(uint32_t addr)
+    {
+        uint32_t a = addr & 0x1FFFu;
+        if (a & 0x1000u) { bsw(a); return rom[(bank << 12) | (a & 0xFFFu)]; }
+        return read_low(a);
+    }
+    __device__ __forceinline__ void write(uint32_t addr, uint32_t v)
+    {
+        uint32_t a = addr & 0x1FFFu;
+        if (a & 0x1000u) { bsw(a); return; }
+        if ((a & 0x280u) == 0x080u) { stp(a & 0x7Fu, v); return; }
+        if (a & 0x200u) { pia_write(a, v); return; }
+        tia_write(a, v);
+    }
+    // A phantom read: only its side effects (hotspot, INTIM) matter.
+    __device__ __forceinline__ void dummy(uint32_t addr)
+    {
+        uint32_t a = addr & 0x1FFFu;
+        if (a & 0x1000u) bsw(a);
+        else if ((a & 0x287u) == 0x284u) uf = 0;
+    }
+    __device__ __forceinline__ uint32_t zp_read(uint32_t z) { return (z & 0x80u) ? ldp(z & 0x7Fu) : tia_read(z); }
+    __device__ __forceinline__ uint32_t fetch() { uint32_t v = read(pc); pc = (pc + 1u) & 0xFFFFu; return v; }
+    __device__ __forceinline__ void push(uint32_t v)
+    {
+        if (sp & 0x80u) stp(sp & 0x7Fu, v); else tia_write(0x100u | sp, v);
+        sp = (sp - 1u) & 0xFFu;
+    }
+    __device__ __forceinline__ uint32_t pull()
+    {
+        sp = (sp + 1u) & 0xFFu;
+        return (sp & 0x80u) ? ldp(sp & 0x7Fu) : tia_read(0x100u | sp);
+    }
+    // Read-modify-write's two writes; a RAM target only needs the second.
+    __device__ __forceinline__ void rmw_store(uint32_t ea, uint32_t oldv, uint32_t newv)
+    {
+        uint32_t a = ea & 0x1FFFu;
+        if ((a & 0x1280u) == 0x080u) { stp(a & 0x7Fu, newv); return; }
+        write(ea, oldv);
+        write(ea, newv);
+    }
+
+    // ------------------------------------------------------------ ALU (cpu.rs:153-241)
+    __device__ __forceinline__ void adc(uint32_t v)
+    {
+        uint32_t c = p & F_C;
+        if (p & F_D) {
+            uint32_t lo = (a & 0xFu) + (v & 0xFu) + c;
+            if (lo > 9u) lo += 6u;
+            uint32_t hi = (a >> 4) + (v >> 4) + (lo > 0xFu ? 1u : 0u);
+            uint32_t bin = (a + v + c) & 0xFFu;
+            uint32_t res = ((hi << 4) | (lo & 0xFu)) & 0xFFu;
+            p &= ~(F_Z | F_N | F_V | F_C);
+            p |= bin ? 0u : F_Z;
+            p |= (hi & 8u) ? F_N : 0u;
+            p |= (~(a ^ v) & (a ^ res) & 0x80u) ? F_V : 0u;
+            if (hi > 9u) hi += 6u;
+            p |= hi > 0xFu ? F_C : 0u;
+            a = ((hi & 0xFu) << 4) | (lo & 0xFu);
+        } else {
+            uint32_t s = a + v + c;
+            uint32_t r = s & 0xFFu;
+            p = (p & ~(F_V | F_C)) | (s >> 8) | ((~(a ^ v) & (a ^ r) & 0x80u) ? F_V : 0u);
+            a = r;
+            nz(a);
+        }
+    }
+    __device__ __forceinline__ void sbc(uint32_t v)
+    {
+        uint32_t b = (p & F_C) ^ 1u;
+        int bin = (int)a - (int)v - (int)b;
+        uint32_t r = (uint32_t)bin & 0xFFu;
+        if (p & F_D) {
+            uint32_t lo = ((a & 0xFu) - (v & 0xFu) - b) & 0xFFu;
+            uint32_t lob = 0;
+            if (lo & 0x80u) { lo = (lo - 6u) & 0xFFu; lob = 1; }
+            uint32_t hi = ((a >> 4) - (v >> 4) - lob) & 0xFFu;
+            if (hi & 0x80u) hi = (hi - 6u) & 0xFFu;
+            p &= ~(F_Z | F_N | F_V | F_C);
+            p |= bin >= 0 ? F_C : 0u;
+            p |= r ? 0u : F_Z;
+            p |= r & F_N;
+            p |= ((a ^ v) & (a ^ r) & 0x80u) ? F_V : 0u;
+            a = ((hi & 0xFu) << 4) | (lo & 0xFu);
+        } else {
+            p = (p & ~(F_V | F_C)) | (bin >= 0 ? F_C : 0u) | (((a ^ v) & (a ^ r) & 0x80u) ? F_V : 0u);
+            a = r;
+            nz(a);
+        }
+    }
+    __device__ __forceinline__ void cmp(uint32_t reg, uint32_t v)
+    {
+        setc(reg >= v);
+        nz((reg - v) & 0xFFu);
+    }
+    __device__ __forceinline__ void bit(uint32_t v)
+    {
+        p = (p & ~(F_Z | F_V | F_N)) | ((a & v) ? 0u : F_Z) | (v & (F_V | F_N));
+    }
+    // Shift/rotate/INC/DEC by the aaa field of a cc=10 opcode.
+    __device__ __forceinline__ uint32_t shift_op(uint32_t aaa, uint32_t v)
+    {
+        uint32_t r;
+        switch (aaa) {
+        case 0: setc(v & 0x80u); r = (v << 1) & 0xFFu; break;                       // ASL
+        case 1: r = ((v << 1) | (p & F_C)) & 0xFFu; setc(v & 0x80u); break;         // ROL
+        case 2: setc(v & 1u); r = v >> 1; break;                                    // LSR
+        case 3: r = (v >> 1) | ((p & F_C) << 7); setc(v & 1u); break;               // ROR
+        case 6: r = (v - 1u) & 0xFFu; break;                                        // DEC
+        default: r = (v + 1u) & 0xFFu; break;                                       // INC
+        }
+        nz(r);
+        return r;
+    }
+
+    // ------------------------------------------------------------ instruction groups
+    // cc = 01: ORA AND EOR ADC STA LDA CMP SBC x 8 addressing modes.
+    __device__ __forceinline__ uint32_t group1(uint32_t aaa, uint32_t bbb)
+    {
+        const bool st = aaa == 4u;
+        uint32_t ea, cyc, v;
+        switch (bbb) {
+        case 0: {                                                   // (zp,X)
+            uint32_t z = (fetch() + x) & 0xFFu;
+            uint32_t lo = zp_read(z);
+            uint32_t hi = zp_read((z + 1u) & 0xFFu);
+            ea = (hi << 8) | lo; cyc = 6; break;
+        }
+        case 1: ea = fetch(); cyc = 3; break;                       // zp
+        case 2:                                                     // #imm
+            if (st) return 0;                                       // $89 is illegal
+            v = fetch();
+            cyc = 2;
+            goto operate;
+        case 3: { uint32_t lo = fetch(); ea = (fetch() << 8) | lo; cyc = 4; break; }
+        case 4: {                                                   // (zp),Y
+            uint32_t z = fetch();
+            uint32_t lo = zp_read(z);
+            uint32_t base = (zp_read((z + 1u) & 0xFFu) << 8) | lo;
+            ea = (base + y) & 0xFFFFu; cyc = 5;
+            if (st || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 6; }
+            break;
+        }
+        case 5: ea = (fetch() + x) & 0xFFu; cyc = 4; break;        // zp,X
+        default: {                                                  // abs,Y / abs,X
+            uint32_t lo = fetch();
+            uint32_t base = (fetch() << 8) | lo;
+            ea = (base + (bbb == 6u ? y : x)) & 0xFFFFu; cyc = 4;
+            if (st || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 5; }
+            break;
+        }
+        }
+        if (st) { write(ea, a); return cyc; }
+        v = read(ea);
+    operate:
+        switch (aaa) {
+        case 0: a |= v; nz(a); break;
+        case 1: a &= v; nz(a); break;
+        case 2: a ^= v; nz(a); break;
+        case 3: adc(v); break;
+        case 5: a = v; nz(a); break;
+        case 6: cmp(a, v); break;
+        default: sbc(v); break;
+        }
+        return cyc;
+    }
+
+    // cc = 10: ASL ROL LSR ROR STX LDX DEC INC, plus TXA TAX DEX NOP TXS TSX.
+    __device__ __forceinline__ uint32_t group2(uint32_t aaa, uint32_t bbb)
+    {
+        uint32_t ea, cyc;
+        switch (bbb) {
+        case 0:                                                     // LDX #imm only
+            if (aaa != 5u) return 0;
+            x = fetch(); nz(x); return 2;
+        case 2:                                                     // accumulator / implied
+            dummy(pc);
+            switch (aaa) {
+            case 4: a = x; nz(a); break;                            // TXA
+            case 5: x = a; nz(x); break;                            // TAX
+            case 6: x = (x - 1u) & 0xFFu; nz(x); break;             // DEX
+            case 7: break;                                          // NOP
+            default: a = shift_op(aaa, a); break;
+            }
+            return 2;
+        case 6:
+            if (aaa == 4u) { dummy(pc); sp = x; return 2; }          // TXS
+            if (aaa == 5u) { dummy(pc); x = sp; nz(x); return 2; }   // TSX
+            return 0;
+        case 4: return 0;
+        case 1: ea = fetch(); cyc = 3; break;                       // zp
+        case 3: { uint32_t lo = fetch(); ea = (fetch() << 8) | lo; cyc = 4; break; }
+        case 5:                                                     // zp,X (zp,Y for STX/LDX)
+            ea = (fetch() + ((aaa == 4u || aaa == 5u) ? y : x)) & 0xFFu; cyc = 4; break;
+        default: {                                                  // abs,X (abs,Y for LDX)
+            if (aaa == 4u) return 0;                                // $9E is illegal
+            uint32_t lo = fetch();
+            uint32_t base = (fetch() << 8) | lo;
+            if (aaa == 5u) {
+                ea = (base + y) & 0xFFFFu; cyc = 4;
+                if ((base ^ ea) & 0xFF00u) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 5; }
+                x = read(ea); nz(x); return cyc;
+            }
+            ea = (base + x) & 0xFFFFu;
+            dummy((base & 0xFF00u) | (ea & 0xFFu));
+            uint32_t v = read(ea);
+            rmw_store(ea, v, shift_op(aaa, v));
+            return 7;
+        }
+        }
+        if (aaa == 4u) { write(ea, x); return cyc; }
+        if (aaa == 5u) { x = read(ea); nz(x); return cyc; }
+        uint32_t v = read(ea);
+        rmw_store(ea, v, shift_op(aaa, v));
+        return cyc + 2u;
+    }
+
+    // cc = 00: control flow, stack, flags, BIT/STY/LDY/CPY/CPX.
+    __device__ __forceinline__ uint32_t group0(uint32_t aaa, uint32_t bbb)
+    {
+        switch (bbb) {
+        case 4: {                                                   // branches
+            uint32_t off = fetch();
+            uint32_t pos = (0x1067u >> (4u * (aaa >> 1))) & 0xFu;    // N V C Z
+            if (((p >> pos) & 1u) != (aaa & 1u)) return 2;
+            dummy(pc);
+            uint32_t npc = (pc + (uint32_t)(int32_t)(int8_t)(uint8_t)off) & 0xFFFFu;
+            uint32_t cyc = 3;
+            if ((pc ^ npc) & 0xFF00u) { dummy((pc & 0xFF00u) | (npc & 0xFFu)); cyc = 4; }
+            pc = npc;
+            return cyc;
+        }
+        case 6:                                                     // flags, TYA
+            dummy(pc);
+            switch (aaa) {
+            case 0: p &= ~F_C; break;
+            case 1: p |= F_C; break;
+            case 2: p &= ~F_I; break;
+            case 3: p |= F_I; break;
+            case 4: a = y; nz(a); break;
+            case 5: p &= ~F_V; break;
+            case 6: p &= ~F_D; break;
+            default: p |= F_D; break;
+            }
+            return 2;
+        case 2:                                                     // stack, DEY TAY INY INX
+            dummy(pc);
+            switch (aaa) {
+            case 0: push(p | F_B | F_U); return 3;                  // PHP
+            case 1: p = pull() & ~(F_B | F_U); return 4;            // PLP
+            case 2: push(a); return 3;                              // PHA
+            case 3: a = pull(); nz(a); return 4;                    // PLA
+            case 4: y = (y - 1u) & 0xFFu; nz(y); return 2;          // DEY
+            case 5: y = a; nz(y); return 2;                         // TAY
+            case 6: y = (y + 1u) & 0xFFu; nz(y); return 2;          // INY
+            default: x = (x + 1u) & 0xFFu; nz(x); return 2;         // INX
+            }
+        case 0:
+            switch (aaa) {
+            case 0: {                                               // BRK
+                dummy(pc); pc = (pc + 1u) & 0xFFFFu;
+                push(pc >> 8); push(pc & 0xFFu); push(p | F_B | F_U);
+                p |= F_I;
+                uint32_t lo = read(0xFFFEu);
+                pc = (read(0xFFFFu) << 8) | lo;
+                return 7;
+            }
+            case 1: {                                               // JSR
+                uint32_t lo = fetch();
+                push(pc >> 8); push(pc & 0xFFu);
+                pc = (read(pc) << 8) | lo;
+                return 6;
+            }
+            case 2: {                                               // RTI
+                dummy(pc);
+                p = pull() & ~(F_B | F_U);
+                uint32_t lo = pull();
+                pc = (pull() << 8) | lo;
+                return 6;
+            }
+            case 3: {                                               // RTS
+                dummy(pc);
+                uint32_t lo = pull();
+                uint32_t ra = (pull() << 8) | lo;
+                dummy(ra);
+                pc = (ra + 1u) & 0xFFFFu;
+                return 6;
+            }
+            case 4: return 0;
+            case 5: y = fetch(); nz(y); return 2;                   // LDY #
+            case 6: cmp(y, fetch()); return 2;                      // CPY #
+            default: cmp(x, fetch()); return 2;                     // CPX #
+            }
+        case 3:                                                     // absolute
+            if (aaa == 0u) return 0;
+            if (aaa == 2u) { uint32_t lo = fetch(); pc = (read(pc) << 8) | lo; return 3; }  // JMP
+            if (aaa == 3u) {                                        // JMP (ind), page-wrap bug
+                uint32_t lo = fetch();
+                uint32_t ptr = (fetch() << 8) | lo;
+                uint32_t tlo = read(ptr);
+                pc = (read((ptr & 0xFF00u) | ((ptr + 1u) & 0xFFu)) << 8) | tlo;
+                return 5;
+            }
+            {
+                uint32_t lo = fetch();
+                uint32_t ea = (fetch() << 8) | lo;
+                return mem0(aaa, ea, 4);
+            }
+        case 1:                                                     // zp
+            if (aaa == 0u || aaa == 2u || aaa == 3u) return 0;
+            return mem0(aaa, fetch(), 3);
+        case 5:                                                     // zp,X: STY LDY
+            if (aaa != 4u && aaa != 5u) return 0;
+            return mem0(aaa, (fetch() + x) & 0xFFu, 4);
+        default: {                                                  // abs,X: LDY
+            if (aaa != 5u) return 0;
+            uint32_t lo = fetch();
+            uint32_t base = (fetch() << 8) | lo;
+            uint32_t ea = (base + x) & 0xFFFFu, cyc = 4;
+            if ((base ^ ea) & 0xFF00u) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 5; }
+            y = read(ea); nz(y);
+            return cyc;
+        }
+        }
+    }
+    __device__ __forceinline__ uint32_t mem0(uint32_t aaa, uint32_t ea, uint32_t cyc)
+    {
+        if (aaa == 4u) { write(ea, y); return cyc; }                // STY
+        uint32_t v = read(ea);
+        switch (aaa) {
+        case 1: bit(v); break;
+        case 5: y = v; nz(y); break;
+        case 6: cmp(y, v); break;
+        default: cmp(x, v); break;
+        }
+        return cyc;
+    }
+
+    // One instruction; returns its cycle count, 0 for an illegal opcode
+    // (pc is then past the opcode and nothing else changed).
+    __device__ __forceinline__ uint32_t step()
+    {
+        uint32_t op = fetch();
+        uint32_t aaa = op >> 5, bbb = (op >> 2) & 7u;
+        switch (op & 3u) {
+        case 1: return group1(aaa, bbb);
+        case 2: return group2(aaa, bbb);
+        case 0: return group0(aaa, bbb);
+        default: return 0;
+        }
+    }
+
+    // HeadlessAtari::set_action (src/atari.rs:571-582).
+    __device__ __forceinline__ void apply_action(uint32_t act)
+    {
+        uint32_t t = c_action_table[act < 18u ? act : 0u];
+        pa_in = t & 0xFFu;
+        inpt4 = (t >> 8) & 1u;
+        pad0 = (t >> 16) & 0xFFu;
+    }
+
+    // ------------------------------------------------------------ state movement
+    __device__ __forceinline__ void load_hot(const uint32_t* col, uint32_t stride)
+    {
+        uint32_t w;
+        w = col[R_AXYS * stride];  a = w & 0xFF; x = (w >> 8) & 0xFF; y = (w >> 16) & 0xFF; sp = w >> 24;
+        w = col[R_PC * stride];    pc = w & 0xFFFF; p = (w >> 16) & 0xFF; bank = w >> 24;
+        cyc_lo = col[R_CYC_LO * stride];
+        cyc_hi = col[R_CYC_HI * stride];
+        w = col[R_PIA0 * stride];  pa_out = w & 0xFF; pa_ddr = (w >> 8) & 0xFF; pa_in = (w >> 16) & 0xFF; pb_out = w >> 24;
+        w = col[R_PIA1 * stride];  pb_ddr = w & 0xFF; pb_in = (w >> 8) & 0xFF; uf = (w >> 16) & 0xFF; pdump = w >> 24;
+        w = col[R_TIMER * stride]; tv = w & 0xFFFF; ps = w >> 16;
+        w = col[R_SELPC * stride]; sel = w & 0xFFFF; pcnt = w >> 16;
+        w = col[R_TIA0 * stride];  clock = w & 0xFFFF; scanline = w >> 16;
+        w = col[R_TIA1 * stride];  wsync = w & 0xFF; fcomp = (w >> 8) & 0xFF; vsync = (w >> 16) & 0xFF; vblank = w >> 24;
+        w = col[R_TIA2 * stride];  inpt4 = w & 0xFF; inpt5 = (w >> 8) & 0xFF; pad0 = (w >> 16) & 0xFF; pad1 = w >> 24;
+        frame_no = col[R_FRAME * stride];
+        status = col[R_STATUS * stride];
+    }
+    __device__ __forceinline__ void store_hot(uint32_t* col, uint32_t stride) const
+    {
+        col[R_AXYS * stride] = a | (x << 8) | (y << 16) | (sp << 24);
+        col[R_PC * stride] = pc | (p << 16) | (bank << 24);
+        col[R_CYC_LO * stride] = cyc_lo;
+        col[R_CYC_HI * stride] = cyc_hi;
+        col[R_PIA0 * stride] = pa_out | (pa_ddr << 8) | (pa_in << 16) | (pb_out << 24);
+        col[R_PIA1 * stride] = pb_ddr | (pb_in << 8) | (uf << 16) | (pdump << 24);
+        col[R_TIMER * stride] = tv | (ps << 16);
+        col[R_SELPC * stride] = sel | (pcnt << 16);
+        col[R_TIA0 * stride] = clock | (scanline << 16);
+        col[R_TIA1 * stride] = wsync | (fcomp << 8) | (vsync << 16) | (vblank << 24);
+        col[R_TIA2 * stride] = inpt4 | (inpt5 << 8) | (pad0 << 16) | (pad1 << 24);
+        col[R_FRAME * stride] = frame_no;
+        col[R_STATUS * stride] = status;
+    }
+    // Private words from global (stride-separated rows) into shared memory.
+    __device__ __forceinline__ void load_priv(const uint32_t* col, uint32_t stride)
+    {
+        uint32_t* w = (uint32_t*)pv;
+#pragma unroll 4
+        for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) w[k * BLOCK] = col[k * stride];
+    }
+    __device__ __forceinline__ void store_priv(uint32_t* col, uint32_t stride) const
+    {
+        const uint32_t* w = (const uint32_t*)pv;
+#pragma unroll 4
+        for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) col[k * stride] = w[k * BLOCK];
+    }
+};
+
+}  // namespace fa

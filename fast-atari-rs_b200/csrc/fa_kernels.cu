@@ -1,0 +1,349 @@
+// fa_kernels.cu — launches of the batched Atari core on sm_100a.
+//
+// One kernel, fa_run, serves both launch forms of the library:
+//   * plain:      one CTA per work unit (grid = number of units);
+//   * persistent: grid sized to the SMs, each CTA pops work units from a
+//                 device counter until the queue is empty.
+// A work unit is up to BLOCK consecutive instances of one group (one cart's
+// instance set).  Groups of different carts, instance counts, frame counts
+// and scheduling policies share one launch.  When a CTA's next unit belongs
+// to a different cart than the ROM it holds, it re-stages the ROM into shared
+// memory with TMA bulk copies (cp.async.bulk, no multicast) on an mbarrier.
+//
+// Every wait is bounded; on expiry the kernel records FA_DEVERR_* in the
+// launch's error word and leaves the unit untouched.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fa_device.cuh"
+#include "fa_internal.h"
+
+namespace fa {
+
+// ------------------------------------------------------------------ TMA / mbarrier
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Stage `bytes` (a multiple of 4 KiB) of ROM into shared memory.  Called by
+// every thread of the CTA after a __syncthreads; returns false if the copy
+// did not complete within the wait bound.
+__device__ bool stage_rom(uint8_t* dst, const uint8_t* src, uint32_t bytes, uint64_t* bar, uint32_t& phase)
+{
+    if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(bar, bytes);
+        for (uint32_t off = 0; off < bytes; off += 4096u) bulk_g2s(dst + off, src + off, 4096u, bar);
+    }
+    bool ok = false;
+    for (uint32_t it = 0; it < (1u << 22); it++) {
+        if (mbar_try_wait(bar, phase)) { ok = true; break; }
+    }
+    phase ^= 1u;
+    return ok;
+}
+
+// ------------------------------------------------------------------ per-unit runner
+template <int BLOCK>
+struct Runner {
+    Emu<BLOCK> e;
+    const FaGroup* G;
+    uint32_t i, f, phase, fcyc;
+    bool active;
+
+    __device__ __forceinline__ bool begin_frame()
+    {
+        if (e.status & FA_STATUS_HALT_MASK) return false;
+        if (G->episode_frames && e.frame_no >= G->episode_frames && G->snapshot) {
+            e.load_priv(G->snapshot, 1);
+            e.load_hot(G->snapshot, 1);
+        }
+        if (G->actions) e.apply_action(G->actions[(size_t)f * G->act_stride + i]);
+        e.fcomp = 0;
+        fcyc = 0;
+        phase = (e.vsync & 2u) ? 0u : 1u;
+        return true;
+    }
+
+    // One HeadlessAtari::run_one_cycle (src/atari.rs:601-614) plus the frame
+    // loop checks of run_frame (src/atari.rs:584-598).  Returns true when the
+    // lane should run again immediately (a WSYNC skip is pending).
+    __device__ __forceinline__ bool one()
+    {
+        if (e.wsync) {
+            uint32_t s = e.tia_skip();
+            e.pia_tick(s);
+            fcyc += s;
+        } else {
+            uint32_t c = e.step();
+            if (c == 0) { e.status |= FA_STATUS_ILLEGAL_OPCODE; active = false; return false; }
+            e.instr++;
+            uint32_t lo = e.cyc_lo + c;
+            e.cyc_hi += lo < c ? 1u : 0u;
+            e.cyc_lo = lo;
+            fcyc += c;
+            e.tia_tick(c);
+            e.pia_tick(c);
+        }
+        if (phase == 0u) {
+            if (fcyc > FA_VSYNC_BUDGET) { e.status |= FA_STATUS_VSYNC_BUDGET; active = false; return false; }
+            if (!(e.vsync & 2u)) phase = 1u;
+        } else {
+            const bool cap = fcyc > FA_FRAME_CYCLE_CAP;
+            if (cap || (e.vsync & 2u)) {
+                if (cap) e.status |= FA_STATUS_CYCLE_CAP;
+                e.frame_no++;
+                f++;
+                if (f >= G->k || !begin_frame()) { active = false; return false; }
+                return false;
+            }
+        }
+        return e.wsync != 0;
+    }
+
+    __device__ __forceinline__ void iterate()
+    {
+#pragma unroll 1
+        for (int rep = 0; rep < 2; rep++)
+            if (!one() || !active) break;
+    }
+};
+
+// Runs every lane of the warp to the end of its frames.  The policy only
+// decides which lanes execute in each round; all lanes share one call site of
+// the emulator so its code is instantiated once.
+template <int BLOCK>
+__device__ __forceinline__ void run_lanes(Runner<BLOCK>& r, uint32_t sched)
+{
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t rem = 0, grp = 0;
+    while (true) {
+        const bool act = r.active;
+        const uint32_t pcb = (r.e.bank << 16) | r.e.pc;
+        bool go;
+        if (sched == FA_SCHED_MATCH) {
+            // __match_any_sync groups lanes by (bank, pc); each group runs its
+            // instruction together, every group once per round.
+            if (rem == 0) {
+                rem = __ballot_sync(FULL, act);
+                if (!rem) break;
+                grp = __match_any_sync(FULL, act ? pcb : 0xFFFFFFFFu);
+            }
+            const uint32_t g = __shfl_sync(FULL, grp, __ffs(rem) - 1u);
+            go = (g >> lane) & 1u;
+            rem &= ~g;
+        } else if (sched == FA_SCHED_PC || sched == FA_SCHED_LINE) {
+            // Convergence scheduling: the lane furthest behind (frame, then
+            // scanline for FA_SCHED_LINE, then pc) leads and every lane at the
+            // leader's (bank, pc) runs with it.  Lanes that branched ahead wait
+            // until the others reach the same pc, so the warp re-converges.
+            if (!__any_sync(FULL, act)) break;
+            const uint32_t fc = r.f < 0x7Fu ? r.f : 0x7Fu;
+            uint32_t key = sched == FA_SCHED_LINE
+                ? (fc << 25) | ((r.e.scanline < 0x1FFu ? r.e.scanline : 0x1FFu) << 16) | r.e.pc
+                : (fc << 16) | r.e.pc;
+            if (!act) key = 0xFFFFFFFFu;
+            const uint32_t mk = __reduce_min_sync(FULL, key);
+            const uint32_t lead = __ffs(__ballot_sync(FULL, key == mk)) - 1u;
+            go = act && pcb == __shfl_sync(FULL, pcb, lead);
+        } else {
+            if (!__any_sync(FULL, act)) break;
+            go = act;
+        }
+        if (go) r.iterate();
+    }
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint32_t count, const uint8_t* rom_s,
+                         uint32_t* priv, unsigned long long* instr_out)
+{
+    const uint32_t t = threadIdx.x;
+    Runner<BLOCK> r;
+    r.G = &G;
+    r.i = first + t;
+    r.f = 0;
+    r.phase = 0;
+    r.fcyc = 0;
+    r.active = false;
+    r.e.pv = (uint8_t*)(priv + t);
+    r.e.rom = rom_s;
+    r.e.hot_lo = G.hot_lo;
+    r.e.nbanks = G.nbanks;
+    r.e.instr = 0;
+    r.e.pc = 0;
+    r.e.bank = 0;
+    r.e.scanline = 0;
+    const bool valid = t < count;
+    uint32_t* col = G.state + r.i;
+    if (valid) {
+        r.e.load_priv(col, G.stride);
+        r.e.load_hot(col, G.stride);
+        if (G.k > 0) r.active = r.begin_frame();
+    }
+    run_lanes<BLOCK>(r, G.sched);
+    if (valid) {
+        r.e.store_priv(col, G.stride);
+        r.e.store_hot(col, G.stride);
+        if (G.obs) {
+            const uint32_t* w = priv + t;
+            uint4* o = (uint4*)(G.obs + (size_t)r.i * 128u);
+#pragma unroll
+            for (uint32_t q = 0; q < 8u; q++)
+                o[q] = make_uint4(w[(4u * q) * BLOCK], w[(4u * q + 1u) * BLOCK], w[(4u * q + 2u) * BLOCK],
+                                  w[(4u * q + 3u) * BLOCK]);
+        }
+    }
+    if (instr_out) {
+        uint32_t n = valid ? r.e.instr : 0u;
+        for (int d = 16; d > 0; d >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, d);
+        if ((t & 31u) == 0 && n) atomicAdd(instr_out, (unsigned long long)n);
+    }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) fa_run(const __grid_constant__ FaLaunch L)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t s_unit;
+
+    uint8_t* rom_s = smem;
+    uint32_t* priv = (uint32_t*)(smem + L.rom_bytes_max);
+    uint32_t phase = 0;
+    int staged = -1;
+
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+
+    for (uint32_t round = 0;; round++) {
+        if (threadIdx.x == 0) {
+            uint32_t u;
+            if (L.queue) u = atomicAdd(L.queue, 1u);
+            else u = round == 0 ? blockIdx.x : 0xFFFFFFFFu;
+            s_unit = u;
+        }
+        __syncthreads();
+        const uint32_t u = s_unit;
+        if (u >= L.nunits) break;
+        int g = 0;
+        while (g + 1 < (int)L.ngroups && u >= L.g[g + 1].unit_begin) g++;
+        const FaGroup& G = L.g[g];
+        if (G.rom != (staged < 0 ? nullptr : L.g[staged].rom)) {
+            if (!stage_rom(rom_s, G.rom, G.nbanks * 4096u, &bar, phase)) {
+                if (threadIdx.x == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
+                break;
+            }
+            staged = g;
+        }
+        const uint32_t first = (u - G.unit_begin) * BLOCK;
+        const uint32_t count = G.n - first < BLOCK ? G.n - first : BLOCK;
+        run_unit<BLOCK>(G, first, count, rom_s, priv, L.instr);
+        __syncthreads();
+    }
+}
+
+// Every instance column of `state` becomes a copy of `col` (FA_ROWS words).
+__global__ void fa_broadcast(uint32_t* state, uint32_t stride, uint32_t n, const uint32_t* col)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (uint32_t w = 0; w < FA_ROWS; w++) state[(size_t)w * stride + i] = col[w];
+}
+
+}  // namespace fa
+
+// ------------------------------------------------------------------ host launchers
+template <int BLOCK>
+static cudaError_t launch_block(const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
+{
+    const size_t smem = (size_t)L.rom_bytes_max + (size_t)FA_PRIV_WORDS * BLOCK * 4u;
+    cudaError_t e = cudaFuncSetAttribute(fa::fa_run<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    uint32_t grid = L.nunits;
+    if (persistent) {
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<BLOCK>, BLOCK, smem);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+        uint32_t cap = (uint32_t)(per_sm * sms);
+        grid = L.nunits < cap ? L.nunits : cap;
+    }
+    if (grid == 0) return cudaSuccess;
+    fa::fa_run<BLOCK><<<grid, BLOCK, smem, s>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t fa_launch_run(const FaLaunch& L, int block, bool persistent, int sms, cudaStream_t s)
+{
+    switch (block) {
+    case 64: return launch_block<64>(L, persistent, sms, s);
+    case 128: return launch_block<128>(L, persistent, sms, s);
+    case 256: return launch_block<256>(L, persistent, sms, s);
+    case 512: return launch_block<512>(L, persistent, sms, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+int fa_launch_occupancy(int block, uint32_t rom_bytes_max)
+{
+    const size_t smem = (size_t)rom_bytes_max + (size_t)FA_PRIV_WORDS * block * 4u;
+    int per_sm = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (block) {
+    case 64: cudaFuncSetAttribute(fa::fa_run<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<64>, 64, smem); break;
+    case 128: cudaFuncSetAttribute(fa::fa_run<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<128>, 128, smem); break;
+    case 256: cudaFuncSetAttribute(fa::fa_run<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<256>, 256, smem); break;
+    case 512: cudaFuncSetAttribute(fa::fa_run<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<512>, 512, smem); break;
+    default: break;
+    }
+    return e == cudaSuccess ? per_sm : -1;
+}
+
+cudaError_t fa_launch_broadcast(uint32_t* state, uint32_t stride, uint32_t n, const uint32_t* col, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    uint32_t grid = (n + 255u) / 256u;
+    if (grid > 4096u) grid = 4096u;
+    fa::fa_broadcast<<<grid, 256, 0, s>>>(state, stride, n, col);
+    return cudaGetLastError();
+}

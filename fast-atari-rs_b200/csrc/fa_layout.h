@@ -1,0 +1,68 @@
+// fa_layout.h — structure-of-arrays layout of instance state in HBM.
+//
+// Each instance is one column of FA_ROWS 32-bit words; row w of instance i
+// lives at state[w * stride + i], so a warp loading row w reads 128
+// contiguous bytes.  Rows [0, FA_PRIV_WORDS) are the instance's "private
+// bytes": its 128 bytes of PIA RAM followed by the TIA registers that only
+// change on a register write.  The kernel keeps these in shared memory while
+// it runs; the remaining rows are the hot fields it keeps in registers.
+//
+// Shared by the host packer (fa_state AoS <-> SoA) and the device code.
+#pragma once
+#include <stdint.h>
+
+#include "../../include/fast_atari.h"
+
+#define FA_PRIV_BYTES 176
+#define FA_PRIV_WORDS (FA_PRIV_BYTES / 4)
+
+// Private-byte offsets: RAM occupies [0, 128).
+enum : uint32_t {
+    PB_CX     = 128,   // 8 collision latches cxm0p..cxppmm
+    PB_POS    = 136,   // 5 x u16: pos_p0 pos_p1 pos_m0 pos_m1 pos_bl
+    PB_HM     = 146,   // 5 x u8: hmp0 hmp1 hmm0 hmm1 hmbl
+    PB_GRP0   = 151, PB_GRP1 = 152, PB_GRP0_OLD = 153, PB_GRP1_OLD = 154,
+    PB_ENAM0  = 155, PB_ENAM1 = 156, PB_ENABL = 157, PB_ENABL_OLD = 158,
+    PB_VDELP0 = 159, PB_VDELP1 = 160, PB_VDELBL = 161,
+    PB_RESMP0 = 162, PB_RESMP1 = 163,
+    PB_NUSIZ0 = 164, PB_NUSIZ1 = 165,
+    PB_COLUP0 = 166, PB_COLUP1 = 167, PB_COLUPF = 168, PB_COLUBK = 169,
+    PB_CTRLPF = 170, PB_REFP0 = 171, PB_REFP1 = 172,
+    PB_PF0    = 173, PB_PF1 = 174, PB_PF2 = 175,
+};
+
+// Hot rows (after the private words).
+enum : uint32_t {
+    R_AXYS   = FA_PRIV_WORDS + 0,   // a | x<<8 | y<<16 | sp<<24
+    R_PC     = FA_PRIV_WORDS + 1,   // pc | p<<16 | bank<<24
+    R_CYC_LO = FA_PRIV_WORDS + 2,
+    R_CYC_HI = FA_PRIV_WORDS + 3,
+    R_PIA0   = FA_PRIV_WORDS + 4,   // pa_out | pa_ddr<<8 | pa_in<<16 | pb_out<<24
+    R_PIA1   = FA_PRIV_WORDS + 5,   // pb_ddr | pb_in<<8 | timer_underflow<<16 | paddle_dumped<<24
+    R_TIMER  = FA_PRIV_WORDS + 6,   // timer_value | timer_prescaler<<16
+    R_SELPC  = FA_PRIV_WORDS + 7,   // timer_prescaler_select | paddle_counter<<16
+    R_TIA0   = FA_PRIV_WORDS + 8,   // clock | scanline<<16
+    R_TIA1   = FA_PRIV_WORDS + 9,   // wsync | frame_complete<<8 | vsync<<16 | vblank<<24
+    R_TIA2   = FA_PRIV_WORDS + 10,  // inpt4 | inpt5<<8 | paddle0<<16 | paddle1<<24
+    R_FRAME  = FA_PRIV_WORDS + 11,  // frame_no
+    R_STATUS = FA_PRIV_WORDS + 12,  // run_status
+    FA_ROWS  = FA_PRIV_WORDS + 13,
+};
+
+// Bank-switch decode: a read or write of (addr & 0x1FFF) - hot_lo < nbanks
+// selects that bank (src/atari.rs:460-492).  Fixed carts use hot_lo 0x2000,
+// which no 13-bit address reaches.
+static inline uint32_t fa_hot_lo(int scheme)
+{
+    return scheme == FA_SCHEME_F8 ? 0x1FF8u : scheme == FA_SCHEME_F6 ? 0x1FF6u
+         : scheme == FA_SCHEME_F4 ? 0x1FF4u : 0x2000u;
+}
+static inline uint32_t fa_nbanks(int scheme)
+{
+    return scheme == FA_SCHEME_F8 ? 2u : scheme == FA_SCHEME_F6 ? 4u : scheme == FA_SCHEME_F4 ? 8u : 1u;
+}
+static inline int fa_detect_scheme(size_t len)        // BankScheme::detect, src/atari.rs:96-105
+{
+    return len <= 4096 ? FA_SCHEME_FIXED : len <= 8192 ? FA_SCHEME_F8
+         : len <= 16384 ? FA_SCHEME_F6 : FA_SCHEME_F4;
+}

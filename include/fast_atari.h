@@ -1,0 +1,235 @@
+/*
+ * fast_atari.h — C ABI of the B200 batched Atari 2600 emulator core.
+ *
+ * This is the drop-in boundary for the reference's `BatchAtariGpu`
+ * (src/cuda_env.rs:99-191 of RPP1011/fast-atari-rs).  Every entry point is
+ * plain C: pointers, sizes and int status codes, no CUDA or torch types in the
+ * signatures (streams are passed as `void*`, i.e. a `cudaStream_t`).
+ *
+ * Conventions
+ *   - Return value 0 (FA_OK) on success, a negative FA_ERR_* code on failure;
+ *     fa_last_error() returns a thread-local text for the last failure.
+ *   - Host buffers are borrowed for the duration of the call and copied.
+ *   - Every call on a handle is synchronous unless its name ends in `_async`
+ *     (those enqueue on the given stream and return immediately).
+ *   - A handle is used by one caller thread at a time (the reference's
+ *     `&mut self` discipline).
+ */
+#ifndef FAST_ATARI_H
+#define FAST_ATARI_H
+
+#include <stddef.h>   /* size_t, offsetof */
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- errors */
+#define FA_OK               0
+#define FA_ERR_INVALID     -1   /* bad argument (null pointer, size mismatch, k < 1) */
+#define FA_ERR_BAD_ROM     -2   /* ROM length the reference cannot construct */
+#define FA_ERR_CUDA        -3   /* a CUDA runtime call failed */
+#define FA_ERR_NO_DEVICE   -4   /* no CUDA device, or the kernels are missing */
+#define FA_ERR_KERNEL      -5   /* a device-side bounded wait gave up (error word set) */
+#define FA_ERR_CAPACITY    -6   /* request exceeds a configured capacity or budget */
+
+/* ------------------------------------------------ per-instance run status */
+/* Halting bits: the instance stops executing until reset or fa_set_states. */
+#define FA_STATUS_ILLEGAL_OPCODE  0x1u   /* reference panics (src/cpu.rs:1139-1141) */
+#define FA_STATUS_VSYNC_BUDGET    0x2u   /* VSYNC held for > FA_VSYNC_BUDGET cycles;
+                                            the reference loops forever (src/atari.rs:588-590) */
+#define FA_STATUS_NOT_RESET       0x4u   /* created but never reset; the reference
+                                            panics when stepping such a state */
+#define FA_STATUS_HALT_MASK       0x7u
+/* Informational, sticky: a frame ended on the 100,000-cycle cap (src/atari.rs:594). */
+#define FA_STATUS_CYCLE_CAP       0x100u
+
+#define FA_FRAME_CYCLE_CAP   100000u
+#define FA_VSYNC_BUDGET      2000000u
+
+/* Bank-switching schemes (src/atari.rs:83-105). */
+#define FA_SCHEME_FIXED 0
+#define FA_SCHEME_F8    1
+#define FA_SCHEME_F6    2
+#define FA_SCHEME_F4    3
+
+#define FA_RAM_BYTES 128
+#define FA_NUM_ACTIONS 18
+
+/*
+ * Full per-instance state, array-of-structs, as returned by fa_get_states.
+ * Bytes [0, 221) have exactly the layout of the reference's `AtariStateGpu`
+ * (src/cuda_env.rs:10-38, repr(C)); the tail adds what the reference GPU state
+ * lacks: the CPU cycle counter (`Cpu::cycles`, src/cpu.rs:104), a frame
+ * counter and the run status word.
+ */
+typedef struct fa_state {
+    uint8_t  a, x, y, sp;
+    uint16_t pc;
+    uint8_t  status;
+    uint8_t  _pad0;
+    uint8_t  ram[FA_RAM_BYTES];
+    uint8_t  port_a_output, port_a_ddr, port_a_input;
+    uint8_t  port_b_output, port_b_ddr, port_b_input;
+    uint16_t timer_value, timer_prescaler, timer_prescaler_select;
+    uint8_t  timer_underflow, _pad1, _pad2, _pad3;
+    uint16_t tia_clock, tia_scanline;
+    uint8_t  tia_wsync, tia_frame_complete, tia_vsync, tia_vblank;
+    uint8_t  cxm0p, cxm1p, cxp0fb, cxp1fb, cxm0fb, cxm1fb, cxblpf, cxppmm;
+    uint8_t  inpt4, inpt5, paddle0, paddle1;
+    uint16_t paddle_counter;
+    uint8_t  paddle_dumped, _pad4;
+    uint16_t pos_p0, pos_p1, pos_m0, pos_m1, pos_bl;
+    uint8_t  hmp0, hmp1, hmm0, hmm1, hmbl, _pad5;
+    uint8_t  grp0, grp1, grp0_old, grp1_old;
+    uint8_t  enam0, enam1, enabl, enabl_old;
+    uint8_t  vdelp0, vdelp1, vdelbl;
+    uint8_t  resmp0, resmp1, nusiz0, nusiz1;
+    uint8_t  colup0, colup1, colupf, colubk;
+    uint8_t  ctrlpf, refp0, refp1;
+    uint8_t  pf0, pf1, pf2;
+    uint8_t  bank, scheme;
+    uint8_t  _pad_end[2];
+    /* ---- extension beyond the reference layout ---- */
+    uint8_t  _pad_ext[3];
+    uint64_t cycles;      /* Cpu::cycles: executed instruction cycles, never reset */
+    uint32_t frame_no;    /* frames run since the last reset (episode counter) */
+    uint32_t run_status;  /* FA_STATUS_* bits */
+} fa_state;
+
+#define FA_STATE_REF_BYTES 221   /* prefix shared with the reference AtariStateGpu */
+#define FA_STATE_BYTES     240
+
+#ifdef __cplusplus
+#define FA_STATIC_ASSERT(c, m) static_assert(c, m)
+#else
+#define FA_STATIC_ASSERT(c, m) _Static_assert(c, m)
+#endif
+FA_STATIC_ASSERT(sizeof(fa_state) == FA_STATE_BYTES, "fa_state size");
+FA_STATIC_ASSERT(offsetof(fa_state, ram) == 8, "ram offset");
+FA_STATIC_ASSERT(offsetof(fa_state, timer_value) == 142, "timer offset");
+FA_STATIC_ASSERT(offsetof(fa_state, tia_clock) == 152, "tia offset");
+FA_STATIC_ASSERT(offsetof(fa_state, paddle_counter) == 172, "paddle offset");
+FA_STATIC_ASSERT(offsetof(fa_state, pos_p0) == 176, "pos offset");
+FA_STATIC_ASSERT(offsetof(fa_state, bank) == 217, "bank offset");
+FA_STATIC_ASSERT(offsetof(fa_state, cycles) == 224, "cycles offset");
+FA_STATIC_ASSERT(offsetof(fa_state, run_status) == 236, "status offset");
+
+/* Opaque handle: one ROM, n instances, resident in HBM (`BatchAtariGpu`). */
+typedef struct fa_handle fa_handle;
+
+/* Text of the last error on this thread ("" if none). */
+const char* fa_last_error(void);
+
+/* Library version string. */
+const char* fa_version(void);
+
+/* Number of CUDA devices visible (0 when none); never fails. */
+int fa_device_count(void);
+
+/*
+ * BatchAtariGpu::new (src/cuda_env.rs:112-126).  Uploads the ROM and allocates
+ * SoA state for n instances on the current device.  The ROM length must be one
+ * the reference can construct: 1..4096 (Fixed, mirrored into the 4K window),
+ * 8192 (F8), 16384 (F6) or >= 32768 (F4, first 32 KiB used).  Instances start
+ * zeroed, as in the reference; call fa_reset before stepping.
+ */
+int fa_create(const uint8_t* rom, size_t rom_len, size_t n, fa_handle** out);
+
+/* Drop (frees every device buffer of the handle). NULL is ignored. */
+void fa_destroy(fa_handle* h);
+
+/* BatchAtariGpu::num_envs (src/cuda_env.rs:190). */
+size_t fa_num_envs(const fa_handle* h);
+
+/*
+ * BatchAtariGpu::set_sorted (src/cuda_env.rs:129).  sorted != 0 turns on warp
+ * grouping of lanes by program counter (__match_any_sync) before each
+ * emulated instruction; 0 runs every lane's own instruction stream.
+ */
+int fa_set_sorted(fa_handle* h, int sorted);
+
+/*
+ * BatchAtariGpu::reset (src/cuda_env.rs:131-142): every instance becomes
+ * HeadlessAtari::new(rom) followed by one run_frame().  Computed on the device
+ * once and broadcast.  obs_out (n*128 bytes, may be NULL) receives the RAM.
+ */
+int fa_reset(fa_handle* h, uint8_t* obs_out);
+
+/*
+ * BatchAtariGpu::step (src/cuda_env.rs:144-161): apply actions[i] (0..17, other
+ * values act as NOOP like Action::from_index) to instance i and run one frame.
+ * obs_out (n*128 bytes, may be NULL) receives each instance's RAM.
+ */
+int fa_step(fa_handle* h, const uint8_t* actions, uint8_t* obs_out);
+
+/*
+ * BatchAtariGpu::step_multi (src/cuda_env.rs:166-184): k frames in one launch,
+ * actions frame-major (actions[f*n + i]); obs_out gets the last frame's RAM.
+ */
+int fa_step_multi(fa_handle* h, const uint8_t* actions, int k, uint8_t* obs_out);
+
+/*
+ * Device-pointer variant of step_multi, enqueued on `stream` (a cudaStream_t,
+ * NULL = the handle's own stream).  d_actions holds k*n bytes and d_obs n*128
+ * bytes of device memory (d_obs may be NULL).  Returns without synchronising.
+ */
+int fa_step_multi_async(fa_handle* h, const uint8_t* d_actions, int k,
+                        uint8_t* d_obs, void* stream);
+
+/* Wait for all work enqueued on the handle's stream; reports kernel errors. */
+int fa_synchronize(fa_handle* h);
+
+/* BatchAtariGpu::download_states (src/cuda_env.rs:186-188), extended layout. */
+int fa_get_states(fa_handle* h, fa_state* out);
+
+/* Upload full states for all n instances (checkpoint restore). */
+int fa_set_states(fa_handle* h, const fa_state* in);
+
+/* Copy instance idx's 128-byte RAM (HeadlessAtari::ram, src/atari.rs:617). */
+int fa_get_ram(fa_handle* h, size_t idx, uint8_t* out128);
+
+/* Copy every instance's run-status word (n entries). */
+int fa_get_status(fa_handle* h, uint32_t* out);
+
+/*
+ * Periodic episode reset: before each frame, an instance whose frame_no has
+ * reached episode_frames is restored to the post-reset snapshot (frame_no 0).
+ * 0 disables it.  Phase offsets are set through fa_set_frame_numbers.
+ */
+int fa_set_episode_frames(fa_handle* h, uint32_t episode_frames);
+
+/* Overwrite every instance's frame_no (n entries). */
+int fa_set_frame_numbers(fa_handle* h, const uint32_t* frame_no);
+
+/* Lane scheduling policies inside a warp (fa_set_launch `sched`). */
+#define FA_SCHED_LANE  0   /* each lane runs its own instruction stream */
+#define FA_SCHED_PC    1   /* lanes at the pc of the lane furthest behind run together */
+#define FA_SCHED_LINE  2   /* as FA_SCHED_PC, ordered by (frame, scanline, pc) */
+#define FA_SCHED_MATCH 3   /* __match_any_sync groups by pc, every group each round */
+
+/*
+ * Launch shape of the handle (no reference counterpart; the reference uses a
+ * fixed 128-thread block, src/cuda_env.rs:147).  block in {64,128,256,512};
+ * persistent != 0 sizes the grid to the SMs and feeds CTAs from a device work
+ * queue instead of one CTA per 'block' instances.
+ */
+int fa_set_launch(fa_handle* h, int block, int sched, int persistent);
+int fa_get_launch(const fa_handle* h, int* block, int* sched, int* persistent);
+
+/* Guest (6502) instructions executed by the handle's last synchronous call. */
+unsigned long long fa_last_instructions(const fa_handle* h);
+
+/* The post-reset snapshot every instance starts from (after fa_reset). */
+int fa_get_snapshot(fa_handle* h, fa_state* out);
+
+/* Device pointer to the SoA state rows (FA layout, for zero-copy readers);
+ * *stride_words receives the row stride in 32-bit words. */
+void* fa_device_state(fa_handle* h, uint32_t* stride_words);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FAST_ATARI_H */

@@ -1,0 +1,827 @@
+/*
+ * fa_oracle.c — CPU oracle: plain-C restatement of the reference HeadlessAtari.
+ *
+ * TEST INFRASTRUCTURE ONLY (see fa_oracle.h).  Each function cites the
+ * reference file:line it restates.  The structure deliberately follows the
+ * reference (flat 8 KiB bus array, 4 KiB bank memcpy, per-instruction bulk
+ * TIA/PIA advance) so that it checks the CUDA path, which is organised very
+ * differently, and so that its timing is representative of the reference's
+ * CPU emulator.
+ */
+#define _GNU_SOURCE
+#include "fa_oracle.h"
+
+#include <pthread.h>
+#include <sched.h>
+#include <stdlib.h>
+#include <string.h>
+
+enum { F_C = 1, F_Z = 2, F_I = 4, F_D = 8, F_B = 16, F_U = 32, F_V = 64, F_N = 128 };
+
+/* ------------------------------------------------------------ CPU (cpu.rs) */
+typedef struct orc_cpu {          /* Cpu, src/cpu.rs:96-105 */
+    uint16_t pc;
+    uint8_t  sp, a, x, y, p;
+    uint64_t cycles;
+} orc_cpu;
+
+static inline void orc_setf(orc_cpu* c, uint8_t f, int on)       /* Status::set :42 */
+{
+    if (on) c->p |= f; else c->p &= (uint8_t)~f;
+}
+static inline void orc_zn(orc_cpu* c, uint8_t v)                 /* Status::set_zn :48 */
+{
+    orc_setf(c, F_Z, v == 0);
+    orc_setf(c, F_N, (v & 0x80) != 0);
+}
+
+static void orc_adc(orc_cpu* c, uint8_t v)                        /* cpu.rs:153-175 */
+{
+    uint8_t carry = (c->p & F_C) ? 1 : 0;
+    if (c->p & F_D) {
+        uint8_t lo = (uint8_t)((c->a & 0x0F) + (v & 0x0F) + carry);
+        if (lo > 9) lo = (uint8_t)(lo + 6);
+        uint8_t hi = (uint8_t)((c->a >> 4) + (v >> 4) + (lo > 0x0F ? 1 : 0));
+        uint16_t bin = (uint16_t)(c->a + v + carry);
+        orc_setf(c, F_Z, (uint8_t)bin == 0);
+        orc_setf(c, F_N, (hi & 0x08) != 0);
+        orc_setf(c, F_V, ((uint8_t)(~(c->a ^ v)) & (uint8_t)(c->a ^ (uint8_t)((hi << 4) | (lo & 0x0F))) & 0x80) != 0);
+        if (hi > 9) hi = (uint8_t)(hi + 6);
+        orc_setf(c, F_C, hi > 0x0F);
+        c->a = (uint8_t)(((hi & 0x0F) << 4) | (lo & 0x0F));
+    } else {
+        uint16_t s = (uint16_t)(c->a + v + carry);
+        uint8_t r = (uint8_t)s;
+        orc_setf(c, F_C, s > 0xFF);
+        orc_setf(c, F_V, ((uint8_t)(~(c->a ^ v)) & (uint8_t)(c->a ^ r) & 0x80) != 0);
+        c->a = r;
+        orc_zn(c, c->a);
+    }
+}
+
+static void orc_sbc(orc_cpu* c, uint8_t v)                        /* cpu.rs:178-200 */
+{
+    uint8_t borrow = (c->p & F_C) ? 0 : 1;
+    if (c->p & F_D) {
+        uint8_t lo = (uint8_t)((c->a & 0x0F) - (v & 0x0F) - borrow);
+        uint8_t lob = 0;
+        if ((int8_t)lo < 0) { lo = (uint8_t)(lo - 6); lob = 1; }
+        uint8_t hi = (uint8_t)((c->a >> 4) - (v >> 4) - lob);
+        if ((int8_t)hi < 0) hi = (uint8_t)(hi - 6);
+        int16_t bin = (int16_t)((int16_t)c->a - (int16_t)v - (int16_t)borrow);
+        orc_setf(c, F_C, bin >= 0);
+        orc_setf(c, F_Z, (uint8_t)bin == 0);
+        orc_setf(c, F_N, ((uint8_t)bin & 0x80) != 0);
+        orc_setf(c, F_V, ((c->a ^ v) & (c->a ^ (uint8_t)bin) & 0x80) != 0);
+        c->a = (uint8_t)(((hi & 0x0F) << 4) | (lo & 0x0F));
+    } else {
+        uint8_t d1 = (uint8_t)(c->a - v);
+        int b1 = v > c->a;
+        uint8_t d2 = (uint8_t)(d1 - borrow);
+        int b2 = borrow > d1;
+        orc_setf(c, F_C, !(b1 || b2));
+        orc_setf(c, F_V, ((c->a ^ v) & (c->a ^ d2) & 0x80) != 0);
+        c->a = d2;
+        orc_zn(c, c->a);
+    }
+}
+
+static inline void orc_compare(orc_cpu* c, uint8_t reg, uint8_t v) /* cpu.rs:203-207 */
+{
+    orc_setf(c, F_C, reg >= v);
+    orc_zn(c, (uint8_t)(reg - v));
+}
+static inline uint8_t orc_asl(orc_cpu* c, uint8_t v)               /* cpu.rs:210-215 */
+{
+    orc_setf(c, F_C, (v & 0x80) != 0);
+    uint8_t r = (uint8_t)(v << 1); orc_zn(c, r); return r;
+}
+static inline uint8_t orc_lsr(orc_cpu* c, uint8_t v)               /* cpu.rs:218-223 */
+{
+    orc_setf(c, F_C, (v & 0x01) != 0);
+    uint8_t r = (uint8_t)(v >> 1); orc_zn(c, r); return r;
+}
+static inline uint8_t orc_rol(orc_cpu* c, uint8_t v)               /* cpu.rs:226-232 */
+{
+    uint8_t oc = (c->p & F_C) ? 1 : 0;
+    orc_setf(c, F_C, (v & 0x80) != 0);
+    uint8_t r = (uint8_t)((v << 1) | oc); orc_zn(c, r); return r;
+}
+static inline uint8_t orc_ror(orc_cpu* c, uint8_t v)               /* cpu.rs:235-241 */
+{
+    uint8_t oc = (c->p & F_C) ? 1 : 0;
+    orc_setf(c, F_C, (v & 0x01) != 0);
+    uint8_t r = (uint8_t)((v >> 1) | (oc << 7)); orc_zn(c, r); return r;
+}
+
+/* The per-opcode operation of the read-type instructions (the inner matches
+ * of cpu.rs:342-354, 371-390, 427-436, 573-590, 668-677, 758-767, 812-820,
+ * 869-877). */
+static void orc_read_op(orc_cpu* c, uint8_t op, uint8_t v)
+{
+    switch (op) {
+    case 0xA9: case 0xA5: case 0xB5: case 0xAD: case 0xBD: case 0xB9: case 0xA1: case 0xB1:
+        c->a = v; orc_zn(c, c->a); break;                                      /* LDA */
+    case 0xA2: case 0xA6: case 0xAE:
+        c->x = v; orc_zn(c, c->x); break;                                      /* LDX */
+    case 0xA0: case 0xA4: case 0xB4: case 0xAC: case 0xBC:
+        c->y = v; orc_zn(c, c->y); break;                                      /* LDY */
+    case 0x69: case 0x65: case 0x75: case 0x6D: case 0x7D: case 0x79: case 0x61: case 0x71:
+        orc_adc(c, v); break;
+    case 0xE9: case 0xE5: case 0xF5: case 0xED: case 0xFD: case 0xF9: case 0xE1: case 0xF1:
+        orc_sbc(c, v); break;
+    case 0x29: case 0x25: case 0x35: case 0x2D: case 0x3D: case 0x39: case 0x21: case 0x31:
+        c->a &= v; orc_zn(c, c->a); break;                                     /* AND */
+    case 0x09: case 0x05: case 0x15: case 0x0D: case 0x1D: case 0x19: case 0x01: case 0x11:
+        c->a |= v; orc_zn(c, c->a); break;                                     /* ORA */
+    case 0x49: case 0x45: case 0x55: case 0x4D: case 0x5D: case 0x59: case 0x41: case 0x51:
+        c->a ^= v; orc_zn(c, c->a); break;                                     /* EOR */
+    case 0xC9: case 0xC5: case 0xD5: case 0xCD: case 0xDD: case 0xD9: case 0xC1: case 0xD1:
+        orc_compare(c, c->a, v); break;                                        /* CMP */
+    case 0xE0: case 0xE4: case 0xEC:
+        orc_compare(c, c->x, v); break;                                        /* CPX */
+    case 0xC0: case 0xC4: case 0xCC:
+        orc_compare(c, c->y, v); break;                                        /* CPY */
+    case 0x24: case 0x2C:                                                      /* BIT */
+        orc_setf(c, F_Z, (c->a & v) == 0);
+        orc_setf(c, F_V, (v & 0x40) != 0);
+        orc_setf(c, F_N, (v & 0x80) != 0);
+        break;
+    default: break;
+    }
+}
+
+static inline uint8_t orc_store_val(const orc_cpu* c, uint8_t op)
+{
+    switch (op) {
+    case 0x86: case 0x8E: case 0x96: return c->x;                              /* STX */
+    case 0x84: case 0x8C: case 0x94: return c->y;                              /* STY */
+    default: return c->a;                                                      /* STA */
+    }
+}
+
+static uint8_t orc_rmw(orc_cpu* c, uint8_t op, uint8_t v)
+{
+    switch (op) {
+    case 0x06: case 0x16: case 0x0E: case 0x1E: return orc_asl(c, v);
+    case 0x46: case 0x56: case 0x4E: case 0x5E: return orc_lsr(c, v);
+    case 0x26: case 0x36: case 0x2E: case 0x3E: return orc_rol(c, v);
+    case 0x66: case 0x76: case 0x6E: case 0x7E: return orc_ror(c, v);
+    case 0xE6: case 0xF6: case 0xEE: case 0xFE: { uint8_t r = (uint8_t)(v + 1); orc_zn(c, r); return r; }
+    default:                                    { uint8_t r = (uint8_t)(v - 1); orc_zn(c, r); return r; }
+    }
+}
+
+/* ----------------------------------------------- HeadlessTia (headless_tia.rs) */
+typedef struct orc_tia {          /* HeadlessTia, headless_tia.rs:16-88 */
+    uint16_t clock, scanline;
+    uint8_t  wsync, frame_complete, vsync, vblank;
+    uint8_t  cx[8];               /* cxm0p cxm1p cxp0fb cxp1fb cxm0fb cxm1fb cxblpf cxppmm */
+    uint8_t  inpt4, inpt5, paddle0, paddle1;
+    uint16_t paddle_counter;
+    uint8_t  paddle_dumped;
+    uint16_t pos[5];              /* p0 p1 m0 m1 bl */
+    uint8_t  hm[5];               /* hmp0 hmp1 hmm0 hmm1 hmbl */
+    uint8_t  grp0, grp1, grp0_old, grp1_old;
+    uint8_t  enam0, enam1, enabl, enabl_old;
+    uint8_t  vdelp0, vdelp1, vdelbl, resmp0, resmp1;
+    uint8_t  nusiz0, nusiz1, colup0, colup1, colupf, colubk, ctrlpf, refp0, refp1;
+    uint8_t  pf0, pf1, pf2;
+} orc_tia;
+
+static void orc_tia_default(orc_tia* t)                            /* headless_tia.rs:90-118 */
+{
+    memset(t, 0, sizeof(*t));
+    t->inpt4 = 1;
+    t->inpt5 = 1;
+}
+
+static void orc_tia_end_scanline(orc_tia* t)                       /* headless_tia.rs:183-198 */
+{
+    t->clock = (uint16_t)(t->clock - 228);
+    t->scanline++;
+    t->wsync = 0;
+    if (!t->paddle_dumped && t->paddle_counter < 256) t->paddle_counter++;
+    if (t->scanline >= 262) {                                      /* SCANLINES_PER_FRAME */
+        t->scanline = 0;
+        if (!t->frame_complete) t->frame_complete = 1;
+    }
+}
+
+static inline void orc_tia_tick_n(orc_tia* t, uint8_t n)           /* headless_tia.rs:153-158 */
+{
+    t->clock = (uint16_t)(t->clock + n * 3);
+    if (t->clock >= 228) orc_tia_end_scanline(t);
+}
+
+static uint16_t orc_tia_skip_to_scanline_end(orc_tia* t)           /* headless_tia.rs:163-180 */
+{
+    uint16_t rem = t->clock >= 228 ? 0 : (uint16_t)(228 - t->clock);
+    uint16_t cpu = (uint16_t)((rem + 2) / 3);
+    if (cpu > 0) {
+        t->clock = 228;
+        orc_tia_end_scanline(t);
+    }
+    return cpu;
+}
+
+static uint16_t orc_hmove(uint16_t pos, uint8_t hm)                /* headless_tia.rs:200-203 */
+{
+    int16_t off = (int16_t)(((int8_t)hm) >> 4);                    /* arithmetic shift of i8 */
+    int r = (int16_t)((int16_t)pos - off) % 160;                   /* i16 wrapping, rem_euclid */
+    if (r < 0) r += 160;
+    return (uint16_t)r;
+}
+
+static uint8_t orc_tia_read(const orc_tia* t, uint16_t addr)       /* headless_tia.rs:205-223 */
+{
+    switch (addr & 0x0F) {
+    case 0x00: case 0x01: case 0x02: case 0x03:
+    case 0x04: case 0x05: case 0x06: case 0x07: return t->cx[addr & 7];
+    case 0x08: return t->paddle_counter >= t->paddle0 ? 0x80 : 0x00;
+    case 0x09: return t->paddle_counter >= t->paddle1 ? 0x80 : 0x00;
+    case 0x0A: case 0x0B: return 0x80;
+    case 0x0C: return t->inpt4 ? 0x80 : 0x00;
+    case 0x0D: return t->inpt5 ? 0x80 : 0x00;
+    default: return 0;
+    }
+}
+
+static uint16_t orc_resp_pos(const orc_tia* t)                     /* headless_tia.rs:257-261 */
+{
+    int r = (int16_t)((int16_t)t->clock - 68 + 5) % 160;          /* i16, rem_euclid */
+    if (r < 0) r += 160;
+    return (uint16_t)r;
+}
+
+static void orc_tia_write(orc_tia* t, uint16_t addr, uint8_t v)    /* headless_tia.rs:225-298 */
+{
+    switch (addr & 0x3F) {
+    case 0x00:
+        if (!(t->vsync & 0x02) && (v & 0x02)) { t->scanline = 0; t->frame_complete = 1; }
+        t->vsync = v; break;
+    case 0x01:
+        if (v & 0x80) { t->paddle_counter = 0; t->paddle_dumped = 1; }
+        else if (t->paddle_dumped) t->paddle_dumped = 0;
+        t->vblank = v; break;
+    case 0x02: t->wsync = 1; break;
+    case 0x04: t->nusiz0 = v; break;
+    case 0x05: t->nusiz1 = v; break;
+    case 0x06: t->colup0 = v; break;
+    case 0x07: t->colup1 = v; break;
+    case 0x08: t->colupf = v; break;
+    case 0x09: t->colubk = v; break;
+    case 0x0A: t->ctrlpf = v; break;
+    case 0x0B: t->refp0 = (v & 0x08) != 0; break;
+    case 0x0C: t->refp1 = (v & 0x08) != 0; break;
+    case 0x0D: t->pf0 = v; break;
+    case 0x0E: t->pf1 = v; break;
+    case 0x0F: t->pf2 = v; break;
+    case 0x10: case 0x11: case 0x12: case 0x13: case 0x14:
+        t->pos[(addr & 0x3F) - 0x10] = orc_resp_pos(t); break;
+    case 0x1B: t->grp0_old = t->grp0; t->grp0 = v; break;
+    case 0x1C: t->grp1_old = t->grp1; t->grp1 = v; t->enabl_old = t->enabl; break;
+    case 0x1D: t->enam0 = (v & 0x02) != 0; break;
+    case 0x1E: t->enam1 = (v & 0x02) != 0; break;
+    case 0x1F: t->enabl = (v & 0x02) != 0; break;
+    case 0x20: case 0x21: case 0x22: case 0x23: case 0x24:
+        t->hm[(addr & 0x3F) - 0x20] = v; break;
+    case 0x25: t->vdelp0 = (v & 0x01) != 0; break;
+    case 0x26: t->vdelp1 = (v & 0x01) != 0; break;
+    case 0x27: t->vdelbl = (v & 0x01) != 0; break;
+    case 0x28: t->resmp0 = (v & 0x02) != 0; break;
+    case 0x29: t->resmp1 = (v & 0x02) != 0; break;
+    case 0x2A:
+        for (int i = 0; i < 5; i++) t->pos[i] = orc_hmove(t->pos[i], t->hm[i]);
+        break;
+    case 0x2B: memset(t->hm, 0, sizeof(t->hm)); break;
+    case 0x2C: memset(t->cx, 0, sizeof(t->cx)); break;
+    default: break;                                                /* 0x03, audio, unused */
+    }
+}
+
+/* ---------------------------------------------------------------- Pia (pia.rs) */
+typedef struct orc_pia {          /* Pia, pia.rs:26-44 */
+    uint8_t  ram[128];
+    uint8_t  pa_out, pa_ddr, pa_in, pb_out, pb_ddr, pb_in;
+    uint16_t timer_value, timer_prescaler, timer_select;
+    uint8_t  timer_underflow;
+} orc_pia;
+
+static void orc_pia_default(orc_pia* p)                            /* pia.rs:46-62 */
+{
+    memset(p, 0, sizeof(*p));
+    p->pa_in = 0xFF;
+    p->pb_in = 0x3F;
+    p->timer_prescaler = 1;
+    p->timer_select = 1;
+}
+
+static void orc_pia_tick_n(orc_pia* p, uint16_t n)                 /* pia.rs:107-166 */
+{
+    if (n == 0) return;
+    if (p->timer_value == 0 && p->timer_underflow) {
+        p->timer_value = (uint16_t)((uint16_t)(0xFF - (n - 1)) & 0xFF);
+        return;
+    }
+    uint16_t rem = n;
+    if (p->timer_prescaler > 0) {
+        if (rem < p->timer_prescaler) { p->timer_prescaler = (uint16_t)(p->timer_prescaler - rem); return; }
+        rem = (uint16_t)(rem - p->timer_prescaler);
+        p->timer_prescaler = 0;
+        if (p->timer_value == 0) {
+            p->timer_underflow = 1;
+            p->timer_value = 0xFF;
+            if (rem > 0) p->timer_value = (uint16_t)((uint16_t)(0xFF - (rem - 1)) & 0xFF);
+            return;
+        }
+        p->timer_value--;
+    }
+    if (rem == 0) { p->timer_prescaler = p->timer_select; return; }
+    uint16_t ps = p->timer_select;
+    uint16_t full = (uint16_t)(rem / ps);
+    uint16_t left = (uint16_t)(rem % ps);
+    if (full >= p->timer_value) {
+        uint16_t to_zero = (uint16_t)(p->timer_value * ps);        /* u16 arithmetic as in Rust */
+        rem = (uint16_t)(rem - to_zero);
+        p->timer_underflow = 1;
+        p->timer_value = 0xFF;
+        if (rem > 0) p->timer_value = (uint16_t)((uint16_t)(0xFF - (rem - 1)) & 0xFF);
+    } else {
+        p->timer_value = (uint16_t)(p->timer_value - full);
+        p->timer_prescaler = (uint16_t)(ps - left);
+    }
+}
+
+static uint8_t orc_pia_read(orc_pia* p, uint16_t addr)             /* pia.rs:169-199 */
+{
+    if (!(addr & 0x200)) return p->ram[addr & 0x7F];
+    switch (addr & 0x07) {
+    case 0x00: return (uint8_t)((p->pa_in & ~p->pa_ddr) | (p->pa_out & p->pa_ddr));
+    case 0x01: return p->pa_ddr;
+    case 0x02: return (uint8_t)((p->pb_in & ~p->pb_ddr) | (p->pb_out & p->pb_ddr));
+    case 0x03: return p->pb_ddr;
+    case 0x04: p->timer_underflow = 0; return (uint8_t)p->timer_value;
+    case 0x05: return p->timer_underflow ? 0x80 : 0x00;
+    default: return 0;
+    }
+}
+
+static void orc_pia_write(orc_pia* p, uint16_t addr, uint8_t v)    /* pia.rs:202-228 */
+{
+    static const uint16_t sel[4] = { 1, 8, 64, 1024 };
+    if (!(addr & 0x200)) { p->ram[addr & 0x7F] = v; return; }
+    if (addr & 0x10) {
+        p->timer_value = v;
+        p->timer_underflow = 0;
+        p->timer_select = sel[addr & 3];
+        p->timer_prescaler = p->timer_select;
+        return;
+    }
+    switch (addr & 0x03) {
+    case 0: p->pa_out = v; break;
+    case 1: p->pa_ddr = v; break;
+    case 2: p->pb_out = v; break;
+    default: p->pb_ddr = v; break;
+    }
+}
+
+/* ------------------------------------------------- HeadlessBus + HeadlessAtari */
+struct orc_atari {
+    orc_cpu  cpu;
+    orc_tia  tia;
+    orc_pia  pia;
+    uint8_t  mem[8192];           /* HeadlessBus::mem, atari.rs:402 */
+    uint8_t* rom;
+    size_t   rom_len;
+    int      bank;
+    int      scheme;
+    uint32_t frame_no;
+    uint32_t run_status;
+    uint64_t instructions;
+};
+
+static int orc_detect(size_t len)                                  /* atari.rs:96-105 */
+{
+    if (len <= 4096) return FA_SCHEME_FIXED;
+    if (len <= 8192) return FA_SCHEME_F8;
+    if (len <= 16384) return FA_SCHEME_F6;
+    return FA_SCHEME_F4;
+}
+
+/* Lengths for which HeadlessBus::new does not panic: the power-on bank's
+ * slice rom[bank*4096 .. bank*4096+4096] must exist (atari.rs:412-448), and
+ * the Fixed mirror i % rom_len needs rom_len > 0. */
+static int orc_rom_len_ok(size_t len)
+{
+    if (len == 0) return 0;
+    switch (orc_detect(len)) {
+    case FA_SCHEME_FIXED: return 1;
+    case FA_SCHEME_F8: return len >= 8192;
+    case FA_SCHEME_F6: return len >= 16384;
+    default: return len >= 32768;
+    }
+}
+
+static void orc_load_bank(orc_atari* e, int bank)                  /* atari.rs:433-449 */
+{
+    if (e->scheme == FA_SCHEME_FIXED) {
+        for (int i = 0; i < 4096; i++) e->mem[0x1000 + i] = e->rom[(size_t)i % e->rom_len];
+        return;
+    }
+    memcpy(&e->mem[0x1000], &e->rom[(size_t)bank * 4096], 4096);
+}
+
+static void orc_sync_ram_to_mem(orc_atari* e)                      /* atari.rs:454-457 */
+{
+    memcpy(&e->mem[0x80], e->pia.ram, 128);
+    memcpy(&e->mem[0x180], e->pia.ram, 128);
+}
+
+static inline void orc_check_bankswitch(orc_atari* e, uint16_t addr) /* atari.rs:460-492 */
+{
+    uint16_t a = addr & 0x1FFF;
+    int nb;
+    switch (e->scheme) {
+    case FA_SCHEME_F8: if (a < 0x1FF8 || a > 0x1FF9) return; nb = a - 0x1FF8; break;
+    case FA_SCHEME_F6: if (a < 0x1FF6 || a > 0x1FF9) return; nb = a - 0x1FF6; break;
+    case FA_SCHEME_F4: if (a < 0x1FF4 || a > 0x1FFB) return; nb = a - 0x1FF4; break;
+    default: return;
+    }
+    if (nb != e->bank) {
+        e->bank = nb;
+        orc_load_bank(e, nb);
+    }
+}
+
+static inline uint8_t orc_bus_read(orc_atari* e, uint16_t addr)   /* atari.rs:497-520 */
+{
+    uint16_t a = addr & 0x1FFF;
+    if ((a & 0x1080) != 0 && (a & 0x1280) != 0x0280) {
+        if ((a & 0x1000) && e->scheme != FA_SCHEME_FIXED) orc_check_bankswitch(e, addr);
+        return e->mem[a];
+    }
+    if ((a & 0x1280) == 0x0280) return orc_pia_read(&e->pia, a);
+    if ((a & 0x1080) == 0) return orc_tia_read(&e->tia, a);
+    return 0;
+}
+
+static inline void orc_bus_write(orc_atari* e, uint16_t addr, uint8_t v) /* atari.rs:523-552 */
+{
+    uint16_t a = addr & 0x1FFF;
+    if (a & 0x1000) {
+        if (e->scheme != FA_SCHEME_FIXED) orc_check_bankswitch(e, addr);
+        return;
+    }
+    if ((a & 0x80) && !(a & 0x200)) {
+        e->pia.ram[a & 0x7F] = v;
+        e->mem[(a | 0x80) & 0x1FF] = v;
+        e->mem[((a | 0x80) & 0x1FF) ^ 0x100] = v;
+        return;
+    }
+    if (a & 0x200) { orc_pia_write(&e->pia, a, v); return; }
+    orc_tia_write(&e->tia, a, v);
+}
+
+/* Cpu::step on the Atari bus. */
+#define STEP_FN orc_step_bus
+#define MEM_T orc_atari
+#define MREAD(m, a) orc_bus_read((m), (uint16_t)(a))
+#define MWRITE(m, a, v) orc_bus_write((m), (uint16_t)(a), (uint8_t)(v))
+#include "cpu_step.h"
+#undef STEP_FN
+#undef MEM_T
+#undef MREAD
+#undef MWRITE
+
+/* Cpu::step on FlatMemory (cpu.rs:69-90). */
+typedef struct orc_flat { uint8_t* ram; } orc_flat;
+#define STEP_FN orc_step_flat
+#define MEM_T orc_flat
+#define MREAD(m, a) ((m)->ram[(uint16_t)(a)])
+#define MWRITE(m, a, v) ((m)->ram[(uint16_t)(a)] = (uint8_t)(v))
+#include "cpu_step.h"
+#undef STEP_FN
+#undef MEM_T
+#undef MREAD
+#undef MWRITE
+
+static void orc_cpu_reset_bus(orc_atari* e)                        /* cpu.rs:125-134 */
+{
+    uint16_t lo = orc_bus_read(e, 0xFFFC);
+    uint16_t hi = orc_bus_read(e, 0xFFFD);
+    e->cpu.pc = (uint16_t)((hi << 8) | lo);
+    e->cpu.sp = 0xFD;
+    e->cpu.p = 0;
+    e->cpu.a = e->cpu.x = e->cpu.y = 0;
+}
+
+orc_atari* orc_create(const uint8_t* rom, size_t rom_len)          /* atari.rs:410-430, 562-569 */
+{
+    if (!rom || !orc_rom_len_ok(rom_len)) return NULL;
+    orc_atari* e = (orc_atari*)calloc(1, sizeof(orc_atari));
+    if (!e) return NULL;
+    e->rom = (uint8_t*)malloc(rom_len);
+    if (!e->rom) { free(e); return NULL; }
+    memcpy(e->rom, rom, rom_len);
+    e->rom_len = rom_len;
+    e->scheme = orc_detect(rom_len);
+    switch (e->scheme) {
+    case FA_SCHEME_FIXED: e->bank = 0; break;
+    case FA_SCHEME_F8: e->bank = 1; break;
+    case FA_SCHEME_F6: e->bank = 3; break;
+    default: e->bank = 7; break;
+    }
+    orc_tia_default(&e->tia);
+    orc_pia_default(&e->pia);
+    e->cpu.sp = 0xFD;                                              /* Cpu::default, cpu.rs:107-119 */
+    orc_load_bank(e, e->bank);
+    orc_sync_ram_to_mem(e);
+    orc_cpu_reset_bus(e);
+    return e;
+}
+
+orc_atari* orc_clone(const orc_atari* e)
+{
+    orc_atari* c = (orc_atari*)malloc(sizeof(orc_atari));
+    if (!c) return NULL;
+    memcpy(c, e, sizeof(*c));
+    c->rom = (uint8_t*)malloc(e->rom_len);
+    if (!c->rom) { free(c); return NULL; }
+    memcpy(c->rom, e->rom, e->rom_len);
+    return c;
+}
+
+void orc_destroy(orc_atari* e)
+{
+    if (!e) return;
+    free(e->rom);
+    free(e);
+}
+
+void orc_set_action(orc_atari* e, unsigned action)                 /* atari.rs:34-81, 571-582 */
+{
+    /* (up, down, left, right, fire) per Action::decode, indexed by from_index */
+    static const uint8_t dec[18][5] = {
+        {0,0,0,0,0}, {0,0,0,0,1}, {1,0,0,0,0}, {0,0,0,1,0}, {0,0,1,0,0}, {0,1,0,0,0},
+        {1,0,0,1,0}, {1,0,1,0,0}, {0,1,0,1,0}, {0,1,1,0,0}, {1,0,0,0,1}, {0,0,0,1,1},
+        {0,0,1,0,1}, {0,1,0,0,1}, {1,0,0,1,1}, {1,0,1,0,1}, {0,1,0,1,1}, {0,1,1,0,1},
+    };
+    const uint8_t* d = dec[action < 18 ? action : 0];
+    uint8_t swcha = 0xFF;
+    if (d[0]) swcha &= (uint8_t)~0x10;
+    if (d[1]) swcha &= (uint8_t)~0x20;
+    if (d[2]) swcha &= (uint8_t)~0x40;
+    if (d[3]) swcha &= (uint8_t)~0x80;
+    e->pia.pa_in = swcha;
+    e->tia.inpt4 = !d[4];
+    e->tia.paddle0 = d[2] ? 200 : (d[3] ? 50 : 128);
+}
+
+static inline int orc_run_one_cycle(orc_atari* e, uint64_t* cycles) /* atari.rs:601-614 */
+{
+    if (e->tia.wsync) {
+        uint16_t skipped = orc_tia_skip_to_scanline_end(&e->tia);
+        orc_pia_tick_n(&e->pia, skipped);
+        *cycles += skipped;
+    } else {
+        uint8_t c = orc_step_bus(&e->cpu, e);
+        if (c == 0) { e->run_status |= FA_STATUS_ILLEGAL_OPCODE; return 0; }
+        e->instructions++;
+        *cycles += c;
+        orc_tia_tick_n(&e->tia, c);
+        orc_pia_tick_n(&e->pia, c);
+    }
+    return 1;
+}
+
+uint64_t orc_run_frame(orc_atari* e)                               /* atari.rs:584-598 */
+{
+    if (e->run_status & FA_STATUS_HALT_MASK) return 0;
+    e->tia.frame_complete = 0;
+    uint64_t cycles = 0;
+    while (e->tia.vsync & 0x02) {
+        if (!orc_run_one_cycle(e, &cycles)) return cycles;
+        /* The reference has no bound here; a ROM that holds VSYNC forever
+         * hangs it.  The oracle and the device stop such an instance. */
+        if (cycles > FA_VSYNC_BUDGET) { e->run_status |= FA_STATUS_VSYNC_BUDGET; return cycles; }
+    }
+    while (!(e->tia.vsync & 0x02)) {
+        if (!orc_run_one_cycle(e, &cycles)) return cycles;
+        if (cycles > FA_FRAME_CYCLE_CAP) { e->run_status |= FA_STATUS_CYCLE_CAP; break; }
+    }
+    e->frame_no++;
+    return cycles;
+}
+
+void orc_ram(const orc_atari* e, uint8_t* out128)                  /* atari.rs:617-619 */
+{
+    memcpy(out128, &e->mem[0x80], 128);
+}
+
+uint64_t orc_instructions(const orc_atari* e) { return e->instructions; }
+
+void orc_get_state(const orc_atari* e, fa_state* s)                /* cuda_env.rs:44-93 */
+{
+    const orc_tia* t = &e->tia;
+    const orc_pia* p = &e->pia;
+    memset(s, 0, sizeof(*s));
+    s->a = e->cpu.a; s->x = e->cpu.x; s->y = e->cpu.y; s->sp = e->cpu.sp;
+    s->pc = e->cpu.pc; s->status = e->cpu.p;
+    memcpy(s->ram, p->ram, 128);
+    s->port_a_output = p->pa_out; s->port_a_ddr = p->pa_ddr; s->port_a_input = p->pa_in;
+    s->port_b_output = p->pb_out; s->port_b_ddr = p->pb_ddr; s->port_b_input = p->pb_in;
+    s->timer_value = p->timer_value; s->timer_prescaler = p->timer_prescaler;
+    s->timer_prescaler_select = p->timer_select; s->timer_underflow = p->timer_underflow;
+    s->tia_clock = t->clock; s->tia_scanline = t->scanline;
+    s->tia_wsync = t->wsync; s->tia_frame_complete = t->frame_complete;
+    s->tia_vsync = t->vsync; s->tia_vblank = t->vblank;
+    s->cxm0p = t->cx[0]; s->cxm1p = t->cx[1]; s->cxp0fb = t->cx[2]; s->cxp1fb = t->cx[3];
+    s->cxm0fb = t->cx[4]; s->cxm1fb = t->cx[5]; s->cxblpf = t->cx[6]; s->cxppmm = t->cx[7];
+    s->inpt4 = t->inpt4; s->inpt5 = t->inpt5; s->paddle0 = t->paddle0; s->paddle1 = t->paddle1;
+    s->paddle_counter = t->paddle_counter; s->paddle_dumped = t->paddle_dumped;
+    s->pos_p0 = t->pos[0]; s->pos_p1 = t->pos[1]; s->pos_m0 = t->pos[2];
+    s->pos_m1 = t->pos[3]; s->pos_bl = t->pos[4];
+    s->hmp0 = t->hm[0]; s->hmp1 = t->hm[1]; s->hmm0 = t->hm[2]; s->hmm1 = t->hm[3]; s->hmbl = t->hm[4];
+    s->grp0 = t->grp0; s->grp1 = t->grp1; s->grp0_old = t->grp0_old; s->grp1_old = t->grp1_old;
+    s->enam0 = t->enam0; s->enam1 = t->enam1; s->enabl = t->enabl; s->enabl_old = t->enabl_old;
+    s->vdelp0 = t->vdelp0; s->vdelp1 = t->vdelp1; s->vdelbl = t->vdelbl;
+    s->resmp0 = t->resmp0; s->resmp1 = t->resmp1; s->nusiz0 = t->nusiz0; s->nusiz1 = t->nusiz1;
+    s->colup0 = t->colup0; s->colup1 = t->colup1; s->colupf = t->colupf; s->colubk = t->colubk;
+    s->ctrlpf = t->ctrlpf; s->refp0 = t->refp0; s->refp1 = t->refp1;
+    s->pf0 = t->pf0; s->pf1 = t->pf1; s->pf2 = t->pf2;
+    s->bank = (uint8_t)e->bank; s->scheme = (uint8_t)e->scheme;
+    s->cycles = e->cpu.cycles;
+    s->frame_no = e->frame_no;
+    s->run_status = e->run_status;
+}
+
+void orc_set_state(orc_atari* e, const fa_state* s)
+{
+    orc_tia* t = &e->tia;
+    orc_pia* p = &e->pia;
+    e->cpu.a = s->a; e->cpu.x = s->x; e->cpu.y = s->y; e->cpu.sp = s->sp;
+    e->cpu.pc = s->pc; e->cpu.p = s->status; e->cpu.cycles = s->cycles;
+    memcpy(p->ram, s->ram, 128);
+    p->pa_out = s->port_a_output; p->pa_ddr = s->port_a_ddr; p->pa_in = s->port_a_input;
+    p->pb_out = s->port_b_output; p->pb_ddr = s->port_b_ddr; p->pb_in = s->port_b_input;
+    p->timer_value = s->timer_value; p->timer_prescaler = s->timer_prescaler;
+    p->timer_select = s->timer_prescaler_select; p->timer_underflow = s->timer_underflow;
+    t->clock = s->tia_clock; t->scanline = s->tia_scanline;
+    t->wsync = s->tia_wsync; t->frame_complete = s->tia_frame_complete;
+    t->vsync = s->tia_vsync; t->vblank = s->tia_vblank;
+    t->cx[0] = s->cxm0p; t->cx[1] = s->cxm1p; t->cx[2] = s->cxp0fb; t->cx[3] = s->cxp1fb;
+    t->cx[4] = s->cxm0fb; t->cx[5] = s->cxm1fb; t->cx[6] = s->cxblpf; t->cx[7] = s->cxppmm;
+    t->inpt4 = s->inpt4; t->inpt5 = s->inpt5; t->paddle0 = s->paddle0; t->paddle1 = s->paddle1;
+    t->paddle_counter = s->paddle_counter; t->paddle_dumped = s->paddle_dumped;
+    t->pos[0] = s->pos_p0; t->pos[1] = s->pos_p1; t->pos[2] = s->pos_m0;
+    t->pos[3] = s->pos_m1; t->pos[4] = s->pos_bl;
+    t->hm[0] = s->hmp0; t->hm[1] = s->hmp1; t->hm[2] = s->hmm0; t->hm[3] = s->hmm1; t->hm[4] = s->hmbl;
+    t->grp0 = s->grp0; t->grp1 = s->grp1; t->grp0_old = s->grp0_old; t->grp1_old = s->grp1_old;
+    t->enam0 = s->enam0; t->enam1 = s->enam1; t->enabl = s->enabl; t->enabl_old = s->enabl_old;
+    t->vdelp0 = s->vdelp0; t->vdelp1 = s->vdelp1; t->vdelbl = s->vdelbl;
+    t->resmp0 = s->resmp0; t->resmp1 = s->resmp1; t->nusiz0 = s->nusiz0; t->nusiz1 = s->nusiz1;
+    t->colup0 = s->colup0; t->colup1 = s->colup1; t->colupf = s->colupf; t->colubk = s->colubk;
+    t->ctrlpf = s->ctrlpf; t->refp0 = s->refp0; t->refp1 = s->refp1;
+    t->pf0 = s->pf0; t->pf1 = s->pf1; t->pf2 = s->pf2;
+    e->frame_no = s->frame_no;
+    e->run_status = s->run_status;
+    /* The bank index is clamped to the scheme's range when the flat array is
+     * rebuilt; the scheme itself always follows the ROM. */
+    int nb = s->bank;
+    int maxb = e->scheme == FA_SCHEME_F8 ? 1 : e->scheme == FA_SCHEME_F6 ? 3 : e->scheme == FA_SCHEME_F4 ? 7 : 0;
+    if (nb > maxb) nb = maxb;
+    e->bank = nb;
+    orc_load_bank(e, nb);
+    orc_sync_ram_to_mem(e);
+}
+
+int orc_reset_state(const uint8_t* rom, size_t rom_len, fa_state* out) /* cuda_env.rs:134-139 */
+{
+    orc_atari* e = orc_create(rom, rom_len);
+    if (!e) return -1;
+    orc_run_frame(e);
+    e->frame_no = 0;
+    orc_get_state(e, out);
+    orc_destroy(e);
+    return 0;
+}
+
+/* ------------------------------------------------------- batch runner (CPU) */
+typedef struct orc_job {
+    const uint8_t* rom; size_t rom_len; size_t n; int k;
+    fa_state* states; const uint8_t* actions; const fa_state* snapshot;
+    uint32_t episode_frames; uint8_t* obs; uint8_t* trace;
+    int tid, nthreads, pin, err;
+    uint64_t instructions;
+} orc_job;
+
+static void* orc_worker(void* arg)
+{
+    orc_job* j = (orc_job*)arg;
+    if (j->pin) {
+        cpu_set_t set;
+        CPU_ZERO(&set);
+        CPU_SET(j->tid, &set);
+        pthread_setaffinity_np(pthread_self(), sizeof(set), &set);
+    }
+    orc_atari* e = orc_create(j->rom, j->rom_len);
+    if (!e) { j->err = 1; return NULL; }
+    /* Contiguous instance range per thread: one emulator per core at a time,
+     * as the reference CPU benchmark runs one HeadlessAtari per OS thread. */
+    size_t per = (j->n + (size_t)j->nthreads - 1) / (size_t)j->nthreads;
+    size_t lo = per * (size_t)j->tid, hi = lo + per;
+    if (hi > j->n) hi = j->n;
+    for (size_t i = lo; i < hi; i++) {
+        orc_set_state(e, &j->states[i]);
+        uint64_t before = e->instructions;
+        for (int f = 0; f < j->k; f++) {
+            if (j->episode_frames && e->frame_no >= j->episode_frames && j->snapshot)
+                orc_set_state(e, j->snapshot);
+            orc_set_action(e, j->actions[(size_t)f * j->n + i]);
+            orc_run_frame(e);
+            if (j->trace) orc_ram(e, &j->trace[((size_t)f * j->n + i) * 128]);
+        }
+        j->instructions += e->instructions - before;
+        orc_get_state(e, &j->states[i]);
+        if (j->obs) orc_ram(e, &j->obs[i * 128]);
+    }
+    orc_destroy(e);
+    return NULL;
+}
+
+static uint64_t orc_run_batch_impl(const uint8_t* rom, size_t rom_len, size_t n, int k,
+                                   fa_state* states, const uint8_t* actions,
+                                   const fa_state* snapshot, uint32_t episode_frames,
+                                   uint8_t* obs, uint8_t* trace, int nthreads, int pin)
+{
+    if (!rom || !states || (k > 0 && !actions) || k < 0 || !orc_rom_len_ok(rom_len)) return (uint64_t)-1;
+    if (nthreads < 1) nthreads = 1;
+    if ((size_t)nthreads > n && n > 0) nthreads = (int)n;
+    orc_job* jobs = (orc_job*)calloc((size_t)nthreads, sizeof(orc_job));
+    pthread_t* th = (pthread_t*)calloc((size_t)nthreads, sizeof(pthread_t));
+    if (!jobs || !th) { free(jobs); free(th); return (uint64_t)-1; }
+    for (int t = 0; t < nthreads; t++) {
+        jobs[t] = (orc_job){ rom, rom_len, n, k, states, actions, snapshot, episode_frames,
+                             obs, trace, t, nthreads, pin, 0, 0 };
+    }
+    for (int t = 1; t < nthreads; t++) pthread_create(&th[t], NULL, orc_worker, &jobs[t]);
+    orc_worker(&jobs[0]);
+    uint64_t total = jobs[0].instructions;
+    int err = jobs[0].err;
+    for (int t = 1; t < nthreads; t++) {
+        pthread_join(th[t], NULL);
+        total += jobs[t].instructions;
+        err |= jobs[t].err;
+    }
+    free(jobs);
+    free(th);
+    return err ? (uint64_t)-1 : total;
+}
+
+uint64_t orc_run_batch(const uint8_t* rom, size_t rom_len, size_t n, int k,
+                       fa_state* states, const uint8_t* actions,
+                       const fa_state* snapshot, uint32_t episode_frames,
+                       uint8_t* obs, int nthreads, int pin)
+{
+    return orc_run_batch_impl(rom, rom_len, n, k, states, actions, snapshot,
+                              episode_frames, obs, NULL, nthreads, pin);
+}
+
+uint64_t orc_run_batch_trace(const uint8_t* rom, size_t rom_len, size_t n, int k,
+                             fa_state* states, const uint8_t* actions,
+                             const fa_state* snapshot, uint32_t episode_frames,
+                             uint8_t* ram_trace, int nthreads)
+{
+    return orc_run_batch_impl(rom, rom_len, n, k, states, actions, snapshot,
+                              episode_frames, NULL, ram_trace, nthreads, 0);
+}
+
+/* ------------------------------------------------- FlatMemory KAT runner */
+int orc_flat_run_from(uint8_t* mem64k, int nsteps, uint8_t* cycles_out, orc_regs* r)
+{
+    orc_cpu c = { r->pc, r->sp, r->a, r->x, r->y, r->p, r->cycles };
+    orc_flat m = { mem64k };
+    int i;
+    for (i = 0; i < nsteps; i++) {
+        uint8_t cy = orc_step_flat(&c, &m);
+        if (cycles_out) cycles_out[i] = cy;
+        if (cy == 0) break;
+    }
+    r->pc = c.pc; r->sp = c.sp; r->a = c.a; r->x = c.x; r->y = c.y; r->p = c.p; r->cycles = c.cycles;
+    return i;
+}
+
+int orc_flat_run(uint8_t* mem64k, int nsteps, uint8_t* cycles_out, orc_regs* r)
+{
+    /* Cpu::new + Cpu::reset (cpu.rs:107-134) */
+    orc_regs s;
+    memset(&s, 0, sizeof(s));
+    s.pc = (uint16_t)(mem64k[0xFFFC] | (mem64k[0xFFFD] << 8));
+    s.sp = 0xFD;
+    int n = orc_flat_run_from(mem64k, nsteps, cycles_out, &s);
+    *r = s;
+    return n;
+}
+
+size_t orc_state_size(void) { return sizeof(fa_state); }

@@ -1,0 +1,67 @@
+"""C ABI checks that need no GPU: the library loads, exports every symbol the
+public header declares, and its state layout matches the header and the
+oracle's restatement of the reference AtariStateGpu (src/cuda_env.rs:10-38)."""
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from fa_pkg import ROOT, fa
+import oracle
+
+HEADER = ROOT / "include" / "fast_atari.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fa_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    out = subprocess.run(["nm", "-D", "--defined-only", str(fa.LIB_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r" T (fa_[a-z0-9_]+)$", out, flags=re.M))
+    missing = [s for s in declared_functions() if s not in exported]
+    assert not missing, missing
+    assert len(declared_functions()) >= 20
+
+
+def test_binding_covers_header():
+    assert set(declared_functions()) == set(fa._SIGS)
+
+
+def test_library_loads_and_reports_version():
+    L = fa.lib()
+    assert b"sm_100a" in L.fa_version()
+
+
+def test_state_dtype_matches_oracle_and_header():
+    assert fa.STATE_DTYPE == oracle.STATE_DTYPE
+    assert oracle.lib().orc_state_size() == 240
+    off = {n: fa.STATE_DTYPE.fields[n][1] for n in fa.STATE_DTYPE.names}
+    # offsets pinned by FA_STATIC_ASSERT in include/fast_atari.h
+    assert (off["ram"], off["timer_value"], off["tia_clock"], off["paddle_counter"],
+            off["pos_p0"], off["bank"], off["cycles"], off["run_status"]) == (8, 142, 152, 172, 176, 217, 224, 236)
+    # the reference AtariStateGpu prefix ends at its _pad_end (221 bytes)
+    assert off["_pad_end"] + 2 == 221
+
+
+def test_no_device_fails_loudly():
+    if fa.device_count() > 0:
+        pytest.skip("a GPU is visible")
+    with pytest.raises(fa.FaError) as ei:
+        fa.BatchAtariGpu(bytes(4096), 4)
+    assert ei.value.code == -4
+
+
+def test_bad_rom_lengths_rejected_before_device():
+    # fa_create validates the ROM before touching the device only when one
+    # exists; without one it reports no-device.  The oracle rejects the same
+    # lengths the reference's HeadlessBus::new panics on.
+    for n in (0, 5000, 9000, 20000):
+        with pytest.raises(ValueError):
+            oracle.Atari(bytes(n))
+    for n in (1, 2048, 4096, 8192, 16384, 32768, 40000):
+        oracle.Atari(bytes([0xEA] * n))
