@@ -21,6 +21,15 @@
 namespace fa {
 
 // ------------------------------------------------------------------ TMA / mbarrier
+constexpr uint64_t FA_WAIT_LIMIT_NS = 2000000000ull;   // 2 s
+
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
 {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -70,9 +79,13 @@ __device__ bool stage_rom(uint8_t* dst, const uint8_t* src, uint32_t bytes, uint
         mbar_expect_tx(bar, bytes);
         for (uint32_t off = 0; off < bytes; off += 4096u) bulk_g2s(dst + off, src + off, 4096u, bar);
     }
+    // Bounded in time, not in iterations: one try_wait may suspend for an
+    // implementation-defined interval.
     bool ok = false;
-    for (uint32_t it = 0; it < (1u << 22); it++) {
+    const uint64_t t0 = globaltimer_ns();
+    while (true) {
         if (mbar_try_wait(bar, phase)) { ok = true; break; }
+        if (globaltimer_ns() - t0 > FA_WAIT_LIMIT_NS) break;
     }
     phase ^= 1u;
     return ok;
@@ -181,7 +194,10 @@ __device__ __forceinline__ void run_lanes(Runner<BLOCK>& r, uint32_t sched)
             if (!act) key = 0xFFFFFFFFu;
             const uint32_t mk = __reduce_min_sync(FULL, key);
             const uint32_t lead = __ffs(__ballot_sync(FULL, key == mk)) - 1u;
-            go = act && pcb == __shfl_sync(FULL, pcb, lead);
+            // Every lane must take part in the full-mask shuffle, so it is
+            // not folded into a short-circuit condition.
+            const uint32_t lpcb = __shfl_sync(FULL, pcb, lead);
+            go = act && pcb == lpcb;
         } else {
             if (!__any_sync(FULL, act)) break;
             go = act;
