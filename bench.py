@@ -1,0 +1,394 @@
+"""Benchmark of the batched Atari 2600 core on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mixed|divergence|plain|scale]
+
+Default workload (the batched configuration the headline metric is quoted
+on): four seeded synthetic carts — 2K Fixed, 8K F8, 16K F6, 32K F4 with
+WSYNC density 100/50/10/0% — at 100,000 / 30,000 / 5,000 / 500 instances,
+K=4 frames per call, int8 actions uniform over 18 precomputed per frame.
+One step = one batched call (K frames of every instance), launched as one
+persistent kernel over all four carts.  Beside it the same trace runs through
+the plain form (one launch per frame per cart) for the batched-vs-plain
+ratio, and once more as one CUDA graph of all timed calls.
+
+`value` is device time (CUDA events on the launching stream, L2 flushed
+before every timed call); `e2e` is the same metric through the public C ABI
+with host buffers (pinned staging, H2D actions and D2H observations inside
+the timed region).  Under torchrun every rank runs its own replica of the
+workload on its GPU (instances are independent: weak scaling, no exchange).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "fast-atari-rs_b200"
+
+METRIC = "frames/s bit-exact: batched/served vs plain kernel, 1 B200; p99 step latency"
+UNIT = "frames/s"
+
+# SASS thread-instructions per emulated 6502 instruction when all 32 lanes of
+# a warp run identical instances (fully converged), from the ncu capture in
+# profiles/fa_run_converged_icount.md.  Used to express guest-instruction
+# throughput in warp-issue slots for the roofline.
+I_CONV = 62.0
+# DRAM bytes moved per instance-frame by fa_run on this workload, from the ncu
+# capture in profiles/fa_run_mixed_ncu.md (None until measured).
+DRAM_BYTES_PER_INSTANCE_FRAME = None
+
+
+def load_pkg():
+    if "fast_atari_b200" in sys.modules:
+        return sys.modules["fast_atari_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "fast_atari_b200", PKG_DIR / "__init__.py", submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["fast_atari_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# ------------------------------------------------------------------ workloads
+def workload(name: str, carts):
+    """(description, [(cart, n)], k, episode_frames)."""
+    if name == "mixed":
+        cs = carts.mixed_carts()
+        return ("mixed 4-cart batch: 2K Fixed/8K F8/16K F6/32K F4, WSYNC 100/50/10/0%, "
+                "100000/30000/5000/500 instances, K=4 frames per call",
+                list(zip(cs, carts.MIXED_COUNTS)), 4, 0)
+    if name == "divergence":
+        return ("divergence-heavy 8K F8 cart, 50000 instances, per-frame step (K=1)",
+                [(carts.divergence_cart(), 50_000)], 1, 0)
+    if name == "plain":
+        return ("plain 4K Fixed cart, 1000 instances, per-frame step (K=1)",
+                [(carts.plain_cart(), 1000)], 1, 0)
+    if name == "scale":
+        return ("scale: 1000000 instances of the 32K F4 cart, K=16, reset every 2000 frames",
+                [(carts.scale_cart(), 1_000_000)], 16, 2000)
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3] not in ("", "[N/A]"))}
+
+
+# ------------------------------------------------------------------ CPU reference
+def cpu_reference(carts, spec, k, seconds_target=15.0):
+    """The oracle (a C restatement of the reference's HeadlessAtari) on the
+    host cores: each cart's sample instances run k-frame calls with all
+    threads; instance counts are proportional to the workload's."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    cores = os.cpu_count() or 1
+    total = sum(n for _, n in spec)
+    per_cart = [(c, max(1, round(n * 4 * cores / total))) for c, n in spec]
+    states = {c.spec.name: np.array([oracle.reset_state(c.rom)] * m, dtype=oracle.STATE_DTYPE)
+              for c, m in per_cart}
+    frames = 0
+    t0 = time.perf_counter()
+    call = 0
+    while True:
+        for c, m in per_cart:
+            acts = carts.actions(seed=7, n=m, frames=k, frame0=call * k)
+            oracle.run_batch(c.rom, states[c.spec.name], acts, k, nthreads=cores, pin=False)
+            frames += m * k
+        call += 1
+        if time.perf_counter() - t0 >= seconds_target:
+            break
+    dt = time.perf_counter() - t0
+    sample = ", ".join(f"{m} x {c.spec.name}" for c, m in per_cart)
+    return frames / dt, cores, f"{call} calls of K={k} frames over [{sample}] ({frames} instance-frames, {dt:.1f} s)"
+
+
+def run_reference_arm(args, carts, rank, world):
+    desc, spec, k, _ = workload(args.workload, carts)
+    if rank != 0:
+        return
+    # Each step is one bounded CPU sample; warmup steps are run untimed.
+    per_step_s = max(2.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
+    vals = []
+    for i in range(args.warmup + args.steps):
+        fps, cores, sample = cpu_reference(carts, spec, k, seconds_target=per_step_s)
+        if i >= args.warmup:
+            vals.append(fps)
+    value = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": desc, "parallelism": "one emulator per host thread"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample + "; C restatement of the reference HeadlessAtari"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_gpu_arm(args, fa, carts, rank, world, local_rank):
+    import torch
+    desc, spec, k, episode = workload(args.workload, carts)
+    fa.set_device(local_rank)
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    pool = fa.AtariPool()
+    groups = []
+    for c, n in spec:
+        g = pool.add_cart(c.rom, n)
+        groups.append(g)
+    if episode:
+        # Periodic reset to the post-init snapshot with per-instance phase
+        # offsets uniform in [0, episode).
+        rng = np.random.default_rng(1234 + rank)
+        for g, (c, n) in zip(groups, spec):
+            view = pool.group(g)
+            view.set_episode_frames(episode)
+            view.set_frame_numbers(rng.integers(0, episode, n, dtype=np.uint32))
+    tuning = args.tuning
+    for g, (c, n) in zip(groups, spec):
+        t = tuning.get(c.spec.name, {})
+        pool.set_group(g, t.get("sched", "pc"), float(t.get("weight", 1.0 + c.spec.rom_size / 32768.0)))
+    pool.set_launch(args.block, True)
+
+    calls = args.warmup + args.steps
+    # Device-resident actions for every call: per cart [calls, k, n] uint8.
+    d_act = []
+    for gi, (c, n) in enumerate(spec):
+        t = torch.empty(calls * k * n, dtype=torch.uint8, device=dev)
+        chunk = max(1, (64 << 20) // max(1, k * n))
+        for c0 in range(0, calls, chunk):
+            c1 = min(calls, c0 + chunk)
+            a = carts.actions(seed=1000 * rank + 17 * gi + 1, n=n, frames=(c1 - c0) * k, frame0=c0 * k)
+            t[c0 * k * n:c1 * k * n].copy_(torch.from_numpy(a.reshape(-1)))
+        d_act.append(t)
+    d_obs = [torch.empty(n * 128, dtype=torch.uint8, device=dev) for _, n in spec]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)       # > 126 MB L2
+    stream = torch.cuda.ExternalStream(pool.stream(), device=dev)
+    sptr = pool.stream()
+    torch.cuda.synchronize()
+
+    def acts_at(call):
+        return [d_act[gi].data_ptr() + call * k * n for gi, (_, n) in enumerate(spec)]
+
+    obs_ptrs = [o.data_ptr() for o in d_obs]
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed_calls(step_fn, first_call, ncalls):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(ncalls)]
+        with torch.cuda.stream(stream):
+            for i in range(ncalls):
+                flush.zero_()
+                evs[i][0].record(stream)
+                step_fn(acts_at(first_call + i), k, obs_ptrs, sptr)
+                evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    # ---- warmup (batched and plain forms)
+    for i in range(args.warmup):
+        pool.step_async(acts_at(i), k, obs_ptrs, sptr)
+    pool.synchronize()
+    # ---- timed: batched persistent form
+    barrier()
+    pool.reset_counters()
+    with ClockSampler(local_rank) as clk:
+        ms = timed_calls(pool.step_async, args.warmup, args.steps)
+    pool.synchronize()
+    instr = pool.last_instructions()
+    slots = pool.last_lane_slots()
+    clocks = clk.summary()
+    total_ms = sum(ms)
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    n_total = sum(n for _, n in spec)
+    frames = n_total * k * args.steps * world
+    value = frames / (total_ms / 1e3)
+
+    # ---- the plain kernel on the same trace (one launch per frame per cart)
+    plain_steps = max(3, min(args.steps, 20))
+    pool.step_plain_async(acts_at(0), k, obs_ptrs, sptr)
+    pool.synchronize()
+    barrier()
+    ms_plain = timed_calls(pool.step_plain_async, args.warmup, plain_steps)
+    plain_value = n_total * k * plain_steps / (sum(ms_plain) / 1e3)
+
+    # ---- the whole timed trace as one CUDA graph (no flushes between calls)
+    graph_value = None
+    if not args.no_graph:
+        graph = pool.graph([d.data_ptr() + args.warmup * k * n for d, (_, n) in zip(d_act, spec)], k,
+                           args.steps, obs_ptrs)
+        graph.launch()
+        pool.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        graph.launch(sptr)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        graph_value = n_total * k * args.steps / (e0.elapsed_time(e1) / 1e3)
+        graph.close()
+
+    # ---- end to end through the public API with host buffers
+    e2e_steps = max(3, min(args.steps, 30))
+    host_acts = [[np.ascontiguousarray(d_act[gi][(args.warmup + i) * k * n:(args.warmup + i + 1) * k * n].cpu().numpy())
+                  for gi, (_, n) in enumerate(spec)] for i in range(e2e_steps)]
+    pool.step(host_acts[0], k, obs=True)
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        obs = pool.step(host_acts[i], k, obs=True)
+    e2e_s = time.perf_counter() - t0
+    del obs
+    e2e_value = n_total * k * e2e_steps * world / e2e_s
+    h2d = n_total * k
+    d2h = n_total * 128
+
+    # ---- roofline: guest instructions in warp-issue slots vs SM issue peak
+    guest_per_s = instr / (total_ms / 1e3)
+    f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    peak = 148 * 4 * f_sm                        # warp-instructions per second
+    achieved = guest_per_s * I_CONV / 32.0
+    traffic = None
+    if DRAM_BYTES_PER_INSTANCE_FRAME is not None:
+        traffic = DRAM_BYTES_PER_INSTANCE_FRAME * n_total * k
+
+    lat = sorted(ms)
+    p = lambda q: lat[min(len(lat) - 1, int(round(q * (len(lat) - 1))))]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": desc, "instances": n_total, "frames_per_call": k,
+                   "launch": f"one persistent kernel per call, block {args.block}",
+                   "l2": "flushed (256 MB write) before every timed call",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "issue", "achieved": achieved / 1e12, "peak": peak / 1e12,
+                     "unit": "T warp-inst/s", "frac": achieved / peak, "traffic": traffic,
+                     "note": f"guest 6502 instr/s x {I_CONV} SASS thread-instr per guest instr (converged) / 32"},
+        "plain_kernel": {"value": plain_value, "unit": UNIT, "steps": plain_steps,
+                         "form": "one launch per frame per cart"},
+        "batched_vs_plain": value / plain_value,
+        "graph": {"value": graph_value, "unit": UNIT, "calls": args.steps} if graph_value else None,
+        "step_latency_ms": {"p50": p(0.5), "p99": p(0.99), "max": lat[-1]},
+        "guest_instructions_per_s": guest_per_s,
+        "lane_efficiency": instr / slots if slots else None,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        fps, cores, sample = cpu_reference(carts, spec, k, seconds_target=args.cpu_seconds)
+        line["cpu_baseline"] = {"value": fps, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": sample + "; C restatement of the reference HeadlessAtari"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    pool.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mixed", choices=["mixed", "divergence", "plain", "scale"])
+    ap.add_argument("--block", type=int, default=128)
+    ap.add_argument("--tuning", default=None, help="JSON file of per-cart tuning records")
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    args.tuning = json.load(open(args.tuning)) if args.tuning else {}
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    fa = load_pkg()
+    from fast_atari_b200 import carts
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, carts, rank, world)
+        else:
+            run_gpu_arm(args, fa, carts, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -64,6 +64,7 @@ _SIGS = {
     "fa_last_error": (ctypes.c_char_p, []),
     "fa_version": (ctypes.c_char_p, []),
     "fa_device_count": (_i, []),
+    "fa_set_device": (_i, [_i]),
     "fa_create": (_i, [_u8p, _sz, _sz, ctypes.POINTER(_vp)]),
     "fa_destroy": (None, [_vp]),
     "fa_num_envs": (_sz, [_vp]),
@@ -82,8 +83,28 @@ _SIGS = {
     "fa_set_launch": (_i, [_vp, _i, _i, _i]),
     "fa_get_launch": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "fa_last_instructions": (ctypes.c_ulonglong, [_vp]),
+    "fa_last_lane_slots": (ctypes.c_ulonglong, [_vp]),
     "fa_get_snapshot": (_i, [_vp, _vp]),
     "fa_device_state": (_vp, [_vp, ctypes.POINTER(_u32)]),
+    "fa_pool_create": (_i, [ctypes.POINTER(_vp)]),
+    "fa_pool_destroy": (None, [_vp]),
+    "fa_pool_add_cart": (_i, [_vp, _u8p, _sz, _sz, ctypes.POINTER(_i)]),
+    "fa_pool_num_groups": (_i, [_vp]),
+    "fa_pool_group": (_vp, [_vp, _i]),
+    "fa_pool_set_group": (_i, [_vp, _i, _i, ctypes.c_float]),
+    "fa_pool_set_launch": (_i, [_vp, _i, _i]),
+    "fa_pool_step": (_i, [_vp, _vp, _i, _vp]),
+    "fa_pool_step_plain": (_i, [_vp, _vp, _i, _vp]),
+    "fa_pool_step_async": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "fa_pool_step_plain_async": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "fa_pool_synchronize": (_i, [_vp]),
+    "fa_pool_reset_counters": (_i, [_vp]),
+    "fa_pool_last_instructions": (ctypes.c_ulonglong, [_vp]),
+    "fa_pool_last_lane_slots": (ctypes.c_ulonglong, [_vp]),
+    "fa_pool_stream": (_vp, [_vp]),
+    "fa_pool_graph_create": (_i, [_vp, _vp, _i, _i, _vp, ctypes.POINTER(_vp)]),
+    "fa_graph_launch": (_i, [_vp, _vp]),
+    "fa_graph_destroy": (None, [_vp]),
 }
 
 _lib: Optional[ctypes.CDLL] = None
@@ -123,22 +144,29 @@ def device_count() -> int:
     return int(lib().fa_device_count())
 
 
+def set_device(device: int) -> None:
+    _check(lib().fa_set_device(int(device)))
+
+
 class BatchAtariGpu:
     """n emulated consoles of one ROM, resident on the current CUDA device."""
 
-    def __init__(self, rom: bytes, n: int):
+    def __init__(self, rom: bytes, n: int, _handle=None):
         L = lib()
-        r = np.frombuffer(bytes(rom), dtype=np.uint8).copy()
-        h = _vp()
-        _check(L.fa_create(_u8(r), len(r), int(n), ctypes.byref(h)))
-        self._h = h
+        self._owned = _handle is None
+        if _handle is None:
+            r = np.frombuffer(bytes(rom), dtype=np.uint8).copy()
+            h = _vp()
+            _check(L.fa_create(_u8(r), len(r), int(n), ctypes.byref(h)))
+            _handle = h
+        self._h = _handle
         self.n = int(n)
         self.rom = bytes(rom)
-        self._obs = np.zeros((self.n, 128), np.uint8)
 
     def close(self) -> None:
         if getattr(self, "_h", None):
-            lib().fa_destroy(self._h)
+            if self._owned:
+                lib().fa_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -224,6 +252,9 @@ class BatchAtariGpu:
     def last_instructions(self) -> int:
         return int(lib().fa_last_instructions(self._h))
 
+    def last_lane_slots(self) -> int:
+        return int(lib().fa_last_lane_slots(self._h))
+
     def step_multi_async(self, d_actions: int, k: int, d_obs: int = 0, stream: int = 0) -> None:
         """Enqueue k frames from device actions (e.g. torch tensor data_ptr())."""
         _check(lib().fa_step_multi_async(self._h, _vp(d_actions), int(k), _vp(d_obs or None),
@@ -231,3 +262,115 @@ class BatchAtariGpu:
 
     def synchronize(self) -> None:
         _check(lib().fa_synchronize(self._h))
+
+
+def _ptrs(seq):
+    arr = (_vp * len(seq))()
+    for i, v in enumerate(seq):
+        arr[i] = v or None
+    return arr
+
+
+class AtariPool:
+    """Several carts' instance sets stepped together (the batched form)."""
+
+    def __init__(self):
+        h = _vp()
+        _check(lib().fa_pool_create(ctypes.byref(h)))
+        self._p = h
+        self.groups = []          # (rom, n)
+
+    def close(self) -> None:
+        if getattr(self, "_p", None):
+            lib().fa_pool_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add_cart(self, rom: bytes, n: int) -> int:
+        r = np.frombuffer(bytes(rom), dtype=np.uint8).copy()
+        g = _i()
+        _check(lib().fa_pool_add_cart(self._p, _u8(r), len(r), int(n), ctypes.byref(g)))
+        self.groups.append((bytes(rom), int(n)))
+        return g.value
+
+    def group(self, g: int) -> BatchAtariGpu:
+        """Non-owning view of group g's handle (states, status, episodes)."""
+        rom, n = self.groups[g]
+        return BatchAtariGpu(rom, n, _handle=_vp(lib().fa_pool_group(self._p, g)))
+
+    def set_group(self, g: int, sched="pc", weight: float = 1.0) -> None:
+        s = SCHED_NAMES[sched] if isinstance(sched, str) else int(sched)
+        _check(lib().fa_pool_set_group(self._p, g, s, float(weight)))
+
+    def set_launch(self, block: int = 128, persistent: bool = True) -> None:
+        _check(lib().fa_pool_set_launch(self._p, int(block), 1 if persistent else 0))
+
+    def _host_step(self, fn, actions, k, obs):
+        acts = [np.ascontiguousarray(a, dtype=np.uint8).reshape(-1) for a in actions]
+        for a, (_, n) in zip(acts, self.groups):
+            if a.size != k * n:
+                raise ValueError("actions size mismatch")
+        outs = [np.empty((n, 128), np.uint8) for _, n in self.groups] if obs else None
+        _check(fn(self._p, _ptrs([a.ctypes.data for a in acts]), int(k),
+                  _ptrs([o.ctypes.data for o in outs]) if obs else None))
+        return outs
+
+    def step(self, actions, k: int, obs: bool = True):
+        return self._host_step(lib().fa_pool_step, actions, k, obs)
+
+    def step_plain(self, actions, k: int, obs: bool = True):
+        return self._host_step(lib().fa_pool_step_plain, actions, k, obs)
+
+    def step_async(self, d_actions, k: int, d_obs=None, stream: int = 0) -> None:
+        _check(lib().fa_pool_step_async(self._p, _ptrs(d_actions), int(k),
+                                         _ptrs(d_obs) if d_obs else None, _vp(stream or None)))
+
+    def step_plain_async(self, d_actions, k: int, d_obs=None, stream: int = 0) -> None:
+        _check(lib().fa_pool_step_plain_async(self._p, _ptrs(d_actions), int(k),
+                                               _ptrs(d_obs) if d_obs else None, _vp(stream or None)))
+
+    def synchronize(self) -> None:
+        _check(lib().fa_pool_synchronize(self._p))
+
+    def reset_counters(self) -> None:
+        _check(lib().fa_pool_reset_counters(self._p))
+
+    def last_instructions(self) -> int:
+        return int(lib().fa_pool_last_instructions(self._p))
+
+    def last_lane_slots(self) -> int:
+        return int(lib().fa_pool_last_lane_slots(self._p))
+
+    def stream(self) -> int:
+        return int(lib().fa_pool_stream(self._p) or 0)
+
+    def graph(self, d_actions, k: int, calls: int, d_obs=None) -> "PoolGraph":
+        g = _vp()
+        _check(lib().fa_pool_graph_create(self._p, _ptrs(d_actions), int(k), int(calls),
+                                           _ptrs(d_obs) if d_obs else None, ctypes.byref(g)))
+        return PoolGraph(g, self)
+
+
+class PoolGraph:
+    def __init__(self, g, pool: AtariPool):
+        self._g = g
+        self.pool = pool
+
+    def launch(self, stream: int = 0) -> None:
+        _check(lib().fa_graph_launch(self._g, _vp(stream or None)))
+
+    def close(self) -> None:
+        if getattr(self, "_g", None):
+            lib().fa_graph_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        self.close()

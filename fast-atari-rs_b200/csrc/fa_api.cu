@@ -34,13 +34,6 @@ int fa_fail(int code, const char* fmt, ...)
     return code;
 }
 
-#define FA_CUDA(call)                                                                          \
-    do {                                                                                       \
-        cudaError_t e_ = (call);                                                               \
-        if (e_ != cudaSuccess)                                                                 \
-            return fa_fail(FA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));       \
-    } while (0)
-
 extern "C" const char* fa_last_error(void) { return g_err.c_str(); }
 extern "C" const char* fa_version(void) { return "fast-atari-b200 0.1 (sm_100a)"; }
 
@@ -49,6 +42,13 @@ extern "C" int fa_device_count(void)
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
     return n;
+}
+
+extern "C" int fa_set_device(int device)
+{
+    if (device < 0 || device >= fa_device_count()) return fa_fail(FA_ERR_NO_DEVICE, "no CUDA device %d", device);
+    FA_CUDA(cudaSetDevice(device));
+    return FA_OK;
 }
 
 // ------------------------------------------------------------------ packing
@@ -162,34 +162,6 @@ void fa_power_on_column(const uint8_t* img, uint32_t nbanks, int scheme, uint32_
 }
 
 // ------------------------------------------------------------------ handle
-struct fa_handle {
-    int device = 0;
-    int sms = 148;
-    size_t n = 0;
-    uint32_t stride = 0;
-    int scheme = 0;
-    uint32_t nbanks = 1, hot_lo = 0x2000;
-    std::vector<uint8_t> image;        // host copy of the bank image
-    uint8_t* d_rom = nullptr;
-    uint32_t* d_state = nullptr;
-    uint32_t* d_snap = nullptr;        // post-reset column (FA_ROWS words)
-    bool have_snap = false;
-    uint8_t* d_actions = nullptr;
-    size_t actions_cap = 0;
-    uint8_t* d_obs = nullptr;
-    uint32_t* d_err = nullptr;         // [0] error word, [1] work-queue counter
-    unsigned long long* d_instr = nullptr;
-    uint8_t* h_actions = nullptr;      // pinned staging
-    size_t h_actions_cap = 0;
-    uint8_t* h_obs = nullptr;          // pinned, n*128
-    cudaStream_t stream = nullptr;
-    int block = 128;
-    int sched = FA_SCHED_LANE;
-    bool persistent = false;
-    uint32_t episode_frames = 0;
-    unsigned long long last_instr = 0;
-};
-
 static int rom_len_ok(size_t len)          // lengths HeadlessBus::new accepts (src/atari.rs:410-449)
 {
     if (len == 0) return 0;
@@ -264,6 +236,7 @@ extern "C" int fa_create(const uint8_t* rom, size_t rom_len, size_t n, fa_handle
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
     // Default launch shape: the plain per-frame form, 128 threads per CTA.
     h->block = 128;
+    h->sched = FA_SCHED_PC;
     cudaError_t e = cudaSuccess;
 #define TRY(call) do { e = (call); if (e != cudaSuccess) { free_handle(h); \
         return fa_fail(FA_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e)); } } while (0)
@@ -277,7 +250,7 @@ extern "C" int fa_create(const uint8_t* rom, size_t rom_len, size_t n, fa_handle
     TRY(cudaMalloc(&h->d_obs, n * 128));
     TRY(cudaMalloc(&h->d_err, 2 * sizeof(uint32_t)));
     TRY(cudaMemset(h->d_err, 0, 2 * sizeof(uint32_t)));
-    TRY(cudaMalloc(&h->d_instr, sizeof(unsigned long long)));
+    TRY(cudaMalloc(&h->d_instr, 2 * sizeof(unsigned long long)));
     TRY(cudaMallocHost(&h->h_obs, n * 128));
     // Every instance starts zeroed and marked not-reset (stepping it is a no-op).
     {
@@ -314,7 +287,7 @@ static int ensure_actions(fa_handle* h, size_t bytes)
     return FA_OK;
 }
 
-static FaGroup make_group(fa_handle* h, const uint8_t* d_actions, uint32_t k, uint8_t* d_obs)
+FaGroup fa_handle_group(fa_handle* h, const uint8_t* d_actions, uint32_t k, uint8_t* d_obs)
 {
     FaGroup g;
     memset(&g, 0, sizeof(g));
@@ -346,6 +319,7 @@ static int enqueue_run(fa_handle* h, const FaGroup& g, cudaStream_t s)
     L.rom_bytes_max = h->nbanks * 4096u;
     L.err = h->d_err;
     L.instr = h->d_instr;
+    L.rounds = h->d_instr + 1;
     if (h->persistent) {
         L.queue = h->d_err + 1;
         FA_CUDA(cudaMemsetAsync(L.queue, 0, sizeof(uint32_t), s));
@@ -359,7 +333,10 @@ static int finish(fa_handle* h)
     FA_CUDA(cudaStreamSynchronize(h->stream));
     uint32_t err[2] = { 0, 0 };
     FA_CUDA(cudaMemcpy(err, h->d_err, sizeof(err), cudaMemcpyDeviceToHost));
-    FA_CUDA(cudaMemcpy(&h->last_instr, h->d_instr, sizeof(h->last_instr), cudaMemcpyDeviceToHost));
+    unsigned long long ctr[2];
+    FA_CUDA(cudaMemcpy(ctr, h->d_instr, sizeof(ctr), cudaMemcpyDeviceToHost));
+    h->last_instr = ctr[0];
+    h->last_slots = ctr[1];
     if (err[0]) {
         cudaMemset(h->d_err, 0, sizeof(uint32_t));
         return fa_fail(FA_ERR_KERNEL, "device wait gave up (error word 0x%x)", err[0]);
@@ -375,14 +352,14 @@ extern "C" int fa_reset(fa_handle* h, uint8_t* obs_out)
     uint32_t col[FA_ROWS];
     fa_power_on_column(h->image.data(), h->nbanks, h->scheme, col);
     FA_CUDA(cudaMemcpyAsync(h->d_snap, col, sizeof(col), cudaMemcpyHostToDevice, h->stream));
-    FaGroup g = make_group(h, nullptr, 1, nullptr);
+    FaGroup g = fa_handle_group(h, nullptr, 1, nullptr);
     g.state = h->d_snap;
     g.stride = 1;
     g.n = 1;
     g.snapshot = nullptr;
     g.episode_frames = 0;
     g.sched = FA_SCHED_LANE;
-    FA_CUDA(cudaMemsetAsync(h->d_instr, 0, sizeof(unsigned long long), h->stream));
+    FA_CUDA(cudaMemsetAsync(h->d_instr, 0, 2 * sizeof(unsigned long long), h->stream));
     bool persistent = h->persistent;
     h->persistent = false;
     int rc = enqueue_run(h, g, h->stream);
@@ -412,8 +389,8 @@ static int step_host(fa_handle* h, const uint8_t* actions, int k, uint8_t* obs_o
     if (rc) return rc;
     memcpy(h->h_actions, actions, bytes);
     FA_CUDA(cudaMemcpyAsync(h->d_actions, h->h_actions, bytes, cudaMemcpyHostToDevice, h->stream));
-    FA_CUDA(cudaMemsetAsync(h->d_instr, 0, sizeof(unsigned long long), h->stream));
-    rc = enqueue_run(h, make_group(h, h->d_actions, (uint32_t)k, obs_out ? h->d_obs : nullptr), h->stream);
+    FA_CUDA(cudaMemsetAsync(h->d_instr, 0, 2 * sizeof(unsigned long long), h->stream));
+    rc = enqueue_run(h, fa_handle_group(h, h->d_actions, (uint32_t)k, obs_out ? h->d_obs : nullptr), h->stream);
     if (rc) return rc;
     if (obs_out) FA_CUDA(cudaMemcpyAsync(h->h_obs, h->d_obs, h->n * 128, cudaMemcpyDeviceToHost, h->stream));
     rc = finish(h);
@@ -438,7 +415,7 @@ extern "C" int fa_step_multi_async(fa_handle* h, const uint8_t* d_actions, int k
     if (!d_actions || k < 1) return fa_fail(FA_ERR_INVALID, "actions null or k < 1");
     if (((uintptr_t)d_obs & 15u) != 0) return fa_fail(FA_ERR_INVALID, "d_obs must be 16-byte aligned");
     cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
-    return enqueue_run(h, make_group(h, d_actions, (uint32_t)k, d_obs), s);
+    return enqueue_run(h, fa_handle_group(h, d_actions, (uint32_t)k, d_obs), s);
 }
 
 extern "C" int fa_synchronize(fa_handle* h)
@@ -536,6 +513,11 @@ extern "C" int fa_get_launch(const fa_handle* h, int* block, int* sched, int* pe
 extern "C" unsigned long long fa_last_instructions(const fa_handle* h)
 {
     return h ? h->last_instr : 0ull;
+}
+
+extern "C" unsigned long long fa_last_lane_slots(const fa_handle* h)
+{
+    return h ? h->last_slots : 0ull;
 }
 
 extern "C" int fa_get_snapshot(fa_handle* h, fa_state* out)

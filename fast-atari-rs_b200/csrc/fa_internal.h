@@ -3,7 +3,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "fa_layout.h"
+
+#include <string>
 
 // Device error word bits.
 #define FA_DEVERR_TMA_TIMEOUT 0x1u
@@ -33,12 +37,61 @@ struct FaLaunch {
     uint32_t* queue;             // work-queue counter (persistent form) or null
     uint32_t* err;               // device error word
     unsigned long long* instr;   // guest-instruction counter, or null
+    unsigned long long* rounds;  // scheduler rounds x 32 (lane slots offered), or null
 };
 
+// Launch fa_run.  For the persistent form the grid is the SM count times the
+// CTAs per SM the occupancy calculator allows (cached per block and shared-
+// memory size, so that the call is safe inside a stream capture).
 cudaError_t fa_launch_run(const FaLaunch& L, int block, bool persistent, int sms, cudaStream_t s);
+// CTAs of fa_run<block> resident per SM for this ROM size (-1 on error).
 int fa_launch_occupancy(int block, uint32_t rom_bytes_max);
 cudaError_t fa_launch_broadcast(uint32_t* state, uint32_t stride, uint32_t n, const uint32_t* col,
                                 cudaStream_t s);
+
+int fa_fail(int code, const char* fmt, ...);
+
+#define FA_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fa_fail(FA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));       \
+    } while (0)
+
+int fa_make_bank_image(const uint8_t* rom, size_t len, std::vector<uint8_t>& img, int& scheme);
+
+// One ROM and its n instances resident in HBM (the C ABI's fa_handle).
+struct fa_handle {
+    int device = 0;
+    int sms = 148;
+    size_t n = 0;
+    uint32_t stride = 0;
+    int scheme = 0;
+    uint32_t nbanks = 1, hot_lo = 0x2000;
+    std::vector<uint8_t> image;        // host copy of the bank image
+    uint8_t* d_rom = nullptr;
+    uint32_t* d_state = nullptr;
+    uint32_t* d_snap = nullptr;        // post-reset column (FA_ROWS words)
+    bool have_snap = false;
+    uint8_t* d_actions = nullptr;
+    size_t actions_cap = 0;
+    uint8_t* d_obs = nullptr;
+    uint32_t* d_err = nullptr;         // [0] error word, [1] work-queue counter
+    unsigned long long* d_instr = nullptr;
+    uint8_t* h_actions = nullptr;      // pinned staging
+    size_t h_actions_cap = 0;
+    uint8_t* h_obs = nullptr;          // pinned, n*128
+    cudaStream_t stream = nullptr;
+    int block = 128;
+    int sched = FA_SCHED_PC;
+    bool persistent = false;
+    uint32_t episode_frames = 0;
+    unsigned long long last_instr = 0;
+    unsigned long long last_slots = 0;
+};
+
+// Enqueue one launch over every instance of the handle (fa_api.cu).
+FaGroup fa_handle_group(fa_handle* h, const uint8_t* d_actions, uint32_t k, uint8_t* d_obs);
 
 // Host packing between the fa_state AoS layout and one SoA column.
 void fa_pack_column(const fa_state& s, uint32_t* col, size_t stride);

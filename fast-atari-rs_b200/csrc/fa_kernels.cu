@@ -161,11 +161,11 @@ struct Runner {
 // decides which lanes execute in each round; all lanes share one call site of
 // the emulator so its code is instantiated once.
 template <int BLOCK>
-__device__ __forceinline__ void run_lanes(Runner<BLOCK>& r, uint32_t sched)
+__device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
 {
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
-    uint32_t rem = 0, grp = 0;
+    uint32_t rem = 0, grp = 0, rounds = 0;
     while (true) {
         const bool act = r.active;
         const uint32_t pcb = (r.e.bank << 16) | r.e.pc;
@@ -202,13 +202,16 @@ __device__ __forceinline__ void run_lanes(Runner<BLOCK>& r, uint32_t sched)
             if (!__any_sync(FULL, act)) break;
             go = act;
         }
+        rounds++;
         if (go) r.iterate();
     }
+    return rounds;
 }
 
 template <int BLOCK>
 __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint32_t count, const uint8_t* rom_s,
-                         uint32_t* priv, unsigned long long* instr_out)
+                                         uint32_t* priv, unsigned long long* instr_out,
+                                         unsigned long long* rounds_out)
 {
     const uint32_t t = threadIdx.x;
     Runner<BLOCK> r;
@@ -233,7 +236,7 @@ __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint3
         r.e.load_hot(col, G.stride);
         if (G.k > 0) r.active = r.begin_frame();
     }
-    run_lanes<BLOCK>(r, G.sched);
+    const uint32_t rounds = run_lanes<BLOCK>(r, G.sched);
     if (valid) {
         r.e.store_priv(col, G.stride);
         r.e.store_hot(col, G.stride);
@@ -251,6 +254,7 @@ __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint3
         for (int d = 16; d > 0; d >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, d);
         if ((t & 31u) == 0 && n) atomicAdd(instr_out, (unsigned long long)n);
     }
+    if (rounds_out && (t & 31u) == 0 && rounds) atomicAdd(rounds_out, 32ull * rounds);
 }
 
 template <int BLOCK>
@@ -290,7 +294,7 @@ __global__ void __launch_bounds__(BLOCK) fa_run(const __grid_constant__ FaLaunch
         }
         const uint32_t first = (u - G.unit_begin) * BLOCK;
         const uint32_t count = G.n - first < BLOCK ? G.n - first : BLOCK;
-        run_unit<BLOCK>(G, first, count, rom_s, priv, L.instr);
+        run_unit<BLOCK>(G, first, count, rom_s, priv, L.instr, L.rounds);
         __syncthreads();
     }
 }
@@ -305,18 +309,40 @@ __global__ void fa_broadcast(uint32_t* state, uint32_t stride, uint32_t n, const
 }  // namespace fa
 
 // ------------------------------------------------------------------ host launchers
+#include <map>
+#include <mutex>
+
+namespace {
+std::mutex g_cfg_mu;
+std::map<std::pair<int, std::pair<int, size_t>>, int> g_per_sm;   // (device, block, smem) -> CTAs/SM
+
+template <int BLOCK>
+int per_sm_for(size_t smem)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_cfg_mu);
+    auto key = std::make_pair(dev, std::make_pair(BLOCK, smem));
+    auto it = g_per_sm.find(key);
+    if (it != g_per_sm.end()) return it->second;
+    if (cudaFuncSetAttribute(fa::fa_run<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return -1;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<BLOCK>, BLOCK, smem) != cudaSuccess)
+        return -1;
+    g_per_sm[key] = per_sm;
+    return per_sm;
+}
+}  // namespace
+
 template <int BLOCK>
 static cudaError_t launch_block(const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
 {
     const size_t smem = (size_t)L.rom_bytes_max + (size_t)FA_PRIV_WORDS * BLOCK * 4u;
-    cudaError_t e = cudaFuncSetAttribute(fa::fa_run<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    const int per_sm = per_sm_for<BLOCK>(smem);
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint32_t grid = L.nunits;
     if (persistent) {
-        int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<BLOCK>, BLOCK, smem);
-        if (e != cudaSuccess) return e;
-        if (per_sm < 1) return cudaErrorInvalidConfiguration;
         uint32_t cap = (uint32_t)(per_sm * sms);
         grid = L.nunits < cap ? L.nunits : cap;
     }
@@ -338,21 +364,14 @@ cudaError_t fa_launch_run(const FaLaunch& L, int block, bool persistent, int sms
 
 int fa_launch_occupancy(int block, uint32_t rom_bytes_max)
 {
-    const size_t smem = (size_t)rom_bytes_max + (size_t)FA_PRIV_WORDS * block * 4u;
-    int per_sm = 0;
-    cudaError_t e = cudaErrorInvalidValue;
+    const size_t base = (size_t)rom_bytes_max + (size_t)FA_PRIV_WORDS * block * 4u;
     switch (block) {
-    case 64: cudaFuncSetAttribute(fa::fa_run<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<64>, 64, smem); break;
-    case 128: cudaFuncSetAttribute(fa::fa_run<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<128>, 128, smem); break;
-    case 256: cudaFuncSetAttribute(fa::fa_run<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<256>, 256, smem); break;
-    case 512: cudaFuncSetAttribute(fa::fa_run<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<512>, 512, smem); break;
-    default: break;
+    case 64: return per_sm_for<64>(base);
+    case 128: return per_sm_for<128>(base);
+    case 256: return per_sm_for<256>(base);
+    case 512: return per_sm_for<512>(base);
+    default: return -1;
     }
-    return e == cudaSuccess ? per_sm : -1;
 }
 
 cudaError_t fa_launch_broadcast(uint32_t* state, uint32_t stride, uint32_t n, const uint32_t* col, cudaStream_t s)

@@ -128,6 +128,11 @@ const char* fa_version(void);
 /* Number of CUDA devices visible (0 when none); never fails. */
 int fa_device_count(void);
 
+/* Make `device` current on the calling thread for handles and pools created
+ * afterwards (the library links its own CUDA runtime, so another runtime's
+ * current device does not carry over). */
+int fa_set_device(int device);
+
 /*
  * BatchAtariGpu::new (src/cuda_env.rs:112-126).  Uploads the ROM and allocates
  * SoA state for n instances on the current device.  The ROM length must be one
@@ -144,9 +149,11 @@ void fa_destroy(fa_handle* h);
 size_t fa_num_envs(const fa_handle* h);
 
 /*
- * BatchAtariGpu::set_sorted (src/cuda_env.rs:129).  sorted != 0 turns on warp
- * grouping of lanes by program counter (__match_any_sync) before each
- * emulated instruction; 0 runs every lane's own instruction stream.
+ * BatchAtariGpu::set_sorted (src/cuda_env.rs:129).  sorted != 0 groups the
+ * lanes of a warp by program counter with __match_any_sync and runs every
+ * group once per round (FA_SCHED_MATCH); 0 runs every lane's own instruction
+ * stream (FA_SCHED_LANE).  A new handle starts with FA_SCHED_PC, the
+ * convergence policy (see fa_set_launch); results never depend on the policy.
  */
 int fa_set_sorted(fa_handle* h, int sorted);
 
@@ -221,12 +228,65 @@ int fa_get_launch(const fa_handle* h, int* block, int* sched, int* persistent);
 /* Guest (6502) instructions executed by the handle's last synchronous call. */
 unsigned long long fa_last_instructions(const fa_handle* h);
 
+/* Lane slots the warp scheduler offered in that call (scheduler rounds x 32);
+ * instructions / lane slots is the SIMT lane efficiency of the emulation. */
+unsigned long long fa_last_lane_slots(const fa_handle* h);
+
 /* The post-reset snapshot every instance starts from (after fa_reset). */
 int fa_get_snapshot(fa_handle* h, fa_state* out);
 
 /* Device pointer to the SoA state rows (FA layout, for zero-copy readers);
  * *stride_words receives the row stride in 32-bit words. */
 void* fa_device_state(fa_handle* h, uint32_t* stride_words);
+
+/* ------------------------------------------------------------------ pools
+ * The batched form (no reference counterpart: the reference steps one ROM per
+ * BatchAtariGpu).  A pool holds up to 16 carts, each with its own instance
+ * set, and steps all of them in ONE launch whose persistent CTAs pull work
+ * units (up to `block` instances of one cart) from a device queue, heaviest
+ * cart first.  Actions and observations are passed per cart: actions[g] is
+ * k * n_g bytes frame-major, obs[g] is n_g * 128 bytes (or NULL).
+ */
+typedef struct fa_pool fa_pool;
+typedef struct fa_graph fa_graph;
+
+int  fa_pool_create(fa_pool** out);
+void fa_pool_destroy(fa_pool* p);
+/* Add a cart with n instances, reset on the device; *group gets its index. */
+int  fa_pool_add_cart(fa_pool* p, const uint8_t* rom, size_t rom_len, size_t n, int* group);
+int  fa_pool_num_groups(const fa_pool* p);
+/* The handle owning group g's instances (get/set states, status, episode
+ * settings apply to it); owned by the pool. */
+fa_handle* fa_pool_group(fa_pool* p, int group);
+/* Per-cart warp policy and relative cost of one of its units (queue order). */
+int  fa_pool_set_group(fa_pool* p, int group, int sched, float weight);
+int  fa_pool_set_launch(fa_pool* p, int block, int persistent);
+/* Synchronous steps from host buffers: batched (one launch for all carts)
+ * and plain (one launch per frame per cart, the reference's form). */
+int  fa_pool_step(fa_pool* p, const uint8_t* const* actions, int k, uint8_t* const* obs);
+int  fa_pool_step_plain(fa_pool* p, const uint8_t* const* actions, int k, uint8_t* const* obs);
+/* Same from device buffers, enqueued on `stream` (NULL: the pool's stream). */
+int  fa_pool_step_async(fa_pool* p, const uint8_t* const* d_actions, int k, uint8_t* const* d_obs,
+                        void* stream);
+int  fa_pool_step_plain_async(fa_pool* p, const uint8_t* const* d_actions, int k,
+                              uint8_t* const* d_obs, void* stream);
+int  fa_pool_synchronize(fa_pool* p);
+/* Zero the instruction / lane-slot counters (read after a synchronize). */
+int  fa_pool_reset_counters(fa_pool* p);
+unsigned long long fa_pool_last_instructions(const fa_pool* p);
+unsigned long long fa_pool_last_lane_slots(const fa_pool* p);
+/* The pool's own stream (a cudaStream_t). */
+void* fa_pool_stream(fa_pool* p);
+/*
+ * Capture `calls` consecutive batched steps of k frames into a CUDA graph.
+ * d_actions[g] holds calls * k * n_g bytes (call c uses the slice starting at
+ * c * k * n_g); d_obs[g] (or NULL) receives each call's RAM.  The graph
+ * replays against the pool's current state.
+ */
+int  fa_pool_graph_create(fa_pool* p, const uint8_t* const* d_actions, int k, int calls,
+                          uint8_t* const* d_obs, fa_graph** out);
+int  fa_graph_launch(fa_graph* g, void* stream);
+void fa_graph_destroy(fa_graph* g);
 
 #ifdef __cplusplus
 }
