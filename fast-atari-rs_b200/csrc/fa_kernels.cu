@@ -316,6 +316,9 @@ namespace {
 std::mutex g_cfg_mu;
 std::map<std::pair<int, std::pair<int, size_t>>, int> g_per_sm;   // (device, block, smem) -> CTAs/SM
 
+// The dynamic shared-memory limit is raised once per (device, BLOCK) to the
+// largest any cart needs (32 KiB of ROM plus the private bytes), so launches
+// of smaller carts never lower it under a larger one.
 template <int BLOCK>
 int per_sm_for(size_t smem)
 {
@@ -325,8 +328,14 @@ int per_sm_for(size_t smem)
     auto key = std::make_pair(dev, std::make_pair(BLOCK, smem));
     auto it = g_per_sm.find(key);
     if (it != g_per_sm.end()) return it->second;
-    if (cudaFuncSetAttribute(fa::fa_run<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return -1;
+    const auto max_key = std::make_pair(dev, std::make_pair(BLOCK, (size_t)0));
+    if (g_per_sm.find(max_key) == g_per_sm.end()) {
+        const int max_smem = 32768 + FA_PRIV_WORDS * BLOCK * 4;
+        if (cudaFuncSetAttribute(fa::fa_run<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem) !=
+            cudaSuccess)
+            return -1;
+        g_per_sm[max_key] = 0;
+    }
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<BLOCK>, BLOCK, smem) != cudaSuccess)
         return -1;
