@@ -41,6 +41,121 @@ __constant__ uint32_t c_action_table[18] = {
     act_word(0, 1, 0, 1, 1), act_word(0, 1, 1, 0, 1),
 };
 
+// Bit op of word op>>5 is set for the 151 legal opcodes (src/cpu.rs:253-1141).
+__constant__ uint32_t c_legal[8] = {
+    0x63636763u, 0x63637773u, 0x63637763u, 0x63637763u,
+    0x27737572u, 0x77737777u, 0x63637773u, 0x63637773u,
+};
+
+// Packed TIA flag word (Emu::tw).
+enum : uint32_t { TW_WSYNC = 1u << 16, TW_FCOMP = 1u << 17, TW_PDUMP = 1u << 18 };
+
+template <int BLOCK>
+__device__ __forceinline__ uint32_t priv_off(uint32_t o) { return (o & ~3u) * BLOCK + (o & 3u); }
+
+__device__ __forceinline__ uint32_t mod160(int v)
+{
+    int r = v % 160;
+    return (uint32_t)(r < 0 ? r + 160 : r);
+}
+
+// TIA or PIA register read (HeadlessTia::read, src/headless_tia.rs:205-223;
+// Pia::read I/O half, src/pia.rs:169-199).  Bit 8 of the result asks the
+// caller to clear the timer underflow flag (an INTIM read).
+template <int BLOCK>
+__device__ __noinline__ uint32_t io_read(uint32_t a, uint32_t pcnt, uint32_t pins, uint32_t pads,
+                                         uint32_t ports, uint32_t timer, const uint8_t* pv)
+{
+    if (a & 0x80u) {                                                 // PIA: (a & 0x280) == 0x280
+        switch (a & 7u) {
+        case 0: return ((pins & ~(ports >> 8)) | (ports & (ports >> 8))) & 0xFFu;
+        case 1: return (ports >> 8) & 0xFFu;
+        case 2: return (((pins >> 8) & ~(ports >> 24)) | ((ports >> 16) & (ports >> 24))) & 0xFFu;
+        case 3: return ports >> 24;
+        case 4: return (timer & 0xFFu) | 0x100u;
+        case 5: return (timer >> 16) ? 0x80u : 0u;
+        default: return 0u;
+        }
+    }
+    const uint32_t r = a & 0x0Fu;
+    if (r < 8u) return pv[priv_off<BLOCK>(PB_CX + r)];
+    switch (r) {
+    case 0x8: return pcnt >= (pads & 0xFFu) ? 0x80u : 0u;
+    case 0x9: return pcnt >= (pads >> 8) ? 0x80u : 0u;
+    case 0xA: case 0xB: return 0x80u;
+    case 0xC: return (pins >> 16) & 1u ? 0x80u : 0u;
+    case 0xD: return (pins >> 17) & 1u ? 0x80u : 0u;
+    default: return 0u;
+    }
+}
+
+// HeadlessTia::write (src/headless_tia.rs:225-298).  tw is the packed flag
+// word, lw = scanline | paddle_counter<<16; both come back updated.
+template <int BLOCK>
+__device__ __noinline__ uint2 tia_write_io(uint32_t a, uint32_t v, uint32_t clock, uint32_t tw, uint32_t lw,
+                                           uint8_t* pv)
+{
+    auto stp = [&](uint32_t o, uint32_t val) { pv[priv_off<BLOCK>(o)] = (uint8_t)val; };
+    auto ldp = [&](uint32_t o) -> uint32_t { return pv[priv_off<BLOCK>(o)]; };
+    auto stp16 = [&](uint32_t o, uint32_t val) { *(uint16_t*)(pv + priv_off<BLOCK>(o)) = (uint16_t)val; };
+    auto ldp16 = [&](uint32_t o) -> uint32_t { return *(const uint16_t*)(pv + priv_off<BLOCK>(o)); };
+    const uint32_t r = a & 0x3Fu;
+    switch (r) {
+    case 0x00:                                                        // VSYNC rising edge starts a frame
+        if (!(tw & 2u) && (v & 2u)) { lw &= 0xFFFF0000u; tw |= TW_FCOMP; }
+        tw = (tw & ~0xFFu) | v;
+        break;
+    case 0x01:                                                        // VBLANK bit 7 dumps the paddles
+        if (v & 0x80u) { lw &= 0xFFFFu; tw |= TW_PDUMP; } else tw &= ~TW_PDUMP;
+        tw = (tw & ~0xFF00u) | (v << 8);
+        break;
+    case 0x02: tw |= TW_WSYNC; break;
+    case 0x04: stp(PB_NUSIZ0, v); break;
+    case 0x05: stp(PB_NUSIZ1, v); break;
+    case 0x06: case 0x07: case 0x08: case 0x09: stp(PB_COLUP0 + (r - 0x06u), v); break;
+    case 0x0A: stp(PB_CTRLPF, v); break;
+    case 0x0B: stp(PB_REFP0, (v >> 3) & 1u); break;
+    case 0x0C: stp(PB_REFP1, (v >> 3) & 1u); break;
+    case 0x0D: case 0x0E: case 0x0F: stp(PB_PF0 + (r - 0x0Du), v); break;
+    case 0x10: case 0x11: case 0x12: case 0x13: case 0x14:
+        // RESPx: (clock as i16 - 68 + 5).rem_euclid(160)
+        stp16(PB_POS + 2u * (r - 0x10u), mod160((int16_t)(uint16_t)(clock - 63u)));
+        break;
+    case 0x1B: stp(PB_GRP0_OLD, ldp(PB_GRP0)); stp(PB_GRP0, v); break;
+    case 0x1C:
+        stp(PB_GRP1_OLD, ldp(PB_GRP1)); stp(PB_GRP1, v);
+        stp(PB_ENABL_OLD, ldp(PB_ENABL)); break;
+    case 0x1D: case 0x1E: case 0x1F: stp(PB_ENAM0 + (r - 0x1Du), (v >> 1) & 1u); break;
+    case 0x20: case 0x21: case 0x22: case 0x23: case 0x24: stp(PB_HM + (r - 0x20u), v); break;
+    case 0x25: case 0x26: case 0x27: stp(PB_VDELP0 + (r - 0x25u), v & 1u); break;
+    case 0x28: case 0x29: stp(PB_RESMP0 + (r - 0x28u), (v >> 1) & 1u); break;
+    case 0x2A:                                                        // HMOVE
+        for (uint32_t k = 0; k < 5u; k++) {
+            int off = ((int)(int8_t)(uint8_t)ldp(PB_HM + k)) >> 4;
+            int16_t d = (int16_t)(uint16_t)(ldp16(PB_POS + 2u * k) - (uint32_t)off);
+            stp16(PB_POS + 2u * k, mod160(d));
+        }
+        break;
+    case 0x2B: for (uint32_t k = 0; k < 5u; k++) stp(PB_HM + k, 0); break;
+    case 0x2C: for (uint32_t k = 0; k < 8u; k++) stp(PB_CX + k, 0); break;
+    default: break;
+    }
+    return make_uint2(tw, lw);
+}
+
+// Pia::write, I/O half (src/pia.rs:202-228).  Returns (ports, timer value,
+// prescaler, select | underflow<<16).
+__device__ __noinline__ uint4 pia_write_io(uint32_t a, uint32_t v, uint32_t ports, uint32_t tv, uint32_t ps,
+                                           uint32_t sel_uf)
+{
+    if (a & 0x10u) {
+        const uint32_t sel = 1u << ((0xA630u >> (4u * (a & 3u))) & 0xFu);   // 1, 8, 64, 1024
+        return make_uint4(ports, v, sel, sel);
+    }
+    const uint32_t sh = 8u * (a & 3u);                                 // pa_out pa_ddr pb_out pb_ddr
+    return make_uint4((ports & ~(0xFFu << sh)) | (v << sh), tv, ps, sel_uf);
+}
+
 template <int BLOCK>
 struct Emu {
     // ---- placement
@@ -50,17 +165,23 @@ struct Emu {
     // ---- CPU (src/cpu.rs:96-105)
     uint32_t a, x, y, sp, p, pc, bank;
     uint32_t cyc_lo, cyc_hi;
-    // ---- PIA (src/pia.rs:26-44)
-    uint32_t pa_out, pa_ddr, pa_in, pb_out, pb_ddr, pb_in;
+    // ---- PIA (src/pia.rs:26-44): timer unpacked (ticked every instruction),
+    //      ports and input pins packed (touched only by I/O accesses)
     uint32_t tv, ps, sel, uf;
-    // ---- TIA hot fields (src/headless_tia.rs:16-45)
-    uint32_t clock, scanline, wsync, fcomp, vsync, vblank;
-    uint32_t pcnt, pdump, inpt4, inpt5, pad0, pad1;
+    uint32_t ports;          // pa_out | pa_ddr<<8 | pb_out<<16 | pb_ddr<<24
+    uint32_t pins;           // pa_in | pb_in<<8 | inpt4<<16 | inpt5<<17
+    uint32_t pads;           // paddle0 | paddle1<<8
+    // ---- TIA (src/headless_tia.rs:16-45): beam position unpacked, flags packed
+    uint32_t clock, scanline, pcnt;
+    uint32_t tw;             // vsync | vblank<<8 | wsync<<16 | frame_complete<<17 | paddle_dumped<<18
     // ---- run bookkeeping
     uint32_t frame_no, status, instr;
 
+    __device__ __forceinline__ bool vsync_on() const { return (tw & 2u) != 0; }
+    __device__ __forceinline__ bool wsync() const { return (tw & TW_WSYNC) != 0; }
+
     // ------------------------------------------------------------ private bytes
-    __device__ __forceinline__ uint32_t poff(uint32_t o) const { return (o & ~3u) * BLOCK + (o & 3u); }
+    __device__ __forceinline__ uint32_t poff(uint32_t o) const { return priv_off<BLOCK>(o); }
     __device__ __forceinline__ uint32_t ldp(uint32_t o) const { return pv[poff(o)]; }
     __device__ __forceinline__ void stp(uint32_t o, uint32_t v) { pv[poff(o)] = (uint8_t)v; }
     __device__ __forceinline__ uint32_t ldp16(uint32_t o) const { return *(const uint16_t*)(pv + poff(o)); }
@@ -82,9 +203,9 @@ struct Emu {
     {
         clock = (clock - 228u) & 0xFFFFu;
         scanline = (scanline + 1u) & 0xFFFFu;
-        wsync = 0;
-        if (!pdump && pcnt < 256u) pcnt++;
-        if (scanline >= 262u) { scanline = 0; fcomp = 1; }
+        tw &= ~TW_WSYNC;
+        if (!(tw & TW_PDUMP) && pcnt < 256u) pcnt++;
+        if (scanline >= 262u) { scanline = 0; tw |= TW_FCOMP; }
     }
     __device__ __forceinline__ void tia_tick(uint32_t n)            // :153-158
     {
@@ -98,69 +219,9 @@ struct Emu {
         if (c) { clock = 228u; end_scanline(); }
         return c;
     }
-    __device__ uint32_t tia_read(uint32_t a) const                   // :205-223
-    {
-        uint32_t r = a & 0x0Fu;
-        if (r < 8u) return ldp(PB_CX + r);
-        switch (r) {
-        case 0x8: return pcnt >= pad0 ? 0x80u : 0u;
-        case 0x9: return pcnt >= pad1 ? 0x80u : 0u;
-        case 0xA: case 0xB: return 0x80u;
-        case 0xC: return inpt4 ? 0x80u : 0u;
-        case 0xD: return inpt5 ? 0x80u : 0u;
-        default: return 0u;
-        }
-    }
-    __device__ static __forceinline__ uint32_t mod160(int v)
-    {
-        int r = v % 160;
-        return (uint32_t)(r < 0 ? r + 160 : r);
-    }
-    __device__ void tia_write(uint32_t a, uint32_t v)                // :225-298
-    {
-        uint32_t r = a & 0x3Fu;
-        switch (r) {
-        case 0x00:
-            if (!(vsync & 2u) && (v & 2u)) { scanline = 0; fcomp = 1; }
-            vsync = v; break;
-        case 0x01:
-            if (v & 0x80u) { pcnt = 0; pdump = 1; } else if (pdump) pdump = 0;
-            vblank = v; break;
-        case 0x02: wsync = 1; break;
-        case 0x04: stp(PB_NUSIZ0, v); break;
-        case 0x05: stp(PB_NUSIZ1, v); break;
-        case 0x06: case 0x07: case 0x08: case 0x09: stp(PB_COLUP0 + (r - 0x06u), v); break;
-        case 0x0A: stp(PB_CTRLPF, v); break;
-        case 0x0B: stp(PB_REFP0, (v >> 3) & 1u); break;
-        case 0x0C: stp(PB_REFP1, (v >> 3) & 1u); break;
-        case 0x0D: case 0x0E: case 0x0F: stp(PB_PF0 + (r - 0x0Du), v); break;
-        case 0x10: case 0x11: case 0x12: case 0x13: case 0x14:
-            // RESPx: (clock as i16 - 68 + 5).rem_euclid(160)
-            stp16(PB_POS + 2u * (r - 0x10u), mod160((int16_t)(uint16_t)(clock - 63u)));
-            break;
-        case 0x1B: stp(PB_GRP0_OLD, ldp(PB_GRP0)); stp(PB_GRP0, v); break;
-        case 0x1C:
-            stp(PB_GRP1_OLD, ldp(PB_GRP1)); stp(PB_GRP1, v);
-            stp(PB_ENABL_OLD, ldp(PB_ENABL)); break;
-        case 0x1D: case 0x1E: case 0x1F: stp(PB_ENAM0 + (r - 0x1Du), (v >> 1) & 1u); break;
-        case 0x20: case 0x21: case 0x22: case 0x23: case 0x24: stp(PB_HM + (r - 0x20u), v); break;
-        case 0x25: case 0x26: case 0x27: stp(PB_VDELP0 + (r - 0x25u), v & 1u); break;
-        case 0x28: case 0x29: stp(PB_RESMP0 + (r - 0x28u), (v >> 1) & 1u); break;
-        case 0x2A:                                                      // HMOVE
-            for (uint32_t k = 0; k < 5u; k++) {
-                int off = ((int)(int8_t)(uint8_t)ldp(PB_HM + k)) >> 4;
-                int16_t d = (int16_t)(uint16_t)(ldp16(PB_POS + 2u * k) - (uint32_t)off);
-                stp16(PB_POS + 2u * k, mod160(d));
-            }
-            break;
-        case 0x2B: for (uint32_t k = 0; k < 5u; k++) stp(PB_HM + k, 0); break;
-        case 0x2C: for (uint32_t k = 0; k < 8u; k++) stp(PB_CX + k, 0); break;
-        default: break;
-        }
-    }
 
-    // ------------------------------------------------------------ PIA (pia.rs)
-    __device__ __forceinline__ void pia_tick(uint32_t n)             // :107-166
+    // ------------------------------------------------------------ PIA timer (pia.rs:107-166)
+    __device__ __forceinline__ void pia_tick(uint32_t n)
     {
         if (n == 0) return;
         if (tv == 0 && uf) { tv = (0xFFu - (n - 1u)) & 0xFFu; return; }
@@ -195,43 +256,33 @@ struct Emu {
             ps = sel - left;
         }
     }
-    __device__ __forceinline__ uint32_t pia_read(uint32_t a)         // :169-199 (I/O half)
-    {
-        switch (a & 7u) {
-        case 0: return (pa_in & ~pa_ddr & 0xFFu) | (pa_out & pa_ddr);
-        case 1: return pa_ddr;
-        case 2: return (pb_in & ~pb_ddr & 0xFFu) | (pb_out & pb_ddr);
-        case 3: return pb_ddr;
-        case 4: uf = 0; return tv & 0xFFu;
-        case 5: return uf ? 0x80u : 0u;
-        default: return 0u;
-        }
-    }
-    __device__ __forceinline__ void pia_write(uint32_t a, uint32_t v) // :202-228 (I/O half)
-    {
-        if (a & 0x10u) {
-            tv = v; uf = 0;
-            sel = 1u << ((0xA630u >> (4u * (a & 3u))) & 0xFu);      // 1, 8, 64, 1024
-            ps = sel;
-            return;
-        }
-        switch (a & 3u) {
-        case 0: pa_out = v; break;
-        case 1: pa_ddr = v; break;
-        case 2: pb_out = v; break;
-        default: pb_ddr = v; break;
-        }
-    }
 
     // ------------------------------------------------------------ bus (atari.rs:497-552)
+    // ROM, RAM and hotspots are handled inline; TIA and PIA registers go
+    // through one out-of-line copy of their decoders (io_read / tia_write_io /
+    // pia_write_io), which keeps the interpreter's code small enough to stay
+    // resident in the instruction cache.
+    __device__ __forceinline__ uint32_t io(uint32_t a)               // TIA or PIA register read
+    {
+        uint32_t r = io_read<BLOCK>(a, pcnt, pins, pads, ports, tv | (uf << 16), pv);
+        if (r & 0x100u) uf = 0;                                     // INTIM read clears the flag
+        return r & 0xFFu;
+    }
+    __device__ __forceinline__ void io_write(uint32_t a, uint32_t v)  // TIA or PIA register write
+    {
+        if (a & 0x200u) {
+            uint4 r = pia_write_io(a, v, ports, tv, ps, sel | (uf << 16));
+            ports = r.x; tv = r.y; ps = r.z; sel = r.w & 0xFFFFu; uf = r.w >> 16;
+        } else {
+            uint2 r = tia_write_io<BLOCK>(a, v, clock, tw, scanline | (pcnt << 16), pv);
+            tw = r.x; scanline = r.y & 0xFFFFu; pcnt = r.y >> 16;
+        }
+    }
     __device__ __forceinline__ uint32_t read_low(uint32_t a)         // a < 0x1000
     {
-        if (a & 0x80u) {
-            if ((a & 0x280u) == 0x280u) return pia_read(a);
-            if (a < 0x200u) return ldp(a & 0x7Fu);
-            return 0u;            // other RAM mirrors read the never-written flat array
-        }
-        return tia_read(a);
+        if ((a & 0x80u) && (a & 0x280u) != 0x280u)                  // RAM and its mirrors
+            return a < 0x200u ? ldp(a & 0x7Fu) : 0u;                // other mirrors read the never-written flat array
+        return io(a);
     }
     __device__ __forceinline__ uint32_t read(uint32_t addr)
     {
@@ -244,8 +295,7 @@ struct Emu {
         uint32_t a = addr & 0x1FFFu;
         if (a & 0x1000u) { bsw(a); return; }
         if ((a & 0x280u) == 0x080u) { stp(a & 0x7Fu, v); return; }
-        if (a & 0x200u) { pia_write(a, v); return; }
-        tia_write(a, v);
+        io_write(a, v);
     }
     // A phantom read: only its side effects (hotspot, INTIM) matter.
     __device__ __forceinline__ void dummy(uint32_t addr)
@@ -254,17 +304,17 @@ struct Emu {
         if (a & 0x1000u) bsw(a);
         else if ((a & 0x287u) == 0x284u) uf = 0;
     }
-    __device__ __forceinline__ uint32_t zp_read(uint32_t z) { return (z & 0x80u) ? ldp(z & 0x7Fu) : tia_read(z); }
+    __device__ __forceinline__ uint32_t zp_read(uint32_t z) { return (z & 0x80u) ? ldp(z & 0x7Fu) : io(z); }
     __device__ __forceinline__ uint32_t fetch() { uint32_t v = read(pc); pc = (pc + 1u) & 0xFFFFu; return v; }
     __device__ __forceinline__ void push(uint32_t v)
     {
-        if (sp & 0x80u) stp(sp & 0x7Fu, v); else tia_write(0x100u | sp, v);
+        if (sp & 0x80u) stp(sp & 0x7Fu, v); else io_write(0x100u | sp, v);
         sp = (sp - 1u) & 0xFFu;
     }
     __device__ __forceinline__ uint32_t pull()
     {
         sp = (sp + 1u) & 0xFFu;
-        return (sp & 0x80u) ? ldp(sp & 0x7Fu) : tia_read(0x100u | sp);
+        return (sp & 0x80u) ? ldp(sp & 0x7Fu) : io(0x100u | sp);
     }
     // Read-modify-write's two writes; a RAM target only needs the second.
     __device__ __forceinline__ void rmw_store(uint32_t ea, uint32_t oldv, uint32_t newv)
@@ -349,42 +399,46 @@ struct Emu {
     }
 
     // ------------------------------------------------------------ instruction groups
+    // The opcode (at pc0) and the byte after it (b1: the operand, or the
+    // phantom read every 1-byte instruction makes at pc0+1) are read by
+    // step() for every legal opcode, in that order, as the reference does on
+    // cycles 1 and 2.  b2 is the byte at pc0+2 for the 3-byte forms, read on
+    // cycle 3 (JSR reads its high byte later and fetches it itself).
+
     // cc = 01: ORA AND EOR ADC STA LDA CMP SBC x 8 addressing modes.
-    __device__ __forceinline__ uint32_t group1(uint32_t aaa, uint32_t bbb)
+    __device__ __forceinline__ uint32_t group1(uint32_t pc0, uint32_t aaa, uint32_t bbb, uint32_t b1, uint32_t b2)
     {
         const bool st = aaa == 4u;
         uint32_t ea, cyc, v;
         switch (bbb) {
         case 0: {                                                   // (zp,X)
-            uint32_t z = (fetch() + x) & 0xFFu;
-            uint32_t lo = zp_read(z);
-            uint32_t hi = zp_read((z + 1u) & 0xFFu);
-            ea = (hi << 8) | lo; cyc = 6; break;
+            const uint32_t z = (b1 + x) & 0xFFu;
+            const uint32_t lo = zp_read(z);
+            ea = (zp_read((z + 1u) & 0xFFu) << 8) | lo;
+            cyc = 6;
+            break;
         }
-        case 1: ea = fetch(); cyc = 3; break;                       // zp
-        case 2:                                                     // #imm
-            if (st) return 0;                                       // $89 is illegal
-            v = fetch();
-            cyc = 2;
-            goto operate;
-        case 3: { uint32_t lo = fetch(); ea = (fetch() << 8) | lo; cyc = 4; break; }
+        case 1: ea = b1; cyc = 3; break;                            // zp
+        case 2: v = b1; cyc = 2; pc = (pc0 + 2u) & 0xFFFFu; goto operate;   // #imm ($89 is illegal)
+        case 3: ea = (b2 << 8) | b1; cyc = 4; break;                // abs
         case 4: {                                                   // (zp),Y
-            uint32_t z = fetch();
-            uint32_t lo = zp_read(z);
-            uint32_t base = (zp_read((z + 1u) & 0xFFu) << 8) | lo;
-            ea = (base + y) & 0xFFFFu; cyc = 5;
+            const uint32_t lo = zp_read(b1);
+            const uint32_t base = (zp_read((b1 + 1u) & 0xFFu) << 8) | lo;
+            ea = (base + y) & 0xFFFFu;
+            cyc = 5;
             if (st || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 6; }
             break;
         }
-        case 5: ea = (fetch() + x) & 0xFFu; cyc = 4; break;        // zp,X
+        case 5: ea = (b1 + x) & 0xFFu; cyc = 4; break;             // zp,X
         default: {                                                  // abs,Y / abs,X
-            uint32_t lo = fetch();
-            uint32_t base = (fetch() << 8) | lo;
-            ea = (base + (bbb == 6u ? y : x)) & 0xFFFFu; cyc = 4;
+            const uint32_t base = (b2 << 8) | b1;
+            ea = (base + (bbb == 6u ? y : x)) & 0xFFFFu;
+            cyc = 4;
             if (st || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 5; }
             break;
         }
         }
+        pc = (pc0 + ((bbb == 3u || bbb >= 6u) ? 3u : 2u)) & 0xFFFFu;
         if (st) { write(ea, a); return cyc; }
         v = read(ea);
     operate:
@@ -401,15 +455,14 @@ struct Emu {
     }
 
     // cc = 10: ASL ROL LSR ROR STX LDX DEC INC, plus TXA TAX DEX NOP TXS TSX.
-    __device__ __forceinline__ uint32_t group2(uint32_t aaa, uint32_t bbb)
+    __device__ __forceinline__ uint32_t group2(uint32_t pc0, uint32_t aaa, uint32_t bbb, uint32_t b1, uint32_t b2)
     {
         uint32_t ea, cyc;
         switch (bbb) {
-        case 0:                                                     // LDX #imm only
-            if (aaa != 5u) return 0;
-            x = fetch(); nz(x); return 2;
+        case 0:                                                     // LDX #imm
+            x = b1; nz(x); pc = (pc0 + 2u) & 0xFFFFu; return 2;
         case 2:                                                     // accumulator / implied
-            dummy(pc);
+            pc = (pc0 + 1u) & 0xFFFFu;
             switch (aaa) {
             case 4: a = x; nz(a); break;                            // TXA
             case 5: x = a; nz(x); break;                            // TAX
@@ -418,19 +471,17 @@ struct Emu {
             default: a = shift_op(aaa, a); break;
             }
             return 2;
-        case 6:
-            if (aaa == 4u) { dummy(pc); sp = x; return 2; }          // TXS
-            if (aaa == 5u) { dummy(pc); x = sp; nz(x); return 2; }   // TSX
-            return 0;
-        case 4: return 0;
-        case 1: ea = fetch(); cyc = 3; break;                       // zp
-        case 3: { uint32_t lo = fetch(); ea = (fetch() << 8) | lo; cyc = 4; break; }
+        case 6:                                                     // TXS / TSX
+            pc = (pc0 + 1u) & 0xFFFFu;
+            if (aaa == 4u) sp = x; else { x = sp; nz(x); }
+            return 2;
+        case 1: ea = b1; cyc = 3; pc = (pc0 + 2u) & 0xFFFFu; break; // zp
+        case 3: ea = (b2 << 8) | b1; cyc = 4; pc = (pc0 + 3u) & 0xFFFFu; break;
         case 5:                                                     // zp,X (zp,Y for STX/LDX)
-            ea = (fetch() + ((aaa == 4u || aaa == 5u) ? y : x)) & 0xFFu; cyc = 4; break;
+            ea = (b1 + ((aaa == 4u || aaa == 5u) ? y : x)) & 0xFFu; cyc = 4; pc = (pc0 + 2u) & 0xFFFFu; break;
         default: {                                                  // abs,X (abs,Y for LDX)
-            if (aaa == 4u) return 0;                                // $9E is illegal
-            uint32_t lo = fetch();
-            uint32_t base = (fetch() << 8) | lo;
+            pc = (pc0 + 3u) & 0xFFFFu;
+            const uint32_t base = (b2 << 8) | b1;
             if (aaa == 5u) {
                 ea = (base + y) & 0xFFFFu; cyc = 4;
                 if ((base ^ ea) & 0xFF00u) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 5; }
@@ -438,35 +489,35 @@ struct Emu {
             }
             ea = (base + x) & 0xFFFFu;
             dummy((base & 0xFF00u) | (ea & 0xFFu));
-            uint32_t v = read(ea);
+            const uint32_t v = read(ea);
             rmw_store(ea, v, shift_op(aaa, v));
             return 7;
         }
         }
         if (aaa == 4u) { write(ea, x); return cyc; }
         if (aaa == 5u) { x = read(ea); nz(x); return cyc; }
-        uint32_t v = read(ea);
+        const uint32_t v = read(ea);
         rmw_store(ea, v, shift_op(aaa, v));
         return cyc + 2u;
     }
 
     // cc = 00: control flow, stack, flags, BIT/STY/LDY/CPY/CPX.
-    __device__ __forceinline__ uint32_t group0(uint32_t aaa, uint32_t bbb)
+    __device__ __forceinline__ uint32_t group0(uint32_t pc0, uint32_t aaa, uint32_t bbb, uint32_t b1, uint32_t b2)
     {
         switch (bbb) {
         case 4: {                                                   // branches
-            uint32_t off = fetch();
-            uint32_t pos = (0x1067u >> (4u * (aaa >> 1))) & 0xFu;    // N V C Z
+            pc = (pc0 + 2u) & 0xFFFFu;
+            const uint32_t pos = (0x1067u >> (4u * (aaa >> 1))) & 0xFu;    // N V C Z
             if (((p >> pos) & 1u) != (aaa & 1u)) return 2;
             dummy(pc);
-            uint32_t npc = (pc + (uint32_t)(int32_t)(int8_t)(uint8_t)off) & 0xFFFFu;
+            const uint32_t npc = (pc + (uint32_t)(int32_t)(int8_t)(uint8_t)b1) & 0xFFFFu;
             uint32_t cyc = 3;
             if ((pc ^ npc) & 0xFF00u) { dummy((pc & 0xFF00u) | (npc & 0xFFu)); cyc = 4; }
             pc = npc;
             return cyc;
         }
         case 6:                                                     // flags, TYA
-            dummy(pc);
+            pc = (pc0 + 1u) & 0xFFFFu;
             switch (aaa) {
             case 0: p &= ~F_C; break;
             case 1: p |= F_C; break;
@@ -479,7 +530,7 @@ struct Emu {
             }
             return 2;
         case 2:                                                     // stack, DEY TAY INY INX
-            dummy(pc);
+            pc = (pc0 + 1u) & 0xFFFFu;
             switch (aaa) {
             case 0: push(p | F_B | F_U); return 3;                  // PHP
             case 1: p = pull() & ~(F_B | F_U); return 4;            // PLP
@@ -492,66 +543,60 @@ struct Emu {
             }
         case 0:
             switch (aaa) {
-            case 0: {                                               // BRK
-                dummy(pc); pc = (pc + 1u) & 0xFFFFu;
+            case 0: {                                               // BRK (b1 is the padding byte)
+                pc = (pc0 + 2u) & 0xFFFFu;
                 push(pc >> 8); push(pc & 0xFFu); push(p | F_B | F_U);
                 p |= F_I;
-                uint32_t lo = read(0xFFFEu);
+                const uint32_t lo = read(0xFFFEu);
                 pc = (read(0xFFFFu) << 8) | lo;
                 return 7;
             }
-            case 1: {                                               // JSR
-                uint32_t lo = fetch();
+            case 1: {                                               // JSR: pushes before the high byte
+                pc = (pc0 + 2u) & 0xFFFFu;
                 push(pc >> 8); push(pc & 0xFFu);
-                pc = (read(pc) << 8) | lo;
+                pc = (read(pc) << 8) | b1;
                 return 6;
             }
             case 2: {                                               // RTI
-                dummy(pc);
                 p = pull() & ~(F_B | F_U);
-                uint32_t lo = pull();
+                const uint32_t lo = pull();
                 pc = (pull() << 8) | lo;
                 return 6;
             }
             case 3: {                                               // RTS
-                dummy(pc);
-                uint32_t lo = pull();
-                uint32_t ra = (pull() << 8) | lo;
+                const uint32_t lo = pull();
+                const uint32_t ra = (pull() << 8) | lo;
                 dummy(ra);
                 pc = (ra + 1u) & 0xFFFFu;
                 return 6;
             }
-            case 4: return 0;
-            case 5: y = fetch(); nz(y); return 2;                   // LDY #
-            case 6: cmp(y, fetch()); return 2;                      // CPY #
-            default: cmp(x, fetch()); return 2;                     // CPX #
+            case 5: y = b1; nz(y); break;                           // LDY #
+            case 6: cmp(y, b1); break;                              // CPY #
+            default: cmp(x, b1); break;                             // CPX #
             }
+            pc = (pc0 + 2u) & 0xFFFFu;
+            return 2;
         case 3:                                                     // absolute
-            if (aaa == 0u) return 0;
-            if (aaa == 2u) { uint32_t lo = fetch(); pc = (read(pc) << 8) | lo; return 3; }  // JMP
+            pc = (pc0 + 3u) & 0xFFFFu;
+            if (aaa == 2u) { pc = (b2 << 8) | b1; return 3; }       // JMP
             if (aaa == 3u) {                                        // JMP (ind), page-wrap bug
-                uint32_t lo = fetch();
-                uint32_t ptr = (fetch() << 8) | lo;
-                uint32_t tlo = read(ptr);
+                const uint32_t ptr = (b2 << 8) | b1;
+                const uint32_t tlo = read(ptr);
                 pc = (read((ptr & 0xFF00u) | ((ptr + 1u) & 0xFFu)) << 8) | tlo;
                 return 5;
             }
-            {
-                uint32_t lo = fetch();
-                uint32_t ea = (fetch() << 8) | lo;
-                return mem0(aaa, ea, 4);
-            }
-        case 1:                                                     // zp
-            if (aaa == 0u || aaa == 2u || aaa == 3u) return 0;
-            return mem0(aaa, fetch(), 3);
+            return mem0(aaa, (b2 << 8) | b1, 4);
+        case 1:                                                     // zp: BIT STY LDY CPY CPX
+            pc = (pc0 + 2u) & 0xFFFFu;
+            return mem0(aaa, b1, 3);
         case 5:                                                     // zp,X: STY LDY
-            if (aaa != 4u && aaa != 5u) return 0;
-            return mem0(aaa, (fetch() + x) & 0xFFu, 4);
+            pc = (pc0 + 2u) & 0xFFFFu;
+            return mem0(aaa, (b1 + x) & 0xFFu, 4);
         default: {                                                  // abs,X: LDY
-            if (aaa != 5u) return 0;
-            uint32_t lo = fetch();
-            uint32_t base = (fetch() << 8) | lo;
-            uint32_t ea = (base + x) & 0xFFFFu, cyc = 4;
+            pc = (pc0 + 3u) & 0xFFFFu;
+            const uint32_t base = (b2 << 8) | b1;
+            const uint32_t ea = (base + x) & 0xFFFFu;
+            uint32_t cyc = 4;
             if ((base ^ ea) & 0xFF00u) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 5; }
             y = read(ea); nz(y);
             return cyc;
@@ -561,7 +606,7 @@ struct Emu {
     __device__ __forceinline__ uint32_t mem0(uint32_t aaa, uint32_t ea, uint32_t cyc)
     {
         if (aaa == 4u) { write(ea, y); return cyc; }                // STY
-        uint32_t v = read(ea);
+        const uint32_t v = read(ea);
         switch (aaa) {
         case 1: bit(v); break;
         case 5: y = v; nz(y); break;
@@ -571,27 +616,29 @@ struct Emu {
         return cyc;
     }
 
-    // One instruction; returns its cycle count, 0 for an illegal opcode
-    // (pc is then past the opcode and nothing else changed).
+    // One instruction; returns its cycle count, or 0 for an illegal opcode
+    // (pc is then past the opcode and nothing else changed: the reference
+    // panics right after the opcode fetch, src/cpu.rs:1139-1141).
     __device__ __forceinline__ uint32_t step()
     {
-        uint32_t op = fetch();
-        uint32_t aaa = op >> 5, bbb = (op >> 2) & 7u;
-        switch (op & 3u) {
-        case 1: return group1(aaa, bbb);
-        case 2: return group2(aaa, bbb);
-        case 0: return group0(aaa, bbb);
-        default: return 0;
-        }
+        const uint32_t pc0 = pc;
+        const uint32_t op = read(pc0);
+        if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }
+        const uint32_t aaa = op >> 5, bbb = (op >> 2) & 7u, cc = op & 3u;
+        const uint32_t b1 = read((pc0 + 1u) & 0xFFFFu);
+        uint32_t b2 = 0;
+        if (bbb == 3u || bbb == 7u || (bbb == 6u && cc == 1u)) b2 = read((pc0 + 2u) & 0xFFFFu);
+        if (cc == 1u) return group1(pc0, aaa, bbb, b1, b2);
+        if (cc == 2u) return group2(pc0, aaa, bbb, b1, b2);
+        return group0(pc0, aaa, bbb, b1, b2);
     }
 
     // HeadlessAtari::set_action (src/atari.rs:571-582).
     __device__ __forceinline__ void apply_action(uint32_t act)
     {
         uint32_t t = c_action_table[act < 18u ? act : 0u];
-        pa_in = t & 0xFFu;
-        inpt4 = (t >> 8) & 1u;
-        pad0 = (t >> 16) & 0xFFu;
+        pins = (pins & ~0x100FFu) | (t & 0xFFu) | (((t >> 8) & 1u) << 16);
+        pads = (pads & ~0xFFu) | ((t >> 16) & 0xFFu);
     }
 
     // ------------------------------------------------------------ state movement
@@ -602,13 +649,18 @@ struct Emu {
         w = col[R_PC * stride];    pc = w & 0xFFFF; p = (w >> 16) & 0xFF; bank = w >> 24;
         cyc_lo = col[R_CYC_LO * stride];
         cyc_hi = col[R_CYC_HI * stride];
-        w = col[R_PIA0 * stride];  pa_out = w & 0xFF; pa_ddr = (w >> 8) & 0xFF; pa_in = (w >> 16) & 0xFF; pb_out = w >> 24;
-        w = col[R_PIA1 * stride];  pb_ddr = w & 0xFF; pb_in = (w >> 8) & 0xFF; uf = (w >> 16) & 0xFF; pdump = w >> 24;
+        const uint32_t p0 = col[R_PIA0 * stride];                  // pa_out pa_ddr pa_in pb_out
+        const uint32_t p1 = col[R_PIA1 * stride];                  // pb_ddr pb_in uf pdump
+        ports = (p0 & 0xFFFFu) | ((p0 >> 24) << 16) | ((p1 & 0xFFu) << 24);
+        uf = (p1 >> 16) & 0xFF;
         w = col[R_TIMER * stride]; tv = w & 0xFFFF; ps = w >> 16;
         w = col[R_SELPC * stride]; sel = w & 0xFFFF; pcnt = w >> 16;
         w = col[R_TIA0 * stride];  clock = w & 0xFFFF; scanline = w >> 16;
-        w = col[R_TIA1 * stride];  wsync = w & 0xFF; fcomp = (w >> 8) & 0xFF; vsync = (w >> 16) & 0xFF; vblank = w >> 24;
-        w = col[R_TIA2 * stride];  inpt4 = w & 0xFF; inpt5 = (w >> 8) & 0xFF; pad0 = (w >> 16) & 0xFF; pad1 = w >> 24;
+        w = col[R_TIA1 * stride];                                   // wsync fcomp vsync vblank
+        tw = ((w >> 16) & 0xFFFFu) | ((w & 1u) << 16) | (((w >> 8) & 1u) << 17) | (((p1 >> 24) & 1u) << 18);
+        w = col[R_TIA2 * stride];                                   // inpt4 inpt5 pad0 pad1
+        pins = ((p0 >> 16) & 0xFFu) | (((p1 >> 8) & 0xFFu) << 8) | ((w & 1u) << 16) | (((w >> 8) & 1u) << 17);
+        pads = w >> 16;
         frame_no = col[R_FRAME * stride];
         status = col[R_STATUS * stride];
     }
@@ -618,13 +670,13 @@ struct Emu {
         col[R_PC * stride] = pc | (p << 16) | (bank << 24);
         col[R_CYC_LO * stride] = cyc_lo;
         col[R_CYC_HI * stride] = cyc_hi;
-        col[R_PIA0 * stride] = pa_out | (pa_ddr << 8) | (pa_in << 16) | (pb_out << 24);
-        col[R_PIA1 * stride] = pb_ddr | (pb_in << 8) | (uf << 16) | (pdump << 24);
+        col[R_PIA0 * stride] = (ports & 0xFFFFu) | ((pins & 0xFFu) << 16) | (((ports >> 16) & 0xFFu) << 24);
+        col[R_PIA1 * stride] = (ports >> 24) | (((pins >> 8) & 0xFFu) << 8) | (uf << 16) | (((tw >> 18) & 1u) << 24);
         col[R_TIMER * stride] = tv | (ps << 16);
         col[R_SELPC * stride] = sel | (pcnt << 16);
         col[R_TIA0 * stride] = clock | (scanline << 16);
-        col[R_TIA1 * stride] = wsync | (fcomp << 8) | (vsync << 16) | (vblank << 24);
-        col[R_TIA2 * stride] = inpt4 | (inpt5 << 8) | (pad0 << 16) | (pad1 << 24);
+        col[R_TIA1 * stride] = ((tw >> 16) & 1u) | (((tw >> 17) & 1u) << 8) | ((tw & 0xFFFFu) << 16);
+        col[R_TIA2 * stride] = ((pins >> 16) & 1u) | (((pins >> 17) & 1u) << 8) | (pads << 16);
         col[R_FRAME * stride] = frame_no;
         col[R_STATUS * stride] = status;
     }

@@ -107,9 +107,9 @@ struct Runner {
             e.load_hot(G->snapshot, 1);
         }
         if (G->actions) e.apply_action(G->actions[(size_t)f * G->act_stride + i]);
-        e.fcomp = 0;
+        e.tw &= ~TW_FCOMP;
         fcyc = 0;
-        phase = (e.vsync & 2u) ? 0u : 1u;
+        phase = e.vsync_on() ? 0u : 1u;
         return true;
     }
 
@@ -118,27 +118,26 @@ struct Runner {
     // lane should run again immediately (a WSYNC skip is pending).
     __device__ __forceinline__ bool one()
     {
-        if (e.wsync) {
-            uint32_t s = e.tia_skip();
-            e.pia_tick(s);
-            fcyc += s;
+        uint32_t n;
+        if (e.wsync()) {
+            n = e.tia_skip();
         } else {
-            uint32_t c = e.step();
-            if (c == 0) { e.status |= FA_STATUS_ILLEGAL_OPCODE; active = false; return false; }
+            n = e.step();
+            if (n == 0) { e.status |= FA_STATUS_ILLEGAL_OPCODE; active = false; return false; }
             e.instr++;
-            uint32_t lo = e.cyc_lo + c;
-            e.cyc_hi += lo < c ? 1u : 0u;
+            uint32_t lo = e.cyc_lo + n;
+            e.cyc_hi += lo < n ? 1u : 0u;
             e.cyc_lo = lo;
-            fcyc += c;
-            e.tia_tick(c);
-            e.pia_tick(c);
+            e.tia_tick(n);
         }
+        e.pia_tick(n);
+        fcyc += n;
         if (phase == 0u) {
             if (fcyc > FA_VSYNC_BUDGET) { e.status |= FA_STATUS_VSYNC_BUDGET; active = false; return false; }
-            if (!(e.vsync & 2u)) phase = 1u;
+            if (!e.vsync_on()) phase = 1u;
         } else {
             const bool cap = fcyc > FA_FRAME_CYCLE_CAP;
-            if (cap || (e.vsync & 2u)) {
+            if (cap || e.vsync_on()) {
                 if (cap) e.status |= FA_STATUS_CYCLE_CAP;
                 e.frame_no++;
                 f++;
@@ -146,7 +145,7 @@ struct Runner {
                 return false;
             }
         }
-        return e.wsync != 0;
+        return e.wsync();
     }
 
     __device__ __forceinline__ void iterate()
