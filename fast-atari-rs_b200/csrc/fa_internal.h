@@ -13,6 +13,9 @@
 #define FA_DEVERR_TMA_TIMEOUT 0x1u
 
 #define FA_MAX_GROUPS 16
+// Dynamic shared memory a CTA may use (227 KiB opt-in limit minus the static
+// barrier word and headroom).
+#define FA_SMEM_PER_CTA_MAX (227 * 1024 - 1024)
 
 // One cart's instance set in a launch.
 struct FaGroup {
@@ -26,14 +29,17 @@ struct FaGroup {
     uint32_t k;                  // frames to run per instance
     uint32_t episode_frames;     // 0 = no periodic reset
     uint32_t sched;              // FA_SCHED_*
-    uint32_t unit_begin;         // first work unit of this group
+    uint32_t unit_begin;         // first work unit of this group (set by fa_launch_run)
+    uint32_t rom_off;            // offset of the ROM in the shared-memory library (set by fa_launch_run)
+    uint32_t rom_owner;          // 1 if this group stages the ROM (set by fa_launch_run)
 };
 
 struct FaLaunch {
     FaGroup g[FA_MAX_GROUPS];
     uint32_t ngroups;
     uint32_t nunits;
-    uint32_t rom_bytes_max;      // shared-memory ROM bytes reserved per CTA
+    uint32_t rom_bytes_max;      // shared-memory ROM bytes reserved per CTA (CTA-granular form)
+    uint32_t romlib_bytes;       // all ROMs of the launch (warp-granular form, set by fa_launch_run)
     uint32_t* queue;             // work-queue counter (persistent form) or null
     uint32_t* err;               // device error word
     unsigned long long* instr;   // guest-instruction counter, or null
@@ -44,6 +50,9 @@ struct FaLaunch {
 // CTAs per SM the occupancy calculator allows (cached per block and shared-
 // memory size, so that the call is safe inside a stream capture).
 cudaError_t fa_launch_run(const FaLaunch& L, int block, bool persistent, int sms, cudaStream_t s);
+// Everything fa_launch_run does before launching (kernel choice, shared-memory
+// attribute, occupancy), so that a later launch is safe inside a capture.
+cudaError_t fa_launch_prepare(const FaLaunch& L, int block, bool persistent);
 // CTAs of fa_run<block> resident per SM for this ROM size (-1 on error).
 int fa_launch_occupancy(int block, uint32_t rom_bytes_max);
 cudaError_t fa_launch_broadcast(uint32_t* state, uint32_t stride, uint32_t n, const uint32_t* col,

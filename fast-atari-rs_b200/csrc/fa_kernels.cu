@@ -207,12 +207,13 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
     return rounds;
 }
 
+// Run one work unit: instances [first, first + count) of group G, one per
+// thread; t is the thread's slot in a private-byte slab of BLOCK slots.
 template <int BLOCK>
 __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint32_t count, const uint8_t* rom_s,
-                                         uint32_t* priv, unsigned long long* instr_out,
+                                         uint32_t* priv, uint32_t t, unsigned long long* instr_out,
                                          unsigned long long* rounds_out)
 {
-    const uint32_t t = threadIdx.x;
     Runner<BLOCK> r;
     r.G = &G;
     r.i = first + t;
@@ -293,8 +294,59 @@ __global__ void __launch_bounds__(BLOCK) fa_run(const __grid_constant__ FaLaunch
         }
         const uint32_t first = (u - G.unit_begin) * BLOCK;
         const uint32_t count = G.n - first < BLOCK ? G.n - first : BLOCK;
-        run_unit<BLOCK>(G, first, count, rom_s, priv, L.instr, L.rounds);
+        run_unit<BLOCK>(G, first, count, rom_s, priv, threadIdx.x, L.instr, L.rounds);
         __syncthreads();
+    }
+}
+
+// Warp-granular form: every warp pops its own 32-instance work units, and
+// every CTA holds all of the launch's ROM images at once (the "ROM library",
+// staged once with TMA bulk copies), so units of any cart run in any warp
+// and a CTA can be as large as shared memory allows.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) fa_run_warps(const __grid_constant__ FaLaunch L)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    const uint32_t FULL = 0xFFFFFFFFu;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    uint32_t* priv = (uint32_t*)(smem + L.romlib_bytes) + warp * (FA_PRIV_WORDS * 32u);
+
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bar, L.romlib_bytes);
+        for (uint32_t g = 0; g < L.ngroups; g++) {
+            if (!L.g[g].rom_owner) continue;
+            for (uint32_t off = 0; off < L.g[g].nbanks * 4096u; off += 4096u)
+                bulk_g2s(smem + L.g[g].rom_off + off, L.g[g].rom + off, 4096u, &bar);
+        }
+    }
+    bool ok = false;
+    const uint64_t t0 = globaltimer_ns();
+    while (true) {
+        if (mbar_try_wait(&bar, 0)) { ok = true; break; }
+        if (globaltimer_ns() - t0 > FA_WAIT_LIMIT_NS) break;
+    }
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
+        return;
+    }
+    for (uint32_t round = 0;; round++) {
+        uint32_t u = 0;
+        if (lane == 0) {
+            if (L.queue) u = atomicAdd(L.queue, 1u);
+            else u = round == 0 ? blockIdx.x * WARPS + warp : 0xFFFFFFFFu;
+        }
+        u = __shfl_sync(FULL, u, 0);
+        if (u >= L.nunits) break;
+        uint32_t g = 0;
+        while (g + 1 < L.ngroups && u >= L.g[g + 1].unit_begin) g++;
+        const FaGroup& G = L.g[g];
+        const uint32_t first = (u - G.unit_begin) * 32u;
+        const uint32_t count = G.n - first < 32u ? G.n - first : 32u;
+        run_unit<32>(G, first, count, smem + G.rom_off, priv, lane, L.instr, L.rounds);
     }
 }
 
@@ -349,6 +401,7 @@ static cudaError_t launch_block(const FaLaunch& L, bool persistent, int sms, cud
     const size_t smem = (size_t)L.rom_bytes_max + (size_t)FA_PRIV_WORDS * BLOCK * 4u;
     const int per_sm = per_sm_for<BLOCK>(smem);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    if (sms <= 0) return cudaSuccess;                                  // prepare only
     uint32_t grid = L.nunits;
     if (persistent) {
         uint32_t cap = (uint32_t)(per_sm * sms);
@@ -359,8 +412,111 @@ static cudaError_t launch_block(const FaLaunch& L, bool persistent, int sms, cud
     return cudaGetLastError();
 }
 
-cudaError_t fa_launch_run(const FaLaunch& L, int block, bool persistent, int sms, cudaStream_t s)
+namespace {
+std::map<std::pair<int, std::pair<int, size_t>>, int> g_warps_per_sm;   // (device, warps, smem) -> CTAs/SM
+
+template <int WARPS>
+int warps_per_sm_for(size_t smem)
 {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_cfg_mu);
+    auto key = std::make_pair(dev, std::make_pair(WARPS, smem));
+    auto it = g_warps_per_sm.find(key);
+    if (it != g_warps_per_sm.end()) return it->second;
+    const auto max_key = std::make_pair(dev, std::make_pair(WARPS, (size_t)0));
+    if (g_warps_per_sm.find(max_key) == g_warps_per_sm.end()) {
+        if (cudaFuncSetAttribute(fa::fa_run_warps<WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 FA_SMEM_PER_CTA_MAX) != cudaSuccess)
+            return -1;
+        g_warps_per_sm[max_key] = 0;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run_warps<WARPS>, WARPS * 32, smem) !=
+        cudaSuccess)
+        return -1;
+    g_warps_per_sm[key] = per_sm;
+    return per_sm;
+}
+
+template <int WARPS>
+cudaError_t launch_warps(const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
+{
+    const size_t smem = (size_t)L.romlib_bytes + (size_t)WARPS * FA_PRIV_WORDS * 32u * 4u;
+    const int per_sm = warps_per_sm_for<WARPS>(smem);
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    if (sms <= 0) return cudaSuccess;                                  // prepare only
+    uint32_t grid = (L.nunits + WARPS - 1) / WARPS;
+    if (persistent) {
+        const uint32_t cap = (uint32_t)(per_sm * sms);
+        grid = grid < cap ? grid : cap;
+    }
+    if (grid == 0) return cudaSuccess;
+    fa::fa_run_warps<WARPS><<<grid, WARPS * 32, smem, s>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_warps_n(int warps, const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
+{
+    switch (warps) {
+    case 2: return launch_warps<2>(L, persistent, sms, s);
+    case 4: return launch_warps<4>(L, persistent, sms, s);
+    case 8: return launch_warps<8>(L, persistent, sms, s);
+    case 16: return launch_warps<16>(L, persistent, sms, s);
+    case 20: return launch_warps<20>(L, persistent, sms, s);
+    case 24: return launch_warps<24>(L, persistent, sms, s);
+    case 28: return launch_warps<28>(L, persistent, sms, s);
+    case 32: return launch_warps<32>(L, persistent, sms, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace
+
+// Lay out the ROM library (one copy per distinct ROM buffer) and the work
+// units; returns the library size, or 0 if it cannot fit beside one warp slab.
+static uint32_t plan_romlib(FaLaunch& L)
+{
+    uint32_t bytes = 0;
+    for (uint32_t g = 0; g < L.ngroups; g++) {
+        L.g[g].rom_owner = 1;
+        for (uint32_t h = 0; h < g; h++)
+            if (L.g[h].rom == L.g[g].rom) { L.g[g].rom_off = L.g[h].rom_off; L.g[g].rom_owner = 0; break; }
+        if (L.g[g].rom_owner) { L.g[g].rom_off = bytes; bytes += L.g[g].nbanks * 4096u; }
+    }
+    return bytes;
+}
+
+static void plan_units(FaLaunch& L, uint32_t unit)
+{
+    uint32_t units = 0;
+    for (uint32_t g = 0; g < L.ngroups; g++) {
+        L.g[g].unit_begin = units;
+        units += (L.g[g].n + unit - 1) / unit;
+    }
+    L.nunits = units;
+}
+
+cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int sms, cudaStream_t s)
+{
+    FaLaunch L = L_in;
+    const uint32_t lib = plan_romlib(L);
+    L.romlib_bytes = lib;
+    const uint32_t slab = FA_PRIV_WORDS * 32u * 4u;
+    const int fit = (int)((FA_SMEM_PER_CTA_MAX - (int)lib) / (int)slab);
+    if (fit >= block / 32) {
+        int warps = block / 32;
+        if (persistent) {
+            // As many warps per CTA as shared memory allows (one CTA per SM).
+            static const int sizes[] = { 32, 28, 24, 20, 16, 8, 4, 2 };
+            for (int w : sizes)
+                if (w <= fit) { warps = w; break; }
+        }
+        plan_units(L, 32u);
+        return launch_warps_n(warps, L, persistent, sms, s);
+    }
+    // ROM library too large for shared memory: CTA-granular units that
+    // re-stage one cart's ROM at a time.
+    plan_units(L, (uint32_t)block);
     switch (block) {
     case 64: return launch_block<64>(L, persistent, sms, s);
     case 128: return launch_block<128>(L, persistent, sms, s);
@@ -368,6 +524,11 @@ cudaError_t fa_launch_run(const FaLaunch& L, int block, bool persistent, int sms
     case 512: return launch_block<512>(L, persistent, sms, s);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t fa_launch_prepare(const FaLaunch& L, int block, bool persistent)
+{
+    return fa_launch_run(L, block, persistent, 0, nullptr);
 }
 
 int fa_launch_occupancy(int block, uint32_t rom_bytes_max)

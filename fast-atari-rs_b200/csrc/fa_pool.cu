@@ -321,8 +321,7 @@ extern "C" int fa_pool_graph_create(fa_pool* p, const uint8_t* const* d_actions,
     // Warm the launch configuration cache outside the capture.
     FaLaunch L;
     build_launch(p, d_actions, (uint32_t)k, d_obs, 0, L);
-    if (fa_launch_occupancy(p->block, L.rom_bytes_max) < 1)
-        return fa_fail(FA_ERR_CUDA, "no resident CTA fits block %d", p->block);
+    FA_CUDA(fa_launch_prepare(L, p->block, p->persistent));
     fa_graph* g = new (std::nothrow) fa_graph();
     if (!g) return fa_fail(FA_ERR_CAPACITY, "out of host memory");
     g->pool = p;
