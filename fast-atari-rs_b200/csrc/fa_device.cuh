@@ -164,7 +164,8 @@ struct Emu {
     uint32_t hot_lo, nbanks;
     // ---- CPU (src/cpu.rs:96-105)
     uint32_t a, x, y, sp, p, pc, bank;
-    uint32_t cyc_lo, cyc_hi;
+    uint32_t cyc_lo, cyc_hi;  // Cpu::cycles, folded in from cyc_acc at frame ends
+    uint32_t cyc_acc;         // instruction cycles not yet folded into cyc_lo/cyc_hi
     // ---- PIA (src/pia.rs:26-44): timer unpacked (ticked every instruction),
     //      ports and input pins packed (touched only by I/O accesses)
     uint32_t tv, ps, sel, uf;
@@ -622,12 +623,24 @@ struct Emu {
     __device__ __forceinline__ uint32_t step()
     {
         const uint32_t pc0 = pc;
-        const uint32_t op = read(pc0);
-        if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }
+        const uint32_t a0 = pc0 & 0x1FFFu;
+        uint32_t op, b1, b2 = 0;
+        if (a0 >= 0x1000u && a0 + 2u < hot_lo) {
+            // Fast path: the three bytes at pc0 lie in the current bank and
+            // below every hotspot, so reading them has no side effect.
+            const uint8_t* q = rom + (bank << 12) + (a0 & 0xFFFu);
+            op = q[0];
+            if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }
+            b1 = q[1];
+            b2 = q[2];
+        } else {
+            op = read(pc0);
+            if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }
+            b1 = read((pc0 + 1u) & 0xFFFFu);
+            const uint32_t bb = (op >> 2) & 7u;
+            if (bb == 3u || bb == 7u || (bb == 6u && (op & 3u) == 1u)) b2 = read((pc0 + 2u) & 0xFFFFu);
+        }
         const uint32_t aaa = op >> 5, bbb = (op >> 2) & 7u, cc = op & 3u;
-        const uint32_t b1 = read((pc0 + 1u) & 0xFFFFu);
-        uint32_t b2 = 0;
-        if (bbb == 3u || bbb == 7u || (bbb == 6u && cc == 1u)) b2 = read((pc0 + 2u) & 0xFFFFu);
         if (cc == 1u) return group1(pc0, aaa, bbb, b1, b2);
         if (cc == 2u) return group2(pc0, aaa, bbb, b1, b2);
         return group0(pc0, aaa, bbb, b1, b2);
@@ -649,6 +662,7 @@ struct Emu {
         w = col[R_PC * stride];    pc = w & 0xFFFF; p = (w >> 16) & 0xFF; bank = w >> 24;
         cyc_lo = col[R_CYC_LO * stride];
         cyc_hi = col[R_CYC_HI * stride];
+        cyc_acc = 0;
         const uint32_t p0 = col[R_PIA0 * stride];                  // pa_out pa_ddr pa_in pb_out
         const uint32_t p1 = col[R_PIA1 * stride];                  // pb_ddr pb_in uf pdump
         ports = (p0 & 0xFFFFu) | ((p0 >> 24) << 16) | ((p1 & 0xFFu) << 24);
@@ -663,6 +677,13 @@ struct Emu {
         pads = w >> 16;
         frame_no = col[R_FRAME * stride];
         status = col[R_STATUS * stride];
+    }
+    __device__ __forceinline__ void fold_cycles()
+    {
+        const uint32_t lo = cyc_lo + cyc_acc;
+        cyc_hi += lo < cyc_acc ? 1u : 0u;
+        cyc_lo = lo;
+        cyc_acc = 0;
     }
     __device__ __forceinline__ void store_hot(uint32_t* col, uint32_t stride) const
     {

@@ -125,9 +125,7 @@ struct Runner {
             n = e.step();
             if (n == 0) { e.status |= FA_STATUS_ILLEGAL_OPCODE; active = false; return false; }
             e.instr++;
-            uint32_t lo = e.cyc_lo + n;
-            e.cyc_hi += lo < n ? 1u : 0u;
-            e.cyc_lo = lo;
+            e.cyc_acc += n;
             e.tia_tick(n);
         }
         e.pia_tick(n);
@@ -139,6 +137,7 @@ struct Runner {
             const bool cap = fcyc > FA_FRAME_CYCLE_CAP;
             if (cap || e.vsync_on()) {
                 if (cap) e.status |= FA_STATUS_CYCLE_CAP;
+                e.fold_cycles();
                 e.frame_no++;
                 f++;
                 if (f >= G->k || !begin_frame()) { active = false; return false; }
@@ -159,16 +158,21 @@ struct Runner {
 // Runs every lane of the warp to the end of its frames.  The policy only
 // decides which lanes execute in each round; all lanes share one call site of
 // the emulator so its code is instantiated once.
+// Instructions a converged group may run per scheduling round.
+constexpr uint32_t FA_STEPS_PER_ROUND = 8;
+
 template <int BLOCK>
 __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
 {
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
+    const bool converge = sched == FA_SCHED_PC || sched == FA_SCHED_LINE;
     uint32_t rem = 0, grp = 0, rounds = 0;
     while (true) {
         const bool act = r.active;
         const uint32_t pcb = (r.e.bank << 16) | r.e.pc;
         bool go;
+        uint32_t gm = FULL, lead = 0;
         if (sched == FA_SCHED_MATCH) {
             // __match_any_sync groups lanes by (bank, pc); each group runs its
             // instruction together, every group once per round.
@@ -180,7 +184,7 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
             const uint32_t g = __shfl_sync(FULL, grp, __ffs(rem) - 1u);
             go = (g >> lane) & 1u;
             rem &= ~g;
-        } else if (sched == FA_SCHED_PC || sched == FA_SCHED_LINE) {
+        } else if (converge) {
             // Convergence scheduling: the lane furthest behind (frame, then
             // scanline for FA_SCHED_LINE, then pc) leads and every lane at the
             // leader's (bank, pc) runs with it.  Lanes that branched ahead wait
@@ -192,17 +196,30 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
                 : (fc << 16) | r.e.pc;
             if (!act) key = 0xFFFFFFFFu;
             const uint32_t mk = __reduce_min_sync(FULL, key);
-            const uint32_t lead = __ffs(__ballot_sync(FULL, key == mk)) - 1u;
-            // Every lane must take part in the full-mask shuffle, so it is
-            // not folded into a short-circuit condition.
+            lead = __ffs(__ballot_sync(FULL, key == mk)) - 1u;
+            // Every lane takes part in the full-mask shuffle, so it is not
+            // folded into a short-circuit condition.
             const uint32_t lpcb = __shfl_sync(FULL, pcb, lead);
             go = act && pcb == lpcb;
+            gm = __ballot_sync(FULL, go);
         } else {
             if (!__any_sync(FULL, act)) break;
             go = act;
         }
-        rounds++;
-        if (go) r.iterate();
+        // One call site of the emulator for every policy.  A converged group
+        // keeps running while its lanes stay at one pc: one vote per
+        // instruction instead of a full scheduling round.
+        uint32_t steps = 0;
+        if (go) {
+            while (true) {
+                r.iterate();
+                if (!converge || ++steps >= FA_STEPS_PER_ROUND) break;
+                const uint32_t mp = (r.e.bank << 16) | r.e.pc;
+                const uint32_t lp = __shfl_sync(gm, mp, lead);
+                if (!__all_sync(gm, r.active && mp == lp)) break;
+            }
+        }
+        rounds += converge ? __shfl_sync(FULL, steps, lead) : 1u;
     }
     return rounds;
 }
@@ -238,6 +255,7 @@ __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint3
     }
     const uint32_t rounds = run_lanes<BLOCK>(r, G.sched);
     if (valid) {
+        r.e.fold_cycles();
         r.e.store_priv(col, G.stride);
         r.e.store_hot(col, G.stride);
         if (G.obs) {
