@@ -147,6 +147,15 @@ struct Runner {
         return e.wsync();
     }
 
+    // Scheduling key: frame, then (FA_SCHED_LINE) scanline, then pc.
+    __device__ __forceinline__ uint32_t key(uint32_t sched) const
+    {
+        const uint32_t fc = f < 0x7Fu ? f : 0x7Fu;
+        return sched == FA_SCHED_LINE
+            ? (fc << 25) | ((e.scanline < 0x1FFu ? e.scanline : 0x1FFu) << 16) | e.pc
+            : (fc << 16) | e.pc;
+    }
+
     __device__ __forceinline__ void iterate()
     {
 #pragma unroll 1
@@ -172,7 +181,7 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
         const bool act = r.active;
         const uint32_t pcb = (r.e.bank << 16) | r.e.pc;
         bool go;
-        uint32_t gm = FULL, lead = 0;
+        uint32_t gm = FULL, lead = 0, wait_key = 0;
         if (sched == FA_SCHED_MATCH) {
             // __match_any_sync groups lanes by (bank, pc); each group runs its
             // instruction together, every group once per round.
@@ -190,11 +199,7 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
             // leader's (bank, pc) runs with it.  Lanes that branched ahead wait
             // until the others reach the same pc, so the warp re-converges.
             if (!__any_sync(FULL, act)) break;
-            const uint32_t fc = r.f < 0x7Fu ? r.f : 0x7Fu;
-            uint32_t key = sched == FA_SCHED_LINE
-                ? (fc << 25) | ((r.e.scanline < 0x1FFu ? r.e.scanline : 0x1FFu) << 16) | r.e.pc
-                : (fc << 16) | r.e.pc;
-            if (!act) key = 0xFFFFFFFFu;
+            const uint32_t key = act ? r.key(sched) : 0xFFFFFFFFu;
             const uint32_t mk = __reduce_min_sync(FULL, key);
             lead = __ffs(__ballot_sync(FULL, key == mk)) - 1u;
             // Every lane takes part in the full-mask shuffle, so it is not
@@ -202,6 +207,11 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
             const uint32_t lpcb = __shfl_sync(FULL, pcb, lead);
             go = act && pcb == lpcb;
             gm = __ballot_sync(FULL, go);
+            // The smallest key among the lanes left waiting: the group keeps
+            // running only while its leader's key stays below it (so it stops
+            // where a waiting lane could join), which is exactly the order
+            // one-instruction rounds would follow.
+            wait_key = __reduce_min_sync(FULL, go ? 0xFFFFFFFFu : key);
         } else {
             if (!__any_sync(FULL, act)) break;
             go = act;
@@ -216,7 +226,8 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
                 if (!converge || ++steps >= FA_STEPS_PER_ROUND) break;
                 const uint32_t mp = (r.e.bank << 16) | r.e.pc;
                 const uint32_t lp = __shfl_sync(gm, mp, lead);
-                if (!__all_sync(gm, r.active && mp == lp)) break;
+                const uint32_t lk = __shfl_sync(gm, r.active ? r.key(sched) : 0xFFFFFFFFu, lead);
+                if (!__all_sync(gm, r.active && mp == lp && lk < wait_key)) break;
             }
         }
         rounds += converge ? __shfl_sync(FULL, steps, lead) : 1u;
