@@ -19,6 +19,7 @@
 #pragma once
 #include <stdint.h>
 
+#include "fa_internal.h"
 #include "fa_layout.h"
 
 namespace fa {
@@ -59,12 +60,15 @@ __device__ __forceinline__ uint32_t mod160(int v)
     return (uint32_t)(r < 0 ? r + 160 : r);
 }
 
+// Byte o (>= 128) of an instance's private bytes, in its HBM state rows:
+// `col` is the instance's column base, stride4 the row stride in bytes.
+__device__ __forceinline__ uint32_t cold_off(uint32_t o, uint32_t stride4) { return (o >> 2) * stride4 + (o & 3u); }
+
 // TIA or PIA register read (HeadlessTia::read, src/headless_tia.rs:205-223;
 // Pia::read I/O half, src/pia.rs:169-199).  Bit 8 of the result asks the
 // caller to clear the timer underflow flag (an INTIM read).
-template <int BLOCK>
 __device__ __noinline__ uint32_t io_read(uint32_t a, uint32_t pcnt, uint32_t pins, uint32_t pads,
-                                         uint32_t ports, uint32_t timer, const uint8_t* pv)
+                                         uint32_t ports, uint32_t timer, const uint8_t* col, uint32_t stride4)
 {
     if (a & 0x80u) {                                                 // PIA: (a & 0x280) == 0x280
         switch (a & 7u) {
@@ -78,7 +82,7 @@ __device__ __noinline__ uint32_t io_read(uint32_t a, uint32_t pcnt, uint32_t pin
         }
     }
     const uint32_t r = a & 0x0Fu;
-    if (r < 8u) return pv[priv_off<BLOCK>(PB_CX + r)];
+    if (r < 8u) return col[cold_off(PB_CX + r, stride4)];
     switch (r) {
     case 0x8: return pcnt >= (pads & 0xFFu) ? 0x80u : 0u;
     case 0x9: return pcnt >= (pads >> 8) ? 0x80u : 0u;
@@ -90,15 +94,15 @@ __device__ __noinline__ uint32_t io_read(uint32_t a, uint32_t pcnt, uint32_t pin
 }
 
 // HeadlessTia::write (src/headless_tia.rs:225-298).  tw is the packed flag
-// word, lw = scanline | paddle_counter<<16; both come back updated.
-template <int BLOCK>
+// word, lw = scanline | paddle_counter<<16; both come back updated.  The
+// write-only registers live in the instance's HBM rows (col, stride4).
 __device__ __noinline__ uint2 tia_write_io(uint32_t a, uint32_t v, uint32_t clock, uint32_t tw, uint32_t lw,
-                                           uint8_t* pv)
+                                           uint8_t* col, uint32_t stride4)
 {
-    auto stp = [&](uint32_t o, uint32_t val) { pv[priv_off<BLOCK>(o)] = (uint8_t)val; };
-    auto ldp = [&](uint32_t o) -> uint32_t { return pv[priv_off<BLOCK>(o)]; };
-    auto stp16 = [&](uint32_t o, uint32_t val) { *(uint16_t*)(pv + priv_off<BLOCK>(o)) = (uint16_t)val; };
-    auto ldp16 = [&](uint32_t o) -> uint32_t { return *(const uint16_t*)(pv + priv_off<BLOCK>(o)); };
+    auto stp = [&](uint32_t o, uint32_t val) { col[cold_off(o, stride4)] = (uint8_t)val; };
+    auto ldp = [&](uint32_t o) -> uint32_t { return col[cold_off(o, stride4)]; };
+    auto stp16 = [&](uint32_t o, uint32_t val) { *(uint16_t*)(col + cold_off(o, stride4)) = (uint16_t)val; };
+    auto ldp16 = [&](uint32_t o) -> uint32_t { return *(const uint16_t*)(col + cold_off(o, stride4)); };
     const uint32_t r = a & 0x3Fu;
     switch (r) {
     case 0x00:                                                        // VSYNC rising edge starts a frame
@@ -159,13 +163,14 @@ __device__ __noinline__ uint4 pia_write_io(uint32_t a, uint32_t v, uint32_t port
 template <int BLOCK>
 struct Emu {
     // ---- placement
-    uint8_t* pv;             // private bytes of this thread (shared memory)
+    uint8_t* pv;             // this thread's RAM (shared memory, interleaved by thread)
+    const FaGroup* G;        // the instance's group (HBM state rows, stride)
+    uint32_t i;              // the instance's index in its group
     const uint8_t* rom;      // shared-memory ROM image, nbanks * 4 KiB
     uint32_t hot_lo, nbanks;
     // ---- CPU (src/cpu.rs:96-105)
     uint32_t a, x, y, sp, p, pc, bank;
-    uint32_t cyc_lo, cyc_hi;  // Cpu::cycles, folded in from cyc_acc at frame ends
-    uint32_t cyc_acc;         // instruction cycles not yet folded into cyc_lo/cyc_hi
+    uint32_t cyc_acc;         // instruction cycles not yet added to Cpu::cycles in HBM
     // ---- PIA (src/pia.rs:26-44): timer unpacked (ticked every instruction),
     //      ports and input pins packed (touched only by I/O accesses)
     uint32_t tv, ps, sel, uf;
@@ -176,7 +181,21 @@ struct Emu {
     uint32_t clock, scanline, pcnt;
     uint32_t tw;             // vsync | vblank<<8 | wsync<<16 | frame_complete<<17 | paddle_dumped<<18
     // ---- run bookkeeping
-    uint32_t frame_no, status, instr;
+    uint32_t instr;           // instructions executed in this launch (statistics)
+
+    // The instance's HBM rows.  Cpu::cycles, the frame counter and the run
+    // status stay there and change only at frame boundaries.
+    __device__ __forceinline__ uint32_t* column() const { return G->state + i; }
+    __device__ __forceinline__ uint32_t& row(uint32_t w) const { return column()[(size_t)w * G->stride]; }
+    __device__ __forceinline__ void fold_cycles()
+    {
+        uint32_t& lo = row(R_CYC_LO);
+        const uint32_t v = lo + cyc_acc;
+        if (v < cyc_acc) row(R_CYC_HI) += 1u;
+        lo = v;
+        cyc_acc = 0;
+    }
+    __device__ __forceinline__ void set_status(uint32_t bits) { row(R_STATUS) |= bits; }
 
     __device__ __forceinline__ bool vsync_on() const { return (tw & 2u) != 0; }
     __device__ __forceinline__ bool wsync() const { return (tw & TW_WSYNC) != 0; }
@@ -265,7 +284,7 @@ struct Emu {
     // resident in the instruction cache.
     __device__ __forceinline__ uint32_t io(uint32_t a)               // TIA or PIA register read
     {
-        uint32_t r = io_read<BLOCK>(a, pcnt, pins, pads, ports, tv | (uf << 16), pv);
+        uint32_t r = io_read(a, pcnt, pins, pads, ports, tv | (uf << 16), (const uint8_t*)column(), G->stride * 4u);
         if (r & 0x100u) uf = 0;                                     // INTIM read clears the flag
         return r & 0xFFu;
     }
@@ -275,7 +294,7 @@ struct Emu {
             uint4 r = pia_write_io(a, v, ports, tv, ps, sel | (uf << 16));
             ports = r.x; tv = r.y; ps = r.z; sel = r.w & 0xFFFFu; uf = r.w >> 16;
         } else {
-            uint2 r = tia_write_io<BLOCK>(a, v, clock, tw, scanline | (pcnt << 16), pv);
+            uint2 r = tia_write_io(a, v, clock, tw, scanline | (pcnt << 16), (uint8_t*)column(), G->stride * 4u);
             tw = r.x; scanline = r.y & 0xFFFFu; pcnt = r.y >> 16;
         }
     }
@@ -660,8 +679,6 @@ struct Emu {
         uint32_t w;
         w = col[R_AXYS * stride];  a = w & 0xFF; x = (w >> 8) & 0xFF; y = (w >> 16) & 0xFF; sp = w >> 24;
         w = col[R_PC * stride];    pc = w & 0xFFFF; p = (w >> 16) & 0xFF; bank = w >> 24;
-        cyc_lo = col[R_CYC_LO * stride];
-        cyc_hi = col[R_CYC_HI * stride];
         cyc_acc = 0;
         const uint32_t p0 = col[R_PIA0 * stride];                  // pa_out pa_ddr pa_in pb_out
         const uint32_t p1 = col[R_PIA1 * stride];                  // pb_ddr pb_in uf pdump
@@ -675,22 +692,11 @@ struct Emu {
         w = col[R_TIA2 * stride];                                   // inpt4 inpt5 pad0 pad1
         pins = ((p0 >> 16) & 0xFFu) | (((p1 >> 8) & 0xFFu) << 8) | ((w & 1u) << 16) | (((w >> 8) & 1u) << 17);
         pads = w >> 16;
-        frame_no = col[R_FRAME * stride];
-        status = col[R_STATUS * stride];
-    }
-    __device__ __forceinline__ void fold_cycles()
-    {
-        const uint32_t lo = cyc_lo + cyc_acc;
-        cyc_hi += lo < cyc_acc ? 1u : 0u;
-        cyc_lo = lo;
-        cyc_acc = 0;
     }
     __device__ __forceinline__ void store_hot(uint32_t* col, uint32_t stride) const
     {
         col[R_AXYS * stride] = a | (x << 8) | (y << 16) | (sp << 24);
         col[R_PC * stride] = pc | (p << 16) | (bank << 24);
-        col[R_CYC_LO * stride] = cyc_lo;
-        col[R_CYC_HI * stride] = cyc_hi;
         col[R_PIA0 * stride] = (ports & 0xFFFFu) | ((pins & 0xFFu) << 16) | (((ports >> 16) & 0xFFu) << 24);
         col[R_PIA1 * stride] = (ports >> 24) | (((pins >> 8) & 0xFFu) << 8) | (uf << 16) | (((tw >> 18) & 1u) << 24);
         col[R_TIMER * stride] = tv | (ps << 16);
@@ -698,21 +704,19 @@ struct Emu {
         col[R_TIA0 * stride] = clock | (scanline << 16);
         col[R_TIA1 * stride] = ((tw >> 16) & 1u) | (((tw >> 17) & 1u) << 8) | ((tw & 0xFFFFu) << 16);
         col[R_TIA2 * stride] = ((pins >> 16) & 1u) | (((pins >> 17) & 1u) << 8) | (pads << 16);
-        col[R_FRAME * stride] = frame_no;
-        col[R_STATUS * stride] = status;
     }
-    // Private words from global (stride-separated rows) into shared memory.
-    __device__ __forceinline__ void load_priv(const uint32_t* col, uint32_t stride)
+    // RAM words from the HBM rows into shared memory and back.
+    __device__ __forceinline__ void load_ram(const uint32_t* c, uint32_t stride)
     {
         uint32_t* w = (uint32_t*)pv;
 #pragma unroll 4
-        for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) w[k * BLOCK] = col[k * stride];
+        for (uint32_t k = 0; k < FA_SMEM_WORDS; k++) w[k * BLOCK] = c[k * stride];
     }
-    __device__ __forceinline__ void store_priv(uint32_t* col, uint32_t stride) const
+    __device__ __forceinline__ void store_ram(uint32_t* c, uint32_t stride) const
     {
         const uint32_t* w = (const uint32_t*)pv;
 #pragma unroll 4
-        for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) col[k * stride] = w[k * BLOCK];
+        for (uint32_t k = 0; k < FA_SMEM_WORDS; k++) c[k * stride] = w[k * BLOCK];
     }
 };
 

@@ -95,18 +95,21 @@ __device__ bool stage_rom(uint8_t* dst, const uint8_t* src, uint32_t bytes, uint
 template <int BLOCK>
 struct Runner {
     Emu<BLOCK> e;
-    const FaGroup* G;
-    uint32_t i, f, phase, fcyc;
+    uint32_t f, phase, fcyc;
     bool active;
 
+    // Start frame f: periodic reset, action, frame_complete cleared
+    // (src/atari.rs:571-586).  False if the instance is halted.
     __device__ __forceinline__ bool begin_frame()
     {
-        if (e.status & FA_STATUS_HALT_MASK) return false;
-        if (G->episode_frames && e.frame_no >= G->episode_frames && G->snapshot) {
-            e.load_priv(G->snapshot, 1);
+        const FaGroup* G = e.G;
+        if (e.row(R_STATUS) & FA_STATUS_HALT_MASK) return false;
+        if (G->episode_frames && G->snapshot && e.row(R_FRAME) >= G->episode_frames) {
+            e.load_ram(G->snapshot, 1);
+            for (uint32_t w = FA_SMEM_WORDS; w < FA_ROWS; w++) e.row(w) = G->snapshot[w];
             e.load_hot(G->snapshot, 1);
         }
-        if (G->actions) e.apply_action(G->actions[(size_t)f * G->act_stride + i]);
+        if (G->actions) e.apply_action(G->actions[(size_t)f * G->act_stride + e.i]);
         e.tw &= ~TW_FCOMP;
         fcyc = 0;
         phase = e.vsync_on() ? 0u : 1u;
@@ -123,7 +126,7 @@ struct Runner {
             n = e.tia_skip();
         } else {
             n = e.step();
-            if (n == 0) { e.status |= FA_STATUS_ILLEGAL_OPCODE; active = false; return false; }
+            if (n == 0) { e.fold_cycles(); e.set_status(FA_STATUS_ILLEGAL_OPCODE); active = false; return false; }
             e.instr++;
             e.cyc_acc += n;
             e.tia_tick(n);
@@ -131,16 +134,21 @@ struct Runner {
         e.pia_tick(n);
         fcyc += n;
         if (phase == 0u) {
-            if (fcyc > FA_VSYNC_BUDGET) { e.status |= FA_STATUS_VSYNC_BUDGET; active = false; return false; }
+            if (fcyc > FA_VSYNC_BUDGET) {
+                e.fold_cycles();
+                e.set_status(FA_STATUS_VSYNC_BUDGET);
+                active = false;
+                return false;
+            }
             if (!e.vsync_on()) phase = 1u;
         } else {
             const bool cap = fcyc > FA_FRAME_CYCLE_CAP;
             if (cap || e.vsync_on()) {
-                if (cap) e.status |= FA_STATUS_CYCLE_CAP;
+                if (cap) e.set_status(FA_STATUS_CYCLE_CAP);
                 e.fold_cycles();
-                e.frame_no++;
+                e.row(R_FRAME) += 1u;
                 f++;
-                if (f >= G->k || !begin_frame()) { active = false; return false; }
+                if (f >= e.G->k || !begin_frame()) { active = false; return false; }
                 return false;
             }
         }
@@ -243,35 +251,36 @@ __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint3
                                          unsigned long long* rounds_out)
 {
     Runner<BLOCK> r;
-    r.G = &G;
-    r.i = first + t;
     r.f = 0;
     r.phase = 0;
     r.fcyc = 0;
     r.active = false;
     r.e.pv = (uint8_t*)(priv + t);
+    r.e.G = &G;
+    r.e.i = first + t;
     r.e.rom = rom_s;
     r.e.hot_lo = G.hot_lo;
     r.e.nbanks = G.nbanks;
     r.e.instr = 0;
+    r.e.cyc_acc = 0;
     r.e.pc = 0;
     r.e.bank = 0;
     r.e.scanline = 0;
     const bool valid = t < count;
-    uint32_t* col = G.state + r.i;
+    uint32_t* col = G.state + r.e.i;
     if (valid) {
-        r.e.load_priv(col, G.stride);
+        r.e.load_ram(col, G.stride);
         r.e.load_hot(col, G.stride);
         if (G.k > 0) r.active = r.begin_frame();
     }
     const uint32_t rounds = run_lanes<BLOCK>(r, G.sched);
     if (valid) {
         r.e.fold_cycles();
-        r.e.store_priv(col, G.stride);
+        r.e.store_ram(col, G.stride);
         r.e.store_hot(col, G.stride);
         if (G.obs) {
             const uint32_t* w = priv + t;
-            uint4* o = (uint4*)(G.obs + (size_t)r.i * 128u);
+            uint4* o = (uint4*)(G.obs + (size_t)r.e.i * 128u);
 #pragma unroll
             for (uint32_t q = 0; q < 8u; q++)
                 o[q] = make_uint4(w[(4u * q) * BLOCK], w[(4u * q + 1u) * BLOCK], w[(4u * q + 2u) * BLOCK],
@@ -339,7 +348,7 @@ __global__ void __launch_bounds__(WARPS * 32) fa_run_warps(const __grid_constant
     __shared__ __align__(8) uint64_t bar;
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    uint32_t* priv = (uint32_t*)(smem + L.romlib_bytes) + warp * (FA_PRIV_WORDS * 32u);
+    uint32_t* priv = (uint32_t*)(smem + L.romlib_bytes) + warp * (FA_SMEM_WORDS * 32u);
 
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
@@ -410,7 +419,7 @@ int per_sm_for(size_t smem)
     if (it != g_per_sm.end()) return it->second;
     const auto max_key = std::make_pair(dev, std::make_pair(BLOCK, (size_t)0));
     if (g_per_sm.find(max_key) == g_per_sm.end()) {
-        const int max_smem = 32768 + FA_PRIV_WORDS * BLOCK * 4;
+        const int max_smem = 32768 + FA_SMEM_WORDS * BLOCK * 4;
         if (cudaFuncSetAttribute(fa::fa_run<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem) !=
             cudaSuccess)
             return -1;
@@ -427,7 +436,7 @@ int per_sm_for(size_t smem)
 template <int BLOCK>
 static cudaError_t launch_block(const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
 {
-    const size_t smem = (size_t)L.rom_bytes_max + (size_t)FA_PRIV_WORDS * BLOCK * 4u;
+    const size_t smem = (size_t)L.rom_bytes_max + (size_t)FA_SMEM_WORDS * BLOCK * 4u;
     const int per_sm = per_sm_for<BLOCK>(smem);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     if (sms <= 0) return cudaSuccess;                                  // prepare only
@@ -471,7 +480,7 @@ int warps_per_sm_for(size_t smem)
 template <int WARPS>
 cudaError_t launch_warps(const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
 {
-    const size_t smem = (size_t)L.romlib_bytes + (size_t)WARPS * FA_PRIV_WORDS * 32u * 4u;
+    const size_t smem = (size_t)L.romlib_bytes + (size_t)WARPS * FA_SMEM_WORDS * 32u * 4u;
     const int per_sm = warps_per_sm_for<WARPS>(smem);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     if (sms <= 0) return cudaSuccess;                                  // prepare only
@@ -492,7 +501,6 @@ cudaError_t launch_warps_n(int warps, const FaLaunch& L, bool persistent, int sm
     case 4: return launch_warps<4>(L, persistent, sms, s);
     case 8: return launch_warps<8>(L, persistent, sms, s);
     case 16: return launch_warps<16>(L, persistent, sms, s);
-    case 20: return launch_warps<20>(L, persistent, sms, s);
     case 24: return launch_warps<24>(L, persistent, sms, s);
     case 28: return launch_warps<28>(L, persistent, sms, s);
     case 32: return launch_warps<32>(L, persistent, sms, s);
@@ -530,13 +538,13 @@ cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int 
     FaLaunch L = L_in;
     const uint32_t lib = plan_romlib(L);
     L.romlib_bytes = lib;
-    const uint32_t slab = FA_PRIV_WORDS * 32u * 4u;
+    const uint32_t slab = FA_SMEM_WORDS * 32u * 4u;
     const int fit = (int)((FA_SMEM_PER_CTA_MAX - (int)lib) / (int)slab);
     if (fit >= block / 32) {
         int warps = block / 32;
         if (persistent) {
             // As many warps per CTA as shared memory allows (one CTA per SM).
-            static const int sizes[] = { 32, 28, 24, 20, 16, 8, 4, 2 };
+            static const int sizes[] = { 32, 28, 24, 16, 8, 4, 2 };
             for (int w : sizes)
                 if (w <= fit) { warps = w; break; }
         }
@@ -562,7 +570,7 @@ cudaError_t fa_launch_prepare(const FaLaunch& L, int block, bool persistent)
 
 int fa_launch_occupancy(int block, uint32_t rom_bytes_max)
 {
-    const size_t base = (size_t)rom_bytes_max + (size_t)FA_PRIV_WORDS * block * 4u;
+    const size_t base = (size_t)rom_bytes_max + (size_t)FA_SMEM_WORDS * block * 4u;
     switch (block) {
     case 64: return per_sm_for<64>(base);
     case 128: return per_sm_for<128>(base);

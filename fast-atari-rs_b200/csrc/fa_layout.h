@@ -15,6 +15,10 @@
 
 #define FA_PRIV_BYTES 176
 #define FA_PRIV_WORDS (FA_PRIV_BYTES / 4)
+// The kernel keeps only the RAM words in shared memory; the write-only TIA
+// registers (rows FA_SMEM_WORDS..FA_PRIV_WORDS-1) stay in their HBM rows and
+// are touched there by the rare TIA register writes and collision reads.
+#define FA_SMEM_WORDS 32
 
 // Private-byte offsets: RAM occupies [0, 128).
 enum : uint32_t {
