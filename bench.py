@@ -44,7 +44,7 @@ UNIT = "frames/s"
 # a warp run identical instances (fully converged), from the ncu capture in
 # profiles/fa_run_converged_icount.md.  Used to express guest-instruction
 # throughput in warp-issue slots for the roofline.
-I_CONV = 62.0
+I_CONV = 196.0
 # DRAM bytes moved per instance-frame by fa_run on this workload, from the ncu
 # capture in profiles/fa_run_mixed_ncu.md (None until measured).
 DRAM_BYTES_PER_INSTANCE_FRAME = None

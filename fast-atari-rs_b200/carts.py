@@ -538,13 +538,16 @@ def _bank_asm(spec: CartSpec, b: int, nb: int, rng: Rng, term, groups: int,
     if nb > 1:
         hs = _hotspots(nb)
         if spec.bank_select == "data":
-            asm.ins("LDA", "zp", 0x80 + 2 + (b * 7) % 0x6D)
+            # Always switches, along a path chosen by a RAM bit (the skeleton's
+            # INTIM mix, which depends on each instance's timing); with more
+            # than two banks the target bank depends on that bit too.
+            asm.ins("LDA", "zp", MIX)
             asm.ins("LSR", "acc")
             asm.ins("BCC", "rel", "tr_b")
             asm.ins("BIT", "abs", hs[(b + 1) % nb])
             asm.ins("JMP", "abs", "tr_done")
             asm.label("tr_b")
-            asm.ins("BIT", "abs", hs[(b + nb - 1) % nb] if nb > 2 else hs[b])
+            asm.ins("BIT", "abs", hs[(b + 2) % nb] if nb > 2 else hs[(b + 1) % nb])
             asm.label("tr_done")
         else:
             asm.ins("BIT", "abs", hs[(b + 1) % nb])

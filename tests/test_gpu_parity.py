@@ -264,3 +264,32 @@ def test_large_batch_identical_streams_and_spot_check():
     o_obs, _ = oracle.run_batch(rom, ref, acts[:, idx], k)
     assert np.array_equal(obs[idx], o_obs)
     assert_states_equal(st[idx], ref, "spot check")
+
+
+# ---------------------------------------------------------------- committed golden vectors
+def _golden():
+    import json
+    from pathlib import Path
+    return json.loads((Path(__file__).parent / "golden" / "oracle_vectors.json").read_text())
+
+
+@pytest.mark.parametrize("name", ALL_CARTS)
+def test_matches_committed_golden_vectors(name):
+    """The CUDA path reproduces the frozen oracle vectors (tests/golden/) without
+    running the oracle: RAM at checkpoint frames and the full final state."""
+    import hashlib
+    want = _golden()[name]
+    rom = cart(name)
+    assert hashlib.sha256(rom).hexdigest() == want["rom_sha256"]
+    n, frames = want["n"], want["frames"]
+    acts = carts.actions(seed=want["action_seed"], n=n, frames=frames)
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.reset()
+        assert hashlib.sha256(g.download_states()[:1].tobytes()).hexdigest() == want["reset_state_sha256"]
+        done = 0
+        for f_end in sorted(int(x) for x in want["ram_sha256_at"]):
+            obs = g.step_multi(acts[done:f_end], f_end - done)
+            done = f_end
+            assert hashlib.sha256(obs.tobytes()).hexdigest() == want["ram_sha256_at"][str(f_end)], f_end
+        st = g.download_states()
+    assert hashlib.sha256(st.tobytes()).hexdigest() == want["final_state_sha256"]
