@@ -105,6 +105,7 @@ _SIGS = {
     "fa_pool_graph_create": (_i, [_vp, _vp, _i, _i, _vp, ctypes.POINTER(_vp)]),
     "fa_graph_launch": (_i, [_vp, _vp]),
     "fa_graph_destroy": (None, [_vp]),
+    "fa_step_static": (_i, [_vp, _i, _vp, _u32, _u32, _vp, _i, _i, _vp, _i, _vp]),
 }
 
 _lib: Optional[ctypes.CDLL] = None

@@ -13,6 +13,8 @@
 #define FA_DEVERR_TMA_TIMEOUT 0x1u
 
 #define FA_MAX_GROUPS 16
+// Calls one fa_step_static may chain (one queue counter each in its fixed scratch).
+#define FA_STATIC_MAX_CALLS 1024
 // Dynamic shared memory a CTA may use (227 KiB opt-in limit minus the static
 // barrier word and headroom).
 #define FA_SMEM_PER_CTA_MAX (227 * 1024 - 1024)

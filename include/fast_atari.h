@@ -288,6 +288,29 @@ int  fa_pool_graph_create(fa_pool* p, const uint8_t* const* d_actions, int k, in
 int  fa_graph_launch(fa_graph* g, void* stream);
 void fa_graph_destroy(fa_graph* g);
 
+/* -------------------------------------------------- no-allocation stepping
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (device memory owned by another allocator, or a stepping loop that must not
+ * trigger cudaMalloc's implicit device synchronisation): runs `calls`
+ * consecutive batched steps of k frames over caller-owned buffers and
+ * allocates nothing.
+ *   d_rom_image  nbanks * 4096 bytes, 16-byte aligned (Fixed carts as their
+ *                mirrored 4 KiB window, banked carts as-is)
+ *   d_state      the FA SoA state rows (fa_device_state layout), stride >= n
+ *   d_actions    calls * k * n bytes; call c uses the slice at c * k * n
+ *   d_obs        n * 128 bytes (16-byte aligned) or NULL; gets each call's RAM
+ * The kernel's scratch (one work-queue counter per call, error word,
+ * counters) is a fixed array compiled into the library, present on every GPU
+ * that loads it: calls is limited to 1..1024 (FA_ERR_CAPACITY beyond).  The
+ * first call on a device looks up that array's device address, so make it
+ * before any stream capture.  Every call shares the array: calls that overlap
+ * on the GPU (other streams, other threads) race and must not be issued.
+ * Blocks until the steps finish and reports device-side errors.
+ */
+int fa_step_static(const uint8_t* d_rom_image, int scheme, uint32_t* d_state, uint32_t stride,
+                   uint32_t n, const uint8_t* d_actions, int k, int calls, uint8_t* d_obs,
+                   int sched, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
