@@ -75,6 +75,11 @@ def workload(name: str, carts):
     if name == "plain":
         return ("plain 4K Fixed cart, 1000 instances, per-frame step (K=1)",
                 [(carts.plain_cart(), 1000)], 1, 0)
+    if name == "converged":
+        # Calibration: identical instances and actions, so every warp runs
+        # fully converged (the instruction cost per guest instruction).
+        return ("converged calibration: plain 4K Fixed cart, 151552 identical instances, "
+                "all actions 0, K=2", [(carts.plain_cart(), 151_552)], 2, 0)
     if name == "scale":
         return ("scale: 1000000 instances of the 32K F4 cart, K=16, reset every 2000 frames",
                 [(carts.scale_cart(), 1_000_000)], 16, 2000)
@@ -213,6 +218,10 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
     for gi, (c, n) in enumerate(spec):
         t = torch.empty(calls * k * n, dtype=torch.uint8, device=dev)
         chunk = max(1, (64 << 20) // max(1, k * n))
+        if args.workload == "converged":
+            t.zero_()
+            d_act.append(t)
+            continue
         for c0 in range(0, calls, chunk):
             c1 = min(calls, c0 + chunk)
             a = carts.actions(seed=1000 * rank + 17 * gi + 1, n=n, frames=(c1 - c0) * k, frame0=c0 * k)
@@ -270,12 +279,14 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
     value = frames / (total_ms / 1e3)
 
     # ---- the plain kernel on the same trace (one launch per frame per cart)
-    plain_steps = max(3, min(args.steps, 20))
-    pool.step_plain_async(acts_at(0), k, obs_ptrs, sptr)
-    pool.synchronize()
-    barrier()
-    ms_plain = timed_calls(pool.step_plain_async, args.warmup, plain_steps)
-    plain_value = n_total * k * plain_steps / (sum(ms_plain) / 1e3)
+    plain_value = None
+    if not args.no_plain:
+        plain_steps = max(3, min(args.steps, 20))
+        pool.step_plain_async(acts_at(0), k, obs_ptrs, sptr)
+        pool.synchronize()
+        barrier()
+        ms_plain = timed_calls(pool.step_plain_async, args.warmup, min(plain_steps, args.steps))
+        plain_value = n_total * k * len(ms_plain) / (sum(ms_plain) / 1e3)
 
     # ---- the whole timed trace as one CUDA graph (no flushes between calls)
     graph_value = None
@@ -295,17 +306,18 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
         graph.close()
 
     # ---- end to end through the public API with host buffers
-    e2e_steps = max(3, min(args.steps, 30))
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 30))
     host_acts = [[np.ascontiguousarray(d_act[gi][(args.warmup + i) * k * n:(args.warmup + i + 1) * k * n].cpu().numpy())
                   for gi, (_, n) in enumerate(spec)] for i in range(e2e_steps)]
-    pool.step(host_acts[0], k, obs=True)
-    barrier()
-    t0 = time.perf_counter()
-    for i in range(e2e_steps):
-        obs = pool.step(host_acts[i], k, obs=True)
-    e2e_s = time.perf_counter() - t0
-    del obs
-    e2e_value = n_total * k * e2e_steps * world / e2e_s
+    e2e_value = None
+    if e2e_steps:
+        pool.step(host_acts[0], k, obs=True)
+        barrier()
+        t0 = time.perf_counter()
+        for i in range(e2e_steps):
+            pool.step(host_acts[i], k, obs=True)
+        e2e_s = time.perf_counter() - t0
+        e2e_value = n_total * k * e2e_steps * world / e2e_s
     h2d = n_total * k
     d2h = n_total * 128
 
@@ -334,12 +346,13 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
         "roofline": {"bound": "issue", "achieved": achieved / 1e12, "peak": peak / 1e12,
                      "unit": "T warp-inst/s", "frac": achieved / peak, "traffic": traffic,
                      "note": f"guest 6502 instr/s x {I_CONV} SASS thread-instr per guest instr (converged) / 32"},
-        "plain_kernel": {"value": plain_value, "unit": UNIT, "steps": plain_steps,
-                         "form": "one launch per frame per cart"},
-        "batched_vs_plain": value / plain_value,
+        "plain_kernel": {"value": plain_value, "unit": UNIT,
+                         "form": "one launch per frame per cart"} if plain_value else None,
+        "batched_vs_plain": value / plain_value if plain_value else None,
         "graph": {"value": graph_value, "unit": UNIT, "calls": args.steps} if graph_value else None,
         "step_latency_ms": {"p50": p(0.5), "p99": p(0.99), "max": lat[-1]},
         "guest_instructions_per_s": guest_per_s,
+        "guest_instructions_per_step": instr / args.steps,
         "lane_efficiency": instr / slots if slots else None,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -357,10 +370,12 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mixed", choices=["mixed", "divergence", "plain", "scale"])
+    ap.add_argument("--workload", default="mixed", choices=["mixed", "divergence", "plain", "scale", "converged"])
     ap.add_argument("--block", type=int, default=128)
     ap.add_argument("--tuning", default=None, help="JSON file of per-cart tuning records")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
