@@ -372,9 +372,11 @@ __global__ void __launch_bounds__(WARPS * 32) fa_run_warps(const __grid_constant
         return;
     }
     for (uint32_t round = 0;; round++) {
+        // First wave: unit warp*grid + cta, so consecutive (heaviest-first)
+        // units land on different SMs; after that the device queue.
         uint32_t u = 0;
         if (lane == 0) {
-            if (L.queue) u = atomicAdd(L.queue, 1u);
+            if (L.queue) u = round == 0 ? warp * gridDim.x + blockIdx.x : gridDim.x * WARPS + atomicAdd(L.queue, 1u);
             else u = round == 0 ? blockIdx.x * WARPS + warp : 0xFFFFFFFFu;
         }
         u = __shfl_sync(FULL, u, 0);
@@ -486,8 +488,10 @@ cudaError_t launch_warps(const FaLaunch& L, bool persistent, int sms, cudaStream
     if (sms <= 0) return cudaSuccess;                                  // prepare only
     uint32_t grid = (L.nunits + WARPS - 1) / WARPS;
     if (persistent) {
+        // One CTA per resident slot on every SM (fewer only if there are fewer
+        // units than slots), so no SM idles while units remain.
         const uint32_t cap = (uint32_t)(per_sm * sms);
-        grid = grid < cap ? grid : cap;
+        grid = L.nunits < cap ? L.nunits : cap;
     }
     if (grid == 0) return cudaSuccess;
     fa::fa_run_warps<WARPS><<<grid, WARPS * 32, smem, s>>>(L);
