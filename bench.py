@@ -42,12 +42,13 @@ UNIT = "frames/s"
 
 # SASS thread-instructions per emulated 6502 instruction when all 32 lanes of
 # a warp run identical instances (fully converged), from the ncu capture in
-# profiles/fa_run_converged_icount.md.  Used to express guest-instruction
+# profiles/fa_run_warps_converged_plain.md.  Used to express guest-instruction
 # throughput in warp-issue slots for the roofline.
-I_CONV = 196.0
+I_CONV = 197.0
 # DRAM bytes moved per instance-frame by fa_run on this workload, from the ncu
-# capture in profiles/fa_run_mixed_ncu.md (None until measured).
-DRAM_BYTES_PER_INSTANCE_FRAME = None
+# capture in profiles/fa_run_warps_mixed_batch_full.md (27.4 MB per 4-frame
+# call of 135,500 instances).
+DRAM_BYTES_PER_INSTANCE_FRAME = 50.6
 
 
 def load_pkg():
