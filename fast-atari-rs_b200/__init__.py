@@ -106,7 +106,21 @@ _SIGS = {
     "fa_graph_launch": (_i, [_vp, _vp]),
     "fa_graph_destroy": (None, [_vp]),
     "fa_step_static": (_i, [_vp, _i, _vp, _u32, _u32, _vp, _i, _i, _vp, _i, _vp]),
+    "fa_set_cta_warps": (_i, [_vp, _i]),
+    "fa_pool_set_cta_warps": (_i, [_vp, _i]),
+    "fa_autotune": (_i, [_u8p, _sz, _sz, _vp, _vp, _i, ctypes.POINTER(_i)]),
+    "fa_obs_to_unit_f32": (_i, [_vp, _vp, _sz, _vp]),
 }
+
+
+class FaTuning(ctypes.Structure):
+    """fa_tuning (include/fast_atari.h)."""
+    _fields_ = [("block", ctypes.c_int), ("persistent", ctypes.c_int), ("cta_warps", ctypes.c_int),
+                ("sched", ctypes.c_int), ("k", ctypes.c_int), ("frames_per_s", ctypes.c_float),
+                ("ns_per_instance_frame", ctypes.c_float)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 _lib: Optional[ctypes.CDLL] = None
 
@@ -241,9 +255,10 @@ class BatchAtariGpu:
         assert f.size == self.n
         _check(lib().fa_set_frame_numbers(self._h, f.ctypes.data_as(ctypes.POINTER(_u32))))
 
-    def set_launch(self, block: int = 128, sched="lane", persistent: bool = False) -> None:
+    def set_launch(self, block: int = 128, sched="lane", persistent: bool = False, cta_warps: int = 0) -> None:
         s = SCHED_NAMES[sched] if isinstance(sched, str) else int(sched)
         _check(lib().fa_set_launch(self._h, int(block), s, 1 if persistent else 0))
+        _check(lib().fa_set_cta_warps(self._h, int(cta_warps)))
 
     def get_launch(self):
         b, s, p = _i(), _i(), _i()
@@ -311,8 +326,9 @@ class AtariPool:
         s = SCHED_NAMES[sched] if isinstance(sched, str) else int(sched)
         _check(lib().fa_pool_set_group(self._p, g, s, float(weight)))
 
-    def set_launch(self, block: int = 128, persistent: bool = True) -> None:
+    def set_launch(self, block: int = 128, persistent: bool = True, cta_warps: int = 0) -> None:
         _check(lib().fa_pool_set_launch(self._p, int(block), 1 if persistent else 0))
+        _check(lib().fa_pool_set_cta_warps(self._p, int(cta_warps)))
 
     def _host_step(self, fn, actions, k, obs):
         acts = [np.ascontiguousarray(a, dtype=np.uint8).reshape(-1) for a in actions]
@@ -375,3 +391,13 @@ class PoolGraph:
 
     def __del__(self):
         self.close()
+
+
+def autotune(rom: bytes, n: int):
+    """Run the project tuner for one cart; returns (best, table) as dicts."""
+    r = np.frombuffer(bytes(rom), dtype=np.uint8).copy()
+    best = FaTuning()
+    table = (FaTuning * 64)()
+    count = _i()
+    _check(lib().fa_autotune(_u8(r), len(r), int(n), ctypes.byref(best), table, 64, ctypes.byref(count)))
+    return best.as_dict(), [table[i].as_dict() for i in range(min(count.value, 64))]

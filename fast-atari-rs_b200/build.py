@@ -18,7 +18,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "lib" / "libfast_atari.so"
-SOURCES = ["fa_kernels.cu", "fa_api.cu", "fa_pool.cu", "fa_noalloc.cu"]
+SOURCES = ["fa_kernels.cu", "fa_api.cu", "fa_pool.cu", "fa_noalloc.cu", "fa_autotune.cu", "fa_env.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-I", str(ROOT / "include")]
 

@@ -320,6 +320,7 @@ static int enqueue_run(fa_handle* h, const FaGroup& g, cudaStream_t s)
     L.err = h->d_err;
     L.instr = h->d_instr;
     L.rounds = h->d_instr + 1;
+    L.cta_warps = (uint32_t)h->cta_warps;
     if (h->persistent) {
         L.queue = h->d_err + 1;
         FA_CUDA(cudaMemsetAsync(L.queue, 0, sizeof(uint32_t), s));
@@ -498,6 +499,16 @@ extern "C" int fa_set_launch(fa_handle* h, int block, int sched, int persistent)
     h->block = block;
     h->sched = sched;
     h->persistent = persistent != 0;
+    return FA_OK;
+}
+
+extern "C" int fa_set_cta_warps(fa_handle* h, int warps)
+{
+    if (!h) return fa_fail(FA_ERR_INVALID, "null handle");
+    if (warps != 0 && warps != 2 && warps != 4 && warps != 8 && warps != 16 && warps != 24 && warps != 28 &&
+        warps != 32)
+        return fa_fail(FA_ERR_INVALID, "warps per CTA must be 0 (auto), 2, 4, 8, 16, 24, 28 or 32");
+    h->cta_warps = warps;
     return FA_OK;
 }
 

@@ -42,6 +42,7 @@ struct FaLaunch {
     uint32_t nunits;
     uint32_t rom_bytes_max;      // shared-memory ROM bytes reserved per CTA (CTA-granular form)
     uint32_t romlib_bytes;       // all ROMs of the launch (warp-granular form, set by fa_launch_run)
+    uint32_t cta_warps;          // persistent form: warps per CTA cap (0 = as many as fit)
     uint32_t* queue;             // work-queue counter (persistent form) or null
     uint32_t* err;               // device error word
     unsigned long long* instr;   // guest-instruction counter, or null
@@ -96,6 +97,7 @@ struct fa_handle {
     int block = 128;
     int sched = FA_SCHED_PC;
     bool persistent = false;
+    int cta_warps = 0;                 // persistent form: warps per CTA (0 = as many as fit)
     uint32_t episode_frames = 0;
     unsigned long long last_instr = 0;
     unsigned long long last_slots = 0;

@@ -547,10 +547,13 @@ cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int 
     if (fit >= block / 32) {
         int warps = block / 32;
         if (persistent) {
-            // As many warps per CTA as shared memory allows (one CTA per SM).
+            // As many warps per CTA as shared memory allows (one CTA per SM),
+            // or fewer when a cap is set (the register budget per thread grows
+            // as 65536 / (32 x warps)).
+            const int cap = L.cta_warps ? (int)L.cta_warps : 32;
             static const int sizes[] = { 32, 28, 24, 16, 8, 4, 2 };
             for (int w : sizes)
-                if (w <= fit) { warps = w; break; }
+                if (w <= fit && w <= cap) { warps = w; break; }
         }
         plan_units(L, 32u);
         return launch_warps_n(warps, L, persistent, sms, s);

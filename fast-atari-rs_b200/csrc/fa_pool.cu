@@ -26,6 +26,7 @@ struct fa_pool {
     std::vector<float> weight;         // relative cost of one unit; heavier units are queued first
     int block = 128;
     bool persistent = true;
+    int cta_warps = 0;
     cudaStream_t stream = nullptr;
     uint32_t* d_err = nullptr;         // device error word
     uint32_t* d_queue = nullptr;       // one work-queue counter per call
@@ -127,6 +128,16 @@ extern "C" int fa_pool_set_launch(fa_pool* p, int block, int persistent)
     return FA_OK;
 }
 
+extern "C" int fa_pool_set_cta_warps(fa_pool* p, int warps)
+{
+    if (!p) return fa_fail(FA_ERR_INVALID, "null pool");
+    if (warps != 0 && warps != 2 && warps != 4 && warps != 8 && warps != 16 && warps != 24 && warps != 28 &&
+        warps != 32)
+        return fa_fail(FA_ERR_INVALID, "warps per CTA must be 0 (auto), 2, 4, 8, 16, 24, 28 or 32");
+    p->cta_warps = warps;
+    return FA_OK;
+}
+
 static int ensure_queues(fa_pool* p, uint32_t calls)
 {
     if (calls <= p->queue_cap) return FA_OK;
@@ -158,6 +169,7 @@ static int build_launch(fa_pool* p, const uint8_t* const* d_actions, uint32_t k,
     }
     L.nunits = units;
     L.rom_bytes_max = rom_max;
+    L.cta_warps = (uint32_t)p->cta_warps;
     L.err = p->d_err;
     L.instr = p->d_ctr;
     L.rounds = p->d_ctr + 1;

@@ -1,0 +1,99 @@
+"""BatchAtariGpuEnv: the reference's batched RL caller on the B200 core.
+
+Mirrors src/rl4burn_env.rs:269-380: N parallel instances of one ROM, a single
+discrete action broadcast to all of them, frameskip (action repeat, default 4)
+through step_multi, truncation after max_steps (default 108,000), reward 0 and
+terminated false (the reference extracts no reward).  Observations are the
+N x 128 RAM bytes as f32 / 255, flattened to N*128 — produced on the device
+into a torch CUDA tensor (fa_obs_to_unit_f32) instead of on the host.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import BatchAtariGpu, _check, _vp, lib
+
+NUM_ACTIONS = 18            # src/rl4burn_env.rs:26
+DEFAULT_MAX_STEPS = 108_000  # :29
+DEFAULT_FRAMESKIP = 4        # :32
+
+
+@dataclass
+class Step:
+    observation: "object"    # torch.Tensor, float32, shape (N*128,), on the device
+    reward: float
+    terminated: bool
+    truncated: bool
+
+
+class BatchAtariGpuEnv:
+    def __init__(self, rom: bytes, n: int, device: int = 0):
+        import torch
+        self.torch = torch
+        self.device = torch.device("cuda", device)
+        self.gpu = BatchAtariGpu(rom, n)
+        self.rom = bytes(rom)
+        self.n = int(n)
+        self.step_count = 0
+        self.max_steps = DEFAULT_MAX_STEPS
+        self.frameskip = DEFAULT_FRAMESKIP
+        self._actions = torch.zeros(self.n * 64, dtype=torch.uint8, device=self.device)
+        self._obs_u8 = torch.zeros(self.n * 128, dtype=torch.uint8, device=self.device)
+        self._obs = torch.zeros(self.n * 128, dtype=torch.float32, device=self.device)
+
+    # builder methods (src/rl4burn_env.rs:298-313)
+    def with_max_steps(self, max_steps: int) -> "BatchAtariGpuEnv":
+        self.max_steps = int(max_steps)
+        return self
+
+    def with_frameskip(self, frameskip: int) -> "BatchAtariGpuEnv":
+        if frameskip < 1:
+            raise ValueError("frameskip must be >= 1")
+        self.frameskip = int(frameskip)
+        if self.frameskip * self.n > self._actions.numel():
+            self._actions = self.torch.zeros(self.frameskip * self.n, dtype=self.torch.uint8, device=self.device)
+        return self
+
+    def with_sorted(self, sorted_: bool) -> "BatchAtariGpuEnv":
+        self.gpu.set_sorted(sorted_)
+        return self
+
+    def num_envs(self) -> int:
+        return self.n
+
+    def observation_space(self):
+        return ("Box", 0.0, 1.0, self.n * 128)
+
+    def action_space(self):
+        return ("Discrete", NUM_ACTIONS)
+
+    def _normalise(self):
+        stream = self.torch.cuda.current_stream(self.device).cuda_stream
+        _check(lib().fa_obs_to_unit_f32(_vp(self._obs_u8.data_ptr()), _vp(self._obs.data_ptr()),
+                                         self._obs.numel(), _vp(stream or None)))
+        return self._obs
+
+    def reset(self):
+        """src/rl4burn_env.rs:331-338: step counter 0, RAM after reset."""
+        self.step_count = 0
+        ram = self.gpu.reset()
+        self._obs_u8.copy_(self.torch.from_numpy(np.ascontiguousarray(ram).reshape(-1)))
+        return self._normalise().clone()
+
+    def step(self, action: int) -> Step:
+        """src/rl4burn_env.rs:340-367: broadcast, frameskip, truncation."""
+        k = self.frameskip
+        acts = self._actions[: k * self.n]
+        acts.fill_(int(action) & 0xFF)
+        self.torch.cuda.current_stream(self.device).synchronize()
+        self.gpu.step_multi_async(acts.data_ptr(), k, self._obs_u8.data_ptr())
+        self.gpu.synchronize()
+        obs = self._normalise().clone()
+        self.step_count += 1
+        truncated = self.max_steps > 0 and self.step_count >= self.max_steps
+        return Step(obs, 0.0, False, truncated)
+
+    def close(self):
+        self.gpu.close()

@@ -225,6 +225,11 @@ int fa_set_frame_numbers(fa_handle* h, const uint32_t* frame_no);
 int fa_set_launch(fa_handle* h, int block, int sched, int persistent);
 int fa_get_launch(const fa_handle* h, int* block, int* sched, int* persistent);
 
+/* Persistent form only: warps per CTA (0 = as many as shared memory fits;
+ * else 2, 4, 8, 16, 24, 28 or 32).  Fewer warps raise the register budget per
+ * thread (65536 / (32 x warps)). */
+int fa_set_cta_warps(fa_handle* h, int warps);
+
 /* Guest (6502) instructions executed by the handle's last synchronous call. */
 unsigned long long fa_last_instructions(const fa_handle* h);
 
@@ -261,6 +266,7 @@ fa_handle* fa_pool_group(fa_pool* p, int group);
 /* Per-cart warp policy and relative cost of one of its units (queue order). */
 int  fa_pool_set_group(fa_pool* p, int group, int sched, float weight);
 int  fa_pool_set_launch(fa_pool* p, int block, int persistent);
+int  fa_pool_set_cta_warps(fa_pool* p, int warps);
 /* Synchronous steps from host buffers: batched (one launch for all carts)
  * and plain (one launch per frame per cart, the reference's form). */
 int  fa_pool_step(fa_pool* p, const uint8_t* const* actions, int k, uint8_t* const* obs);
@@ -287,6 +293,32 @@ int  fa_pool_graph_create(fa_pool* p, const uint8_t* const* d_actions, int k, in
                           uint8_t* const* d_obs, fa_graph** out);
 int  fa_graph_launch(fa_graph* g, void* stream);
 void fa_graph_destroy(fa_graph* g);
+
+/* Observation bytes -> f32 in [0, 1] (b / 255, IEEE single division), on the
+ * device: BatchAtariGpuEnv's RAM observation (src/rl4burn_env.rs:320-322)
+ * written into a caller buffer of `count` floats, enqueued on `stream`. */
+int fa_obs_to_unit_f32(const uint8_t* d_obs, float* d_out, size_t count, void* stream);
+
+/* ---------------------------------------------------------------- autotuning
+ * Project-written tuner (no reference counterpart; the reference hard-codes
+ * 128-thread blocks and a manual set_sorted).  For one ROM and n instances it
+ * times, on the current device, the warp policy, then the launch shape
+ * (persistent CTAs of 8..32 warps = register caps of 256..64 per thread, or
+ * the plain form with 64..512-thread CTAs), then the frames per launch K, and
+ * returns the fastest record.  All configurations give identical results.
+ */
+typedef struct fa_tuning {
+    int   block;                  /* CTA size of the plain form */
+    int   persistent;             /* 1: persistent form */
+    int   cta_warps;              /* persistent form: warps per CTA (0 = auto) */
+    int   sched;                  /* FA_SCHED_* */
+    int   k;                      /* frames per launch */
+    float frames_per_s;           /* measured */
+    float ns_per_instance_frame;  /* measured cost; a pool's queue weight */
+} fa_tuning;
+
+int fa_autotune(const uint8_t* rom, size_t rom_len, size_t n, fa_tuning* best,
+                fa_tuning* table, int table_cap, int* table_len);
 
 /* -------------------------------------------------- no-allocation stepping
  * No counterpart in the reference.  For callers that cannot call cudaMalloc

