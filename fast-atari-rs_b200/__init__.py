@@ -110,7 +110,22 @@ _SIGS = {
     "fa_pool_set_cta_warps": (_i, [_vp, _i]),
     "fa_autotune": (_i, [_u8p, _sz, _sz, _vp, _vp, _i, ctypes.POINTER(_i)]),
     "fa_obs_to_unit_f32": (_i, [_vp, _vp, _sz, _vp]),
+    "fa_server_create": (_i, [_vp, _vp, _i, _vp, ctypes.POINTER(_vp)]),
+    "fa_server_destroy": (None, [_vp]),
+    "fa_server_open": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_int64)]),
+    "fa_server_close": (_i, [_vp, ctypes.c_int64]),
+    "fa_server_submit": (_i, [_vp, ctypes.c_int64, _vp, _u32, _i, _vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "fa_server_wait": (_i, [_vp, ctypes.c_uint64, _i, _vp]),
+    "fa_server_step": (_i, [_vp, ctypes.c_int64, _vp, _u32, _i, _vp, _vp]),
+    "fa_server_session_size": (_i, [_vp, ctypes.c_int64, ctypes.POINTER(_u32)]),
+    "fa_server_get_states": (_i, [_vp, ctypes.c_int64, _u32, _u32, _vp]),
+    "fa_server_stats_get": (_i, [_vp, _vp]),
+    "fa_server_loadgen": (_i, [_vp, _vp, _vp, _vp]),
 }
+
+FA_ERR_CAPACITY = -6
+FA_ERR_TIMEOUT = -7
+SERVE_BATCHED, SERVE_PLAIN = 0, 1
 
 
 class FaTuning(ctypes.Structure):
@@ -401,3 +416,148 @@ def autotune(rom: bytes, n: int):
     count = _i()
     _check(lib().fa_autotune(_u8(r), len(r), int(n), ctypes.byref(best), table, 64, ctypes.byref(count)))
     return best.as_dict(), [table[i].as_dict() for i in range(min(count.value, 64))]
+
+
+# ------------------------------------------------------------------ serving
+class ServerConfig(ctypes.Structure):
+    """fa_server_config (include/fast_atari.h)."""
+    _fields_ = [("state_budget_bytes", ctypes.c_size_t), ("mode", ctypes.c_int), ("block", ctypes.c_int),
+                ("max_inflight", ctypes.c_int), ("sched", ctypes.c_int)]
+
+
+class RequestInfo(ctypes.Structure):
+    """fa_request_info (include/fast_atari.h)."""
+    _fields_ = [("status", ctypes.c_int), ("waited_admission", ctypes.c_int), ("batch_requests", ctypes.c_uint),
+                ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class ServerStats(ctypes.Structure):
+    """fa_server_stats (include/fast_atari.h)."""
+    _fields_ = [(n, ctypes.c_ulonglong) for n in (
+        "requests_submitted", "requests_done", "requests_failed", "instance_frames", "dispatches",
+        "dispatched_requests", "launches", "admission_waits", "guest_instructions", "lane_slots")] + \
+        [("sessions_open", ctypes.c_longlong), ("state_bytes_in_use", ctypes.c_size_t),
+         ("state_bytes_peak", ctypes.c_size_t), ("state_budget_bytes", ctypes.c_size_t)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class LoadgenConfig(ctypes.Structure):
+    """fa_loadgen_config (include/fast_atari.h)."""
+    _fields_ = [("clients", ctypes.c_int), ("requests", ctypes.c_int), ("offered_frames_per_s", ctypes.c_double),
+                ("seed", ctypes.c_uint64), ("batch_median", ctypes.c_uint32), ("batch_min", ctypes.c_uint32),
+                ("batch_max", ctypes.c_uint32), ("batch_sigma", ctypes.c_double), ("k_min", ctypes.c_int),
+                ("k_max", ctypes.c_int)]
+
+
+class LoadgenResult(ctypes.Structure):
+    """fa_loadgen_result (include/fast_atari.h)."""
+    _fields_ = [("requests", ctypes.c_ulonglong), ("admission_waits", ctypes.c_ulonglong)] + \
+        [(n, ctypes.c_double) for n in (
+            "instance_frames", "elapsed_s", "frames_per_s", "offered_frames_per_s", "arrival_window_s",
+            "p50_ms", "p90_ms", "p99_ms", "max_ms", "mean_ms", "mean_queue_ms", "mean_batch_requests")] + \
+        [("errors", ctypes.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class AtariServer:
+    """Continuous-batching server over several carts (fa_server_*).
+
+    Sessions are instance sets of one cart resident in HBM; `submit` queues a
+    step of instances [0, n) of a session for k frames and returns a ticket,
+    `wait` returns that request's observations (n x 128 RAM bytes) and timing.
+    Thread-safe: ctypes releases the GIL, so clients on several Python threads
+    overlap.
+    """
+
+    def __init__(self, roms, mode: str = "batched", state_budget_bytes: int = 0, block: int = 0,
+                 max_inflight: int = 0, sched="pc"):
+        self.roms = [np.frombuffer(bytes(r), dtype=np.uint8).copy() for r in roms]
+        cfg = ServerConfig(int(state_budget_bytes), SERVE_PLAIN if mode == "plain" else SERVE_BATCHED,
+                           int(block), int(max_inflight), SCHED_NAMES[sched] if isinstance(sched, str) else int(sched))
+        ptrs = (_vp * len(self.roms))(*[r.ctypes.data for r in self.roms])
+        lens = (ctypes.c_size_t * len(self.roms))(*[len(r) for r in self.roms])
+        h = _vp()
+        _check(lib().fa_server_create(ptrs, lens, len(self.roms), ctypes.byref(cfg), ctypes.byref(h)))
+        self._s = h
+        self._held = {}           # ticket -> (actions, obs) kept alive until waited
+
+    def close(self) -> None:
+        if getattr(self, "_s", None):
+            lib().fa_server_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def open(self, cart: int) -> int:
+        sid = ctypes.c_int64()
+        _check(lib().fa_server_open(self._s, int(cart), ctypes.byref(sid)))
+        return sid.value
+
+    def close_session(self, session: int) -> None:
+        _check(lib().fa_server_close(self._s, int(session)))
+
+    def submit(self, session: int, actions, n: int, k: int, obs: bool = True) -> int:
+        a = np.ascontiguousarray(actions, dtype=np.uint8).reshape(-1)
+        if a.size != n * k:
+            raise ValueError("actions must hold k * n bytes")
+        out = np.empty((n, 128), np.uint8) if obs else None
+        t = ctypes.c_uint64()
+        _check(lib().fa_server_submit(self._s, int(session), a.ctypes.data, int(n), int(k),
+                                      out.ctypes.data if obs else None, ctypes.byref(t)))
+        self._held[t.value] = (a, out)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """(observations or None, info dict); raises FaError on failure."""
+        info = RequestInfo()
+        rc = lib().fa_server_wait(self._s, ctypes.c_uint64(ticket), int(timeout_ms), ctypes.byref(info))
+        if rc == FA_ERR_TIMEOUT:
+            raise FaError(rc, lib().fa_last_error().decode())
+        _, out = self._held.pop(ticket, (None, None))
+        _check(rc)
+        return out, info.as_dict()
+
+    def step(self, session: int, actions, n: int, k: int):
+        return self.wait(self.submit(session, actions, n, k))
+
+    def session_size(self, session: int) -> int:
+        v = _u32()
+        _check(lib().fa_server_session_size(self._s, int(session), ctypes.byref(v)))
+        return v.value
+
+    def states(self, session: int, first: int = 0, count: Optional[int] = None) -> np.ndarray:
+        if count is None:
+            count = self.session_size(session) - first
+        out = np.zeros(count, dtype=STATE_DTYPE)
+        _check(lib().fa_server_get_states(self._s, int(session), int(first), int(count), out.ctypes.data))
+        return out
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().fa_server_stats_get(self._s, ctypes.byref(st)))
+        return st.as_dict()
+
+    def loadgen(self, requests: int, offered_frames_per_s: float, clients: int = 64, seed: int = 1,
+                batch_median: int = 256, batch_min: int = 16, batch_max: int = 16384, batch_sigma: float = 1.0,
+                k_min: int = 1, k_max: int = 8):
+        """Run the simulated actor clients; returns (result dict, latencies ms)."""
+        cfg = LoadgenConfig(int(clients), int(requests), float(offered_frames_per_s), int(seed), int(batch_median),
+                            int(batch_min), int(batch_max), float(batch_sigma), int(k_min), int(k_max))
+        res = LoadgenResult()
+        lat = np.zeros(int(requests), np.float32)
+        _check(lib().fa_server_loadgen(self._s, ctypes.byref(cfg), ctypes.byref(res), lat.ctypes.data))
+        return res.as_dict(), lat

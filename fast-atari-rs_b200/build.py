@@ -18,7 +18,11 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "lib" / "libfast_atari.so"
-SOURCES = ["fa_kernels.cu", "fa_api.cu", "fa_pool.cu", "fa_noalloc.cu", "fa_autotune.cu", "fa_env.cu"]
+SOURCES = ["fa_kernels.cu", "fa_api.cu", "fa_pool.cu", "fa_noalloc.cu", "fa_autotune.cu", "fa_env.cu", "fa_serve.cu",
+           "fa_serve_kernel.cu"]
+# The serving kernel reads state rows that a concurrently running launch may
+# have written: its global loads are cached in L2 only (the coherence point).
+EXTRA = {"fa_serve_kernel.cu": ["-Xptxas", "-dlcm=cg"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-I", str(ROOT / "include")]
 
@@ -43,7 +47,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
 
     def compile_one(src: str) -> Path:
         out = OBJ / (Path(src).stem + ".o")
-        cmd = [nvcc, *ARCH, *FLAGS, "-c", str(CSRC / src), "-o", str(out)]
+        cmd = [nvcc, *ARCH, *FLAGS, *EXTRA.get(src, []), "-c", str(CSRC / src), "-o", str(out)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -34,7 +34,7 @@ constexpr uint32_t act_word(int up, int down, int left, int right, int fire)
 }
 
 // Action::decode order (src/atari.rs:59-80): up, down, left, right, fire.
-__constant__ uint32_t c_action_table[18] = {
+static __constant__ uint32_t c_action_table[18] = {
     act_word(0, 0, 0, 0, 0), act_word(0, 0, 0, 0, 1), act_word(1, 0, 0, 0, 0), act_word(0, 0, 0, 1, 0),
     act_word(0, 0, 1, 0, 0), act_word(0, 1, 0, 0, 0), act_word(1, 0, 0, 1, 0), act_word(1, 0, 1, 0, 0),
     act_word(0, 1, 0, 1, 0), act_word(0, 1, 1, 0, 0), act_word(1, 0, 0, 0, 1), act_word(0, 0, 0, 1, 1),
@@ -43,7 +43,7 @@ __constant__ uint32_t c_action_table[18] = {
 };
 
 // Bit op of word op>>5 is set for the 151 legal opcodes (src/cpu.rs:253-1141).
-__constant__ uint32_t c_legal[8] = {
+static __constant__ uint32_t c_legal[8] = {
     0x63636763u, 0x63637773u, 0x63637763u, 0x63637763u,
     0x27737572u, 0x77737777u, 0x63637773u, 0x63637773u,
 };
@@ -67,7 +67,7 @@ __device__ __forceinline__ uint32_t cold_off(uint32_t o, uint32_t stride4) { ret
 // TIA or PIA register read (HeadlessTia::read, src/headless_tia.rs:205-223;
 // Pia::read I/O half, src/pia.rs:169-199).  Bit 8 of the result asks the
 // caller to clear the timer underflow flag (an INTIM read).
-__device__ __noinline__ uint32_t io_read(uint32_t a, uint32_t pcnt, uint32_t pins, uint32_t pads,
+static __device__ __noinline__ uint32_t io_read(uint32_t a, uint32_t pcnt, uint32_t pins, uint32_t pads,
                                          uint32_t ports, uint32_t timer, const uint8_t* col, uint32_t stride4)
 {
     if (a & 0x80u) {                                                 // PIA: (a & 0x280) == 0x280
@@ -96,7 +96,7 @@ __device__ __noinline__ uint32_t io_read(uint32_t a, uint32_t pcnt, uint32_t pin
 // HeadlessTia::write (src/headless_tia.rs:225-298).  tw is the packed flag
 // word, lw = scanline | paddle_counter<<16; both come back updated.  The
 // write-only registers live in the instance's HBM rows (col, stride4).
-__device__ __noinline__ uint2 tia_write_io(uint32_t a, uint32_t v, uint32_t clock, uint32_t tw, uint32_t lw,
+static __device__ __noinline__ uint2 tia_write_io(uint32_t a, uint32_t v, uint32_t clock, uint32_t tw, uint32_t lw,
                                            uint8_t* col, uint32_t stride4)
 {
     auto stp = [&](uint32_t o, uint32_t val) { col[cold_off(o, stride4)] = (uint8_t)val; };
@@ -149,7 +149,7 @@ __device__ __noinline__ uint2 tia_write_io(uint32_t a, uint32_t v, uint32_t cloc
 
 // Pia::write, I/O half (src/pia.rs:202-228).  Returns (ports, timer value,
 // prescaler, select | underflow<<16).
-__device__ __noinline__ uint4 pia_write_io(uint32_t a, uint32_t v, uint32_t ports, uint32_t tv, uint32_t ps,
+static __device__ __noinline__ uint4 pia_write_io(uint32_t a, uint32_t v, uint32_t ports, uint32_t tv, uint32_t ps,
                                            uint32_t sel_uf)
 {
     if (a & 0x10u) {

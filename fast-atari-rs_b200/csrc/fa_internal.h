@@ -49,6 +49,50 @@ struct FaLaunch {
     unsigned long long* rounds;  // scheduler rounds x 32 (lane slots offered), or null
 };
 
+// ------------------------------------------------------------------ serving form
+// Instance state of the server lives in blocks of FA_SERVE_BLOCK_COLS columns
+// (row w of column c of a block at block[w * FA_SERVE_BLOCK_COLS + c]); a
+// session's instances are a list of such blocks, so it grows without moving.
+#define FA_SERVE_BLOCK_COLS 256u
+
+// One request of a serving launch (device table).
+struct FaServeReq {
+    const uint8_t* actions;      // k * n bytes, frame-major (actions[f * n + i])
+    uint8_t* obs;                // n * 128 bytes, or null
+    uint32_t n, k, sched, pad;
+};
+
+// One CTA of a serving launch (device table): up to `block` consecutive
+// instances of one request, all inside one state block.
+struct FaServeUnit {
+    uint32_t* state;             // first column of the unit (row stride FA_SERVE_BLOCK_COLS)
+    uint32_t req;                // request index in the launch's table
+    uint32_t first;              // index of the unit's first instance within the request
+};
+
+// A serving launch: every unit belongs to one cart (ROM staged per CTA).
+// per_frame != 0 runs frame `frame` of every request only (the plain form:
+// actions of that frame, observations only after the request's last frame).
+// With `done` set, completion is signalled per request: remaining[r] counts
+// the request's units still running (over every launch of the batch); the
+// last one sets done[r] (host-mapped) to 1, or 2 if a unit failed.
+struct FaServeLaunch {
+    const uint8_t* rom;
+    uint32_t nbanks, hot_lo;
+    const FaServeReq* req;
+    const FaServeUnit* unit;
+    uint32_t nunits;
+    uint32_t per_frame, frame;
+    uint32_t* remaining;         // device, one counter per request, or null
+    uint32_t* done;              // host-mapped, one flag per request, or null
+    uint32_t* err;
+    unsigned long long* instr;
+    unsigned long long* rounds;
+};
+
+// Launch fa_serve<block> (block 128 or 256) with one CTA per unit.
+cudaError_t fa_launch_serve(const FaServeLaunch& L, int block, cudaStream_t s);
+
 // Launch fa_run.  For the persistent form the grid is the SM count times the
 // CTAs per SM the occupancy calculator allows (cached per block and shared-
 // memory size, so that the call is safe inside a stream capture).

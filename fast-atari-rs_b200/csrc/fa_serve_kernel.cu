@@ -1,0 +1,130 @@
+// fa_serve_kernel.cu — the serving kernel (fa_serve) and its launcher.
+//
+// One CTA per unit (up to BLOCK instances of one request, inside one state
+// block of the server's arena), no queue and no persistence, so the CTAs of
+// several launches in flight interleave on the SMs as the hardware block
+// scheduler frees them: requests dispatched while others run start on
+// whichever SM slots drain first.  Every unit of a launch belongs to one cart,
+// whose ROM the CTA stages into shared memory with TMA bulk copies; the
+// launch's shared memory is sized to that cart's ROM alone.
+//
+// Completion is per request, not per launch: the last CTA of a request (a
+// device counter per request) fences at system scope and raises the
+// request's flag in host-mapped memory, after its observations — written
+// straight into host-mapped memory — are visible.  The host then lets the
+// session's next request run, possibly in another launch while this one is
+// still running.  That next kernel must read the state rows this one wrote,
+// so this file is compiled with global loads cached in L2 only
+// (-Xptxas -dlcm=cg): L2 is the point of coherence, and no SM can serve a
+// stale copy from its L1.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <mutex>
+
+#include "fa_run.cuh"
+
+namespace fa {
+
+constexpr uint32_t FA_REQ_FAILED = 0x80000000u;   // bit of a request's unit counter
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) fa_serve(const __grid_constant__ FaServeLaunch L)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ FaGroup sg;
+    __shared__ uint32_t s_count, s_req;
+
+    const uint32_t rom_bytes = L.nbanks * 4096u;
+    uint32_t* priv = (uint32_t*)(smem + rom_bytes);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        const FaServeUnit U = L.unit[blockIdx.x];
+        const FaServeReq R = L.req[U.req];
+        FaGroup g;
+        memset(&g, 0, sizeof(g));
+        g.rom = L.rom;
+        g.state = U.state;
+        g.stride = FA_SERVE_BLOCK_COLS;
+        g.nbanks = L.nbanks;
+        g.hot_lo = L.hot_lo;
+        g.sched = R.sched;
+        g.act_stride = R.n;
+        const uint32_t count = R.n - U.first < (uint32_t)BLOCK ? R.n - U.first : (uint32_t)BLOCK;
+        g.n = count;
+        if (L.per_frame) {
+            g.actions = R.actions + (size_t)L.frame * R.n + U.first;
+            g.k = L.frame < R.k ? 1u : 0u;
+            g.obs = (L.frame + 1u == R.k && R.obs) ? R.obs + (size_t)U.first * 128u : nullptr;
+        } else {
+            g.actions = R.actions + U.first;
+            g.k = R.k;
+            g.obs = R.obs ? R.obs + (size_t)U.first * 128u : nullptr;
+        }
+        sg = g;
+        s_count = count;
+        s_req = U.req;
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    const bool staged = stage_rom(smem, L.rom, rom_bytes, &bar, phase);
+    if (staged) run_unit<BLOCK>(sg, 0, s_count, smem, priv, threadIdx.x, L.instr, L.rounds);
+    else if (threadIdx.x == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
+    if (L.done) {
+        // Every thread's state and observation stores precede the barrier;
+        // the fence by thread 0 after it is cumulative over them.
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (!staged) atomicOr(L.remaining + s_req, FA_REQ_FAILED);
+            __threadfence_system();
+            const uint32_t old = atomicSub(L.remaining + s_req, 1u);
+            if ((old & ~FA_REQ_FAILED) == 1u) {
+                __threadfence_system();
+                *(volatile uint32_t*)(L.done + s_req) = (old & FA_REQ_FAILED) ? 2u : 1u;
+            }
+        }
+    }
+}
+
+}  // namespace fa
+
+namespace {
+std::mutex g_serve_mu;
+// (device, block) pairs whose dynamic shared-memory limit was raised to the
+// largest serving launch (32 KiB of ROM plus the RAM slab).
+std::map<std::pair<int, int>, bool> g_serve_cfg;
+
+template <int BLOCK>
+cudaError_t launch_serve(const FaServeLaunch& L, cudaStream_t s)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lk(g_serve_mu);
+        auto key = std::make_pair(dev, BLOCK);
+        if (g_serve_cfg.find(key) == g_serve_cfg.end()) {
+            e = cudaFuncSetAttribute(fa::fa_serve<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     32768 + FA_SMEM_WORDS * BLOCK * 4);
+            if (e != cudaSuccess) return e;
+            g_serve_cfg[key] = true;
+        }
+    }
+    if (L.nunits == 0) return cudaSuccess;
+    const size_t smem = (size_t)L.nbanks * 4096u + (size_t)FA_SMEM_WORDS * BLOCK * 4u;
+    fa::fa_serve<BLOCK><<<L.nunits, BLOCK, smem, s>>>(L);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t fa_launch_serve(const FaServeLaunch& L, int block, cudaStream_t s)
+{
+    if (L.nbanks < 1 || L.nbanks > 8) return cudaErrorInvalidValue;
+    switch (block) {
+    case 128: return launch_serve<128>(L, s);
+    case 256: return launch_serve<256>(L, s);
+    default: return cudaErrorInvalidValue;
+    }
+}

@@ -320,6 +320,125 @@ typedef struct fa_tuning {
 int fa_autotune(const uint8_t* rom, size_t rom_len, size_t n, fa_tuning* best,
                 fa_tuning* table, int table_cap, int* table_len);
 
+/* ------------------------------------------------------------------ serving
+ * Continuous-batching server (no reference counterpart: BatchAtariGpu,
+ * src/cuda_env.rs:99-191, serves one caller with one synchronous step per
+ * call).  A server holds up to 16 carts and any number of sessions; a session
+ * is one client's instance set of one cart, resident in HBM between requests.
+ * A step request names a session, a batch size n, a frame count k and k*n
+ * actions (frame-major), and steps instances [0, n) of the session k frames;
+ * if n exceeds the instances the session holds, the new ones are admitted
+ * first, each starting from the cart's post-reset snapshot (BatchAtariGpu::
+ * reset, src/cuda_env.rs:131-142).  Admission is charged against a budget of
+ * state bytes (whole 256-instance blocks of 58,368 bytes); when the budget is
+ * spent, admissions wait in FIFO order until a session is closed.  A
+ * session's requests run one at a time in submission order; requests of
+ * different sessions are batched into shared launches whenever they are
+ * ready, with up to max_inflight batches on the GPU at once.  Every result is
+ * identical to stepping the same session alone.  All calls are thread-safe.
+ */
+#define FA_ERR_TIMEOUT     -7   /* fa_server_wait: the request was not done in time */
+
+#define FA_SERVE_BATCHED 0   /* continuous batching (fa_serve launches, batches overlap) */
+#define FA_SERVE_PLAIN   1   /* FIFO of static batches, one on the GPU at a time, one
+                                launch per frame per cart (the reference's per-frame form) */
+
+typedef struct fa_server fa_server;
+
+typedef struct fa_server_config {
+    size_t state_budget_bytes;   /* resident state admitted at most (0 = 64 GiB) */
+    int    mode;                 /* FA_SERVE_BATCHED or FA_SERVE_PLAIN */
+    int    block;                /* CTA size, 128 or 256 (0 = 256 batched, 128 plain) */
+    int    max_inflight;         /* batches on the GPU at once, 1..64 (0 = 32; plain: 1) */
+    int    sched;                /* FA_SCHED_* warp policy (a NULL config: FA_SCHED_PC) */
+} fa_server_config;
+
+typedef struct fa_request_info {
+    int    status;               /* FA_OK or an FA_ERR_* code */
+    int    waited_admission;     /* 1 if its admission waited for budget */
+    unsigned batch_requests;     /* requests in the launch batch it ran in */
+    double latency_ms;           /* submit -> observations in the caller's buffer */
+    double queue_ms;             /* submit -> dispatch to the GPU */
+} fa_request_info;
+
+typedef struct fa_server_stats {
+    unsigned long long requests_submitted, requests_done, requests_failed;
+    unsigned long long instance_frames;       /* sum of n * k over completed requests */
+    unsigned long long dispatches;            /* batches sent to the GPU */
+    unsigned long long dispatched_requests;
+    unsigned long long launches;              /* kernel launches */
+    unsigned long long admission_waits;       /* requests whose admission waited */
+    unsigned long long guest_instructions;    /* 6502 instructions executed */
+    unsigned long long lane_slots;            /* warp lane slots offered */
+    long long sessions_open;
+    size_t state_bytes_in_use, state_bytes_peak, state_budget_bytes;
+} fa_server_stats;
+
+/* Create a server on the current device for ncarts ROMs (each checked and
+ * reset as by fa_create + fa_reset); cfg may be NULL (defaults).  Starts the
+ * engine thread. */
+int  fa_server_create(const uint8_t* const* roms, const size_t* rom_lens, int ncarts,
+                      const fa_server_config* cfg, fa_server** out);
+/* Stop the engine after the work on the GPU finishes (requests still waiting
+ * for admission fail with FA_ERR_CAPACITY) and free everything. */
+void fa_server_destroy(fa_server* s);
+/* Open an empty session of cart `cart` (instances are admitted by requests). */
+int  fa_server_open(fa_server* s, int cart, int64_t* session);
+/* Close a session: its queued requests still run, then its state is freed. */
+int  fa_server_close(fa_server* s, int64_t session);
+/* Queue a step request; actions (k*n bytes) are copied, obs (n*128 bytes, or
+ * NULL) is written before the request completes and must stay valid until
+ * fa_server_wait returns for the ticket.  n larger than the whole budget
+ * fails with FA_ERR_CAPACITY. */
+int  fa_server_submit(fa_server* s, int64_t session, const uint8_t* actions, uint32_t n, int k,
+                      uint8_t* obs, uint64_t* ticket);
+/* Wait for a ticket (timeout_ms < 0: no limit; FA_ERR_TIMEOUT on expiry, the
+ * ticket stays valid).  Each ticket is waited for until it completes, once. */
+int  fa_server_wait(fa_server* s, uint64_t ticket, int timeout_ms, fa_request_info* info);
+/* Submit and wait. */
+int  fa_server_step(fa_server* s, int64_t session, const uint8_t* actions, uint32_t n, int k,
+                    uint8_t* obs, fa_request_info* info);
+/* Instances the session holds (the largest n of its requests so far). */
+int  fa_server_session_size(fa_server* s, int64_t session, uint32_t* size);
+/* Full states of instances [first, first+count) of a session, after its
+ * queued requests complete (fa_state layout, as fa_get_states). */
+int  fa_server_get_states(fa_server* s, int64_t session, uint32_t first, uint32_t count, fa_state* out);
+int  fa_server_stats_get(fa_server* s, fa_server_stats* out);
+
+/* Simulated actor clients.  `requests` step requests arrive as a Poisson
+ * process at `offered_frames_per_s` instance-frames per second (0: all at
+ * once, the saturation throughput); each picks one of `clients` clients and
+ * one of the server's carts uniformly, a batch size lognormal(batch_median,
+ * batch_sigma) clipped to [batch_min, batch_max] and k uniform in
+ * [k_min, k_max], with actions uniform over the 18 joystick actions.  The
+ * trace depends only on the configuration (seed included), not on timing.
+ * Every (client, cart) is a session opened for the run and closed after it.
+ * latency_ms (NULL or `requests` floats) receives each request's latency. */
+typedef struct fa_loadgen_config {
+    int      clients;
+    int      requests;
+    double   offered_frames_per_s;
+    uint64_t seed;
+    uint32_t batch_median, batch_min, batch_max;
+    double   batch_sigma;
+    int      k_min, k_max;
+} fa_loadgen_config;
+
+typedef struct fa_loadgen_result {
+    unsigned long long requests, admission_waits;
+    double instance_frames;
+    double elapsed_s;              /* first arrival -> last completion */
+    double frames_per_s;           /* instance_frames / elapsed_s */
+    double offered_frames_per_s;
+    double arrival_window_s;       /* last arrival time */
+    double p50_ms, p90_ms, p99_ms, max_ms, mean_ms;
+    double mean_queue_ms;          /* submit -> dispatch */
+    double mean_batch_requests;    /* requests per launch batch, averaged over requests */
+    int    errors;
+} fa_loadgen_result;
+
+int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_loadgen_result* out, float* latency_ms);
+
 /* -------------------------------------------------- no-allocation stepping
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (device memory owned by another allocator, or a stepping loop that must not

@@ -65,3 +65,11 @@ def test_bad_rom_lengths_rejected_before_device():
             oracle.Atari(bytes(n))
     for n in (1, 2048, 4096, 8192, 16384, 32768, 40000):
         oracle.Atari(bytes([0xEA] * n))
+
+
+def test_server_without_device_fails_loudly():
+    if fa.device_count() > 0:
+        pytest.skip("a GPU is visible")
+    with pytest.raises(fa.FaError) as ei:
+        fa.AtariServer([bytes(4096)])
+    assert ei.value.code == -4
