@@ -1,7 +1,7 @@
 """Benchmark of the batched Atari 2600 core on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mixed|divergence|plain|scale]
+                    [--workload mixed|divergence|plain|scale|serve]
 
 Default workload (the batched configuration the headline metric is quoted
 on): four seeded synthetic carts — 2K Fixed, 8K F8, 16K F6, 32K F4 with
@@ -17,6 +17,14 @@ before every timed call); `e2e` is the same metric through the public C ABI
 with host buffers (pinned staging, H2D actions and D2H observations inside
 the timed region).  Under torchrun every rank runs its own replica of the
 workload on its GPU (instances are independent: weak scaling, no exchange).
+
+Serving (`--workload serve`, and a short summary in the default line): 64
+simulated actor clients send step requests by Poisson arrival to the
+continuous-batching server; each request picks one of the four carts
+uniformly, a batch size lognormal (median 256, sigma 1) clipped to
+16..16,384 and K uniform in 1..8.  The peak is the steady completion rate
+with every request queued at once; p50/p99 step latency are measured at
+20/40/70/100% of that peak, and the plain per-frame server runs the same trace.
 """
 from __future__ import annotations
 
@@ -81,10 +89,60 @@ def workload(name: str, carts):
         # fully converged (the instruction cost per guest instruction).
         return ("converged calibration: plain 4K Fixed cart, 151552 identical instances, "
                 "all actions 0, K=2", [(carts.plain_cart(), 151_552)], 2, 0)
+    if name == "serve":
+        # The serving trace's cart mix (uniform over the four carts per
+        # request; mean batch 422 instances, mean K 4.5) for the CPU baseline.
+        cs = carts.mixed_carts()
+        return (SERVE_DESC, [(c, 422) for c in cs], 4, 0)
     if name == "scale":
         return ("scale: 1000000 instances of the 32K F4 cart, K=16, reset every 2000 frames",
                 [(carts.scale_cart(), 1_000_000)], 16, 2000)
     raise SystemExit(f"unknown workload {name}")
+
+
+SERVE_DESC = ("serving: 64 Poisson actor clients, carts 2K Fixed/8K F8/16K F6/32K F4 uniform per request, "
+              "batch lognormal(median 256, sigma 1) clipped 16..16384, K uniform 1..8, "
+              "states resident in HBM, 64 GiB state budget")
+
+
+def serve_measure(fa, carts, sat_requests, level_requests, plain_requests, levels=(0.2, 0.4, 0.7, 1.0)):
+    """Batched server: steady peak and latency at fractions of it; plain server: peak on the same trace."""
+    roms = [c.rom for c in carts.mixed_carts()]
+    out = {"clients": 64, "levels": []}
+    with fa.AtariServer(roms) as srv:
+        srv.loadgen(requests=400, offered_frames_per_s=0.0, seed=99)              # warm-up
+        st0 = srv.stats()
+        sat, _ = srv.loadgen(requests=sat_requests, offered_frames_per_s=0.0, seed=1)
+        st1 = srv.stats()
+        peak = sat["steady_frames_per_s"]
+        out["saturation"] = sat
+        out["guest_instructions_per_s"] = (st1["guest_instructions"] - st0["guest_instructions"]) / sat["elapsed_s"]
+        out["lane_efficiency"] = ((st1["guest_instructions"] - st0["guest_instructions"]) /
+                                  max(1, st1["lane_slots"] - st0["lane_slots"]))
+        out["launches"] = st1["launches"] - st0["launches"]
+        for frac in levels:
+            r, _ = srv.loadgen(requests=level_requests, offered_frames_per_s=frac * peak, seed=2)
+            out["levels"].append({"load": frac, "offered_frames_per_s": r["offered_frames_per_s"],
+                                  "frames_per_s": r["frames_per_s"], "p50_ms": r["p50_ms"],
+                                  "p99_ms": r["p99_ms"], "max_ms": r["max_ms"], "mean_queue_ms": r["mean_queue_ms"],
+                                  "mean_batch_requests": r["mean_batch_requests"], "requests": r["requests"]})
+    with fa.AtariServer(roms, mode="plain") as srv:
+        srv.loadgen(requests=200, offered_frames_per_s=0.0, seed=99)
+        psat, _ = srv.loadgen(requests=plain_requests, offered_frames_per_s=0.0, seed=1)
+    out["plain_saturation"] = psat
+    out["peak_frames_per_s"] = peak
+    out["plain_peak_frames_per_s"] = psat["steady_frames_per_s"]
+    return out
+
+
+def serve_summary(sv):
+    lv = {l["load"]: l for l in sv["levels"]}
+    at70 = lv.get(0.7, sv["levels"][-1])
+    return {"workload": SERVE_DESC, "peak_frames_per_s": sv["peak_frames_per_s"],
+            "plain_peak_frames_per_s": sv["plain_peak_frames_per_s"],
+            "served_vs_plain": sv["peak_frames_per_s"] / sv["plain_peak_frames_per_s"],
+            "p50_ms_at_70pct": at70["p50_ms"], "p99_ms_at_70pct": at70["p99_ms"],
+            "levels": [{k: round(v, 3) if isinstance(v, float) else v for k, v in l.items()} for l in sv["levels"]]}
 
 
 # ------------------------------------------------------------------ clocks
@@ -356,6 +414,8 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
         "guest_instructions_per_step": instr / args.steps,
         "lane_efficiency": instr / slots if slots else None,
     }
+    if world == 1 and not args.no_serve:
+        line["serving"] = serve_summary(serve_measure(fa, carts, 8000, 3000, 2000, levels=(0.7,)))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         fps, cores, sample = cpu_reference(carts, spec, k, seconds_target=args.cpu_seconds)
         line["cpu_baseline"] = {"value": fps, "unit": UNIT, "cores": cores, "kind": "port",
@@ -365,13 +425,61 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
     pool.close()
 
 
+def run_serve_arm(args, fa, carts, rank, world, local_rank):
+    """The serving workload: its own JSON line (replicas under torchrun)."""
+    fa.set_device(local_rank)
+    n_sat = args.serve_requests
+    with ClockSampler(local_rank) as clk:
+        sv = serve_measure(fa, carts, n_sat, max(1000, n_sat // 6), max(1000, n_sat // 4))
+    clocks = clk.summary()
+    sat = sv["saturation"]
+    value = sv["peak_frames_per_s"]
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([value], device=torch.device("cuda", local_rank), dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        value = float(t.item()) * world        # replicas: the slowest rank's rate on every GPU
+    f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    peak_issue = 148 * 4 * f_sm
+    achieved = sv["guest_instructions_per_s"] * I_CONV / 32.0
+    mean_req_frames = sat["instance_frames"] / sat["requests"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": int(sat["requests"]),
+        "warmup": 400, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": SERVE_DESC, "step": "one step request (n instances x K frames)",
+                   "requests": int(sat["requests"]), "mean_instance_frames_per_request": mean_req_frames,
+                   "l2": "inputs resident in HBM between requests; not flushed",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "clocks": clocks,
+        "e2e": {"value": sat["frames_per_s"], "unit": UNIT,
+                "h2d_bytes_per_step": mean_req_frames, "d2h_bytes_per_step": 128.0 * sat["instances"] / sat["requests"],
+                "note": "whole saturation run (first arrival to last completion), actions from and observations to host memory"},
+        "gpu_launches": sv["launches"],
+        "roofline": {"bound": "issue", "achieved": achieved / 1e12, "peak": peak_issue / 1e12,
+                     "unit": "T warp-inst/s", "frac": achieved / peak_issue, "traffic": None,
+                     "note": f"guest 6502 instr/s x {I_CONV} SASS thread-instr per guest instr (converged) / 32"},
+        "plain_kernel": {"value": sv["plain_peak_frames_per_s"], "unit": UNIT,
+                         "form": "FIFO of static batches, one launch per frame per cart"},
+        "batched_vs_plain": value / world / sv["plain_peak_frames_per_s"] if world == 1 else None,
+        "serving": serve_summary(sv),
+        "lane_efficiency": sv["lane_efficiency"],
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mixed", choices=["mixed", "divergence", "plain", "scale", "converged"])
+    ap.add_argument("--workload", default="mixed",
+                    choices=["mixed", "divergence", "plain", "scale", "converged", "serve"])
+    ap.add_argument("--serve-requests", type=int, default=20000, help="saturation requests of the serve workload")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     ap.add_argument("--block", type=int, default=128)
     ap.add_argument("--tuning", default=None, help="JSON file of per-cart tuning records")
     ap.add_argument("--no-graph", action="store_true")
@@ -398,6 +506,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, carts, rank, world)
+        elif args.workload == "serve":
+            run_serve_arm(args, fa, carts, rank, world, local_rank)
         else:
             run_gpu_arm(args, fa, carts, rank, world, local_rank)
     finally:

@@ -458,7 +458,7 @@ class LoadgenResult(ctypes.Structure):
     """fa_loadgen_result (include/fast_atari.h)."""
     _fields_ = [("requests", ctypes.c_ulonglong), ("admission_waits", ctypes.c_ulonglong)] + \
         [(n, ctypes.c_double) for n in (
-            "instance_frames", "elapsed_s", "frames_per_s", "offered_frames_per_s", "arrival_window_s",
+            "instances", "instance_frames", "elapsed_s", "frames_per_s", "steady_frames_per_s", "offered_frames_per_s", "arrival_window_s",
             "p50_ms", "p90_ms", "p99_ms", "max_ms", "mean_ms", "mean_queue_ms", "mean_batch_requests")] + \
         [("errors", ctypes.c_int)]
 

@@ -62,7 +62,7 @@ struct FaServeReq {
     uint32_t n, k, sched, pad;
 };
 
-// One CTA of a serving launch (device table): up to `block` consecutive
+// One warp of a serving launch (device table): up to 32 consecutive
 // instances of one request, all inside one state block.
 struct FaServeUnit {
     uint32_t* state;             // first column of the unit (row stride FA_SERVE_BLOCK_COLS)
@@ -74,7 +74,7 @@ struct FaServeUnit {
 // per_frame != 0 runs frame `frame` of every request only (the plain form:
 // actions of that frame, observations only after the request's last frame).
 // With `done` set, completion is signalled per request: remaining[r] counts
-// the request's units still running (over every launch of the batch); the
+// the request's warp units still running; the
 // last one sets done[r] (host-mapped) to 1, or 2 if a unit failed.
 struct FaServeLaunch {
     const uint8_t* rom;
@@ -90,7 +90,8 @@ struct FaServeLaunch {
     unsigned long long* rounds;
 };
 
-// Launch fa_serve<block> (block 128 or 256) with one CTA per unit.
+// Launch fa_serve with CTAs of block / 32 warps (block 128, 256 or 512), one
+// warp per unit.
 cudaError_t fa_launch_serve(const FaServeLaunch& L, int block, cudaStream_t s);
 
 // Launch fa_run.  For the persistent form the grid is the SM count times the

@@ -286,7 +286,7 @@ int launch_slot(fa_server* s, int si, std::vector<ReqP>& reqs)
     for (size_t ri = 0; ri < reqs.size(); ri++) {
         const Request& r = *reqs[ri];
         const Session& ss = s->sessions[r.sid];
-        for (uint32_t first = 0; first < r.n; first += B) {
+        for (uint32_t first = 0; first < r.n; first += 32u) {
             const uint32_t j = first / FA_SERVE_BLOCK_COLS, c = first % FA_SERVE_BLOCK_COLS;
             units[ss.cart].push_back(FaServeUnit{ ss.blocks[j] + c, (uint32_t)ri, first });
             unit_k[ss.cart].push_back(r.k);
@@ -319,7 +319,7 @@ int launch_slot(fa_server* s, int si, std::vector<ReqP>& reqs)
         const Request& r = *reqs[ri];
         const size_t ab = (size_t)r.k * r.n;
         memcpy(sl.h_stage + ao, r.actions.data(), ab);
-        rem[ri] = (r.n + B - 1u) / B;
+        rem[ri] = (r.n + 31u) / 32u;
         rt[ri].actions = sl.d_stage + ao;
         rt[ri].obs = r.obs ? sl.dh_out + sl.flags_bytes + oo : nullptr;
         rt[ri].n = r.n;
@@ -586,8 +586,9 @@ extern "C" int fa_server_create(const uint8_t* const* roms, const size_t* rom_le
     if (cfg) c = *cfg;
     if (c.mode != FA_SERVE_BATCHED && c.mode != FA_SERVE_PLAIN) return fa_fail(FA_ERR_INVALID, "bad mode %d", c.mode);
     if (c.state_budget_bytes == 0) c.state_budget_bytes = (size_t)64 << 30;
-    if (c.block == 0) c.block = c.mode == FA_SERVE_PLAIN ? 128 : 256;
-    if (c.block != 128 && c.block != 256) return fa_fail(FA_ERR_INVALID, "block must be 128 or 256");
+    if (c.block == 0) c.block = c.mode == FA_SERVE_PLAIN ? 128 : 512;
+    if (c.block != 128 && c.block != 256 && c.block != 512)
+        return fa_fail(FA_ERR_INVALID, "block must be 128, 256 or 512");
     if (c.max_inflight == 0) c.max_inflight = 32;
     if (c.mode == FA_SERVE_PLAIN) c.max_inflight = 1;
     if (c.max_inflight < 1 || c.max_inflight > kMaxSlots)
@@ -856,7 +857,7 @@ extern "C" int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_
     // [k_min, k_max]; actions are uniform over the 18 joystick actions.
     std::vector<TraceReq> tr(c.requests);
     uint64_t rng = c.seed * 0x2545F4914F6CDD1Dull + 1u;
-    double t = 0.0, work = 0.0;
+    double t = 0.0, work = 0.0, insts = 0.0;
     for (int i = 0; i < c.requests; i++) {
         TraceReq& q = tr[i];
         t += -std::log(1.0 - unit01(rng));
@@ -873,6 +874,7 @@ extern "C" int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_
         uint64_t ar = c.seed ^ (0xA5A5A5A5ull + (uint64_t)i * 0x9E3779B97F4A7C15ull);
         for (auto& a : q.actions) a = (uint8_t)(splitmix64(ar) % FA_NUM_ACTIONS);
         work += (double)q.n * q.k;
+        insts += q.n;
     }
     // Scale arrival times so the trace offers `offered_frames_per_s`
     // instance-frames per second; 0 submits everything at once (saturation).
@@ -886,6 +888,7 @@ extern "C" int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_
             if (rc) return rc;
         }
     std::vector<uint64_t> tickets(c.requests, 0);
+    std::vector<double> t_sub(c.requests, 0.0);
     std::vector<std::unique_ptr<uint8_t[]>> obs(c.requests);
     std::vector<fa_request_info> info(c.requests);
     std::mutex mu;
@@ -917,6 +920,7 @@ extern "C" int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_
             if (due - now > std::chrono::microseconds(300)) std::this_thread::sleep_for(due - now - std::chrono::microseconds(200));
         }
         obs[i].reset(new uint8_t[(size_t)q.n * 128u]);
+        t_sub[i] = std::chrono::duration<double>(Clock::now() - t0).count();
         uint64_t tk = 0;
         int rc = fa_server_submit(s, sid[(size_t)q.client * ncarts + q.cart], q.actions.data(), q.n, (int)q.k,
                                   obs[i].get(), &tk);
@@ -945,13 +949,27 @@ extern "C" int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_
         bsum += info[i].batch_requests;
         waited += info[i].waited_admission;
     }
+    // Steady-state completion rate: instance-frames of the requests that
+    // complete between the 10th and the 60th percentile of completion times,
+    // over that span (the run's start and its tail, where only the sessions
+    // with the most work remain, are left out).
+    std::vector<std::pair<double, double>> done_at(c.requests);
+    for (int i = 0; i < c.requests; i++)
+        done_at[i] = { t_sub[i] + info[i].latency_ms * 1e-3, (double)tr[i].n * tr[i].k };
+    std::sort(done_at.begin(), done_at.end());
+    const size_t i10 = (size_t)(0.10 * (c.requests - 1)), i60 = (size_t)(0.60 * (c.requests - 1));
+    double steady_work = 0.0;
+    for (size_t i = i10 + 1; i <= i60; i++) steady_work += done_at[i].second;
+    const double steady_span = done_at[i60].first - done_at[i10].first;
     std::sort(lat.begin(), lat.end());
     auto pct = [&](double q) { return lat[std::min((size_t)c.requests - 1, (size_t)std::llround(q * (c.requests - 1)))]; };
     memset(out, 0, sizeof(*out));
     out->requests = (unsigned long long)c.requests;
+    out->instances = insts;
     out->instance_frames = work;
     out->elapsed_s = std::chrono::duration<double>(t_end - t0).count();
     out->frames_per_s = work / out->elapsed_s;
+    out->steady_frames_per_s = steady_span > 0.0 ? steady_work / steady_span : out->frames_per_s;
     out->offered_frames_per_s = c.offered_frames_per_s;
     out->arrival_window_s = tr.back().t;
     out->p50_ms = pct(0.50);

@@ -1,14 +1,16 @@
 // fa_serve_kernel.cu — the serving kernel (fa_serve) and its launcher.
 //
-// One CTA per unit (up to BLOCK instances of one request, inside one state
-// block of the server's arena), no queue and no persistence, so the CTAs of
-// several launches in flight interleave on the SMs as the hardware block
-// scheduler frees them: requests dispatched while others run start on
-// whichever SM slots drain first.  Every unit of a launch belongs to one cart,
-// whose ROM the CTA stages into shared memory with TMA bulk copies; the
-// launch's shared memory is sized to that cart's ROM alone.
+// One warp per unit (up to 32 consecutive instances of one request, inside
+// one state block of the server's arena), units packed densely into CTAs of
+// WARPS warps in the order the host lists them (longest requests first), no
+// queue and no persistence, so the CTAs of several launches in flight
+// interleave on the SMs as the hardware block scheduler frees them: requests
+// dispatched while others run start on whichever SM slots drain first.  Every
+// unit of a launch belongs to one cart, whose ROM the CTA stages into shared
+// memory with TMA bulk copies; the launch's shared memory is sized to that
+// cart's ROM alone.
 //
-// Completion is per request, not per launch: the last CTA of a request (a
+// Completion is per request, not per launch: the last warp of a request (a
 // device counter per request) fences at system scope and raises the
 // request's flag in host-mapped memory, after its observations — written
 // straight into host-mapped memory — are visible.  The host then lets the
@@ -29,19 +31,22 @@ namespace fa {
 
 constexpr uint32_t FA_REQ_FAILED = 0x80000000u;   // bit of a request's unit counter
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) fa_serve(const __grid_constant__ FaServeLaunch L)
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) fa_serve(const __grid_constant__ FaServeLaunch L)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ FaGroup sg;
-    __shared__ uint32_t s_count, s_req;
+    __shared__ FaGroup sg[WARPS];
+    __shared__ uint32_t s_count[WARPS], s_req[WARPS];
 
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t rom_bytes = L.nbanks * 4096u;
-    uint32_t* priv = (uint32_t*)(smem + rom_bytes);
-    if (threadIdx.x == 0) {
-        mbar_init(&bar, 1);
-        const FaServeUnit U = L.unit[blockIdx.x];
+    uint32_t* priv = (uint32_t*)(smem + rom_bytes) + warp * (FA_SMEM_WORDS * 32u);
+    const uint32_t u = blockIdx.x * WARPS + warp;
+    const bool have = u < L.nunits;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    if (have && lane == 0) {
+        const FaServeUnit U = L.unit[u];
         const FaServeReq R = L.req[U.req];
         FaGroup g;
         memset(&g, 0, sizeof(g));
@@ -52,7 +57,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) fa_serve(const __grid_con
         g.hot_lo = L.hot_lo;
         g.sched = R.sched;
         g.act_stride = R.n;
-        const uint32_t count = R.n - U.first < (uint32_t)BLOCK ? R.n - U.first : (uint32_t)BLOCK;
+        const uint32_t count = R.n - U.first < 32u ? R.n - U.first : 32u;
         g.n = count;
         if (L.per_frame) {
             g.actions = R.actions + (size_t)L.frame * R.n + U.first;
@@ -63,26 +68,28 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) fa_serve(const __grid_con
             g.k = R.k;
             g.obs = R.obs ? R.obs + (size_t)U.first * 128u : nullptr;
         }
-        sg = g;
-        s_count = count;
-        s_req = U.req;
+        sg[warp] = g;
+        s_count[warp] = count;
+        s_req[warp] = U.req;
     }
     __syncthreads();
     uint32_t phase = 0;
     const bool staged = stage_rom(smem, L.rom, rom_bytes, &bar, phase);
-    if (staged) run_unit<BLOCK>(sg, 0, s_count, smem, priv, threadIdx.x, L.instr, L.rounds);
-    else if (threadIdx.x == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
+    if (!have) return;
+    if (staged) run_unit<32>(sg[warp], 0, s_count[warp], smem, priv, lane, L.instr, L.rounds);
+    else if (lane == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
     if (L.done) {
-        // Every thread's state and observation stores precede the barrier;
-        // the fence by thread 0 after it is cumulative over them.
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            if (!staged) atomicOr(L.remaining + s_req, FA_REQ_FAILED);
+        // Every lane's state and observation stores precede the warp barrier;
+        // lane 0's fence after it is cumulative over them.
+        __syncwarp();
+        if (lane == 0) {
+            const uint32_t r = s_req[warp];
+            if (!staged) atomicOr(L.remaining + r, FA_REQ_FAILED);
             __threadfence_system();
-            const uint32_t old = atomicSub(L.remaining + s_req, 1u);
+            const uint32_t old = atomicSub(L.remaining + r, 1u);
             if ((old & ~FA_REQ_FAILED) == 1u) {
                 __threadfence_system();
-                *(volatile uint32_t*)(L.done + s_req) = (old & FA_REQ_FAILED) ? 2u : 1u;
+                *(volatile uint32_t*)(L.done + r) = (old & FA_REQ_FAILED) ? 2u : 1u;
             }
         }
     }
@@ -92,11 +99,11 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) fa_serve(const __grid_con
 
 namespace {
 std::mutex g_serve_mu;
-// (device, block) pairs whose dynamic shared-memory limit was raised to the
+// (device, warps) pairs whose dynamic shared-memory limit was raised to the
 // largest serving launch (32 KiB of ROM plus the RAM slab).
 std::map<std::pair<int, int>, bool> g_serve_cfg;
 
-template <int BLOCK>
+template <int WARPS>
 cudaError_t launch_serve(const FaServeLaunch& L, cudaStream_t s)
 {
     int dev = 0;
@@ -104,17 +111,17 @@ cudaError_t launch_serve(const FaServeLaunch& L, cudaStream_t s)
     if (e != cudaSuccess) return e;
     {
         std::lock_guard<std::mutex> lk(g_serve_mu);
-        auto key = std::make_pair(dev, BLOCK);
+        auto key = std::make_pair(dev, WARPS);
         if (g_serve_cfg.find(key) == g_serve_cfg.end()) {
-            e = cudaFuncSetAttribute(fa::fa_serve<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     32768 + FA_SMEM_WORDS * BLOCK * 4);
+            e = cudaFuncSetAttribute(fa::fa_serve<WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     32768 + WARPS * FA_SMEM_WORDS * 32 * 4);
             if (e != cudaSuccess) return e;
             g_serve_cfg[key] = true;
         }
     }
     if (L.nunits == 0) return cudaSuccess;
-    const size_t smem = (size_t)L.nbanks * 4096u + (size_t)FA_SMEM_WORDS * BLOCK * 4u;
-    fa::fa_serve<BLOCK><<<L.nunits, BLOCK, smem, s>>>(L);
+    const size_t smem = (size_t)L.nbanks * 4096u + (size_t)WARPS * FA_SMEM_WORDS * 32u * 4u;
+    fa::fa_serve<WARPS><<<(L.nunits + WARPS - 1) / WARPS, WARPS * 32, smem, s>>>(L);
     return cudaGetLastError();
 }
 }  // namespace
@@ -123,8 +130,9 @@ cudaError_t fa_launch_serve(const FaServeLaunch& L, int block, cudaStream_t s)
 {
     if (L.nbanks < 1 || L.nbanks > 8) return cudaErrorInvalidValue;
     switch (block) {
-    case 128: return launch_serve<128>(L, s);
-    case 256: return launch_serve<256>(L, s);
+    case 128: return launch_serve<4>(L, s);
+    case 256: return launch_serve<8>(L, s);
+    case 512: return launch_serve<16>(L, s);
     default: return cudaErrorInvalidValue;
     }
 }

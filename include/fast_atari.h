@@ -348,7 +348,7 @@ typedef struct fa_server fa_server;
 typedef struct fa_server_config {
     size_t state_budget_bytes;   /* resident state admitted at most (0 = 64 GiB) */
     int    mode;                 /* FA_SERVE_BATCHED or FA_SERVE_PLAIN */
-    int    block;                /* CTA size, 128 or 256 (0 = 256 batched, 128 plain) */
+    int    block;                /* CTA size, 128, 256 or 512 (0 = 512 batched, 128 plain) */
     int    max_inflight;         /* batches on the GPU at once, 1..64 (0 = 32; plain: 1) */
     int    sched;                /* FA_SCHED_* warp policy (a NULL config: FA_SCHED_PC) */
 } fa_server_config;
@@ -426,9 +426,12 @@ typedef struct fa_loadgen_config {
 
 typedef struct fa_loadgen_result {
     unsigned long long requests, admission_waits;
-    double instance_frames;
+    double instances;              /* sum of n over the requests */
+    double instance_frames;        /* sum of n * k */
     double elapsed_s;              /* first arrival -> last completion */
     double frames_per_s;           /* instance_frames / elapsed_s */
+    double steady_frames_per_s;    /* completion rate between the 10th and 60th
+                                      percentile of completion times */
     double offered_frames_per_s;
     double arrival_window_s;       /* last arrival time */
     double p50_ms, p90_ms, p99_ms, max_ms, mean_ms;
