@@ -122,7 +122,7 @@ def test_mixed_sessions_match_oracle(mixed, expected, threads):
     assert st["dispatched_requests"] == n_req and 1 <= st["dispatches"] <= n_req
 
 
-@pytest.mark.parametrize("block", [128, 512])
+@pytest.mark.parametrize("block", [128, 256])     # the default is 512
 def test_batched_cta_sizes_match_oracle(mixed, expected, block):
     with fa.AtariServer([c.rom for c in mixed], block=block, max_inflight=3) as srv:
         got, states, _ = run_mixed(srv, threads=False)
