@@ -52,11 +52,11 @@ UNIT = "frames/s"
 # a warp run identical instances (fully converged), from the ncu capture in
 # profiles/fa_run_warps_converged_plain.md.  Used to express guest-instruction
 # throughput in warp-issue slots for the roofline.
-I_CONV = 197.0
+I_CONV = 187.6
 # DRAM bytes moved per instance-frame by fa_run on this workload, from the ncu
-# capture in profiles/fa_run_warps_mixed_batch_full.md (27.4 MB per 4-frame
+# capture in profiles/fa_run_warps_mixed_batch_full.md (28.2 MB per 4-frame
 # call of 135,500 instances).
-DRAM_BYTES_PER_INSTANCE_FRAME = 50.6
+DRAM_BYTES_PER_INSTANCE_FRAME = 52.0
 
 
 def load_pkg():
@@ -143,6 +143,37 @@ def serve_summary(sv):
             "served_vs_plain": sv["peak_frames_per_s"] / sv["plain_peak_frames_per_s"],
             "p50_ms_at_70pct": at70["p50_ms"], "p99_ms_at_70pct": at70["p99_ms"],
             "levels": [{k: round(v, 3) if isinstance(v, float) else v for k, v in l.items()} for l in sv["levels"]]}
+
+
+def divergence_policies(fa, carts, n=50_000, frames=32, k_multi=16):
+    """The divergence cart under every warp policy (opcode grouping on/off),
+    per-frame launches (K=1, one launch per frame) vs step_multi (K=16 per
+    persistent launch): frames/s by CUDA events on the launching stream, and
+    the SIMT lane efficiency of each policy."""
+    import torch
+    rom = carts.divergence_cart().rom
+    dev = torch.device("cuda", torch.cuda.current_device())
+    acts = torch.from_numpy(np.ascontiguousarray(carts.actions(seed=5, n=n, frames=frames)).reshape(-1)).to(dev)
+    stream = torch.cuda.Stream()          # a real stream: the library launches on it, the events see it
+    out = {}
+    for sched in ("lane", "match", "pc", "line"):
+        for form, persistent, k in (("per_frame", False, 1), ("step_multi", True, k_multi)):
+            with fa.BatchAtariGpu(rom, n) as g:
+                g.set_launch(128, sched, persistent)
+                g.reset()
+                g.step_multi_async(acts.data_ptr(), k, 0, stream.cuda_stream)      # warm-up
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for c in range(frames // k):
+                    g.step_multi_async(acts.data_ptr() + c * k * n, k, 0, stream.cuda_stream)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                fps = n * (frames // k) * k / (e0.elapsed_time(e1) / 1e3)
+                g.step_multi(carts.actions(seed=6, n=n, frames=k), k, obs=False)
+                eff = g.last_instructions() / max(1, g.last_lane_slots())
+            out[f"{sched}/{form}"] = {"frames_per_s": fps, "lane_efficiency": eff}
+    return out
 
 
 # ------------------------------------------------------------------ clocks
@@ -414,7 +445,9 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
         "guest_instructions_per_step": instr / args.steps,
         "lane_efficiency": instr / slots if slots else None,
     }
-    if world == 1 and not args.no_serve:
+    if world == 1 and args.workload == "divergence":
+        line["policies"] = divergence_policies(fa, carts)
+    if world == 1 and args.workload == "mixed" and not args.no_serve:
         line["serving"] = serve_summary(serve_measure(fa, carts, 8000, 3000, 2000, levels=(0.7,)))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         fps, cores, sample = cpu_reference(carts, spec, k, seconds_target=args.cpu_seconds)

@@ -169,7 +169,9 @@ struct Emu {
     const uint8_t* rom;      // shared-memory ROM image, nbanks * 4 KiB
     uint32_t hot_lo, nbanks;
     // ---- CPU (src/cpu.rs:96-105)
-    uint32_t a, x, y, sp, p, pc, bank;
+    uint32_t a, x, y, sp, p, pc;
+    uint32_t bank;           // bank index (bits 0-2) | hotspot accesses this frame << 3,
+                             // saturating at 511: the count is a scheduling key only
     uint32_t cyc_acc;         // instruction cycles not yet added to Cpu::cycles in HBM
     // ---- PIA (src/pia.rs:26-44): timer unpacked (ticked every instruction),
     //      ports and input pins packed (touched only by I/O accesses)
@@ -212,10 +214,12 @@ struct Emu {
     __device__ __forceinline__ void setc(bool c) { p = (p & ~F_C) | (c ? F_C : 0u); }
 
     // ------------------------------------------------------------ bank switching
+    // A hotspot access selects its bank (src/atari.rs:460-492) and counts one
+    // more bank-switch point passed this frame in bank's upper bits.
     __device__ __forceinline__ void bsw(uint32_t a13)
     {
         uint32_t d = a13 - hot_lo;
-        if (d < nbanks) bank = d;
+        if (d < nbanks) bank = (bank < (511u << 3) ? ((bank + 8u) & ~7u) : (bank & ~7u)) | d;
     }
 
     // ------------------------------------------------------------ TIA (headless_tia.rs)
@@ -307,7 +311,7 @@ struct Emu {
     __device__ __forceinline__ uint32_t read(uint32_t addr)
     {
         uint32_t a = addr & 0x1FFFu;
-        if (a & 0x1000u) { bsw(a); return rom[(bank << 12) | (a & 0xFFFu)]; }
+        if (a & 0x1000u) { bsw(a); return rom[((bank & 7u) << 12) | (a & 0xFFFu)]; }
         return read_low(a);
     }
     __device__ __forceinline__ void write(uint32_t addr, uint32_t v)
@@ -647,7 +651,7 @@ struct Emu {
         if (a0 >= 0x1000u && a0 + 2u < hot_lo) {
             // Fast path: the three bytes at pc0 lie in the current bank and
             // below every hotspot, so reading them has no side effect.
-            const uint8_t* q = rom + (bank << 12) + (a0 & 0xFFFu);
+            const uint8_t* q = rom + ((bank & 7u) << 12) + (a0 & 0xFFFu);
             op = q[0];
             if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }
             b1 = q[1];
@@ -696,7 +700,7 @@ struct Emu {
     __device__ __forceinline__ void store_hot(uint32_t* col, uint32_t stride) const
     {
         col[R_AXYS * stride] = a | (x << 8) | (y << 16) | (sp << 24);
-        col[R_PC * stride] = pc | (p << 16) | (bank << 24);
+        col[R_PC * stride] = pc | (p << 16) | ((bank & 7u) << 24);
         col[R_PIA0 * stride] = (ports & 0xFFFFu) | ((pins & 0xFFu) << 16) | (((ports >> 16) & 0xFFu) << 24);
         col[R_PIA1 * stride] = (ports >> 24) | (((pins >> 8) & 0xFFu) << 8) | (uf << 16) | (((tw >> 18) & 1u) << 24);
         col[R_TIMER * stride] = tv | (ps << 16);

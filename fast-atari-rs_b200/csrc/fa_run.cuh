@@ -104,6 +104,7 @@ struct Runner {
         if (G->actions) e.apply_action(G->actions[(size_t)f * G->act_stride + e.i]);
         e.tw &= ~TW_FCOMP;
         fcyc = 0;
+        e.bank &= 7u;
         phase = e.vsync_on() ? 0u : 1u;
         return true;
     }
@@ -147,13 +148,16 @@ struct Runner {
         return e.wsync();
     }
 
-    // Scheduling key: frame, then (FA_SCHED_LINE) scanline, then pc.
+    // Scheduling key, a measure of how far the lane has progressed: frame,
+    // then the hotspot accesses of this frame (FA_SCHED_PC; the same code
+    // address in two banks is two program points, and a lane that has
+    // switched banks once more is ahead whatever its pc) or the scanline
+    // (FA_SCHED_LINE), then pc.
     __device__ __forceinline__ uint32_t key(uint32_t sched) const
     {
         const uint32_t fc = f < 0x7Fu ? f : 0x7Fu;
-        return sched == FA_SCHED_LINE
-            ? (fc << 25) | ((e.scanline < 0x1FFu ? e.scanline : 0x1FFu) << 16) | e.pc
-            : (fc << 16) | e.pc;
+        const uint32_t mid = sched == FA_SCHED_LINE ? (e.scanline < 0x1FFu ? e.scanline : 0x1FFu) : (e.bank >> 3);
+        return (fc << 25) | (mid << 16) | e.pc;
     }
 
     __device__ __forceinline__ void iterate()
@@ -168,7 +172,7 @@ struct Runner {
 // decides which lanes execute in each round; all lanes share one call site of
 // the emulator so its code is instantiated once.
 // Instructions a converged group may run per scheduling round.
-constexpr uint32_t FA_STEPS_PER_ROUND = 8;
+constexpr uint32_t FA_STEPS_PER_ROUND = 32;
 
 template <int BLOCK>
 __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
@@ -194,9 +198,9 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
             go = (g >> lane) & 1u;
             rem &= ~g;
         } else if (converge) {
-            // Convergence scheduling: the lane furthest behind (frame, then
-            // scanline for FA_SCHED_LINE, then pc) leads and every lane at the
-            // leader's (bank, pc) runs with it.  Lanes that branched ahead wait
+            // Convergence scheduling: the lane furthest behind (key()) leads
+            // and every lane at the leader's (bank and bank-switch count, pc)
+            // runs with it.  Lanes that branched ahead wait
             // until the others reach the same pc, so the warp re-converges.
             if (!__any_sync(FULL, act)) break;
             const uint32_t key = act ? r.key(sched) : 0xFFFFFFFFu;
@@ -208,8 +212,9 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
             go = act && pcb == lpcb;
             gm = __ballot_sync(FULL, go);
             // The smallest key among the lanes left waiting: the group keeps
-            // running only while its leader's key stays below it (so it stops
-            // where a waiting lane could join), which is exactly the order
+            // running only while every member's key stays below it (so it
+            // stops where a waiting lane could join); it may stop earlier than
+            // needed, never later, so the order of execution is the one
             // one-instruction rounds would follow.
             wait_key = __reduce_min_sync(FULL, go ? 0xFFFFFFFFu : key);
         } else {
@@ -217,8 +222,9 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
             go = act;
         }
         // One call site of the emulator for every policy.  A converged group
-        // keeps running while its lanes stay at one pc: one vote per
-        // instruction instead of a full scheduling round.
+        // keeps running (up to FA_STEPS_PER_ROUND instructions) while its
+        // lanes stay at one pc: one shuffle and one vote per instruction
+        // instead of a full scheduling round.
         uint32_t steps = 0;
         if (go) {
             while (true) {
@@ -226,8 +232,7 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
                 if (!converge || ++steps >= FA_STEPS_PER_ROUND) break;
                 const uint32_t mp = (r.e.bank << 16) | r.e.pc;
                 const uint32_t lp = __shfl_sync(gm, mp, lead);
-                const uint32_t lk = __shfl_sync(gm, r.active ? r.key(sched) : 0xFFFFFFFFu, lead);
-                if (!__all_sync(gm, r.active && mp == lp && lk < wait_key)) break;
+                if (!__all_sync(gm, r.active && mp == lp && r.key(sched) < wait_key)) break;
             }
         }
         rounds += converge ? __shfl_sync(FULL, steps, lead) : 1u;

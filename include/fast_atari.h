@@ -212,8 +212,9 @@ int fa_set_frame_numbers(fa_handle* h, const uint32_t* frame_no);
 
 /* Lane scheduling policies inside a warp (fa_set_launch `sched`). */
 #define FA_SCHED_LANE  0   /* each lane runs its own instruction stream */
-#define FA_SCHED_PC    1   /* lanes at the pc of the lane furthest behind run together */
-#define FA_SCHED_LINE  2   /* as FA_SCHED_PC, ordered by (frame, scanline, pc) */
+#define FA_SCHED_PC    1   /* lanes at the (bank, pc) of the lane furthest behind run together;
+                              "behind" by (frame, bank-switch hotspot accesses this frame, pc) */
+#define FA_SCHED_LINE  2   /* as FA_SCHED_PC, behind by (frame, scanline, pc) */
 #define FA_SCHED_MATCH 3   /* __match_any_sync groups by pc, every group each round */
 
 /*

@@ -266,6 +266,45 @@ def test_large_batch_identical_streams_and_spot_check():
     assert_states_equal(st[idx], ref, "spot check")
 
 
+def test_scale_config_spot_check():
+    """The scale configuration at full size: 1,000,000 instances of the 32K F4
+    cart, K=16 per call, reset to the post-init snapshot every 2,000 frames
+    with per-instance phase offsets uniform in [0, 2000).  1,024 random
+    instances, plus instances whose reset falls inside the call, match the
+    oracle bit for bit; instances that share a phase and an action stream end
+    identical."""
+    rom = cart("scale")
+    n, k, ep = 1_000_000, 16, 2000
+    rng = np.random.default_rng(11)
+    phase = rng.integers(0, ep, n, dtype=np.uint32)
+    # 4,096 distinct action streams, repeated: instance i follows stream i % 4096.
+    base = carts.actions(seed=77, n=4096, frames=k)
+    acts = np.ascontiguousarray(base[:, np.arange(n) % 4096])
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.set_launch(128, "pc", True)
+        g.reset()
+        g.set_episode_frames(ep)
+        g.set_frame_numbers(phase)
+        obs = g.step_multi(acts, k)
+        st = g.download_states()
+    resets = np.nonzero(phase > ep - k)[0]
+    assert len(resets) > 1000
+    idx = np.unique(np.concatenate([rng.choice(n, 1024, replace=False), resets[:256]]))
+    ref = oracle_states(rom, len(idx))
+    ref["frame_no"] = phase[idx]
+    o_obs, _ = oracle.run_batch(rom, ref, acts[:, idx], k, snapshot=oracle.reset_state(rom), episode_frames=ep)
+    assert np.array_equal(obs[idx], o_obs)
+    assert_states_equal(st[idx], ref, "scale spot check")
+    # Same stream and same phase: identical end state (a size-independent check over all n).
+    key = (np.arange(n) % 4096).astype(np.int64) * ep + phase
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    first = np.r_[True, ks[1:] != ks[:-1]]
+    head = order[np.maximum.accumulate(np.where(first, np.arange(n), 0))]
+    assert (st["ram"][order] == st["ram"][head]).all()
+    assert (st["cycles"][order] == st["cycles"][head]).all()
+
+
 # ---------------------------------------------------------------- committed golden vectors
 def _golden():
     import json
