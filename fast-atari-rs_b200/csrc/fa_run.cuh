@@ -224,7 +224,9 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
         // One call site of the emulator for every policy.  A converged group
         // keeps running (up to FA_STEPS_PER_ROUND instructions) while its
         // lanes stay at one pc: one shuffle and one vote per instruction
-        // instead of a full scheduling round.
+        // instead of a full scheduling round.  With no lane waiting
+        // (wait_key all ones, the common fully converged warp) the keys need
+        // not be compared.
         uint32_t steps = 0;
         if (go) {
             while (true) {
@@ -232,7 +234,9 @@ __device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
                 if (!converge || ++steps >= FA_STEPS_PER_ROUND) break;
                 const uint32_t mp = (r.e.bank << 16) | r.e.pc;
                 const uint32_t lp = __shfl_sync(gm, mp, lead);
-                if (!__all_sync(gm, r.active && mp == lp && r.key(sched) < wait_key)) break;
+                const bool cont = wait_key == 0xFFFFFFFFu ? (r.active && mp == lp)
+                                                          : (r.active && mp == lp && r.key(sched) < wait_key);
+                if (!__all_sync(gm, cont)) break;
             }
         }
         rounds += converge ? __shfl_sync(FULL, steps, lead) : 1u;
