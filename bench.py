@@ -226,6 +226,31 @@ class ClockSampler:
                 "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3] not in ("", "[N/A]"))}
 
 
+# ------------------------------------------------------------------ ranks
+def dist_backend() -> str:
+    """NCCL between GPUs; gloo where no GPU is visible (the CPU tests of the
+    multi-rank path)."""
+    import torch
+    return "nccl" if torch.cuda.is_available() else "gloo"
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """The largest of every rank's x (times: the job ends with its slowest rank)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(rank: int, group: int) -> int:
+    """Action seed of cart group `group` on rank `rank`: every rank steps its own
+    replica of the workload (instances are independent; no exchange)."""
+    return 1000 * rank + 17 * group + 1
+
+
 # ------------------------------------------------------------------ CPU reference
 def cpu_reference(carts, spec, k, seconds_target=15.0):
     """The oracle (a C restatement of the reference's HeadlessAtari) on the
@@ -259,7 +284,7 @@ def run_reference_arm(args, carts, rank, world):
     if rank != 0:
         return
     # Each step is one bounded CPU sample; warmup steps are run untimed.
-    per_step_s = max(2.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
+    per_step_s = args.ref_step_seconds or max(2.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
     vals = []
     for i in range(args.warmup + args.steps):
         fps, cores, sample = cpu_reference(carts, spec, k, seconds_target=per_step_s)
@@ -314,7 +339,7 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
             continue
         for c0 in range(0, calls, chunk):
             c1 = min(calls, c0 + chunk)
-            a = carts.actions(seed=1000 * rank + 17 * gi + 1, n=n, frames=(c1 - c0) * k, frame0=c0 * k)
+            a = carts.actions(seed=replica_seed(rank, gi), n=n, frames=(c1 - c0) * k, frame0=c0 * k)
             t[c0 * k * n:c1 * k * n].copy_(torch.from_numpy(a.reshape(-1)))
         d_act.append(t)
     d_obs = [torch.empty(n * 128, dtype=torch.uint8, device=dev) for _, n in spec]
@@ -359,11 +384,7 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
     slots = pool.last_lane_slots()
     clocks = clk.summary()
     total_ms = sum(ms)
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = max_over_ranks(total_ms, world, dev)
     n_total = sum(n for _, n in spec)
     frames = n_total * k * args.steps * world
     value = frames / (total_ms / 1e3)
@@ -406,7 +427,7 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
         t0 = time.perf_counter()
         for i in range(e2e_steps):
             pool.step(host_acts[i], k, obs=True)
-        e2e_s = time.perf_counter() - t0
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
         e2e_value = n_total * k * e2e_steps * world / e2e_s
     h2d = n_total * k
     d2h = n_total * 128
@@ -520,6 +541,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-step-seconds", type=float, default=0.0,
+                    help="CPU sample per step of the reference arm (0: sized so the run takes about 2 minutes)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     args.tuning = json.load(open(args.tuning)) if args.tuning else {}
@@ -534,8 +557,9 @@ def main():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group(dist_backend(), timeout=datetime.timedelta(seconds=300))
     try:
         if args.impl == "reference":
             run_reference_arm(args, carts, rank, world)
