@@ -322,6 +322,15 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
             view.set_episode_frames(episode)
             view.set_frame_numbers(rng.integers(0, episode, n, dtype=np.uint32))
     tuning = args.tuning
+    if not tuning and not args.no_autotune and args.workload != "converged":
+        # The project autotuner, per cart at up to 8,192 instances: it times
+        # every warp policy, launch shape and K; the batched launch takes each
+        # cart's policy and its measured cost per instance-frame (the queue
+        # order, heaviest units first).  K stays the workload's.
+        sys.path.insert(0, str(PKG_DIR))
+        import tune
+        tuning = tune.tune_workload([(c, n) for c, n in spec], cap=8192)
+    args.tuning_used = tuning
     for g, (c, n) in zip(groups, spec):
         t = tuning.get(c.spec.name, {})
         pool.set_group(g, t.get("sched", "pc"), float(t.get("weight", 1.0 + c.spec.rom_size / 32768.0)))
@@ -453,6 +462,10 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "tuning": {name: {k2: (round(v, 3) if isinstance(v, float) else v) for k2, v in t.items()
+                          if k2 in ("sched_name", "weight", "k", "persistent", "cta_warps", "block", "frames_per_s",
+                                    "instances")}
+                   for name, t in (args.tuning_used or {}).items()} or None,
         "gpu_launches": args.steps,
         "roofline": {"bound": "issue", "achieved": achieved / 1e12, "peak": peak / 1e12,
                      "unit": "T warp-inst/s", "frac": achieved / peak, "traffic": traffic,
@@ -535,7 +548,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=20000, help="saturation requests of the serve workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     ap.add_argument("--block", type=int, default=128)
-    ap.add_argument("--tuning", default=None, help="JSON file of per-cart tuning records")
+    ap.add_argument("--tuning", default=None, help="JSON file of per-cart tuning records (skips the autotuner)")
+    ap.add_argument("--no-autotune", action="store_true", help="default policy and weights instead of the autotuner")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg")
