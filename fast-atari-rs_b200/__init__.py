@@ -121,6 +121,18 @@ _SIGS = {
     "fa_server_get_states": (_i, [_vp, ctypes.c_int64, _u32, _u32, _vp]),
     "fa_server_stats_get": (_i, [_vp, _vp]),
     "fa_server_loadgen": (_i, [_vp, _vp, _vp, _vp]),
+    "fa_render_create": (_i, [_u8p, _sz, _sz, ctypes.POINTER(_vp)]),
+    "fa_render_destroy": (None, [_vp]),
+    "fa_render_num_envs": (_sz, [_vp]),
+    "fa_render_set_launch": (_i, [_vp, _i, _i]),
+    "fa_render_reset": (_i, [_vp, _vp, _vp]),
+    "fa_render_step_multi": (_i, [_vp, _u8p, _i, _vp, _vp]),
+    "fa_render_step_multi_async": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "fa_render_synchronize": (_i, [_vp]),
+    "fa_render_device_framebuffers": (_vp, [_vp]),
+    "fa_render_get_framebuffers": (_i, [_vp, _vp]),
+    "fa_render_get_states": (_i, [_vp, _vp]),
+    "fa_render_last_instructions": (ctypes.c_ulonglong, [_vp]),
 }
 
 FA_ERR_CAPACITY = -6
@@ -561,3 +573,73 @@ class AtariServer:
         lat = np.zeros(int(requests), np.float32)
         _check(lib().fa_server_loadgen(self._s, ctypes.byref(cfg), ctypes.byref(res), lat.ctypes.data))
         return res.as_dict(), lat
+
+
+# ------------------------------------------------------------------ rendering
+FB_H, FB_W = 192, 160
+
+
+class AtariRender:
+    """The rendering console (src/atari.rs:107-306, src/tia.rs) for n consoles
+    of one ROM: each frame also renders a 160 x 192 framebuffer of NTSC
+    palette indices (Atari::framebuffer), kept on the device."""
+
+    def __init__(self, rom: bytes, n: int, cta_warps: int = 8, sched="pc"):
+        r = np.frombuffer(bytes(rom), dtype=np.uint8).copy()
+        h = _vp()
+        _check(lib().fa_render_create(_u8(r), len(r), int(n), ctypes.byref(h)))
+        self._r = h
+        self.n = int(n)
+        _check(lib().fa_render_set_launch(h, int(cta_warps), SCHED_NAMES[sched] if isinstance(sched, str) else int(sched)))
+
+    def close(self) -> None:
+        if getattr(self, "_r", None):
+            lib().fa_render_destroy(self._r)
+            self._r = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def reset(self):
+        """(framebuffers [n, 192, 160], RAM [n, 128]) after new + one frame."""
+        fb = np.empty((self.n, FB_H, FB_W), np.uint8)
+        ram = np.empty((self.n, 128), np.uint8)
+        _check(lib().fa_render_reset(self._r, fb.ctypes.data, ram.ctypes.data))
+        return fb, ram
+
+    def step_multi(self, actions, k: int, fb: bool = True):
+        a = np.ascontiguousarray(actions, dtype=np.uint8).reshape(-1)
+        if a.size != k * self.n:
+            raise ValueError(f"expected {k}*{self.n} actions, got {a.size}")
+        out = np.empty((self.n, FB_H, FB_W), np.uint8) if fb else None
+        ram = np.empty((self.n, 128), np.uint8)
+        _check(lib().fa_render_step_multi(self._r, _u8(a), int(k), out.ctypes.data if fb else None, ram.ctypes.data))
+        return out, ram
+
+    def step_multi_async(self, d_actions: int, k: int, d_obs: int = 0, stream: int = 0) -> None:
+        _check(lib().fa_render_step_multi_async(self._r, _vp(d_actions), int(k), _vp(d_obs or None), _vp(stream or None)))
+
+    def synchronize(self) -> None:
+        _check(lib().fa_render_synchronize(self._r))
+
+    def framebuffers(self) -> np.ndarray:
+        out = np.empty((self.n, FB_H, FB_W), np.uint8)
+        _check(lib().fa_render_get_framebuffers(self._r, out.ctypes.data))
+        return out
+
+    def device_framebuffers(self) -> int:
+        return int(lib().fa_render_device_framebuffers(self._r) or 0)
+
+    def states(self) -> np.ndarray:
+        out = np.zeros(self.n, dtype=STATE_DTYPE)
+        _check(lib().fa_render_get_states(self._r, out.ctypes.data))
+        return out
+
+    def last_instructions(self) -> int:
+        return int(lib().fa_render_last_instructions(self._r))

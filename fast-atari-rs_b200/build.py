@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "lib" / "libfast_atari.so"
 SOURCES = ["fa_kernels.cu", "fa_api.cu", "fa_pool.cu", "fa_noalloc.cu", "fa_autotune.cu", "fa_env.cu", "fa_serve.cu",
-           "fa_serve_kernel.cu"]
+           "fa_serve_kernel.cu", "fa_render.cu"]
 # The serving kernel reads state rows that a concurrently running launch may
 # have written: its global loads are cached in L2 only (the coherence point).
 EXTRA = {"fa_serve_kernel.cu": ["-Xptxas", "-dlcm=cg"]}

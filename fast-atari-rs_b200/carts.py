@@ -608,3 +608,121 @@ def scale_cart(seed: int = 4) -> Cart:
     """32K F4, 0% WSYNC lines, bank switch every 8 lines."""
     return build_cart(CartSpec("scale_32k_f4", 32768, seed, wsync_density=0.0,
                                ops_min=8, ops_max=40, lines_per_group=8, subroutines=2))
+
+
+# ------------------------------------------------------------- rendering cart
+# Graphics registers the rendering cart writes (Tia::write, src/tia.rs:570-674).
+_GFX_REGS = [0x04, 0x05, 0x06, 0x07, 0x08, 0x09, 0x0A, 0x0B, 0x0C, 0x0D, 0x0E, 0x0F,
+             0x1B, 0x1C, 0x1D, 0x1E, 0x1F, 0x20, 0x21, 0x22, 0x23, 0x24, 0x25, 0x26, 0x27, 0x28, 0x29]
+_POS_REGS = [0x10, 0x11, 0x12, 0x13, 0x14]       # RESP0 RESP1 RESM0 RESM1 RESBL
+_CX_READS = [0x30, 0x31, 0x32, 0x33, 0x34, 0x35, 0x36, 0x37]
+
+
+def render_cart(seed: int = 5) -> Cart:
+    """A 4K Fixed cart for the rendering console (the pixel-accurate TIA):
+    the frame skeleton (3 VSYNC, 37 VBLANK with the input-latch or paddle-dump
+    bits, 192 visible, 30 overscan lines) with visible lines that write every
+    graphics register from RAM-dependent values at varying cycles within the
+    line -- colours, playfield (mid-line, through the delayed write), player,
+    missile and ball graphics, NUSIZ copies and sizes, reflection, priority
+    and score modes, vertical delay, mid-line RESPx/RESMx/RESBL, HMOVE and
+    HMCLR, read-modify-write on TIA registers -- read the collision latches
+    and the inputs back into RAM, and fold SWCHA into that RAM every line, so
+    the picture depends on the actions.  Control flow is straight-line blocks
+    and counted loops only."""
+    rng = Rng(seed * 0x9E3779B1 + 4096)
+    a = Asm()
+    a.label("reset")
+    for mn, mode, arg in (("SEI", "imp", None), ("CLD", "imp", None), ("LDX", "imm", 0xFF), ("TXS", "imp", None),
+                          ("LDA", "imm", 0), ("LDX", "imm", 0x80)):
+        a.ins(mn, mode, arg)
+    a.label("clr")
+    a.ins("STA", "zpx", 0)
+    a.ins("INX")
+    a.ins("BNE", "rel", "clr")
+    a.label("frame")
+    a.ins("LDA", "imm", 2)
+    a.ins("STA", "zp", VSYNC)
+    for _ in range(3):
+        a.ins("STA", "zp", WSYNC)
+    a.ins("LDA", "imm", 0)
+    a.ins("STA", "zp", VSYNC)
+    a.ins("LDA", "imm", 0x02 | (0x40 if rng.chance(0.5) else 0) | (0x80 if rng.chance(0.5) else 0))
+    a.ins("STA", "zp", VBLANK)
+    _wsync_lines(asm=a, n=36, tag="vbl")
+    # per frame: inputs into RAM, a per-frame seed byte
+    a.ins("LDA", "abs", SWCHA)
+    a.ins("EOR", "zp", 0x81)
+    a.ins("ADC", "imm", rng.below(256))
+    a.ins("STA", "zp", 0x81)
+    a.ins("LDA", "zp", INPT4)
+    a.ins("STA", "zp", 0x82)
+    a.ins("STA", "zp", WSYNC)
+    a.ins("LDA", "imm", 0)
+    a.ins("STA", "zp", VBLANK)
+    a.ins("LDA", "imm", 192)
+    a.ins("STA", "zp", 0x80)
+    a.label("line")
+    a.ins("STA", "zp", WSYNC)
+    nblocks = 8
+    # line dispatch: a RAM-counter-selected block (8 blocks of lines)
+    a.ins("LDA", "zp", 0x80)
+    a.ins("AND", "imm", 7)
+    a.ins("TAX")
+    for b in range(nblocks):
+        a.ins("CPX", "imm", b)
+        a.ins("BNE", "rel", f"nb{b}")
+        a.ins("JMP", "abs", f"blk{b}")
+        a.label(f"nb{b}")
+    a.ins("JMP", "abs", "blk0")
+    for b in range(nblocks):
+        a.label(f"blk{b}")
+        if rng.chance(0.3):
+            a.ins("STA", "zp", 0x2A)                               # HMOVE right after WSYNC
+        for _u in range(rng.range(6, 11)):
+            k = rng.below(10)
+            r1, r2 = rng.range(0x81, 0xBF), rng.range(0x83, 0xBF)
+            if k <= 3:                                             # graphics register from RAM
+                a.ins("LDA", "zp", r1)
+                if rng.chance(0.5):
+                    a.ins("EOR", "zp", 0x80)                       # the line counter
+                a.ins("STA", "zp" if rng.chance(0.7) else "abs", rng.choice(_GFX_REGS))
+            elif k == 4:                                           # position reset at this cycle
+                if rng.chance(0.5):
+                    a.ins("NOP")
+                a.ins("STA", "zp", rng.choice(_POS_REGS))
+            elif k == 5:                                           # collisions into RAM
+                a.ins("LDA", "zp", rng.choice(_CX_READS))
+                a.ins("ORA", "zp", r1)
+                a.ins("STA", "zp", r2)
+            elif k == 6:                                           # read-modify-write on a TIA register
+                a.ins(rng.choice(["INC", "DEC", "ASL", "ROL"]), "zp", rng.choice([0x06, 0x07, 0x08, 0x09, 0x0E, 0x1B]))
+            elif k == 7:                                           # motion registers
+                a.ins("LDA", "imm", rng.below(256))
+                a.ins("STA", "zp", rng.choice([0x20, 0x21, 0x22, 0x23, 0x24, 0x2B]))
+            elif k == 8:                                           # RAM evolution from the inputs
+                a.ins("LDA", "abs", SWCHA)
+                a.ins("ADC", "zp", r1)
+                a.ins("STA", "zp", r2)
+            else:                                                  # timer and paddle reads into RAM
+                if rng.chance(0.5):
+                    a.ins("LDA", "abs", INTIM)
+                else:
+                    a.ins("LDA", "abs" if rng.chance(0.5) else "zp", INPT0)
+                a.ins("EOR", "zp", r1)
+                a.ins("STA", "zp", r2)
+        a.ins("JMP", "abs", "lend")
+    a.label("lend")
+    a.ins("DEC", "zp", 0x80)
+    a.ins("BEQ", "rel", "ovs")
+    a.ins("JMP", "abs", "line")
+    a.label("ovs")
+    a.ins("LDA", "imm", 2)
+    a.ins("STA", "zp", VBLANK)
+    a.ins("STA", "zp", 0x2C)                                       # CXCLR
+    _wsync_lines(asm=a, n=30, tag="ovl")
+    a.ins("JMP", "abs", "frame")
+    a.org(0xFFFC)
+    a.raw(bytes([0x00, 0xF0, 0x00, 0xF0]))
+    img, labels, _ = a.assemble(4096)
+    return Cart(CartSpec("render_4k_fixed", 4096, seed, wsync_density=1.0), bytes(img), labels)

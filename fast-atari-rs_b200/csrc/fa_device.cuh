@@ -49,7 +49,13 @@ static __constant__ uint32_t c_legal[8] = {
 };
 
 // Packed TIA flag word (Emu::tw).
-enum : uint32_t { TW_WSYNC = 1u << 16, TW_FCOMP = 1u << 17, TW_PDUMP = 1u << 18 };
+enum : uint32_t { TW_WSYNC = 1u << 16, TW_FCOMP = 1u << 17, TW_PDUMP = 1u << 18,
+                  // rendering console only
+                  TW_HMOVE = 1u << 19, TW_LATCH = 1u << 20, TW_L4 = 1u << 21, TW_L5 = 1u << 22 };
+
+// NUSIZ copy offsets as a mask over {0, 16, 32, 64} (tia.rs:440-450, 480-488).
+static __constant__ uint32_t c_copies[8] = { 0x1, 0x3, 0x5, 0x7, 0x9, 0x1, 0xD, 0x1 };
+
 
 template <int BLOCK>
 __device__ __forceinline__ uint32_t priv_off(uint32_t o) { return (o & ~3u) * BLOCK + (o & 3u); }
@@ -160,7 +166,304 @@ static __device__ __noinline__ uint4 pia_write_io(uint32_t a, uint32_t v, uint32
     return make_uint4((ports & ~(0xFFu << sh)) | (v << sh), tv, ps, sel_uf);
 }
 
-template <int BLOCK>
+// ---------------------------------------------------------------- rendering console
+// The pixel-accurate Tia (src/tia.rs) and the per-cycle Pia::tick
+// (src/pia.rs:80-103) of the reference's rendering console, as out-of-line
+// functions on the state they touch.  The registers of the TIA are the
+// console's private bytes in shared memory (PB_* graphics registers, RB_*
+// extras), interleaved by lane in 32-lane slabs; the framebuffer is HBM.
+struct RState {
+    uint32_t clock, scanline, tw, pcnt, vtop;   // beam, TIA flags, paddle counter, visible_top | vblank_top << 16
+    uint32_t pix, pmask, pword;                 // framebuffer word being assembled
+    uint32_t tv, ps, sel, uf;                   // PIA timer
+};
+
+static __device__ __forceinline__ uint32_t rp8(const uint8_t* pv, uint32_t o) { return pv[(o & ~3u) * 32u + (o & 3u)]; }
+static __device__ __forceinline__ void wp8(uint8_t* pv, uint32_t o, uint32_t v) { pv[(o & ~3u) * 32u + (o & 3u)] = (uint8_t)v; }
+static __device__ __forceinline__ uint32_t rp16(const uint8_t* pv, uint32_t o) { return *(const uint16_t*)(pv + (o & ~3u) * 32u + (o & 3u)); }
+static __device__ __forceinline__ void wp16(uint8_t* pv, uint32_t o, uint32_t v) { *(uint16_t*)(pv + (o & ~3u) * 32u + (o & 3u)) = (uint16_t)v; }
+
+static __device__ void render_fb_flush(uint32_t pix, uint32_t pmask, uint32_t pword, uint8_t* fbp)
+{
+    if (!pmask) return;
+    uint32_t* w = (uint32_t*)fbp + pword;
+    if (pmask == 0xFu) { *w = pix; return; }
+    uint32_t keep = 0;
+    for (uint32_t b = 0; b < 4u; b++) keep |= ((pmask >> b) & 1u) ? 0u : (0xFFu << (8u * b));
+    *w = (*w & keep) | pix;
+}
+
+static __device__ __forceinline__ uint32_t dist160(uint32_t x, uint32_t pos, uint32_t off)
+{
+    uint32_t cp = pos + off;
+    if (cp >= 160u) cp -= 160u;
+    const uint32_t d = x + 160u - cp;
+    return d >= 160u ? d - 160u : d;
+}
+
+static __device__ __forceinline__ bool r_player(const uint8_t* pv, uint32_t n, uint32_t x)      // tia.rs:423-465
+{
+    const uint32_t grp = rp8(pv, n ? (rp8(pv, PB_VDELP1) ? PB_GRP1_OLD : PB_GRP1) : (rp8(pv, PB_VDELP0) ? PB_GRP0_OLD : PB_GRP0));
+    if (grp == 0) return false;
+    const uint32_t mode = rp8(pv, n ? PB_NUSIZ1 : PB_NUSIZ0) & 7u;
+    const uint32_t width = mode == 5u ? 2u : mode == 7u ? 4u : 1u, span = 8u * width;
+    const uint32_t pos = rp16(pv, PB_POS + 2u * n), refp = rp8(pv, n ? PB_REFP1 : PB_REFP0);
+    const uint32_t copies = c_copies[mode];
+    for (uint32_t c = 0; c < 4u; c++) {
+        if (!((copies >> c) & 1u)) continue;
+        const uint32_t off = dist160(x, pos, c == 0 ? 0u : 8u << c);
+        if (off < span && off < 80u) {
+            const uint32_t bit = off / width;
+            if (refp ? (grp & (0x01u << bit)) : (grp & (0x80u >> bit))) return true;
+        }
+    }
+    return false;
+}
+
+static __device__ __forceinline__ bool r_missile(const uint8_t* pv, uint32_t n, uint32_t x)     // tia.rs:468-497
+{
+    if (!rp8(pv, n ? PB_ENAM1 : PB_ENAM0) || rp8(pv, n ? PB_RESMP1 : PB_RESMP0)) return false;
+    const uint32_t nusiz = rp8(pv, n ? PB_NUSIZ1 : PB_NUSIZ0);
+    const uint32_t width = 1u << ((nusiz >> 4) & 3u), pos = rp16(pv, PB_POS + 4u + 2u * n);
+    const uint32_t copies = c_copies[nusiz & 7u];
+    for (uint32_t c = 0; c < 4u; c++) {
+        if (!((copies >> c) & 1u)) continue;
+        const uint32_t off = dist160(x, pos, c == 0 ? 0u : 8u << c);
+        if (off < width && off < 80u) return true;
+    }
+    return false;
+}
+
+static __device__ __forceinline__ void r_pixel(RState& s, uint8_t* pv, uint8_t* fbp, uint32_t vis, uint32_t x)
+{
+    const uint32_t ctrlpf = rp8(pv, PB_CTRLPF);
+    // playfield bit (tia.rs:406-420)
+    const uint32_t pfx = x < 80u ? x >> 2 : ((ctrlpf & 1u) ? 19u - ((x - 80u) >> 2) : (x - 80u) >> 2);
+    const bool pf = pfx <= 3u ? (rp8(pv, PB_PF0) & (0x10u << pfx)) != 0
+                  : pfx <= 11u ? (rp8(pv, PB_PF1) & (0x80u >> (pfx - 4u))) != 0
+                               : (rp8(pv, PB_PF2) & (0x01u << (pfx - 12u))) != 0;
+    const bool p0 = r_player(pv, 0, x), p1 = r_player(pv, 1, x);
+    const bool m0 = r_missile(pv, 0, x), m1 = r_missile(pv, 1, x);
+    bool bl = false;                                                 // tia.rs:500-507
+    if (rp8(pv, rp8(pv, PB_VDELBL) ? PB_ENABL_OLD : PB_ENABL)) {
+        const uint32_t off = dist160(x, rp16(pv, PB_POS + 8u), 0u);
+        bl = off < (1u << ((ctrlpf >> 4) & 3u)) && off < 80u;
+    }
+    const uint32_t c0 = rp8(pv, PB_COLUP0), c1 = rp8(pv, PB_COLUP1), cbk = rp8(pv, PB_COLUBK);
+    const uint32_t pfc = (ctrlpf & 2u) ? (x < 80u ? c0 : c1) : rp8(pv, PB_COLUPF);        // tia.rs:375-403
+    uint32_t color;
+    if (ctrlpf & 4u) color = (pf || bl) ? pfc : (p0 || m0) ? c0 : (p1 || m1) ? c1 : cbk;
+    else color = (p0 || m0) ? c0 : (p1 || m1) ? c1 : (pf || bl) ? pfc : cbk;
+    if ((s.tw & TW_HMOVE) && x < 8u) color = cbk;                 // HMOVE comb
+    const uint32_t idx = vis * FA_FB_W + x;
+    if ((idx >> 2) != s.pword || !s.pmask) {
+        render_fb_flush(s.pix, s.pmask, s.pword, fbp);
+        s.pmask = 0;
+        s.pword = idx >> 2;
+        s.pix = 0;
+    }
+    s.pix |= color << (8u * (idx & 3u));
+    s.pmask |= 1u << (idx & 3u);
+    if ((idx & 3u) == 3u) { render_fb_flush(s.pix, s.pmask, s.pword, fbp); s.pmask = 0; }
+    if (m0 | m1 | p0 | p1 | bl) {                                   // collision latches (tia.rs:329-343)
+        const uint32_t cx[8] = {
+            (m0 && p1 ? 0x80u : 0u) | (m0 && p0 ? 0x40u : 0u), (m1 && p0 ? 0x80u : 0u) | (m1 && p1 ? 0x40u : 0u),
+            (p0 && pf ? 0x80u : 0u) | (p0 && bl ? 0x40u : 0u), (p1 && pf ? 0x80u : 0u) | (p1 && bl ? 0x40u : 0u),
+            (m0 && pf ? 0x80u : 0u) | (m0 && bl ? 0x40u : 0u), (m1 && pf ? 0x80u : 0u) | (m1 && bl ? 0x40u : 0u),
+            (bl && pf ? 0x80u : 0u), (p0 && p1 ? 0x80u : 0u) | (m0 && m1 ? 0x40u : 0u) };
+#pragma unroll
+        for (uint32_t r = 0; r < 8u; r++)
+            if (cx[r]) wp8(pv, PB_CX + r, rp8(pv, PB_CX + r) | cx[r]);
+    }
+}
+
+// One TIA clock (tia.rs:271-372).
+static __device__ __forceinline__ void r_tick(RState& s, uint32_t pins, uint8_t* pv, uint8_t* fbp)
+{
+    if (s.tw & TW_LATCH) {
+        if (!(pins & 0x10000u)) s.tw &= ~TW_L4;
+        if (!(pins & 0x20000u)) s.tw &= ~TW_L5;
+    }
+    if (!(s.tw & 0x200u) && s.scanline >= 23u && s.scanline < (s.vtop >> 16)) s.vtop = (s.vtop & 0xFFFFu) | (s.scanline << 16);
+    const uint32_t dlen = rp8(pv, RB_DLEN);
+    if (dlen) {
+        uint32_t dst = 0;
+        for (uint32_t i = 0; i < dlen; i++) {
+            const uint32_t rem = rp8(pv, RB_DQ + 3u * i) - 1u, reg = rp8(pv, RB_DQ + 3u * i + 1u), val = rp8(pv, RB_DQ + 3u * i + 2u);
+            if (rem == 0) {
+                wp8(pv, reg == 0x0Du ? PB_PF0 : reg == 0x0Eu ? PB_PF1 : PB_PF2, val);
+            } else {
+                wp8(pv, RB_DQ + 3u * dst, rem);
+                wp8(pv, RB_DQ + 3u * dst + 1u, reg);
+                wp8(pv, RB_DQ + 3u * dst + 2u, val);
+                dst++;
+            }
+        }
+        wp8(pv, RB_DLEN, dst);
+    }
+    const uint32_t px = (s.clock - 68u) & 0xFFFFu;
+    const uint32_t vis = (s.scanline - (s.vtop & 0xFFFFu)) & 0xFFFFu;
+    if (s.clock >= 68u && px < FA_FB_W && !(s.tw & 0x200u) && vis < FA_FB_H) r_pixel(s, pv, fbp, vis, px);
+    s.clock++;
+    if (s.clock >= 228u) {
+        s.clock = 0;
+        s.scanline = (s.scanline + 1u) & 0xFFFFu;
+        s.tw &= ~(TW_WSYNC | TW_HMOVE);
+        if (s.scanline == (s.vtop & 0xFFFFu)) {                  // framebuffer cleared (tia.rs:349-351)
+            s.pmask = 0;
+            uint4* w = (uint4*)fbp;
+            for (uint32_t q = 0; q < FA_FB_BYTES / 16u; q++) w[q] = make_uint4(0u, 0u, 0u, 0u);
+        }
+        if (!(s.tw & TW_PDUMP) && s.pcnt < 256u) s.pcnt++;
+        if (s.scanline >= 262u) { s.scanline = 0; s.tw |= TW_FCOMP; }
+    }
+}
+
+static __device__ __forceinline__ void r_pia_tick(RState& s)     // pia.rs:80-103
+{
+    if (s.tv == 0 && s.uf) { s.tv = 0xFFu; return; }
+    s.ps = (s.ps - 1u) & 0xFFFFu;
+    if (s.ps == 0) {
+        s.ps = s.uf ? 1u : s.sel;
+        if (s.tv == 0) { s.uf = 1; s.tv = 0xFFu; } else s.tv -= 1u;
+    }
+}
+
+// n CPU cycles of the rendering console: three TIA clocks and one PIA clock each.
+static __device__ __noinline__ RState render_cycles(RState s, uint32_t n, uint32_t pins, uint8_t* pv, uint8_t* fbp)
+{
+    for (uint32_t c = 0; c < n; c++) {
+        r_tick(s, pins, pv, fbp);
+        r_tick(s, pins, pv, fbp);
+        r_tick(s, pins, pv, fbp);
+        r_pia_tick(s);
+    }
+    return s;
+}
+
+// n TIA clocks alone (the clocks around a write, src/atari.rs:207-222).
+static __device__ __noinline__ RState render_tia_ticks(RState s, uint32_t n, uint32_t pins, uint8_t* pv, uint8_t* fbp)
+{
+    for (uint32_t c = 0; c < n; c++) r_tick(s, pins, pv, fbp);
+    return s;
+}
+
+static __device__ __forceinline__ uint32_t r_resp_player(uint32_t clk)       // tia.rs:512-520
+{
+    const uint32_t dc = (clk + (clk < 68u ? 3u : 4u) + 156u) % 228u;
+    return dc >= 68u ? dc - 68u : dc + 160u - 68u;
+}
+
+static __device__ __forceinline__ void r_resize_commit(RState& s, uint8_t* pv)  // tia.rs:247-268
+{
+    const uint32_t vbt = s.vtop >> 16, top = s.vtop & 0xFFFFu;
+    if (vbt > 262u) return;
+    const uint32_t clamped = vbt < 23u ? 23u : vbt > 32u ? 32u : vbt;
+    const uint32_t cand = clamped < top ? clamped : top;
+    uint32_t ntop = top;
+    const uint32_t ptop = rp16(pv, RB_PTOP), pfr = rp8(pv, RB_PFRAMES);
+    if (cand != ptop) { wp16(pv, RB_PTOP, cand); wp8(pv, RB_PFRAMES, 3u); }
+    else if (pfr > 0) { wp8(pv, RB_PFRAMES, pfr - 1u); if (pfr == 1u) ntop = ptop; }
+    s.vtop = ntop | (ntop << 16);
+}
+
+// Tia::write (tia.rs:570-674) of register a & 0x3F.
+static __device__ __noinline__ RState render_write(uint32_t a, uint32_t v, RState s, uint8_t* pv, uint8_t* fbp)
+{
+    (void)fbp;
+    switch (a & 0x3Fu) {
+    case 0x00:
+        if (!(s.tw & 2u) && (v & 2u)) { r_resize_commit(s, pv); s.scanline = 0; s.tw |= TW_FCOMP; }
+        s.tw = (s.tw & ~0xFFu) | v;
+        break;
+    case 0x01:
+        if (v & 0x40u) s.tw |= TW_LATCH | TW_L4 | TW_L5;
+        else s.tw &= ~TW_LATCH;
+        if (v & 0x80u) { s.pcnt = 0; s.tw |= TW_PDUMP; }
+        else s.tw &= ~TW_PDUMP;
+        s.tw = (s.tw & ~0xFF00u) | (v << 8);
+        break;
+    case 0x02: s.tw |= TW_WSYNC; break;
+    case 0x04: wp8(pv, PB_NUSIZ0, v); break;
+    case 0x05: wp8(pv, PB_NUSIZ1, v); break;
+    case 0x06: wp8(pv, PB_COLUP0, v); break;
+    case 0x07: wp8(pv, PB_COLUP1, v); break;
+    case 0x08: wp8(pv, PB_COLUPF, v); break;
+    case 0x09: wp8(pv, PB_COLUBK, v); break;
+    case 0x0A: wp8(pv, PB_CTRLPF, v); break;
+    case 0x0B: wp8(pv, PB_REFP0, (v & 8u) ? 1u : 0u); break;
+    case 0x0C: wp8(pv, PB_REFP1, (v & 8u) ? 1u : 0u); break;
+    case 0x0D: case 0x0E: case 0x0F: {                              // written after one TIA clock
+        const uint32_t n = rp8(pv, RB_DLEN);
+        if (n < 4u) {
+            wp8(pv, RB_DQ + 3u * n, 1u);
+            wp8(pv, RB_DQ + 3u * n + 1u, a & 0x3Fu);
+            wp8(pv, RB_DQ + 3u * n + 2u, v);
+            wp8(pv, RB_DLEN, n + 1u);
+        } else {
+            wp8(pv, (a & 0x3Fu) == 0x0Du ? PB_PF0 : (a & 0x3Fu) == 0x0Eu ? PB_PF1 : PB_PF2, v);
+        }
+        break;
+    }
+    case 0x10: wp16(pv, PB_POS + 0u, r_resp_player(s.clock)); break;
+    case 0x11: wp16(pv, PB_POS + 2u, r_resp_player(s.clock)); break;
+    case 0x12: wp16(pv, PB_POS + 4u, mod160((int)s.clock - 68 + 5)); break;
+    case 0x13: wp16(pv, PB_POS + 6u, mod160((int)s.clock - 68 + 5)); break;
+    case 0x14: wp16(pv, PB_POS + 8u, mod160((int)s.clock - 68 + 5)); break;
+    case 0x1B: wp8(pv, PB_GRP0_OLD, rp8(pv, PB_GRP0)); wp8(pv, PB_GRP0, v); break;
+    case 0x1C: wp8(pv, PB_GRP1_OLD, rp8(pv, PB_GRP1)); wp8(pv, PB_GRP1, v); wp8(pv, PB_ENABL_OLD, rp8(pv, PB_ENABL)); break;
+    case 0x1D: wp8(pv, PB_ENAM0, (v & 2u) ? 1u : 0u); break;
+    case 0x1E: wp8(pv, PB_ENAM1, (v & 2u) ? 1u : 0u); break;
+    case 0x1F: wp8(pv, PB_ENABL, (v & 2u) ? 1u : 0u); break;
+    case 0x20: case 0x21: case 0x22: case 0x23: case 0x24: wp8(pv, PB_HM + ((a & 0x3Fu) - 0x20u), v); break;
+    case 0x25: wp8(pv, PB_VDELP0, v & 1u); break;
+    case 0x26: wp8(pv, PB_VDELP1, v & 1u); break;
+    case 0x27: wp8(pv, PB_VDELBL, v & 1u); break;
+    case 0x28: wp8(pv, PB_RESMP0, (v & 2u) ? 1u : 0u); break;
+    case 0x29: wp8(pv, PB_RESMP1, (v & 2u) ? 1u : 0u); break;
+    case 0x2A:                                                      // HMOVE
+        for (uint32_t o = 0; o < 5u; o++) {
+            const int hm = (int)(int8_t)(uint8_t)rp8(pv, PB_HM + o) >> 4;
+            wp16(pv, PB_POS + 2u * o, mod160((int)rp16(pv, PB_POS + 2u * o) - hm));
+        }
+        s.tw |= TW_HMOVE;
+        break;
+    case 0x2B: for (uint32_t o = 0; o < 5u; o++) wp8(pv, PB_HM + o, 0u); break;
+    case 0x2C: for (uint32_t o = 0; o < 8u; o++) wp8(pv, PB_CX + o, 0u); break;
+    default: break;                                                 // RSYNC, audio
+    }
+    return s;
+}
+
+// Tia::read (tia.rs:533-566) or Pia::read of an I/O register (pia.rs:169-199);
+// .y = 1 when the read clears the timer's underflow flag (INTIM).
+static __device__ __noinline__ uint2 render_read(uint32_t a, RState s, uint32_t pins, uint32_t pads, uint32_t ports,
+                                                 const uint8_t* pv)
+{
+    if ((a & 0x1080u) == 0) {
+        const uint32_t r = a & 0x0Fu;
+        if (r < 8u) return make_uint2(rp8(pv, PB_CX + r), 0u);
+        switch (r) {
+        case 0x8: return make_uint2(s.pcnt >= (pads & 0xFFu) ? 0x80u : 0u, 0u);
+        case 0x9: return make_uint2(s.pcnt >= ((pads >> 8) & 0xFFu) ? 0x80u : 0u, 0u);
+        case 0xA: case 0xB: return make_uint2(0x80u, 0u);
+        case 0xC: return make_uint2((s.tw & TW_LATCH) ? ((s.tw & TW_L4) ? 0x80u : 0u) : ((pins & 0x10000u) ? 0x80u : 0u), 0u);
+        case 0xD: return make_uint2((s.tw & TW_LATCH) ? ((s.tw & TW_L5) ? 0x80u : 0u) : ((pins & 0x20000u) ? 0x80u : 0u), 0u);
+        default: return make_uint2(0u, 0u);
+        }
+    }
+    switch (a & 7u) {
+    case 0: { const uint32_t ddr = (ports >> 8) & 0xFFu; return make_uint2(((pins & 0xFFu) & ~ddr) | (ports & ddr & 0xFFu), 0u); }
+    case 1: return make_uint2((ports >> 8) & 0xFFu, 0u);
+    case 2: { const uint32_t ddr = ports >> 24; return make_uint2((((pins >> 8) & 0xFFu) & ~ddr) | ((ports >> 16) & ddr & 0xFFu), 0u); }
+    case 3: return make_uint2(ports >> 24, 0u);
+    case 4: return make_uint2(s.tv & 0xFFu, 1u);
+    case 5: return make_uint2(s.uf ? 0x80u : 0u, 0u);
+    default: return make_uint2(0u, 0u);
+    }
+}
+
+template <int BLOCK, bool RENDER = false>
 struct Emu {
     // ---- placement
     uint8_t* pv;             // this thread's RAM (shared memory, interleaved by thread)
@@ -281,20 +584,41 @@ struct Emu {
         }
     }
 
-    // ------------------------------------------------------------ bus (atari.rs:497-552)
-    // ROM, RAM and hotspots are handled inline; TIA and PIA registers go
-    // through one out-of-line copy of their decoders (io_read / tia_write_io /
-    // pia_write_io), which keeps the interpreter's code small enough to stay
-    // resident in the instruction cache.
-    __device__ __forceinline__ uint32_t io(uint32_t a)               // TIA or PIA register read
+    // ------------------------------------------------------------ bus
+    // Every access carries j, its cycle within the instruction: the
+    // reference's CPU makes exactly one bus access per cycle (src/cpu.rs).
+    // The headless console (atari.rs:497-552) ignores j: it ticks the TIA and
+    // PIA once per instruction, after it.  The rendering console (RENDER,
+    // atari.rs:195-222) ticks them up to cycle j before any access that
+    // reaches a TIA or PIA register, whose state depends on the beam, and
+    // gives writes the Bus's timing (two TIA clocks, the write, one TIA clock
+    // and the PIA clock); accesses to ROM and RAM do not depend on the beam
+    // and are ticked with the rest of the instruction.
+    // Headless: ROM, RAM and hotspots are handled inline; TIA and PIA
+    // registers go through one out-of-line copy of their decoders (io_read /
+    // tia_write_io / pia_write_io), which keeps the interpreter's code small
+    // enough to stay resident in the instruction cache.
+    __device__ __forceinline__ uint32_t io(uint32_t a, uint32_t j)   // TIA or PIA register read
     {
-        uint32_t r = io_read(a, pcnt, pins, pads, ports, tv | (uf << 16), (const uint8_t*)column(), G->stride * 4u);
-        if (r & 0x100u) uf = 0;                                     // INTIM read clears the flag
-        return r & 0xFFu;
+        if constexpr (RENDER) {
+            rsync(j);
+            const uint32_t v = r_io_read(a);
+            rcycle();
+            done = j + 1u;
+            return v;
+        } else {
+            uint32_t r = io_read(a, pcnt, pins, pads, ports, tv | (uf << 16), (const uint8_t*)column(), G->stride * 4u);
+            if (r & 0x100u) uf = 0;                                 // INTIM read clears the flag
+            return r & 0xFFu;
+        }
     }
-    __device__ __forceinline__ void io_write(uint32_t a, uint32_t v)  // TIA or PIA register write
+    __device__ __forceinline__ void io_write(uint32_t a, uint32_t v, uint32_t j)  // TIA or PIA register write
     {
-        if (a & 0x200u) {
+        if constexpr (RENDER) {
+            rsync(j);
+            r_write_cycle(a, v);
+            done = j + 1u;
+        } else if (a & 0x200u) {
             uint4 r = pia_write_io(a, v, ports, tv, ps, sel | (uf << 16));
             ports = r.x; tv = r.y; ps = r.z; sel = r.w & 0xFFFFu; uf = r.w >> 16;
         } else {
@@ -302,51 +626,56 @@ struct Emu {
             tw = r.x; scanline = r.y & 0xFFFFu; pcnt = r.y >> 16;
         }
     }
-    __device__ __forceinline__ uint32_t read_low(uint32_t a)         // a < 0x1000
+    __device__ __forceinline__ uint32_t read_low(uint32_t a, uint32_t j)   // a < 0x1000
     {
-        if ((a & 0x80u) && (a & 0x280u) != 0x280u)                  // RAM and its mirrors
-            return a < 0x200u ? ldp(a & 0x7Fu) : 0u;                // other mirrors read the never-written flat array
-        return io(a);
+        if ((a & 0x80u) && (a & 0x280u) != 0x280u) {                // RAM and its mirrors
+            if constexpr (RENDER) return ldp(a & 0x7Fu);           // the rendering bus reads PIA RAM at every mirror
+            else return a < 0x200u ? ldp(a & 0x7Fu) : 0u;           // other mirrors read the never-written flat array
+        }
+        return io(a, j);
     }
-    __device__ __forceinline__ uint32_t read(uint32_t addr)
+    __device__ __forceinline__ uint32_t read(uint32_t addr, uint32_t j)
     {
         uint32_t a = addr & 0x1FFFu;
         if (a & 0x1000u) { bsw(a); return rom[((bank & 7u) << 12) | (a & 0xFFFu)]; }
-        return read_low(a);
+        return read_low(a, j);
     }
-    __device__ __forceinline__ void write(uint32_t addr, uint32_t v)
+    __device__ __forceinline__ void write(uint32_t addr, uint32_t v, uint32_t j)
     {
         uint32_t a = addr & 0x1FFFu;
         if (a & 0x1000u) { bsw(a); return; }
         if ((a & 0x280u) == 0x080u) { stp(a & 0x7Fu, v); return; }
-        io_write(a, v);
+        io_write(a, v, j);
     }
     // A phantom read: only its side effects (hotspot, INTIM) matter.
-    __device__ __forceinline__ void dummy(uint32_t addr)
+    __device__ __forceinline__ void dummy(uint32_t addr, uint32_t j)
     {
         uint32_t a = addr & 0x1FFFu;
         if (a & 0x1000u) bsw(a);
-        else if ((a & 0x287u) == 0x284u) uf = 0;
+        else if ((a & 0x287u) == 0x284u) {
+            if constexpr (RENDER) (void)io(a, j);
+            else uf = 0;
+        }
     }
-    __device__ __forceinline__ uint32_t zp_read(uint32_t z) { return (z & 0x80u) ? ldp(z & 0x7Fu) : io(z); }
-    __device__ __forceinline__ uint32_t fetch() { uint32_t v = read(pc); pc = (pc + 1u) & 0xFFFFu; return v; }
-    __device__ __forceinline__ void push(uint32_t v)
+    __device__ __forceinline__ uint32_t zp_read(uint32_t z, uint32_t j) { return (z & 0x80u) ? ldp(z & 0x7Fu) : io(z, j); }
+    __device__ __forceinline__ void push(uint32_t v, uint32_t j)
     {
-        if (sp & 0x80u) stp(sp & 0x7Fu, v); else io_write(0x100u | sp, v);
+        if (sp & 0x80u) stp(sp & 0x7Fu, v); else io_write(0x100u | sp, v, j);
         sp = (sp - 1u) & 0xFFu;
     }
-    __device__ __forceinline__ uint32_t pull()
+    __device__ __forceinline__ uint32_t pull(uint32_t j)
     {
         sp = (sp + 1u) & 0xFFu;
-        return (sp & 0x80u) ? ldp(sp & 0x7Fu) : io(0x100u | sp);
+        return (sp & 0x80u) ? ldp(sp & 0x7Fu) : io(0x100u | sp, j);
     }
-    // Read-modify-write's two writes; a RAM target only needs the second.
-    __device__ __forceinline__ void rmw_store(uint32_t ea, uint32_t oldv, uint32_t newv)
+    // Read-modify-write's two writes, on cycles j and j+1; a RAM target only
+    // needs the second.
+    __device__ __forceinline__ void rmw_store(uint32_t ea, uint32_t oldv, uint32_t newv, uint32_t j)
     {
         uint32_t a = ea & 0x1FFFu;
         if ((a & 0x1280u) == 0x080u) { stp(a & 0x7Fu, newv); return; }
-        write(ea, oldv);
-        write(ea, newv);
+        write(ea, oldv, j);
+        write(ea, newv, j + 1u);
     }
 
     // ------------------------------------------------------------ ALU (cpu.rs:153-241)
@@ -437,8 +766,8 @@ struct Emu {
         switch (bbb) {
         case 0: {                                                   // (zp,X)
             const uint32_t z = (b1 + x) & 0xFFu;
-            const uint32_t lo = zp_read(z);
-            ea = (zp_read((z + 1u) & 0xFFu) << 8) | lo;
+            const uint32_t lo = zp_read(z, 3);
+            ea = (zp_read((z + 1u) & 0xFFu, 4) << 8) | lo;
             cyc = 6;
             break;
         }
@@ -446,11 +775,11 @@ struct Emu {
         case 2: v = b1; cyc = 2; pc = (pc0 + 2u) & 0xFFFFu; goto operate;   // #imm ($89 is illegal)
         case 3: ea = (b2 << 8) | b1; cyc = 4; break;                // abs
         case 4: {                                                   // (zp),Y
-            const uint32_t lo = zp_read(b1);
-            const uint32_t base = (zp_read((b1 + 1u) & 0xFFu) << 8) | lo;
+            const uint32_t lo = zp_read(b1, 2);
+            const uint32_t base = (zp_read((b1 + 1u) & 0xFFu, 3) << 8) | lo;
             ea = (base + y) & 0xFFFFu;
             cyc = 5;
-            if (st || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 6; }
+            if (st || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu), 4); cyc = 6; }
             break;
         }
         case 5: ea = (b1 + x) & 0xFFu; cyc = 4; break;             // zp,X
@@ -458,13 +787,13 @@ struct Emu {
             const uint32_t base = (b2 << 8) | b1;
             ea = (base + (bbb == 6u ? y : x)) & 0xFFFFu;
             cyc = 4;
-            if (st || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 5; }
+            if (st || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu), 3); cyc = 5; }
             break;
         }
         }
         pc = (pc0 + ((bbb == 3u || bbb >= 6u) ? 3u : 2u)) & 0xFFFFu;
-        if (st) { write(ea, a); return cyc; }
-        v = read(ea);
+        if (st) { write(ea, a, cyc - 1u); return cyc; }
+        v = read(ea, cyc - 1u);
     operate:
         switch (aaa) {
         case 0: a |= v; nz(a); break;
@@ -508,20 +837,20 @@ struct Emu {
             const uint32_t base = (b2 << 8) | b1;
             if (aaa == 5u) {
                 ea = (base + y) & 0xFFFFu; cyc = 4;
-                if ((base ^ ea) & 0xFF00u) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 5; }
-                x = read(ea); nz(x); return cyc;
+                if ((base ^ ea) & 0xFF00u) { dummy((base & 0xFF00u) | (ea & 0xFFu), 3); cyc = 5; }
+                x = read(ea, cyc - 1u); nz(x); return cyc;
             }
             ea = (base + x) & 0xFFFFu;
-            dummy((base & 0xFF00u) | (ea & 0xFFu));
-            const uint32_t v = read(ea);
-            rmw_store(ea, v, shift_op(aaa, v));
+            dummy((base & 0xFF00u) | (ea & 0xFFu), 3);
+            const uint32_t v = read(ea, 4);
+            rmw_store(ea, v, shift_op(aaa, v), 5);
             return 7;
         }
         }
-        if (aaa == 4u) { write(ea, x); return cyc; }
-        if (aaa == 5u) { x = read(ea); nz(x); return cyc; }
-        const uint32_t v = read(ea);
-        rmw_store(ea, v, shift_op(aaa, v));
+        if (aaa == 4u) { write(ea, x, cyc - 1u); return cyc; }
+        if (aaa == 5u) { x = read(ea, cyc - 1u); nz(x); return cyc; }
+        const uint32_t v = read(ea, cyc - 1u);
+        rmw_store(ea, v, shift_op(aaa, v), cyc);
         return cyc + 2u;
     }
 
@@ -533,10 +862,10 @@ struct Emu {
             pc = (pc0 + 2u) & 0xFFFFu;
             const uint32_t pos = (0x1067u >> (4u * (aaa >> 1))) & 0xFu;    // N V C Z
             if (((p >> pos) & 1u) != (aaa & 1u)) return 2;
-            dummy(pc);
+            dummy(pc, 2);
             const uint32_t npc = (pc + (uint32_t)(int32_t)(int8_t)(uint8_t)b1) & 0xFFFFu;
             uint32_t cyc = 3;
-            if ((pc ^ npc) & 0xFF00u) { dummy((pc & 0xFF00u) | (npc & 0xFFu)); cyc = 4; }
+            if ((pc ^ npc) & 0xFF00u) { dummy((pc & 0xFF00u) | (npc & 0xFFu), 3); cyc = 4; }
             pc = npc;
             return cyc;
         }
@@ -556,10 +885,10 @@ struct Emu {
         case 2:                                                     // stack, DEY TAY INY INX
             pc = (pc0 + 1u) & 0xFFFFu;
             switch (aaa) {
-            case 0: push(p | F_B | F_U); return 3;                  // PHP
-            case 1: p = pull() & ~(F_B | F_U); return 4;            // PLP
-            case 2: push(a); return 3;                              // PHA
-            case 3: a = pull(); nz(a); return 4;                    // PLA
+            case 0: push(p | F_B | F_U, 2); return 3;               // PHP
+            case 1: p = pull(3) & ~(F_B | F_U); return 4;           // PLP
+            case 2: push(a, 2); return 3;                           // PHA
+            case 3: a = pull(3); nz(a); return 4;                   // PLA
             case 4: y = (y - 1u) & 0xFFu; nz(y); return 2;          // DEY
             case 5: y = a; nz(y); return 2;                         // TAY
             case 6: y = (y + 1u) & 0xFFu; nz(y); return 2;          // INY
@@ -569,28 +898,28 @@ struct Emu {
             switch (aaa) {
             case 0: {                                               // BRK (b1 is the padding byte)
                 pc = (pc0 + 2u) & 0xFFFFu;
-                push(pc >> 8); push(pc & 0xFFu); push(p | F_B | F_U);
+                push(pc >> 8, 2); push(pc & 0xFFu, 3); push(p | F_B | F_U, 4);
                 p |= F_I;
-                const uint32_t lo = read(0xFFFEu);
-                pc = (read(0xFFFFu) << 8) | lo;
+                const uint32_t lo = read(0xFFFEu, 5);
+                pc = (read(0xFFFFu, 6) << 8) | lo;
                 return 7;
             }
             case 1: {                                               // JSR: pushes before the high byte
                 pc = (pc0 + 2u) & 0xFFFFu;
-                push(pc >> 8); push(pc & 0xFFu);
-                pc = (read(pc) << 8) | b1;
+                push(pc >> 8, 3); push(pc & 0xFFu, 4);
+                pc = (read(pc, 5) << 8) | b1;
                 return 6;
             }
             case 2: {                                               // RTI
-                p = pull() & ~(F_B | F_U);
-                const uint32_t lo = pull();
-                pc = (pull() << 8) | lo;
+                p = pull(3) & ~(F_B | F_U);
+                const uint32_t lo = pull(4);
+                pc = (pull(5) << 8) | lo;
                 return 6;
             }
             case 3: {                                               // RTS
-                const uint32_t lo = pull();
-                const uint32_t ra = (pull() << 8) | lo;
-                dummy(ra);
+                const uint32_t lo = pull(3);
+                const uint32_t ra = (pull(4) << 8) | lo;
+                dummy(ra, 5);
                 pc = (ra + 1u) & 0xFFFFu;
                 return 6;
             }
@@ -605,8 +934,8 @@ struct Emu {
             if (aaa == 2u) { pc = (b2 << 8) | b1; return 3; }       // JMP
             if (aaa == 3u) {                                        // JMP (ind), page-wrap bug
                 const uint32_t ptr = (b2 << 8) | b1;
-                const uint32_t tlo = read(ptr);
-                pc = (read((ptr & 0xFF00u) | ((ptr + 1u) & 0xFFu)) << 8) | tlo;
+                const uint32_t tlo = read(ptr, 3);
+                pc = (read((ptr & 0xFF00u) | ((ptr + 1u) & 0xFFu), 4) << 8) | tlo;
                 return 5;
             }
             return mem0(aaa, (b2 << 8) | b1, 4);
@@ -621,16 +950,16 @@ struct Emu {
             const uint32_t base = (b2 << 8) | b1;
             const uint32_t ea = (base + x) & 0xFFFFu;
             uint32_t cyc = 4;
-            if ((base ^ ea) & 0xFF00u) { dummy((base & 0xFF00u) | (ea & 0xFFu)); cyc = 5; }
-            y = read(ea); nz(y);
+            if ((base ^ ea) & 0xFF00u) { dummy((base & 0xFF00u) | (ea & 0xFFu), 3); cyc = 5; }
+            y = read(ea, cyc - 1u); nz(y);
             return cyc;
         }
         }
     }
     __device__ __forceinline__ uint32_t mem0(uint32_t aaa, uint32_t ea, uint32_t cyc)
     {
-        if (aaa == 4u) { write(ea, y); return cyc; }                // STY
-        const uint32_t v = read(ea);
+        if (aaa == 4u) { write(ea, y, cyc - 1u); return cyc; }      // STY
+        const uint32_t v = read(ea, cyc - 1u);
         switch (aaa) {
         case 1: bit(v); break;
         case 5: y = v; nz(y); break;
@@ -657,17 +986,76 @@ struct Emu {
             b1 = q[1];
             b2 = q[2];
         } else {
-            op = read(pc0);
+            op = read(pc0, 0);
             if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }
-            b1 = read((pc0 + 1u) & 0xFFFFu);
+            b1 = read((pc0 + 1u) & 0xFFFFu, 1);
             const uint32_t bb = (op >> 2) & 7u;
-            if (bb == 3u || bb == 7u || (bb == 6u && (op & 3u) == 1u)) b2 = read((pc0 + 2u) & 0xFFFFu);
+            if (bb == 3u || bb == 7u || (bb == 6u && (op & 3u) == 1u)) b2 = read((pc0 + 2u) & 0xFFFFu, 2);
         }
         const uint32_t aaa = op >> 5, bbb = (op >> 2) & 7u, cc = op & 3u;
         if (cc == 1u) return group1(pc0, aaa, bbb, b1, b2);
         if (cc == 2u) return group2(pc0, aaa, bbb, b1, b2);
         return group0(pc0, aaa, bbb, b1, b2);
     }
+
+    // ------------------------------------------------------------ rendering console
+    // Used only by RENDER instantiations.  The pixel-accurate Tia of the
+    // reference's rendering console (src/tia.rs) and Pia::tick run out of
+    // line (render_cycles / render_tia_ticks / render_read / render_write,
+    // below), on the state they touch passed by value: one copy of the pixel
+    // pipeline however many bus-access sites the interpreter has.
+    uint32_t done;            // cycles of the current instruction already ticked
+    uint32_t vtop;            // visible_top | vblank_top << 16
+    uint8_t* fbp;             // this instance's framebuffer, 160 x 192 palette indices
+    uint32_t pix, pmask, pword;   // the framebuffer word being assembled: pixels, their mask, its index
+
+    __device__ __forceinline__ RState rpack() const
+    {
+        RState r;
+        r.clock = clock; r.scanline = scanline; r.tw = tw; r.pcnt = pcnt; r.vtop = vtop;
+        r.pix = pix; r.pmask = pmask; r.pword = pword; r.tv = tv; r.ps = ps; r.sel = sel; r.uf = uf;
+        return r;
+    }
+    __device__ __forceinline__ void runpack(const RState& r)
+    {
+        clock = r.clock; scanline = r.scanline; tw = r.tw; pcnt = r.pcnt; vtop = r.vtop;
+        pix = r.pix; pmask = r.pmask; pword = r.pword; tv = r.tv; ps = r.ps; sel = r.sel; uf = r.uf;
+    }
+    __device__ __forceinline__ void rsync(uint32_t j)
+    {
+        if (done < j) { runpack(render_cycles(rpack(), j - done, pins, pv, fbp)); done = j; }
+    }
+    __device__ __forceinline__ void rcycle() { runpack(render_cycles(rpack(), 1u, pins, pv, fbp)); }
+    __device__ __forceinline__ uint32_t r_io_read(uint32_t a)
+    {
+        const uint2 r = render_read(a, rpack(), pins, pads, ports, pv);
+        if (r.y) uf = 0;                                            // INTIM read clears the flag
+        return r.x;
+    }
+    // Bus::write of a TIA or PIA register (src/atari.rs:207-222).
+    __device__ __forceinline__ void r_write_cycle(uint32_t a, uint32_t v)
+    {
+        RState r = render_tia_ticks(rpack(), 2u, pins, pv, fbp);
+        if ((a & 0x1080u) != 0) {
+            const uint4 q = pia_write_io(a, v, ports, r.tv, r.ps, r.sel | (r.uf << 16));
+            ports = q.x; r.tv = q.y; r.ps = q.z; r.sel = q.w & 0xFFFFu; r.uf = q.w >> 16;
+        } else {
+            r = render_write(a, v, r, pv, fbp);
+        }
+        r = render_tia_ticks(r, 1u, pins, pv, fbp);
+        runpack(r);
+        pia_tick1();
+    }
+    __device__ __forceinline__ void pia_tick1()                      // pia.rs:80-103
+    {
+        if (tv == 0 && uf) { tv = 0xFFu; return; }
+        ps = (ps - 1u) & 0xFFFFu;
+        if (ps == 0) {
+            ps = uf ? 1u : sel;
+            if (tv == 0) { uf = 1; tv = 0xFFu; } else tv -= 1u;
+        }
+    }
+    __device__ __forceinline__ void fb_flush() { render_fb_flush(pix, pmask, pword, fbp); pmask = 0; }
 
     // HeadlessAtari::set_action (src/atari.rs:571-582).
     __device__ __forceinline__ void apply_action(uint32_t act)

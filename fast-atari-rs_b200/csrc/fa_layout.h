@@ -70,3 +70,25 @@ static inline int fa_detect_scheme(size_t len)        // BankScheme::detect, src
     return len <= 4096 ? FA_SCHEME_FIXED : len <= 8192 ? FA_SCHEME_F8
          : len <= 16384 ? FA_SCHEME_F6 : FA_SCHEME_F4;
 }
+
+// ---- rendering console (src/tia.rs, src/atari.rs:107-306)
+// Its state is the headless layout's rows (the same R_* and PB_* meaning)
+// followed by what only the pixel-accurate TIA has.  While a unit runs, the
+// private bytes [0, FA_RPRIV_BYTES) sit in shared memory: the RAM, the
+// graphics registers PB_*, and the RB_* extras, which are stored in rows
+// FA_RROW_EXTRA.. of HBM.
+enum : uint32_t {
+    RB_DLEN    = 176,          // pending playfield writes (0..4)
+    RB_DQ      = 177,          // 4 x (remaining, register, value)
+    RB_PFRAMES = 189,          // resizer: pending_frames
+    RB_PTOP    = 190,          // resizer: pending_top (u16, 2-byte aligned)
+    FA_RPRIV_BYTES = 192,
+    FA_RPRIV_WORDS = FA_RPRIV_BYTES / 4,
+    FA_RROW_EXTRA = FA_ROWS,                           // rows holding RB_* words
+    RR_VTOP  = FA_ROWS + (FA_RPRIV_WORDS - FA_PRIV_WORDS),   // visible_top | vblank_top << 16
+    RR_FLAGS = RR_VTOP + 1,    // hmove_pending | input_latch_enabled << 1 | inpt4_latch << 2 | inpt5_latch << 3
+    FA_RROWS = RR_FLAGS + 1,
+};
+#define FA_FB_W 160
+#define FA_FB_H 192
+#define FA_FB_BYTES (FA_FB_W * FA_FB_H)

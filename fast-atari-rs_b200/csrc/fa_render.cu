@@ -1,0 +1,526 @@
+// fa_render.cu — the reference's rendering console on sm_100a.
+//
+// The rendering console (src/atari.rs:107-306 with the pixel-accurate Tia of
+// src/tia.rs) differs from the headless one in time, not in instructions: its
+// bus ticks the TIA three times and the PIA once on every CPU cycle, a write
+// lands on the third TIA clock of its cycle, and every TIA clock inside the
+// visible window renders a pixel of a 160 x 192 framebuffer of palette
+// indices.  The 6502 here is the same core as the headless kernels
+// (Emu<32, true>): each of its bus accesses knows its cycle within the
+// instruction, and before an access reaches a TIA or PIA register the TIA
+// and PIA are ticked up to that cycle, so register writes land at the beam
+// position the reference gives them; the rest of the instruction's cycles
+// are ticked after it.
+//
+// One warp per unit of 32 consoles, WARPS units per CTA; the cart's ROM and
+// one private-byte slab per warp (RAM + graphics registers, FA_RPRIV_BYTES
+// per console, interleaved by lane) in shared memory; state rows in HBM
+// (the headless layout plus the rendering rows); one framebuffer per console
+// in HBM, persistent across launches (pixels the program does not redraw keep
+// their value, as in the reference).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/fast_atari.h"
+#include "fa_internal.h"
+#include "fa_run.cuh"
+
+struct FaRenderLaunch {
+    const uint8_t* rom;
+    uint32_t nbanks, hot_lo;
+    uint32_t* state;             // FA_RROWS rows of `stride` words
+    uint32_t stride, n;
+    const uint8_t* actions;      // k * n frame-major, or null (no set_action: the reset frame)
+    uint32_t k, sched;
+    uint8_t* fb;                 // n * FA_FB_BYTES
+    uint8_t* obs;                // n * 128, or null
+    uint32_t* err;
+    unsigned long long* instr;
+    unsigned long long* rounds;
+};
+
+namespace fa {
+
+// One rendering console per lane: HeadlessAtari's frame loop with the
+// rendering console's per-cycle run_one_cycle (src/atari.rs:284-318).
+struct RRunner {
+    Emu<32, true> e;
+    uint32_t f, phase, fcyc;
+    bool active;
+
+    __device__ __forceinline__ bool begin_frame()
+    {
+        const FaGroup* G = e.G;
+        if (e.row(R_STATUS) & FA_STATUS_HALT_MASK) return false;
+        if (G->actions) e.apply_action(G->actions[(size_t)f * G->act_stride + e.i]);
+        e.tw &= ~TW_FCOMP;
+        e.bank &= 7u;
+        fcyc = 0;
+        phase = e.vsync_on() ? 0u : 1u;
+        return true;
+    }
+    // One run_one_cycle: a WSYNC cycle (tick_components) or an instruction,
+    // then the frame-end checks of run_frame.
+    __device__ __forceinline__ bool one()
+    {
+        uint32_t n;
+        if (e.wsync()) {
+            e.rcycle();
+            n = 1;
+        } else {
+            e.done = 0;
+            n = e.step();
+            if (n == 0) { e.fold_cycles(); e.set_status(FA_STATUS_ILLEGAL_OPCODE); active = false; return false; }
+            e.rsync(n);
+            e.instr++;
+            e.cyc_acc += n;
+        }
+        fcyc += n;
+        if (phase == 0u) {
+            if (fcyc > FA_VSYNC_BUDGET) {
+                e.fold_cycles();
+                e.set_status(FA_STATUS_VSYNC_BUDGET);
+                active = false;
+                return false;
+            }
+            if (!e.vsync_on()) phase = 1u;
+        } else {
+            const bool cap = fcyc > FA_FRAME_CYCLE_CAP;
+            if (cap || e.vsync_on()) {
+                if (cap) e.set_status(FA_STATUS_CYCLE_CAP);
+                e.fold_cycles();
+                e.row(R_FRAME) += 1u;
+                f++;
+                if (f >= e.G->k || !begin_frame()) { active = false; return false; }
+                return false;
+            }
+        }
+        return e.wsync();
+    }
+    __device__ __forceinline__ uint32_t key(uint32_t sched) const
+    {
+        const uint32_t fc = f < 0x7Fu ? f : 0x7Fu;
+        const uint32_t mid = sched == FA_SCHED_LINE ? (e.scanline < 0x1FFu ? e.scanline : 0x1FFu) : (e.bank >> 3);
+        return (fc << 25) | (mid << 16) | e.pc;
+    }
+    // A WSYNC wait is consumed cycle by cycle, with the frame checks after
+    // each cycle, without going back to the warp scheduler.
+    __device__ __forceinline__ void iterate()
+    {
+#pragma unroll 1
+        while (one() && active) {
+        }
+    }
+};
+
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) fa_render_run(const __grid_constant__ FaRenderLaunch L)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ FaGroup sg;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t rom_bytes = L.nbanks * 4096u;
+    uint32_t* slab = (uint32_t*)(smem + rom_bytes) + warp * (FA_RPRIV_WORDS * 32u);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        FaGroup g;
+        memset(&g, 0, sizeof(g));
+        g.rom = L.rom;
+        g.state = L.state;
+        g.stride = L.stride;
+        g.n = L.n;
+        g.actions = L.actions;
+        g.act_stride = L.n;
+        g.nbanks = L.nbanks;
+        g.hot_lo = L.hot_lo;
+        g.k = L.k;
+        g.sched = L.sched;
+        g.obs = L.obs;
+        sg = g;
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    if (!stage_rom(smem, L.rom, rom_bytes, &bar, phase)) {
+        if (threadIdx.x == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
+        return;
+    }
+    const uint32_t first = (blockIdx.x * WARPS + warp) * 32u;
+    if (first >= L.n) return;
+    const uint32_t i = first + lane;
+    const bool valid = i < L.n;
+
+    RRunner r;
+    r.f = 0;
+    r.phase = 0;
+    r.fcyc = 0;
+    r.active = false;
+    Emu<32, true>& e = r.e;
+    e.pv = (uint8_t*)(slab + lane);
+    e.G = &sg;
+    e.i = i;
+    e.rom = smem;
+    e.hot_lo = L.hot_lo;
+    e.nbanks = L.nbanks;
+    e.instr = 0;
+    e.cyc_acc = 0;
+    e.pc = 0;
+    e.bank = 0;
+    e.scanline = 0;
+    e.done = 0;
+    e.pix = 0;
+    e.pmask = 0;
+    e.pword = 0;
+    e.vtop = 0;
+    e.fbp = L.fb + (size_t)(valid ? i : 0u) * FA_FB_BYTES;
+    uint32_t* col = L.state + i;
+    const uint32_t S = L.stride;
+    if (valid) {
+        uint32_t* w = slab + lane;
+#pragma unroll 4
+        for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) w[k * 32u] = col[(size_t)k * S];
+        for (uint32_t k = FA_PRIV_WORDS; k < FA_RPRIV_WORDS; k++)
+            w[k * 32u] = col[(size_t)(FA_RROW_EXTRA + (k - FA_PRIV_WORDS)) * S];
+        e.load_hot(col, S);
+        e.vtop = col[(size_t)RR_VTOP * S];
+        const uint32_t fl = col[(size_t)RR_FLAGS * S];
+        e.tw |= ((fl & 1u) ? TW_HMOVE : 0u) | ((fl & 2u) ? TW_LATCH : 0u) | ((fl & 4u) ? TW_L4 : 0u) |
+                ((fl & 8u) ? TW_L5 : 0u);
+        if (L.k > 0) r.active = r.begin_frame();
+    }
+    const uint32_t rounds = run_lanes(r, L.sched);
+    if (valid) {
+        e.fb_flush();
+        e.fold_cycles();
+        uint32_t* w = slab + lane;
+#pragma unroll 4
+        for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) col[(size_t)k * S] = w[k * 32u];
+        for (uint32_t k = FA_PRIV_WORDS; k < FA_RPRIV_WORDS; k++)
+            col[(size_t)(FA_RROW_EXTRA + (k - FA_PRIV_WORDS)) * S] = w[k * 32u];
+        e.store_hot(col, S);
+        col[(size_t)RR_VTOP * S] = e.vtop;
+        col[(size_t)RR_FLAGS * S] = ((e.tw & TW_HMOVE) ? 1u : 0u) | ((e.tw & TW_LATCH) ? 2u : 0u) |
+                                    ((e.tw & TW_L4) ? 4u : 0u) | ((e.tw & TW_L5) ? 8u : 0u);
+        if (L.obs) {
+            uint4* o = (uint4*)(L.obs + (size_t)i * 128u);
+#pragma unroll
+            for (uint32_t q = 0; q < 8u; q++)
+                o[q] = make_uint4(w[(4u * q) * 32u], w[(4u * q + 1u) * 32u], w[(4u * q + 2u) * 32u],
+                                  w[(4u * q + 3u) * 32u]);
+        }
+    }
+    if (L.instr) {
+        uint32_t c = valid ? e.instr : 0u;
+        for (int d = 16; d > 0; d >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, d);
+        if (lane == 0 && c) atomicAdd(L.instr, (unsigned long long)c);
+    }
+    if (L.rounds && lane == 0 && rounds) atomicAdd(L.rounds, 32ull * rounds);
+}
+
+}  // namespace fa
+
+// ------------------------------------------------------------------ host side
+struct fa_render {
+    int device = 0;
+    size_t n = 0;
+    uint32_t stride = 0;
+    int scheme = 0;
+    uint32_t nbanks = 1, hot_lo = 0x2000;
+    std::vector<uint8_t> image;
+    uint8_t* d_rom = nullptr;
+    uint32_t* d_state = nullptr;
+    uint8_t* d_fb = nullptr;
+    uint8_t* d_actions = nullptr;
+    size_t actions_cap = 0;
+    uint8_t* d_obs = nullptr;
+    uint32_t* d_err = nullptr;
+    unsigned long long* d_ctr = nullptr;
+    cudaStream_t stream = nullptr;
+    int warps = 8;
+    int sched = FA_SCHED_PC;
+    bool reset_done = false;
+    unsigned long long last_instr = 0, last_slots = 0;
+};
+
+namespace {
+std::mutex g_rmu;
+std::map<std::pair<int, int>, bool> g_rcfg;   // (device, warps) whose smem limit was raised
+
+template <int WARPS>
+cudaError_t launch_render(const FaRenderLaunch& L, cudaStream_t s)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const size_t smem = (size_t)L.nbanks * 4096u + (size_t)WARPS * FA_RPRIV_WORDS * 32u * 4u;
+    {
+        std::lock_guard<std::mutex> lk(g_rmu);
+        auto key = std::make_pair(dev, WARPS);
+        if (g_rcfg.find(key) == g_rcfg.end()) {
+            e = cudaFuncSetAttribute(fa::fa_render_run<WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     32768 + WARPS * FA_RPRIV_WORDS * 32 * 4);
+            if (e != cudaSuccess) return e;
+            g_rcfg[key] = true;
+        }
+    }
+    const uint32_t units = (L.n + 31u) / 32u;
+    const uint32_t grid = (units + WARPS - 1u) / WARPS;
+    if (grid == 0) return cudaSuccess;
+    fa::fa_render_run<WARPS><<<grid, WARPS * 32, smem, s>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_render_n(int warps, const FaRenderLaunch& L, cudaStream_t s)
+{
+    switch (warps) {
+    case 4: return launch_render<4>(L, s);
+    case 8: return launch_render<8>(L, s);
+    case 16: return launch_render<16>(L, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+void free_render(fa_render* r)
+{
+    if (!r) return;
+    cudaSetDevice(r->device);
+    if (r->stream) cudaStreamSynchronize(r->stream);
+    cudaFree(r->d_rom);
+    cudaFree(r->d_state);
+    cudaFree(r->d_fb);
+    cudaFree(r->d_actions);
+    cudaFree(r->d_obs);
+    cudaFree(r->d_err);
+    cudaFree(r->d_ctr);
+    if (r->stream) cudaStreamDestroy(r->stream);
+    delete r;
+}
+
+// Atari::new (src/atari.rs:240-247) as one state column: the headless power-on
+// column with the rendering Tia's defaults (src/tia.rs:192-238), then the two
+// bus reads of Cpu::reset (src/cpu.rs:125-134), which each tick three TIA
+// clocks (in horizontal blank of scanline 0: nothing renders) and one PIA clock.
+void render_power_on(const fa_render* r, std::vector<uint32_t>& col)
+{
+    col.assign(FA_RROWS, 0u);
+    fa_power_on_column(r->image.data(), r->nbanks, r->scheme, col.data());
+    fa_state s;
+    fa_unpack_column(col.data(), 1, r->scheme, s);
+    s.paddle0 = 128;
+    s.paddle1 = 128;
+    s.tia_clock = 6;
+    // Pia::tick twice from its default (timer 0, prescaler 1, select 1).
+    uint32_t tv = s.timer_value, ps = s.timer_prescaler, sel = s.timer_prescaler_select, uf = s.timer_underflow;
+    for (int c = 0; c < 2; c++) {
+        if (tv == 0 && uf) { tv = 0xFF; continue; }
+        ps = (ps - 1u) & 0xFFFFu;
+        if (ps == 0) {
+            ps = uf ? 1u : sel;
+            if (tv == 0) { uf = 1; tv = 0xFF; } else tv -= 1u;
+        }
+    }
+    s.timer_value = (uint16_t)tv;
+    s.timer_prescaler = (uint16_t)ps;
+    s.timer_underflow = (uint8_t)uf;
+    fa_pack_column(s, col.data(), 1);
+    // Rendering rows: pending_top 32 (RB_PTOP in the RB_* words), visible_top 32,
+    // vblank_top 262, input latches 0x80.
+    uint8_t rb[FA_RPRIV_BYTES - FA_PRIV_BYTES] = {};
+    rb[RB_PTOP - FA_PRIV_BYTES] = 32;
+    for (uint32_t w = 0; w < (FA_RPRIV_WORDS - FA_PRIV_WORDS); w++) memcpy(&col[FA_RROW_EXTRA + w], rb + 4 * w, 4);
+    col[RR_VTOP] = 32u | (262u << 16);
+    col[RR_FLAGS] = 4u | 8u;
+}
+
+int enqueue(fa_render* r, const uint8_t* d_actions, int k, uint8_t* d_obs, cudaStream_t s)
+{
+    FaRenderLaunch L;
+    memset(&L, 0, sizeof(L));
+    L.rom = r->d_rom;
+    L.nbanks = r->nbanks;
+    L.hot_lo = r->hot_lo;
+    L.state = r->d_state;
+    L.stride = r->stride;
+    L.n = (uint32_t)r->n;
+    L.actions = d_actions;
+    L.k = (uint32_t)k;
+    L.sched = (uint32_t)r->sched;
+    L.fb = r->d_fb;
+    L.obs = d_obs;
+    L.err = r->d_err;
+    L.instr = r->d_ctr;
+    L.rounds = r->d_ctr + 1;
+    FA_CUDA(launch_render_n(r->warps, L, s));
+    return FA_OK;
+}
+
+int finish(fa_render* r)
+{
+    FA_CUDA(cudaStreamSynchronize(r->stream));
+    uint32_t err = 0;
+    FA_CUDA(cudaMemcpy(&err, r->d_err, sizeof(err), cudaMemcpyDeviceToHost));
+    unsigned long long ctr[2];
+    FA_CUDA(cudaMemcpy(ctr, r->d_ctr, sizeof(ctr), cudaMemcpyDeviceToHost));
+    r->last_instr = ctr[0];
+    r->last_slots = ctr[1];
+    if (err) {
+        cudaMemset(r->d_err, 0, sizeof(uint32_t));
+        return fa_fail(FA_ERR_KERNEL, "device wait gave up (error word 0x%x)", err);
+    }
+    return FA_OK;
+}
+
+int copy_out(fa_render* r, uint8_t* fb_out, uint8_t* ram_out)
+{
+    if (fb_out) FA_CUDA(cudaMemcpy(fb_out, r->d_fb, r->n * (size_t)FA_FB_BYTES, cudaMemcpyDeviceToHost));
+    if (ram_out) FA_CUDA(cudaMemcpy(ram_out, r->d_obs, r->n * 128u, cudaMemcpyDeviceToHost));
+    return FA_OK;
+}
+}  // namespace
+
+#define CHECK_R(r)                                                                      \
+    do {                                                                                \
+        if (!(r)) return fa_fail(FA_ERR_INVALID, "null render handle");                 \
+        cudaError_t e_ = cudaSetDevice((r)->device);                                    \
+        if (e_ != cudaSuccess) return fa_fail(FA_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" int fa_render_create(const uint8_t* rom, size_t rom_len, size_t n, fa_render** out)
+{
+    if (!out) return fa_fail(FA_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!rom || n == 0) return fa_fail(FA_ERR_INVALID, "need a ROM and n >= 1");
+    if (n > (size_t)UINT32_MAX / 2) return fa_fail(FA_ERR_CAPACITY, "too many instances");
+    if (fa_device_count() < 1) return fa_fail(FA_ERR_NO_DEVICE, "no CUDA device visible");
+    fa_render* r = new (std::nothrow) fa_render();
+    if (!r) return fa_fail(FA_ERR_CAPACITY, "out of host memory");
+    int rc = fa_make_bank_image(rom, rom_len, r->image, r->scheme);
+    if (rc) { delete r; return rc; }
+    cudaGetDevice(&r->device);
+    r->n = n;
+    r->stride = (uint32_t)((n + 31u) & ~(size_t)31u);
+    r->nbanks = fa_nbanks(r->scheme);
+    r->hot_lo = fa_hot_lo(r->scheme);
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaMalloc(&r->d_rom, r->image.size())) != cudaSuccess ||
+        (e = cudaMemcpy(r->d_rom, r->image.data(), r->image.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&r->d_state, (size_t)FA_RROWS * r->stride * 4u)) != cudaSuccess ||
+        (e = cudaMemset(r->d_state, 0, (size_t)FA_RROWS * r->stride * 4u)) != cudaSuccess ||
+        (e = cudaMalloc(&r->d_fb, n * (size_t)FA_FB_BYTES)) != cudaSuccess ||
+        (e = cudaMemset(r->d_fb, 0, n * (size_t)FA_FB_BYTES)) != cudaSuccess ||
+        (e = cudaMalloc(&r->d_obs, n * 128u)) != cudaSuccess ||
+        (e = cudaMalloc(&r->d_err, sizeof(uint32_t))) != cudaSuccess ||
+        (e = cudaMemset(r->d_err, 0, sizeof(uint32_t))) != cudaSuccess ||
+        (e = cudaMalloc(&r->d_ctr, 2 * sizeof(unsigned long long))) != cudaSuccess) {
+        free_render(r);
+        return fa_fail(FA_ERR_CUDA, "render allocation: %s", cudaGetErrorString(e));
+    }
+    // Until reset, every console is halted (as fa_create's NOT_RESET state).
+    std::vector<uint32_t> st((size_t)r->stride, FA_STATUS_NOT_RESET);
+    e = cudaMemcpy(r->d_state + (size_t)R_STATUS * r->stride, st.data(), st.size() * 4u, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { free_render(r); return fa_fail(FA_ERR_CUDA, "render init: %s", cudaGetErrorString(e)); }
+    *out = r;
+    return FA_OK;
+}
+
+extern "C" void fa_render_destroy(fa_render* r) { free_render(r); }
+
+extern "C" int fa_render_set_launch(fa_render* r, int cta_warps, int sched)
+{
+    if (!r) return fa_fail(FA_ERR_INVALID, "null render handle");
+    if (cta_warps != 4 && cta_warps != 8 && cta_warps != 16) return fa_fail(FA_ERR_INVALID, "cta_warps must be 4, 8 or 16");
+    if (sched < FA_SCHED_LANE || sched > FA_SCHED_MATCH) return fa_fail(FA_ERR_INVALID, "bad sched %d", sched);
+    r->warps = cta_warps;
+    r->sched = sched;
+    return FA_OK;
+}
+
+extern "C" int fa_render_reset(fa_render* r, uint8_t* fb_out, uint8_t* ram_out)
+{
+    CHECK_R(r);
+    std::vector<uint32_t> col;
+    render_power_on(r, col);
+    std::vector<uint32_t> rows((size_t)FA_RROWS * r->stride);
+    for (uint32_t w = 0; w < FA_RROWS; w++)
+        for (size_t i = 0; i < r->n; i++) rows[(size_t)w * r->stride + i] = col[w];
+    FA_CUDA(cudaMemcpyAsync(r->d_state, rows.data(), rows.size() * 4u, cudaMemcpyHostToDevice, r->stream));
+    FA_CUDA(cudaMemsetAsync(r->d_fb, 0, r->n * (size_t)FA_FB_BYTES, r->stream));
+    FA_CUDA(cudaMemsetAsync(r->d_ctr, 0, 2 * sizeof(unsigned long long), r->stream));
+    // One frame without set_action, as the batched reset does.
+    int rc = enqueue(r, nullptr, 1, r->d_obs, r->stream);
+    if (rc) return rc;
+    rc = finish(r);
+    if (rc) return rc;
+    // The reset frame is not counted: frame numbers restart at 0.
+    FA_CUDA(cudaMemset(r->d_state + (size_t)R_FRAME * r->stride, 0, r->n * 4u));
+    r->reset_done = true;
+    return copy_out(r, fb_out, ram_out);
+}
+
+extern "C" int fa_render_step_multi_async(fa_render* r, const uint8_t* d_actions, int k, uint8_t* d_obs, void* stream)
+{
+    CHECK_R(r);
+    if (!d_actions || k < 1) return fa_fail(FA_ERR_INVALID, "actions null or k < 1");
+    if (((uintptr_t)d_obs & 15u) != 0) return fa_fail(FA_ERR_INVALID, "d_obs must be 16-byte aligned");
+    return enqueue(r, d_actions, k, d_obs, stream ? (cudaStream_t)stream : r->stream);
+}
+
+extern "C" int fa_render_step_multi(fa_render* r, const uint8_t* actions, int k, uint8_t* fb_out, uint8_t* ram_out)
+{
+    CHECK_R(r);
+    if (!actions || k < 1) return fa_fail(FA_ERR_INVALID, "actions null or k < 1");
+    const size_t bytes = (size_t)k * r->n;
+    if (bytes > r->actions_cap) {
+        cudaFree(r->d_actions);
+        r->d_actions = nullptr;
+        r->actions_cap = 0;
+        FA_CUDA(cudaMalloc(&r->d_actions, bytes));
+        r->actions_cap = bytes;
+    }
+    FA_CUDA(cudaMemcpyAsync(r->d_actions, actions, bytes, cudaMemcpyHostToDevice, r->stream));
+    FA_CUDA(cudaMemsetAsync(r->d_ctr, 0, 2 * sizeof(unsigned long long), r->stream));
+    int rc = enqueue(r, r->d_actions, k, r->d_obs, r->stream);
+    if (rc) return rc;
+    rc = finish(r);
+    if (rc) return rc;
+    return copy_out(r, fb_out, ram_out);
+}
+
+extern "C" int fa_render_synchronize(fa_render* r)
+{
+    CHECK_R(r);
+    return finish(r);
+}
+
+extern "C" size_t fa_render_num_envs(const fa_render* r) { return r ? r->n : 0; }
+
+extern "C" uint8_t* fa_render_device_framebuffers(fa_render* r) { return r ? r->d_fb : nullptr; }
+
+extern "C" int fa_render_get_framebuffers(fa_render* r, uint8_t* out)
+{
+    CHECK_R(r);
+    if (!out) return fa_fail(FA_ERR_INVALID, "out is null");
+    FA_CUDA(cudaStreamSynchronize(r->stream));
+    FA_CUDA(cudaMemcpy(out, r->d_fb, r->n * (size_t)FA_FB_BYTES, cudaMemcpyDeviceToHost));
+    return FA_OK;
+}
+
+extern "C" int fa_render_get_states(fa_render* r, fa_state* out)
+{
+    CHECK_R(r);
+    if (!out) return fa_fail(FA_ERR_INVALID, "out is null");
+    FA_CUDA(cudaStreamSynchronize(r->stream));
+    std::vector<uint32_t> rows((size_t)FA_RROWS * r->stride);
+    FA_CUDA(cudaMemcpy(rows.data(), r->d_state, rows.size() * 4u, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < r->n; i++) fa_unpack_column(rows.data() + i, r->stride, r->scheme, out[i]);
+    return FA_OK;
+}
+
+extern "C" unsigned long long fa_render_last_instructions(const fa_render* r) { return r ? r->last_instr : 0ull; }

@@ -174,8 +174,8 @@ struct Runner {
 // Instructions a converged group may run per scheduling round.
 constexpr uint32_t FA_STEPS_PER_ROUND = 32;
 
-template <int BLOCK>
-__device__ __forceinline__ uint32_t run_lanes(Runner<BLOCK>& r, uint32_t sched)
+template <class RUNNER>
+__device__ __forceinline__ uint32_t run_lanes(RUNNER& r, uint32_t sched)
 {
     const uint32_t FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
@@ -274,7 +274,7 @@ __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint3
         r.e.load_hot(col, G.stride);
         if (G.k > 0) r.active = r.begin_frame();
     }
-    const uint32_t rounds = run_lanes<BLOCK>(r, G.sched);
+    const uint32_t rounds = run_lanes(r, G.sched);
     if (valid) {
         r.e.fold_cycles();
         r.e.store_ram(col, G.stride);

@@ -443,6 +443,44 @@ typedef struct fa_loadgen_result {
 
 int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_loadgen_result* out, float* latency_ms);
 
+/* ------------------------------------------------------------ rendering
+ * The reference's rendering console (Atari, src/atari.rs:107-306, with the
+ * pixel-accurate Tia of src/tia.rs): every CPU bus access ticks the TIA three
+ * times and the PIA once, writes land on the third TIA clock of their cycle,
+ * and each TIA clock inside the visible window renders one pixel of a
+ * 160 x 192 framebuffer of NTSC palette indices (Atari::framebuffer).  One
+ * console per GPU thread, as the headless core; framebuffers stay on the
+ * device between calls (FA_FB_BYTES = 30,720 bytes per console).  The
+ * reference renders one console per call on the CPU; the batched form and
+ * this API have no counterpart there.
+ */
+#define FA_FB_WIDTH  160
+#define FA_FB_HEIGHT 192
+typedef struct fa_render fa_render;
+/* n rendering consoles of one ROM on the current device (lengths as fa_create). */
+int  fa_render_create(const uint8_t* rom, size_t rom_len, size_t n, fa_render** out);
+void fa_render_destroy(fa_render* r);
+size_t fa_render_num_envs(const fa_render* r);
+/* CTA size in warps (4, 8 or 16) and warp policy (FA_SCHED_*). */
+int  fa_render_set_launch(fa_render* r, int cta_warps, int sched);
+/* Every console becomes Atari::new(rom) followed by one run_frame() without
+ * an action.  fb_out (n * 160 * 192 bytes) and ram_out (n * 128) may be NULL. */
+int  fa_render_reset(fa_render* r, uint8_t* fb_out, uint8_t* ram_out);
+/* k frames per console (actions frame-major, k * n bytes, set_action before
+ * each frame); fb_out receives the framebuffers after the last frame,
+ * ram_out the RAM (either may be NULL). */
+int  fa_render_step_multi(fa_render* r, const uint8_t* actions, int k, uint8_t* fb_out, uint8_t* ram_out);
+/* Device-buffer variant on `stream` (NULL: the handle's stream); d_obs
+ * (n * 128, 16-byte aligned, or NULL) receives the RAM. */
+int  fa_render_step_multi_async(fa_render* r, const uint8_t* d_actions, int k, uint8_t* d_obs, void* stream);
+int  fa_render_synchronize(fa_render* r);
+/* The device framebuffers (n * FA_FB_WIDTH * FA_FB_HEIGHT bytes, console-major). */
+uint8_t* fa_render_device_framebuffers(fa_render* r);
+int  fa_render_get_framebuffers(fa_render* r, uint8_t* out);
+/* CPU, RAM, PIA and TIA register state (fa_state layout; cycles, frame_no, run_status). */
+int  fa_render_get_states(fa_render* r, fa_state* out);
+unsigned long long fa_render_last_instructions(const fa_render* r);
+
 /* -------------------------------------------------- no-allocation stepping
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (device memory owned by another allocator, or a stepping loop that must not

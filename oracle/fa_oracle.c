@@ -825,3 +825,493 @@ int orc_flat_run(uint8_t* mem64k, int nsteps, uint8_t* cycles_out, orc_regs* r)
 }
 
 size_t orc_state_size(void) { return sizeof(fa_state); }
+
+/* ======================================================== rendering console
+ * The reference's rendering path, restated: the pixel-accurate Tia
+ * (src/tia.rs), the per-cycle Bus (src/atari.rs:107-225), the Atari console
+ * (src/atari.rs:227-306) and Pia::tick (src/pia.rs:80-103).  The 6502 issues
+ * one bus access per cycle (cpu_step.h); every access ticks the TIA three
+ * times and the PIA once, and a write lands on the third TIA clock of its
+ * cycle (the Gopher2600 timing of Bus::write, src/atari.rs:206-222). */
+
+#define R_FRAME_W 160
+#define R_FRAME_H 192
+#define R_EXT_TOP 23                 /* tia.rs:84-86 */
+#define R_IDEAL_TOP 32
+#define R_RESIZE_FRAMES 3
+#define R_DELAYED_CAP 4              /* tia.rs:89 */
+
+typedef struct { uint8_t remaining, reg, value; } orc_delayed;
+
+typedef struct orc_rtia {            /* Tia, tia.rs:98-190 */
+    uint16_t clock, scanline;
+    uint8_t  wsync, hmove_pending;
+    uint16_t visible_top, vblank_top, pending_top;
+    uint8_t  pending_frames;
+    orc_delayed delayed[R_DELAYED_CAP];
+    uint8_t  delayed_len;
+    uint8_t  frame_complete;
+    uint8_t  vsync, vblank, colup0, colup1, colupf, colubk, ctrlpf, refp0, refp1, pf0, pf1, pf2;
+    uint8_t  grp0, grp1, grp0_old, grp1_old, enam0, enam1, enabl, enabl_old;
+    uint8_t  hmp0, hmp1, hmm0, hmm1, hmbl, nusiz0, nusiz1, vdelp0, vdelp1, vdelbl, resmp0, resmp1;
+    uint16_t pos_p0, pos_p1, pos_m0, pos_m1, pos_bl;
+    uint8_t  cxm0p, cxm1p, cxp0fb, cxp1fb, cxm0fb, cxm1fb, cxblpf, cxppmm;
+    uint8_t  paddle0, paddle1;
+    uint16_t paddle_counter;
+    uint8_t  paddle_dumped;
+    uint8_t  inpt4, inpt5, inpt4_latch, inpt5_latch, input_latch_enabled;
+    uint8_t  fb[R_FRAME_W * R_FRAME_H];
+} orc_rtia;
+
+static void orc_rtia_default(orc_rtia* t)                          /* tia.rs:192-238 */
+{
+    memset(t, 0, sizeof(*t));
+    t->visible_top = R_IDEAL_TOP;
+    t->vblank_top = 262;
+    t->pending_top = R_IDEAL_TOP;
+    t->paddle0 = 128;
+    t->paddle1 = 128;
+    t->inpt4 = 1;
+    t->inpt5 = 1;
+    t->inpt4_latch = 0x80;
+    t->inpt5_latch = 0x80;
+}
+
+static void orc_rtia_resize_commit(orc_rtia* t)                    /* tia.rs:247-268 */
+{
+    if (t->vblank_top > 262) return;
+    uint16_t clamped = t->vblank_top < R_EXT_TOP ? R_EXT_TOP : t->vblank_top > R_IDEAL_TOP ? R_IDEAL_TOP : t->vblank_top;
+    uint16_t candidate = clamped < t->visible_top ? clamped : t->visible_top;
+    if (candidate != t->pending_top) {
+        t->pending_top = candidate;
+        t->pending_frames = R_RESIZE_FRAMES;
+    } else if (t->pending_frames > 0) {
+        t->pending_frames--;
+        if (t->pending_frames == 0) t->visible_top = t->pending_top;
+    }
+    t->vblank_top = t->visible_top;
+}
+
+static int orc_rtia_pf_bit(const orc_rtia* t, uint8_t x)            /* tia.rs:406-420 */
+{
+    unsigned pf_x = x < 80 ? x / 4u : ((t->ctrlpf & 0x01) ? 19u - (unsigned)(x - 80) / 4u : (unsigned)(x - 80) / 4u);
+    if (pf_x <= 3) return (t->pf0 & (0x10u << pf_x)) != 0;
+    if (pf_x <= 11) return (t->pf1 & (0x80u >> (pf_x - 4))) != 0;
+    if (pf_x <= 19) return (t->pf2 & (0x01u << (pf_x - 12))) != 0;
+    return 0;
+}
+
+/* NUSIZ copy offsets (tia.rs:440-450, 480-488). */
+static const uint16_t orc_copies[8][4] = {
+    {1, 0, 0, 0}, {2, 0, 16, 0}, {2, 0, 32, 0}, {3, 0, 16, 32}, {2, 0, 64, 0}, {1, 0, 0, 0}, {3, 0, 32, 64}, {1, 0, 0, 0},
+};
+
+static int orc_rtia_player(const orc_rtia* t, int player, uint8_t x) /* tia.rs:423-465 */
+{
+    uint8_t grp = player ? (t->vdelp1 ? t->grp1_old : t->grp1) : (t->vdelp0 ? t->grp0_old : t->grp0);
+    uint16_t pos = player ? t->pos_p1 : t->pos_p0;
+    uint8_t refp = player ? t->refp1 : t->refp0;
+    uint8_t nusiz = player ? t->nusiz1 : t->nusiz0;
+    if (grp == 0) return 0;
+    unsigned size_mode = nusiz & 7u;
+    uint16_t pixel_width = size_mode == 5 ? 2 : size_mode == 7 ? 4 : 1;
+    uint16_t pixel_span = (uint16_t)(8 * pixel_width);
+    for (unsigned c = 0; c < orc_copies[size_mode][0]; c++) {
+        uint16_t copy_pos = (uint16_t)((pos + orc_copies[size_mode][1 + c]) % 160);
+        uint16_t offset = (uint16_t)((x + 160 - copy_pos) % 160);
+        if (offset < pixel_span && offset < 80) {
+            uint16_t bit = offset / pixel_width;
+            int hit = refp ? (grp & (0x01u << bit)) != 0 : (grp & (0x80u >> bit)) != 0;
+            if (hit) return 1;
+        }
+    }
+    return 0;
+}
+
+static int orc_rtia_missile(const orc_rtia* t, int m, uint8_t x)    /* tia.rs:468-497 */
+{
+    uint8_t enabled = m ? t->enam1 : t->enam0;
+    uint16_t pos = m ? t->pos_m1 : t->pos_m0;
+    uint8_t nusiz = m ? t->nusiz1 : t->nusiz0;
+    uint8_t resmp = m ? t->resmp1 : t->resmp0;
+    if (!enabled || resmp) return 0;
+    uint16_t width = (uint16_t)(1u << ((nusiz >> 4) & 3u));
+    unsigned mode = nusiz & 7u;
+    for (unsigned c = 0; c < orc_copies[mode][0]; c++) {
+        uint16_t copy_pos = (uint16_t)((pos + orc_copies[mode][1 + c]) % 160);
+        uint16_t offset = (uint16_t)((x + 160 - copy_pos) % 160);
+        if (offset < width && offset < 80) return 1;
+    }
+    return 0;
+}
+
+static int orc_rtia_ball(const orc_rtia* t, uint8_t x)              /* tia.rs:500-507 */
+{
+    uint8_t enabled = t->vdelbl ? t->enabl_old : t->enabl;
+    if (!enabled) return 0;
+    uint16_t width = (uint16_t)(1u << ((t->ctrlpf >> 4) & 3u));
+    uint16_t offset = (uint16_t)((x + 160 - t->pos_bl) % 160);
+    return offset < width && offset < 80;
+}
+
+static void orc_rtia_tick(orc_rtia* t)                              /* tia.rs:271-372 */
+{
+    if (t->input_latch_enabled) {
+        if (!t->inpt4) t->inpt4_latch = 0x00;
+        if (!t->inpt5) t->inpt5_latch = 0x00;
+    }
+    if (!(t->vblank & 0x02) && t->scanline >= R_EXT_TOP && t->scanline < t->vblank_top) t->vblank_top = t->scanline;
+    if (t->delayed_len > 0) {
+        unsigned dst = 0;
+        for (unsigned i = 0; i < t->delayed_len; i++) {
+            orc_delayed e = t->delayed[i];
+            e.remaining--;
+            if (e.remaining == 0) {
+                if (e.reg == 0x0D) t->pf0 = e.value;
+                else if (e.reg == 0x0E) t->pf1 = e.value;
+                else if (e.reg == 0x0F) t->pf2 = e.value;
+            } else {
+                t->delayed[dst++] = e;
+            }
+        }
+        t->delayed_len = (uint8_t)dst;
+    }
+    uint16_t pixel_x = (uint16_t)(t->clock - 68);
+    uint16_t vis_line = (uint16_t)(t->scanline - t->visible_top);
+    if (t->clock >= 68 && pixel_x < R_FRAME_W && !(t->vblank & 0x02) && vis_line < R_FRAME_H) {
+        uint8_t x = (uint8_t)pixel_x;
+        int pf = orc_rtia_pf_bit(t, x), p0 = orc_rtia_player(t, 0, x), p1 = orc_rtia_player(t, 1, x);
+        int m0 = orc_rtia_missile(t, 0, x), m1 = orc_rtia_missile(t, 1, x), bl = orc_rtia_ball(t, x);
+        uint8_t pf_color = (t->ctrlpf & 0x02) ? (x < 80 ? t->colup0 : t->colup1) : t->colupf;    /* :382-389 */
+        uint8_t color;
+        if (t->ctrlpf & 0x04) color = (pf || bl) ? pf_color : (p0 || m0) ? t->colup0 : (p1 || m1) ? t->colup1 : t->colubk;
+        else color = (p0 || m0) ? t->colup0 : (p1 || m1) ? t->colup1 : (pf || bl) ? pf_color : t->colubk;
+        if (t->hmove_pending && pixel_x < 8) color = t->colubk;
+        t->fb[vis_line * R_FRAME_W + pixel_x] = color;
+        if (m0 && p1) t->cxm0p |= 0x80;
+        if (m0 && p0) t->cxm0p |= 0x40;
+        if (m1 && p0) t->cxm1p |= 0x80;
+        if (m1 && p1) t->cxm1p |= 0x40;
+        if (p0 && pf) t->cxp0fb |= 0x80;
+        if (p0 && bl) t->cxp0fb |= 0x40;
+        if (p1 && pf) t->cxp1fb |= 0x80;
+        if (p1 && bl) t->cxp1fb |= 0x40;
+        if (m0 && pf) t->cxm0fb |= 0x80;
+        if (m0 && bl) t->cxm0fb |= 0x40;
+        if (m1 && pf) t->cxm1fb |= 0x80;
+        if (m1 && bl) t->cxm1fb |= 0x40;
+        if (bl && pf) t->cxblpf |= 0x80;
+        if (p0 && p1) t->cxppmm |= 0x80;
+        if (m0 && m1) t->cxppmm |= 0x40;
+    }
+    t->clock++;
+    if (t->clock >= 228) {
+        t->clock = 0;
+        t->scanline++;
+        t->wsync = 0;
+        t->hmove_pending = 0;
+        if (t->scanline == t->visible_top) memset(t->fb, 0, sizeof(t->fb));
+        if (!t->paddle_dumped && t->paddle_counter < 256) t->paddle_counter++;
+        if (t->scanline >= 262) { t->scanline = 0; t->frame_complete = 1; }
+    }
+}
+
+static uint16_t orc_rtia_resp(const orc_rtia* t)                    /* tia.rs:512-520: players */
+{
+    uint16_t delay = t->clock < 68 ? 3 : 4;
+    uint16_t draw_clock = (uint16_t)((t->clock + delay + 156) % 228);
+    return draw_clock >= 68 ? (uint16_t)(draw_clock - 68) : (uint16_t)(draw_clock + 160 - 68);
+}
+
+static uint16_t orc_rtia_resp_simple(const orc_rtia* t)             /* tia.rs:523-525: missiles, ball */
+{
+    int r = ((int)t->clock - 68 + 5) % 160;
+    return (uint16_t)(r < 0 ? r + 160 : r);
+}
+
+static uint8_t orc_rtia_read(const orc_rtia* t, uint16_t addr)      /* tia.rs:533-566 */
+{
+    switch (addr & 0x0F) {
+    case 0x0: return t->cxm0p;
+    case 0x1: return t->cxm1p;
+    case 0x2: return t->cxp0fb;
+    case 0x3: return t->cxp1fb;
+    case 0x4: return t->cxm0fb;
+    case 0x5: return t->cxm1fb;
+    case 0x6: return t->cxblpf;
+    case 0x7: return t->cxppmm;
+    case 0x8: return t->paddle_counter >= t->paddle0 ? 0x80 : 0x00;
+    case 0x9: return t->paddle_counter >= t->paddle1 ? 0x80 : 0x00;
+    case 0xA: case 0xB: return 0x80;
+    case 0xC: return t->input_latch_enabled ? t->inpt4_latch : (t->inpt4 ? 0x80 : 0x00);
+    case 0xD: return t->input_latch_enabled ? t->inpt5_latch : (t->inpt5 ? 0x80 : 0x00);
+    default: return 0;
+    }
+}
+
+static void orc_rtia_write(orc_rtia* t, uint16_t addr, uint8_t v)   /* tia.rs:570-674 */
+{
+    switch (addr & 0x3F) {
+    case 0x00:
+        if (!(t->vsync & 0x02) && (v & 0x02)) { orc_rtia_resize_commit(t); t->scanline = 0; t->frame_complete = 1; }
+        t->vsync = v;
+        break;
+    case 0x01:
+        if (v & 0x40) { t->input_latch_enabled = 1; t->inpt4_latch = 0x80; t->inpt5_latch = 0x80; }
+        else t->input_latch_enabled = 0;
+        if (v & 0x80) { t->paddle_counter = 0; t->paddle_dumped = 1; }
+        else if (t->paddle_dumped) t->paddle_dumped = 0;
+        t->vblank = v;
+        break;
+    case 0x02: t->wsync = 1; break;
+    case 0x04: t->nusiz0 = v; break;
+    case 0x05: t->nusiz1 = v; break;
+    case 0x06: t->colup0 = v; break;
+    case 0x07: t->colup1 = v; break;
+    case 0x08: t->colupf = v; break;
+    case 0x09: t->colubk = v; break;
+    case 0x0A: t->ctrlpf = v; break;
+    case 0x0B: t->refp0 = (v & 0x08) != 0; break;
+    case 0x0C: t->refp1 = (v & 0x08) != 0; break;
+    case 0x0D: case 0x0E: case 0x0F:
+        if (t->delayed_len < R_DELAYED_CAP) {
+            orc_delayed* e = &t->delayed[t->delayed_len++];
+            e->remaining = 1;
+            e->reg = (uint8_t)(addr & 0x3F);
+            e->value = v;
+        } else if ((addr & 0x3F) == 0x0D) t->pf0 = v;
+        else if ((addr & 0x3F) == 0x0E) t->pf1 = v;
+        else t->pf2 = v;
+        break;
+    case 0x10: t->pos_p0 = orc_rtia_resp(t); break;
+    case 0x11: t->pos_p1 = orc_rtia_resp(t); break;
+    case 0x12: t->pos_m0 = orc_rtia_resp_simple(t); break;
+    case 0x13: t->pos_m1 = orc_rtia_resp_simple(t); break;
+    case 0x14: t->pos_bl = orc_rtia_resp_simple(t); break;
+    case 0x1B: t->grp0_old = t->grp0; t->grp0 = v; break;
+    case 0x1C: t->grp1_old = t->grp1; t->grp1 = v; t->enabl_old = t->enabl; break;
+    case 0x1D: t->enam0 = (v & 0x02) != 0; break;
+    case 0x1E: t->enam1 = (v & 0x02) != 0; break;
+    case 0x1F: t->enabl = (v & 0x02) != 0; break;
+    case 0x20: t->hmp0 = v; break;
+    case 0x21: t->hmp1 = v; break;
+    case 0x22: t->hmm0 = v; break;
+    case 0x23: t->hmm1 = v; break;
+    case 0x24: t->hmbl = v; break;
+    case 0x25: t->vdelp0 = v & 0x01; break;
+    case 0x26: t->vdelp1 = v & 0x01; break;
+    case 0x27: t->vdelbl = v & 0x01; break;
+    case 0x28: t->resmp0 = (v & 0x02) != 0; break;
+    case 0x29: t->resmp1 = (v & 0x02) != 0; break;
+    case 0x2A:
+        t->pos_p0 = orc_hmove(t->pos_p0, t->hmp0);
+        t->pos_p1 = orc_hmove(t->pos_p1, t->hmp1);
+        t->pos_m0 = orc_hmove(t->pos_m0, t->hmm0);
+        t->pos_m1 = orc_hmove(t->pos_m1, t->hmm1);
+        t->pos_bl = orc_hmove(t->pos_bl, t->hmbl);
+        t->hmove_pending = 1;
+        break;
+    case 0x2B: t->hmp0 = t->hmp1 = t->hmm0 = t->hmm1 = t->hmbl = 0; break;
+    case 0x2C: t->cxm0p = t->cxm1p = t->cxp0fb = t->cxp1fb = t->cxm0fb = t->cxm1fb = t->cxblpf = t->cxppmm = 0; break;
+    default: break;                                                 /* RSYNC, audio */
+    }
+}
+
+static void orc_pia_tick1(orc_pia* p)                              /* pia.rs:80-103 */
+{
+    if (p->timer_value == 0 && p->timer_underflow) { p->timer_value = 0xFF; return; }
+    p->timer_prescaler = (uint16_t)(p->timer_prescaler - 1);
+    if (p->timer_prescaler == 0) {
+        p->timer_prescaler = p->timer_underflow ? 1 : p->timer_select;
+        if (p->timer_value == 0) { p->timer_underflow = 1; p->timer_value = 0xFF; }
+        else p->timer_value--;
+    }
+}
+
+struct orc_ratari {
+    orc_cpu  cpu;
+    orc_rtia tia;
+    orc_pia  pia;
+    uint8_t* rom;
+    size_t   rom_len;
+    int      bank, scheme;
+    uint32_t bus_ticks;
+    uint32_t frame_no, run_status;
+    uint64_t instructions;
+};
+
+static inline uint8_t orc_rrom_read(const orc_ratari* e, uint16_t addr) /* atari.rs:139-150 */
+{
+    if (e->scheme == FA_SCHEME_FIXED) return e->rom[(addr & 0x0FFF) % e->rom_len];
+    size_t off = (size_t)e->bank * 4096 + (addr & 0x0FFF);
+    return off < e->rom_len ? e->rom[off] : 0;
+}
+
+static inline void orc_rcheck_bankswitch(orc_ratari* e, uint16_t addr) /* atari.rs:153-180 */
+{
+    uint16_t a = addr & 0x1FFF;
+    int first = e->scheme == FA_SCHEME_F8 ? 0x1FF8 : e->scheme == FA_SCHEME_F6 ? 0x1FF6 : e->scheme == FA_SCHEME_F4 ? 0x1FF4 : 0;
+    int nb = e->scheme == FA_SCHEME_F8 ? 2 : e->scheme == FA_SCHEME_F6 ? 4 : e->scheme == FA_SCHEME_F4 ? 8 : 0;
+    if (nb && a >= first && a < first + nb) e->bank = a - first;
+}
+
+static inline void orc_rtick_components(orc_ratari* e)             /* atari.rs:273-279 */
+{
+    orc_rtia_tick(&e->tia);
+    orc_rtia_tick(&e->tia);
+    orc_rtia_tick(&e->tia);
+    orc_pia_tick1(&e->pia);
+}
+
+static inline void orc_rtick_cycle(orc_ratari* e)                  /* atari.rs:186-192 */
+{
+    orc_rtick_components(e);
+    e->bus_ticks++;
+}
+
+static uint8_t orc_rbus_read(orc_ratari* e, uint16_t addr)          /* atari.rs:195-205 */
+{
+    orc_rcheck_bankswitch(e, addr);
+    uint16_t a = addr & 0x1FFF;
+    uint8_t v;
+    if ((a & 0x1080) == 0x0000) v = orc_rtia_read(&e->tia, a);
+    else if ((a & 0x1280) == 0x0080 || (a & 0x1280) == 0x0280) v = orc_pia_read(&e->pia, a);
+    else if (a & 0x1000) v = orc_rrom_read(e, a);
+    else v = 0;
+    orc_rtick_cycle(e);
+    return v;
+}
+
+static void orc_rbus_write(orc_ratari* e, uint16_t addr, uint8_t v) /* atari.rs:207-222 */
+{
+    orc_rtia_tick(&e->tia);
+    orc_rtia_tick(&e->tia);
+    orc_rcheck_bankswitch(e, addr);
+    uint16_t a = addr & 0x1FFF;
+    if ((a & 0x1080) == 0x0000) orc_rtia_write(&e->tia, a, v);
+    else if ((a & 0x1280) == 0x0080 || (a & 0x1280) == 0x0280) orc_pia_write(&e->pia, a, v);
+    orc_rtia_tick(&e->tia);
+    orc_pia_tick1(&e->pia);
+    e->bus_ticks++;
+}
+
+/* Cpu::step on the rendering bus. */
+#define STEP_FN orc_step_rbus
+#define MEM_T orc_ratari
+#define MREAD(m, a) orc_rbus_read((m), (uint16_t)(a))
+#define MWRITE(m, a, v) orc_rbus_write((m), (uint16_t)(a), (uint8_t)(v))
+#include "cpu_step.h"
+#undef STEP_FN
+#undef MEM_T
+#undef MREAD
+#undef MWRITE
+
+orc_ratari* orc_rcreate(const uint8_t* rom, size_t rom_len)        /* atari.rs:120-136, 240-247 */
+{
+    if (!rom || !orc_rom_len_ok(rom_len)) return NULL;
+    orc_ratari* e = (orc_ratari*)calloc(1, sizeof(orc_ratari));
+    if (!e) return NULL;
+    e->rom = (uint8_t*)malloc(rom_len);
+    if (!e->rom) { free(e); return NULL; }
+    memcpy(e->rom, rom, rom_len);
+    e->rom_len = rom_len;
+    e->scheme = orc_detect(rom_len);
+    e->bank = e->scheme == FA_SCHEME_FIXED ? 0 : e->scheme == FA_SCHEME_F8 ? 1 : e->scheme == FA_SCHEME_F6 ? 3 : 7;
+    orc_rtia_default(&e->tia);
+    orc_pia_default(&e->pia);
+    e->cpu.sp = 0xFD;                                              /* Cpu::default */
+    uint16_t lo = orc_rbus_read(e, 0xFFFC);                        /* Cpu::reset, cpu.rs:125-134 */
+    uint16_t hi = orc_rbus_read(e, 0xFFFD);
+    e->cpu.pc = (uint16_t)((hi << 8) | lo);
+    e->cpu.sp = 0xFD;
+    e->cpu.p = 0;
+    e->cpu.a = e->cpu.x = e->cpu.y = 0;
+    return e;
+}
+
+orc_ratari* orc_rclone(const orc_ratari* e)
+{
+    orc_ratari* c = (orc_ratari*)malloc(sizeof(orc_ratari));
+    if (!c) return NULL;
+    memcpy(c, e, sizeof(*c));
+    c->rom = (uint8_t*)malloc(e->rom_len);
+    if (!c->rom) { free(c); return NULL; }
+    memcpy(c->rom, e->rom, e->rom_len);
+    return c;
+}
+
+void orc_rdestroy(orc_ratari* e)
+{
+    if (!e) return;
+    free(e->rom);
+    free(e);
+}
+
+void orc_rset_action(orc_ratari* e, unsigned action)              /* atari.rs:250-270 */
+{
+    static const uint8_t dec[18][5] = {
+        {0,0,0,0,0}, {0,0,0,0,1}, {1,0,0,0,0}, {0,0,0,1,0}, {0,0,1,0,0}, {0,1,0,0,0},
+        {1,0,0,1,0}, {1,0,1,0,0}, {0,1,0,1,0}, {0,1,1,0,0}, {1,0,0,0,1}, {0,0,0,1,1},
+        {0,0,1,0,1}, {0,1,0,0,1}, {1,0,0,1,1}, {1,0,1,0,1}, {0,1,0,1,1}, {0,1,1,0,1},
+    };
+    const uint8_t* d = dec[action < 18 ? action : 0];
+    uint8_t swcha = 0xFF;
+    if (d[0]) swcha &= (uint8_t)~0x10;
+    if (d[1]) swcha &= (uint8_t)~0x20;
+    if (d[2]) swcha &= (uint8_t)~0x40;
+    if (d[3]) swcha &= (uint8_t)~0x80;
+    e->pia.pa_in = swcha;
+    e->tia.inpt4 = !d[4];
+    e->tia.paddle0 = d[2] ? 200 : (d[3] ? 50 : 128);
+}
+
+static inline int orc_rrun_one_cycle(orc_ratari* e, uint64_t* cycles) /* atari.rs:309-318 */
+{
+    if (e->tia.wsync) {
+        orc_rtick_components(e);
+        *cycles += 1;
+    } else {
+        uint8_t c = orc_step_rbus(&e->cpu, e);
+        if (c == 0) { e->run_status |= FA_STATUS_ILLEGAL_OPCODE; return 0; }
+        e->instructions++;
+        *cycles += c;
+    }
+    return 1;
+}
+
+uint64_t orc_rrun_frame(orc_ratari* e)                             /* atari.rs:284-306 */
+{
+    if (e->run_status & FA_STATUS_HALT_MASK) return 0;
+    e->tia.frame_complete = 0;
+    uint64_t cycles = 0;
+    while (e->tia.vsync & 0x02) {
+        if (!orc_rrun_one_cycle(e, &cycles)) return cycles;
+        if (cycles > FA_VSYNC_BUDGET) { e->run_status |= FA_STATUS_VSYNC_BUDGET; return cycles; }
+    }
+    while (!(e->tia.vsync & 0x02)) {
+        if (!orc_rrun_one_cycle(e, &cycles)) return cycles;
+        if (cycles > FA_FRAME_CYCLE_CAP) { e->run_status |= FA_STATUS_CYCLE_CAP; break; }
+    }
+    e->frame_no++;
+    return cycles;
+}
+
+const uint8_t* orc_rframebuffer(const orc_ratari* e) { return e->tia.fb; }
+void orc_rram(const orc_ratari* e, uint8_t* out128) { memcpy(out128, e->pia.ram, 128); }
+size_t orc_rtia_size(void) { return sizeof(orc_rtia); }
+
+/* Registers and frame bookkeeping of one rendering console. */
+void orc_rregs(const orc_ratari* e, uint32_t* out8)
+{
+    out8[0] = e->cpu.a | (e->cpu.x << 8) | (e->cpu.y << 16) | ((uint32_t)e->cpu.sp << 24);
+    out8[1] = e->cpu.pc | ((uint32_t)e->cpu.p << 16) | ((uint32_t)e->bank << 24);
+    out8[2] = (uint32_t)e->cpu.cycles;
+    out8[3] = (uint32_t)(e->cpu.cycles >> 32);
+    out8[4] = e->tia.clock | ((uint32_t)e->tia.scanline << 16);
+    out8[5] = e->frame_no;
+    out8[6] = e->run_status;
+    out8[7] = e->pia.timer_value | ((uint32_t)e->pia.timer_prescaler << 16);
+}
+
+/* The whole TIA record (orc_rtia, its framebuffer last) for full-state comparisons. */
+void orc_rtia_copy(const orc_ratari* e, void* out) { memcpy(out, &e->tia, sizeof(e->tia)); }

@@ -94,6 +94,21 @@ int orc_flat_run_from(uint8_t* mem64k, int nsteps, uint8_t* cycles_out, orc_regs
 /* sizeof(fa_state) as compiled into the oracle (ABI check). */
 size_t orc_state_size(void);
 
+/* ---- rendering console (src/tia.rs, src/atari.rs:107-306): one bus access per
+ * CPU cycle, three TIA clocks and one PIA clock per access, 160 x 192 palette
+ * index framebuffer. */
+typedef struct orc_ratari orc_ratari;
+orc_ratari*    orc_rcreate(const uint8_t* rom, size_t rom_len);   /* Atari::new */
+orc_ratari*    orc_rclone(const orc_ratari* e);
+void           orc_rdestroy(orc_ratari* e);
+void           orc_rset_action(orc_ratari* e, unsigned action);
+uint64_t       orc_rrun_frame(orc_ratari* e);
+const uint8_t* orc_rframebuffer(const orc_ratari* e);
+void           orc_rram(const orc_ratari* e, uint8_t* out128);
+void           orc_rregs(const orc_ratari* e, uint32_t* out8);
+size_t         orc_rtia_size(void);
+void           orc_rtia_copy(const orc_ratari* e, void* out);
+
 #ifdef __cplusplus
 }
 #endif

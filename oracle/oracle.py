@@ -104,6 +104,20 @@ def lib() -> ctypes.CDLL:
         L.orc_flat_run_from.restype = ctypes.c_int
         L.orc_flat_run_from.argtypes = [u8p, ctypes.c_int, u8p, ctypes.POINTER(OrcRegs)]
         L.orc_state_size.restype = ctypes.c_size_t
+        L.orc_rcreate.restype = vp
+        L.orc_rcreate.argtypes = [u8p, sz]
+        L.orc_rclone.restype = vp
+        L.orc_rclone.argtypes = [vp]
+        L.orc_rdestroy.argtypes = [vp]
+        L.orc_rset_action.argtypes = [vp, ctypes.c_uint]
+        L.orc_rrun_frame.restype = ctypes.c_uint64
+        L.orc_rrun_frame.argtypes = [vp]
+        L.orc_rframebuffer.restype = vp
+        L.orc_rframebuffer.argtypes = [vp]
+        L.orc_rram.argtypes = [vp, u8p]
+        L.orc_rregs.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
+        L.orc_rtia_size.restype = sz
+        L.orc_rtia_copy.argtypes = [vp, vp]
         _lib = L
     return _lib
 
@@ -158,6 +172,97 @@ class Atari:
     def set_state(self, s) -> None:
         a = np.ascontiguousarray(np.array(s, dtype=STATE_DTYPE).reshape(1))
         lib().orc_set_state(self._p, a.ctypes.data)
+
+
+# orc_rtia (oracle/fa_oracle.c), the rendering Tia's record, C layout.
+RTIA_DTYPE = np.dtype([
+    ("clock", "<u2"), ("scanline", "<u2"), ("wsync", "u1"), ("hmove_pending", "u1"),
+    ("visible_top", "<u2"), ("vblank_top", "<u2"), ("pending_top", "<u2"), ("pending_frames", "u1"),
+    ("delayed", "u1", (12,)), ("delayed_len", "u1"), ("frame_complete", "u1"),
+    ("vsync", "u1"), ("vblank", "u1"), ("colup0", "u1"), ("colup1", "u1"), ("colupf", "u1"), ("colubk", "u1"),
+    ("ctrlpf", "u1"), ("refp0", "u1"), ("refp1", "u1"), ("pf0", "u1"), ("pf1", "u1"), ("pf2", "u1"),
+    ("grp0", "u1"), ("grp1", "u1"), ("grp0_old", "u1"), ("grp1_old", "u1"),
+    ("enam0", "u1"), ("enam1", "u1"), ("enabl", "u1"), ("enabl_old", "u1"),
+    ("hmp0", "u1"), ("hmp1", "u1"), ("hmm0", "u1"), ("hmm1", "u1"), ("hmbl", "u1"),
+    ("nusiz0", "u1"), ("nusiz1", "u1"), ("vdelp0", "u1"), ("vdelp1", "u1"), ("vdelbl", "u1"),
+    ("resmp0", "u1"), ("resmp1", "u1"),
+    ("pos_p0", "<u2"), ("pos_p1", "<u2"), ("pos_m0", "<u2"), ("pos_m1", "<u2"), ("pos_bl", "<u2"),
+    ("cxm0p", "u1"), ("cxm1p", "u1"), ("cxp0fb", "u1"), ("cxp1fb", "u1"),
+    ("cxm0fb", "u1"), ("cxm1fb", "u1"), ("cxblpf", "u1"), ("cxppmm", "u1"),
+    ("paddle0", "u1"), ("paddle1", "u1"), ("paddle_counter", "<u2"), ("paddle_dumped", "u1"),
+    ("inpt4", "u1"), ("inpt5", "u1"), ("inpt4_latch", "u1"), ("inpt5_latch", "u1"), ("input_latch_enabled", "u1"),
+    ("fb", "u1", (192, 160)),
+], align=True)
+
+
+class RenderAtari:
+    """One rendering console, Atari (src/atari.rs:227-306) with the pixel-
+    accurate Tia (src/tia.rs): a 160 x 192 framebuffer of palette indices."""
+
+    FRAME_W, FRAME_H = 160, 192
+
+    def __init__(self, rom: bytes, _ptr=None):
+        L = lib()
+        if _ptr is None:
+            r = _bytes_arr(rom)
+            _ptr = L.orc_rcreate(_u8(r), len(r))
+            if not _ptr:
+                raise ValueError(f"ROM length {len(rom)} cannot be constructed")
+        self._p = _ptr
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            lib().orc_rdestroy(self._p)
+            self._p = None
+
+    def clone(self) -> "RenderAtari":
+        return RenderAtari(b"", _ptr=lib().orc_rclone(self._p))
+
+    def set_action(self, action: int) -> None:
+        lib().orc_rset_action(self._p, int(action))
+
+    def run_frame(self) -> int:
+        return int(lib().orc_rrun_frame(self._p))
+
+    def framebuffer(self) -> np.ndarray:
+        ptr = lib().orc_rframebuffer(self._p)
+        buf = (ctypes.c_uint8 * (self.FRAME_W * self.FRAME_H)).from_address(ptr)
+        return np.frombuffer(buf, np.uint8).reshape(self.FRAME_H, self.FRAME_W).copy()
+
+    def ram(self) -> np.ndarray:
+        out = np.zeros(128, np.uint8)
+        lib().orc_rram(self._p, _u8(out))
+        return out
+
+    def regs(self) -> np.ndarray:
+        """[axys, pc|p<<16|bank<<24, cycles lo, cycles hi, clock|scanline<<16, frame_no, run_status, timer]"""
+        out = np.zeros(8, np.uint32)
+        lib().orc_rregs(self._p, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+        return out
+
+    def tia_record(self) -> np.ndarray:
+        out = np.zeros(1, RTIA_DTYPE)
+        assert RTIA_DTYPE.itemsize == lib().orc_rtia_size()
+        lib().orc_rtia_copy(self._p, out.ctypes.data)
+        return out[0]
+
+
+def render_reset(rom: bytes, n: int):
+    """n rendering consoles after new + one frame (the batched reset)."""
+    first = RenderAtari(rom)
+    first.run_frame()
+    return [first] + [first.clone() for _ in range(n - 1)]
+
+
+def render_steps(consoles, actions: np.ndarray):
+    """Run k frames (actions [k, n]) on every console; returns the last frame's
+    framebuffers [n, 192, 160] and RAM [n, 128]."""
+    k, n = actions.shape
+    for i, c in enumerate(consoles):
+        for f in range(k):
+            c.set_action(int(actions[f, i]))
+            c.run_frame()
+    return (np.stack([c.framebuffer() for c in consoles]), np.stack([c.ram() for c in consoles]))
 
 
 def reset_state(rom: bytes) -> np.ndarray:

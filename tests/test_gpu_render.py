@@ -1,0 +1,90 @@
+"""GPU parity of the rendering console (src/atari.rs:107-306, src/tia.rs).
+
+Every console's framebuffer (160 x 192 palette indices), RAM, CPU registers,
+cycle counter and TIA registers after each call equal the CPU oracle's
+restatement of the rendering console, bit for bit: on the rendering cart
+(every graphics register, mid-line writes, HMOVE, collisions, input latches),
+on the divergence cart (F8 bank switching, no WSYNC) and on the 32K F4 cart.
+The rendering oracle is unpinned: the reference's own rendering checks need
+Breakout.bin or the Gopher2600 tool, and neither is available."""
+import numpy as np
+import pytest
+
+import oracle
+from fa_pkg import carts, fa
+
+pytestmark = pytest.mark.gpu
+
+TIA_FIELDS = ["colup0", "colup1", "colupf", "colubk", "ctrlpf", "refp0", "refp1", "pf0", "pf1", "pf2",
+              "grp0", "grp1", "grp0_old", "grp1_old", "enam0", "enam1", "enabl", "enabl_old",
+              "hmp0", "hmp1", "hmm0", "hmm1", "hmbl", "nusiz0", "nusiz1", "vdelp0", "vdelp1", "vdelbl",
+              "resmp0", "resmp1", "pos_p0", "pos_p1", "pos_m0", "pos_m1", "pos_bl",
+              "cxm0p", "cxm1p", "cxp0fb", "cxp1fb", "cxm0fb", "cxm1fb", "cxblpf", "cxppmm",
+              "paddle0", "paddle1", "paddle_counter", "paddle_dumped", "inpt4", "inpt5"]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def need_gpu():
+    if fa.device_count() < 1:
+        pytest.skip("no CUDA device")
+
+
+def check(gpu_fb, gpu_ram, gpu_st, consoles, what):
+    for i, c in enumerate(consoles):
+        t = c.tia_record()
+        assert np.array_equal(gpu_fb[i], t["fb"]), f"{what}: framebuffer of console {i}, " \
+            f"{int((gpu_fb[i] != t['fb']).sum())} pixels differ, first at {np.argwhere(gpu_fb[i] != t['fb'])[0].tolist()}"
+        assert np.array_equal(gpu_ram[i], c.ram()), f"{what}: RAM of console {i}"
+        r = c.regs()
+        s = gpu_st[i]
+        got = [int(s["a"]) | int(s["x"]) << 8 | int(s["y"]) << 16 | int(s["sp"]) << 24,
+               int(s["pc"]) | int(s["status"]) << 16 | int(s["bank"]) << 24,
+               int(s["cycles"]) & 0xFFFFFFFF, int(s["cycles"]) >> 32,
+               int(s["tia_clock"]) | int(s["tia_scanline"]) << 16, int(s["frame_no"]), int(s["run_status"]),
+               int(s["timer_value"]) | int(s["timer_prescaler"]) << 16]
+        want = [int(v) for v in r]
+        want[5] -= 1                       # the library's frame counter restarts after the reset frame
+        assert got == want, f"{what}: registers of console {i}: gpu {got} oracle {want}"
+        for f in TIA_FIELDS:
+            assert int(s[f]) == int(t[f]), f"{what}: {f} of console {i}: gpu {int(s[f])} oracle {int(t[f])}"
+        assert int(s["tia_vsync"]) == int(t["vsync"]) and int(s["tia_vblank"]) == int(t["vblank"]), what
+
+
+@pytest.mark.parametrize("name", ["render", "divergence", "mixed_32k"])
+def test_render_matches_oracle(name):
+    rom = {"render": carts.render_cart, "divergence": carts.divergence_cart,
+           "mixed_32k": lambda: carts.mixed_carts()[3]}[name]().rom
+    n, calls, k = 40, 3, 4
+    consoles = oracle.render_reset(rom, n)
+    with fa.AtariRender(rom, n) as g:
+        fb, ram = g.reset()
+        check(fb, ram, g.states(), consoles, f"{name} reset")
+        for c in range(calls):
+            acts = carts.actions(seed=60 + c, n=n, frames=k)
+            fb, ram = g.step_multi(acts, k)
+            oracle.render_steps(consoles, acts)
+            check(fb, ram, g.states(), consoles, f"{name} call {c}")
+
+
+@pytest.mark.parametrize("warps,sched", [(4, "lane"), (16, "line")])
+def test_render_launch_shapes_and_policies(warps, sched):
+    rom = carts.render_cart().rom
+    n, k = 70, 5                                    # a partial warp
+    acts = carts.actions(seed=71, n=n, frames=k)
+    consoles = oracle.render_reset(rom, n)
+    oracle.render_steps(consoles, acts)
+    with fa.AtariRender(rom, n, cta_warps=warps, sched=sched) as g:
+        g.reset()
+        fb, ram = g.step_multi(acts, k)
+        check(fb, ram, g.states(), consoles, f"{warps} warps, {sched}")
+
+
+def test_render_frames_are_pictures_and_depend_on_actions():
+    rom = carts.render_cart().rom
+    n, k = 64, 6
+    with fa.AtariRender(rom, n) as g:
+        g.reset()
+        fb, _ = g.step_multi(carts.actions(seed=5, n=n, frames=k), k)
+    assert (fb != 0).sum(axis=(1, 2)).min() > 1000                 # every console drew something
+    assert len(np.unique(fb)) > 8                                    # several colours
+    assert len({fb[i].tobytes() for i in range(n)}) >= 4             # the actions show in the pictures
