@@ -57,6 +57,11 @@ I_CONV = 187.6
 # capture in profiles/fa_run_warps_mixed_batch_full.md (28.2 MB per 4-frame
 # call of 135,500 instances).
 DRAM_BYTES_PER_INSTANCE_FRAME = 52.0
+# The rendering kernel (fa_render_run<8>) per rendered console-frame, from
+# the ncu capture in profiles/fa_render_run_render_cart.md: SASS
+# thread-instructions and DRAM bytes (framebuffer writes included).
+RENDER_THREAD_INST_PER_FRAME = 1.594e7   # smsp__thread_inst_executed / console-frames
+RENDER_DRAM_BYTES_PER_FRAME = 108_100    # (dram read + write) / console-frames
 
 
 def load_pkg():
@@ -280,9 +285,26 @@ def cpu_reference(carts, spec, k, seconds_target=15.0):
 
 
 def run_reference_arm(args, carts, rank, world):
-    desc, spec, k, _ = workload(args.workload, carts)
     if rank != 0:
         return
+    if args.workload == "render":
+        per_step_s = args.ref_step_seconds or 10.0
+        vals = []
+        for i in range(args.warmup + args.steps):
+            fps, cores, sample = render_cpu_baseline(carts, per_step_s)
+            if i >= args.warmup:
+                vals.append(fps)
+        value = statistics.mean(vals)
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+                          "config": {"workload": RENDER_DESC, "parallelism": "one console per host thread"},
+                          "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                                           "sample": sample + "; C restatement of the reference's rendering Atari + Tia"},
+                          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    desc, spec, k, _ = workload(args.workload, carts)
     # Each step is one bounded CPU sample; warmup steps are run untimed.
     per_step_s = args.ref_step_seconds or max(2.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
     vals = []
@@ -492,6 +514,113 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
     pool.close()
 
 
+RENDER_DESC = ("rendering console (pixel-accurate TIA, 160x192 palette-index framebuffer per console): "
+               "render_4k_fixed cart, 113664 consoles (one wave: 148 SMs x 24 warps x 32), K=4 frames per call")
+RENDER_N, RENDER_K = 113_664, 4
+
+
+def render_cpu_baseline(carts, seconds_target):
+    """The rendering oracle (C restatement of the reference's Atari + Tia) on
+    every host thread: a bounded sample of consoles, frames/s."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    cores = os.cpu_count() or 1
+    rom = carts.render_cart().rom
+    m = 4 * cores
+    consoles = oracle.render_reset(rom, m)
+    frames, call = 0, 0
+    t0 = time.perf_counter()
+    while True:
+        oracle.render_steps(consoles, carts.actions(seed=11, n=m, frames=RENDER_K, frame0=call * RENDER_K),
+                            nthreads=cores, outputs=False)
+        frames += m * RENDER_K
+        call += 1
+        if time.perf_counter() - t0 >= seconds_target:
+            break
+    dt = time.perf_counter() - t0
+    return frames / dt, cores, f"{call} calls of K={RENDER_K} frames over {m} consoles ({frames} frames, {dt:.1f} s)"
+
+
+def run_render_arm(args, fa, carts, rank, world, local_rank):
+    """The rendering console: frames/s with framebuffers (its own JSON line)."""
+    import torch
+    fa.set_device(local_rank)
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n, k = args.render_instances, RENDER_K
+    steps = max(1, min(args.steps, 20))
+    calls = args.warmup + steps
+    rom = carts.render_cart().rom
+    g = fa.AtariRender(rom, n, cta_warps=8)
+    g.reset()
+    acts = torch.empty(calls * k * n, dtype=torch.uint8, device=dev)
+    for c in range(calls):
+        a = carts.actions(seed=replica_seed(rank, 0), n=n, frames=k, frame0=c * k)
+        acts[c * k * n:(c + 1) * k * n].copy_(torch.from_numpy(a.reshape(-1)))
+    d_obs = torch.empty(n * 128, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    for c in range(args.warmup):
+        g.step_multi_async(acts.data_ptr() + c * k * n, k, d_obs.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            for i in range(steps):
+                flush.zero_()
+                evs[i][0].record(stream)
+                g.step_multi_async(acts.data_ptr() + (args.warmup + i) * k * n, k, d_obs.data_ptr(), stream.cuda_stream)
+                evs[i][1].record(stream)
+        torch.cuda.synchronize()
+    clocks = clk.summary()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = max_over_ranks(sum(ms), world, dev)
+    value = n * k * steps * world / (total_ms / 1e3)
+    g.synchronize()
+    # End to end through the C ABI: host actions in, every framebuffer and the RAM out.
+    host_acts = [acts[(args.warmup + i) * k * n:(args.warmup + i + 1) * k * n].cpu().numpy() for i in range(min(steps, 3))]
+    g.step_multi(host_acts[0], k)
+    t0 = time.perf_counter()
+    for a in host_acts:
+        g.step_multi(a, k)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
+    e2e = n * k * len(host_acts) * world / e2e_s
+    g.step_multi(host_acts[0], k, fb=False)
+    instr_per_frame = g.last_instructions() / (n * k)
+    f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    peak = 148 * 4 * f_sm
+    achieved = value * RENDER_THREAD_INST_PER_FRAME / 32.0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic",
+        "config": {"workload": RENDER_DESC.replace("113664 consoles (one wave: 148 SMs x 24 warps x 32)", f"{n} consoles"),
+                   "instances": n, "frames_per_call": k,
+                   "framebuffer_bytes_per_frame": 160 * 192,
+                   "l2": "flushed (256 MB write) before every timed call",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "clocks": clocks,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": n * k, "d2h_bytes_per_step": n * (160 * 192 + 128)},
+        "gpu_launches": steps,
+        "roofline": {"bound": "issue", "achieved": achieved / 1e12, "peak": peak / 1e12,
+                     "unit": "T warp-inst/s", "frac": achieved / peak,
+                     "traffic": RENDER_DRAM_BYTES_PER_FRAME * n * k,
+                     "note": f"frames/s x {RENDER_THREAD_INST_PER_FRAME:.4g} SASS thread-instr per rendered frame (ncu) / 32"},
+        "guest_instructions_per_frame": instr_per_frame,
+        "step_latency_ms": {"p50": sorted(ms)[len(ms) // 2], "max": max(ms)},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        fps, cores, sample = render_cpu_baseline(carts, min(args.cpu_seconds, 15.0))
+        line["cpu_baseline"] = {"value": fps, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": sample + "; C restatement of the reference's rendering Atari + Tia"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.close()
+
+
 def run_serve_arm(args, fa, carts, rank, world, local_rank):
     """The serving workload: its own JSON line (replicas under torchrun)."""
     fa.set_device(local_rank)
@@ -544,9 +673,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed",
-                    choices=["mixed", "divergence", "plain", "scale", "converged", "serve"])
+                    choices=["mixed", "divergence", "plain", "scale", "converged", "serve", "render"])
     ap.add_argument("--serve-requests", type=int, default=20000, help="saturation requests of the serve workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
+    ap.add_argument("--render-instances", type=int, default=RENDER_N, help="consoles of the render workload")
     ap.add_argument("--block", type=int, default=128)
     ap.add_argument("--tuning", default=None, help="JSON file of per-cart tuning records (skips the autotuner)")
     ap.add_argument("--no-autotune", action="store_true", help="default policy and weights instead of the autotuner")
@@ -579,6 +709,8 @@ def main():
             run_reference_arm(args, carts, rank, world)
         elif args.workload == "serve":
             run_serve_arm(args, fa, carts, rank, world, local_rank)
+        elif args.workload == "render":
+            run_render_arm(args, fa, carts, rank, world, local_rank)
         else:
             run_gpu_arm(args, fa, carts, rank, world, local_rank)
     finally:

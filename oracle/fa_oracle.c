@@ -1315,3 +1315,50 @@ void orc_rregs(const orc_ratari* e, uint32_t* out8)
 
 /* The whole TIA record (orc_rtia, its framebuffer last) for full-state comparisons. */
 void orc_rtia_copy(const orc_ratari* e, void* out) { memcpy(out, &e->tia, sizeof(e->tia)); }
+
+/* k frames on each of n rendering consoles (actions [k][n]) with nthreads
+ * threads, console i on thread i % nthreads.  Returns the instructions
+ * executed, or (uint64_t)-1 on a bad argument. */
+typedef struct orc_rjob {
+    orc_ratari** cs;
+    size_t n;
+    int k, tid, nth;
+    const uint8_t* actions;
+    uint64_t instructions;
+} orc_rjob;
+
+static void* orc_rworker(void* arg)
+{
+    orc_rjob* j = (orc_rjob*)arg;
+    for (size_t i = (size_t)j->tid; i < j->n; i += (size_t)j->nth) {
+        orc_ratari* e = j->cs[i];
+        uint64_t before = e->instructions;
+        for (int f = 0; f < j->k; f++) {
+            orc_rset_action(e, j->actions[(size_t)f * j->n + i]);
+            orc_rrun_frame(e);
+        }
+        j->instructions += e->instructions - before;
+    }
+    return NULL;
+}
+
+uint64_t orc_rrun_batch(orc_ratari** cs, size_t n, int k, const uint8_t* actions, int nthreads)
+{
+    if (!cs || !actions || k < 0) return (uint64_t)-1;
+    if (nthreads < 1) nthreads = 1;
+    if ((size_t)nthreads > n && n > 0) nthreads = (int)n;
+    orc_rjob* jobs = (orc_rjob*)calloc((size_t)nthreads, sizeof(orc_rjob));
+    pthread_t* th = (pthread_t*)calloc((size_t)nthreads, sizeof(pthread_t));
+    if (!jobs || !th) { free(jobs); free(th); return (uint64_t)-1; }
+    for (int t = 0; t < nthreads; t++) jobs[t] = (orc_rjob){ cs, n, k, t, nthreads, actions, 0 };
+    for (int t = 1; t < nthreads; t++) pthread_create(&th[t], NULL, orc_rworker, &jobs[t]);
+    orc_rworker(&jobs[0]);
+    uint64_t total = jobs[0].instructions;
+    for (int t = 1; t < nthreads; t++) {
+        pthread_join(th[t], NULL);
+        total += jobs[t].instructions;
+    }
+    free(jobs);
+    free(th);
+    return total;
+}

@@ -108,6 +108,8 @@ void           orc_rram(const orc_ratari* e, uint8_t* out128);
 void           orc_rregs(const orc_ratari* e, uint32_t* out8);
 size_t         orc_rtia_size(void);
 void           orc_rtia_copy(const orc_ratari* e, void* out);
+/* k frames on each of n rendering consoles (actions [k][n]), nthreads threads. */
+uint64_t       orc_rrun_batch(orc_ratari** cs, size_t n, int k, const uint8_t* actions, int nthreads);
 
 #ifdef __cplusplus
 }

@@ -118,6 +118,8 @@ def lib() -> ctypes.CDLL:
         L.orc_rregs.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
         L.orc_rtia_size.restype = sz
         L.orc_rtia_copy.argtypes = [vp, vp]
+        L.orc_rrun_batch.restype = ctypes.c_uint64
+        L.orc_rrun_batch.argtypes = [ctypes.POINTER(vp), sz, ctypes.c_int, u8p, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -254,14 +256,18 @@ def render_reset(rom: bytes, n: int):
     return [first] + [first.clone() for _ in range(n - 1)]
 
 
-def render_steps(consoles, actions: np.ndarray):
-    """Run k frames (actions [k, n]) on every console; returns the last frame's
-    framebuffers [n, 192, 160] and RAM [n, 128]."""
+def render_steps(consoles, actions: np.ndarray, nthreads: int | None = None, outputs: bool = True):
+    """Run k frames (actions [k, n]) on every console, on all host threads;
+    returns the last frame's framebuffers [n, 192, 160] and RAM [n, 128]
+    (None with outputs=False)."""
     k, n = actions.shape
-    for i, c in enumerate(consoles):
-        for f in range(k):
-            c.set_action(int(actions[f, i]))
-            c.run_frame()
+    ptrs = (ctypes.c_void_p * n)(*[c._p for c in consoles])
+    a = np.ascontiguousarray(actions, dtype=np.uint8)
+    instr = lib().orc_rrun_batch(ptrs, n, k, _u8(a), nthreads or os.cpu_count() or 1)
+    if instr == 2**64 - 1:
+        raise RuntimeError("oracle render batch failed")
+    if not outputs:
+        return None
     return (np.stack([c.framebuffer() for c in consoles]), np.stack([c.ram() for c in consoles]))
 
 
