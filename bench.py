@@ -288,7 +288,7 @@ def run_reference_arm(args, carts, rank, world):
     if rank != 0:
         return
     if args.workload == "render":
-        per_step_s = args.ref_step_seconds or 10.0
+        per_step_s = args.ref_step_seconds or max(0.2, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
         vals = []
         for i in range(args.warmup + args.steps):
             fps, cores, sample = render_cpu_baseline(carts, per_step_s)
@@ -306,7 +306,8 @@ def run_reference_arm(args, carts, rank, world):
         return
     desc, spec, k, _ = workload(args.workload, carts)
     # Each step is one bounded CPU sample; warmup steps are run untimed.
-    per_step_s = args.ref_step_seconds or max(2.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
+    # Each step is a bounded sample sized so the whole run takes about two minutes.
+    per_step_s = args.ref_step_seconds or max(0.2, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
     vals = []
     for i in range(args.warmup + args.steps):
         fps, cores, sample = cpu_reference(carts, spec, k, seconds_target=per_step_s)
