@@ -174,6 +174,7 @@ static __device__ __noinline__ uint4 pia_write_io(uint32_t a, uint32_t v, uint32
 // extras), interleaved by lane in 32-lane slabs; the framebuffer is HBM.
 struct RState {
     uint32_t clock, scanline, tw, pcnt, vtop;   // beam, TIA flags, paddle counter, visible_top | vblank_top << 16
+    uint32_t rx;                                // the current line's pixels are drawn up to this clock
     uint32_t pix, pmask, pword;                 // framebuffer word being assembled
     uint32_t tv, ps, sel, uf;                   // PIA timer
 };
@@ -193,130 +194,208 @@ static __device__ void render_fb_flush(uint32_t pix, uint32_t pmask, uint32_t pw
     *w = (*w & keep) | pix;
 }
 
-static __device__ __forceinline__ uint32_t dist160(uint32_t x, uint32_t pos, uint32_t off)
+// Bits 0..7 of b, each repeated over two bits.
+static __device__ __forceinline__ uint32_t r_spread2(uint32_t b)
 {
-    uint32_t cp = pos + off;
-    if (cp >= 160u) cp -= 160u;
-    const uint32_t d = x + 160u - cp;
-    return d >= 160u ? d - 160u : d;
+    uint32_t t = (b | (b << 4)) & 0x0F0Fu;
+    t = (t | (t << 2)) & 0x3333u;
+    t = (t | (t << 1)) & 0x5555u;
+    return t * 3u;
 }
 
-static __device__ __forceinline__ bool r_player(const uint8_t* pv, uint32_t n, uint32_t x)      // tia.rs:423-465
+// Bits 0..7 of b, each repeated over four bits.
+static __device__ __forceinline__ uint32_t r_spread4(uint32_t b)
+{
+    uint32_t t = (b & 0x0Fu) | ((b & 0xF0u) << 12);
+    t = (t | (t << 6)) & 0x03030303u;
+    t = (t | (t << 3)) & 0x11111111u;
+    return t * 0xFu;
+}
+
+// Bits 0..3 of n as byte masks.
+static __device__ __forceinline__ uint32_t r_bytes(uint32_t n)
+{
+    return (((n & 0xFu) * 0x00204081u) & 0x01010101u) * 0xFFu;
+}
+
+// Pixels [X, X + 32) of the 160-pixel line covered by an object of len <= 32
+// pixels starting at pixel s < 160, whose graphics g hold pixel d from its
+// left edge in bit d: bit i = pixel X + i.  An object wraps from pixel 159
+// to pixel 0, as the position arithmetic of tia.rs:406-507 does mod 160.
+static __device__ __forceinline__ uint32_t r_place(uint32_t g, uint32_t len, uint32_t s, uint32_t X)
+{
+    const uint32_t i0 = s >= X ? s - X : s + 160u - X;
+    if (i0 < 32u) return g << i0;
+    const uint32_t d0 = 160u - i0;
+    return d0 < len ? g >> d0 : 0u;
+}
+
+static __device__ __forceinline__ uint32_t r_copies(uint32_t g, uint32_t len, uint32_t pos, uint32_t copies, uint32_t X)
+{
+    uint32_t m = r_place(g, len, pos, X);
+#pragma unroll
+    for (uint32_t c = 1; c < 4u; c++)
+        if ((copies >> c) & 1u) {
+            uint32_t st = pos + (8u << c);                            // copies at +16, +32, +64
+            if (st >= 160u) st -= 160u;
+            m |= r_place(g, len, st, X);
+        }
+    return m;
+}
+
+// Player n over pixels [X, X + 32) (tia.rs:423-465): NUSIZ copies and
+// widths, REFP reflection, VDELP's old graphics.
+static __device__ __forceinline__ uint32_t r_player_mask(const uint8_t* pv, uint32_t n, uint32_t X)
 {
     const uint32_t grp = rp8(pv, n ? (rp8(pv, PB_VDELP1) ? PB_GRP1_OLD : PB_GRP1) : (rp8(pv, PB_VDELP0) ? PB_GRP0_OLD : PB_GRP0));
-    if (grp == 0) return false;
+    if (grp == 0) return 0;
     const uint32_t mode = rp8(pv, n ? PB_NUSIZ1 : PB_NUSIZ0) & 7u;
-    const uint32_t width = mode == 5u ? 2u : mode == 7u ? 4u : 1u, span = 8u * width;
-    const uint32_t pos = rp16(pv, PB_POS + 2u * n), refp = rp8(pv, n ? PB_REFP1 : PB_REFP0);
-    const uint32_t copies = c_copies[mode];
-    for (uint32_t c = 0; c < 4u; c++) {
-        if (!((copies >> c) & 1u)) continue;
-        const uint32_t off = dist160(x, pos, c == 0 ? 0u : 8u << c);
-        if (off < span && off < 80u) {
-            const uint32_t bit = off / width;
-            if (refp ? (grp & (0x01u << bit)) : (grp & (0x80u >> bit))) return true;
-        }
-    }
-    return false;
+    const uint32_t g8 = rp8(pv, n ? PB_REFP1 : PB_REFP0) ? grp : __brev(grp) >> 24;
+    const uint32_t g = mode == 5u ? r_spread2(g8) : mode == 7u ? r_spread4(g8) : g8;
+    const uint32_t len = mode == 5u ? 16u : mode == 7u ? 32u : 8u;
+    return r_copies(g, len, rp16(pv, PB_POS + 2u * n), c_copies[mode], X);
 }
 
-static __device__ __forceinline__ bool r_missile(const uint8_t* pv, uint32_t n, uint32_t x)     // tia.rs:468-497
+// Missile n over pixels [X, X + 32) (tia.rs:468-497).
+static __device__ __forceinline__ uint32_t r_missile_mask(const uint8_t* pv, uint32_t n, uint32_t X)
 {
-    if (!rp8(pv, n ? PB_ENAM1 : PB_ENAM0) || rp8(pv, n ? PB_RESMP1 : PB_RESMP0)) return false;
+    if (!rp8(pv, n ? PB_ENAM1 : PB_ENAM0) || rp8(pv, n ? PB_RESMP1 : PB_RESMP0)) return 0;
     const uint32_t nusiz = rp8(pv, n ? PB_NUSIZ1 : PB_NUSIZ0);
-    const uint32_t width = 1u << ((nusiz >> 4) & 3u), pos = rp16(pv, PB_POS + 4u + 2u * n);
-    const uint32_t copies = c_copies[nusiz & 7u];
-    for (uint32_t c = 0; c < 4u; c++) {
-        if (!((copies >> c) & 1u)) continue;
-        const uint32_t off = dist160(x, pos, c == 0 ? 0u : 8u << c);
-        if (off < width && off < 80u) return true;
-    }
-    return false;
+    const uint32_t len = 1u << ((nusiz >> 4) & 3u);
+    return r_copies((1u << len) - 1u, len, rp16(pv, PB_POS + 4u + 2u * n), c_copies[nusiz & 7u], X);
 }
 
-static __device__ __forceinline__ void r_pixel(RState& s, uint8_t* pv, uint8_t* fbp, uint32_t vis, uint32_t x)
+static __device__ __forceinline__ uint32_t r_sel(uint32_t w, uint32_t color, uint32_t m)
+{
+    return (w & ~m) | (color * 0x01010101u & m);
+}
+
+// Pixels [x0, x1) of visible line `vis` with the TIA registers as they are:
+// Tia::tick's pixel stage (tia.rs:311-346) with compute_pixel (tia.rs:375-403)
+// and the object tests (tia.rs:406-507), over a span in which no register
+// changes.  Each object is a bit mask over 32 pixels at a time; the
+// collision latches are the masks' intersections, and the priority of
+// compute_pixel is the order in which the colors are laid down.  Pixels go
+// to the framebuffer four to a word; a word that the span leaves partly
+// written stays in s.pix / s.pmask for the next span.
+static __device__ __noinline__ RState r_span(RState s, uint8_t* pv, uint8_t* fbp, uint32_t vis, uint32_t x0, uint32_t x1)
 {
     const uint32_t ctrlpf = rp8(pv, PB_CTRLPF);
-    // playfield bit (tia.rs:406-420)
-    const uint32_t pfx = x < 80u ? x >> 2 : ((ctrlpf & 1u) ? 19u - ((x - 80u) >> 2) : (x - 80u) >> 2);
-    const bool pf = pfx <= 3u ? (rp8(pv, PB_PF0) & (0x10u << pfx)) != 0
-                  : pfx <= 11u ? (rp8(pv, PB_PF1) & (0x80u >> (pfx - 4u))) != 0
-                               : (rp8(pv, PB_PF2) & (0x01u << (pfx - 12u))) != 0;
-    const bool p0 = r_player(pv, 0, x), p1 = r_player(pv, 1, x);
-    const bool m0 = r_missile(pv, 0, x), m1 = r_missile(pv, 1, x);
-    bool bl = false;                                                 // tia.rs:500-507
-    if (rp8(pv, rp8(pv, PB_VDELBL) ? PB_ENABL_OLD : PB_ENABL)) {
-        const uint32_t off = dist160(x, rp16(pv, PB_POS + 8u), 0u);
-        bl = off < (1u << ((ctrlpf >> 4) & 3u)) && off < 80u;
+    const uint32_t pfw = (rp8(pv, PB_PF0) >> 4) | (__brev(rp8(pv, PB_PF1)) >> 24 << 4) | (rp8(pv, PB_PF2) << 12);
+    const uint32_t pfr = (ctrlpf & 1u) ? __brev(pfw) >> 12 : pfw;    // the right half, reflected or repeated
+    const uint64_t line = (uint64_t)pfw | ((uint64_t)pfr << 20);     // bit g = playfield pixels 4g..4g+3
+    const bool ben = rp8(pv, rp8(pv, PB_VDELBL) ? PB_ENABL_OLD : PB_ENABL) != 0;
+    const uint32_t blen = 1u << ((ctrlpf >> 4) & 3u);
+    uint32_t cx = 0;                                                 // bit 2r: 0x80 of CXr, bit 2r+1: 0x40
+    for (uint32_t X = x0 & ~31u; X < x1; X += 32u) {
+        const uint32_t lo = x0 > X ? x0 - X : 0u, hi = x1 < X + 32u ? x1 - X : 32u;
+        const uint32_t in = (hi >= 32u ? 0xFFFFFFFFu : (1u << hi) - 1u) & ~((1u << lo) - 1u);
+        const uint32_t pf = r_spread4((uint32_t)(line >> (X >> 2)) & 0xFFu) & in;
+        const uint32_t p0 = r_player_mask(pv, 0, X) & in, p1 = r_player_mask(pv, 1, X) & in;
+        const uint32_t m0 = r_missile_mask(pv, 0, X) & in, m1 = r_missile_mask(pv, 1, X) & in;
+        const uint32_t bl = ben ? r_place((1u << blen) - 1u, blen, rp16(pv, PB_POS + 8u), X) & in : 0u;
+        cx |= ((m0 & p1) ? 0x1u : 0u) | ((m0 & p0) ? 0x2u : 0u) | ((m1 & p0) ? 0x4u : 0u) | ((m1 & p1) ? 0x8u : 0u)
+            | ((p0 & pf) ? 0x10u : 0u) | ((p0 & bl) ? 0x20u : 0u) | ((p1 & pf) ? 0x40u : 0u) | ((p1 & bl) ? 0x80u : 0u)
+            | ((m0 & pf) ? 0x100u : 0u) | ((m0 & bl) ? 0x200u : 0u) | ((m1 & pf) ? 0x400u : 0u) | ((m1 & bl) ? 0x800u : 0u)
+            | ((bl & pf) ? 0x1000u : 0u) | ((p0 & p1) ? 0x4000u : 0u) | ((m0 & m1) ? 0x8000u : 0u);
+        uint32_t A = p0 | m0, B = p1 | m1, F = pf | bl;
+        if ((s.tw & TW_HMOVE) && X == 0u) { A &= ~0xFFu; B &= ~0xFFu; F &= ~0xFFu; }   // HMOVE comb: background
+        const uint32_t c0 = rp8(pv, PB_COLUP0), c1 = rp8(pv, PB_COLUP1), cbk = rp8(pv, PB_COLUBK);
+        const uint32_t cpf = rp8(pv, PB_COLUPF);
+        for (uint32_t q = lo >> 2; q < (hi + 3u) >> 2; q++) {
+            const uint32_t x = X + 4u * q;
+            const uint32_t mA = r_bytes(A >> (4u * q)), mB = r_bytes(B >> (4u * q)), mF = r_bytes(F >> (4u * q));
+            const uint32_t pfc = (ctrlpf & 2u) ? (x < 80u ? c0 : c1) : cpf;   // score mode
+            uint32_t w = cbk * 0x01010101u;
+            if (ctrlpf & 4u) w = r_sel(r_sel(r_sel(w, c1, mB), c0, mA), pfc, mF);   // playfield priority
+            else w = r_sel(r_sel(r_sel(w, pfc, mF), c1, mB), c0, mA);
+            const uint32_t wl = lo > 4u * q ? lo - 4u * q : 0u, wh = hi < 4u * q + 4u ? hi - 4u * q : 4u;
+            const uint32_t pm = ((1u << wh) - 1u) & ~((1u << wl) - 1u);
+            const uint32_t word = (vis * FA_FB_W + x) >> 2;
+            if (word != s.pword || !s.pmask) {
+                render_fb_flush(s.pix, s.pmask, s.pword, fbp);
+                s.pmask = 0;
+                s.pword = word;
+                s.pix = 0;
+            }
+            const uint32_t bm = r_bytes(pm);
+            s.pix = (s.pix & ~bm) | (w & bm);
+            s.pmask |= pm;
+            if (wh == 4u) { render_fb_flush(s.pix, s.pmask, s.pword, fbp); s.pmask = 0; }
+        }
     }
-    const uint32_t c0 = rp8(pv, PB_COLUP0), c1 = rp8(pv, PB_COLUP1), cbk = rp8(pv, PB_COLUBK);
-    const uint32_t pfc = (ctrlpf & 2u) ? (x < 80u ? c0 : c1) : rp8(pv, PB_COLUPF);        // tia.rs:375-403
-    uint32_t color;
-    if (ctrlpf & 4u) color = (pf || bl) ? pfc : (p0 || m0) ? c0 : (p1 || m1) ? c1 : cbk;
-    else color = (p0 || m0) ? c0 : (p1 || m1) ? c1 : (pf || bl) ? pfc : cbk;
-    if ((s.tw & TW_HMOVE) && x < 8u) color = cbk;                 // HMOVE comb
-    const uint32_t idx = vis * FA_FB_W + x;
-    if ((idx >> 2) != s.pword || !s.pmask) {
-        render_fb_flush(s.pix, s.pmask, s.pword, fbp);
-        s.pmask = 0;
-        s.pword = idx >> 2;
-        s.pix = 0;
-    }
-    s.pix |= color << (8u * (idx & 3u));
-    s.pmask |= 1u << (idx & 3u);
-    if ((idx & 3u) == 3u) { render_fb_flush(s.pix, s.pmask, s.pword, fbp); s.pmask = 0; }
-    if (m0 | m1 | p0 | p1 | bl) {                                   // collision latches (tia.rs:329-343)
-        const uint32_t cx[8] = {
-            (m0 && p1 ? 0x80u : 0u) | (m0 && p0 ? 0x40u : 0u), (m1 && p0 ? 0x80u : 0u) | (m1 && p1 ? 0x40u : 0u),
-            (p0 && pf ? 0x80u : 0u) | (p0 && bl ? 0x40u : 0u), (p1 && pf ? 0x80u : 0u) | (p1 && bl ? 0x40u : 0u),
-            (m0 && pf ? 0x80u : 0u) | (m0 && bl ? 0x40u : 0u), (m1 && pf ? 0x80u : 0u) | (m1 && bl ? 0x40u : 0u),
-            (bl && pf ? 0x80u : 0u), (p0 && p1 ? 0x80u : 0u) | (m0 && m1 ? 0x40u : 0u) };
+    if (cx) {                                                        // collision latches (tia.rs:329-343)
 #pragma unroll
-        for (uint32_t r = 0; r < 8u; r++)
-            if (cx[r]) wp8(pv, PB_CX + r, rp8(pv, PB_CX + r) | cx[r]);
+        for (uint32_t r = 0; r < 8u; r++) {
+            const uint32_t b = (((cx >> (2u * r)) & 1u) ? 0x80u : 0u) | (((cx >> (2u * r + 1u)) & 1u) ? 0x40u : 0u);
+            if (b) wp8(pv, PB_CX + r, rp8(pv, PB_CX + r) | b);
+        }
     }
+    return s;
 }
 
-// One TIA clock (tia.rs:271-372).
-static __device__ __forceinline__ void r_tick(RState& s, uint32_t pins, uint8_t* pv, uint8_t* fbp)
+// The pixels of the current line from clock s.rx up to clock `upto`, with
+// the registers as they are: pixels are drawn only when something that
+// affects them is about to change (a register write, a delayed playfield
+// write, a collision read, the end of the line or of the call).
+static __device__ __forceinline__ void r_pending(RState& s, uint8_t* pv, uint8_t* fbp, uint32_t upto)
 {
+    const uint32_t from = s.rx > 68u ? s.rx : 68u;
+    s.rx = upto;
+    if (upto <= from || (s.tw & 0x200u)) return;
+    const uint32_t vis = (s.scanline - (s.vtop & 0xFFFFu)) & 0xFFFFu;
+    if (vis < FA_FB_H) s = r_span(s, pv, fbp, vis, from - 68u, upto - 68u);
+}
+
+// n TIA clocks, exactly as n calls of Tia::tick (tia.rs:271-372), advanced a
+// line at a time: between register writes nothing but the pixels, the
+// collision latches and the beam changes from one clock to the next (the
+// input latches are idempotent, the resizer's candidate is the scanline
+// itself, and a delayed playfield write fires on the first clock after it).
+static __device__ __forceinline__ void r_advance(RState& s, uint32_t n, uint32_t pins, uint8_t* pv, uint8_t* fbp)
+{
+    if (n == 0) return;
+    const uint32_t dlen = rp8(pv, RB_DLEN);
+    if (dlen) {                                                      // every pending write has one clock left
+        r_pending(s, pv, fbp, s.clock);
+        for (uint32_t i = 0; i < dlen; i++) {
+            const uint32_t reg = rp8(pv, RB_DQ + 3u * i + 1u), val = rp8(pv, RB_DQ + 3u * i + 2u);
+            wp8(pv, reg == 0x0Du ? PB_PF0 : reg == 0x0Eu ? PB_PF1 : PB_PF2, val);
+        }
+        wp8(pv, RB_DLEN, 0u);
+    }
     if (s.tw & TW_LATCH) {
         if (!(pins & 0x10000u)) s.tw &= ~TW_L4;
         if (!(pins & 0x20000u)) s.tw &= ~TW_L5;
     }
-    if (!(s.tw & 0x200u) && s.scanline >= 23u && s.scanline < (s.vtop >> 16)) s.vtop = (s.vtop & 0xFFFFu) | (s.scanline << 16);
-    const uint32_t dlen = rp8(pv, RB_DLEN);
-    if (dlen) {
-        uint32_t dst = 0;
-        for (uint32_t i = 0; i < dlen; i++) {
-            const uint32_t rem = rp8(pv, RB_DQ + 3u * i) - 1u, reg = rp8(pv, RB_DQ + 3u * i + 1u), val = rp8(pv, RB_DQ + 3u * i + 2u);
-            if (rem == 0) {
-                wp8(pv, reg == 0x0Du ? PB_PF0 : reg == 0x0Eu ? PB_PF1 : PB_PF2, val);
-            } else {
-                wp8(pv, RB_DQ + 3u * dst, rem);
-                wp8(pv, RB_DQ + 3u * dst + 1u, reg);
-                wp8(pv, RB_DQ + 3u * dst + 2u, val);
-                dst++;
+    while (n) {
+        if (!(s.tw & 0x200u) && s.scanline >= 23u && s.scanline < (s.vtop >> 16))
+            s.vtop = (s.vtop & 0xFFFFu) | (s.scanline << 16);
+        const uint32_t seg = n < 228u - s.clock ? n : 228u - s.clock;
+        s.clock += seg;
+        n -= seg;
+        if (s.clock >= 228u) {
+            r_pending(s, pv, fbp, 228u);
+            s.clock = 0;
+            s.rx = 0;
+            s.scanline = (s.scanline + 1u) & 0xFFFFu;
+            s.tw &= ~(TW_WSYNC | TW_HMOVE);
+            if (s.scanline == (s.vtop & 0xFFFFu)) {                  // framebuffer cleared (tia.rs:349-351)
+                s.pmask = 0;
+                uint4* w = (uint4*)fbp;
+                for (uint32_t q = 0; q < FA_FB_BYTES / 16u; q++) w[q] = make_uint4(0u, 0u, 0u, 0u);
             }
+            if (!(s.tw & TW_PDUMP) && s.pcnt < 256u) s.pcnt++;
+            if (s.scanline >= 262u) { s.scanline = 0; s.tw |= TW_FCOMP; }
         }
-        wp8(pv, RB_DLEN, dst);
     }
-    const uint32_t px = (s.clock - 68u) & 0xFFFFu;
-    const uint32_t vis = (s.scanline - (s.vtop & 0xFFFFu)) & 0xFFFFu;
-    if (s.clock >= 68u && px < FA_FB_W && !(s.tw & 0x200u) && vis < FA_FB_H) r_pixel(s, pv, fbp, vis, px);
-    s.clock++;
-    if (s.clock >= 228u) {
-        s.clock = 0;
-        s.scanline = (s.scanline + 1u) & 0xFFFFu;
-        s.tw &= ~(TW_WSYNC | TW_HMOVE);
-        if (s.scanline == (s.vtop & 0xFFFFu)) {                  // framebuffer cleared (tia.rs:349-351)
-            s.pmask = 0;
-            uint4* w = (uint4*)fbp;
-            for (uint32_t q = 0; q < FA_FB_BYTES / 16u; q++) w[q] = make_uint4(0u, 0u, 0u, 0u);
-        }
-        if (!(s.tw & TW_PDUMP) && s.pcnt < 256u) s.pcnt++;
-        if (s.scanline >= 262u) { s.scanline = 0; s.tw |= TW_FCOMP; }
-    }
+}
+
+// The pending pixels of the current line, up to the beam.
+static __device__ __noinline__ RState render_pending(RState s, uint8_t* pv, uint8_t* fbp)
+{
+    r_pending(s, pv, fbp, s.clock);
+    return s;
 }
 
 static __device__ __forceinline__ void r_pia_tick(RState& s)     // pia.rs:80-103
@@ -329,22 +408,32 @@ static __device__ __forceinline__ void r_pia_tick(RState& s)     // pia.rs:80-10
     }
 }
 
-// n CPU cycles of the rendering console: three TIA clocks and one PIA clock each.
+// m calls of Pia::tick (pia.rs:80-103), a prescaler period at a time.
+static __device__ __forceinline__ void r_pia_ticks(RState& s, uint32_t m)
+{
+    while (m) {
+        if (s.ps == 0 || (s.uf && s.tv == 0)) { r_pia_tick(s); m--; continue; }
+        if (s.uf && s.ps == 1u) { s.tv = (s.tv - m) & 0xFFu; return; }   // after underflow: one count per tick
+        if (m < s.ps) { s.ps -= m; return; }
+        m -= s.ps;                                                   // the tick that empties the prescaler
+        s.ps = s.uf ? 1u : s.sel;
+        if (s.tv == 0) { s.uf = 1; s.tv = 0xFFu; } else s.tv -= 1u;
+    }
+}
+
+// n CPU cycles of the rendering console: three TIA clocks and one PIA clock
+// each (the TIA and the PIA do not interact, so each is advanced in bulk).
 static __device__ __noinline__ RState render_cycles(RState s, uint32_t n, uint32_t pins, uint8_t* pv, uint8_t* fbp)
 {
-    for (uint32_t c = 0; c < n; c++) {
-        r_tick(s, pins, pv, fbp);
-        r_tick(s, pins, pv, fbp);
-        r_tick(s, pins, pv, fbp);
-        r_pia_tick(s);
-    }
+    r_advance(s, 3u * n, pins, pv, fbp);
+    r_pia_ticks(s, n);
     return s;
 }
 
-// n TIA clocks alone (the clocks around a write, src/atari.rs:207-222).
+// n TIA clocks alone (the clocks around a PIA write, src/atari.rs:207-222).
 static __device__ __noinline__ RState render_tia_ticks(RState s, uint32_t n, uint32_t pins, uint8_t* pv, uint8_t* fbp)
 {
-    for (uint32_t c = 0; c < n; c++) r_tick(s, pins, pv, fbp);
+    r_advance(s, n, pins, pv, fbp);
     return s;
 }
 
@@ -368,9 +457,9 @@ static __device__ __forceinline__ void r_resize_commit(RState& s, uint8_t* pv)  
 }
 
 // Tia::write (tia.rs:570-674) of register a & 0x3F.
-static __device__ __noinline__ RState render_write(uint32_t a, uint32_t v, RState s, uint8_t* pv, uint8_t* fbp)
+static __device__ __forceinline__ void r_write(uint32_t a, uint32_t v, RState& s, uint8_t* pv, uint8_t* fbp)
 {
-    (void)fbp;
+    r_pending(s, pv, fbp, s.clock);                                  // the pixels drawn before the write
     switch (a & 0x3Fu) {
     case 0x00:
         if (!(s.tw & 2u) && (v & 2u)) { r_resize_commit(s, pv); s.scanline = 0; s.tw |= TW_FCOMP; }
@@ -432,6 +521,16 @@ static __device__ __noinline__ RState render_write(uint32_t a, uint32_t v, RStat
     case 0x2C: for (uint32_t o = 0; o < 8u; o++) wp8(pv, PB_CX + o, 0u); break;
     default: break;                                                 // RSYNC, audio
     }
+}
+
+// Bus::write of a TIA register (src/atari.rs:207-222): two TIA clocks, the
+// write, one TIA clock (the PIA clock follows in the caller).
+static __device__ __noinline__ RState render_write_cycle(uint32_t a, uint32_t v, RState s, uint32_t pins, uint8_t* pv,
+                                                         uint8_t* fbp)
+{
+    r_advance(s, 2u, pins, pv, fbp);
+    r_write(a, v, s, pv, fbp);
+    r_advance(s, 1u, pins, pv, fbp);
     return s;
 }
 
@@ -603,7 +702,7 @@ struct Emu {
         if constexpr (RENDER) {
             rsync(j);
             const uint32_t v = r_io_read(a);
-            rcycle();
+            rcycles(1u);
             done = j + 1u;
             return v;
         } else {
@@ -1001,33 +1100,47 @@ struct Emu {
     // ------------------------------------------------------------ rendering console
     // Used only by RENDER instantiations.  The pixel-accurate Tia of the
     // reference's rendering console (src/tia.rs) and Pia::tick run out of
-    // line (render_cycles / render_tia_ticks / render_read / render_write,
+    // line (render_cycles / render_tia_ticks / render_read / render_write_cycle,
     // below), on the state they touch passed by value: one copy of the pixel
     // pipeline however many bus-access sites the interpreter has.
-    uint32_t done;            // cycles of the current instruction already ticked
+    uint32_t done;            // cycle of the current instruction the TIA and PIA have reached (0 - lag at its start)
+    uint32_t lag;             // CPU cycles of earlier instructions not yet given to the TIA and PIA
     uint32_t vtop;            // visible_top | vblank_top << 16
     uint8_t* fbp;             // this instance's framebuffer, 160 x 192 palette indices
     uint32_t pix, pmask, pword;   // the framebuffer word being assembled: pixels, their mask, its index
+    uint32_t rx;              // the current line's pixels are drawn up to this TIA clock
 
     __device__ __forceinline__ RState rpack() const
     {
         RState r;
         r.clock = clock; r.scanline = scanline; r.tw = tw; r.pcnt = pcnt; r.vtop = vtop;
         r.pix = pix; r.pmask = pmask; r.pword = pword; r.tv = tv; r.ps = ps; r.sel = sel; r.uf = uf;
+        r.rx = rx;
         return r;
     }
     __device__ __forceinline__ void runpack(const RState& r)
     {
         clock = r.clock; scanline = r.scanline; tw = r.tw; pcnt = r.pcnt; vtop = r.vtop;
         pix = r.pix; pmask = r.pmask; pword = r.pword; tv = r.tv; ps = r.ps; sel = r.sel; uf = r.uf;
+        rx = r.rx;
     }
+    // The TIA and the PIA up to cycle j of the current instruction.  They are
+    // advanced only before an access that observes or changes them: the
+    // cycles of instructions that touch only ROM and RAM are owed (lag) and
+    // given in one piece.
     __device__ __forceinline__ void rsync(uint32_t j)
     {
-        if (done < j) { runpack(render_cycles(rpack(), j - done, pins, pv, fbp)); done = j; }
+        const uint32_t d = j - done;
+        if ((int32_t)d > 0) { runpack(render_cycles(rpack(), d, pins, pv, fbp)); done = j; }
     }
-    __device__ __forceinline__ void rcycle() { runpack(render_cycles(rpack(), 1u, pins, pv, fbp)); }
+    __device__ __forceinline__ void rcycles(uint32_t n) { runpack(render_cycles(rpack(), n, pins, pv, fbp)); }
+    __device__ __forceinline__ void settle()
+    {
+        if (lag) { runpack(render_cycles(rpack(), lag, pins, pv, fbp)); lag = 0; }
+    }
     __device__ __forceinline__ uint32_t r_io_read(uint32_t a)
     {
+        if ((a & 0x1080u) == 0 && (a & 0x0Fu) < 8u) runpack(render_pending(rpack(), pv, fbp));   // collisions so far
         const uint2 r = render_read(a, rpack(), pins, pads, ports, pv);
         if (r.y) uf = 0;                                            // INTIM read clears the flag
         return r.x;
@@ -1035,14 +1148,15 @@ struct Emu {
     // Bus::write of a TIA or PIA register (src/atari.rs:207-222).
     __device__ __forceinline__ void r_write_cycle(uint32_t a, uint32_t v)
     {
-        RState r = render_tia_ticks(rpack(), 2u, pins, pv, fbp);
+        RState r;
         if ((a & 0x1080u) != 0) {
+            r = render_tia_ticks(rpack(), 2u, pins, pv, fbp);
             const uint4 q = pia_write_io(a, v, ports, r.tv, r.ps, r.sel | (r.uf << 16));
             ports = q.x; r.tv = q.y; r.ps = q.z; r.sel = q.w & 0xFFFFu; r.uf = q.w >> 16;
+            r = render_tia_ticks(r, 1u, pins, pv, fbp);
         } else {
-            r = render_write(a, v, r, pv, fbp);
+            r = render_write_cycle(a, v, rpack(), pins, pv, fbp);
         }
-        r = render_tia_ticks(r, 1u, pins, pv, fbp);
         runpack(r);
         pia_tick1();
     }
@@ -1055,7 +1169,13 @@ struct Emu {
             if (tv == 0) { uf = 1; tv = 0xFFu; } else tv -= 1u;
         }
     }
-    __device__ __forceinline__ void fb_flush() { render_fb_flush(pix, pmask, pword, fbp); pmask = 0; }
+    __device__ __forceinline__ void fb_flush()
+    {
+        settle();
+        runpack(render_pending(rpack(), pv, fbp));
+        render_fb_flush(pix, pmask, pword, fbp);
+        pmask = 0;
+    }
 
     // HeadlessAtari::set_action (src/atari.rs:571-582).
     __device__ __forceinline__ void apply_action(uint32_t act)

@@ -9,8 +9,10 @@
 // (Emu<32, true>): each of its bus accesses knows its cycle within the
 // instruction, and before an access reaches a TIA or PIA register the TIA
 // and PIA are ticked up to that cycle, so register writes land at the beam
-// position the reference gives them; the rest of the instruction's cycles
-// are ticked after it.
+// position the reference gives them.  Cycles of instructions that touch
+// only ROM and RAM are owed and given at the next such access (or at the end
+// of the frame), and pixels are drawn a span at a time, when something that
+// affects them is about to change: the same framebuffer, fewer calls.
 //
 // One warp per unit of 32 consoles, WARPS units per CTA; the cart's ROM and
 // one private-byte slab per warp (RAM + graphics registers, FA_RPRIV_BYTES
@@ -21,10 +23,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "../../include/fast_atari.h"
@@ -70,14 +75,28 @@ struct RRunner {
     __device__ __forceinline__ bool one()
     {
         uint32_t n;
+        if (e.wsync()) e.settle();                                   // the wait starts where the beam is
         if (e.wsync()) {
-            e.rcycle();
-            n = 1;
+            // The cycles of a WSYNC wait up to the end of the line, cut where
+            // a per-cycle frame check would first fire: nothing else changes
+            // from one cycle of the wait to the next.
+            n = (228u - e.clock + 2u) / 3u;
+            uint32_t lim;
+            if (phase == 0u) lim = e.vsync_on() ? FA_VSYNC_BUDGET + 1u - fcyc : 1u;
+            else lim = FA_FRAME_CYCLE_CAP + 1u - fcyc;
+            n = n < lim ? n : lim;
+            e.rcycles(n);
         } else {
-            e.done = 0;
+            e.done = 0u - e.lag;
             n = e.step();
-            if (n == 0) { e.fold_cycles(); e.set_status(FA_STATUS_ILLEGAL_OPCODE); active = false; return false; }
-            e.rsync(n);
+            if (n == 0) {
+                if ((int32_t)e.done >= 0) e.lag = 0;                 // the owed cycles went with an access
+                e.fold_cycles();
+                e.set_status(FA_STATUS_ILLEGAL_OPCODE);
+                active = false;
+                return false;
+            }
+            e.lag = n - e.done;
             e.instr++;
             e.cyc_acc += n;
         }
@@ -94,6 +113,7 @@ struct RRunner {
             const bool cap = fcyc > FA_FRAME_CYCLE_CAP;
             if (cap || e.vsync_on()) {
                 if (cap) e.set_status(FA_STATUS_CYCLE_CAP);
+                e.settle();                                          // before the next frame's action moves the pins
                 e.fold_cycles();
                 e.row(R_FRAME) += 1u;
                 f++;
@@ -109,8 +129,7 @@ struct RRunner {
         const uint32_t mid = sched == FA_SCHED_LINE ? (e.scanline < 0x1FFu ? e.scanline : 0x1FFu) : (e.bank >> 3);
         return (fc << 25) | (mid << 16) | e.pc;
     }
-    // A WSYNC wait is consumed cycle by cycle, with the frame checks after
-    // each cycle, without going back to the warp scheduler.
+    // A WSYNC wait is consumed without going back to the warp scheduler.
     __device__ __forceinline__ void iterate()
     {
 #pragma unroll 1
@@ -119,8 +138,11 @@ struct RRunner {
     }
 };
 
+// 80 registers: 24 resident warps per SM (three 256-thread CTAs), the
+// occupancy that the shared-memory slabs allow; ptxas would otherwise take
+// 128 for the pixel code and hold the SM to 16 warps.
 template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) fa_render_run(const __grid_constant__ FaRenderLaunch L)
+__global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLaunch L)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t bar;
@@ -174,10 +196,12 @@ __global__ void __launch_bounds__(WARPS * 32) fa_render_run(const __grid_constan
     e.bank = 0;
     e.scanline = 0;
     e.done = 0;
+    e.lag = 0;
     e.pix = 0;
     e.pmask = 0;
     e.pword = 0;
     e.vtop = 0;
+    e.rx = 0;
     e.fbp = L.fb + (size_t)(valid ? i : 0u) * FA_FB_BYTES;
     uint32_t* col = L.state + i;
     const uint32_t S = L.stride;
@@ -189,6 +213,7 @@ __global__ void __launch_bounds__(WARPS * 32) fa_render_run(const __grid_constan
             w[k * 32u] = col[(size_t)(FA_RROW_EXTRA + (k - FA_PRIV_WORDS)) * S];
         e.load_hot(col, S);
         e.vtop = col[(size_t)RR_VTOP * S];
+        e.rx = e.clock;
         const uint32_t fl = col[(size_t)RR_FLAGS * S];
         e.tw |= ((fl & 1u) ? TW_HMOVE : 0u) | ((fl & 2u) ? TW_LATCH : 0u) | ((fl & 4u) ? TW_L4 : 0u) |
                 ((fl & 8u) ? TW_L5 : 0u);
@@ -226,6 +251,15 @@ __global__ void __launch_bounds__(WARPS * 32) fa_render_run(const __grid_constan
 }  // namespace fa
 
 // ------------------------------------------------------------------ host side
+// One host thread's share of a device-to-host copy into pageable memory:
+// two pinned chunks and a stream, so that the GPU fills one chunk while the
+// thread copies the other into the caller's buffer.
+struct FaStager {
+    uint8_t* buf[2] = {nullptr, nullptr};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done[2] = {nullptr, nullptr};
+};
+
 struct fa_render {
     int device = 0;
     size_t n = 0;
@@ -246,6 +280,7 @@ struct fa_render {
     int sched = FA_SCHED_PC;
     bool reset_done = false;
     unsigned long long last_instr = 0, last_slots = 0;
+    std::vector<FaStager> stagers;   // made on the first large copy out
 };
 
 namespace {
@@ -298,8 +333,72 @@ void free_render(fa_render* r)
     cudaFree(r->d_obs);
     cudaFree(r->d_err);
     cudaFree(r->d_ctr);
+    for (FaStager& g : r->stagers) {
+        if (g.stream) cudaStreamSynchronize(g.stream);
+        for (int b = 0; b < 2; b++) {
+            if (g.buf[b]) cudaFreeHost(g.buf[b]);
+            if (g.done[b]) cudaEventDestroy(g.done[b]);
+        }
+        if (g.stream) cudaStreamDestroy(g.stream);
+    }
     if (r->stream) cudaStreamDestroy(r->stream);
     delete r;
+}
+
+constexpr size_t kStageChunk = 8u << 20;   // bytes per pinned chunk
+constexpr unsigned kStageThreads = 8;      // host threads of a staged copy (at most)
+
+// bytes from device memory to pageable host memory, after the work already
+// finished on the device.  A plain cudaMemcpy into pageable memory goes
+// through the driver's own bounce buffer at a few GB/s; here up to
+// kStageThreads host threads each move a contiguous share through their own
+// two pinned chunks, so the PCIe transfer and the host-side copies overlap.
+int copy_d2h(fa_render* r, uint8_t* dst, const uint8_t* src, size_t bytes)
+{
+    if (bytes < 2 * kStageChunk) {
+        FA_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+        return FA_OK;
+    }
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned T = (unsigned)std::min<size_t>({(size_t)kStageThreads, (size_t)hw, bytes / kStageChunk});
+    while (r->stagers.size() < T) {
+        FaStager g;
+        cudaError_t e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking);
+        for (int b = 0; b < 2 && e == cudaSuccess; b++) {
+            e = cudaHostAlloc((void**)&g.buf[b], kStageChunk, cudaHostAllocDefault);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.done[b], cudaEventDisableTiming);
+        }
+        r->stagers.push_back(g);   // freed with the handle, complete or not
+        if (e != cudaSuccess) return fa_fail(FA_ERR_CUDA, "pinned staging: %s", cudaGetErrorString(e));
+    }
+    std::atomic<int> bad{0};
+    std::vector<std::thread> th;
+    th.reserve(T);
+    for (unsigned t = 0; t < T; t++) {
+        th.emplace_back([&, t] {
+            if (cudaSetDevice(r->device) != cudaSuccess) { bad.store(1); return; }
+            FaStager& g = r->stagers[t];
+            const size_t lo = bytes * t / T, hi = bytes * (t + 1) / T;
+            const size_t chunks = (hi - lo + kStageChunk - 1) / kStageChunk;
+            auto issue = [&](size_t c) {
+                const size_t off = lo + c * kStageChunk, len = std::min(kStageChunk, hi - off);
+                if (cudaMemcpyAsync(g.buf[c & 1], src + off, len, cudaMemcpyDeviceToHost, g.stream) != cudaSuccess ||
+                    cudaEventRecord(g.done[c & 1], g.stream) != cudaSuccess)
+                    bad.store(1);
+            };
+            issue(0);
+            for (size_t c = 0; c < chunks && !bad.load(); c++) {
+                if (c + 1 < chunks) issue(c + 1);   // its chunk was emptied in the previous round
+                if (cudaEventSynchronize(g.done[c & 1]) != cudaSuccess) { bad.store(1); break; }
+                const size_t off = lo + c * kStageChunk;
+                std::memcpy(dst + off, g.buf[c & 1], std::min(kStageChunk, hi - off));
+            }
+            cudaStreamSynchronize(g.stream);
+        });
+    }
+    for (std::thread& x : th) x.join();
+    if (bad.load()) return fa_fail(FA_ERR_CUDA, "staged device-to-host copy failed");
+    return FA_OK;
 }
 
 // Atari::new (src/atari.rs:240-247) as one state column: the headless power-on
@@ -378,8 +477,11 @@ int finish(fa_render* r)
 
 int copy_out(fa_render* r, uint8_t* fb_out, uint8_t* ram_out)
 {
-    if (fb_out) FA_CUDA(cudaMemcpy(fb_out, r->d_fb, r->n * (size_t)FA_FB_BYTES, cudaMemcpyDeviceToHost));
-    if (ram_out) FA_CUDA(cudaMemcpy(ram_out, r->d_obs, r->n * 128u, cudaMemcpyDeviceToHost));
+    if (fb_out) {
+        const int rc = copy_d2h(r, fb_out, r->d_fb, r->n * (size_t)FA_FB_BYTES);
+        if (rc) return rc;
+    }
+    if (ram_out) return copy_d2h(r, ram_out, r->d_obs, r->n * 128u);
     return FA_OK;
 }
 }  // namespace
@@ -508,8 +610,7 @@ extern "C" int fa_render_get_framebuffers(fa_render* r, uint8_t* out)
     CHECK_R(r);
     if (!out) return fa_fail(FA_ERR_INVALID, "out is null");
     FA_CUDA(cudaStreamSynchronize(r->stream));
-    FA_CUDA(cudaMemcpy(out, r->d_fb, r->n * (size_t)FA_FB_BYTES, cudaMemcpyDeviceToHost));
-    return FA_OK;
+    return copy_d2h(r, out, r->d_fb, r->n * (size_t)FA_FB_BYTES);
 }
 
 extern "C" int fa_render_get_states(fa_render* r, fa_state* out)
