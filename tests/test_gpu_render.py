@@ -88,3 +88,19 @@ def test_render_frames_are_pictures_and_depend_on_actions():
     assert (fb != 0).sum(axis=(1, 2)).min() > 1000                 # every console drew something
     assert len(np.unique(fb)) > 8                                    # several colours
     assert len({fb[i].tobytes() for i in range(n)}) >= 4             # the actions show in the pictures
+
+
+def test_render_large_batch_copy_out():
+    # 1,500 framebuffers (46 MB) leave the device through the pipelined copy
+    # (several host threads with pinned chunks, uneven shares, a short last
+    # chunk); every byte must land where the oracle puts it.
+    rom = carts.render_cart().rom
+    n, k = 1500, 2
+    acts = carts.actions(seed=91, n=n, frames=k)
+    consoles = oracle.render_reset(rom, n)
+    oracle.render_steps(consoles, acts)
+    with fa.AtariRender(rom, n) as g:
+        g.reset()
+        fb, ram = g.step_multi(acts, k)
+        assert np.array_equal(g.framebuffers(), fb)
+        check(fb, ram, g.states(), consoles, "1500 consoles")
