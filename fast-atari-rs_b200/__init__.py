@@ -53,7 +53,7 @@ STATE_DTYPE = np.dtype([
     ("ctrlpf", "u1"), ("refp0", "u1"), ("refp1", "u1"),
     ("pf0", "u1"), ("pf1", "u1"), ("pf2", "u1"),
     ("bank", "u1"), ("scheme", "u1"), ("_pad_end", "u1", (2,)),
-    ("_pad_ext", "u1", (3,)),
+    ("mapper", "u1", (2,)), ("_pad_ext", "u1"),
     ("cycles", "<u8"), ("frame_no", "<u4"), ("run_status", "<u4"),
 ])
 assert STATE_DTYPE.itemsize == 240
@@ -121,6 +121,9 @@ _SIGS = {
     "fa_server_get_states": (_i, [_vp, ctypes.c_int64, _u32, _u32, _vp]),
     "fa_server_stats_get": (_i, [_vp, _vp]),
     "fa_server_loadgen": (_i, [_vp, _vp, _vp, _vp]),
+    "fa_rom_set_scheme": (_i, [_u8p, _sz, _i]),
+    "fa_rom_scheme": (_i, [_u8p, _sz]),
+    "fa_rom_guess_scheme": (_i, [_u8p, _sz]),
     "fa_render_create": (_i, [_u8p, _sz, _sz, ctypes.POINTER(_vp)]),
     "fa_render_destroy": (None, [_vp]),
     "fa_render_num_envs": (_sz, [_vp]),
@@ -135,6 +138,7 @@ _SIGS = {
     "fa_render_last_instructions": (ctypes.c_ulonglong, [_vp]),
 }
 
+FA_ERR_BAD_ROM = -2
 FA_ERR_CAPACITY = -6
 FA_ERR_TIMEOUT = -7
 SERVE_BATCHED, SERVE_PLAIN = 0, 1
@@ -188,6 +192,37 @@ def device_count() -> int:
 
 def set_device(device: int) -> None:
     _check(lib().fa_set_device(int(device)))
+
+
+SCHEME_NAMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "auto": -1}
+
+
+def _scheme_code(scheme) -> int:
+    return SCHEME_NAMES[scheme.lower()] if isinstance(scheme, str) else int(scheme)
+
+
+def set_rom_scheme(rom: bytes, scheme) -> None:
+    """Every later handle, pool, server or rendering console given these ROM
+    bytes uses `scheme` ("e0", "3f", ... or "auto" to forget it) instead of
+    the reference's size rule (fa_rom_set_scheme)."""
+    r = np.frombuffer(bytes(rom), dtype=np.uint8).copy()
+    _check(lib().fa_rom_set_scheme(_u8(r), len(r), _scheme_code(scheme)))
+
+
+def rom_scheme(rom: bytes) -> int:
+    """The scheme the library will use for these bytes (fa_rom_scheme)."""
+    r = np.frombuffer(bytes(rom), dtype=np.uint8).copy()
+    rc = int(lib().fa_rom_scheme(_u8(r), len(r)))
+    _check(min(rc, 0))
+    return rc
+
+
+def guess_rom_scheme(rom: bytes) -> int:
+    """A scheme guessed from the ROM's code (fa_rom_guess_scheme); not applied."""
+    r = np.frombuffer(bytes(rom), dtype=np.uint8).copy()
+    rc = int(lib().fa_rom_guess_scheme(_u8(r), len(r)))
+    _check(min(rc, 0))
+    return rc
 
 
 class BatchAtariGpu:

@@ -726,3 +726,180 @@ def render_cart(seed: int = 5) -> Cart:
     a.raw(bytes([0x00, 0xF0, 0x00, 0xF0]))
     img, labels, _ = a.assemble(4096)
     return Cart(CartSpec("render_4k_fixed", 4096, seed, wsync_density=1.0), bytes(img), labels)
+
+
+# ------------------------------------------------ sliced-bank carts (E0, 3F)
+# Routines that run from a switchable window are position-independent:
+# relative branches only, entered by JSR at the window's base, leaving by RTS.
+# They write RAM ($82-$EF) and, where the scheme allows, TIA registers, and
+# read ROM data through every window, so a wrong mapping changes RAM.
+
+def _window_routine(rng: Rng, size: int, tia_writes: bool, data_lo: int, data_hi: int,
+                    avoid=(0, 0), tail: bytes = b"") -> bytes:
+    a = Asm(0xF000)
+    nunits = rng.range(10, 24)
+
+    def ram() -> int:
+        return rng.range(RAM_W_LO, RAM_W_HI)
+
+    def rom_data() -> int:
+        while True:
+            d = rng.range(data_lo, data_hi)
+            if not (avoid[0] <= d <= avoid[1]):
+                return d
+
+    for u in range(nunits):
+        k = rng.below(9)
+        if k == 0:
+            a.ins("LDA", "zp", ram()); a.ins("ADC", "imm", rng.below(256)); a.ins("STA", "zp", ram())
+        elif k == 1:                                                # ROM data through any window
+            a.ins("LDA", "zp", ram()); a.ins("EOR", "abs", rom_data()); a.ins("STA", "zp", ram())
+        elif k == 2:                                                # indexed ROM data
+            a.ins("LDX", "zp", ram()); a.ins("LDA", "absx", rom_data() & 0xFF00 | rng.below(0x80))
+            a.ins("STA", "zp", ram())
+        elif k == 3:
+            a.ins(rng.choice(["INC", "DEC", "ASL", "ROR"]), "zp", ram())
+        elif k == 4:                                                # counted loop
+            a.ins("LDY", "imm", rng.range(1, 6)); a.label(f"l{u}"); a.ins("DEY"); a.ins("BNE", "rel", f"l{u}")
+        elif k == 5:                                                # data-dependent skip
+            a.ins("LDA", "zp", ram()); a.ins(rng.choice(["BMI", "BPL", "BEQ", "BNE"]), "rel", f"s{u}")
+            a.ins("INC", "zp", ram()); a.label(f"s{u}")
+        elif k == 6 and tia_writes:
+            a.ins("LDA", "zp", ram()); a.ins("STA", "zp", rng.choice(TIA_WRITABLE))
+        elif k == 7:                                                # timer and inputs
+            a.ins("LDA", "abs", rng.choice([INTIM, SWCHA])); a.ins("EOR", "zp", ram()); a.ins("STA", "zp", ram())
+        else:
+            a.ins("LDA", "zp", ram()); a.ins("PHA"); a.ins("LDA", "zp", ram()); a.ins("STA", "zp", ram())
+            a.ins("PLA"); a.ins("ADC", "zp", ram()); a.ins("STA", "zp", ram())
+    a.ins("RTS")
+    img = bytearray(a.assemble(size)[0])
+    body_end = 0
+    for i in range(len(img) - 1, -1, -1):
+        if img[i]:
+            body_end = i + 1
+            break
+    for i in range(body_end, size - len(tail)):                     # the rest is ROM data
+        img[i] = rng.below(256)
+    if tail:
+        assert body_end <= size - len(tail)
+        img[size - len(tail):] = tail
+    return bytes(img)
+
+
+def _frame_head(a: Asm, lines: int):
+    a.label("frame")
+    a.ins("LDA", "imm", 0x02); a.ins("STA", "zp", VSYNC)
+    a.ins("STA", "zp", WSYNC); a.ins("STA", "zp", WSYNC); a.ins("STA", "zp", WSYNC)
+    a.ins("LDA", "imm", 0x00); a.ins("STA", "zp", VSYNC)
+    a.ins("LDA", "imm", 0x82); a.ins("STA", "zp", VBLANK)
+    _wsync_lines(asm=a, n=36, tag="vbl")
+    a.ins("LDA", "abs", SWCHA); a.ins("EOR", "zp", MIX); a.ins("STA", "zp", MIX)
+    a.ins("LDA", "zp", INPT4); a.ins("ADC", "zp", MIX); a.ins("STA", "zp", MIX)
+    a.ins("LDA", "imm", 0x00); a.ins("STA", "zp", VBLANK)
+    a.ins("LDA", "imm", lines); a.ins("STA", "zp", LINE_CTR)
+
+
+def _frame_tail(a: Asm):
+    a.ins("DEC", "zp", LINE_CTR)
+    a.ins("BEQ", "rel", "ovs")
+    a.ins("JMP", "abs", "line")
+    a.label("ovs")
+    _wsync_lines(asm=a, n=30, tag="ovl")
+    a.ins("JMP", "abs", "frame")
+
+
+def _reset_code(a: Asm):
+    a.label("reset")
+    a.ins("SEI"); a.ins("CLD"); a.ins("LDA", "imm", 0); a.ins("LDX", "imm", 0x7F)
+    a.label("clr")
+    a.ins("STA", "zpx", 0x80); a.ins("DEX"); a.ins("BPL", "rel", "clr")
+    a.ins("LDX", "imm", 0xFF); a.ins("TXS")
+
+
+def e0_cart(seed: int = 6, lines: int = 64) -> Cart:
+    """8K Parker Brothers E0 cart: 1K slices 0-6 hold position-independent
+    routines (TIA writes included); slice 7 (window 3, fixed) holds the frame
+    skeleton.  Every line picks the slices of windows 0-2 from RAM through
+    the hotspots $1FE0-$1FF7 (an abs,X load, an abs,Y store and an abs,X load
+    of the hotspot rows) and calls each window; every fourth line also runs
+    an instruction that straddles windows 2 and 3 (LDA $0080 from $1BFE)."""
+    rng = Rng(seed * 0x9E3779B1 + 0xE0)
+    slices = [_window_routine(rng, 1024, True, 0xF000, 0xFFDF, avoid=(0xFFE0, 0xFFF7), tail=bytes([0xAD, 0x80]))
+              for _ in range(7)]
+    a = Asm(0xFC00)
+    a.raw(bytes([0x00, 0x60]))                  # $1C00: high byte of the straddling LDA, then RTS
+    _reset_code(a)
+    _frame_head(a, lines)
+    a.label("line")
+    a.ins("STA", "zp", WSYNC)
+    for w, (base, how) in enumerate(((0xFFE0, "ldx"), (0xFFE8, "sty"), (0xFFF0, "ldx"))):
+        a.ins("LDA", "zp", MIX); a.ins("ADC", "zp", LINE_CTR)
+        for _ in range(w):
+            a.ins("LSR", "acc")
+        a.ins("STA", "zp", MIX)
+        a.ins("AND", "imm", 7)
+        if how == "ldx":
+            a.ins("TAX"); a.ins("LDA", "absx", "map7"); a.ins("TAX"); a.ins("LDA", "absx", base)
+        else:
+            a.ins("TAY"); a.ins("LDA", "absy", "map7"); a.ins("TAY"); a.ins("STA", "absy", base)
+    for base in (0xF000, 0xF400, 0xF800):
+        a.ins("JSR", "abs", base)
+    a.ins("LDA", "zp", LINE_CTR); a.ins("AND", "imm", 3); a.ins("BNE", "rel", "nostr")
+    a.ins("JSR", "abs", 0xFBFE)
+    a.label("nostr")
+    _frame_tail(a)
+    a.label("map7")
+    a.raw(bytes([0, 1, 2, 3, 4, 5, 6, rng.below(7)]))
+    a.org(0xFFE0)
+    a.raw(bytes(rng.below(256) for _ in range(0x18)))     # hotspot rows: data only
+    a.org(0xFFFC)
+    a.raw(bytes([0x02, 0xFC, 0x02, 0xFC]))
+    img, labels, _ = a.assemble(1024)
+    assert labels["reset"] == 0xFC02 and labels["map7"] < 0xFFE0
+    rom = b"".join(slices) + img
+    assert len(rom) == 8192
+    return Cart(CartSpec("e0_8k", 8192, seed, wsync_density=1.0), rom, labels)
+
+
+def f3_cart(size: int = 16384, seed: int = 7, lines: int = 64) -> Cart:
+    """Tigervision 3F cart of `size` bytes (a multiple of 2K): 2K banks
+    0..n-2 hold position-independent routines (no TIA writes: any write to
+    $00-$3F switches the bank under them); the last 2K (fixed at $1800)
+    holds the frame skeleton.  Every line selects banks through STA/STX/STY
+    $3F with values above n (the bank is the value mod n), writes a colour
+    register (which selects bank COLUBK-value mod n), reads the lower window
+    through that mapping, and calls the routines of three selected banks."""
+    n = size // 2048
+    assert size % 2048 == 0 and n >= 2
+    rng = Rng(seed * 0x9E3779B1 + size)
+    banks = [_window_routine(rng, 2048, False, 0xF000, 0xFFF0) for _ in range(n - 1)]
+    sel = [b + n * rng.below(256 // n) for b in range(n - 1) for _ in range(2)]
+    sel = (sel * 8)[:8]
+    assert all(v % n != n - 1 and v < 256 for v in sel)
+    a = Asm(0xF800)
+    _reset_code(a)
+    _frame_head(a, lines)
+    a.label("line")
+    a.ins("STA", "zp", WSYNC)
+    for reg in ("A", "X", "Y"):
+        a.ins("LDA", "zp", MIX); a.ins("ADC", "zp", LINE_CTR); a.ins("STA", "zp", MIX)
+        a.ins("AND", "imm", 7); a.ins("TAX")
+        if reg == "A":
+            a.ins("LDA", "zp", MIX); a.ins("STA", "zp", 0x09)       # COLUBK: also a bank select
+            a.ins("LDA", "abs", 0xF000 + rng.below(0x800)); a.ins("EOR", "zp", 0x83); a.ins("STA", "zp", 0x83)
+            a.ins("LDA", "absx", "sel"); a.ins("STA", "zp", 0x3F)
+        elif reg == "X":
+            a.ins("LDA", "absx", "sel"); a.ins("TAX"); a.ins("STX", "zp", 0x3F)
+        else:
+            a.ins("LDY", "absx", "sel"); a.ins("STY", "zp", 0x3F)
+        a.ins("JSR", "abs", 0xF000)
+    _frame_tail(a)
+    a.label("sel")
+    a.raw(bytes(sel))
+    a.org(0xFFFC)
+    a.raw(bytes([0x00, 0xF8, 0x00, 0xF8]))
+    img, labels, _ = a.assemble(2048)
+    assert labels["reset"] == 0xF800
+    rom = b"".join(banks) + img
+    assert len(rom) == size
+    return Cart(CartSpec(f"3f_{size // 1024}k", size, seed, wsync_density=1.0), rom, labels)

@@ -96,7 +96,8 @@ void fa_pack_column(const fa_state& s, uint32_t* col, size_t stride)
     col[R_TIMER * stride] = (uint32_t)s.timer_value | ((uint32_t)s.timer_prescaler << 16);
     col[R_SELPC * stride] = (uint32_t)s.timer_prescaler_select | ((uint32_t)s.paddle_counter << 16);
     col[R_TIA0 * stride] = (uint32_t)s.tia_clock | ((uint32_t)s.tia_scanline << 16);
-    col[R_TIA1 * stride] = b4(!!s.tia_wsync, !!s.tia_frame_complete, s.tia_vsync, s.tia_vblank);
+    col[R_TIA1 * stride] = b4(!!s.tia_wsync, !!s.tia_frame_complete, s.tia_vsync, s.tia_vblank) |
+                           fa_mapper_tia1((uint32_t)s.mapper[0] | ((uint32_t)s.mapper[1] << 8));
     col[R_TIA2 * stride] = b4(!!s.inpt4, !!s.inpt5, s.paddle0, s.paddle1);
     col[R_FRAME * stride] = s.frame_no;
     col[R_STATUS * stride] = s.run_status;
@@ -135,22 +136,36 @@ void fa_unpack_column(const uint32_t* col, size_t stride, int scheme, fa_state& 
     w = col[R_TIMER * stride]; s.timer_value = (uint16_t)w; s.timer_prescaler = (uint16_t)(w >> 16);
     w = col[R_SELPC * stride]; s.timer_prescaler_select = (uint16_t)w; s.paddle_counter = (uint16_t)(w >> 16);
     w = col[R_TIA0 * stride]; s.tia_clock = (uint16_t)w; s.tia_scanline = (uint16_t)(w >> 16);
-    w = col[R_TIA1 * stride]; s.tia_wsync = w; s.tia_frame_complete = w >> 8; s.tia_vsync = w >> 16; s.tia_vblank = w >> 24;
+    w = col[R_TIA1 * stride]; s.tia_wsync = w & 1u; s.tia_frame_complete = (w >> 8) & 1u; s.tia_vsync = w >> 16; s.tia_vblank = w >> 24;
+    const uint32_t m = fa_tia1_mapper(w);
+    s.mapper[0] = (uint8_t)m;
+    s.mapper[1] = (uint8_t)(m >> 8);
     w = col[R_TIA2 * stride]; s.inpt4 = w; s.inpt5 = w >> 8; s.paddle0 = w >> 16; s.paddle1 = w >> 24;
     s.frame_no = col[R_FRAME * stride];
     s.run_status = col[R_STATUS * stride];
     s.scheme = (uint8_t)scheme;
 }
 
-void fa_power_on_column(const uint8_t* img, uint32_t nbanks, int scheme, uint32_t* col)
+void fa_power_on_column(const uint8_t* img, uint32_t nbanks, int scheme, uint32_t hot_lo, uint32_t* col)
 {
     // HeadlessBus::new (src/atari.rs:410-430): power-on bank is the last one;
     // Cpu::reset (src/cpu.rs:125-134) reads the vector at $FFFC/$FFFD.
     fa_state s;
     memset(&s, 0, sizeof(s));
-    const uint32_t bank = scheme == FA_SCHEME_FIXED ? 0u : nbanks - 1u;
-    s.bank = (uint8_t)bank;
-    s.pc = (uint16_t)(img[(bank << 12) | 0xFFC] | (img[(bank << 12) | 0xFFD] << 8));
+    if (fa_map_kind(hot_lo)) {
+        // Sliced carts: E0 windows 4, 5, 6, 7 (the image's last 4K, as the
+        // reference powers on in its last bank); 3F bank 0.  The vector is in
+        // window 3 ($1C00-$1FFF), whose slice is byte 3.
+        const uint32_t m = fa_map_kind(hot_lo) == FA_MAP_E0 ? (4u | 5u << 4 | 6u << 8) : 0u;
+        const uint32_t vec = (fa_slices_from_mapper(hot_lo, m) >> 24) * 1024u + 0x3FCu;
+        s.mapper[0] = (uint8_t)m;
+        s.mapper[1] = (uint8_t)(m >> 8);
+        s.pc = (uint16_t)(img[vec] | (img[vec + 1] << 8));
+    } else {
+        const uint32_t bank = scheme == FA_SCHEME_FIXED ? 0u : nbanks - 1u;
+        s.bank = (uint8_t)bank;
+        s.pc = (uint16_t)(img[(bank << 12) | 0xFFC] | (img[(bank << 12) | 0xFFD] << 8));
+    }
     s.sp = 0xFD;
     s.port_a_input = 0xFF;                   // Pia::default, src/pia.rs:46-62
     s.port_b_input = 0x3F;
@@ -161,7 +176,7 @@ void fa_power_on_column(const uint8_t* img, uint32_t nbanks, int scheme, uint32_
     fa_pack_column(s, col, 1);
 }
 
-// ------------------------------------------------------------------ handle
+// ------------------------------------------------------------------ ROM schemes
 static int rom_len_ok(size_t len)          // lengths HeadlessBus::new accepts (src/atari.rs:410-449)
 {
     if (len == 0) return 0;
@@ -173,23 +188,126 @@ static int rom_len_ok(size_t len)          // lengths HeadlessBus::new accepts (
     }
 }
 
-// 4 KiB-per-bank image of a ROM: Fixed carts mirror into one 4K window
-// (HeadlessBus::load_bank, src/atari.rs:433-449); banked carts use their
-// first nbanks * 4 KiB.
-int fa_make_bank_image(const uint8_t* rom, size_t len, std::vector<uint8_t>& img, int& scheme)
+static int scheme_len_ok(int scheme, size_t len)
 {
-    if (!rom || !rom_len_ok(len))
-        return fa_fail(FA_ERR_BAD_ROM, "ROM length %zu cannot be constructed (reference panics)", len);
-    scheme = fa_detect_scheme(len);
-    const uint32_t nb = fa_nbanks(scheme);
-    img.resize((size_t)nb * 4096);
-    if (scheme == FA_SCHEME_FIXED)
-        for (size_t i = 0; i < 4096; i++) img[i] = rom[i % len];
-    else
-        memcpy(img.data(), rom, img.size());
+    switch (scheme) {
+    case FA_SCHEME_E0: return len == 8192;
+    case FA_SCHEME_3F: return len >= 2048 && len <= 32768 && len % 2048 == 0;
+    case FA_SCHEME_FIXED: case FA_SCHEME_F8: case FA_SCHEME_F6: case FA_SCHEME_F4:
+        return rom_len_ok(len) && fa_detect_scheme(len) == scheme;
+    default: return 0;
+    }
+}
+
+namespace {
+std::mutex g_scheme_mu;
+std::vector<std::pair<std::pair<uint64_t, size_t>, int>> g_schemes;   // (content hash, length) -> scheme
+
+uint64_t rom_hash(const uint8_t* rom, size_t len)    // FNV-1a, 64-bit
+{
+    uint64_t h = 0xCBF29CE484222325ull;
+    for (size_t i = 0; i < len; i++) h = (h ^ rom[i]) * 0x100000001B3ull;
+    return h;
+}
+
+int registered_scheme(const uint8_t* rom, size_t len)
+{
+    const auto key = std::make_pair(rom_hash(rom, len), len);
+    std::lock_guard<std::mutex> lk(g_scheme_mu);
+    for (const auto& e : g_schemes)
+        if (e.first == key) return e.second;
+    return FA_SCHEME_AUTO;
+}
+}  // namespace
+
+extern "C" int fa_rom_set_scheme(const uint8_t* rom, size_t rom_len, int scheme)
+{
+    if (!rom || rom_len == 0) return fa_fail(FA_ERR_INVALID, "need a ROM");
+    if (scheme != FA_SCHEME_AUTO && !scheme_len_ok(scheme, rom_len))
+        return fa_fail(FA_ERR_BAD_ROM, "scheme %d cannot hold a %zu-byte ROM", scheme, rom_len);
+    const auto key = std::make_pair(rom_hash(rom, rom_len), rom_len);
+    std::lock_guard<std::mutex> lk(g_scheme_mu);
+    for (size_t i = 0; i < g_schemes.size(); i++)
+        if (g_schemes[i].first == key) { g_schemes.erase(g_schemes.begin() + (ptrdiff_t)i); break; }
+    if (scheme != FA_SCHEME_AUTO) g_schemes.emplace_back(key, scheme);
     return FA_OK;
 }
 
+extern "C" int fa_rom_scheme(const uint8_t* rom, size_t rom_len)
+{
+    if (!rom || rom_len == 0) return fa_fail(FA_ERR_BAD_ROM, "empty ROM");
+    const int reg = registered_scheme(rom, rom_len);
+    if (reg != FA_SCHEME_AUTO) return reg;
+    if (!rom_len_ok(rom_len))
+        return fa_fail(FA_ERR_BAD_ROM, "ROM length %zu cannot be constructed (reference panics)", rom_len);
+    return fa_detect_scheme(rom_len);
+}
+
+extern "C" int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len)
+{
+    if (!rom || rom_len == 0) return fa_fail(FA_ERR_BAD_ROM, "empty ROM");
+    // Absolute and absolute-indexed loads and stores (LDA/LDX/LDY/STA/STX/
+    // STY/BIT/CMP) aimed at ROM-space hotspots, and zero-page stores to $3F.
+    // Data bytes can look like either, so the counts are compared with the
+    // accesses to the hotspots of the scheme the size rule gives.
+    static const uint8_t abs_ops[] = { 0xAD, 0xAE, 0xAC, 0x8D, 0x8E, 0x8C, 0x2C, 0xCD,
+                                       0xBD, 0xB9, 0xBE, 0xBC, 0x9D, 0x99 };
+    const int by_size = rom_len_ok(rom_len) ? fa_detect_scheme(rom_len) : -1;
+    const uint32_t hlo = by_size > 0 ? fa_hot_lo(by_size) : 0x2000u, hn = by_size > 0 ? fa_nbanks(by_size) : 0u;
+    size_t e0 = 0, own = 0, st3f = 0;
+    for (size_t i = 0; i + 2 < rom_len; i++) {
+        const uint8_t op = rom[i];
+        if ((op == 0x85 || op == 0x86 || op == 0x84) && rom[i + 1] == 0x3F) st3f++;
+        if (std::find(std::begin(abs_ops), std::end(abs_ops), op) == std::end(abs_ops)) continue;
+        const uint32_t a = (uint32_t)rom[i + 1] | ((uint32_t)rom[i + 2] << 8);
+        if (!(a & 0x1000u)) continue;
+        const uint32_t a13 = a & 0x1FFFu;
+        if (a13 >= 0x1FE0u && a13 <= 0x1FF7u) e0++;
+        if (a13 - hlo < hn) own++;
+    }
+    if (rom_len == 8192 && e0 >= 2 && e0 > 2 * own) return FA_SCHEME_E0;
+    if (st3f >= 2 && st3f > 2 * own && scheme_len_ok(FA_SCHEME_3F, rom_len)) return FA_SCHEME_3F;
+    if (by_size < 0)
+        return fa_fail(FA_ERR_BAD_ROM, "ROM length %zu cannot be constructed (reference panics)", rom_len);
+    return by_size;
+}
+
+// The shared-memory image of a ROM, in 4 KiB units: Fixed carts mirror into
+// one 4K window (HeadlessBus::load_bank, src/atari.rs:433-449); 4K-bank carts
+// use their first nbanks * 4 KiB; sliced carts (E0, 3F) the whole ROM,
+// zero-padded to a 4K multiple.  The scheme is the registered one for these
+// bytes, else the reference's size rule.
+int fa_make_bank_image(const uint8_t* rom, size_t len, std::vector<uint8_t>& img, int& scheme, uint32_t* nbanks,
+                       uint32_t* hot_lo)
+{
+    if (!rom || len == 0) return fa_fail(FA_ERR_BAD_ROM, "empty ROM");
+    scheme = registered_scheme(rom, len);
+    if (scheme == FA_SCHEME_AUTO) {
+        if (!rom_len_ok(len))
+            return fa_fail(FA_ERR_BAD_ROM, "ROM length %zu cannot be constructed (reference panics)", len);
+        scheme = fa_detect_scheme(len);
+    }
+    uint32_t nb, hl;
+    if (scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_3F) {
+        nb = (uint32_t)((len + 4095) / 4096);
+        hl = scheme == FA_SCHEME_E0 ? (FA_MAP_E0 << 8) : ((FA_MAP_3F << 8) | (uint32_t)(len / 2048));
+        img.assign((size_t)nb * 4096, 0);
+        memcpy(img.data(), rom, len);
+    } else {
+        nb = fa_nbanks(scheme);
+        hl = fa_hot_lo(scheme);
+        img.resize((size_t)nb * 4096);
+        if (scheme == FA_SCHEME_FIXED)
+            for (size_t i = 0; i < 4096; i++) img[i] = rom[i % len];
+        else
+            memcpy(img.data(), rom, img.size());
+    }
+    if (nbanks) *nbanks = nb;
+    if (hot_lo) *hot_lo = hl;
+    return FA_OK;
+}
+
+// ------------------------------------------------------------------ handle
 static void free_handle(fa_handle* h)
 {
     if (!h) return;
@@ -226,10 +344,8 @@ extern "C" int fa_create(const uint8_t* rom, size_t rom_len, size_t n, fa_handle
     if (fa_device_count() < 1) return fa_fail(FA_ERR_NO_DEVICE, "no CUDA device visible");
     fa_handle* h = new (std::nothrow) fa_handle();
     if (!h) return fa_fail(FA_ERR_CAPACITY, "out of host memory");
-    int rc = fa_make_bank_image(rom, rom_len, h->image, h->scheme);
+    int rc = fa_make_bank_image(rom, rom_len, h->image, h->scheme, &h->nbanks, &h->hot_lo);
     if (rc) { delete h; return rc; }
-    h->nbanks = fa_nbanks(h->scheme);
-    h->hot_lo = fa_hot_lo(h->scheme);
     h->n = n;
     h->stride = (uint32_t)((n + 31) & ~(size_t)31);
     cudaGetDevice(&h->device);
@@ -351,7 +467,7 @@ extern "C" int fa_reset(fa_handle* h, uint8_t* obs_out)
     // HeadlessAtari::new + one run_frame without set_action
     // (src/cuda_env.rs:134-139): one instance on the device, then broadcast.
     uint32_t col[FA_ROWS];
-    fa_power_on_column(h->image.data(), h->nbanks, h->scheme, col);
+    fa_power_on_column(h->image.data(), h->nbanks, h->scheme, h->hot_lo, col);
     FA_CUDA(cudaMemcpyAsync(h->d_snap, col, sizeof(col), cudaMemcpyHostToDevice, h->stream));
     FaGroup g = fa_handle_group(h, nullptr, 1, nullptr);
     g.state = h->d_snap;
@@ -447,6 +563,11 @@ extern "C" int fa_set_states(fa_handle* h, const fa_state* in)
             return fa_fail(FA_ERR_INVALID, "instance %zu: timer_prescaler_select 0 (reference divides by it)", i);
         fa_state s = in[i];
         if (s.bank >= h->nbanks) s.bank = (uint8_t)(h->nbanks - 1);
+        // E0 slices to 3 bits, 3F banks modulo the bank count, 0 for the 4K-bank schemes.
+        const uint32_t m = fa_mapper_from_slices(
+            h->hot_lo, fa_slices_from_mapper(h->hot_lo, (uint32_t)s.mapper[0] | ((uint32_t)s.mapper[1] << 8)));
+        s.mapper[0] = (uint8_t)m;
+        s.mapper[1] = (uint8_t)(m >> 8);
         fa_pack_column(s, buf.data() + i, h->stride);
     }
     FA_CUDA(cudaStreamSynchronize(h->stream));

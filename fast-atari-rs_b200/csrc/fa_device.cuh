@@ -562,7 +562,7 @@ static __device__ __noinline__ uint2 render_read(uint32_t a, RState s, uint32_t 
     }
 }
 
-template <int BLOCK, bool RENDER = false>
+template <int BLOCK, bool RENDER = false, bool SLICED = false>
 struct Emu {
     // ---- placement
     uint8_t* pv;             // this thread's RAM (shared memory, interleaved by thread)
@@ -574,6 +574,7 @@ struct Emu {
     uint32_t a, x, y, sp, p, pc;
     uint32_t bank;           // bank index (bits 0-2) | hotspot accesses this frame << 3,
                              // saturating at 511: the count is a scheduling key only
+    uint32_t slices;         // SLICED (E0, 3F carts): the 1K ROM slice of window k in byte k
     uint32_t cyc_acc;         // instruction cycles not yet added to Cpu::cycles in HBM
     // ---- PIA (src/pia.rs:26-44): timer unpacked (ticked every instruction),
     //      ports and input pins packed (touched only by I/O accesses)
@@ -622,6 +623,32 @@ struct Emu {
     {
         uint32_t d = a13 - hot_lo;
         if (d < nbanks) bank = (bank < (511u << 3) ? ((bank + 8u) & ~7u) : (bank & ~7u)) | d;
+    }
+    // Sliced carts.  The ROM byte at a (A12 set): window (a >> 10) & 3 holds
+    // slice `slices` byte k.
+    __device__ __forceinline__ uint32_t srom(uint32_t a) const
+    {
+        return (((slices >> ((a >> 7) & 0x18u)) & 0x1Fu) << 10) | (a & 0x3FFu);
+    }
+    __device__ __forceinline__ void sbump() { bank = bank < (511u << 3) ? bank + 8u : bank; }
+    // E0: any access to $1FE0-$1FF7 maps slice (a & 7) into window (a - $1FE0) >> 3.
+    __device__ __forceinline__ void e0_hot(uint32_t a13)
+    {
+        const uint32_t d = a13 - 0x1FE0u;
+        if (d < 24u && fa_map_kind(hot_lo) == FA_MAP_E0) {
+            const uint32_t sh = (d >> 3) * 8u;
+            slices = (slices & ~(0xFFu << sh)) | ((a13 & 7u) << sh);
+            sbump();
+        }
+    }
+    // 3F: a write of v to $0000-$003F maps 2K bank v mod n at $1000-$17FF.
+    __device__ __forceinline__ void f3_write(uint32_t a13, uint32_t v)
+    {
+        if (a13 < 0x40u && fa_map_kind(hot_lo) == FA_MAP_3F) {
+            const uint32_t b = v % (hot_lo & 0xFFu);
+            slices = (slices & 0xFFFF0000u) | (2u * b) | ((2u * b + 1u) << 8);
+            sbump();
+        }
     }
 
     // ------------------------------------------------------------ TIA (headless_tia.rs)
@@ -713,6 +740,7 @@ struct Emu {
     }
     __device__ __forceinline__ void io_write(uint32_t a, uint32_t v, uint32_t j)  // TIA or PIA register write
     {
+        if constexpr (SLICED) f3_write(a, v);                       // the write still reaches the TIA
         if constexpr (RENDER) {
             rsync(j);
             r_write_cycle(a, v);
@@ -736,13 +764,24 @@ struct Emu {
     __device__ __forceinline__ uint32_t read(uint32_t addr, uint32_t j)
     {
         uint32_t a = addr & 0x1FFFu;
-        if (a & 0x1000u) { bsw(a); return rom[((bank & 7u) << 12) | (a & 0xFFFu)]; }
+        if (a & 0x1000u) {
+            if constexpr (SLICED) {
+                e0_hot(a);
+                return rom[srom(a)];
+            } else {
+                bsw(a);
+                return rom[((bank & 7u) << 12) | (a & 0xFFFu)];
+            }
+        }
         return read_low(a, j);
     }
     __device__ __forceinline__ void write(uint32_t addr, uint32_t v, uint32_t j)
     {
         uint32_t a = addr & 0x1FFFu;
-        if (a & 0x1000u) { bsw(a); return; }
+        if (a & 0x1000u) {
+            if constexpr (SLICED) e0_hot(a); else bsw(a);
+            return;
+        }
         if ((a & 0x280u) == 0x080u) { stp(a & 0x7Fu, v); return; }
         io_write(a, v, j);
     }
@@ -750,8 +789,9 @@ struct Emu {
     __device__ __forceinline__ void dummy(uint32_t addr, uint32_t j)
     {
         uint32_t a = addr & 0x1FFFu;
-        if (a & 0x1000u) bsw(a);
-        else if ((a & 0x287u) == 0x284u) {
+        if (a & 0x1000u) {
+            if constexpr (SLICED) e0_hot(a); else bsw(a);
+        } else if ((a & 0x287u) == 0x284u) {
             if constexpr (RENDER) (void)io(a, j);
             else uf = 0;
         }
@@ -1076,10 +1116,12 @@ struct Emu {
         const uint32_t pc0 = pc;
         const uint32_t a0 = pc0 & 0x1FFFu;
         uint32_t op, b1, b2 = 0;
-        if (a0 >= 0x1000u && a0 + 2u < hot_lo) {
-            // Fast path: the three bytes at pc0 lie in the current bank and
-            // below every hotspot, so reading them has no side effect.
-            const uint8_t* q = rom + ((bank & 7u) << 12) + (a0 & 0xFFFu);
+        // Fast path: the three bytes at pc0 lie in the current bank (SLICED:
+        // in one window) and clear of every hotspot, so reading them has no
+        // side effect.
+        if (SLICED ? (a0 >= 0x1000u && (a0 & 0x3FFu) <= 0x3FDu && (a0 + 2u < 0x1FE0u || a0 > 0x1FF7u))
+                   : (a0 >= 0x1000u && a0 + 2u < hot_lo)) {
+            const uint8_t* q = SLICED ? rom + srom(a0) : rom + ((bank & 7u) << 12) + (a0 & 0xFFFu);
             op = q[0];
             if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }
             b1 = q[1];
@@ -1201,6 +1243,7 @@ struct Emu {
         w = col[R_TIA0 * stride];  clock = w & 0xFFFF; scanline = w >> 16;
         w = col[R_TIA1 * stride];                                   // wsync fcomp vsync vblank
         tw = ((w >> 16) & 0xFFFFu) | ((w & 1u) << 16) | (((w >> 8) & 1u) << 17) | (((p1 >> 24) & 1u) << 18);
+        if constexpr (SLICED) slices = fa_slices_from_mapper(hot_lo, fa_tia1_mapper(w));
         w = col[R_TIA2 * stride];                                   // inpt4 inpt5 pad0 pad1
         pins = ((p0 >> 16) & 0xFFu) | (((p1 >> 8) & 0xFFu) << 8) | ((w & 1u) << 16) | (((w >> 8) & 1u) << 17);
         pads = w >> 16;
@@ -1214,7 +1257,9 @@ struct Emu {
         col[R_TIMER * stride] = tv | (ps << 16);
         col[R_SELPC * stride] = sel | (pcnt << 16);
         col[R_TIA0 * stride] = clock | (scanline << 16);
-        col[R_TIA1 * stride] = ((tw >> 16) & 1u) | (((tw >> 17) & 1u) << 8) | ((tw & 0xFFFFu) << 16);
+        uint32_t t1 = ((tw >> 16) & 1u) | (((tw >> 17) & 1u) << 8) | ((tw & 0xFFFFu) << 16);
+        if constexpr (SLICED) t1 |= fa_mapper_tia1(fa_mapper_from_slices(hot_lo, slices));
+        col[R_TIA1 * stride] = t1;
         col[R_TIA2 * stride] = ((pins >> 16) & 1u) | (((pins >> 17) & 1u) << 8) | (pads << 16);
     }
     // RAM words from the HBM rows into shared memory and back.

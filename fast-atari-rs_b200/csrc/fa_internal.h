@@ -115,7 +115,8 @@ int fa_fail(int code, const char* fmt, ...);
             return fa_fail(FA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));       \
     } while (0)
 
-int fa_make_bank_image(const uint8_t* rom, size_t len, std::vector<uint8_t>& img, int& scheme);
+int fa_make_bank_image(const uint8_t* rom, size_t len, std::vector<uint8_t>& img, int& scheme,
+                       uint32_t* nbanks = nullptr, uint32_t* hot_lo = nullptr);
 
 // One ROM and its n instances resident in HBM (the C ABI's fa_handle).
 struct fa_handle {
@@ -155,4 +156,4 @@ FaGroup fa_handle_group(fa_handle* h, const uint8_t* d_actions, uint32_t k, uint
 void fa_pack_column(const fa_state& s, uint32_t* col, size_t stride);
 void fa_unpack_column(const uint32_t* col, size_t stride, int scheme, fa_state& s);
 // Power-on state of HeadlessAtari::new (src/atari.rs:562-569) for a bank image.
-void fa_power_on_column(const uint8_t* bank_image, uint32_t nbanks, int scheme, uint32_t* col);
+void fa_power_on_column(const uint8_t* bank_image, uint32_t nbanks, int scheme, uint32_t hot_lo, uint32_t* col);

@@ -19,7 +19,7 @@
 
 namespace fa {
 
-template <int BLOCK>
+template <int BLOCK, bool SLICED_OK>
 __global__ void __launch_bounds__(BLOCK) fa_run(const __grid_constant__ FaLaunch L)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(BLOCK) fa_run(const __grid_constant__ FaLaunch
         }
         const uint32_t first = (u - G.unit_begin) * BLOCK;
         const uint32_t count = G.n - first < BLOCK ? G.n - first : BLOCK;
-        run_unit<BLOCK>(G, first, count, rom_s, priv, threadIdx.x, L.instr, L.rounds);
+        run_unit<BLOCK, SLICED_OK>(G, first, count, rom_s, priv, threadIdx.x, L.instr, L.rounds);
         __syncthreads();
     }
 }
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(BLOCK) fa_run(const __grid_constant__ FaLaunch
 // every CTA holds all of the launch's ROM images at once (the "ROM library",
 // staged once with TMA bulk copies), so units of any cart run in any warp
 // and a CTA can be as large as shared memory allows.
-template <int WARPS>
+template <int WARPS, bool SLICED_OK>
 __global__ void __launch_bounds__(WARPS * 32) fa_run_warps(const __grid_constant__ FaLaunch L)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(WARPS * 32) fa_run_warps(const __grid_constant
         const FaGroup& G = L.g[g];
         const uint32_t first = (u - G.unit_begin) * 32u;
         const uint32_t count = G.n - first < 32u ? G.n - first : 32u;
-        run_unit<32>(G, first, count, smem + G.rom_off, priv, lane, L.instr, L.rounds);
+        run_unit<32, SLICED_OK>(G, first, count, smem + G.rom_off, priv, lane, L.instr, L.rounds);
     }
 }
 
@@ -134,36 +134,36 @@ std::map<std::pair<int, std::pair<int, size_t>>, int> g_per_sm;   // (device, bl
 // The dynamic shared-memory limit is raised once per (device, BLOCK) to the
 // largest any cart needs (32 KiB of ROM plus the private bytes), so launches
 // of smaller carts never lower it under a larger one.
-template <int BLOCK>
+template <int BLOCK, bool SL = false>
 int per_sm_for(size_t smem)
 {
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lk(g_cfg_mu);
-    auto key = std::make_pair(dev, std::make_pair(BLOCK, smem));
+    auto key = std::make_pair(dev, std::make_pair(BLOCK * 2 + (SL ? 1 : 0), smem));
     auto it = g_per_sm.find(key);
     if (it != g_per_sm.end()) return it->second;
-    const auto max_key = std::make_pair(dev, std::make_pair(BLOCK, (size_t)0));
+    const auto max_key = std::make_pair(dev, std::make_pair(BLOCK * 2 + (SL ? 1 : 0), (size_t)0));
     if (g_per_sm.find(max_key) == g_per_sm.end()) {
         const int max_smem = 32768 + FA_SMEM_WORDS * BLOCK * 4;
-        if (cudaFuncSetAttribute(fa::fa_run<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem) !=
+        if (cudaFuncSetAttribute(fa::fa_run<BLOCK, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem) !=
             cudaSuccess)
             return -1;
         g_per_sm[max_key] = 0;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<BLOCK>, BLOCK, smem) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run<BLOCK, SL>, BLOCK, smem) != cudaSuccess)
         return -1;
     g_per_sm[key] = per_sm;
     return per_sm;
 }
 }  // namespace
 
-template <int BLOCK>
+template <int BLOCK, bool SL>
 static cudaError_t launch_block(const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
 {
     const size_t smem = (size_t)L.rom_bytes_max + (size_t)FA_SMEM_WORDS * BLOCK * 4u;
-    const int per_sm = per_sm_for<BLOCK>(smem);
+    const int per_sm = per_sm_for<BLOCK, SL>(smem);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     if (sms <= 0) return cudaSuccess;                                  // prepare only
     uint32_t grid = L.nunits;
@@ -172,42 +172,42 @@ static cudaError_t launch_block(const FaLaunch& L, bool persistent, int sms, cud
         grid = L.nunits < cap ? L.nunits : cap;
     }
     if (grid == 0) return cudaSuccess;
-    fa::fa_run<BLOCK><<<grid, BLOCK, smem, s>>>(L);
+    fa::fa_run<BLOCK, SL><<<grid, BLOCK, smem, s>>>(L);
     return cudaGetLastError();
 }
 
 namespace {
 std::map<std::pair<int, std::pair<int, size_t>>, int> g_warps_per_sm;   // (device, warps, smem) -> CTAs/SM
 
-template <int WARPS>
+template <int WARPS, bool SL>
 int warps_per_sm_for(size_t smem)
 {
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lk(g_cfg_mu);
-    auto key = std::make_pair(dev, std::make_pair(WARPS, smem));
+    auto key = std::make_pair(dev, std::make_pair(WARPS * 2 + (SL ? 1 : 0), smem));
     auto it = g_warps_per_sm.find(key);
     if (it != g_warps_per_sm.end()) return it->second;
-    const auto max_key = std::make_pair(dev, std::make_pair(WARPS, (size_t)0));
+    const auto max_key = std::make_pair(dev, std::make_pair(WARPS * 2 + (SL ? 1 : 0), (size_t)0));
     if (g_warps_per_sm.find(max_key) == g_warps_per_sm.end()) {
-        if (cudaFuncSetAttribute(fa::fa_run_warps<WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(fa::fa_run_warps<WARPS, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  FA_SMEM_PER_CTA_MAX) != cudaSuccess)
             return -1;
         g_warps_per_sm[max_key] = 0;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run_warps<WARPS>, WARPS * 32, smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fa::fa_run_warps<WARPS, SL>, WARPS * 32, smem) !=
         cudaSuccess)
         return -1;
     g_warps_per_sm[key] = per_sm;
     return per_sm;
 }
 
-template <int WARPS>
+template <int WARPS, bool SL>
 cudaError_t launch_warps(const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
 {
     const size_t smem = (size_t)L.romlib_bytes + (size_t)WARPS * FA_SMEM_WORDS * 32u * 4u;
-    const int per_sm = warps_per_sm_for<WARPS>(smem);
+    const int per_sm = warps_per_sm_for<WARPS, SL>(smem);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     if (sms <= 0) return cudaSuccess;                                  // prepare only
     uint32_t grid = (L.nunits + WARPS - 1) / WARPS;
@@ -218,20 +218,21 @@ cudaError_t launch_warps(const FaLaunch& L, bool persistent, int sms, cudaStream
         grid = L.nunits < cap ? L.nunits : cap;
     }
     if (grid == 0) return cudaSuccess;
-    fa::fa_run_warps<WARPS><<<grid, WARPS * 32, smem, s>>>(L);
+    fa::fa_run_warps<WARPS, SL><<<grid, WARPS * 32, smem, s>>>(L);
     return cudaGetLastError();
 }
 
+template <bool SL>
 cudaError_t launch_warps_n(int warps, const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
 {
     switch (warps) {
-    case 2: return launch_warps<2>(L, persistent, sms, s);
-    case 4: return launch_warps<4>(L, persistent, sms, s);
-    case 8: return launch_warps<8>(L, persistent, sms, s);
-    case 16: return launch_warps<16>(L, persistent, sms, s);
-    case 24: return launch_warps<24>(L, persistent, sms, s);
-    case 28: return launch_warps<28>(L, persistent, sms, s);
-    case 32: return launch_warps<32>(L, persistent, sms, s);
+    case 2: return launch_warps<2, SL>(L, persistent, sms, s);
+    case 4: return launch_warps<4, SL>(L, persistent, sms, s);
+    case 8: return launch_warps<8, SL>(L, persistent, sms, s);
+    case 16: return launch_warps<16, SL>(L, persistent, sms, s);
+    case 24: return launch_warps<24, SL>(L, persistent, sms, s);
+    case 28: return launch_warps<28, SL>(L, persistent, sms, s);
+    case 32: return launch_warps<32, SL>(L, persistent, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -264,6 +265,8 @@ static void plan_units(FaLaunch& L, uint32_t unit)
 cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int sms, cudaStream_t s)
 {
     FaLaunch L = L_in;
+    bool sliced = false;                                               // an E0 or 3F cart in the launch
+    for (uint32_t g = 0; g < L.ngroups; g++) sliced = sliced || fa_map_kind(L.g[g].hot_lo) != 0;
     const uint32_t lib = plan_romlib(L);
     L.romlib_bytes = lib;
     const uint32_t slab = FA_SMEM_WORDS * 32u * 4u;
@@ -280,16 +283,17 @@ cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int 
                 if (w <= fit && w <= cap) { warps = w; break; }
         }
         plan_units(L, 32u);
-        return launch_warps_n(warps, L, persistent, sms, s);
+        return sliced ? launch_warps_n<true>(warps, L, persistent, sms, s)
+                      : launch_warps_n<false>(warps, L, persistent, sms, s);
     }
     // ROM library too large for shared memory: CTA-granular units that
     // re-stage one cart's ROM at a time.
     plan_units(L, (uint32_t)block);
     switch (block) {
-    case 64: return launch_block<64>(L, persistent, sms, s);
-    case 128: return launch_block<128>(L, persistent, sms, s);
-    case 256: return launch_block<256>(L, persistent, sms, s);
-    case 512: return launch_block<512>(L, persistent, sms, s);
+    case 64: return sliced ? launch_block<64, true>(L, persistent, sms, s) : launch_block<64, false>(L, persistent, sms, s);
+    case 128: return sliced ? launch_block<128, true>(L, persistent, sms, s) : launch_block<128, false>(L, persistent, sms, s);
+    case 256: return sliced ? launch_block<256, true>(L, persistent, sms, s) : launch_block<256, false>(L, persistent, sms, s);
+    case 512: return sliced ? launch_block<512, true>(L, persistent, sms, s) : launch_block<512, false>(L, persistent, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -71,6 +71,46 @@ static inline int fa_detect_scheme(size_t len)        // BankScheme::detect, src
          : len <= 16384 ? FA_SCHEME_F6 : FA_SCHEME_F4;
 }
 
+#ifdef __CUDACC__
+#define FA_HD __host__ __device__
+#else
+#define FA_HD
+#endif
+
+// Sliced carts (E0, 3F) map 1K slices of the ROM image into the four 1K
+// windows of $1000-$1FFF; `slices` holds the slice of window k in byte k.
+// Their hot_lo is FA_MAP_* << 8 (3F: | the number of 2K banks), below 0x1000,
+// so no ROM address passes the 4K-bank hotspot decode or the 4K-bank fetch
+// path.  The bank state a caller sees is 16 bits (fa_state::mapper): E0 =
+// window 0 | window 1 << 4 | window 2 << 8; 3F = the 2K bank at $1000.
+enum : uint32_t { FA_MAP_E0 = 1u, FA_MAP_3F = 2u };
+
+FA_HD static inline uint32_t fa_map_kind(uint32_t hot_lo) { return hot_lo < 0x1000u ? hot_lo >> 8 : 0u; }
+
+FA_HD static inline uint32_t fa_slices_from_mapper(uint32_t hot_lo, uint32_t m)
+{
+    if (fa_map_kind(hot_lo) == FA_MAP_E0)
+        return (m & 7u) | (((m >> 4) & 7u) << 8) | (((m >> 8) & 7u) << 16) | (7u << 24);
+    if (fa_map_kind(hot_lo) == FA_MAP_3F) {
+        const uint32_t n = hot_lo & 0xFFu, b = (m & 0xFFu) % n, l = n - 1u;
+        return (2u * b) | ((2u * b + 1u) << 8) | ((2u * l) << 16) | ((2u * l + 1u) << 24);
+    }
+    return 0u;
+}
+
+FA_HD static inline uint32_t fa_mapper_from_slices(uint32_t hot_lo, uint32_t slices)
+{
+    if (fa_map_kind(hot_lo) == FA_MAP_E0)
+        return (slices & 7u) | (((slices >> 8) & 7u) << 4) | (((slices >> 16) & 7u) << 8);
+    if (fa_map_kind(hot_lo) == FA_MAP_3F) return (slices & 0xFFu) >> 1;
+    return 0u;
+}
+
+// The bank state's 14 stored bits ride in R_TIA1's flag bytes, above the
+// wsync and frame_complete bits: bits 1-7 of byte 0 and bits 1-7 of byte 1.
+FA_HD static inline uint32_t fa_tia1_mapper(uint32_t w) { return ((w >> 1) & 0x7Fu) | (((w >> 9) & 0x7Fu) << 7); }
+FA_HD static inline uint32_t fa_mapper_tia1(uint32_t m) { return ((m & 0x7Fu) << 1) | (((m >> 7) & 0x7Fu) << 9); }
+
 // ---- rendering console (src/tia.rs, src/atari.rs:107-306)
 // Its state is the headless layout's rows (the same R_* and PB_* meaning)
 // followed by what only the pixel-accurate TIA has.  While a unit runs, the

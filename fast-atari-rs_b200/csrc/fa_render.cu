@@ -6,7 +6,7 @@
 // lands on the third TIA clock of its cycle, and every TIA clock inside the
 // visible window renders a pixel of a 160 x 192 framebuffer of palette
 // indices.  The 6502 here is the same core as the headless kernels
-// (Emu<32, true>): each of its bus accesses knows its cycle within the
+// (Emu<32, true, SLICED>): each of its bus accesses knows its cycle within the
 // instruction, and before an access reaches a TIA or PIA register the TIA
 // and PIA are ticked up to that cycle, so register writes land at the beam
 // position the reference gives them.  Cycles of instructions that touch
@@ -54,8 +54,9 @@ namespace fa {
 
 // One rendering console per lane: HeadlessAtari's frame loop with the
 // rendering console's per-cycle run_one_cycle (src/atari.rs:284-318).
+template <bool SLICED>
 struct RRunner {
-    Emu<32, true> e;
+    Emu<32, true, SLICED> e;
     uint32_t f, phase, fcyc;
     bool active;
 
@@ -141,7 +142,7 @@ struct RRunner {
 // 80 registers: 24 resident warps per SM (three 256-thread CTAs), the
 // occupancy that the shared-memory slabs allow; ptxas would otherwise take
 // 128 for the pixel code and hold the SM to 16 warps.
-template <int WARPS>
+template <int WARPS, bool SLICED>
 __global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLaunch L)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -178,12 +179,12 @@ __global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLa
     const uint32_t i = first + lane;
     const bool valid = i < L.n;
 
-    RRunner r;
+    RRunner<SLICED> r;
     r.f = 0;
     r.phase = 0;
     r.fcyc = 0;
     r.active = false;
-    Emu<32, true>& e = r.e;
+    Emu<32, true, SLICED>& e = r.e;
     e.pv = (uint8_t*)(slab + lane);
     e.G = &sg;
     e.i = i;
@@ -194,6 +195,7 @@ __global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLa
     e.cyc_acc = 0;
     e.pc = 0;
     e.bank = 0;
+    e.slices = 0;
     e.scanline = 0;
     e.done = 0;
     e.lag = 0;
@@ -287,7 +289,7 @@ namespace {
 std::mutex g_rmu;
 std::map<std::pair<int, int>, bool> g_rcfg;   // (device, warps) whose smem limit was raised
 
-template <int WARPS>
+template <int WARPS, bool SLICED>
 cudaError_t launch_render(const FaRenderLaunch& L, cudaStream_t s)
 {
     int dev = 0;
@@ -296,9 +298,9 @@ cudaError_t launch_render(const FaRenderLaunch& L, cudaStream_t s)
     const size_t smem = (size_t)L.nbanks * 4096u + (size_t)WARPS * FA_RPRIV_WORDS * 32u * 4u;
     {
         std::lock_guard<std::mutex> lk(g_rmu);
-        auto key = std::make_pair(dev, WARPS);
+        auto key = std::make_pair(dev, WARPS * 2 + (SLICED ? 1 : 0));
         if (g_rcfg.find(key) == g_rcfg.end()) {
-            e = cudaFuncSetAttribute(fa::fa_render_run<WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            e = cudaFuncSetAttribute(fa::fa_render_run<WARPS, SLICED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      32768 + WARPS * FA_RPRIV_WORDS * 32 * 4);
             if (e != cudaSuccess) return e;
             g_rcfg[key] = true;
@@ -307,16 +309,17 @@ cudaError_t launch_render(const FaRenderLaunch& L, cudaStream_t s)
     const uint32_t units = (L.n + 31u) / 32u;
     const uint32_t grid = (units + WARPS - 1u) / WARPS;
     if (grid == 0) return cudaSuccess;
-    fa::fa_render_run<WARPS><<<grid, WARPS * 32, smem, s>>>(L);
+    fa::fa_render_run<WARPS, SLICED><<<grid, WARPS * 32, smem, s>>>(L);
     return cudaGetLastError();
 }
 
 cudaError_t launch_render_n(int warps, const FaRenderLaunch& L, cudaStream_t s)
 {
+    const bool sliced = fa_map_kind(L.hot_lo) != 0;                    // E0 / 3F carts
     switch (warps) {
-    case 4: return launch_render<4>(L, s);
-    case 8: return launch_render<8>(L, s);
-    case 16: return launch_render<16>(L, s);
+    case 4: return sliced ? launch_render<4, true>(L, s) : launch_render<4, false>(L, s);
+    case 8: return sliced ? launch_render<8, true>(L, s) : launch_render<8, false>(L, s);
+    case 16: return sliced ? launch_render<16, true>(L, s) : launch_render<16, false>(L, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -408,7 +411,7 @@ int copy_d2h(fa_render* r, uint8_t* dst, const uint8_t* src, size_t bytes)
 void render_power_on(const fa_render* r, std::vector<uint32_t>& col)
 {
     col.assign(FA_RROWS, 0u);
-    fa_power_on_column(r->image.data(), r->nbanks, r->scheme, col.data());
+    fa_power_on_column(r->image.data(), r->nbanks, r->scheme, r->hot_lo, col.data());
     fa_state s;
     fa_unpack_column(col.data(), 1, r->scheme, s);
     s.paddle0 = 128;
@@ -502,13 +505,11 @@ extern "C" int fa_render_create(const uint8_t* rom, size_t rom_len, size_t n, fa
     if (fa_device_count() < 1) return fa_fail(FA_ERR_NO_DEVICE, "no CUDA device visible");
     fa_render* r = new (std::nothrow) fa_render();
     if (!r) return fa_fail(FA_ERR_CAPACITY, "out of host memory");
-    int rc = fa_make_bank_image(rom, rom_len, r->image, r->scheme);
+    int rc = fa_make_bank_image(rom, rom_len, r->image, r->scheme, &r->nbanks, &r->hot_lo);
     if (rc) { delete r; return rc; }
     cudaGetDevice(&r->device);
     r->n = n;
     r->stride = (uint32_t)((n + 31u) & ~(size_t)31u);
-    r->nbanks = fa_nbanks(r->scheme);
-    r->hot_lo = fa_hot_lo(r->scheme);
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaMalloc(&r->d_rom, r->image.size())) != cudaSuccess ||

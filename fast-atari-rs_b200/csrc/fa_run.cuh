@@ -84,9 +84,9 @@ static __device__ bool stage_rom(uint8_t* dst, const uint8_t* src, uint32_t byte
 }
 
 // ------------------------------------------------------------------ per-unit runner
-template <int BLOCK>
+template <int BLOCK, bool SLICED = false>
 struct Runner {
-    Emu<BLOCK> e;
+    Emu<BLOCK, false, SLICED> e;
     uint32_t f, phase, fcyc;
     bool active;
 
@@ -246,12 +246,12 @@ __device__ __forceinline__ uint32_t run_lanes(RUNNER& r, uint32_t sched)
 
 // Run one work unit: instances [first, first + count) of group G, one per
 // thread; t is the thread's slot in a private-byte slab of BLOCK slots.
-template <int BLOCK>
-__device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint32_t count, const uint8_t* rom_s,
-                                         uint32_t* priv, uint32_t t, unsigned long long* instr_out,
-                                         unsigned long long* rounds_out)
+template <int BLOCK, bool SLICED>
+__device__ __forceinline__ void run_unit_as(const FaGroup& G, uint32_t first, uint32_t count, const uint8_t* rom_s,
+                                            uint32_t* priv, uint32_t t, unsigned long long* instr_out,
+                                            unsigned long long* rounds_out)
 {
-    Runner<BLOCK> r;
+    Runner<BLOCK, SLICED> r;
     r.f = 0;
     r.phase = 0;
     r.fcyc = 0;
@@ -266,6 +266,7 @@ __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint3
     r.e.cyc_acc = 0;
     r.e.pc = 0;
     r.e.bank = 0;
+    r.e.slices = 0;
     r.e.scanline = 0;
     const bool valid = t < count;
     uint32_t* col = G.state + r.e.i;
@@ -294,6 +295,22 @@ __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint3
         if ((t & 31u) == 0 && n) atomicAdd(instr_out, (unsigned long long)n);
     }
     if (rounds_out && (t & 31u) == 0 && rounds) atomicAdd(rounds_out, 32ull * rounds);
+}
+
+// Kernels come in two builds.  SLICED_OK = false (every launch without an E0
+// or 3F cart) holds the 4K-bank core alone.  SLICED_OK = true runs a unit of
+// a sliced cart (hot_lo below 0x1000) on the SLICED core and every other unit
+// on the 4K-bank core; its register budget is the larger of the two, so it is
+// launched only when the launch has a sliced cart.
+template <int BLOCK, bool SLICED_OK>
+__device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint32_t count, const uint8_t* rom_s,
+                                         uint32_t* priv, uint32_t t, unsigned long long* instr_out,
+                                         unsigned long long* rounds_out)
+{
+    if (SLICED_OK && fa_map_kind(G.hot_lo))
+        run_unit_as<BLOCK, SLICED_OK>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
+    else
+        run_unit_as<BLOCK, false>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
 }
 
 }  // namespace fa

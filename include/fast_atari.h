@@ -53,6 +53,18 @@ extern "C" {
 #define FA_SCHEME_F8    1
 #define FA_SCHEME_F6    2
 #define FA_SCHEME_F4    3
+/* Schemes the reference does not have (its BankScheme::detect picks by size
+ * alone, so these carts run as F8 there and crash or misbehave).  They are
+ * never picked by size: register them per ROM with fa_rom_set_scheme. */
+#define FA_SCHEME_E0    4   /* Parker Brothers, 8K: four 1K windows; any access to
+                               $1FE0-$1FE7 / $1FE8-$1FEF / $1FF0-$1FF7 maps 1K slice
+                               (addr & 7) into window 0 / 1 / 2; window 3 holds
+                               slice 7.  Power-on windows: slices 4, 5, 6, 7. */
+#define FA_SCHEME_3F    5   /* Tigervision, 2K multiples up to 32K: $1000-$17FF is a
+                               switchable 2K bank, $1800-$1FFF the last 2K; a write
+                               of v to $0000-$003F selects bank v mod (len / 2K) and
+                               also reaches the TIA.  Power-on bank: 0. */
+#define FA_SCHEME_AUTO  (-1)
 
 #define FA_RAM_BYTES 128
 #define FA_NUM_ACTIONS 18
@@ -92,7 +104,11 @@ typedef struct fa_state {
     uint8_t  bank, scheme;
     uint8_t  _pad_end[2];
     /* ---- extension beyond the reference layout ---- */
-    uint8_t  _pad_ext[3];
+    /* E0 and 3F bank state, 16 bits little-endian: E0 = slice of window 0 |
+     * window 1 << 4 | window 2 << 8; 3F = the 2K bank at $1000.  0 for the
+     * reference's schemes, whose bank is `bank`. */
+    uint8_t  mapper[2];
+    uint8_t  _pad_ext;
     uint64_t cycles;      /* Cpu::cycles: executed instruction cycles, never reset */
     uint32_t frame_no;    /* frames run since the last reset (episode counter) */
     uint32_t run_status;  /* FA_STATUS_* bits */
@@ -132,6 +148,32 @@ int fa_device_count(void);
  * afterwards (the library links its own CUDA runtime, so another runtime's
  * current device does not carry over). */
 int fa_set_device(int device);
+
+/*
+ * ROM schemes.  No counterpart in the reference, which picks a scheme from
+ * the ROM length alone (src/atari.rs:96-105).  fa_rom_set_scheme records,
+ * process-wide, the scheme of one ROM image (identified by its bytes); every
+ * entry point that is later given the same bytes (fa_create, fa_pool_add_cart,
+ * fa_server_create, fa_render_create, fa_autotune) uses it instead of the
+ * size rule.  FA_SCHEME_AUTO removes the record.  The length must suit the
+ * scheme: E0 exactly 8192; 3F a multiple of 2048 up to 32768; the reference's
+ * schemes the lengths fa_create accepts for them.  FA_ERR_BAD_ROM otherwise.
+ */
+int fa_rom_set_scheme(const uint8_t* rom, size_t rom_len, int scheme);
+
+/* The scheme the entry points will use for these bytes (a registered one,
+ * else the size rule), or FA_ERR_BAD_ROM for a length that cannot be built. */
+int fa_rom_scheme(const uint8_t* rom, size_t rom_len);
+
+/* A guess from the ROM's code, for a caller deciding what to register; never
+ * applied by itself.  It counts absolute and indexed loads and stores aimed at
+ * the E0 hotspots $1FE0-$1FF7, zero-page stores to $3F (STA/STX/STY $3F), and
+ * accesses to the hotspots of the scheme the size rule gives (F8 $1FF8-$1FF9,
+ * F6 $1FF6-$1FF9, F4 $1FF4-$1FFB).  An 8K image with at least two E0 accesses,
+ * over twice the size-rule ones, is E0; at least two $3F stores, over twice
+ * the size-rule accesses, make a 2K-multiple image 3F; anything else gets the
+ * size rule. */
+int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len);
 
 /*
  * BatchAtariGpu::new (src/cuda_env.rs:112-126).  Uploads the ROM and allocates

@@ -396,6 +396,7 @@ struct orc_atari {
     size_t   rom_len;
     int      bank;
     int      scheme;
+    int      slice[4];            /* E0 / 3F: the 1K ROM slice in each 1K window of $1000-$1FFF */
     uint32_t frame_no;
     uint32_t run_status;
     uint64_t instructions;
@@ -423,8 +424,90 @@ static int orc_rom_len_ok(size_t len)
     }
 }
 
+/* Schemes registered per ROM image, as the library's fa_rom_set_scheme does:
+ * keyed by FNV-1a of the bytes and the length.  E0 and 3F are never picked by
+ * size (the reference has neither). */
+#define ORC_MAX_SCHEMES 64
+static struct { uint64_t h; size_t len; int scheme; } g_orc_reg[ORC_MAX_SCHEMES];
+static int g_orc_nreg;
+
+static uint64_t orc_rom_hash(const uint8_t* rom, size_t len)
+{
+    uint64_t h = 0xCBF29CE484222325ull;
+    for (size_t i = 0; i < len; i++) h = (h ^ rom[i]) * 0x100000001B3ull;
+    return h;
+}
+
+static int orc_scheme_len_ok(int scheme, size_t len)
+{
+    if (scheme == FA_SCHEME_E0) return len == 8192;
+    if (scheme == FA_SCHEME_3F) return len >= 2048 && len <= 32768 && len % 2048 == 0;
+    return orc_rom_len_ok(len) && orc_detect(len) == scheme;
+}
+
+int orc_rom_set_scheme(const uint8_t* rom, size_t len, int scheme)
+{
+    if (!rom || len == 0) return -1;
+    if (scheme >= 0 && !orc_scheme_len_ok(scheme, len)) return -1;
+    const uint64_t h = orc_rom_hash(rom, len);
+    for (int i = 0; i < g_orc_nreg; i++)
+        if (g_orc_reg[i].h == h && g_orc_reg[i].len == len) { g_orc_reg[i] = g_orc_reg[--g_orc_nreg]; break; }
+    if (scheme < 0) return 0;
+    if (g_orc_nreg == ORC_MAX_SCHEMES) return -1;
+    g_orc_reg[g_orc_nreg].h = h;
+    g_orc_reg[g_orc_nreg].len = len;
+    g_orc_reg[g_orc_nreg].scheme = scheme;
+    g_orc_nreg++;
+    return 0;
+}
+
+/* The scheme of a ROM image: registered, else the size rule; -1 when the
+ * reference could not construct it. */
+static int orc_scheme_for(const uint8_t* rom, size_t len)
+{
+    if (!rom || len == 0) return -1;
+    const uint64_t h = orc_rom_hash(rom, len);
+    for (int i = 0; i < g_orc_nreg; i++)
+        if (g_orc_reg[i].h == h && g_orc_reg[i].len == len) return g_orc_reg[i].scheme;
+    return orc_rom_len_ok(len) ? orc_detect(len) : -1;
+}
+
+static int orc_sliced(int scheme) { return scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_3F; }
+
+/* Power-on windows of the sliced schemes: E0 slices 4, 5, 6, 7; 3F 2K bank 0
+ * under the last 2K. */
+static void orc_power_on_slices(int scheme, size_t len, int* slice)
+{
+    if (scheme == FA_SCHEME_E0) { slice[0] = 4; slice[1] = 5; slice[2] = 6; slice[3] = 7; return; }
+    const int l = (int)(len / 2048) - 1;
+    slice[0] = 0; slice[1] = 1; slice[2] = 2 * l; slice[3] = 2 * l + 1;
+}
+
+static unsigned orc_mapper_of(int scheme, const int* slice)
+{
+    if (scheme == FA_SCHEME_E0) return (unsigned)(slice[0] | slice[1] << 4 | slice[2] << 8);
+    if (scheme == FA_SCHEME_3F) return (unsigned)(slice[0] / 2);
+    return 0;
+}
+
+static void orc_slices_of(int scheme, size_t len, unsigned m, int* slice)
+{
+    orc_power_on_slices(scheme, len, slice);
+    if (scheme == FA_SCHEME_E0) { slice[0] = m & 7; slice[1] = (m >> 4) & 7; slice[2] = (m >> 8) & 7; }
+    else if (scheme == FA_SCHEME_3F) { const int b = (int)((m & 0xFF) % (len / 2048)); slice[0] = 2 * b; slice[1] = 2 * b + 1; }
+}
+
+static void orc_load_window(orc_atari* e, int w)
+{
+    memcpy(&e->mem[0x1000 + 1024 * w], &e->rom[(size_t)e->slice[w] * 1024], 1024);
+}
+
 static void orc_load_bank(orc_atari* e, int bank)                  /* atari.rs:433-449 */
 {
+    if (orc_sliced(e->scheme)) {
+        for (int w = 0; w < 4; w++) orc_load_window(e, w);
+        return;
+    }
     if (e->scheme == FA_SCHEME_FIXED) {
         for (int i = 0; i < 4096; i++) e->mem[0x1000 + i] = e->rom[(size_t)i % e->rom_len];
         return;
@@ -446,6 +529,13 @@ static inline void orc_check_bankswitch(orc_atari* e, uint16_t addr) /* atari.rs
     case FA_SCHEME_F8: if (a < 0x1FF8 || a > 0x1FF9) return; nb = a - 0x1FF8; break;
     case FA_SCHEME_F6: if (a < 0x1FF6 || a > 0x1FF9) return; nb = a - 0x1FF6; break;
     case FA_SCHEME_F4: if (a < 0x1FF4 || a > 0x1FFB) return; nb = a - 0x1FF4; break;
+    case FA_SCHEME_E0:                       /* $1FE0-$1FF7: slice a & 7 into window (a - $1FE0) / 8 */
+        if (a >= 0x1FE0 && a <= 0x1FF7) {
+            const int w = (a - 0x1FE0) >> 3;
+            e->slice[w] = a & 7;
+            orc_load_window(e, w);
+        }
+        return;
     default: return;
     }
     if (nb != e->bank) {
@@ -480,6 +570,13 @@ static inline void orc_bus_write(orc_atari* e, uint16_t addr, uint8_t v) /* atar
         return;
     }
     if (a & 0x200) { orc_pia_write(&e->pia, a, v); return; }
+    if (e->scheme == FA_SCHEME_3F && a < 0x40) {   /* 3F: the written value selects the 2K bank at $1000 */
+        const int b = (int)(v % (e->rom_len / 2048));
+        e->slice[0] = 2 * b;
+        e->slice[1] = 2 * b + 1;
+        orc_load_window(e, 0);
+        orc_load_window(e, 1);
+    }
     orc_tia_write(&e->tia, a, v);
 }
 
@@ -518,18 +615,20 @@ static void orc_cpu_reset_bus(orc_atari* e)                        /* cpu.rs:125
 
 orc_atari* orc_create(const uint8_t* rom, size_t rom_len)          /* atari.rs:410-430, 562-569 */
 {
-    if (!rom || !orc_rom_len_ok(rom_len)) return NULL;
+    const int scheme = orc_scheme_for(rom, rom_len);
+    if (scheme < 0) return NULL;
     orc_atari* e = (orc_atari*)calloc(1, sizeof(orc_atari));
     if (!e) return NULL;
     e->rom = (uint8_t*)malloc(rom_len);
     if (!e->rom) { free(e); return NULL; }
     memcpy(e->rom, rom, rom_len);
     e->rom_len = rom_len;
-    e->scheme = orc_detect(rom_len);
+    e->scheme = scheme;
     switch (e->scheme) {
     case FA_SCHEME_FIXED: e->bank = 0; break;
     case FA_SCHEME_F8: e->bank = 1; break;
     case FA_SCHEME_F6: e->bank = 3; break;
+    case FA_SCHEME_E0: case FA_SCHEME_3F: e->bank = 0; orc_power_on_slices(scheme, rom_len, e->slice); break;
     default: e->bank = 7; break;
     }
     orc_tia_default(&e->tia);
@@ -651,6 +750,8 @@ void orc_get_state(const orc_atari* e, fa_state* s)                /* cuda_env.r
     s->ctrlpf = t->ctrlpf; s->refp0 = t->refp0; s->refp1 = t->refp1;
     s->pf0 = t->pf0; s->pf1 = t->pf1; s->pf2 = t->pf2;
     s->bank = (uint8_t)e->bank; s->scheme = (uint8_t)e->scheme;
+    const unsigned m = orc_mapper_of(e->scheme, e->slice);
+    s->mapper[0] = (uint8_t)m; s->mapper[1] = (uint8_t)(m >> 8);
     s->cycles = e->cpu.cycles;
     s->frame_no = e->frame_no;
     s->run_status = e->run_status;
@@ -692,6 +793,8 @@ void orc_set_state(orc_atari* e, const fa_state* s)
     int maxb = e->scheme == FA_SCHEME_F8 ? 1 : e->scheme == FA_SCHEME_F6 ? 3 : e->scheme == FA_SCHEME_F4 ? 7 : 0;
     if (nb > maxb) nb = maxb;
     e->bank = nb;
+    if (orc_sliced(e->scheme))
+        orc_slices_of(e->scheme, e->rom_len, (unsigned)s->mapper[0] | ((unsigned)s->mapper[1] << 8), e->slice);
     orc_load_bank(e, nb);
     orc_sync_ram_to_mem(e);
 }
@@ -755,7 +858,7 @@ static uint64_t orc_run_batch_impl(const uint8_t* rom, size_t rom_len, size_t n,
                                    const fa_state* snapshot, uint32_t episode_frames,
                                    uint8_t* obs, uint8_t* trace, int nthreads, int pin)
 {
-    if (!rom || !states || (k > 0 && !actions) || k < 0 || !orc_rom_len_ok(rom_len)) return (uint64_t)-1;
+    if (!rom || !states || (k > 0 && !actions) || k < 0 || orc_scheme_for(rom, rom_len) < 0) return (uint64_t)-1;
     if (nthreads < 1) nthreads = 1;
     if ((size_t)nthreads > n && n > 0) nthreads = (int)n;
     orc_job* jobs = (orc_job*)calloc((size_t)nthreads, sizeof(orc_job));
@@ -1135,6 +1238,7 @@ struct orc_ratari {
     uint8_t* rom;
     size_t   rom_len;
     int      bank, scheme;
+    int      slice[4];            /* E0 / 3F windows, as in orc_atari */
     uint32_t bus_ticks;
     uint32_t frame_no, run_status;
     uint64_t instructions;
@@ -1143,6 +1247,7 @@ struct orc_ratari {
 static inline uint8_t orc_rrom_read(const orc_ratari* e, uint16_t addr) /* atari.rs:139-150 */
 {
     if (e->scheme == FA_SCHEME_FIXED) return e->rom[(addr & 0x0FFF) % e->rom_len];
+    if (orc_sliced(e->scheme)) return e->rom[(size_t)e->slice[(addr >> 10) & 3] * 1024 + (addr & 0x03FF)];
     size_t off = (size_t)e->bank * 4096 + (addr & 0x0FFF);
     return off < e->rom_len ? e->rom[off] : 0;
 }
@@ -1153,6 +1258,7 @@ static inline void orc_rcheck_bankswitch(orc_ratari* e, uint16_t addr) /* atari.
     int first = e->scheme == FA_SCHEME_F8 ? 0x1FF8 : e->scheme == FA_SCHEME_F6 ? 0x1FF6 : e->scheme == FA_SCHEME_F4 ? 0x1FF4 : 0;
     int nb = e->scheme == FA_SCHEME_F8 ? 2 : e->scheme == FA_SCHEME_F6 ? 4 : e->scheme == FA_SCHEME_F4 ? 8 : 0;
     if (nb && a >= first && a < first + nb) e->bank = a - first;
+    if (e->scheme == FA_SCHEME_E0 && a >= 0x1FE0 && a <= 0x1FF7) e->slice[(a - 0x1FE0) >> 3] = a & 7;
 }
 
 static inline void orc_rtick_components(orc_ratari* e)             /* atari.rs:273-279 */
@@ -1188,6 +1294,11 @@ static void orc_rbus_write(orc_ratari* e, uint16_t addr, uint8_t v) /* atari.rs:
     orc_rtia_tick(&e->tia);
     orc_rcheck_bankswitch(e, addr);
     uint16_t a = addr & 0x1FFF;
+    if (e->scheme == FA_SCHEME_3F && a < 0x40) {   /* 3F bank select; the write also reaches the TIA */
+        const int b = (int)(v % (e->rom_len / 2048));
+        e->slice[0] = 2 * b;
+        e->slice[1] = 2 * b + 1;
+    }
     if ((a & 0x1080) == 0x0000) orc_rtia_write(&e->tia, a, v);
     else if ((a & 0x1280) == 0x0080 || (a & 0x1280) == 0x0280) orc_pia_write(&e->pia, a, v);
     orc_rtia_tick(&e->tia);
@@ -1208,15 +1319,17 @@ static void orc_rbus_write(orc_ratari* e, uint16_t addr, uint8_t v) /* atari.rs:
 
 orc_ratari* orc_rcreate(const uint8_t* rom, size_t rom_len)        /* atari.rs:120-136, 240-247 */
 {
-    if (!rom || !orc_rom_len_ok(rom_len)) return NULL;
+    const int scheme = orc_scheme_for(rom, rom_len);
+    if (scheme < 0) return NULL;
     orc_ratari* e = (orc_ratari*)calloc(1, sizeof(orc_ratari));
     if (!e) return NULL;
     e->rom = (uint8_t*)malloc(rom_len);
     if (!e->rom) { free(e); return NULL; }
     memcpy(e->rom, rom, rom_len);
     e->rom_len = rom_len;
-    e->scheme = orc_detect(rom_len);
+    e->scheme = scheme;
     e->bank = e->scheme == FA_SCHEME_FIXED ? 0 : e->scheme == FA_SCHEME_F8 ? 1 : e->scheme == FA_SCHEME_F6 ? 3 : 7;
+    if (orc_sliced(scheme)) { e->bank = 0; orc_power_on_slices(scheme, rom_len, e->slice); }
     orc_rtia_default(&e->tia);
     orc_pia_default(&e->pia);
     e->cpu.sp = 0xFD;                                              /* Cpu::default */
@@ -1312,6 +1425,9 @@ void orc_rregs(const orc_ratari* e, uint32_t* out8)
     out8[6] = e->run_status;
     out8[7] = e->pia.timer_value | ((uint32_t)e->pia.timer_prescaler << 16);
 }
+
+/* E0 / 3F bank state, as fa_state::mapper (0 for the reference's schemes). */
+unsigned orc_rmapper(const orc_ratari* e) { return orc_mapper_of(e->scheme, e->slice); }
 
 /* The whole TIA record (orc_rtia, its framebuffer last) for full-state comparisons. */
 void orc_rtia_copy(const orc_ratari* e, void* out) { memcpy(out, &e->tia, sizeof(e->tia)); }

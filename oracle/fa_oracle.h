@@ -36,6 +36,14 @@ typedef struct orc_regs {
     uint64_t cycles;
 } orc_regs;
 
+/* The oracle's counterpart of fa_rom_set_scheme: the scheme of one ROM image
+ * (by its bytes) for every later orc_create / orc_rcreate / orc_reset_state /
+ * orc_run_batch given the same bytes; scheme < 0 removes the record.  E0 and
+ * 3F are restated from the published behaviour of those carts (the reference
+ * has neither).  Returns 0, or -1 for a length the scheme cannot hold.  Not
+ * thread-safe: register before running. */
+int orc_rom_set_scheme(const uint8_t* rom, size_t rom_len, int scheme);
+
 /* HeadlessAtari::new (src/atari.rs:562-569).  Returns NULL for ROM lengths the
  * reference cannot construct (it panics on those). */
 orc_atari* orc_create(const uint8_t* rom, size_t rom_len);
@@ -106,6 +114,7 @@ uint64_t       orc_rrun_frame(orc_ratari* e);
 const uint8_t* orc_rframebuffer(const orc_ratari* e);
 void           orc_rram(const orc_ratari* e, uint8_t* out128);
 void           orc_rregs(const orc_ratari* e, uint32_t* out8);
+unsigned       orc_rmapper(const orc_ratari* e);
 size_t         orc_rtia_size(void);
 void           orc_rtia_copy(const orc_ratari* e, void* out);
 /* k frames on each of n rendering consoles (actions [k][n]), nthreads threads. */

@@ -46,7 +46,7 @@ _fields = [
     ("ctrlpf", "u1"), ("refp0", "u1"), ("refp1", "u1"),
     ("pf0", "u1"), ("pf1", "u1"), ("pf2", "u1"),
     ("bank", "u1"), ("scheme", "u1"), ("_pad_end", "u1", (2,)),
-    ("_pad_ext", "u1", (3,)),
+    ("mapper", "u1", (2,)), ("_pad_ext", "u1"),
     ("cycles", "<u8"), ("frame_no", "<u4"), ("run_status", "<u4"),
 ]
 STATE_DTYPE = np.dtype(_fields, align=False)
@@ -116,6 +116,10 @@ def lib() -> ctypes.CDLL:
         L.orc_rframebuffer.argtypes = [vp]
         L.orc_rram.argtypes = [vp, u8p]
         L.orc_rregs.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32)]
+        L.orc_rmapper.restype = ctypes.c_uint
+        L.orc_rmapper.argtypes = [vp]
+        L.orc_rom_set_scheme.restype = ctypes.c_int
+        L.orc_rom_set_scheme.argtypes = [u8p, sz, ctypes.c_int]
         L.orc_rtia_size.restype = sz
         L.orc_rtia_copy.argtypes = [vp, vp]
         L.orc_rrun_batch.restype = ctypes.c_uint64
@@ -242,6 +246,10 @@ class RenderAtari:
         lib().orc_rregs(self._p, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
         return out
 
+    def mapper(self) -> int:
+        """E0 / 3F bank state, as fa_state.mapper (little-endian 16 bits)."""
+        return int(lib().orc_rmapper(self._p))
+
     def tia_record(self) -> np.ndarray:
         out = np.zeros(1, RTIA_DTYPE)
         assert RTIA_DTYPE.itemsize == lib().orc_rtia_size()
@@ -269,6 +277,18 @@ def render_steps(consoles, actions: np.ndarray, nthreads: int | None = None, out
     if not outputs:
         return None
     return (np.stack([c.framebuffer() for c in consoles]), np.stack([c.ram() for c in consoles]))
+
+
+SCHEMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "auto": -1}
+
+
+def set_rom_scheme(rom: bytes, scheme) -> None:
+    """The oracle's fa_rom_set_scheme: these bytes run under `scheme` in every
+    later Atari / RenderAtari / reset_state / run_batch ("auto" forgets it)."""
+    r = _bytes_arr(rom)
+    code = SCHEMES[scheme.lower()] if isinstance(scheme, str) else int(scheme)
+    if lib().orc_rom_set_scheme(_u8(r), len(r), code) != 0:
+        raise ValueError(f"scheme {scheme!r} cannot hold a {len(r)}-byte ROM")
 
 
 def reset_state(rom: bytes) -> np.ndarray:

@@ -1,0 +1,126 @@
+"""GPU parity of the E0 and 3F bank-switching schemes (registered per ROM).
+
+The reference has neither scheme (it crashes on E0 carts), so the oracle's
+restatement, pinned by the hand-checked programs of test_mappers.py, is the
+checker here: full state (including the slice map) and RAM after every call,
+through the handle's persistent and plain forms, every warp policy, a pool
+that mixes sliced and 4K-bank carts in one launch, state upload, and the
+rendering console."""
+import numpy as np
+import pytest
+
+import oracle
+from fa_pkg import carts, fa
+from test_gpu_parity import assert_states_equal, oracle_states
+from test_gpu_render import check as render_check
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def need_gpu():
+    if fa.device_count() < 1:
+        pytest.skip("no CUDA device")
+
+
+@pytest.fixture(scope="module")
+def sliced():
+    out = {"e0": (carts.e0_cart(), "e0"), "3f16": (carts.f3_cart(16384), "3f"), "3f6": (carts.f3_cart(6144), "3f")}
+    for c, sch in out.values():
+        fa.set_rom_scheme(c.rom, sch)
+        oracle.set_rom_scheme(c.rom, sch)
+    yield {k: c for k, (c, _) in out.items()}
+    for c, _ in out.values():
+        fa.set_rom_scheme(c.rom, "auto")
+        oracle.set_rom_scheme(c.rom, "auto")
+
+
+@pytest.mark.parametrize("name", ["e0", "3f16", "3f6"])
+@pytest.mark.parametrize("sched", ["pc", "lane", "line", "match"])
+def test_sliced_carts_match_oracle(sliced, name, sched):
+    rom = sliced[name].rom
+    n, k, chunk = 150, 12, 4
+    acts = carts.actions(seed=21, n=n, frames=k)
+    ref = oracle_states(rom, n)
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.set_launch(128, sched, False)
+        obs = g.reset()
+        assert np.array_equal(obs, ref["ram"])
+        assert_states_equal(g.download_states(), ref, f"{name} reset")
+        for f0 in range(0, k, chunk):
+            obs = g.step_multi(acts[f0:f0 + chunk], chunk)
+            o_obs, _ = oracle.run_batch(rom, ref, acts[f0:f0 + chunk], chunk)
+            assert np.array_equal(obs, o_obs), f"{name}/{sched} frames {f0}..{f0 + chunk}"
+            assert_states_equal(g.download_states(), ref, f"{name}/{sched} after {f0 + chunk}")
+    maps = {int(m[0]) | int(m[1]) << 8 for m in ref["mapper"]}
+    assert int(ref["scheme"][0]) in (4, 5)
+    assert len(maps) >= 1
+
+
+@pytest.mark.parametrize("block,persistent", [(256, False), (128, True)])
+def test_sliced_launch_shapes_and_per_frame(sliced, block, persistent):
+    rom = sliced["e0"].rom
+    n, k = 500, 6
+    acts = carts.actions(seed=22, n=n, frames=k)
+    ref = oracle_states(rom, n)
+    o_obs, _ = oracle.run_batch(rom, ref, acts, k)
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.set_launch(block, "pc", persistent)
+        g.reset()
+        for f in range(k):
+            obs = g.step(acts[f])
+        assert np.array_equal(obs, o_obs)
+        assert_states_equal(g.download_states(), ref, f"block {block} persistent {persistent}")
+
+
+def test_pool_mixes_sliced_and_4k_bank_carts(sliced):
+    mixed = carts.mixed_carts()
+    roms = [mixed[0].rom, sliced["e0"].rom, mixed[2].rom, sliced["3f16"].rom, sliced["3f6"].rom, mixed[3].rom]
+    counts = [300, 200, 90, 130, 64, 33]
+    k = 5
+    acts = [carts.actions(seed=50 + i, n=n, frames=k) for i, n in enumerate(counts)]
+    with fa.AtariPool() as pool:
+        for r, n in zip(roms, counts):
+            pool.add_cart(r, n)
+        obs = pool.step(acts, k)
+        for g, (r, n) in enumerate(zip(roms, counts)):
+            st = oracle_states(r, n)
+            o, _ = oracle.run_batch(r, st, acts[g], k)
+            assert np.array_equal(obs[g], o), f"group {g}"
+            assert_states_equal(pool.group(g).download_states(), st, f"group {g}")
+
+
+def test_sliced_state_upload_round_trip(sliced):
+    rom = sliced["3f16"].rom
+    n = 64
+    ref = oracle_states(rom, n)
+    oracle.run_batch(rom, ref, carts.actions(seed=3, n=n, frames=5), 5)
+    ref["mapper"][:, 0] = np.arange(n) % 7                  # every lower bank, set by hand
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.upload_states(ref)
+        got = g.download_states()
+        assert_states_equal(got, ref, "round trip")
+        acts = carts.actions(seed=4, n=n, frames=3)
+        obs = g.step_multi(acts, 3)
+        # The oracle rebuilds its windows from the uploaded mapper field too.
+        o_obs, _ = oracle.run_batch(rom, ref, acts, 3)
+        assert np.array_equal(obs, o_obs)
+        assert_states_equal(g.download_states(), ref, "continued")
+
+
+@pytest.mark.parametrize("name", ["e0", "3f16"])
+def test_sliced_rendering_console_matches_oracle(sliced, name):
+    rom = sliced[name].rom
+    n, k = 40, 3
+    consoles = oracle.render_reset(rom, n)
+    with fa.AtariRender(rom, n) as g:
+        fb, ram = g.reset()
+        render_check(fb, ram, g.states(), consoles, f"{name} reset")
+        for c in range(2):
+            acts = carts.actions(seed=70 + c, n=n, frames=k)
+            fb, ram = g.step_multi(acts, k)
+            oracle.render_steps(consoles, acts)
+            st = g.states()
+            render_check(fb, ram, st, consoles, f"{name} call {c}")
+            for i, con in enumerate(consoles):
+                assert int(st[i]["mapper"][0]) | int(st[i]["mapper"][1]) << 8 == con.mapper(), f"{name} mapper {i}"
