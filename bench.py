@@ -102,6 +102,10 @@ def workload(name: str, carts):
     if name == "scale":
         return ("scale: 1000000 instances of the 32K F4 cart, K=16, reset every 2000 frames",
                 [(carts.scale_cart(), 1_000_000)], 16, 2000)
+    if name == "mappers":
+        # Schemes the reference lacks, registered per ROM (fa_rom_set_scheme).
+        return ("sliced-bank carts: 8K E0 / 16K 3F / 6K 3F, 40000/40000/20000 instances, K=4 frames per call",
+                [(carts.e0_cart(), 40_000), (carts.f3_cart(16384), 40_000), (carts.f3_cart(6144), 20_000)], 4, 0)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -264,6 +268,9 @@ def cpu_reference(carts, spec, k, seconds_target=15.0):
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
     cores = os.cpu_count() or 1
+    for c, _ in spec:
+        if c.scheme:
+            oracle.set_rom_scheme(c.rom, c.scheme)
     total = sum(n for _, n in spec)
     per_cart = [(c, max(1, round(n * 4 * cores / total))) for c, n in spec]
     states = {c.spec.name: np.array([oracle.reset_state(c.rom)] * m, dtype=oracle.STATE_DTYPE)
@@ -331,6 +338,9 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
     fa.set_device(local_rank)
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    for c, _ in spec:
+        if c.scheme:
+            fa.set_rom_scheme(c.rom, c.scheme)
     pool = fa.AtariPool()
     groups = []
     for c, n in spec:
@@ -674,7 +684,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed",
-                    choices=["mixed", "divergence", "plain", "scale", "converged", "serve", "render"])
+                    choices=["mixed", "divergence", "plain", "scale", "converged", "serve", "render", "mappers"])
     ap.add_argument("--serve-requests", type=int, default=20000, help="saturation requests of the serve workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     ap.add_argument("--render-instances", type=int, default=RENDER_N, help="consoles of the render workload")

@@ -250,6 +250,7 @@ class Cart:
     spec: CartSpec
     rom: bytes
     labels: Dict[str, int] = field(default_factory=dict)
+    scheme: str = ""            # a scheme to register for this ROM ("e0", "3f"); "" = the size rule
 
 
 class _BlockGen:
@@ -858,7 +859,7 @@ def e0_cart(seed: int = 6, lines: int = 64) -> Cart:
     assert labels["reset"] == 0xFC02 and labels["map7"] < 0xFFE0
     rom = b"".join(slices) + img
     assert len(rom) == 8192
-    return Cart(CartSpec("e0_8k", 8192, seed, wsync_density=1.0), rom, labels)
+    return Cart(CartSpec("e0_8k", 8192, seed, wsync_density=1.0), rom, labels, scheme="e0")
 
 
 def f3_cart(size: int = 16384, seed: int = 7, lines: int = 64) -> Cart:
@@ -902,4 +903,4 @@ def f3_cart(size: int = 16384, seed: int = 7, lines: int = 64) -> Cart:
     assert labels["reset"] == 0xF800
     rom = b"".join(banks) + img
     assert len(rom) == size
-    return Cart(CartSpec(f"3f_{size // 1024}k", size, seed, wsync_density=1.0), rom, labels)
+    return Cart(CartSpec(f"3f_{size // 1024}k", size, seed, wsync_density=1.0), rom, labels, scheme="3f")

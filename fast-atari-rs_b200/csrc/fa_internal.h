@@ -36,6 +36,14 @@ struct FaGroup {
     uint32_t rom_owner;          // 1 if this group stages the ROM (set by fa_launch_run)
 };
 
+// The kernel build a set of groups needs (FA_MAPS_*).
+static inline int fa_maps_of(const FaGroup* g, uint32_t ngroups)
+{
+    bool sl = false, std4k = false;
+    for (uint32_t i = 0; i < ngroups; i++) (fa_map_kind(g[i].hot_lo) ? sl : std4k) = true;
+    return sl ? (std4k ? FA_MAPS_BOTH : FA_MAPS_SLICED) : FA_MAPS_4K;
+}
+
 struct FaLaunch {
     FaGroup g[FA_MAX_GROUPS];
     uint32_t ngroups;

@@ -19,7 +19,7 @@
 
 namespace fa {
 
-template <int BLOCK, bool SLICED_OK>
+template <int BLOCK, int MAPS>
 __global__ void __launch_bounds__(BLOCK) fa_run(const __grid_constant__ FaLaunch L)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(BLOCK) fa_run(const __grid_constant__ FaLaunch
         }
         const uint32_t first = (u - G.unit_begin) * BLOCK;
         const uint32_t count = G.n - first < BLOCK ? G.n - first : BLOCK;
-        run_unit<BLOCK, SLICED_OK>(G, first, count, rom_s, priv, threadIdx.x, L.instr, L.rounds);
+        run_unit<BLOCK, MAPS>(G, first, count, rom_s, priv, threadIdx.x, L.instr, L.rounds);
         __syncthreads();
     }
 }
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(BLOCK) fa_run(const __grid_constant__ FaLaunch
 // every CTA holds all of the launch's ROM images at once (the "ROM library",
 // staged once with TMA bulk copies), so units of any cart run in any warp
 // and a CTA can be as large as shared memory allows.
-template <int WARPS, bool SLICED_OK>
+template <int WARPS, int MAPS>
 __global__ void __launch_bounds__(WARPS * 32) fa_run_warps(const __grid_constant__ FaLaunch L)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(WARPS * 32) fa_run_warps(const __grid_constant
         const FaGroup& G = L.g[g];
         const uint32_t first = (u - G.unit_begin) * 32u;
         const uint32_t count = G.n - first < 32u ? G.n - first : 32u;
-        run_unit<32, SLICED_OK>(G, first, count, smem + G.rom_off, priv, lane, L.instr, L.rounds);
+        run_unit<32, MAPS>(G, first, count, smem + G.rom_off, priv, lane, L.instr, L.rounds);
     }
 }
 
@@ -134,16 +134,16 @@ std::map<std::pair<int, std::pair<int, size_t>>, int> g_per_sm;   // (device, bl
 // The dynamic shared-memory limit is raised once per (device, BLOCK) to the
 // largest any cart needs (32 KiB of ROM plus the private bytes), so launches
 // of smaller carts never lower it under a larger one.
-template <int BLOCK, bool SL = false>
+template <int BLOCK, int SL = 0>
 int per_sm_for(size_t smem)
 {
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lk(g_cfg_mu);
-    auto key = std::make_pair(dev, std::make_pair(BLOCK * 2 + (SL ? 1 : 0), smem));
+    auto key = std::make_pair(dev, std::make_pair(BLOCK * 4 + SL, smem));
     auto it = g_per_sm.find(key);
     if (it != g_per_sm.end()) return it->second;
-    const auto max_key = std::make_pair(dev, std::make_pair(BLOCK * 2 + (SL ? 1 : 0), (size_t)0));
+    const auto max_key = std::make_pair(dev, std::make_pair(BLOCK * 4 + SL, (size_t)0));
     if (g_per_sm.find(max_key) == g_per_sm.end()) {
         const int max_smem = 32768 + FA_SMEM_WORDS * BLOCK * 4;
         if (cudaFuncSetAttribute(fa::fa_run<BLOCK, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem) !=
@@ -159,7 +159,7 @@ int per_sm_for(size_t smem)
 }
 }  // namespace
 
-template <int BLOCK, bool SL>
+template <int BLOCK, int SL>
 static cudaError_t launch_block(const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
 {
     const size_t smem = (size_t)L.rom_bytes_max + (size_t)FA_SMEM_WORDS * BLOCK * 4u;
@@ -176,19 +176,27 @@ static cudaError_t launch_block(const FaLaunch& L, bool persistent, int sms, cud
     return cudaGetLastError();
 }
 
+template <int BLOCK>
+static cudaError_t launch_block_m(int maps, const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
+{
+    return maps == FA_MAPS_4K   ? launch_block<BLOCK, FA_MAPS_4K>(L, persistent, sms, s)
+         : maps == FA_MAPS_BOTH ? launch_block<BLOCK, FA_MAPS_BOTH>(L, persistent, sms, s)
+                                : launch_block<BLOCK, FA_MAPS_SLICED>(L, persistent, sms, s);
+}
+
 namespace {
 std::map<std::pair<int, std::pair<int, size_t>>, int> g_warps_per_sm;   // (device, warps, smem) -> CTAs/SM
 
-template <int WARPS, bool SL>
+template <int WARPS, int SL>
 int warps_per_sm_for(size_t smem)
 {
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lk(g_cfg_mu);
-    auto key = std::make_pair(dev, std::make_pair(WARPS * 2 + (SL ? 1 : 0), smem));
+    auto key = std::make_pair(dev, std::make_pair(WARPS * 4 + SL, smem));
     auto it = g_warps_per_sm.find(key);
     if (it != g_warps_per_sm.end()) return it->second;
-    const auto max_key = std::make_pair(dev, std::make_pair(WARPS * 2 + (SL ? 1 : 0), (size_t)0));
+    const auto max_key = std::make_pair(dev, std::make_pair(WARPS * 4 + SL, (size_t)0));
     if (g_warps_per_sm.find(max_key) == g_warps_per_sm.end()) {
         if (cudaFuncSetAttribute(fa::fa_run_warps<WARPS, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  FA_SMEM_PER_CTA_MAX) != cudaSuccess)
@@ -203,7 +211,7 @@ int warps_per_sm_for(size_t smem)
     return per_sm;
 }
 
-template <int WARPS, bool SL>
+template <int WARPS, int SL>
 cudaError_t launch_warps(const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
 {
     const size_t smem = (size_t)L.romlib_bytes + (size_t)WARPS * FA_SMEM_WORDS * 32u * 4u;
@@ -222,7 +230,7 @@ cudaError_t launch_warps(const FaLaunch& L, bool persistent, int sms, cudaStream
     return cudaGetLastError();
 }
 
-template <bool SL>
+template <int SL>
 cudaError_t launch_warps_n(int warps, const FaLaunch& L, bool persistent, int sms, cudaStream_t s)
 {
     switch (warps) {
@@ -265,8 +273,7 @@ static void plan_units(FaLaunch& L, uint32_t unit)
 cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int sms, cudaStream_t s)
 {
     FaLaunch L = L_in;
-    bool sliced = false;                                               // an E0 or 3F cart in the launch
-    for (uint32_t g = 0; g < L.ngroups; g++) sliced = sliced || fa_map_kind(L.g[g].hot_lo) != 0;
+    const int maps = fa_maps_of(L.g, L.ngroups);                       // which cores the carts need
     const uint32_t lib = plan_romlib(L);
     L.romlib_bytes = lib;
     const uint32_t slab = FA_SMEM_WORDS * 32u * 4u;
@@ -283,17 +290,18 @@ cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int 
                 if (w <= fit && w <= cap) { warps = w; break; }
         }
         plan_units(L, 32u);
-        return sliced ? launch_warps_n<true>(warps, L, persistent, sms, s)
-                      : launch_warps_n<false>(warps, L, persistent, sms, s);
+        return maps == FA_MAPS_4K   ? launch_warps_n<FA_MAPS_4K>(warps, L, persistent, sms, s)
+             : maps == FA_MAPS_BOTH ? launch_warps_n<FA_MAPS_BOTH>(warps, L, persistent, sms, s)
+                                    : launch_warps_n<FA_MAPS_SLICED>(warps, L, persistent, sms, s);
     }
     // ROM library too large for shared memory: CTA-granular units that
     // re-stage one cart's ROM at a time.
     plan_units(L, (uint32_t)block);
     switch (block) {
-    case 64: return sliced ? launch_block<64, true>(L, persistent, sms, s) : launch_block<64, false>(L, persistent, sms, s);
-    case 128: return sliced ? launch_block<128, true>(L, persistent, sms, s) : launch_block<128, false>(L, persistent, sms, s);
-    case 256: return sliced ? launch_block<256, true>(L, persistent, sms, s) : launch_block<256, false>(L, persistent, sms, s);
-    case 512: return sliced ? launch_block<512, true>(L, persistent, sms, s) : launch_block<512, false>(L, persistent, sms, s);
+    case 64: return launch_block_m<64>(maps, L, persistent, sms, s);
+    case 128: return launch_block_m<128>(maps, L, persistent, sms, s);
+    case 256: return launch_block_m<256>(maps, L, persistent, sms, s);
+    case 512: return launch_block_m<512>(maps, L, persistent, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }

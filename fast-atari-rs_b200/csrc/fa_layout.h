@@ -87,6 +87,10 @@ enum : uint32_t { FA_MAP_E0 = 1u, FA_MAP_3F = 2u };
 
 FA_HD static inline uint32_t fa_map_kind(uint32_t hot_lo) { return hot_lo < 0x1000u ? hot_lo >> 8 : 0u; }
 
+// Kernel builds by the cores they hold (see run_unit): 4K-bank carts only,
+// both kinds, sliced carts only.
+enum : int { FA_MAPS_4K = 0, FA_MAPS_BOTH = 1, FA_MAPS_SLICED = 2 };
+
 FA_HD static inline uint32_t fa_slices_from_mapper(uint32_t hot_lo, uint32_t m)
 {
     if (fa_map_kind(hot_lo) == FA_MAP_E0)

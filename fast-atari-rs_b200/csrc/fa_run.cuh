@@ -297,18 +297,19 @@ __device__ __forceinline__ void run_unit_as(const FaGroup& G, uint32_t first, ui
     if (rounds_out && (t & 31u) == 0 && rounds) atomicAdd(rounds_out, 32ull * rounds);
 }
 
-// Kernels come in two builds.  SLICED_OK = false (every launch without an E0
-// or 3F cart) holds the 4K-bank core alone.  SLICED_OK = true runs a unit of
-// a sliced cart (hot_lo below 0x1000) on the SLICED core and every other unit
-// on the 4K-bank core; its register budget is the larger of the two, so it is
-// launched only when the launch has a sliced cart.
-template <int BLOCK, bool SLICED_OK>
+// Kernels come in three builds, picked by the host from the carts of a
+// launch: FA_MAPS_4K (no E0 or 3F cart) holds the 4K-bank core alone,
+// FA_MAPS_SLICED (only E0 and 3F carts) the SLICED core alone, and
+// FA_MAPS_BOTH runs each unit on its cart's core (hot_lo below 0x1000:
+// sliced).  A build's register budget is the largest of the cores it holds,
+// so the single-core builds keep their own.
+template <int BLOCK, int MAPS>
 __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint32_t count, const uint8_t* rom_s,
                                          uint32_t* priv, uint32_t t, unsigned long long* instr_out,
                                          unsigned long long* rounds_out)
 {
-    if (SLICED_OK && fa_map_kind(G.hot_lo))
-        run_unit_as<BLOCK, SLICED_OK>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
+    if (MAPS == FA_MAPS_SLICED || (MAPS == FA_MAPS_BOTH && fa_map_kind(G.hot_lo)))
+        run_unit_as<BLOCK, MAPS != FA_MAPS_4K>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
     else
         run_unit_as<BLOCK, false>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
 }

@@ -31,7 +31,7 @@ namespace fa {
 
 constexpr uint32_t FA_REQ_FAILED = 0x80000000u;   // bit of a request's unit counter
 
-template <int WARPS, bool SLICED_OK>
+template <int WARPS, int MAPS>
 __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) fa_serve(const __grid_constant__ FaServeLaunch L)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) fa_serve(const __grid_
     uint32_t phase = 0;
     const bool staged = stage_rom(smem, L.rom, rom_bytes, &bar, phase);
     if (!have) return;
-    if (staged) run_unit<32, SLICED_OK>(sg[warp], 0, s_count[warp], smem, priv, lane, L.instr, L.rounds);
+    if (staged) run_unit<32, MAPS>(sg[warp], 0, s_count[warp], smem, priv, lane, L.instr, L.rounds);
     else if (lane == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
     if (L.done) {
         // Every lane's state and observation stores precede the warp barrier;
@@ -103,7 +103,7 @@ std::mutex g_serve_mu;
 // largest serving launch (32 KiB of ROM plus the RAM slab).
 std::map<std::pair<int, int>, bool> g_serve_cfg;
 
-template <int WARPS, bool SL>
+template <int WARPS, int SL>
 cudaError_t launch_serve(const FaServeLaunch& L, cudaStream_t s)
 {
     int dev = 0;
@@ -111,7 +111,7 @@ cudaError_t launch_serve(const FaServeLaunch& L, cudaStream_t s)
     if (e != cudaSuccess) return e;
     {
         std::lock_guard<std::mutex> lk(g_serve_mu);
-        auto key = std::make_pair(dev, WARPS * 2 + (SL ? 1 : 0));
+        auto key = std::make_pair(dev, WARPS * 4 + SL);
         if (g_serve_cfg.find(key) == g_serve_cfg.end()) {
             e = cudaFuncSetAttribute(fa::fa_serve<WARPS, SL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      32768 + WARPS * FA_SMEM_WORDS * 32 * 4);
@@ -129,11 +129,11 @@ cudaError_t launch_serve(const FaServeLaunch& L, cudaStream_t s)
 cudaError_t fa_launch_serve(const FaServeLaunch& L, int block, cudaStream_t s)
 {
     if (L.nbanks < 1 || L.nbanks > 8) return cudaErrorInvalidValue;
-    const bool sl = fa_map_kind(L.hot_lo) != 0;                        // an E0 or 3F cart
+    const bool sl = fa_map_kind(L.hot_lo) != 0;                        // one cart per launch: E0 / 3F or not
     switch (block) {
-    case 128: return sl ? launch_serve<4, true>(L, s) : launch_serve<4, false>(L, s);
-    case 256: return sl ? launch_serve<8, true>(L, s) : launch_serve<8, false>(L, s);
-    case 512: return sl ? launch_serve<16, true>(L, s) : launch_serve<16, false>(L, s);
+    case 128: return sl ? launch_serve<4, FA_MAPS_SLICED>(L, s) : launch_serve<4, FA_MAPS_4K>(L, s);
+    case 256: return sl ? launch_serve<8, FA_MAPS_SLICED>(L, s) : launch_serve<8, FA_MAPS_4K>(L, s);
+    case 512: return sl ? launch_serve<16, FA_MAPS_SLICED>(L, s) : launch_serve<16, FA_MAPS_4K>(L, s);
     default: return cudaErrorInvalidValue;
     }
 }

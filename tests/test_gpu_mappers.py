@@ -124,3 +124,18 @@ def test_sliced_rendering_console_matches_oracle(sliced, name):
             render_check(fb, ram, st, consoles, f"{name} call {c}")
             for i, con in enumerate(consoles):
                 assert int(st[i]["mapper"][0]) | int(st[i]["mapper"][1]) << 8 == con.mapper(), f"{name} mapper {i}"
+
+
+def test_sliced_carts_in_the_server(sliced):
+    roms = [sliced["e0"].rom, carts.mixed_carts()[1].rom, sliced["3f6"].rom]
+    reqs = [(0, 70, 3), (1, 40, 2), (2, 33, 4), (0, 70, 2)]
+    with fa.AtariServer(roms) as srv:
+        sids = {c: srv.open(c) for c in (0, 1, 2)}
+        got = [srv.step(sids[c], carts.actions(seed=90 + i, n=n, frames=k), n, k)[0] for i, (c, n, k) in enumerate(reqs)]
+        states = {c: srv.states(sids[c]) for c in (0, 1, 2)}
+    ref = {c: oracle_states(roms[c], 70 if c == 0 else (40 if c == 1 else 33)) for c in (0, 1, 2)}
+    for i, (c, n, k) in enumerate(reqs):
+        o, _ = oracle.run_batch(roms[c], ref[c], carts.actions(seed=90 + i, n=n, frames=k), k)
+        assert np.array_equal(got[i], o), f"request {i}"
+    for c in (0, 1, 2):
+        assert_states_equal(states[c], ref[c], f"cart {c}")
