@@ -110,6 +110,7 @@ _SIGS = {
     "fa_pool_set_cta_warps": (_i, [_vp, _i]),
     "fa_autotune": (_i, [_u8p, _sz, _sz, _vp, _vp, _i, ctypes.POINTER(_i)]),
     "fa_obs_to_unit_f32": (_i, [_vp, _vp, _sz, _vp]),
+    "fa_obs_reward": (_i, [_vp, _sz, _vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "fa_server_create": (_i, [_vp, _vp, _i, _vp, ctypes.POINTER(_vp)]),
     "fa_server_destroy": (None, [_vp]),
     "fa_server_open": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_int64)]),
@@ -223,6 +224,40 @@ def guess_rom_scheme(rom: bytes) -> int:
     rc = int(lib().fa_rom_guess_scheme(_u8(r), len(r)))
     _check(min(rc, 0))
     return rc
+
+
+class RewardSpec(ctypes.Structure):
+    """fa_reward_spec: where a game keeps its score, lives and end flag in RAM
+    (offsets 0..127).  Score bytes most significant first, BCD or binary."""
+    _fields_ = [("score_addr", ctypes.c_uint8 * 4), ("score_bytes", ctypes.c_uint8), ("score_bcd", ctypes.c_uint8),
+                ("lives_addr", ctypes.c_uint8), ("lives_mask", ctypes.c_uint8), ("lives_shift", ctypes.c_uint8),
+                ("terminal_addr", ctypes.c_uint8), ("terminal_mask", ctypes.c_uint8),
+                ("terminal_value", ctypes.c_uint8)]
+
+    @classmethod
+    def make(cls, score=(), bcd=True, lives=None, terminal=None) -> "RewardSpec":
+        """score: RAM offsets (most significant first); lives: (offset, mask,
+        shift); terminal: (offset, mask, value)."""
+        sp = cls()
+        for i, a in enumerate(score):
+            sp.score_addr[i] = a
+        sp.score_bytes = len(score)
+        sp.score_bcd = 1 if bcd else 0
+        if lives:
+            sp.lives_addr, sp.lives_mask, sp.lives_shift = lives
+        if terminal:
+            sp.terminal_addr, sp.terminal_mask, sp.terminal_value = terminal
+        return sp
+
+
+EPISODE_TERMINAL, EPISODE_LIFE_LOST = 0x1, 0x2
+
+
+def obs_reward(d_obs: int, n: int, spec: RewardSpec, init: bool, d_score: int, d_lives: int,
+               d_reward: int = 0, d_flags: int = 0, stream: int = 0) -> None:
+    """fa_obs_reward on device pointers (torch tensors' data_ptr())."""
+    _check(lib().fa_obs_reward(_vp(d_obs), int(n), ctypes.byref(spec), 1 if init else 0, _vp(d_score), _vp(d_lives),
+                               _vp(d_reward or None), _vp(d_flags or None), _vp(stream or None)))
 
 
 class BatchAtariGpu:

@@ -6,6 +6,10 @@ through step_multi, truncation after max_steps (default 108,000), reward 0 and
 terminated false (the reference extracts no reward).  Observations are the
 N x 128 RAM bytes as f32 / 255, flattened to N*128 — produced on the device
 into a torch CUDA tensor (fa_obs_to_unit_f32) instead of on the host.
+
+with_reward(spec) adds what the reference lacks: per-instance rewards (score
+change) and episode flags (terminal test, life lost) decoded from RAM on the
+device (fa_obs_reward), returned as CUDA tensors of shape (N,).
 """
 from __future__ import annotations
 
@@ -13,7 +17,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import BatchAtariGpu, _check, _vp, lib
+from . import BatchAtariGpu, RewardSpec, _check, _vp, lib, obs_reward
 
 NUM_ACTIONS = 18            # src/rl4burn_env.rs:26
 DEFAULT_MAX_STEPS = 108_000  # :29
@@ -23,9 +27,10 @@ DEFAULT_FRAMESKIP = 4        # :32
 @dataclass
 class Step:
     observation: "object"    # torch.Tensor, float32, shape (N*128,), on the device
-    reward: float
-    terminated: bool
+    reward: "object"         # 0.0, or with a reward spec a float32 tensor (N,)
+    terminated: "object"     # False, or with a reward spec a bool tensor (N,) (terminal test)
     truncated: bool
+    life_lost: "object" = None   # with a reward spec: bool tensor (N,)
 
 
 class BatchAtariGpuEnv:
@@ -42,6 +47,22 @@ class BatchAtariGpuEnv:
         self._actions = torch.zeros(self.n * 64, dtype=torch.uint8, device=self.device)
         self._obs_u8 = torch.zeros(self.n * 128, dtype=torch.uint8, device=self.device)
         self._obs = torch.zeros(self.n * 128, dtype=torch.float32, device=self.device)
+        self.reward_spec = None
+
+    def with_reward(self, spec: RewardSpec) -> "BatchAtariGpuEnv":
+        """Score, lives and end-of-episode positions in RAM (fa_obs_reward)."""
+        t = self.torch
+        self.reward_spec = spec
+        self._score = t.zeros(self.n, dtype=t.int32, device=self.device)
+        self._lives = t.zeros(self.n, dtype=t.int32, device=self.device)
+        self._reward = t.zeros(self.n, dtype=t.float32, device=self.device)
+        self._flags = t.zeros(self.n, dtype=t.uint8, device=self.device)
+        return self
+
+    def _rewards(self, init: bool):
+        stream = self.torch.cuda.current_stream(self.device).cuda_stream
+        obs_reward(self._obs_u8.data_ptr(), self.n, self.reward_spec, init, self._score.data_ptr(),
+                   self._lives.data_ptr(), self._reward.data_ptr(), self._flags.data_ptr(), stream)
 
     # builder methods (src/rl4burn_env.rs:298-313)
     def with_max_steps(self, max_steps: int) -> "BatchAtariGpuEnv":
@@ -80,6 +101,8 @@ class BatchAtariGpuEnv:
         self.step_count = 0
         ram = self.gpu.reset()
         self._obs_u8.copy_(self.torch.from_numpy(np.ascontiguousarray(ram).reshape(-1)))
+        if self.reward_spec is not None:
+            self._rewards(init=True)
         return self._normalise().clone()
 
     def step(self, action: int) -> Step:
@@ -93,7 +116,11 @@ class BatchAtariGpuEnv:
         obs = self._normalise().clone()
         self.step_count += 1
         truncated = self.max_steps > 0 and self.step_count >= self.max_steps
-        return Step(obs, 0.0, False, truncated)
+        if self.reward_spec is None:
+            return Step(obs, 0.0, False, truncated)
+        self._rewards(init=False)
+        f = self._flags
+        return Step(obs, self._reward.clone(), (f & 1).bool(), truncated, (f & 2).bool())
 
     def close(self):
         self.gpu.close()

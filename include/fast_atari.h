@@ -342,6 +342,38 @@ void fa_graph_destroy(fa_graph* g);
  * written into a caller buffer of `count` floats, enqueued on `stream`. */
 int fa_obs_to_unit_f32(const uint8_t* d_obs, float* d_out, size_t count, void* stream);
 
+/*
+ * Reward and termination from RAM.  No counterpart in the reference, which
+ * returns reward 0 and never terminates (src/atari.rs:348,
+ * src/rl4burn_env.rs:123); where a game keeps its score and lives is per-game
+ * knowledge the caller supplies.  Offsets are RAM offsets 0..127 ($80 + offset).
+ */
+typedef struct fa_reward_spec {
+    uint8_t score_addr[4];   /* score bytes, most significant first */
+    uint8_t score_bytes;     /* 0..4 (0: no score, reward 0) */
+    uint8_t score_bcd;       /* 1: two decimal digits per byte (high nibble first); 0: binary */
+    uint8_t lives_addr;      /* lives = (ram[lives_addr] & lives_mask) >> lives_shift */
+    uint8_t lives_mask;      /* 0: no lives counter */
+    uint8_t lives_shift;
+    uint8_t terminal_addr;   /* terminal when (ram[terminal_addr] & terminal_mask) == terminal_value */
+    uint8_t terminal_mask;   /* 0: no terminal test */
+    uint8_t terminal_value;
+} fa_reward_spec;
+
+#define FA_EPISODE_TERMINAL  0x1u   /* the terminal test holds */
+#define FA_EPISODE_LIFE_LOST 0x2u   /* the lives counter went down */
+
+/*
+ * For n observation rows (128 bytes each, as fa_step writes them) on the
+ * device: reward[i] = score - d_score[i] as float, flags[i] = FA_EPISODE_*,
+ * then d_score[i] = score and d_lives[i] = lives.  With init != 0 only the
+ * scores and lives are recorded (reward 0, no life lost), as after a reset.
+ * d_score / d_lives persist between calls (n int32 each, caller-owned);
+ * d_reward (n floats) and d_flags (n bytes) may be null.  Enqueued on stream.
+ */
+int fa_obs_reward(const uint8_t* d_obs, size_t n, const fa_reward_spec* spec, int init, int32_t* d_score,
+                  int32_t* d_lives, float* d_reward, uint8_t* d_flags, void* stream);
+
 /* ---------------------------------------------------------------- autotuning
  * Project-written tuner (no reference counterpart; the reference hard-codes
  * 128-thread blocks and a manual set_sorted).  For one ROM and n instances it

@@ -1,6 +1,7 @@
 """C ABI checks that need no GPU: the library loads, exports every symbol the
 public header declares, and its state layout matches the header and the
 oracle's restatement of the reference AtariStateGpu (src/cuda_env.rs:10-38)."""
+import ctypes
 import re
 import subprocess
 
@@ -73,3 +74,24 @@ def test_server_without_device_fails_loudly():
     with pytest.raises(fa.FaError) as ei:
         fa.AtariServer([bytes(4096)])
     assert ei.value.code == -4
+
+
+def test_reward_spec_rejected_before_any_device_work():
+    # Invalid specs fail in host code, before a launch; the fake device
+    # pointers are never dereferenced.
+    L = fa.lib()
+    fake = 4096
+    for kw in ({"score": (1, 2, 3, 4, 5)}, {"score": (200,)}, {"lives": (130, 1, 0)}, {"lives": (1, 1, 9)},
+               {"terminal": (128, 1, 1)}):
+        sp = fa.RewardSpec()
+        if "score" in kw:
+            sc = kw["score"]
+            for i, a in enumerate(sc[:4]):
+                sp.score_addr[i] = a
+            sp.score_bytes = len(sc)
+        if "lives" in kw:
+            sp.lives_addr, sp.lives_mask, sp.lives_shift = kw["lives"]
+        if "terminal" in kw:
+            sp.terminal_addr, sp.terminal_mask, sp.terminal_value = kw["terminal"]
+        rc = L.fa_obs_reward(fa._vp(fake), 8, ctypes.byref(sp), 0, fa._vp(fake), fa._vp(fake), None, None, None)
+        assert rc == -1, (kw, rc)                     # FA_ERR_INVALID

@@ -56,3 +56,45 @@ def test_autotune_returns_a_measured_best():
     assert len({(t["sched"], t["persistent"], t["cta_warps"], t["block"]) for t in last}) == 1
     assert best == max(last, key=lambda t: t["frames_per_s"])
     assert best["sched"] in (0, 1, 2, 3) and best["k"] in (1, 2, 4, 8, 16)
+
+
+def _decode(ram, spec_args):
+    """The reward rule of fa_obs_reward restated in numpy (int32 arithmetic)."""
+    score, bcd, lives, terminal = spec_args
+    s = np.zeros(len(ram), np.int64)
+    for a in score:
+        v = ram[:, a].astype(np.int64)
+        s = s * 100 + (v >> 4) * 10 + (v & 15) if bcd else (s << 8) | v
+    s = s.astype(np.uint64).astype(np.uint32).view(np.int32)
+    l = ((ram[:, lives[0]] & lives[1]) >> lives[2]).astype(np.int32) if lives else np.zeros(len(ram), np.int32)
+    t = ((ram[:, terminal[0]] & terminal[1]) == terminal[2]) if terminal else np.zeros(len(ram), bool)
+    return s, l, t
+
+
+@pytest.mark.parametrize("spec_args", [((3, 4, 5), True, (7, 0x0C, 2), (9, 0x80, 0x80)),
+                                       ((10, 11, 12, 13), False, (20, 0xFF, 0), None),
+                                       ((), True, None, (30, 0x01, 0x00))])
+def test_env_rewards_from_ram(spec_args):
+    import fast_atari_b200.env as fenv
+    score, bcd, lives, terminal = spec_args
+    rom = carts.divergence_cart().rom
+    n = 70
+    spec = fa.RewardSpec.make(score, bcd, lives, terminal)
+    env = fenv.BatchAtariGpuEnv(rom, n).with_reward(spec)
+    env.reset()
+    ref = np.array([oracle.reset_state(rom)] * n, dtype=oracle.STATE_DTYPE)
+    prev_s, prev_l, _ = _decode(ref["ram"], spec_args)
+    saw_reward = False
+    for t, action in enumerate([3, 12, 0, 7, 17, 5]):
+        step = env.step(action)
+        o_obs, _ = oracle.run_batch(rom, ref, np.full(4 * n, action, np.uint8), 4)
+        s, l, term = _decode(o_obs, spec_args)
+        want_r = (s - prev_s).astype(np.int32).astype(np.float32)
+        assert np.array_equal(step.reward.cpu().numpy(), want_r), t
+        assert np.array_equal(step.terminated.cpu().numpy(), term), t
+        want_lost = (l < prev_l) if lives else np.zeros(n, bool)
+        assert np.array_equal(step.life_lost.cpu().numpy(), want_lost), t
+        saw_reward = saw_reward or bool((want_r != 0).any())
+        prev_s, prev_l = s, l
+    assert saw_reward or not score
+    env.close()
