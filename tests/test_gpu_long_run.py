@@ -1,8 +1,8 @@
 """Ten thousand frames, bit for bit: the four mappers of the mixed batch in one
 pool, stepped 100 frames per batched call for 10,000 frames, against the oracle
 after every call (RAM) and at the end (full state: registers, flags, cycle
-counter, RAM, TIA/PIA fields, bank, frame counter, status).  The north star's
-correctness bar is 0 mismatches over 10^4 frames."""
+counter, RAM, TIA/PIA fields, bank, frame counter, status).  The bar is 0
+mismatches over 10^4 frames."""
 import numpy as np
 import pytest
 
