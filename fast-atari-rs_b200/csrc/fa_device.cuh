@@ -457,9 +457,16 @@ static __device__ __forceinline__ void r_resize_commit(RState& s, uint8_t* pv)  
 }
 
 // Tia::write (tia.rs:570-674) of register a & 0x3F.
+// Registers whose write can change a pixel or a collision latch from the
+// next clock on: VSYNC, VBLANK, NUSIZx-REFPx, RESPx-RESBL, GRPx-ENABL,
+// VDELx-RESMPx, HMOVE and CXCLR.  The playfield registers reach the pixels
+// through the delayed-write queue (flushed when it fires); WSYNC, RSYNC,
+// audio, HMxx and HMCLR never do.
+constexpr uint64_t R_PIXEL_REGS = 0x17E0F81F1FF3ull;
+
 static __device__ __forceinline__ void r_write(uint32_t a, uint32_t v, RState& s, uint8_t* pv, uint8_t* fbp)
 {
-    r_pending(s, pv, fbp, s.clock);                                  // the pixels drawn before the write
+    if ((R_PIXEL_REGS >> (a & 0x3Fu)) & 1u) r_pending(s, pv, fbp, s.clock);   // the pixels drawn before the write
     switch (a & 0x3Fu) {
     case 0x00:
         if (!(s.tw & 2u) && (v & 2u)) { r_resize_commit(s, pv); s.scanline = 0; s.tw |= TW_FCOMP; }
@@ -523,21 +530,27 @@ static __device__ __forceinline__ void r_write(uint32_t a, uint32_t v, RState& s
     }
 }
 
-// Bus::write of a TIA register (src/atari.rs:207-222): two TIA clocks, the
-// write, one TIA clock (the PIA clock follows in the caller).
-static __device__ __noinline__ RState render_write_cycle(uint32_t a, uint32_t v, RState s, uint32_t pins, uint8_t* pv,
-                                                         uint8_t* fbp)
+// `owed` whole CPU cycles, then Bus::write of a TIA register
+// (src/atari.rs:207-222): two TIA clocks, the write, one TIA clock and the
+// PIA clock.  One call per write: the cycles before it ride along.
+static __device__ __noinline__ RState render_write_cycle(uint32_t a, uint32_t v, uint32_t owed, RState s, uint32_t pins,
+                                                         uint8_t* pv, uint8_t* fbp)
 {
+    if (owed) {
+        r_advance(s, 3u * owed, pins, pv, fbp);
+        r_pia_ticks(s, owed);
+    }
     r_advance(s, 2u, pins, pv, fbp);
     r_write(a, v, s, pv, fbp);
     r_advance(s, 1u, pins, pv, fbp);
+    r_pia_tick(s);
     return s;
 }
 
 // Tia::read (tia.rs:533-566) or Pia::read of an I/O register (pia.rs:169-199);
 // .y = 1 when the read clears the timer's underflow flag (INTIM).
-static __device__ __noinline__ uint2 render_read(uint32_t a, RState s, uint32_t pins, uint32_t pads, uint32_t ports,
-                                                 const uint8_t* pv)
+static __device__ __forceinline__ uint2 r_read_value(uint32_t a, const RState& s, uint32_t pins, uint32_t pads,
+                                                     uint32_t ports, const uint8_t* pv)
 {
     if ((a & 0x1080u) == 0) {
         const uint32_t r = a & 0x0Fu;
@@ -560,6 +573,32 @@ static __device__ __noinline__ uint2 render_read(uint32_t a, RState s, uint32_t 
     case 5: return make_uint2(s.uf ? 0x80u : 0u, 0u);
     default: return make_uint2(0u, 0u);
     }
+}
+
+struct RRead {
+    RState s;
+    uint32_t v;
+};
+
+// `owed` whole CPU cycles, then the read of a TIA or PIA register in its own
+// cycle (Bus::read, src/atari.rs:195-205): collisions drawn up to the beam,
+// the value, then three TIA clocks and the PIA clock.  One call per read.
+static __device__ __noinline__ RRead render_io_read(uint32_t a, uint32_t owed, RState s, uint32_t pins, uint32_t pads,
+                                                    uint32_t ports, uint8_t* pv, uint8_t* fbp)
+{
+    if (owed) {
+        r_advance(s, 3u * owed, pins, pv, fbp);
+        r_pia_ticks(s, owed);
+    }
+    if ((a & 0x1080u) == 0 && (a & 0x0Fu) < 8u) r_pending(s, pv, fbp, s.clock);   // collisions so far
+    const uint2 r = r_read_value(a, s, pins, pads, ports, pv);
+    if (r.y) s.uf = 0;                                               // INTIM read clears the flag
+    r_advance(s, 3u, pins, pv, fbp);
+    r_pia_tick(s);
+    RRead out;
+    out.s = s;
+    out.v = r.x;
+    return out;
 }
 
 template <int BLOCK, bool RENDER = false, bool SLICED = false>
@@ -727,11 +766,11 @@ struct Emu {
     __device__ __forceinline__ uint32_t io(uint32_t a, uint32_t j)   // TIA or PIA register read
     {
         if constexpr (RENDER) {
-            rsync(j);
-            const uint32_t v = r_io_read(a);
-            rcycles(1u);
+            const uint32_t d = j - done;                              // cycles owed before this one
+            const RRead r = render_io_read(a, (int32_t)d > 0 ? d : 0u, rpack(), pins, pads, ports, pv, fbp);
+            runpack(r.s);
             done = j + 1u;
-            return v;
+            return r.v;
         } else {
             uint32_t r = io_read(a, pcnt, pins, pads, ports, tv | (uf << 16), (const uint8_t*)column(), G->stride * 4u);
             if (r & 0x100u) uf = 0;                                 // INTIM read clears the flag
@@ -742,8 +781,13 @@ struct Emu {
     {
         if constexpr (SLICED) f3_write(a, v);                       // the write still reaches the TIA
         if constexpr (RENDER) {
-            rsync(j);
-            r_write_cycle(a, v);
+            if ((a & 0x1080u) != 0) {                                 // PIA register: rare, the general path
+                rsync(j);
+                r_write_cycle(a, v);
+            } else {
+                const uint32_t d = j - done;
+                runpack(render_write_cycle(a, v, (int32_t)d > 0 ? d : 0u, rpack(), pins, pv, fbp));
+            }
             done = j + 1u;
         } else if (a & 0x200u) {
             uint4 r = pia_write_io(a, v, ports, tv, ps, sel | (uf << 16));
@@ -1142,7 +1186,7 @@ struct Emu {
     // ------------------------------------------------------------ rendering console
     // Used only by RENDER instantiations.  The pixel-accurate Tia of the
     // reference's rendering console (src/tia.rs) and Pia::tick run out of
-    // line (render_cycles / render_tia_ticks / render_read / render_write_cycle,
+    // line (render_cycles / render_tia_ticks / render_io_read / render_write_cycle,
     // below), on the state they touch passed by value: one copy of the pixel
     // pipeline however many bus-access sites the interpreter has.
     uint32_t done;            // cycle of the current instruction the TIA and PIA have reached (0 - lag at its start)
@@ -1180,25 +1224,14 @@ struct Emu {
     {
         if (lag) { runpack(render_cycles(rpack(), lag, pins, pv, fbp)); lag = 0; }
     }
-    __device__ __forceinline__ uint32_t r_io_read(uint32_t a)
-    {
-        if ((a & 0x1080u) == 0 && (a & 0x0Fu) < 8u) runpack(render_pending(rpack(), pv, fbp));   // collisions so far
-        const uint2 r = render_read(a, rpack(), pins, pads, ports, pv);
-        if (r.y) uf = 0;                                            // INTIM read clears the flag
-        return r.x;
-    }
-    // Bus::write of a TIA or PIA register (src/atari.rs:207-222).
+    // Bus::write of a PIA register (src/atari.rs:207-222): two TIA clocks, the
+    // write, one TIA clock, the PIA clock.
     __device__ __forceinline__ void r_write_cycle(uint32_t a, uint32_t v)
     {
-        RState r;
-        if ((a & 0x1080u) != 0) {
-            r = render_tia_ticks(rpack(), 2u, pins, pv, fbp);
-            const uint4 q = pia_write_io(a, v, ports, r.tv, r.ps, r.sel | (r.uf << 16));
-            ports = q.x; r.tv = q.y; r.ps = q.z; r.sel = q.w & 0xFFFFu; r.uf = q.w >> 16;
-            r = render_tia_ticks(r, 1u, pins, pv, fbp);
-        } else {
-            r = render_write_cycle(a, v, rpack(), pins, pv, fbp);
-        }
+        RState r = render_tia_ticks(rpack(), 2u, pins, pv, fbp);
+        const uint4 q = pia_write_io(a, v, ports, r.tv, r.ps, r.sel | (r.uf << 16));
+        ports = q.x; r.tv = q.y; r.ps = q.z; r.sel = q.w & 0xFFFFu; r.uf = q.w >> 16;
+        r = render_tia_ticks(r, 1u, pins, pv, fbp);
         runpack(r);
         pia_tick1();
     }
