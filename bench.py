@@ -562,7 +562,7 @@ def run_render_arm(args, fa, carts, rank, world, local_rank):
     steps = max(1, min(args.steps, 20))
     calls = args.warmup + steps
     rom = carts.render_cart().rom
-    g = fa.AtariRender(rom, n, cta_warps=8)
+    g = fa.AtariRender(rom, n, cta_warps=args.render_cta_warps)
     g.reset()
     acts = torch.empty(calls * k * n, dtype=torch.uint8, device=dev)
     for c in range(calls):
@@ -688,6 +688,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=20000, help="saturation requests of the serve workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     ap.add_argument("--render-instances", type=int, default=RENDER_N, help="consoles of the render workload")
+    ap.add_argument("--render-cta-warps", type=int, default=8, choices=[4, 8, 16],
+                    help="warps per CTA of the render kernel (80 registers: 8 -> 24 warps/SM, 16 -> 16)")
     ap.add_argument("--block", type=int, default=128)
     ap.add_argument("--tuning", default=None, help="JSON file of per-cart tuning records (skips the autotuner)")
     ap.add_argument("--no-autotune", action="store_true", help="default policy and weights instead of the autotuner")
