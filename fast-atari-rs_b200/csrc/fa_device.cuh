@@ -212,6 +212,13 @@ static __device__ __forceinline__ uint32_t r_spread4(uint32_t b)
     return t * 0xFu;
 }
 
+// Bits 0..3 of n moved to bits 0, 4, 8, 12.
+static __device__ __forceinline__ uint32_t r_nib(uint32_t n)
+{
+    const uint32_t t = (n | (n << 6)) & 0x303u;
+    return (t | (t << 3)) & 0x1111u;
+}
+
 // Bits 0..3 of n as byte masks.
 static __device__ __forceinline__ uint32_t r_bytes(uint32_t n)
 {
@@ -265,11 +272,6 @@ static __device__ __forceinline__ uint32_t r_missile_mask(const uint8_t* pv, uin
     return r_copies((1u << len) - 1u, len, rp16(pv, PB_POS + 4u + 2u * n), c_copies[nusiz & 7u], X);
 }
 
-static __device__ __forceinline__ uint32_t r_sel(uint32_t w, uint32_t color, uint32_t m)
-{
-    return (w & ~m) | (color * 0x01010101u & m);
-}
-
 // Pixels [x0, x1) of visible line `vis` with the TIA registers as they are:
 // Tia::tick's pixel stage (tia.rs:311-346) with compute_pixel (tia.rs:375-403)
 // and the object tests (tia.rs:406-507), over a span in which no register
@@ -300,15 +302,19 @@ static __device__ __noinline__ RState r_span(RState s, uint8_t* pv, uint8_t* fbp
             | ((bl & pf) ? 0x1000u : 0u) | ((p0 & p1) ? 0x4000u : 0u) | ((m0 & m1) ? 0x8000u : 0u);
         uint32_t A = p0 | m0, B = p1 | m1, F = pf | bl;
         if ((s.tw & TW_HMOVE) && X == 0u) { A &= ~0xFFu; B &= ~0xFFu; F &= ~0xFFu; }   // HMOVE comb: background
+        // compute_pixel's choice as a 2-bit index per pixel, for all 32 at once:
+        // 0 background, 1 playfield/ball, 2 player 1, 3 player 0.
+        const uint32_t I1 = (ctrlpf & 4u) ? (A | B) & ~F : A | B;    // playfield priority: F wins
+        const uint32_t I0 = (ctrlpf & 4u) ? F | A : A | (F & ~B);
         const uint32_t c0 = rp8(pv, PB_COLUP0), c1 = rp8(pv, PB_COLUP1), cbk = rp8(pv, PB_COLUBK);
         const uint32_t cpf = rp8(pv, PB_COLUPF);
+        const uint32_t tl = cbk | (((ctrlpf & 2u) ? c0 : cpf) << 8) | (c1 << 16) | (c0 << 24);   // x < 80 (score mode)
+        const uint32_t tr = cbk | (((ctrlpf & 2u) ? c1 : cpf) << 8) | (c1 << 16) | (c0 << 24);
         for (uint32_t q = lo >> 2; q < (hi + 3u) >> 2; q++) {
             const uint32_t x = X + 4u * q;
-            const uint32_t mA = r_bytes(A >> (4u * q)), mB = r_bytes(B >> (4u * q)), mF = r_bytes(F >> (4u * q));
-            const uint32_t pfc = (ctrlpf & 2u) ? (x < 80u ? c0 : c1) : cpf;   // score mode
-            uint32_t w = cbk * 0x01010101u;
-            if (ctrlpf & 4u) w = r_sel(r_sel(r_sel(w, c1, mB), c0, mA), pfc, mF);   // playfield priority
-            else w = r_sel(r_sel(r_sel(w, pfc, mF), c1, mB), c0, mA);
+            // Four pixels' indices as a byte-permute selector, one nibble each.
+            const uint32_t sel = r_nib((I0 >> (4u * q)) & 0xFu) | (r_nib((I1 >> (4u * q)) & 0xFu) << 1);
+            const uint32_t w = __byte_perm(x < 80u ? tl : tr, 0u, sel);
             const uint32_t wl = lo > 4u * q ? lo - 4u * q : 0u, wh = hi < 4u * q + 4u ? hi - 4u * q : 4u;
             const uint32_t pm = ((1u << wh) - 1u) & ~((1u << wl) - 1u);
             const uint32_t word = (vis * FA_FB_W + x) >> 2;
