@@ -502,7 +502,8 @@ static __device__ __forceinline__ void r_write(uint32_t a, uint32_t v, RState& s
             wp8(pv, RB_DQ + 3u * n + 1u, a & 0x3Fu);
             wp8(pv, RB_DQ + 3u * n + 2u, v);
             wp8(pv, RB_DLEN, n + 1u);
-        } else {
+        } else {                                                    // queue full: written now
+            r_pending(s, pv, fbp, s.clock);
             wp8(pv, (a & 0x3Fu) == 0x0Du ? PB_PF0 : (a & 0x3Fu) == 0x0Eu ? PB_PF1 : PB_PF2, v);
         }
         break;
