@@ -179,8 +179,9 @@ int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len);
  * BatchAtariGpu::new (src/cuda_env.rs:112-126).  Uploads the ROM and allocates
  * SoA state for n instances on the current device.  The ROM length must be one
  * the reference can construct: 1..4096 (Fixed, mirrored into the 4K window),
- * 8192 (F8), 16384 (F6) or >= 32768 (F4, first 32 KiB used).  Instances start
- * zeroed, as in the reference; call fa_reset before stepping.
+ * 8192 (F8), 16384 (F6) or >= 32768 (F4, first 32 KiB used); or, for bytes
+ * registered with fa_rom_set_scheme, one the registered scheme holds.
+ * Instances start zeroed, as in the reference; call fa_reset before stepping.
  */
 int fa_create(const uint8_t* rom, size_t rom_len, size_t n, fa_handle** out);
 
@@ -563,6 +564,7 @@ unsigned long long fa_render_last_instructions(const fa_render* r);
  * allocates nothing.
  *   d_rom_image  nbanks * 4096 bytes, 16-byte aligned (Fixed carts as their
  *                mirrored 4 KiB window, banked carts as-is)
+ *   scheme       FA_SCHEME_FIXED, _F8, _F6 or _F4 (E0 and 3F are not taken here)
  *   d_state      the FA SoA state rows (fa_device_state layout), stride >= n
  *   d_actions    calls * k * n bytes; call c uses the slice at c * k * n
  *   d_obs        n * 128 bytes (16-byte aligned) or NULL; gets each call's RAM
