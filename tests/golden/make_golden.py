@@ -28,6 +28,10 @@ CASES = {
     "mixed_8k": (lambda: carts.mixed_carts()[1], 16, 60, 105),
     "mixed_16k": (lambda: carts.mixed_carts()[2], 16, 60, 106),
     "mixed_32k": (lambda: carts.mixed_carts()[3], 16, 60, 107),
+    # Schemes the reference lacks, registered per ROM for the run (cart.scheme).
+    "e0_8k": (carts.e0_cart, 16, 30, 108),
+    "3f_16k": (lambda: carts.f3_cart(16384), 16, 30, 109),
+    "3f_6k": (lambda: carts.f3_cart(6144), 16, 30, 110),
 }
 CHECKPOINTS = (1, 10, 30)
 
@@ -38,13 +42,21 @@ def sha(b) -> str:
 
 def vectors(name):
     make, n, frames, seed = CASES[name]
-    rom = make().rom
-    acts = carts.actions(seed=seed, n=n, frames=frames)
-    st = np.array([oracle.reset_state(rom)] * n, dtype=oracle.STATE_DTYPE)
-    trace, instr = oracle.run_batch(rom, st, acts, frames, trace=True)
+    cart = make()
+    rom = cart.rom
+    if cart.scheme:
+        oracle.set_rom_scheme(rom, cart.scheme)
+    try:
+        acts = carts.actions(seed=seed, n=n, frames=frames)
+        st = np.array([oracle.reset_state(rom)] * n, dtype=oracle.STATE_DTYPE)
+        trace, instr = oracle.run_batch(rom, st, acts, frames, trace=True)
+        reset_sha = sha(np.array([oracle.reset_state(rom)]).tobytes())
+    finally:
+        if cart.scheme:
+            oracle.set_rom_scheme(rom, "auto")
     return {
         "rom_sha256": sha(rom), "n": n, "frames": frames, "action_seed": seed,
-        "reset_state_sha256": sha(np.array([oracle.reset_state(rom)]).tobytes()),
+        "reset_state_sha256": reset_sha,
         "ram_sha256_at": {str(f): sha(trace[f - 1].tobytes()) for f in CHECKPOINTS + (frames,)},
         "final_state_sha256": sha(st.tobytes()),
         "instructions": instr,

@@ -139,3 +139,27 @@ def test_sliced_carts_in_the_server(sliced):
         assert np.array_equal(got[i], o), f"request {i}"
     for c in (0, 1, 2):
         assert_states_equal(states[c], ref[c], f"cart {c}")
+
+
+@pytest.mark.parametrize("name", ["e0_8k", "3f_16k", "3f_6k"])
+def test_sliced_carts_match_committed_golden_vectors(sliced, name):
+    """The frozen oracle vectors of tests/golden/ (RAM at checkpoint frames and
+    the full final state, mapper field included), without running the oracle."""
+    import hashlib
+    import json
+    from pathlib import Path
+    want = json.loads((Path(__file__).parent / "golden" / "oracle_vectors.json").read_text())[name]
+    rom = {"e0_8k": sliced["e0"], "3f_16k": sliced["3f16"], "3f_6k": sliced["3f6"]}[name].rom
+    assert hashlib.sha256(rom).hexdigest() == want["rom_sha256"]
+    n, frames = want["n"], want["frames"]
+    acts = carts.actions(seed=want["action_seed"], n=n, frames=frames)
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.reset()
+        assert hashlib.sha256(g.download_states()[:1].tobytes()).hexdigest() == want["reset_state_sha256"]
+        done = 0
+        for f_end in sorted(int(x) for x in want["ram_sha256_at"]):
+            obs = g.step_multi(acts[done:f_end], f_end - done)
+            done = f_end
+            assert hashlib.sha256(obs.tobytes()).hexdigest() == want["ram_sha256_at"][str(f_end)], f_end
+        st = g.download_states()
+    assert hashlib.sha256(st.tobytes()).hexdigest() == want["final_state_sha256"]
