@@ -169,10 +169,12 @@ int fa_rom_scheme(const uint8_t* rom, size_t rom_len);
  * applied by itself.  It counts absolute and indexed loads and stores aimed at
  * the E0 hotspots $1FE0-$1FF7, zero-page stores to $3F (STA/STX/STY $3F), and
  * accesses to the hotspots of the scheme the size rule gives (F8 $1FF8-$1FF9,
- * F6 $1FF6-$1FF9, F4 $1FF4-$1FFB).  An 8K image with at least two E0 accesses,
- * over twice the size-rule ones, is E0; at least two $3F stores, over twice
- * the size-rule accesses, make a 2K-multiple image 3F; anything else gets the
- * size rule. */
+ * F6 $1FF6-$1FF9, F4 $1FF4-$1FFB).  An 8K image with at least three E0
+ * accesses, over eight times the size-rule ones, and a reset vector in
+ * $1C00-$1FFF is E0; at least three $3F stores, over eight times the size-rule
+ * accesses, and a reset vector in $1800-$1FFF make a 2K-multiple image 3F;
+ * anything else gets the size rule.  On random bytes it picks E0 or 3F for a
+ * few percent of 8K images. */
 int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len);
 
 /*

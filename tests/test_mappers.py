@@ -156,3 +156,12 @@ def test_library_registry_and_guess():
         fa.set_rom_scheme(bytes(6144), "auto")
     with pytest.raises(fa.FaError):
         fa.rom_scheme(bytes(6144))                           # no size-rule scheme for 6K
+
+
+def test_guess_rarely_fires_on_random_bytes():
+    # Data regions look like code to a byte scan; the guess stays a hint.
+    rng = np.random.default_rng(7)
+    for size, by_size in ((4096, 0), (8192, 1), (16384, 2)):
+        wrong = sum(fa.guess_rom_scheme(rng.integers(0, 256, size, dtype=np.uint8).tobytes()) != by_size
+                    for _ in range(200))
+        assert wrong <= 10, (size, wrong)
