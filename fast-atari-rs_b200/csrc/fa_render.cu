@@ -371,8 +371,15 @@ int copy_d2h(fa_render* r, uint8_t* dst, const uint8_t* src, size_t bytes)
             e = cudaHostAlloc((void**)&g.buf[b], kStageChunk, cudaHostAllocDefault);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.done[b], cudaEventDisableTiming);
         }
-        r->stagers.push_back(g);   // freed with the handle, complete or not
-        if (e != cudaSuccess) return fa_fail(FA_ERR_CUDA, "pinned staging: %s", cudaGetErrorString(e));
+        if (e != cudaSuccess) {                    // keep only complete stagers
+            for (int b = 0; b < 2; b++) {
+                if (g.buf[b]) cudaFreeHost(g.buf[b]);
+                if (g.done[b]) cudaEventDestroy(g.done[b]);
+            }
+            if (g.stream) cudaStreamDestroy(g.stream);
+            return fa_fail(FA_ERR_CUDA, "pinned staging: %s", cudaGetErrorString(e));
+        }
+        r->stagers.push_back(g);
     }
     std::atomic<int> bad{0};
     std::vector<std::thread> th;
