@@ -268,7 +268,7 @@ extern "C" int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len)
     // The reset vector (the image's last two words but two) must point into
     // the part of the address space that is fixed at power-on: window 3
     // ($1C00-$1FFF) for E0, the last 2K ($1800-$1FFF) for 3F.
-    const uint32_t vec_hi = rom[rom_len - 3] & 0x1Fu;
+    const uint32_t vec_hi = rom_len >= 4 ? rom[rom_len - 3] & 0x1Fu : 0u;
     if (rom_len == 8192 && e0 >= 3 && e0 > 8 * own && (vec_hi & 0x1Cu) == 0x1Cu) return FA_SCHEME_E0;
     if (st3f >= 3 && st3f > 8 * own && (vec_hi & 0x18u) == 0x18u && scheme_len_ok(FA_SCHEME_3F, rom_len))
         return FA_SCHEME_3F;

@@ -165,3 +165,10 @@ def test_guess_rarely_fires_on_random_bytes():
         wrong = sum(fa.guess_rom_scheme(rng.integers(0, 256, size, dtype=np.uint8).tobytes()) != by_size
                     for _ in range(200))
         assert wrong <= 10, (size, wrong)
+
+
+def test_guess_and_scheme_of_tiny_roms():
+    for n in (1, 2, 3, 4):
+        rom = bytes(range(1, n + 1))
+        assert fa.guess_rom_scheme(rom) == 0                 # Fixed, mirrored: the size rule
+        assert fa.rom_scheme(rom) == 0
