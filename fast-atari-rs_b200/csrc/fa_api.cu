@@ -568,6 +568,7 @@ extern "C" int fa_set_states(fa_handle* h, const fa_state* in)
             return fa_fail(FA_ERR_INVALID, "instance %zu: timer_prescaler_select 0 (reference divides by it)", i);
         fa_state s = in[i];
         if (s.bank >= h->nbanks) s.bank = (uint8_t)(h->nbanks - 1);
+        if (fa_map_kind(h->hot_lo)) s.bank = 0;                 // sliced carts keep their banks in `mapper`
         // E0 slices to 3 bits, 3F banks modulo the bank count, 0 for the 4K-bank schemes.
         const uint32_t m = fa_mapper_from_slices(
             h->hot_lo, fa_slices_from_mapper(h->hot_lo, (uint32_t)s.mapper[0] | ((uint32_t)s.mapper[1] << 8)));
