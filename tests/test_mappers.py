@@ -172,3 +172,28 @@ def test_guess_and_scheme_of_tiny_roms():
         rom = bytes(range(1, n + 1))
         assert fa.guess_rom_scheme(rom) == 0                 # Fixed, mirrored: the size rule
         assert fa.rom_scheme(rom) == 0
+
+
+def test_registry_is_safe_across_threads():
+    import threading
+    roms = [bytes([i]) * 8192 for i in range(16)]
+    errors = []
+
+    def worker(k):
+        try:
+            for rep in range(200):
+                rom = roms[(k + rep) % len(roms)]
+                fa.set_rom_scheme(rom, "e0" if rep % 2 else "auto")
+                assert fa.rom_scheme(rom) in (1, 4)
+        except Exception as e:                       # surfaced below
+            errors.append(e)
+
+    ts = [threading.Thread(target=worker, args=(k,)) for k in range(8)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert not errors, errors
+    for rom in roms:
+        fa.set_rom_scheme(rom, "auto")
+        assert fa.rom_scheme(rom) == 1
