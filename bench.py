@@ -1,7 +1,7 @@
 """Benchmark of the batched Atari 2600 core on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mixed|divergence|plain|scale|serve]
+                    [--workload mixed|divergence|plain|scale|serve|render|mappers|micro]
 
 Default workload (the batched configuration the headline metric is quoted
 on): four seeded synthetic carts — 2K Fixed, 8K F8, 16K F6, 32K F4 with
@@ -185,6 +185,134 @@ def divergence_policies(fa, carts, n=50_000, frames=32, k_multi=16):
     return out
 
 
+# ------------------------------------------------------------------ the reference's own kernel
+REF_CUDA_LIB = ROOT / "oracle" / "_ref" / "libref_cuda.so"
+
+
+def ref_kernel_compare(fa, carts, n=50_000, frames=16):
+    """The kernel the reference ships (atari_frame_kernel and
+    atari_multi_frame_kernel of cuda/src/atari_kernel.cu, built for sm_100a
+    from the reference's sources into oracle/_ref/ by `make -C oracle ref`,
+    launched as its host binding does: grid ceil(n/128), block 128) against
+    this library on the plain 4K Fixed cart, the one cart on which the two
+    agree with the oracle.  Both start from this library's post-reset states
+    (the first 221 bytes of fa_state are the reference's AtariState) with the
+    same actions; each side is timed by CUDA events around its launches only.
+    Per-frame form (one launch per frame, BatchAtariGpu::step) and
+    step_multi form (all frames in one launch).  None where the reference's
+    kernels were not built."""
+    import ctypes
+    if not REF_CUDA_LIB.exists():
+        return None
+    import torch
+    L = ctypes.CDLL(str(REF_CUDA_LIB))
+    L.ref_state_size.restype = ctypes.c_int
+    L.ref_run.restype = ctypes.c_int
+    L.ref_run.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                          ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]
+    rom = carts.plain_cart().rom
+    acts = np.ascontiguousarray(carts.actions(seed=9, n=n, frames=frames))
+    size = L.ref_state_size()
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.reset()
+        snap = g.download_states().view(np.uint8).reshape(n, -1)[:, :221]
+    ref_st = np.zeros((n, size), np.uint8)
+    ref_st[:, :221] = snap
+    r = np.frombuffer(rom, np.uint8).copy()
+
+    def ref_ms(multi, nn, a):
+        st = np.ascontiguousarray(ref_st[:nn])
+        obs = np.empty((nn, 128), np.uint8)
+        ms = ctypes.c_float()
+        rc = L.ref_run(r.ctypes.data, len(r), st.ctypes.data, nn, np.ascontiguousarray(a).ctypes.data,
+                       a.shape[0], multi, 0, obs.ctypes.data, ctypes.byref(ms))
+        if rc:
+            raise RuntimeError(f"reference kernel launch failed: cudaError {rc}")
+        return ms.value, obs
+
+    d_acts = torch.from_numpy(acts.reshape(-1)).cuda()
+    stream = torch.cuda.Stream()
+    d_obs = torch.empty(n * 128, dtype=torch.uint8, device="cuda")
+
+    def ours_ms(multi):
+        with fa.BatchAtariGpu(rom, n) as g:
+            g.set_launch(128, "pc", bool(multi))
+            g.reset()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if multi:
+                g.step_multi_async(d_acts.data_ptr(), frames, d_obs.data_ptr(), stream.cuda_stream)
+            else:
+                for f in range(frames):
+                    g.step_multi_async(d_acts.data_ptr() + f * n, 1, d_obs.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1), d_obs.cpu().numpy().reshape(n, 128)
+
+    ref_ms(0, min(n, 1024), acts[:1, :min(n, 1024)])                   # module load, first launch
+    out = {"cart": "plain_4k_fixed", "instances": n, "frames": frames,
+           "reference": "cuda/src/atari_kernel.cu built for sm_100a (the kernels the reference ships)"}
+    for form, multi in (("per_frame", 0), ("step_multi", 1)):
+        ms_ref, obs_ref = ref_ms(multi, n, acts)
+        ms_our, obs_our = ours_ms(multi)
+        out[form] = {"reference_frames_per_s": n * frames / (ms_ref / 1e3),
+                     "ours_frames_per_s": n * frames / (ms_our / 1e3),
+                     "speedup": ms_ref / ms_our,
+                     "same_ram": bool(np.array_equal(obs_ref, obs_our))}
+    return out
+
+
+def run_micro_arm(args, fa, carts, rank, world, local_rank):
+    """Instruction-cost micro-carts (carts.micro_cart): one instruction kind
+    per visible line, 151,552 identical instances with all actions 0 (fully
+    converged), K=2, three calls timed with CUDA events on the launching
+    stream.  The cost of one guest instruction of each kind is given in
+    warp-issue slots at 100 % issue: 148 SMs x 4 schedulers x the sampled
+    clock / (guest instructions/s / 32).  The guest instruction count is the
+    kernel's own."""
+    import torch
+    fa.set_device(local_rank)
+    torch.cuda.set_device(local_rank)
+    n, k, calls = 151_552, 2, 3
+    s = torch.cuda.Stream()
+    acts = torch.zeros(k * n, dtype=torch.uint8, device="cuda")
+    kinds = {}
+    with ClockSampler(local_rank) as clk:
+        for kind in carts.MICRO_KINDS:
+            with fa.BatchAtariGpu(carts.micro_cart(kind).rom, n) as g:
+                g.set_launch(args.block, "pc", True)
+                g.reset()
+                g.step_multi_async(acts.data_ptr(), k, 0, s.cuda_stream)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                for _ in range(calls):
+                    g.step_multi_async(acts.data_ptr(), k, 0, s.cuda_stream)
+                e1.record(s)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                g.step_multi_async(acts.data_ptr(), k, 0, s.cuda_stream)
+                g.synchronize()
+                instr = g.last_instructions()
+            kinds[kind] = {"frames_per_s": n * k * calls / (ms / 1e3), "guest_instr_per_frame": instr / (n * k),
+                           "guest_instr_per_s": instr * calls / (ms / 1e3)}
+    clocks = clk.summary()
+    f_sm = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    for v in kinds.values():
+        v["issue_slots_per_guest_instr_at_100pct"] = 148 * 4 * f_sm / (v["guest_instr_per_s"] / 32.0)
+    nop = kinds["nop"]
+    line = {"metric": METRIC, "value": nop["frames_per_s"], "unit": UNIT, "n_gpus": world, "steps": calls,
+            "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8", "data": "synthetic",
+            "config": {"workload": f"instruction-cost micro-carts, {n} identical instances, K={k}; value = the NOP cart",
+                       "l2": "state (34 MB) resident; not flushed", "parallelism": "single GPU"},
+            "clocks": clocks, "gpu_launches": calls * len(kinds),
+            "micro": {kk: {k2: round(v2, 2) for k2, v2 in v.items()} for kk, v in kinds.items()}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """nvidia-smi clock/throttle samples every 200 ms while running."""
@@ -263,32 +391,41 @@ def replica_seed(rank: int, group: int) -> int:
 # ------------------------------------------------------------------ CPU reference
 def cpu_reference(carts, spec, k, seconds_target=15.0):
     """The oracle (a C restatement of the reference's HeadlessAtari) on the
-    host cores: each cart's sample instances run k-frame calls with all
-    threads; instance counts are proportional to the workload's."""
+    host cores.  Each cart is timed on its own, with every host thread busy
+    (4 instances per thread, k-frame calls, an equal share of the time), and
+    the workload's rate combines the per-cart rates with the workload's true
+    instance counts: total instance-frames / sum over carts of (that cart's
+    instance-frames / its rate).  Returns (frames/s, threads, sample text,
+    per-cart frames/s)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
     cores = os.cpu_count() or 1
     for c, _ in spec:
         if c.scheme:
             oracle.set_rom_scheme(c.rom, c.scheme)
-    total = sum(n for _, n in spec)
-    per_cart = [(c, max(1, round(n * 4 * cores / total))) for c, n in spec]
-    states = {c.spec.name: np.array([oracle.reset_state(c.rom)] * m, dtype=oracle.STATE_DTYPE)
-              for c, m in per_cart}
-    frames = 0
-    t0 = time.perf_counter()
-    call = 0
-    while True:
-        for c, m in per_cart:
+    m = 4 * cores
+    share = seconds_target / len(spec)
+    rates, parts = {}, []
+    for c, _ in spec:
+        st = np.array([oracle.reset_state(c.rom)] * m, dtype=oracle.STATE_DTYPE)
+        frames, call = 0, 0
+        t0 = time.perf_counter()
+        while True:
             acts = carts.actions(seed=7, n=m, frames=k, frame0=call * k)
-            oracle.run_batch(c.rom, states[c.spec.name], acts, k, nthreads=cores, pin=False)
+            oracle.run_batch(c.rom, st, acts, k, nthreads=cores, pin=False)
             frames += m * k
-        call += 1
-        if time.perf_counter() - t0 >= seconds_target:
-            break
-    dt = time.perf_counter() - t0
-    sample = ", ".join(f"{m} x {c.spec.name}" for c, m in per_cart)
-    return frames / dt, cores, f"{call} calls of K={k} frames over [{sample}] ({frames} instance-frames, {dt:.1f} s)"
+            call += 1
+            if time.perf_counter() - t0 >= share:
+                break
+        dt = time.perf_counter() - t0
+        rates[c.spec.name] = frames / dt
+        parts.append(f"{c.spec.name}: {frames} instance-frames in {dt:.1f} s")
+    total = sum(n for _, n in spec)
+    value = total / sum(n / rates[c.spec.name] for c, n in spec)
+    weights = ", ".join(f"{n} x {c.spec.name}" for c, n in spec)
+    sample = (f"each cart alone on {cores} threads ({m} instances, K={k} calls): " + "; ".join(parts) +
+              f"; combined with the workload's instance counts [{weights}]")
+    return value, cores, sample, rates
 
 
 def run_reference_arm(args, carts, rank, world):
@@ -315,18 +452,21 @@ def run_reference_arm(args, carts, rank, world):
     # Each step is one bounded CPU sample; warmup steps are run untimed.
     # Each step is a bounded sample sized so the whole run takes about two minutes.
     per_step_s = args.ref_step_seconds or max(0.2, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
-    vals = []
+    vals, per_cart = [], {}
     for i in range(args.warmup + args.steps):
-        fps, cores, sample = cpu_reference(carts, spec, k, seconds_target=per_step_s)
+        fps, cores, sample, rates = cpu_reference(carts, spec, k, seconds_target=per_step_s)
         if i >= args.warmup:
             vals.append(fps)
+            for name, r in rates.items():
+                per_cart.setdefault(name, []).append(r)
     value = statistics.mean(vals)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": {"workload": desc, "parallelism": "one emulator per host thread"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": sample + "; C restatement of the reference HeadlessAtari"},
+                             "sample": sample + "; C restatement of the reference HeadlessAtari",
+                             "per_cart_frames_per_s": {n2: statistics.mean(v) for n2, v in per_cart.items()}},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -517,9 +657,12 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
     if world == 1 and args.workload == "mixed" and not args.no_serve:
         line["serving"] = serve_summary(serve_measure(fa, carts, 8000, 3000, 2000, levels=(0.7,)))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        fps, cores, sample = cpu_reference(carts, spec, k, seconds_target=args.cpu_seconds)
+        fps, cores, sample, rates = cpu_reference(carts, spec, k, seconds_target=args.cpu_seconds)
         line["cpu_baseline"] = {"value": fps, "unit": UNIT, "cores": cores, "kind": "port",
-                                "sample": sample + "; C restatement of the reference HeadlessAtari"}
+                                "sample": sample + "; C restatement of the reference HeadlessAtari",
+                                "per_cart_frames_per_s": rates}
+    if rank == 0 and world == 1 and args.workload == "mixed" and not args.no_ref_kernel:
+        line["ref_kernel"] = ref_kernel_compare(fa, carts)
     if rank == 0:
         print(json.dumps(line), flush=True)
     pool.close()
@@ -684,7 +827,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed",
-                    choices=["mixed", "divergence", "plain", "scale", "converged", "serve", "render", "mappers"])
+                    choices=["mixed", "divergence", "plain", "scale", "converged", "serve", "render", "mappers",
+                             "micro"])
     ap.add_argument("--serve-requests", type=int, default=20000, help="saturation requests of the serve workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     ap.add_argument("--render-instances", type=int, default=RENDER_N, help="consoles of the render workload")
@@ -697,6 +841,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-kernel", action="store_true",
+                    help="skip the timing of the reference's own CUDA kernel (oracle/_ref) in the default line")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=0.0,
                     help="CPU sample per step of the reference arm (0: sized so the run takes about 2 minutes)")
@@ -724,6 +870,8 @@ def main():
             run_serve_arm(args, fa, carts, rank, world, local_rank)
         elif args.workload == "render":
             run_render_arm(args, fa, carts, rank, world, local_rank)
+        elif args.workload == "micro":
+            run_micro_arm(args, fa, carts, rank, world, local_rank)
         else:
             run_gpu_arm(args, fa, carts, rank, world, local_rank)
     finally:

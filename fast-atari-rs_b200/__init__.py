@@ -65,6 +65,8 @@ _SIGS = {
     "fa_version": (ctypes.c_char_p, []),
     "fa_device_count": (_i, []),
     "fa_set_device": (_i, [_i]),
+    "fa_set_wait_limit_ns": (_i, [ctypes.c_uint64]),
+    "fa_wait_limit_ns_get": (ctypes.c_uint64, []),
     "fa_create": (_i, [_u8p, _sz, _sz, ctypes.POINTER(_vp)]),
     "fa_destroy": (None, [_vp]),
     "fa_num_envs": (_sz, [_vp]),
@@ -193,6 +195,16 @@ def device_count() -> int:
 
 def set_device(device: int) -> None:
     _check(lib().fa_set_device(int(device)))
+
+
+def set_wait_limit_ns(ns: int) -> None:
+    """Bound of the device-side ROM staging wait for later launches (0 gives
+    up at once; the call then returns FA_ERR_KERNEL with states untouched)."""
+    _check(lib().fa_set_wait_limit_ns(int(ns)))
+
+
+def wait_limit_ns() -> int:
+    return int(lib().fa_wait_limit_ns_get())
 
 
 SCHEME_NAMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "auto": -1}

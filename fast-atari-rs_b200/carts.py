@@ -904,3 +904,277 @@ def f3_cart(size: int = 16384, seed: int = 7, lines: int = 64) -> Cart:
     rom = b"".join(banks) + img
     assert len(rom) == size
     return Cart(CartSpec(f"3f_{size // 1024}k", size, seed, wsync_density=1.0), rom, labels, scheme="3f")
+
+
+# ------------------------------------------------------- phantom-access carts
+# The reference CPU makes a bus access on every cycle (src/cpu.rs:245-1146),
+# including reads whose value it throws away: the fix-up read of an indexed
+# access at the un-carried address, the read at the next pc of a taken
+# branch, RTS's read of the address it pulled, and the write of the original
+# value in a read-modify-write.  On the Atari bus such an access can switch
+# banks (src/atari.rs:460-492), clear the timer's underflow flag through an
+# INTIM mirror (src/pia.rs:187-190) or shift the TIA's GRP0/GRP1/ENABL
+# shadow registers (src/headless_tia.rs:225-298).  These carts are built to
+# make every one of those accesses matter.  They break the safety rules
+# above on purpose, and stay hang-free a different way: every bank holds the
+# same code at the same addresses (only a bank-id byte at $FE80 differs), so
+# whatever bank a phantom access selects, the next fetch finds the same
+# legal instruction.
+PHANTOM_BANKID = 0xFE80
+
+
+def phantom_cart(rom_size: int = 8192, variant: str = "rts", passes: int = 10) -> Cart:
+    """A 4K Fixed, 8K F8, 16K F6 or 32K F4 cart whose visible lines each
+    exercise phantom bus accesses, with the bank they select and the values
+    they read mixed into RAM:
+
+      * indexed accesses whose fix-up read lands on a hotspot while the real
+        access lands in RAM: STA/LDA/ADC/SBC/CMP abs,X, LDA abs,Y,
+        LDX abs,Y, LDY abs,X, LDA/STA (zp),Y from base $1FFF with an index
+        that carries into $20xx (RAM $F4-$FB);
+      * STA (zp),Y without a carry (the fix-up read is the hotspot itself);
+      * fix-up reads on an INTIM mirror ($0384) just after the timer
+        underflowed, with INSTAT read back (LDA abs,X, LDA (zp),Y, LDY
+        abs,X, LDX abs,Y, STA abs,X), with an index that carries or not;
+      * read-modify-writes on GRP0, GRP1 and ENABL with vertical delay on,
+        on HMOVE, and on hotspots, directly and through a carrying abs,X;
+      * taken branches whose page-crossing fix-up read is a hotspot
+        ($FF00 -> $FExx);
+      * variant "row": a branch at the hotspot row whose next-pc read is the
+        first hotspot (and, not taken, a JMP fetched from the hotspots);
+        variant "rts": a JSR whose last byte is the first hotspot, so RTS's
+        read of the pulled address switches banks;
+      * BRK/RTI, zero-page-indexed reads whose base read reaches RAM or TIA.
+
+    Indices, carries and branch directions come from RAM mixed with the
+    inputs, so instances of one cart diverge.  Frames keep the 3 VSYNC / 36
+    VBLANK skeleton with `passes` passes over the lines."""
+    assert rom_size in (4096, 8192, 16384, 32768) and variant in ("row", "rts")
+    nb = rom_size // 4096
+    hot = _hotspots(nb) if nb > 1 else [0xFFF8]
+    mask = len(hot) - 1
+    lo = [h & 0xFF for h in hot]
+    t_cross = [v + 1 for v in lo]                  # $1FFF + this = $20xx: fix-up read at $1Fxx
+    t_nocross = [v - 0xF0 for v in lo]             # $1FF0 + this = $1Fxx
+    t_intim = [0x85, 0x05]                         # $03FF + this: fix-up at $0384 (INTIM) or $0304
+    a = Asm(0xF000)
+    _reset_code(a)
+    for reg in (0x25, 0x26, 0x27):                 # VDELP0 VDELP1 VDELBL
+        a.ins("LDA", "imm", 1); a.ins("STA", "zp", reg)
+    for ptr, val in ((0xE0, 0x1FFF), (0xE2, 0x1FF0), (0xE4, 0x03FF)):
+        a.ins("LDA", "imm", val & 0xFF); a.ins("STA", "zp", ptr)
+        a.ins("LDA", "imm", val >> 8); a.ins("STA", "zp", ptr + 1)
+    a.ins("LDA", "imm", 0x70); a.ins("STA", "zp", 0x20)          # HMP0
+    a.ins("LDA", "imm", 0x90); a.ins("STA", "zp", 0x24)          # HMBL
+    _frame_head(a, passes)
+    a.label("line")
+
+    def end_line():
+        a.ins("LDA", "abs", PHANTOM_BANKID); a.ins("EOR", "zp", MIX)
+        a.ins("ADC", "zp", LINE_CTR); a.ins("STA", "zp", MIX)
+        a.ins("STA", "zp", WSYNC)
+
+    def index(reg: str, table: str, shift: int, m: int = mask):
+        """reg <- table[(MIX >> shift) & m], through the other index register."""
+        a.ins("LDA", "zp", MIX)
+        for _ in range(shift):
+            a.ins("LSR", "acc")
+        a.ins("AND", "imm", m)
+        if reg == "X":
+            a.ins("TAY"); a.ins("LDX", "absy", table)
+        else:
+            a.ins("TAX"); a.ins("LDY", "absx", table)
+
+    # --- fix-up reads on hotspots, real accesses in RAM $F4-$FB
+    index("X", "t_cross", 0); a.ins("LDA", "zp", MIX); a.ins("STA", "absx", 0x1FFF); end_line()
+    index("X", "t_cross", 1); a.ins("LDA", "absx", 0x1FFF); a.ins("EOR", "zp", MIX); a.ins("STA", "zp", MIX)
+    end_line()
+    index("Y", "t_cross", 2); a.ins("LDA", "absy", 0x1FFF); a.ins("ADC", "zp", 0x82); a.ins("STA", "zp", 0x82)
+    end_line()
+    index("Y", "t_cross", 3); a.ins("LDX", "absy", 0x1FFF); a.ins("STX", "zp", 0x83); end_line()
+    index("X", "t_cross", 4); a.ins("LDY", "absx", 0x1FFF); a.ins("STY", "zp", 0x84); end_line()
+    index("X", "t_cross", 5); a.ins("SEC"); a.ins("SBC", "absx", 0x1FFF); a.ins("STA", "zp", 0x85)
+    a.ins("CMP", "absx", 0x1FFF); a.ins("ROL", "zp", 0x85); end_line()
+    index("Y", "t_cross", 1); a.ins("LDA", "indy", 0xE0); a.ins("EOR", "zp", MIX); a.ins("STA", "zp", MIX)
+    index("Y", "t_cross", 3); a.ins("LDA", "zp", 0x86); a.ins("STA", "indy", 0xE0); end_line()
+    index("Y", "t_nocross", 2); a.ins("LDA", "zp", 0x87); a.ins("STA", "indy", 0xE2); end_line()
+    # --- fix-up reads on an INTIM mirror right after a timer underflow
+    for k, (mn, mode) in enumerate((("LDA", "absx"), ("LDA", "indy"), ("LDY", "absx"), ("LDX", "absy"))):
+        a.ins("LDA", "imm", 0); a.ins("STA", "abs", TIM1T)
+        index("Y" if mode in ("indy", "absy") else "X", "t_intim", k, 1)
+        if mode == "indy":
+            a.ins(mn, "indy", 0xE4)
+        else:
+            a.ins(mn, mode, 0x03FF)
+        a.ins("LDA", "abs", INSTAT); a.ins("EOR", "zp", MIX); a.ins("STA", "zp", MIX)
+        if k % 2:
+            end_line()
+    a.ins("LDA", "imm", 0); a.ins("STA", "abs", TIM1T)
+    a.ins("LDX", "imm", 4); a.ins("LDA", "zp", 0x88); a.ins("STA", "absx", 0x0380)   # always a fix-up read
+    a.ins("LDA", "abs", INSTAT); a.ins("ADC", "zp", 0x88); a.ins("STA", "zp", 0x88); end_line()
+    # --- read-modify-writes: GRP0/GRP1/ENABL under VDEL, HMOVE, hotspots
+    a.ins("LDA", "zp", MIX); a.ins("STA", "zp", 0x1B)
+    a.ins("INC", "zp", 0x1B); a.ins("ASL", "zp", 0x1C); a.ins("LDX", "imm", 0)
+    a.ins("ROL", "zpx", 0x1B); a.ins("DEC", "zp", 0x1F); a.ins("LSR", "abs", 0x011C)
+    a.ins("LDX", "imm", 1); a.ins("INC", "zpx", 0x1A); a.ins("INC", "zp", 0x2A); end_line()
+    a.ins("INC", "abs", hot[-1])
+    index("X", "t_cross", 2); a.ins("INC", "absx", 0x1FFF)
+    index("X", "t_cross", 6); a.ins("ASL", "absx", 0x1FFF); end_line()
+    # --- a taken branch whose page-crossing fix-up read is a hotspot
+    a.ins("LDA", "zp", MIX); a.ins("LSR", "acc"); a.ins("JMP", "abs", 0xFF00)
+    a.label("br_ret")
+    end_line()
+    # --- the hotspot row (variant) and BRK/RTI
+    a.ins("LDA", "zp", MIX); a.ins("AND", "imm", 2)
+    a.ins("JMP", "abs", hot[0] - 2)
+    a.label("row_ret")
+    a.ins("LDA", "zp", MIX); a.ins("BRK"); a.raw(b"\xEA")
+    end_line()
+    # --- zero-page-indexed reads: the base read reaches RAM or the TIA
+    a.ins("LDX", "zp", MIX); a.ins("LDA", "zpx", 0x80); a.ins("STA", "zp", 0x8A)
+    a.ins("LDX", "imm", 0x0C); a.ins("LDA", "indx", 0x00); a.ins("EOR", "zp", 0x8A); a.ins("STA", "zp", 0x8A)
+    end_line()
+    _frame_tail(a)
+    # --- tables and the bank id
+    a.org(0xFE00)
+    a.label("t_cross"); a.raw(bytes((t_cross * 8)[:8]))
+    a.label("t_nocross"); a.raw(bytes((t_nocross * 8)[:8]))
+    a.label("t_intim"); a.raw(bytes(t_intim))
+    a.org(PHANTOM_BANKID)
+    a.raw(b"\x00")
+    # branch targets at $FExx (xx a hotspot's low byte): the fix-up read of
+    # a taken branch from page $FF lands on $FFxx
+    sites = [(0xFF00, "BCS", lo[0])]
+    if lo[-1] - lo[0] >= 3:
+        sites.append((0xFF10, "BCC", lo[-1]))
+    for _, _, t in sorted(sites, key=lambda s: s[2]):
+        a.org(0xFE00 | t)
+        a.ins("JMP", "abs", "br_ret")
+    for site, mn, t in sites:
+        a.org(site)
+        a.ins(mn, "rel", 0xFE00 | t)
+        if site == 0xFF00 and len(sites) > 1:
+            a.ins("JMP", "abs", 0xFF10)                             # not taken: try the other site
+        else:
+            a.ins("JMP", "abs", "br_ret")
+    a.org(0xFF40)
+    a.label("sub")
+    a.ins("INC", "zp", 0x89); a.ins("RTS")
+    a.org(0xFF60)
+    a.label("brk")
+    a.ins("PHA"); a.ins("LDA", "zp", 0x89); a.ins("ADC", "imm", 3); a.ins("STA", "zp", 0x89); a.ins("PLA")
+    a.ins("RTI")
+    a.org(0xFF80)
+    a.label("row_far")
+    a.ins("JMP", "abs", "row_ret")
+    a.org(hot[0] - 2)
+    if variant == "row":
+        a.ins("BNE", "rel", "row_far")          # taken: next-pc read at hot[0]
+        a.ins("JMP", "abs", "row_ret")          # not taken: fetched from the hotspots
+    else:
+        a.ins("JSR", "abs", "sub")              # its last byte is hot[0]; RTS reads it
+        a.ins("JMP", "abs", "row_ret")
+    a.org(0xFFFC)
+    a.raw(bytes([0x00, 0xF0]))
+    img, labels, _ = a.assemble(4096)
+    img = bytearray(img)
+    img[0xFFE:0x1000] = bytes([labels["brk"] & 0xFF, labels["brk"] >> 8])
+    banks = []
+    for b in range(nb):
+        bank = bytearray(img)
+        bank[PHANTOM_BANKID - 0xF000] = 0x30 + 0x11 * b
+        banks.append(bytes(bank))
+    name = f"phantom_{rom_size // 1024}k_{variant}"
+    return Cart(CartSpec(name, rom_size, 0, wsync_density=1.0), b"".join(banks), labels)
+
+
+def phantom_carts() -> List[Cart]:
+    """Every phantom-access cart: 4K Fixed, and F8, F6 and F4 in both variants."""
+    out = [phantom_cart(4096, "rts")]
+    for size in (8192, 16384, 32768):
+        out += [phantom_cart(size, "row"), phantom_cart(size, "rts")]
+    return out
+
+
+# ------------------------------------------------------------- failure carts
+def stall_cart(kind: str) -> Cart:
+    """A 4K Fixed cart for the frame loop's limits (src/atari.rs:584-598):
+
+      * "no_vsync": never writes VSYNC, so every frame runs to the
+        reference's 100,000-cycle cap (FA_STATUS_CYCLE_CAP, informational);
+      * "vsync_held": raises VSYNC once and never lowers it, so the frame
+        after the reset frame waits for VSYNC to drop forever (the reference
+        loops; this library halts the instance with FA_STATUS_VSYNC_BUDGET
+        after 2,000,000 cycles).
+
+    Both loops read the inputs and the timer into RAM and end lines with
+    STA WSYNC, so the state keeps changing while they run."""
+    assert kind in ("no_vsync", "vsync_held")
+    a = Asm(0xF000)
+    _reset_code(a)
+    a.ins("LDA", "imm", 43); a.ins("STA", "abs", TIM64T)
+    if kind == "vsync_held":
+        a.ins("LDA", "imm", 2); a.ins("STA", "zp", VSYNC)
+    a.label("loop")
+    a.ins("LDA", "abs", SWCHA); a.ins("EOR", "zp", MIX); a.ins("ADC", "abs", INTIM); a.ins("STA", "zp", MIX)
+    a.ins("INC", "zp", LINE_CTR)
+    a.ins("BNE", "rel", "skip")
+    a.ins("LDA", "imm", 43); a.ins("STA", "abs", TIM64T)
+    a.label("skip")
+    a.ins("LDA", "zp", LINE_CTR); a.ins("AND", "imm", 0x7F); a.ins("TAX")
+    a.ins("LDA", "zp", MIX); a.ins("STA", "zpx", 0x80)                 # RAM $80-$FF
+    a.ins("STA", "zp", WSYNC)
+    a.ins("JMP", "abs", "loop")
+    a.org(0xFFFC)
+    a.raw(bytes([0x00, 0xF0, 0x00, 0xF0]))
+    img, labels, _ = a.assemble(4096)
+    return Cart(CartSpec(f"stall_{kind}", 4096, 0, wsync_density=1.0), img, labels)
+
+
+# ------------------------------------------------------- instruction-cost carts
+MICRO_KINDS = {
+    "nop": [("NOP", "imp", None)],
+    "lda_imm": [("LDA", "imm", 0x12)],
+    "lda_zp": [("LDA", "zp", 0x85)],
+    "sta_zp": [("STA", "zp", 0x86)],
+    "adc_zp": [("ADC", "zp", 0x87)],
+    "inc_zp": [("INC", "zp", 0x88)],
+    "lda_absx": [("LDA", "absx", 0x0090)],
+    "lda_rom": [("LDA", "abs", 0xF800)],
+    "lda_indy": [("LDA", "indy", 0x90)],
+    "sta_tia": [("STA", "zp", 0x09)],
+    "lda_intim": [("LDA", "abs", 0x284)],
+    "tax_inx": [("TAX", "imp", None), ("INX", "imp", None)],
+}
+
+
+def micro_cart(kind: str, reps: int = 24) -> Cart:
+    """A 4K Fixed cart whose 192 visible lines each run `reps` copies of one
+    instruction kind (MICRO_KINDS) and STA WSYNC, inside the frame skeleton
+    (3 VSYNC, 37 VBLANK, 192 visible, 30 overscan lines).  Run converged
+    (identical instances and actions), it gives the cost of one guest
+    instruction of that kind."""
+    a = Asm()
+    a.label("reset"); a.ins("SEI"); a.ins("CLD"); a.ins("LDX", "imm", 0xFF); a.ins("TXS")
+    a.ins("LDA", "imm", 0); a.ins("LDX", "imm", 0x80)
+    a.label("clr"); a.ins("STA", "zpx", 0); a.ins("INX"); a.ins("BNE", "rel", "clr")
+    a.label("frame")
+    a.ins("LDA", "imm", 2); a.ins("STA", "zp", VSYNC)
+    for _ in range(3):
+        a.ins("STA", "zp", WSYNC)
+    a.ins("LDA", "imm", 0); a.ins("STA", "zp", VSYNC)
+    _wsync_lines(a, 37, "vb")
+    a.ins("LDA", "imm", 192); a.ins("STA", "zp", LINE_CTR)
+    a.ins("LDX", "imm", 0); a.ins("LDY", "imm", 0)
+    a.label("line")
+    for _ in range(reps):
+        for mn, mode, arg in MICRO_KINDS[kind]:
+            a.ins(mn, mode, arg)
+    a.ins("STA", "zp", WSYNC); a.ins("DEC", "zp", LINE_CTR); a.ins("BEQ", "rel", "ov"); a.ins("JMP", "abs", "line")
+    a.label("ov")
+    _wsync_lines(a, 30, "os")
+    a.ins("JMP", "abs", "frame")
+    a.org(0xFFFC)
+    a.raw(bytes([0x00, 0xF0, 0x00, 0xF0]))
+    img, labels, _ = a.assemble(4096)
+    return Cart(CartSpec(f"micro_{kind}", 4096, 0, wsync_density=1.0), img, labels)

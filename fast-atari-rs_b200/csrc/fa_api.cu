@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -36,6 +37,21 @@ int fa_fail(int code, const char* fmt, ...)
 
 extern "C" const char* fa_last_error(void) { return g_err.c_str(); }
 extern "C" const char* fa_version(void) { return "fast-atari-b200 0.1 (sm_100a)"; }
+
+namespace {
+std::atomic<uint64_t> g_wait_ns{2000000000ull};
+}
+
+uint64_t fa_wait_limit_ns() { return g_wait_ns.load(std::memory_order_relaxed); }
+
+extern "C" int fa_set_wait_limit_ns(uint64_t ns)
+{
+    if (ns > 10000000000ull) return fa_fail(FA_ERR_INVALID, "wait limit %llu ns is above 10 s", (unsigned long long)ns);
+    g_wait_ns.store(ns, std::memory_order_relaxed);
+    return FA_OK;
+}
+
+extern "C" uint64_t fa_wait_limit_ns_get(void) { return fa_wait_limit_ns(); }
 
 extern "C" int fa_device_count(void)
 {

@@ -55,7 +55,12 @@ struct FaLaunch {
     uint32_t* err;               // device error word
     unsigned long long* instr;   // guest-instruction counter, or null
     unsigned long long* rounds;  // scheduler rounds x 32 (lane slots offered), or null
+    uint64_t wait_ns;            // bound of the ROM staging wait (set by fa_launch_run)
 };
+
+// The bound in nanoseconds that launches give their ROM staging wait
+// (fa_set_wait_limit_ns; 2 s by default).
+uint64_t fa_wait_limit_ns();
 
 // ------------------------------------------------------------------ serving form
 // Instance state of the server lives in blocks of FA_SERVE_BLOCK_COLS columns
@@ -96,6 +101,7 @@ struct FaServeLaunch {
     uint32_t* err;
     unsigned long long* instr;
     unsigned long long* rounds;
+    uint64_t wait_ns;            // bound of the ROM staging wait (set by fa_launch_serve)
 };
 
 // Launch fa_serve with CTAs of block / 32 warps (block 128, 256 or 512), one

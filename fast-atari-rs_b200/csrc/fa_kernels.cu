@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(BLOCK) fa_run(const __grid_constant__ FaLaunch
         while (g + 1 < (int)L.ngroups && u >= L.g[g + 1].unit_begin) g++;
         const FaGroup& G = L.g[g];
         if (G.rom != (staged < 0 ? nullptr : L.g[staged].rom)) {
-            if (!stage_rom(rom_s, G.rom, G.nbanks * 4096u, &bar, phase)) {
+            if (!stage_rom(rom_s, G.rom, G.nbanks * 4096u, &bar, phase, L.wait_ns)) {
                 if (threadIdx.x == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
                 break;
             }
@@ -85,14 +85,9 @@ __global__ void __launch_bounds__(WARPS * 32) fa_run_warps(const __grid_constant
                 bulk_g2s(smem + L.g[g].rom_off + off, L.g[g].rom + off, 4096u, &bar);
         }
     }
-    bool ok = false;
-    const uint64_t t0 = globaltimer_ns();
-    while (true) {
-        if (mbar_try_wait(&bar, 0)) { ok = true; break; }
-        if (globaltimer_ns() - t0 > FA_WAIT_LIMIT_NS) break;
-    }
-    if (!ok) {
+    if (!mbar_wait_bounded(&bar, 0, L.wait_ns)) {
         if (threadIdx.x == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
+        mbar_drain(&bar, 0);
         return;
     }
     for (uint32_t round = 0;; round++) {
@@ -273,6 +268,7 @@ static void plan_units(FaLaunch& L, uint32_t unit)
 cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int sms, cudaStream_t s)
 {
     FaLaunch L = L_in;
+    L.wait_ns = fa_wait_limit_ns();
     const int maps = fa_maps_of(L.g, L.ngroups);                       // which cores the carts need
     const uint32_t lib = plan_romlib(L);
     L.romlib_bytes = lib;

@@ -95,9 +95,11 @@ extern "C" int fa_step_static(const uint8_t* d_rom_image, int scheme, uint32_t* 
         L.queue = scratch + 8 + c;
         FA_CUDA(fa_launch_run(L, 128, true, sms, s));
     }
-    FA_CUDA(cudaStreamSynchronize(s));
+    // The error word comes back on the caller's stream: only that stream is
+    // waited for, not every blocking stream of the device.
     uint32_t err = 0;
-    FA_CUDA(cudaMemcpy(&err, scratch, sizeof(err), cudaMemcpyDeviceToHost));
+    FA_CUDA(cudaMemcpyAsync(&err, scratch, sizeof(err), cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
     if (err) return fa_fail(FA_ERR_KERNEL, "device wait gave up (error word 0x%x)", err);
     return FA_OK;
 }

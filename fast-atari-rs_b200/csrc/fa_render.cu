@@ -48,6 +48,7 @@ struct FaRenderLaunch {
     uint32_t* err;
     unsigned long long* instr;
     unsigned long long* rounds;
+    uint64_t wait_ns;            // bound of the ROM staging wait (set by launch_render)
 };
 
 namespace fa {
@@ -60,11 +61,14 @@ struct RRunner {
     uint32_t f, phase, fcyc;
     bool active;
 
+    // set_action, then run_frame, which does nothing for a halted console
+    // (src/atari.rs:250-270, 284-306): a halted console's inputs still take
+    // the frame's action.
     __device__ __forceinline__ bool begin_frame()
     {
         const FaGroup* G = e.G;
-        if (e.row(R_STATUS) & FA_STATUS_HALT_MASK) return false;
         if (G->actions) e.apply_action(G->actions[(size_t)f * G->act_stride + e.i]);
+        if (e.row(R_STATUS) & FA_STATUS_HALT_MASK) return false;
         e.tw &= ~TW_FCOMP;
         e.bank &= 7u;
         fcyc = 0;
@@ -170,7 +174,7 @@ __global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLa
     }
     __syncthreads();
     uint32_t phase = 0;
-    if (!stage_rom(smem, L.rom, rom_bytes, &bar, phase)) {
+    if (!stage_rom(smem, L.rom, rom_bytes, &bar, phase, L.wait_ns)) {
         if (threadIdx.x == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
         return;
     }
@@ -225,6 +229,10 @@ __global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLa
     if (valid) {
         e.fb_flush();
         e.fold_cycles();
+        // A console that halted before the call's last frame took the later
+        // frames' set_action too; the last one is what its inputs hold.
+        if (L.actions && r.f + 1u < L.k && (e.row(R_STATUS) & FA_STATUS_HALT_MASK))
+            e.apply_action(L.actions[(size_t)(L.k - 1u) * L.n + i]);
         uint32_t* w = slab + lane;
 #pragma unroll 4
         for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) col[(size_t)k * S] = w[k * 32u];
@@ -309,7 +317,9 @@ cudaError_t launch_render(const FaRenderLaunch& L, cudaStream_t s)
     const uint32_t units = (L.n + 31u) / 32u;
     const uint32_t grid = (units + WARPS - 1u) / WARPS;
     if (grid == 0) return cudaSuccess;
-    fa::fa_render_run<WARPS, SLICED><<<grid, WARPS * 32, smem, s>>>(L);
+    FaRenderLaunch Lw = L;
+    Lw.wait_ns = fa_wait_limit_ns();
+    fa::fa_render_run<WARPS, SLICED><<<grid, WARPS * 32, smem, s>>>(Lw);
     return cudaGetLastError();
 }
 

@@ -13,6 +13,8 @@
 namespace fa {
 
 // ------------------------------------------------------------------ TMA / mbarrier
+// Default bound of every device wait (fa_set_wait_limit_ns changes the
+// bound of the ROM staging wait of later launches).
 constexpr uint64_t FA_WAIT_LIMIT_NS = 2000000000ull;   // 2 s
 
 __device__ __forceinline__ uint64_t globaltimer_ns()
@@ -61,24 +63,38 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
+// Waits for phase `parity` of the barrier for at most limit_ns nanoseconds
+// (a limit of 0 gives up without waiting).  Bounded in time, not in
+// iterations: one try_wait may suspend for an implementation-defined interval.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns)
+{
+    const uint64_t t0 = globaltimer_ns();
+    while (globaltimer_ns() - t0 < limit_ns)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// After a wait that gave up: the copies already issued still land in this
+// CTA's shared memory, so the CTA waits for them (bounded by the default
+// limit) before it reuses that memory or exits.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity)
+{
+    (void)mbar_wait_bounded(bar, parity, FA_WAIT_LIMIT_NS);
+}
+
 // Stage `bytes` (a multiple of 4 KiB) of ROM into shared memory.  Called by
 // every thread of the CTA after a __syncthreads; returns false if the copy
-// did not complete within the wait bound.
-static __device__ bool stage_rom(uint8_t* dst, const uint8_t* src, uint32_t bytes, uint64_t* bar, uint32_t& phase)
+// did not complete within limit_ns (the launch's wait bound).
+static __device__ bool stage_rom(uint8_t* dst, const uint8_t* src, uint32_t bytes, uint64_t* bar, uint32_t& phase,
+                                 uint64_t limit_ns)
 {
     if (threadIdx.x == 0) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect_tx(bar, bytes);
         for (uint32_t off = 0; off < bytes; off += 4096u) bulk_g2s(dst + off, src + off, 4096u, bar);
     }
-    // Bounded in time, not in iterations: one try_wait may suspend for an
-    // implementation-defined interval.
-    bool ok = false;
-    const uint64_t t0 = globaltimer_ns();
-    while (true) {
-        if (mbar_try_wait(bar, phase)) { ok = true; break; }
-        if (globaltimer_ns() - t0 > FA_WAIT_LIMIT_NS) break;
-    }
+    const bool ok = mbar_wait_bounded(bar, phase, limit_ns);
+    if (!ok) mbar_drain(bar, phase);
     phase ^= 1u;
     return ok;
 }
@@ -90,42 +106,42 @@ struct Runner {
     uint32_t f, phase, fcyc;
     bool active;
 
-    // Start frame f: periodic reset, action, frame_complete cleared
-    // (src/atari.rs:571-586).  False if the instance is halted.
+    // Start frame f in the order of one frame of a batched step: the
+    // periodic reset, set_action (src/atari.rs:571-582), then run_frame
+    // (:584-586), which does nothing for a halted instance.  False if the
+    // instance is halted: its inputs still take the frame's action.
     __device__ __forceinline__ bool begin_frame()
     {
         const FaGroup* G = e.G;
-        if (e.row(R_STATUS) & FA_STATUS_HALT_MASK) return false;
         if (G->episode_frames && G->snapshot && e.row(R_FRAME) >= G->episode_frames) {
             e.load_ram(G->snapshot, 1);
             for (uint32_t w = FA_SMEM_WORDS; w < FA_ROWS; w++) e.row(w) = G->snapshot[w];
             e.load_hot(G->snapshot, 1);
         }
         if (G->actions) e.apply_action(G->actions[(size_t)f * G->act_stride + e.i]);
+        if (e.row(R_STATUS) & FA_STATUS_HALT_MASK) return false;
         e.tw &= ~TW_FCOMP;
         fcyc = 0;
         e.bank &= 7u;
         phase = e.vsync_on() ? 0u : 1u;
+        e.flim = frame_limit();
         return true;
     }
 
-    // One HeadlessAtari::run_one_cycle (src/atari.rs:601-614) plus the frame
-    // loop checks of run_frame (src/atari.rs:584-598).  Returns true when the
-    // lane should run again immediately (a WSYNC skip is pending).
-    __device__ __forceinline__ bool one()
+    // The frame's cycle count at which the checks of run_frame can first
+    // change anything without a VSYNC write: past the VSYNC budget while
+    // VSYNC is held (phase 0), past the reference's 100,000-cycle cap after it.
+    __device__ __forceinline__ uint32_t frame_limit() const
     {
-        uint32_t n;
-        if (e.wsync()) {
-            n = e.tia_skip();
-        } else {
-            n = e.step();
-            if (n == 0) { e.fold_cycles(); e.set_status(FA_STATUS_ILLEGAL_OPCODE); active = false; return false; }
-            e.instr++;
-            e.cyc_acc += n;
-            e.tia_tick(n);
-        }
-        e.pia_tick(n);
-        fcyc += n;
+        return phase == 0u ? FA_VSYNC_BUDGET + 1u : FA_FRAME_CYCLE_CAP + 1u;
+    }
+
+    // The loop conditions of run_frame (src/atari.rs:584-598) after one
+    // run_one_cycle: VSYNC only changes on a write to it, and the limits only
+    // when the cycle count reaches them, so this runs after a VSYNC write or
+    // at a limit (e.flim), never per instruction.
+    __device__ __forceinline__ bool frame_event()
+    {
         if (phase == 0u) {
             if (fcyc > FA_VSYNC_BUDGET) {
                 e.fold_cycles();
@@ -145,6 +161,29 @@ struct Runner {
                 return false;
             }
         }
+        e.flim = frame_limit();
+        return e.wsync();
+    }
+
+    // One HeadlessAtari::run_one_cycle (src/atari.rs:601-614) plus the frame
+    // loop checks of run_frame.  Returns true when the lane should run again
+    // immediately (a WSYNC skip is pending).
+    __device__ __forceinline__ bool one()
+    {
+        uint32_t n;
+        if (e.wsync()) {
+            n = e.tia_skip();
+            e.pia_tick_general(n);
+        } else {
+            n = e.step();
+            if (n == 0) { e.fold_cycles(); e.set_status(FA_STATUS_ILLEGAL_OPCODE); active = false; return false; }
+            e.instr++;
+            e.cyc_acc += n;
+            e.tia_tick(n);
+            e.pia_tick(n);
+        }
+        fcyc += n;
+        if (fcyc >= e.flim) return frame_event();
         return e.wsync();
     }
 
@@ -267,6 +306,7 @@ __device__ __forceinline__ void run_unit_as(const FaGroup& G, uint32_t first, ui
     r.e.hot_lo = G.hot_lo;
     r.e.nbanks = G.nbanks;
     r.e.instr = 0;
+    r.e.flim = 0;
     r.e.cyc_acc = 0;
     r.e.pc = 0;
     r.e.bank = 0;
@@ -282,6 +322,10 @@ __device__ __forceinline__ void run_unit_as(const FaGroup& G, uint32_t first, ui
     const uint32_t rounds = run_lanes(r, G.sched);
     if (valid) {
         r.e.fold_cycles();
+        // An instance that halted before the call's last frame still took
+        // the later frames' set_action; the last one is what its inputs hold.
+        if (G.actions && r.f + 1u < G.k && (r.e.row(R_STATUS) & FA_STATUS_HALT_MASK))
+            r.e.apply_action(G.actions[(size_t)(G.k - 1u) * G.act_stride + r.e.i]);
         r.e.store_ram(col, G.stride);
         r.e.store_hot(col, G.stride);
         if (G.obs) {

@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) fa_serve(const __grid_
     }
     __syncthreads();
     uint32_t phase = 0;
-    const bool staged = stage_rom(smem, L.rom, rom_bytes, &bar, phase);
+    const bool staged = stage_rom(smem, L.rom, rom_bytes, &bar, phase, L.wait_ns);
     if (!have) return;
     if (staged) run_unit<32, MAPS>(sg[warp], 0, s_count[warp], smem, priv, lane, L.instr, L.rounds);
     else if (lane == 0) atomicOr(L.err, FA_DEVERR_TMA_TIMEOUT);
@@ -121,7 +121,9 @@ cudaError_t launch_serve(const FaServeLaunch& L, cudaStream_t s)
     }
     if (L.nunits == 0) return cudaSuccess;
     const size_t smem = (size_t)L.nbanks * 4096u + (size_t)WARPS * FA_SMEM_WORDS * 32u * 4u;
-    fa::fa_serve<WARPS, SL><<<(L.nunits + WARPS - 1) / WARPS, WARPS * 32, smem, s>>>(L);
+    FaServeLaunch Lw = L;
+    Lw.wait_ns = fa_wait_limit_ns();
+    fa::fa_serve<WARPS, SL><<<(L.nunits + WARPS - 1) / WARPS, WARPS * 32, smem, s>>>(Lw);
     return cudaGetLastError();
 }
 }  // namespace

@@ -149,6 +149,17 @@ int fa_device_count(void);
  * current device does not carry over). */
 int fa_set_device(int device);
 
+/* Bound, in nanoseconds, of the device-side wait for the ROM images that a
+ * launch stages into shared memory (2,000,000,000 = 2 s by default;
+ * 0..10,000,000,000 accepted, process-wide, for launches enqueued after the
+ * call).  A wait that gives up leaves every instance of its CTA untouched,
+ * sets bit 0x1 of the launch's device error word, and the call returns
+ * FA_ERR_KERNEL (fa_last_error names the word).  0 gives up at once, which lets a test exercise that
+ * path without a fault.  No counterpart in the reference, which has no
+ * device-side waits. */
+int fa_set_wait_limit_ns(uint64_t ns);
+uint64_t fa_wait_limit_ns_get(void);
+
 /*
  * ROM schemes.  No counterpart in the reference, which picks a scheme from
  * the ROM length alone (src/atari.rs:96-105).  fa_rom_set_scheme records,
@@ -567,7 +578,10 @@ unsigned long long fa_render_last_instructions(const fa_render* r);
  *   d_rom_image  nbanks * 4096 bytes, 16-byte aligned (Fixed carts as their
  *                mirrored 4 KiB window, banked carts as-is)
  *   scheme       FA_SCHEME_FIXED, _F8, _F6 or _F4 (E0 and 3F are not taken here)
- *   d_state      the FA SoA state rows (fa_device_state layout), stride >= n
+ *   d_state      the FA SoA state rows (fa_device_state layout), stride >= n,
+ *                of instances created for the same scheme (rows of another
+ *                scheme keep bank numbers this one does not have, and step
+ *                wrongly)
  *   d_actions    calls * k * n bytes; call c uses the slice at c * k * n
  *   d_obs        n * 128 bytes (16-byte aligned) or NULL; gets each call's RAM
  * The kernel's scratch (one work-queue counter per call, error word,
@@ -576,7 +590,10 @@ unsigned long long fa_render_last_instructions(const fa_render* r);
  * first call on a device looks up that array's device address, so make it
  * before any stream capture.  Every call shares the array: calls that overlap
  * on the GPU (other streams, other threads) race and must not be issued.
- * Blocks until the steps finish and reports device-side errors.
+ * No periodic episode reset is applied here (a handle's
+ * fa_set_episode_frames does not carry over to its rows).  Each call waits
+ * on the host until its steps on `stream` finish (it synchronises that
+ * stream only) and reports device-side errors.
  */
 int fa_step_static(const uint8_t* d_rom_image, int scheme, uint32_t* d_state, uint32_t stride,
                    uint32_t n, const uint8_t* d_actions, int k, int calls, uint8_t* d_obs,

@@ -10,6 +10,8 @@
  *   MEM_T           memory type
  *   MREAD(m, a)     one bus read  (uint16_t a) -> uint8_t
  *   MWRITE(m, a, v) one bus write
+ *   PHANTOM_READ(m, a)      a read whose value the reference discards
+ *   RMW_OLD_WRITE(m, a, v)  read-modify-write's write of the original value
  * The bus operations are issued in exactly the order of the reference,
  * including every phantom read and the read-modify-write double write,
  * because phantom accesses have side effects on the Atari bus (bank
@@ -29,12 +31,12 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
     switch (op) {
     /* NOP (cpu.rs:257-261) */
     case 0xEA:
-        (void)MREAD(m, c->pc); cyc++;
+        PHANTOM_READ(m, c->pc); cyc++;
         break;
 
     /* flag ops (cpu.rs:266-280) */
     case 0x18: case 0x38: case 0x58: case 0x78: case 0xB8: case 0xD8: case 0xF8:
-        (void)MREAD(m, c->pc); cyc++;
+        PHANTOM_READ(m, c->pc); cyc++;
         switch (op) {
         case 0x18: orc_setf(c, F_C, 0); break;
         case 0x38: orc_setf(c, F_C, 1); break;
@@ -48,7 +50,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
 
     /* register transfers (cpu.rs:285-298) */
     case 0xAA: case 0xA8: case 0x8A: case 0x98: case 0xBA: case 0x9A:
-        (void)MREAD(m, c->pc); cyc++;
+        PHANTOM_READ(m, c->pc); cyc++;
         switch (op) {
         case 0xAA: c->x = c->a; orc_zn(c, c->x); break;
         case 0xA8: c->y = c->a; orc_zn(c, c->y); break;
@@ -61,7 +63,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
 
     /* INX/INY/DEX/DEY (cpu.rs:303-314) */
     case 0xE8: case 0xC8: case 0xCA: case 0x88:
-        (void)MREAD(m, c->pc); cyc++;
+        PHANTOM_READ(m, c->pc); cyc++;
         switch (op) {
         case 0xE8: c->x++; orc_zn(c, c->x); break;
         case 0xC8: c->y++; orc_zn(c, c->y); break;
@@ -72,7 +74,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
 
     /* shifts on A (cpu.rs:319-330) */
     case 0x0A: case 0x4A: case 0x2A: case 0x6A:
-        (void)MREAD(m, c->pc); cyc++;
+        PHANTOM_READ(m, c->pc); cyc++;
         switch (op) {
         case 0x0A: c->a = orc_asl(c, c->a); break;
         case 0x4A: c->a = orc_lsr(c, c->a); break;
@@ -108,7 +110,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
     /* zp,X read (cpu.rs:415-438) */
     case 0xB5: case 0xB4: case 0x75: case 0x35: case 0xD5: case 0x55: case 0x15: case 0xF5: {
         uint8_t base = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
-        (void)MREAD(m, base); cyc++;
+        PHANTOM_READ(m, base); cyc++;
         uint8_t v = MREAD(m, (uint8_t)(base + c->x)); cyc++;
         orc_read_op(c, op, v);
         break;
@@ -117,7 +119,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
     /* zp,X write (cpu.rs:443-460) */
     case 0x95: case 0x94: {
         uint8_t base = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
-        (void)MREAD(m, base); cyc++;
+        PHANTOM_READ(m, base); cyc++;
         MWRITE(m, (uint8_t)(base + c->x), orc_store_val(c, op)); cyc++;
         break;
     }
@@ -125,7 +127,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
     /* zp,Y read: LDX (cpu.rs:465-479) */
     case 0xB6: {
         uint8_t base = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
-        (void)MREAD(m, base); cyc++;
+        PHANTOM_READ(m, base); cyc++;
         uint8_t v = MREAD(m, (uint8_t)(base + c->y)); cyc++;
         c->x = v; orc_zn(c, c->x);
         break;
@@ -134,7 +136,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
     /* zp,Y write: STX (cpu.rs:484-493) */
     case 0x96: {
         uint8_t base = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
-        (void)MREAD(m, base); cyc++;
+        PHANTOM_READ(m, base); cyc++;
         MWRITE(m, (uint8_t)(base + c->y), c->x); cyc++;
         break;
     }
@@ -143,7 +145,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
     case 0x06: case 0x46: case 0x26: case 0x66: case 0xE6: case 0xC6: {
         uint16_t ad = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
         uint8_t v = MREAD(m, ad); cyc++;
-        MWRITE(m, ad, v); cyc++;
+        RMW_OLD_WRITE(m, ad, v); cyc++;
         MWRITE(m, ad, orc_rmw(c, op, v)); cyc++;
         break;
     }
@@ -151,10 +153,10 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
     /* zp,X RMW (cpu.rs:526-553) */
     case 0x16: case 0x56: case 0x36: case 0x76: case 0xF6: case 0xD6: {
         uint8_t base = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
-        (void)MREAD(m, base); cyc++;
+        PHANTOM_READ(m, base); cyc++;
         uint16_t ad = (uint8_t)(base + c->x);
         uint8_t v = MREAD(m, ad); cyc++;
-        MWRITE(m, ad, v); cyc++;
+        RMW_OLD_WRITE(m, ad, v); cyc++;
         MWRITE(m, ad, orc_rmw(c, op, v)); cyc++;
         break;
     }
@@ -183,7 +185,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
         uint16_t hi = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
         uint16_t ad = (uint16_t)((hi << 8) | lo);
         uint8_t v = MREAD(m, ad); cyc++;
-        MWRITE(m, ad, v); cyc++;
+        RMW_OLD_WRITE(m, ad, v); cyc++;
         MWRITE(m, ad, orc_rmw(c, op, v)); cyc++;
         break;
     }
@@ -197,7 +199,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
         uint8_t idx = ((op & 0x1C) == 0x1C && op != 0xBE) ? c->x : c->y;
         uint16_t eff = (uint16_t)(base + idx);
         if ((base & 0xFF00) != (eff & 0xFF00)) {
-            (void)MREAD(m, (uint16_t)((base & 0xFF00) | (eff & 0x00FF))); cyc++;
+            PHANTOM_READ(m, (uint16_t)((base & 0xFF00) | (eff & 0x00FF))); cyc++;
         }
         uint8_t v = MREAD(m, eff); cyc++;
         if (op == 0xBE) { c->x = v; orc_zn(c, c->x); }
@@ -211,7 +213,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
         uint16_t hi = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
         uint16_t base = (uint16_t)((hi << 8) | lo);
         uint16_t eff = (uint16_t)(base + (op == 0x9D ? c->x : c->y));
-        (void)MREAD(m, (uint16_t)((base & 0xFF00) | (eff & 0x00FF))); cyc++;
+        PHANTOM_READ(m, (uint16_t)((base & 0xFF00) | (eff & 0x00FF))); cyc++;
         MWRITE(m, eff, c->a); cyc++;
         break;
     }
@@ -222,9 +224,9 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
         uint16_t hi = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
         uint16_t base = (uint16_t)((hi << 8) | lo);
         uint16_t eff = (uint16_t)(base + c->x);
-        (void)MREAD(m, (uint16_t)((base & 0xFF00) | (eff & 0x00FF))); cyc++;
+        PHANTOM_READ(m, (uint16_t)((base & 0xFF00) | (eff & 0x00FF))); cyc++;
         uint8_t v = MREAD(m, eff); cyc++;
-        MWRITE(m, eff, v); cyc++;
+        RMW_OLD_WRITE(m, eff, v); cyc++;
         MWRITE(m, eff, orc_rmw(c, op, v)); cyc++;
         break;
     }
@@ -232,7 +234,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
     /* (zp,X) read (cpu.rs:793-822) */
     case 0xA1: case 0x61: case 0x21: case 0xC1: case 0x41: case 0x01: case 0xE1: {
         uint8_t base = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
-        (void)MREAD(m, base); cyc++;
+        PHANTOM_READ(m, base); cyc++;
         uint8_t ptr = (uint8_t)(base + c->x);
         uint16_t lo = MREAD(m, ptr); cyc++;
         uint16_t hi = MREAD(m, (uint8_t)(ptr + 1)); cyc++;
@@ -244,7 +246,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
     /* STA (zp,X) (cpu.rs:827-841) */
     case 0x81: {
         uint8_t base = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
-        (void)MREAD(m, base); cyc++;
+        PHANTOM_READ(m, base); cyc++;
         uint8_t ptr = (uint8_t)(base + c->x);
         uint16_t lo = MREAD(m, ptr); cyc++;
         uint16_t hi = MREAD(m, (uint8_t)(ptr + 1)); cyc++;
@@ -260,7 +262,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
         uint16_t base = (uint16_t)((hi << 8) | lo);
         uint16_t eff = (uint16_t)(base + c->y);
         if ((base & 0xFF00) != (eff & 0xFF00)) {
-            (void)MREAD(m, (uint16_t)((base & 0xFF00) | (eff & 0x00FF))); cyc++;
+            PHANTOM_READ(m, (uint16_t)((base & 0xFF00) | (eff & 0x00FF))); cyc++;
         }
         uint8_t v = MREAD(m, eff); cyc++;
         orc_read_op(c, op, v);
@@ -274,7 +276,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
         uint16_t hi = MREAD(m, (uint8_t)(zp + 1)); cyc++;
         uint16_t base = (uint16_t)((hi << 8) | lo);
         uint16_t eff = (uint16_t)(base + c->y);
-        (void)MREAD(m, (uint16_t)((base & 0xFF00) | (eff & 0x00FF))); cyc++;
+        PHANTOM_READ(m, (uint16_t)((base & 0xFF00) | (eff & 0x00FF))); cyc++;
         MWRITE(m, eff, c->a); cyc++;
         break;
     }
@@ -294,11 +296,11 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
         default:   taken = (c->p & F_V) != 0; break;
         }
         if (taken) {
-            (void)MREAD(m, c->pc); cyc++;
+            PHANTOM_READ(m, c->pc); cyc++;
             uint16_t old = c->pc;
             uint16_t npc = (uint16_t)(c->pc + (uint16_t)(int16_t)off);
             if ((old & 0xFF00) != (npc & 0xFF00)) {
-                (void)MREAD(m, (uint16_t)((old & 0xFF00) | (npc & 0x00FF))); cyc++;
+                PHANTOM_READ(m, (uint16_t)((old & 0xFF00) | (npc & 0x00FF))); cyc++;
             }
             c->pc = npc;
         }
@@ -327,7 +329,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
     /* JSR (cpu.rs:983-1005) */
     case 0x20: {
         uint16_t lo = MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
-        (void)MREAD(m, (uint16_t)(0x0100 | c->sp)); cyc++;
+        PHANTOM_READ(m, (uint16_t)(0x0100 | c->sp)); cyc++;
         uint16_t ret = c->pc;
         MWRITE(m, (uint16_t)(0x0100 | c->sp), (uint8_t)(ret >> 8)); c->sp--; cyc++;
         MWRITE(m, (uint16_t)(0x0100 | c->sp), (uint8_t)ret); c->sp--; cyc++;
@@ -338,20 +340,20 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
 
     /* RTS (cpu.rs:1010-1028) */
     case 0x60: {
-        (void)MREAD(m, c->pc); cyc++;
-        (void)MREAD(m, (uint16_t)(0x0100 | c->sp)); cyc++;
+        PHANTOM_READ(m, c->pc); cyc++;
+        PHANTOM_READ(m, (uint16_t)(0x0100 | c->sp)); cyc++;
         c->sp++; uint16_t lo = MREAD(m, (uint16_t)(0x0100 | c->sp)); cyc++;
         c->sp++; uint16_t hi = MREAD(m, (uint16_t)(0x0100 | c->sp)); cyc++;
         uint16_t ra = (uint16_t)((hi << 8) | lo);
-        (void)MREAD(m, ra); cyc++;
+        PHANTOM_READ(m, ra); cyc++;
         c->pc = (uint16_t)(ra + 1);
         break;
     }
 
     /* RTI (cpu.rs:1033-1051) */
     case 0x40: {
-        (void)MREAD(m, c->pc); cyc++;
-        (void)MREAD(m, (uint16_t)(0x0100 | c->sp)); cyc++;
+        PHANTOM_READ(m, c->pc); cyc++;
+        PHANTOM_READ(m, (uint16_t)(0x0100 | c->sp)); cyc++;
         c->sp++; c->p = (uint8_t)(MREAD(m, (uint16_t)(0x0100 | c->sp)) & ~(F_B | F_U)); cyc++;
         c->sp++; uint16_t lo = MREAD(m, (uint16_t)(0x0100 | c->sp)); cyc++;
         c->sp++; uint16_t hi = MREAD(m, (uint16_t)(0x0100 | c->sp)); cyc++;
@@ -361,7 +363,7 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
 
     /* BRK (cpu.rs:1056-1080) */
     case 0x00: {
-        (void)MREAD(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
+        PHANTOM_READ(m, c->pc); c->pc = (uint16_t)(c->pc + 1); cyc++;
         MWRITE(m, (uint16_t)(0x0100 | c->sp), (uint8_t)(c->pc >> 8)); c->sp--; cyc++;
         MWRITE(m, (uint16_t)(0x0100 | c->sp), (uint8_t)c->pc); c->sp--; cyc++;
         MWRITE(m, (uint16_t)(0x0100 | c->sp), (uint8_t)(c->p | F_B | F_U)); c->sp--; cyc++;
@@ -374,15 +376,15 @@ static uint8_t STEP_FN(orc_cpu* c, MEM_T* m)
 
     /* PHA / PHP (cpu.rs:1085-1105) */
     case 0x48: case 0x08:
-        (void)MREAD(m, c->pc); cyc++;
+        PHANTOM_READ(m, c->pc); cyc++;
         MWRITE(m, (uint16_t)(0x0100 | c->sp), op == 0x48 ? c->a : (uint8_t)(c->p | F_B | F_U));
         c->sp--; cyc++;
         break;
 
     /* PLA / PLP (cpu.rs:1110-1137) */
     case 0x68: case 0x28: {
-        (void)MREAD(m, c->pc); cyc++;
-        (void)MREAD(m, (uint16_t)(0x0100 | c->sp)); cyc++;
+        PHANTOM_READ(m, c->pc); cyc++;
+        PHANTOM_READ(m, (uint16_t)(0x0100 | c->sp)); cyc++;
         c->sp++; uint8_t v = MREAD(m, (uint16_t)(0x0100 | c->sp)); cyc++;
         if (op == 0x68) { c->a = v; orc_zn(c, c->a); }
         else c->p = (uint8_t)(v & ~(F_B | F_U));

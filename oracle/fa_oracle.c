@@ -580,16 +580,28 @@ static inline void orc_bus_write(orc_atari* e, uint16_t addr, uint8_t v) /* atar
     orc_tia_write(&e->tia, a, v);
 }
 
+/* Phantom accesses on the headless bus are issued unless a test switches
+ * them off (orc_set_phantoms): with them off the oracle behaves like a core
+ * that skips them, as the reference's CUDA kernels do, which lets a test
+ * show that a cart depends on them. */
+static int orc_phantoms = 1;
+
+void orc_set_phantoms(int on) { orc_phantoms = on != 0; }
+
 /* Cpu::step on the Atari bus. */
 #define STEP_FN orc_step_bus
 #define MEM_T orc_atari
 #define MREAD(m, a) orc_bus_read((m), (uint16_t)(a))
 #define MWRITE(m, a, v) orc_bus_write((m), (uint16_t)(a), (uint8_t)(v))
+#define PHANTOM_READ(m, a) do { if (orc_phantoms) (void)MREAD(m, a); } while (0)
+#define RMW_OLD_WRITE(m, a, v) do { if (orc_phantoms) MWRITE(m, a, v); } while (0)
 #include "cpu_step.h"
 #undef STEP_FN
 #undef MEM_T
 #undef MREAD
 #undef MWRITE
+#undef PHANTOM_READ
+#undef RMW_OLD_WRITE
 
 /* Cpu::step on FlatMemory (cpu.rs:69-90). */
 typedef struct orc_flat { uint8_t* ram; } orc_flat;
@@ -597,7 +609,11 @@ typedef struct orc_flat { uint8_t* ram; } orc_flat;
 #define MEM_T orc_flat
 #define MREAD(m, a) ((m)->ram[(uint16_t)(a)])
 #define MWRITE(m, a, v) ((m)->ram[(uint16_t)(a)] = (uint8_t)(v))
+#define PHANTOM_READ(m, a) ((void)MREAD(m, a))
+#define RMW_OLD_WRITE(m, a, v) MWRITE(m, a, v)
 #include "cpu_step.h"
+#undef PHANTOM_READ
+#undef RMW_OLD_WRITE
 #undef STEP_FN
 #undef MEM_T
 #undef MREAD
@@ -1311,7 +1327,11 @@ static void orc_rbus_write(orc_ratari* e, uint16_t addr, uint8_t v) /* atari.rs:
 #define MEM_T orc_ratari
 #define MREAD(m, a) orc_rbus_read((m), (uint16_t)(a))
 #define MWRITE(m, a, v) orc_rbus_write((m), (uint16_t)(a), (uint8_t)(v))
+#define PHANTOM_READ(m, a) ((void)MREAD(m, a))
+#define RMW_OLD_WRITE(m, a, v) MWRITE(m, a, v)
 #include "cpu_step.h"
+#undef PHANTOM_READ
+#undef RMW_OLD_WRITE
 #undef STEP_FN
 #undef MEM_T
 #undef MREAD

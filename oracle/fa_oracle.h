@@ -102,6 +102,11 @@ int orc_flat_run_from(uint8_t* mem64k, int nsteps, uint8_t* cycles_out, orc_regs
 /* sizeof(fa_state) as compiled into the oracle (ABI check). */
 size_t orc_state_size(void);
 
+/* Test switch: 0 skips the headless bus's phantom reads and read-modify-
+ * write's first write (their cycles still count), as a core without them
+ * would; 1 (the default) issues them as the reference does. */
+void orc_set_phantoms(int on);
+
 /* ---- rendering console (src/tia.rs, src/atari.rs:107-306): one bus access per
  * CPU cycle, three TIA clocks and one PIA clock per access, 160 x 192 palette
  * index framebuffer. */

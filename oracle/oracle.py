@@ -124,6 +124,7 @@ def lib() -> ctypes.CDLL:
         L.orc_rtia_copy.argtypes = [vp, vp]
         L.orc_rrun_batch.restype = ctypes.c_uint64
         L.orc_rrun_batch.argtypes = [ctypes.POINTER(vp), sz, ctypes.c_int, u8p, ctypes.c_int]
+        L.orc_set_phantoms.argtypes = [ctypes.c_int]
         _lib = L
     return _lib
 
@@ -289,6 +290,19 @@ def set_rom_scheme(rom: bytes, scheme) -> None:
     code = SCHEMES[scheme.lower()] if isinstance(scheme, str) else int(scheme)
     if lib().orc_rom_set_scheme(_u8(r), len(r), code) != 0:
         raise ValueError(f"scheme {scheme!r} cannot hold a {len(r)}-byte ROM")
+
+
+class phantoms_off:
+    """Context manager: inside it the oracle skips the headless bus's phantom
+    reads and read-modify-write's first write (a deliberately wrong oracle,
+    for tests that show a cart depends on those accesses)."""
+
+    def __enter__(self):
+        lib().orc_set_phantoms(0)
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_phantoms(1)
 
 
 def reset_state(rom: bytes) -> np.ndarray:

@@ -95,3 +95,14 @@ def test_reward_spec_rejected_before_any_device_work():
             sp.terminal_addr, sp.terminal_mask, sp.terminal_value = kw["terminal"]
         rc = L.fa_obs_reward(fa._vp(fake), 8, ctypes.byref(sp), 0, fa._vp(fake), fa._vp(fake), None, None, None)
         assert rc == -1, (kw, rc)                     # FA_ERR_INVALID
+
+
+def test_wait_limit_setting_is_bounded():
+    """fa_set_wait_limit_ns: host-side only (no device needed); 0..10 s."""
+    assert fa.wait_limit_ns() == 2_000_000_000
+    with pytest.raises(fa.FaError):
+        fa.set_wait_limit_ns(10_000_000_001)
+    assert fa.wait_limit_ns() == 2_000_000_000
+    fa.set_wait_limit_ns(0)
+    assert fa.wait_limit_ns() == 0
+    fa.set_wait_limit_ns(2_000_000_000)

@@ -97,3 +97,47 @@ def test_oracle_matches_frozen_vectors(name):
     want = GOLDEN[name]
     for key in ("rom_sha256", "reset_state_sha256", "ram_sha256_at", "final_state_sha256", "instructions"):
         assert got[key] == want[key], (name, key)
+
+
+# ---------------------------------------------------------------- phantom-access carts
+def test_phantom_carts_run_2k_frames_without_a_halt():
+    """The phantom-access carts (every bank the same code) never reach an
+    illegal opcode, the VSYNC budget or the cycle cap."""
+    cs = carts.phantom_carts()
+    with ThreadPoolExecutor(max_workers=len(cs)) as ex:
+        for name, st in ex.map(_run_long, [(c, 2_000) for c in cs]):
+            assert (st["run_status"] == 0).all(), (name, st["run_status"])
+            assert (st["frame_no"] == 2_000).all(), name
+
+
+def test_phantom_carts_banks_identical_but_the_id_byte():
+    for c in carts.phantom_carts():
+        nb = c.spec.nbanks
+        off = carts.PHANTOM_BANKID - 0xF000
+        banks = [bytearray(c.rom[b * 4096:(b + 1) * 4096]) for b in range(nb)]
+        assert [bk[off] for bk in banks] == [0x30 + 0x11 * b for b in range(nb)], c.spec.name
+        for bk in banks:
+            bk[off] = 0
+        assert len({bytes(bk) for bk in banks}) == 1, c.spec.name
+
+
+@pytest.mark.parametrize("c", carts.phantom_carts(), ids=lambda c: c.spec.name)
+def test_phantom_carts_depend_on_phantom_accesses(c):
+    """With the oracle's phantom reads and first RMW writes switched off (as
+    a core that skips them would run), every instance ends in a different
+    state: the carts detect a core that drops those accesses."""
+    n, k = 32, 6
+    acts = carts.actions(seed=11, n=n, frames=k)
+    st_on = np.array([oracle.reset_state(c.rom)] * n, dtype=oracle.STATE_DTYPE)
+    oracle.run_batch(c.rom, st_on, acts, k)
+    with oracle.phantoms_off():
+        st_off = np.array([oracle.reset_state(c.rom)] * n, dtype=oracle.STATE_DTYPE)
+        oracle.run_batch(c.rom, st_off, acts, k)
+    differs = np.zeros(n, bool)
+    for f in oracle.COMPARED_FIELDS:
+        differs |= (st_on[f] != st_off[f]).reshape(n, -1).any(axis=1)
+    assert differs.all()
+    assert not np.array_equal(st_on["grp0_old"], st_off["grp0_old"])      # RMW double write
+    assert not np.array_equal(st_on["ram"], st_off["ram"])
+    if c.spec.nbanks > 1:
+        assert not np.array_equal(st_on["bank"], st_off["bank"]) or "rts" in c.spec.name

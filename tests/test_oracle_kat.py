@@ -209,3 +209,19 @@ def test_jmp_indirect_page_bug():
     m = mem_with([0x6C, 0xFF, 0x30], extra={0x30FF: 0x34, 0x3000: 0x12, 0x3100: 0x99})
     regs, cyc, _ = oracle.flat_run(m, 1)
     assert cyc[0] == 5 and regs.pc == 0x1234
+
+
+# ---- the same KATs on the 2600 bus (the form the GPU tests run them in) ----
+
+@pytest.mark.parametrize("name", [k.name for k in __import__("kat_2600").KATS])
+def test_reference_kats_relocated_to_the_2600_bus(name):
+    """Each KAT as a 4K Fixed cart from $F100, run for one frame by the
+    oracle's Atari console, gives the values of tests/cycle_counts.rs once
+    the terminator's share is taken off (kat_2600.py)."""
+    import kat_2600
+    k = next(k for k in kat_2600.KATS if k.name == name)
+    rom = k.image()
+    st = kat_2600.kat_start_state(k, rom)
+    oracle.run_batch(rom, st, np.zeros((1, 1), np.uint8), 1)
+    assert st["run_status"][0] == 0
+    kat_2600.check_kat(k, st[0], "oracle")
