@@ -1,0 +1,53 @@
+// Test infrastructure: the device core run on the host.  fa_device.cuh's Emu
+// and fa_run.cuh's Runner step one instance at a time (one lane, so the
+// warp scheduler of run_lanes is not involved: it only orders the lanes),
+// over the bank image, SoA state columns and packing of fa_api.cu.  run_one
+// follows run_unit_as (fa_run.cuh) for one lane.
+#include "shim.h"
+#include "../../fast-atari-rs_b200/csrc/fa_api.cu"
+#include "../../fast-atari-rs_b200/csrc/fa_run.cuh"
+
+template <bool SL>
+static void run_one(const FaGroup& G, uint32_t i, uint8_t* rom, unsigned long long* instr)
+{
+    uint32_t priv[FA_SMEM_WORDS];
+    fa::Runner<1, SL> r;
+    r.f = 0; r.phase = 0; r.fcyc = 0; r.active = false;
+    r.e.pv = (uint8_t*)priv;
+    r.e.G = &G; r.e.i = i; r.e.rom = rom; r.e.hot_lo = G.hot_lo; r.e.nbanks = G.nbanks;
+    r.e.instr = 0; r.e.flim = 0; r.e.cyc_acc = 0; r.e.pc = 0; r.e.bank = 0; r.e.slices = 0; r.e.scanline = 0;
+    uint32_t* col = G.state + i;
+    r.e.load_ram(col, G.stride);
+    r.e.load_hot(col, G.stride);
+    if (G.k > 0) r.active = r.begin_frame();
+    while (r.active) r.iterate();
+    r.e.fold_cycles();
+    if (G.actions && r.f + 1u < G.k && (r.e.row(R_STATUS) & FA_STATUS_HALT_MASK))       // as run_unit_as
+        r.e.apply_action(G.actions[(size_t)(G.k - 1u) * G.act_stride + r.e.i]);
+    r.e.store_ram(col, G.stride);
+    r.e.store_hot(col, G.stride);
+    *instr += r.e.instr;
+}
+
+extern "C" long long hs_run(const uint8_t* rom, size_t len, fa_state* st, size_t n, const uint8_t* actions, int k)
+{
+    std::vector<uint8_t> img;
+    int scheme = 0;
+    uint32_t nbanks = 0, hot_lo = 0;
+    if (fa_make_bank_image(rom, len, img, scheme, &nbanks, &hot_lo)) return -1;
+    std::vector<uint8_t> simg(img.size() + 64, 0);
+    memcpy(simg.data(), img.data(), img.size());
+    std::vector<uint32_t> rows((size_t)FA_ROWS * n);
+    for (size_t i = 0; i < n; i++) fa_pack_column(st[i], rows.data() + i, n);
+    FaGroup G;
+    memset(&G, 0, sizeof(G));
+    G.rom = simg.data(); G.state = rows.data(); G.stride = (uint32_t)n; G.n = (uint32_t)n;
+    G.actions = actions; G.act_stride = (uint32_t)n; G.nbanks = nbanks; G.hot_lo = hot_lo; G.k = (uint32_t)k;
+    unsigned long long instr = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        if (fa_map_kind(hot_lo)) run_one<true>(G, i, simg.data(), &instr);
+        else run_one<false>(G, i, simg.data(), &instr);
+    }
+    for (size_t i = 0; i < n; i++) fa_unpack_column(rows.data() + i, n, scheme, st[i]);
+    return (long long)instr;
+}

@@ -1,0 +1,116 @@
+"""The CUDA interpreter's own device code, compiled for the host, against the
+oracle (CPU only).
+
+tests/hostsim/ compiles fa_device.cuh (the 6502, bus, mappers, headless TIA
+and PIA) and fa_run.cuh (the frame loop of run_frame / run_one_cycle) with
+g++, one instance per lane of a host loop.  The full state after every call
+must equal the oracle's on every cart family (the mixed batch, divergence,
+scale, phantom-access, stall, E0 and 3F carts), on the reference's KATs
+relocated to the 2600 bus, and on random ROMs started from random CPU
+states.  The warp scheduling of the GPU only orders the lanes, so this
+checks the interpreter's arithmetic and bus order without a GPU; the -m gpu
+tests check the same on the device.
+"""
+import ctypes
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import kat_2600
+import oracle
+from fa_pkg import ROOT, carts
+
+HERE = Path(__file__).resolve().parent / "hostsim"
+
+
+@pytest.fixture(scope="module")
+def sim():
+    out = Path(tempfile.mkdtemp(prefix="fa_hostsim_")) / "libhostsim.so"
+    cxx = os.environ.get("CXX", "g++")
+    subprocess.run([cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-I", str(HERE), "-I", str(ROOT / "include"),
+                    str(HERE / "host_run.cpp"), "-o", str(out)], check=True)
+    L = ctypes.CDLL(str(out))
+    L.hs_run.restype = ctypes.c_longlong
+    L.hs_run.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                         ctypes.c_int]
+    L.fa_rom_set_scheme.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    return L
+
+
+def run_both(L, rom, start, acts, k):
+    ref, got = start.copy(), start.copy()
+    oracle.run_batch(rom, ref, acts, k)
+    r = np.frombuffer(rom, np.uint8).copy()
+    a = np.ascontiguousarray(acts, dtype=np.uint8)
+    assert L.hs_run(r.ctypes.data, len(r), got.ctypes.data, len(got), a.ctypes.data, k) >= 0
+    return got, ref
+
+
+def assert_same(got, ref, what):
+    for f in oracle.COMPARED_FIELDS:
+        if not np.array_equal(got[f], ref[f]):
+            i = int(np.nonzero((got[f] != ref[f]).reshape(len(got), -1).any(axis=1))[0][0])
+            raise AssertionError(f"{what}: {f} differs, first instance {i}: device code {got[f][i]} oracle {ref[f][i]}")
+
+
+def cart_list():
+    out = carts.mixed_carts() + [carts.plain_cart(), carts.divergence_cart(), carts.scale_cart()]
+    out += carts.phantom_carts() + [carts.stall_cart("no_vsync"), carts.stall_cart("vsync_held")]
+    return out
+
+
+@pytest.mark.parametrize("c", cart_list(), ids=lambda c: c.spec.name)
+def test_device_core_matches_oracle_on_carts(sim, c):
+    n, k = 48, 5
+    start = np.array([oracle.reset_state(c.rom)] * n, dtype=oracle.STATE_DTYPE)
+    got, ref = run_both(sim, c.rom, start, carts.actions(seed=1, n=n, frames=k), k)
+    assert_same(got, ref, c.spec.name)
+
+
+@pytest.mark.parametrize("name", ["e0", "3f16", "3f6"])
+def test_device_core_matches_oracle_on_sliced_carts(sim, name):
+    c, code = {"e0": (carts.e0_cart(), 4), "3f16": (carts.f3_cart(16384), 5), "3f6": (carts.f3_cart(6144), 5)}[name]
+    r = np.frombuffer(c.rom, np.uint8).copy()
+    sim.fa_rom_set_scheme(r.ctypes.data, len(r), code)
+    oracle.set_rom_scheme(c.rom, code)
+    try:
+        n, k = 40, 4
+        start = np.array([oracle.reset_state(c.rom)] * n, dtype=oracle.STATE_DTYPE)
+        got, ref = run_both(sim, c.rom, start, carts.actions(seed=2, n=n, frames=k), k)
+        assert_same(got, ref, name)
+    finally:
+        sim.fa_rom_set_scheme(r.ctypes.data, len(r), -1)
+        oracle.set_rom_scheme(c.rom, "auto")
+
+
+def test_device_core_runs_the_reference_kats(sim):
+    for k in kat_2600.KATS:
+        rom = k.image()
+        start = np.repeat(kat_2600.kat_start_state(k, rom), 2)
+        got, ref = run_both(sim, rom, start, np.zeros((1, 2), np.uint8), 1)
+        assert_same(got, ref, k.name)
+        kat_2600.check_kat(k, got[0], "device code")
+
+
+@pytest.mark.parametrize("size", [2048, 4096, 8192, 16384, 32768])
+def test_device_core_on_random_roms_and_states(sim, size):
+    rng = np.random.default_rng(size)
+    for t in range(6):
+        rom = bytearray(rng.integers(0, 256, size, dtype=np.uint8).tobytes())
+        for b in range(max(1, size // 4096)):
+            base = b * 4096 + min(size, 4096) - 4
+            rom[base:base + 2] = bytes([0x00, 0xF0])
+        rom = bytes(rom)
+        n = 64
+        st = np.array([oracle.reset_state(rom)] * n, dtype=oracle.STATE_DTYPE)
+        st["a"], st["x"], st["y"] = rng.integers(0, 256, n), rng.integers(0, 256, n), rng.integers(0, 256, n)
+        st["sp"], st["status"] = rng.integers(0, 256, n), rng.integers(0, 256, n) & 0xCF
+        st["pc"] = 0xF000 + rng.integers(0, 0x1000, n)
+        st["ram"] = rng.integers(0, 256, (n, 128))
+        st["run_status"] = 0
+        got, ref = run_both(sim, rom, st, carts.actions(seed=t, n=n, frames=3), 3)
+        assert_same(got, ref, f"random {size}-byte ROM {t}")
