@@ -114,3 +114,26 @@ def test_device_core_on_random_roms_and_states(sim, size):
         st["run_status"] = 0
         got, ref = run_both(sim, rom, st, carts.actions(seed=t, n=n, frames=3), 3)
         assert_same(got, ref, f"random {size}-byte ROM {t}")
+
+
+def test_device_core_every_opcode_first(sim):
+    """Instance i starts on a byte equal to i, with random registers and RAM:
+    every one of the 256 opcodes (the 151 and the illegal ones) executes
+    first at least once."""
+    rng = np.random.default_rng(99)
+    for size in (4096, 32768):
+        rom = bytearray(rng.integers(0, 256, size, dtype=np.uint8).tobytes())
+        for b in range(size // 4096):
+            rom[b * 4096 + 0xFFC:b * 4096 + 0xFFE] = bytes([0x00, 0xF0])
+            rom[b * 4096 + 0x800:b * 4096 + 0x900] = bytes(range(256))     # opcode i at $F800 + i
+        rom = bytes(rom)
+        n = 256
+        st = np.array([oracle.reset_state(rom)] * n, dtype=oracle.STATE_DTYPE)
+        st["a"], st["x"], st["y"] = rng.integers(0, 256, n), rng.integers(0, 256, n), rng.integers(0, 256, n)
+        st["sp"], st["status"] = rng.integers(0, 256, n), rng.integers(0, 256, n) & 0xCF
+        st["pc"] = 0xF800 + np.arange(n)
+        st["ram"] = rng.integers(0, 256, (n, 128))
+        st["run_status"] = 0
+        got, ref = run_both(sim, rom, st, carts.actions(seed=5, n=n, frames=2), 2)
+        assert_same(got, ref, f"every opcode first, {size}-byte ROM")
+        assert (ref["run_status"] & 1).sum() >= 105          # the illegal opcodes halt at once
