@@ -522,7 +522,8 @@ class ServerConfig(ctypes.Structure):
 class RequestInfo(ctypes.Structure):
     """fa_request_info (include/fast_atari.h)."""
     _fields_ = [("status", ctypes.c_int), ("waited_admission", ctypes.c_int), ("batch_requests", ctypes.c_uint),
-                ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double)]
+                ("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double),
+                ("session_wait_ms", ctypes.c_double), ("service_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -558,6 +559,12 @@ class LoadgenResult(ctypes.Structure):
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+# fa_loadgen_record (include/fast_atari.h).
+LOADGEN_RECORD = np.dtype([("cart", "<u4"), ("n", "<u4"), ("k", "<u4"), ("batch_requests", "<u4"),
+                           ("arrival_s", "<f8"), ("latency_ms", "<f8"), ("session_wait_ms", "<f8"),
+                           ("dispatch_ms", "<f8"), ("service_ms", "<f8")])
 
 
 class AtariServer:
@@ -648,13 +655,14 @@ class AtariServer:
     def loadgen(self, requests: int, offered_frames_per_s: float, clients: int = 64, seed: int = 1,
                 batch_median: int = 256, batch_min: int = 16, batch_max: int = 16384, batch_sigma: float = 1.0,
                 k_min: int = 1, k_max: int = 8):
-        """Run the simulated actor clients; returns (result dict, latencies ms)."""
+        """Run the simulated actor clients; returns (result dict, per-request
+        records: a LOADGEN_RECORD structured array in arrival order)."""
         cfg = LoadgenConfig(int(clients), int(requests), float(offered_frames_per_s), int(seed), int(batch_median),
                             int(batch_min), int(batch_max), float(batch_sigma), int(k_min), int(k_max))
         res = LoadgenResult()
-        lat = np.zeros(int(requests), np.float32)
-        _check(lib().fa_server_loadgen(self._s, ctypes.byref(cfg), ctypes.byref(res), lat.ctypes.data))
-        return res.as_dict(), lat
+        rec = np.zeros(int(requests), LOADGEN_RECORD)
+        _check(lib().fa_server_loadgen(self._s, ctypes.byref(cfg), ctypes.byref(res), rec.ctypes.data))
+        return res.as_dict(), rec
 
 
 # ------------------------------------------------------------------ rendering

@@ -77,6 +77,7 @@ struct Request {
     uint8_t* obs = nullptr;
     std::vector<uint32_t*> fresh;      // blocks admitted for this request (set to the snapshot first)
     Clock::time_point t_submit, t_dispatch, t_done;
+    Clock::time_point t_ready;         // its session's earlier requests were done (>= t_submit)
     int status = FA_OK;
     bool done = false, waited_admission = false;
     uint32_t batch = 0;
@@ -89,6 +90,7 @@ struct Session {
     std::vector<uint32_t*> blocks;
     std::deque<ReqP> pending;          // not yet dispatched, in submission order
     bool busy = false;                 // a request of the session is on the GPU
+    Clock::time_point t_free{};        // when its last request finished
     bool closing = false;
 };
 
@@ -216,6 +218,7 @@ void finish_request(fa_server* s, const ReqP& r, int status)
     auto it = s->sessions.find(r->sid);
     if (it != s->sessions.end()) {
         it->second.busy = false;
+        it->second.t_free = r->t_done;
         if (it->second.closing && it->second.pending.empty()) release_session(s, r->sid);
     }
     if (status == FA_OK) {
@@ -463,6 +466,7 @@ void dispatch_ready(fa_server* s)
         ss.size = std::max(ss.size, r->n);
         ss.pending.pop_front();
         ss.busy = true;
+        r->t_ready = std::max(r->t_submit, ss.t_free);
         batch.push_back(r);
     }
     if (batch.empty()) return;
@@ -752,7 +756,10 @@ extern "C" int fa_server_wait(fa_server* s, uint64_t ticket, int timeout_ms, fa_
     if (info) {
         info->status = r->status;
         info->latency_ms = ms_between(r->t_submit, r->t_done);
-        info->queue_ms = r->t_dispatch.time_since_epoch().count() ? ms_between(r->t_submit, r->t_dispatch) : 0.0;
+        const bool sent = r->t_dispatch.time_since_epoch().count() != 0;
+        info->queue_ms = sent ? ms_between(r->t_submit, r->t_dispatch) : 0.0;
+        info->session_wait_ms = sent ? ms_between(r->t_submit, r->t_ready) : 0.0;
+        info->service_ms = sent ? ms_between(r->t_dispatch, r->t_done) : 0.0;
         info->batch_requests = r->batch;
         info->waited_admission = r->waited_admission ? 1 : 0;
     }
@@ -843,7 +850,7 @@ struct TraceReq {
 }  // namespace
 
 extern "C" int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_loadgen_result* out,
-                                 float* latency_ms)
+                                 fa_loadgen_record* records)
 {
     if (!s || !cfg || !out) return fa_fail(FA_ERR_INVALID, "null argument");
     const int ncarts = (int)s->carts.size();
@@ -943,7 +950,18 @@ extern "C" int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_
     unsigned long long waited = 0;
     for (int i = 0; i < c.requests; i++) {
         lat[i] = info[i].latency_ms;
-        if (latency_ms) latency_ms[i] = (float)info[i].latency_ms;
+        if (records) {
+            fa_loadgen_record& rec = records[i];
+            rec.cart = (uint32_t)tr[i].cart;
+            rec.n = tr[i].n;
+            rec.k = tr[i].k;
+            rec.batch_requests = info[i].batch_requests;
+            rec.arrival_s = t_sub[i];
+            rec.latency_ms = info[i].latency_ms;
+            rec.session_wait_ms = info[i].session_wait_ms;
+            rec.dispatch_ms = info[i].queue_ms - info[i].session_wait_ms;
+            rec.service_ms = info[i].service_ms;
+        }
         sum += info[i].latency_ms;
         qsum += info[i].queue_ms;
         bsum += info[i].batch_requests;

@@ -28,7 +28,13 @@ def _pkg():
     return sys.modules["fast_atari_b200"]
 
 
-def tune_workload(carts_with_counts, cap: int = 150_000):
+def tune_workload(carts_with_counts, cap: int = 150_000, keep: int = 6):
+    """Per cart: fa_autotune's best record, its cost per instance-frame as
+    the queue weight, and the `keep` fastest measured configurations (the
+    sweep's table of alternatives).  In a pool every cart shares one launch,
+    so only the policy and the weight apply there; the launch shape and K
+    apply when the cart runs on a handle of its own (fa_set_launch,
+    fa_set_cta_warps, step_multi's k)."""
     fa = _pkg()
     names = {v: k for k, v in fa.SCHED_NAMES.items()}
     out = {}
@@ -38,6 +44,11 @@ def tune_workload(carts_with_counts, cap: int = 150_000):
         best["weight"] = best["ns_per_instance_frame"]
         best["instances"] = min(n, cap)
         best["measurements"] = len(table)
+        alts = sorted(table, key=lambda t: -t["frames_per_s"])[:keep]
+        best["alternatives"] = [{"sched": names[t["sched"]], "persistent": t["persistent"], "cta_warps": t["cta_warps"],
+                                 "block": t["block"], "k": t["k"], "frames_per_s": round(t["frames_per_s"])}
+                                for t in alts]
+        best["applied_in_pool"] = ["sched", "weight"]
         out[cart.spec.name] = best
     return out
 

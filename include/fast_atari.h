@@ -448,6 +448,10 @@ typedef struct fa_request_info {
     unsigned batch_requests;     /* requests in the launch batch it ran in */
     double latency_ms;           /* submit -> observations in the caller's buffer */
     double queue_ms;             /* submit -> dispatch to the GPU */
+    double session_wait_ms;      /* of queue_ms: waiting for the same session's earlier
+                                    requests (an actor steps after it sees its observations) */
+    double service_ms;           /* dispatch -> done: the GPU work of its batch and the
+                                    completion signal */
 } fa_request_info;
 
 typedef struct fa_server_stats {
@@ -502,7 +506,8 @@ int  fa_server_stats_get(fa_server* s, fa_server_stats* out);
  * [k_min, k_max], with actions uniform over the 18 joystick actions.  The
  * trace depends only on the configuration (seed included), not on timing.
  * Every (client, cart) is a session opened for the run and closed after it.
- * latency_ms (NULL or `requests` floats) receives each request's latency. */
+ * records (NULL or `requests` entries, in arrival order) receives each
+ * request's shape and the parts of its latency. */
 typedef struct fa_loadgen_config {
     int      clients;
     int      requests;
@@ -529,7 +534,17 @@ typedef struct fa_loadgen_result {
     int    errors;
 } fa_loadgen_result;
 
-int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_loadgen_result* out, float* latency_ms);
+typedef struct fa_loadgen_record {
+    uint32_t cart, n, k, batch_requests;
+    double   arrival_s;            /* submit time from the run's start */
+    double   latency_ms;           /* = session_wait_ms + dispatch_ms + service_ms */
+    double   session_wait_ms;      /* the same session's earlier requests still running */
+    double   dispatch_ms;          /* ready -> dispatched: launch slots and state admission */
+    double   service_ms;           /* dispatched -> done */
+} fa_loadgen_record;
+
+int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_loadgen_result* out,
+                      fa_loadgen_record* records);
 
 /* ------------------------------------------------------------ rendering
  * The reference's rendering console (Atari, src/atari.rs:107-306, with the

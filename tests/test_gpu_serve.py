@@ -219,6 +219,13 @@ def test_loadgen_trace_same_work_in_both_modes(mixed):
     assert rb["errors"] == 0 and rp["errors"] == 0
     assert rb["requests"] == rp["requests"] == 120
     assert rb["instance_frames"] == rp["instance_frames"] == stb["instance_frames"]
-    assert (lat_b > 0).all() and (lat_p > 0).all()
+    for rec, res in ((lat_b, rb), (lat_p, rp)):
+        assert (rec["latency_ms"] > 0).all() and (rec["service_ms"] > 0).all()
+        # the parts of every request's latency add up to it
+        parts = rec["session_wait_ms"] + rec["dispatch_ms"] + rec["service_ms"]
+        assert np.allclose(parts, rec["latency_ms"], rtol=0, atol=1e-6)
+        assert (rec["session_wait_ms"] >= 0).all() and (rec["dispatch_ms"] >= -1e-9).all()
+        assert float((rec["n"].astype(np.float64) * rec["k"]).sum()) == res["instance_frames"]
+        assert set(np.unique(rec["cart"])) <= set(range(len(roms)))
     assert rb["p50_ms"] <= rb["p99_ms"] <= rb["max_ms"]
     assert stb["sessions_open"] == 0 and stb["state_bytes_in_use"] == 0
