@@ -139,6 +139,9 @@ _SIGS = {
     "fa_render_get_framebuffers": (_i, [_vp, _vp]),
     "fa_render_get_states": (_i, [_vp, _vp]),
     "fa_render_last_instructions": (ctypes.c_ulonglong, [_vp]),
+    "fa_render_rgba_async": (_i, [_vp, _sz, _sz, _vp, _vp]),
+    "fa_render_get_rgba": (_i, [_vp, _sz, _sz, _vp]),
+    "fa_palette_rgba": (ctypes.c_uint32, [ctypes.c_uint8]),
 }
 
 FA_ERR_BAD_ROM = -2
@@ -195,6 +198,12 @@ def device_count() -> int:
 
 def set_device(device: int) -> None:
     _check(lib().fa_set_device(int(device)))
+
+
+def palette_rgba(index: int) -> tuple:
+    """ntsc_palette of one palette index as (R, G, B, A)."""
+    v = int(lib().fa_palette_rgba(int(index) & 0xFF))
+    return (v & 0xFF, (v >> 8) & 0xFF, (v >> 16) & 0xFF, v >> 24)
 
 
 def set_wait_limit_ns(ns: int) -> None:
@@ -717,6 +726,18 @@ class AtariRender:
 
     def synchronize(self) -> None:
         _check(lib().fa_render_synchronize(self._r))
+
+    def rgba(self, first: int = 0, count: Optional[int] = None) -> np.ndarray:
+        """Atari::render of consoles [first, first + count): (count, 192, 160, 4)
+        uint8 RGBA, converted on the device."""
+        if count is None:
+            count = self.n - first
+        out = np.empty((count, FB_H, FB_W, 4), np.uint8)
+        _check(lib().fa_render_get_rgba(self._r, int(first), int(count), out.ctypes.data))
+        return out
+
+    def rgba_async(self, first: int, count: int, d_rgba: int, stream: int = 0) -> None:
+        _check(lib().fa_render_rgba_async(self._r, int(first), int(count), _vp(d_rgba), _vp(stream or None)))
 
     def framebuffers(self) -> np.ndarray:
         out = np.empty((self.n, FB_H, FB_W), np.uint8)

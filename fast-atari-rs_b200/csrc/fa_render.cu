@@ -260,6 +260,42 @@ __global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLa
 
 }  // namespace fa
 
+// ------------------------------------------------------------------ RGBA
+// Atari::render (src/atari.rs:356-369): every palette index of a framebuffer
+// becomes R, G, B, 255 through ntsc_palette (src/atari.rs:624-645), whose 128
+// entries come in equal pairs indexed by (index >> 1) & 0x7F; so the colour
+// depends on index >> 2 only, and the 64 distinct colours are kept here as
+// packed little-endian RGBA words (R in the low byte, alpha 255).
+#define FA_NTSC_RGBA \
+    0xFF000000u, 0xFF004444u, 0xFF002870u, 0xFF001884u, 0xFF000088u, 0xFF5C0078u, 0xFF780048u, 0xFF840014u, \
+    0xFF880000u, 0xFF780000u, 0xFF600000u, 0xFF2C1400u, 0xFF002800u, 0xFF002C00u, 0xFF002C00u, 0xFF001800u, \
+    0xFF282828u, 0xFF106464u, 0xFF104890u, 0xFF0038A8u, 0xFF0014B8u, 0xFF7400A0u, 0xFFA40064u, 0xFFB00030u, \
+    0xFFB80000u, 0xFFA81800u, 0xFF802C00u, 0xFF4C3C00u, 0xFF004400u, 0xFF004C00u, 0xFF004400u, 0xFF003800u, \
+    0xFF545454u, 0xFF248484u, 0xFF2464B0u, 0xFF1050C8u, 0xFF1438DCu, 0xFF9014C4u, 0xFFC80084u, 0xFFD40050u, \
+    0xFFDC0018u, 0xFFD43000u, 0xFFA44C00u, 0xFF6C5C00u, 0xFF006400u, 0xFF006C00u, 0xFF106400u, 0xFF005400u, \
+    0xFF787878u, 0xFF38A8A8u, 0xFF3888CCu, 0xFF2470E8u, 0xFF285CFCu, 0xFFAC30E8u, 0xFFE800A8u, 0xFFF40070u, \
+    0xFFFC0038u, 0xFFF84C0Cu, 0xFFC46C00u, 0xFF8C8000u, 0xFF008800u, 0xFF009000u, 0xFF288800u, 0xFF007400u
+static const uint32_t kNtscRgba[64] = { FA_NTSC_RGBA };
+
+namespace fa {
+
+static __constant__ uint32_t c_ntsc_rgba[64] = { FA_NTSC_RGBA };
+
+// Four pixels per thread: one 32-bit load of palette indices, one 16-byte
+// store of RGBA, the 64 colours in shared memory (two lanes per bank at most).
+__global__ void fa_fb_rgba(const uint32_t* __restrict__ fb4, uint4* __restrict__ rgba, size_t words)
+{
+    __shared__ uint32_t pal[64];
+    if (threadIdx.x < 64) pal[threadIdx.x] = c_ntsc_rgba[threadIdx.x];
+    __syncthreads();
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t w = fb4[i];
+        rgba[i] = make_uint4(pal[(w >> 2) & 63u], pal[(w >> 10) & 63u], pal[(w >> 18) & 63u], pal[(w >> 26) & 63u]);
+    }
+}
+
+}  // namespace fa
+
 // ------------------------------------------------------------------ host side
 // One host thread's share of a device-to-host copy into pageable memory:
 // two pinned chunks and a stream, so that the GPU fills one chunk while the
@@ -291,6 +327,7 @@ struct fa_render {
     bool reset_done = false;
     unsigned long long last_instr = 0, last_slots = 0;
     std::vector<FaStager> stagers;   // made on the first large copy out
+    uint8_t* d_rgba = nullptr;         // RGBA of a chunk of consoles for fa_render_get_rgba (made on first use)
 };
 
 namespace {
@@ -346,6 +383,7 @@ void free_render(fa_render* r)
     cudaFree(r->d_obs);
     cudaFree(r->d_err);
     cudaFree(r->d_ctr);
+    cudaFree(r->d_rgba);
     for (FaStager& g : r->stagers) {
         if (g.stream) cudaStreamSynchronize(g.stream);
         for (int b = 0; b < 2; b++) {
@@ -629,6 +667,48 @@ extern "C" int fa_render_get_framebuffers(fa_render* r, uint8_t* out)
     if (!out) return fa_fail(FA_ERR_INVALID, "out is null");
     FA_CUDA(cudaStreamSynchronize(r->stream));
     return copy_d2h(r, out, r->d_fb, r->n * (size_t)FA_FB_BYTES);
+}
+
+namespace {
+constexpr size_t kRgbaChunkConsoles = 2048;                        // 240 MiB of RGBA per device chunk
+
+cudaError_t launch_rgba(const uint8_t* fb, uint8_t* rgba, size_t consoles, cudaStream_t s)
+{
+    const size_t words = consoles * (size_t)FA_FB_BYTES / 4u;
+    if (words == 0) return cudaSuccess;
+    size_t grid = (words + 255u) / 256u;
+    if (grid > 148u * 16u) grid = 148u * 16u;
+    fa::fa_fb_rgba<<<(unsigned)grid, 256, 0, s>>>((const uint32_t*)fb, (uint4*)rgba, words);
+    return cudaGetLastError();
+}
+}  // namespace
+
+extern "C" uint32_t fa_palette_rgba(uint8_t index) { return kNtscRgba[(index >> 2) & 63u]; }
+
+extern "C" int fa_render_rgba_async(fa_render* r, size_t first, size_t count, uint8_t* d_rgba, void* stream)
+{
+    CHECK_R(r);
+    if (first > r->n || count > r->n - first) return fa_fail(FA_ERR_INVALID, "consoles [%zu, %zu) out of range", first, first + count);
+    if (!d_rgba || ((uintptr_t)d_rgba & 15u)) return fa_fail(FA_ERR_INVALID, "d_rgba null or not 16-byte aligned");
+    FA_CUDA(launch_rgba(r->d_fb + first * (size_t)FA_FB_BYTES, d_rgba, count, stream ? (cudaStream_t)stream : r->stream));
+    return FA_OK;
+}
+
+extern "C" int fa_render_get_rgba(fa_render* r, size_t first, size_t count, uint8_t* out)
+{
+    CHECK_R(r);
+    if (first > r->n || count > r->n - first) return fa_fail(FA_ERR_INVALID, "consoles [%zu, %zu) out of range", first, first + count);
+    if (!out) return fa_fail(FA_ERR_INVALID, "null output");
+    const size_t per = (size_t)FA_FB_BYTES * 4u;
+    if (!r->d_rgba) FA_CUDA(cudaMalloc(&r->d_rgba, std::min(r->n, kRgbaChunkConsoles) * per));
+    for (size_t c0 = 0; c0 < count; c0 += kRgbaChunkConsoles) {
+        const size_t m = std::min(kRgbaChunkConsoles, count - c0);
+        FA_CUDA(launch_rgba(r->d_fb + (first + c0) * (size_t)FA_FB_BYTES, r->d_rgba, m, r->stream));
+        FA_CUDA(cudaStreamSynchronize(r->stream));
+        const int rc = copy_d2h(r, out + c0 * per, r->d_rgba, m * per);
+        if (rc) return rc;
+    }
+    return FA_OK;
 }
 
 extern "C" int fa_render_get_states(fa_render* r, fa_state* out)

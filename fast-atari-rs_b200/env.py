@@ -59,6 +59,16 @@ class BatchAtariGpuEnv:
         self._flags = t.zeros(self.n, dtype=t.uint8, device=self.device)
         return self
 
+    def with_reward_table(self, table, game: str = None) -> "BatchAtariGpuEnv":
+        """The reward spec of this env's game from a reward table (a path or a
+        rewards.RewardTable): by `game` name, else by the ROM's SHA-256."""
+        from .rewards import RewardTable
+        tab = table if isinstance(table, RewardTable) else RewardTable.load(table)
+        spec = tab.for_game(game) if game is not None else tab.for_rom(self.rom)
+        if spec is None:
+            raise KeyError("no entry of the reward table matches this ROM; name the game")
+        return self.with_reward(spec)
+
     def _rewards(self, init: bool):
         stream = self.torch.cuda.current_stream(self.device).cuda_stream
         obs_reward(self._obs_u8.data_ptr(), self.n, self.reward_spec, init, self._score.data_ptr(),

@@ -583,6 +583,17 @@ int  fa_render_get_framebuffers(fa_render* r, uint8_t* out);
 /* CPU, RAM, PIA and TIA register state (fa_state layout; cycles, frame_no, run_status). */
 int  fa_render_get_states(fa_render* r, fa_state* out);
 unsigned long long fa_render_last_instructions(const fa_render* r);
+/* Atari::render (src/atari.rs:356-369): consoles [first, first + count) as
+ * RGBA, 160 x 192 x 4 bytes each (R, G, B from ntsc_palette,
+ * src/atari.rs:624-645, then 255), converted on the device.  The _async form
+ * writes into a device buffer (16-byte aligned) on `stream` (NULL: the
+ * handle's); fa_render_get_rgba converts a chunk at a time on the device and
+ * copies each into the host buffer. */
+int  fa_render_rgba_async(fa_render* r, size_t first, size_t count, uint8_t* d_rgba, void* stream);
+int  fa_render_get_rgba(fa_render* r, size_t first, size_t count, uint8_t* rgba_out);
+/* ntsc_palette (src/atari.rs:624-645) of one palette index, packed as
+ * R | G << 8 | B << 16 | 255 << 24. */
+uint32_t fa_palette_rgba(uint8_t index);
 
 /* -------------------------------------------------- no-allocation stepping
  * No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -1498,3 +1498,36 @@ uint64_t orc_rrun_batch(orc_ratari** cs, size_t n, int k, const uint8_t* actions
     free(th);
     return total;
 }
+
+/* ------------------------------------------------------------ Atari::render */
+/* Atari::render (src/atari.rs:356-369): R, G, B of ntsc_palette
+ * (src/atari.rs:624-645: 128 entries indexed by (index >> 1) & 0x7F), then 255,
+ * for each palette index of a framebuffer. */
+void orc_rgba(const uint8_t* fb, size_t pixels, uint8_t* out)
+{
+    static const uint8_t pal[128][3] = {
+        {0,0,0}, {0,0,0}, {68,68,0}, {68,68,0}, {112,40,0}, {112,40,0}, {132,24,0}, {132,24,0},
+        {136,0,0}, {136,0,0}, {120,0,92}, {120,0,92}, {72,0,120}, {72,0,120}, {20,0,132}, {20,0,132},
+        {0,0,136}, {0,0,136}, {0,0,120}, {0,0,120}, {0,0,96}, {0,0,96}, {0,20,44}, {0,20,44},
+        {0,40,0}, {0,40,0}, {0,44,0}, {0,44,0}, {0,44,0}, {0,44,0}, {0,24,0}, {0,24,0},
+        {40,40,40}, {40,40,40}, {100,100,16}, {100,100,16}, {144,72,16}, {144,72,16}, {168,56,0}, {168,56,0},
+        {184,20,0}, {184,20,0}, {160,0,116}, {160,0,116}, {100,0,164}, {100,0,164}, {48,0,176}, {48,0,176},
+        {0,0,184}, {0,0,184}, {0,24,168}, {0,24,168}, {0,44,128}, {0,44,128}, {0,60,76}, {0,60,76},
+        {0,68,0}, {0,68,0}, {0,76,0}, {0,76,0}, {0,68,0}, {0,68,0}, {0,56,0}, {0,56,0},
+        {84,84,84}, {84,84,84}, {132,132,36}, {132,132,36}, {176,100,36}, {176,100,36}, {200,80,16}, {200,80,16},
+        {220,56,20}, {220,56,20}, {196,20,144}, {196,20,144}, {132,0,200}, {132,0,200}, {80,0,212}, {80,0,212},
+        {24,0,220}, {24,0,220}, {0,48,212}, {0,48,212}, {0,76,164}, {0,76,164}, {0,92,108}, {0,92,108},
+        {0,100,0}, {0,100,0}, {0,108,0}, {0,108,0}, {0,100,16}, {0,100,16}, {0,84,0}, {0,84,0},
+        {120,120,120}, {120,120,120}, {168,168,56}, {168,168,56}, {204,136,56}, {204,136,56}, {232,112,36}, {232,112,36},
+        {252,92,40}, {252,92,40}, {232,48,172}, {232,48,172}, {168,0,232}, {168,0,232}, {112,0,244}, {112,0,244},
+        {56,0,252}, {56,0,252}, {12,76,248}, {12,76,248}, {0,108,196}, {0,108,196}, {0,128,140}, {0,128,140},
+        {0,136,0}, {0,136,0}, {0,144,0}, {0,144,0}, {0,136,40}, {0,136,40}, {0,116,0}, {0,116,0},
+    };
+    for (size_t i = 0; i < pixels; i++) {
+        const uint8_t* c = pal[(fb[i] >> 1) & 0x7F];
+        out[4 * i] = c[0];
+        out[4 * i + 1] = c[1];
+        out[4 * i + 2] = c[2];
+        out[4 * i + 3] = 255;
+    }
+}

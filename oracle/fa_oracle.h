@@ -107,6 +107,9 @@ size_t orc_state_size(void);
  * would; 1 (the default) issues them as the reference does. */
 void orc_set_phantoms(int on);
 
+/* Atari::render: RGBA (4 bytes per pixel) of `pixels` palette indices. */
+void orc_rgba(const uint8_t* fb, size_t pixels, uint8_t* out);
+
 /* ---- rendering console (src/tia.rs, src/atari.rs:107-306): one bus access per
  * CPU cycle, three TIA clocks and one PIA clock per access, 160 x 192 palette
  * index framebuffer. */

@@ -125,6 +125,7 @@ def lib() -> ctypes.CDLL:
         L.orc_rrun_batch.restype = ctypes.c_uint64
         L.orc_rrun_batch.argtypes = [ctypes.POINTER(vp), sz, ctypes.c_int, u8p, ctypes.c_int]
         L.orc_set_phantoms.argtypes = [ctypes.c_int]
+        L.orc_rgba.argtypes = [u8p, sz, u8p]
         _lib = L
     return _lib
 
@@ -290,6 +291,15 @@ def set_rom_scheme(rom: bytes, scheme) -> None:
     code = SCHEMES[scheme.lower()] if isinstance(scheme, str) else int(scheme)
     if lib().orc_rom_set_scheme(_u8(r), len(r), code) != 0:
         raise ValueError(f"scheme {scheme!r} cannot hold a {len(r)}-byte ROM")
+
+
+def rgba(fb: np.ndarray) -> np.ndarray:
+    """Atari::render of framebuffers (any shape of palette indices): the same
+    shape plus a last axis of R, G, B, A."""
+    f = np.ascontiguousarray(fb, dtype=np.uint8)
+    out = np.empty(f.shape + (4,), np.uint8)
+    lib().orc_rgba(_u8(f.reshape(-1)), f.size, _u8(out.reshape(-1)))
+    return out
 
 
 class phantoms_off:

@@ -106,3 +106,13 @@ def test_wait_limit_setting_is_bounded():
     fa.set_wait_limit_ns(0)
     assert fa.wait_limit_ns() == 0
     fa.set_wait_limit_ns(2_000_000_000)
+
+
+def test_palette_rgba_matches_the_oracle_for_every_index():
+    """fa_palette_rgba (the device's packed 64-colour table) equals the oracle's
+    restatement of ntsc_palette (src/atari.rs:624-645, 128 entries indexed by
+    (index >> 1) & 0x7F) for all 256 palette indices; two entries by hand."""
+    want = oracle.rgba(np.arange(256, dtype=np.uint8))
+    got = np.array([fa.palette_rgba(i) for i in range(256)], np.uint8)
+    assert np.array_equal(got, want)
+    assert tuple(got[0x1E]) == (20, 0, 132, 255) and tuple(got[0xFC]) == (0, 116, 0, 255)

@@ -98,3 +98,27 @@ def test_env_rewards_from_ram(spec_args):
         prev_s, prev_l = s, l
     assert saw_reward or not score
     env.close()
+
+
+def test_env_reward_table_from_file():
+    """with_reward_table picks the divergence cart's entry of the shipped table
+    by the ROM's SHA-256; rewards and flags equal those of the same spec given
+    directly."""
+    import fast_atari_b200.env as fenv
+    from fa_pkg import ROOT
+    rom = carts.divergence_cart().rom
+    n = 48
+    a = fenv.BatchAtariGpuEnv(rom, n).with_reward_table(ROOT / "fast-atari-rs_b200" / "reward_tables" / "synthetic_carts.json")
+    b = fenv.BatchAtariGpuEnv(rom, n).with_reward(fa.RewardSpec.make((3, 4, 5), True, (7, 0x0C, 2), (9, 0x80, 0x80)))
+    a.reset()
+    b.reset()
+    for action in (3, 12, 7, 17):
+        sa, sb = a.step(action), b.step(action)
+        assert np.array_equal(sa.reward.cpu().numpy(), sb.reward.cpu().numpy())
+        assert np.array_equal(sa.terminated.cpu().numpy(), sb.terminated.cpu().numpy())
+        assert np.array_equal(sa.life_lost.cpu().numpy(), sb.life_lost.cpu().numpy())
+    a.close()
+    b.close()
+    with pytest.raises(KeyError):
+        fenv.BatchAtariGpuEnv(carts.plain_cart().rom, 4).with_reward_table(
+            ROOT / "fast-atari-rs_b200" / "reward_tables" / "synthetic_carts.json")

@@ -104,3 +104,30 @@ def test_render_large_batch_copy_out():
         fb, ram = g.step_multi(acts, k)
         assert np.array_equal(g.framebuffers(), fb)
         check(fb, ram, g.states(), consoles, "1500 consoles")
+
+
+def test_rgba_output_matches_oracle_render():
+    """Atari::render on the device: fa_render_get_rgba (host buffer, converted
+    a chunk at a time on the GPU) and fa_render_rgba_async (device buffer)
+    equal the oracle's RGBA of its own framebuffers."""
+    import torch
+    rom = carts.render_cart().rom
+    n = 37
+    consoles = oracle.render_reset(rom, n)
+    with fa.AtariRender(rom, n) as g:
+        g.reset()
+        acts = carts.actions(seed=12, n=n, frames=2)
+        g.step_multi(acts, 2)
+        oracle.render_steps(consoles, acts)
+        want = oracle.rgba(np.stack([c.tia_record()["fb"] for c in consoles]))
+        got = g.rgba()
+        assert got.shape == (n, 192, 160, 4)
+        assert np.array_equal(got, want.reshape(got.shape))
+        part = g.rgba(5, 9)
+        assert np.array_equal(part, got[5:14])
+        d = torch.empty(9 * 192 * 160 * 4, dtype=torch.uint8, device="cuda")
+        g.rgba_async(5, 9, d.data_ptr())
+        g.synchronize()
+        assert np.array_equal(d.cpu().numpy().reshape(part.shape), part)
+        with pytest.raises(fa.FaError):
+            g.rgba(30, 8)
