@@ -633,8 +633,6 @@ struct Emu {
     uint32_t tw;             // vsync | vblank<<8 | wsync<<16 | frame_complete<<17 | paddle_dumped<<18
     // ---- run bookkeeping
     uint32_t instr;           // instructions executed in this launch (statistics)
-    uint32_t flim;            // the frame loop looks at VSYNC and the cycle limits once the
-                              // frame's cycle count reaches this; a VSYNC write sets it to 0
 
     // The instance's HBM rows.  Cpu::cycles, the frame counter and the run
     // status stay there and change only at frame boundaries.
@@ -722,16 +720,7 @@ struct Emu {
     }
 
     // ------------------------------------------------------------ PIA timer (pia.rs:107-166)
-    // Until the prescaler runs out the timer is a plain down-counter, so n
-    // cycles that end before that only shorten it (the reference's
-    // `remaining < timer_prescaler` branch, :122-126); everything else takes
-    // the general closed form below.
     __device__ __forceinline__ void pia_tick(uint32_t n)
-    {
-        if (ps > n && (tv != 0u || uf == 0u)) { ps -= n; return; }
-        pia_tick_general(n);
-    }
-    __device__ __forceinline__ void pia_tick_general(uint32_t n)
     {
         if (n == 0) return;
         if (tv == 0 && uf) { tv = (0xFFu - (n - 1u)) & 0xFFu; return; }
@@ -813,7 +802,6 @@ struct Emu {
         } else {
             uint2 r = tia_write_io(a, v, clock, tw, scanline | (pcnt << 16), (uint8_t*)column(), G->stride * 4u);
             tw = r.x; scanline = r.y & 0xFFFFu; pcnt = r.y >> 16;
-            if ((a & 0x3Fu) == 0u) flim = 0u;                      // VSYNC: the frame loop looks again
         }
     }
     __device__ __forceinline__ uint32_t read_low(uint32_t a, uint32_t j)   // a < 0x1000
@@ -1184,16 +1172,11 @@ struct Emu {
         // side effect.
         if (SLICED ? (a0 >= 0x1000u && (a0 & 0x3FFu) <= 0x3FDu && (a0 + 2u < 0x1FE0u || a0 > 0x1FF7u))
                    : (a0 >= 0x1000u && a0 + 2u < hot_lo)) {
-            // The three bytes from the two aligned words that hold them (the
-            // ROM image is 4 KiB aligned; the word after the last one of an
-            // image is the next image's or the RAM slabs', never used).
-            const uint32_t off = SLICED ? srom(a0) : (((bank & 7u) << 12) | (a0 & 0xFFFu));
-            const uint32_t* w = (const uint32_t*)(rom + (off & ~3u));
-            const uint32_t bytes = __funnelshift_r(w[0], w[1], (off & 3u) * 8u);
-            op = bytes & 0xFFu;
+            const uint8_t* q = SLICED ? rom + srom(a0) : rom + ((bank & 7u) << 12) + (a0 & 0xFFFu);
+            op = q[0];
             if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }
-            b1 = (bytes >> 8) & 0xFFu;
-            b2 = (bytes >> 16) & 0xFFu;
+            b1 = q[1];
+            b2 = q[2];
         } else {
             op = read(pc0, 0);
             if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }

@@ -124,24 +124,26 @@ struct Runner {
         fcyc = 0;
         e.bank &= 7u;
         phase = e.vsync_on() ? 0u : 1u;
-        e.flim = frame_limit();
         return true;
     }
 
-    // The frame's cycle count at which the checks of run_frame can first
-    // change anything without a VSYNC write: past the VSYNC budget while
-    // VSYNC is held (phase 0), past the reference's 100,000-cycle cap after it.
-    __device__ __forceinline__ uint32_t frame_limit() const
+    // One HeadlessAtari::run_one_cycle (src/atari.rs:601-614) plus the frame
+    // loop checks of run_frame (src/atari.rs:584-598).  Returns true when the
+    // lane should run again immediately (a WSYNC skip is pending).
+    __device__ __forceinline__ bool one()
     {
-        return phase == 0u ? FA_VSYNC_BUDGET + 1u : FA_FRAME_CYCLE_CAP + 1u;
-    }
-
-    // The loop conditions of run_frame (src/atari.rs:584-598) after one
-    // run_one_cycle: VSYNC only changes on a write to it, and the limits only
-    // when the cycle count reaches them, so this runs after a VSYNC write or
-    // at a limit (e.flim), never per instruction.
-    __device__ __forceinline__ bool frame_event()
-    {
+        uint32_t n;
+        if (e.wsync()) {
+            n = e.tia_skip();
+        } else {
+            n = e.step();
+            if (n == 0) { e.fold_cycles(); e.set_status(FA_STATUS_ILLEGAL_OPCODE); active = false; return false; }
+            e.instr++;
+            e.cyc_acc += n;
+            e.tia_tick(n);
+        }
+        e.pia_tick(n);
+        fcyc += n;
         if (phase == 0u) {
             if (fcyc > FA_VSYNC_BUDGET) {
                 e.fold_cycles();
@@ -161,29 +163,6 @@ struct Runner {
                 return false;
             }
         }
-        e.flim = frame_limit();
-        return e.wsync();
-    }
-
-    // One HeadlessAtari::run_one_cycle (src/atari.rs:601-614) plus the frame
-    // loop checks of run_frame.  Returns true when the lane should run again
-    // immediately (a WSYNC skip is pending).
-    __device__ __forceinline__ bool one()
-    {
-        uint32_t n;
-        if (e.wsync()) {
-            n = e.tia_skip();
-            e.pia_tick_general(n);
-        } else {
-            n = e.step();
-            if (n == 0) { e.fold_cycles(); e.set_status(FA_STATUS_ILLEGAL_OPCODE); active = false; return false; }
-            e.instr++;
-            e.cyc_acc += n;
-            e.tia_tick(n);
-            e.pia_tick(n);
-        }
-        fcyc += n;
-        if (fcyc >= e.flim) return frame_event();
         return e.wsync();
     }
 
@@ -306,7 +285,6 @@ __device__ __forceinline__ void run_unit_as(const FaGroup& G, uint32_t first, ui
     r.e.hot_lo = G.hot_lo;
     r.e.nbanks = G.nbanks;
     r.e.instr = 0;
-    r.e.flim = 0;
     r.e.cyc_acc = 0;
     r.e.pc = 0;
     r.e.bank = 0;

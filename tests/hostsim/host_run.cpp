@@ -15,7 +15,7 @@ static void run_one(const FaGroup& G, uint32_t i, uint8_t* rom, unsigned long lo
     r.f = 0; r.phase = 0; r.fcyc = 0; r.active = false;
     r.e.pv = (uint8_t*)priv;
     r.e.G = &G; r.e.i = i; r.e.rom = rom; r.e.hot_lo = G.hot_lo; r.e.nbanks = G.nbanks;
-    r.e.instr = 0; r.e.flim = 0; r.e.cyc_acc = 0; r.e.pc = 0; r.e.bank = 0; r.e.slices = 0; r.e.scanline = 0;
+    r.e.instr = 0; r.e.cyc_acc = 0; r.e.pc = 0; r.e.bank = 0; r.e.slices = 0; r.e.scanline = 0;
     uint32_t* col = G.state + i;
     r.e.load_ram(col, G.stride);
     r.e.load_hot(col, G.stride);

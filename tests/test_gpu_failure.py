@@ -6,8 +6,8 @@ hanging the device.
   the oracle does.
 * A cart that holds VSYNC: the reference waits for it to drop forever
   (src/atari.rs:588-590); this library halts the instance after 2,000,000
-  cycles with FA_STATUS_VSYNC_BUDGET, as the oracle does, and later frames
-  leave it untouched.
+  cycles with FA_STATUS_VSYNC_BUDGET, as the oracle does; later frames run
+  nothing, and only their set_action reaches its inputs.
 * The device-side bound on the ROM staging wait set to 0 (give up at once),
   through the handle's warp-granular kernel, the CTA-granular kernel (a
   pool whose ROM library does not fit in shared memory), the rendering
@@ -78,8 +78,15 @@ def test_vsync_held_cart_halts_with_budget_status():
         assert_states_equal(st, ref, "budget frame")
         assert (st["run_status"] & STATUS_VSYNC_BUDGET).all()
         assert (st["cycles"] > 1_000_000).all()
-        g.step_multi(acts[1:], 2)                           # halted: later frames change nothing
-        assert_states_equal(g.download_states(), st, "after halt")
+        # Halted: later frames run nothing; only set_action reaches the inputs.
+        g.step_multi(acts[1:], 2)
+        oracle.run_batch(rom, ref, acts[1:], 2)
+        after = g.download_states()
+        assert_states_equal(after, ref, "after halt")
+        inputs = {"port_a_input", "inpt4", "paddle0"}
+        for name in oracle.COMPARED_FIELDS:
+            if name not in inputs:
+                assert np.array_equal(after[name], st[name]), name
         assert (g.status() & STATUS_VSYNC_BUDGET).all()
 
 
