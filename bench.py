@@ -25,7 +25,7 @@ uniformly, a batch size lognormal (median 256, sigma 1) clipped to
 16..16,384 and K uniform in 1..8.  The peak is the sustained completion rate
 of a saturation run (every request queued at once, first arrival to last
 completion); at 20/40/70/100% of it each level reports achieved / offered
-(the completion rate with the final drain taken out) and the growth of the
+(the completion rate in the middle 80% of the arrival window) and the growth of the
 median latency from the first to the last third of the arrivals (kept up:
 at least 0.95 and under 1.5), p50/p99 step latency and its parts (waiting for
 the same session's earlier requests, dispatch, service), per (cart, K) at
@@ -188,15 +188,19 @@ def serve_measure(fa, carts, sat_requests, level_requests, plain_requests, level
         out["launches"] = st1["launches"] - st0["launches"]
         for frac in levels:
             r, rec = srv.loadgen(requests=level_requests, offered_frames_per_s=frac * peak, seed=2)
-            # The run's completion rate counts the drain after the last arrival
-            # (about one latency), which a short run overweights; take it out.
-            # A server that keeps up also shows no growth of latency over the run.
+            # Achieved rate: the instance-frames of the requests that complete
+            # inside the middle 80% of the arrival window, over that span (the
+            # start and the drain after the last arrival left out).  A server
+            # that keeps up also shows no growth of latency over the run.
             order = np.argsort(rec["arrival_s"])
             third = max(1, len(order) // 3)
             growth = (np.median(rec["latency_ms"][order[-third:]]) /
                       max(1e-9, np.median(rec["latency_ms"][order[:third]])))
-            busy_s = max(1e-9, r["elapsed_s"] - np.median(rec["latency_ms"]) * 1e-3)
-            achieved = (r["instance_frames"] / busy_s) / r["offered_frames_per_s"]
+            w = r["arrival_window_s"]
+            done_at = rec["arrival_s"] + rec["latency_ms"] * 1e-3
+            mid = (done_at >= 0.1 * w) & (done_at <= 0.9 * w)
+            frames_mid = float((rec["n"][mid].astype(np.float64) * rec["k"][mid]).sum())
+            achieved = (frames_mid / max(1e-9, 0.8 * w)) / r["offered_frames_per_s"]
             out["levels"].append({"load": frac, "offered_frames_per_s": r["offered_frames_per_s"],
                                   "frames_per_s": r["frames_per_s"], "achieved_over_offered": achieved,
                                   "latency_growth": float(growth),
@@ -299,7 +303,7 @@ def ref_kernel_compare(fa, carts, n=50_000, frames=16):
     r = np.frombuffer(rom, np.uint8).copy()
 
     def ref_ms(multi, nn, a):
-        st = np.ascontiguousarray(ref_st[:nn])
+        st = ref_st[:nn].copy()                                      # ref_run writes the states back
         obs = np.empty((nn, 128), np.uint8)
         ms = ctypes.c_float()
         rc = L.ref_run(r.ctypes.data, len(r), st.ctypes.data, nn, np.ascontiguousarray(a).ctypes.data,
@@ -389,6 +393,31 @@ def run_micro_arm(args, fa, carts, rank, world, local_rank):
             "micro": {kk: {k2: round(v2, 2) for k2, v2 in v.items()} for kk, v in kinds.items()}}
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def unit_trace_summary(tr, names, bins=20):
+    """Per-unit records of one batched call (fa_pool_set_trace): per cart the
+    latest start and the median and last finish (ms from the call's first
+    start), and the warps still running and SMs busy at `bins` points."""
+    tr = tr[tr[:, 1] > 0]
+    if tr.size == 0:
+        return None
+    t0 = tr[:, 0].min()
+    start = (tr[:, 0] - t0).astype(np.float64) / 1e6
+    end = (tr[:, 1] - t0).astype(np.float64) / 1e6
+    tag = (tr[:, 2] & np.uint64(0xFFFF)).astype(int)
+    sm = (tr[:, 2] >> np.uint64(32)).astype(int)
+    out = {"call_ms": round(float(end.max()), 3), "carts": {}}
+    for g, name in enumerate(names):
+        m = tag == g
+        if m.any():
+            out["carts"][name] = {"units": int(m.sum()), "start_max_ms": round(float(start[m].max()), 3),
+                                  "end_p50_ms": round(float(np.median(end[m])), 3),
+                                  "end_max_ms": round(float(end[m].max()), 3)}
+    pts = np.linspace(0.0, float(end.max()), bins + 1)[:-1]
+    out["warps_running"] = [int(((start <= t) & (end > t)).sum()) for t in pts]
+    out["sms_busy"] = [int(np.unique(sm[(start <= t) & (end > t)]).size) for t in pts]
+    return out
 
 
 # ------------------------------------------------------------------ clocks
@@ -649,6 +678,19 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
     frames = n_total * k * args.steps * world
     value = frames / (total_ms / 1e3)
 
+    # ---- one more batched call with per-unit records: when each cart's
+    # warps finish, and how many warps run as the call drains
+    unit_trace = None
+    if world == 1:
+        nu = sum((n + 31) // 32 for _, n in spec)
+        d_tr = torch.zeros(nu * 3, dtype=torch.int64, device=dev)
+        pool.set_trace(d_tr.data_ptr(), nu)
+        pool.step_async(acts_at(args.warmup), k, obs_ptrs, sptr)
+        pool.synchronize()
+        pool.set_trace()
+        unit_trace = unit_trace_summary(d_tr.cpu().numpy().view(np.uint64).reshape(nu, 3),
+                                        [c.spec.name for c, _ in spec])
+
     # ---- the plain kernel on the same trace (one launch per frame per cart)
     plain_value = None
     if not args.no_plain:
@@ -729,6 +771,7 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
         "guest_instructions_per_s": guest_per_s,
         "guest_instructions_per_step": instr / args.steps,
         "lane_efficiency": instr / slots if slots else None,
+        "unit_trace": unit_trace,
     }
     if world == 1 and args.workload == "divergence":
         line["policies"] = divergence_policies(fa, carts)

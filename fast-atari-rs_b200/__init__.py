@@ -100,6 +100,8 @@ _SIGS = {
     "fa_pool_step_async": (_i, [_vp, _vp, _i, _vp, _vp]),
     "fa_pool_step_plain_async": (_i, [_vp, _vp, _i, _vp, _vp]),
     "fa_pool_synchronize": (_i, [_vp]),
+    "fa_pool_set_balance": (_i, [_vp, _i]),
+    "fa_pool_set_trace": (_i, [_vp, _vp, ctypes.c_uint32]),
     "fa_pool_reset_counters": (_i, [_vp]),
     "fa_pool_last_instructions": (ctypes.c_ulonglong, [_vp]),
     "fa_pool_last_lane_slots": (ctypes.c_ulonglong, [_vp]),
@@ -477,6 +479,17 @@ class AtariPool:
 
     def reset_counters(self) -> None:
         _check(lib().fa_pool_reset_counters(self._p))
+
+    def set_balance(self, on: bool = True) -> None:
+        """Spread the persistent launch's first wave over the warp schedulers
+        by cart weight (on by default)."""
+        _check(lib().fa_pool_set_balance(self._p, 1 if on else 0))
+
+    def set_trace(self, d_trace: int = 0, cap: int = 0) -> None:
+        """Per-unit records of later batched launches into a device buffer of
+        cap x 3 uint64 (start ns, end ns, smid << 32 | warp << 16 | group);
+        set_trace() stops them."""
+        _check(lib().fa_pool_set_trace(self._p, _vp(d_trace or None), int(cap)))
 
     def last_instructions(self) -> int:
         return int(lib().fa_pool_last_instructions(self._p))

@@ -71,10 +71,10 @@ __device__ __forceinline__ uint32_t mod160(int v)
 __device__ __forceinline__ uint32_t cold_off(uint32_t o, uint32_t stride4) { return (o >> 2) * stride4 + (o & 3u); }
 
 // TIA or PIA register read (HeadlessTia::read, src/headless_tia.rs:205-223;
-// Pia::read I/O half, src/pia.rs:169-199).  Bit 8 of the result asks the
-// caller to clear the timer underflow flag (an INTIM read).
+// Pia::read I/O half, src/pia.rs:169-199), INTIM apart (pia_intim_io):
+// sel_uf carries the timer's underflow flag in bits 16 and up.
 static __device__ __noinline__ uint32_t io_read(uint32_t a, uint32_t pcnt, uint32_t pins, uint32_t pads,
-                                         uint32_t ports, uint32_t timer, const uint8_t* col, uint32_t stride4)
+                                         uint32_t ports, uint32_t sel_uf, const uint8_t* col, uint32_t stride4)
 {
     if (a & 0x80u) {                                                 // PIA: (a & 0x280) == 0x280
         switch (a & 7u) {
@@ -82,8 +82,7 @@ static __device__ __noinline__ uint32_t io_read(uint32_t a, uint32_t pcnt, uint3
         case 1: return (ports >> 8) & 0xFFu;
         case 2: return (((pins >> 8) & ~(ports >> 24)) | ((ports >> 16) & (ports >> 24))) & 0xFFu;
         case 3: return ports >> 24;
-        case 4: return (timer & 0xFFu) | 0x100u;
-        case 5: return (timer >> 16) ? 0x80u : 0u;
+        case 5: return (sel_uf >> 16) ? 0x80u : 0u;
         default: return 0u;
         }
     }
@@ -175,23 +174,62 @@ static __device__ __noinline__ uint4 pia_write_io(uint32_t a, uint32_t v, uint32
 struct RState {
     uint32_t clock, scanline, tw, pcnt, vtop;   // beam, TIA flags, paddle counter, visible_top | vblank_top << 16
     uint32_t rx;                                // the current line's pixels are drawn up to this clock
-    uint32_t pix, pmask, pword;                 // framebuffer word being assembled
+    uint32_t sc;                                // the framebuffer sector (32 pixels) whose pixels the sector buffer holds
+    uint32_t zr;                                // rows written since the clear point | R_ZPEND (rows after them not yet zeroed)
     uint32_t tv, ps, sel, uf;                   // PIA timer
 };
+constexpr uint32_t R_ZPEND = 0x100u;
 
 static __device__ __forceinline__ uint32_t rp8(const uint8_t* pv, uint32_t o) { return pv[(o & ~3u) * 32u + (o & 3u)]; }
 static __device__ __forceinline__ void wp8(uint8_t* pv, uint32_t o, uint32_t v) { pv[(o & ~3u) * 32u + (o & 3u)] = (uint8_t)v; }
 static __device__ __forceinline__ uint32_t rp16(const uint8_t* pv, uint32_t o) { return *(const uint16_t*)(pv + (o & ~3u) * 32u + (o & 3u)); }
 static __device__ __forceinline__ void wp16(uint8_t* pv, uint32_t o, uint32_t v) { *(uint16_t*)(pv + (o & ~3u) * 32u + (o & 3u)) = (uint16_t)v; }
 
-static __device__ void render_fb_flush(uint32_t pix, uint32_t pmask, uint32_t pword, uint8_t* fbp)
+// ---- framebuffer writes through a one-sector buffer
+// Pixels of a line are drawn left to right, so a console stages the 32
+// pixels of the framebuffer sector it is drawing (8 words after its private
+// bytes in its shared-memory slab) and writes each sector whole, with two
+// 16-byte stores, when the drawing moves past it: every sector of a visible
+// row is written once, with zeros where nothing was drawn.  The reference
+// clears the framebuffer where the visible area starts (tia.rs:349-351);
+// here the rows are written as the beam completes them, and the rows the
+// frame has not reached are zeroed when the framebuffer can next be seen
+// (VSYNC, the end of a frame, the end of a call).
+static __device__ __forceinline__ uint32_t* r_sbuf(uint8_t* pv, uint32_t k)
 {
-    if (!pmask) return;
-    uint32_t* w = (uint32_t*)fbp + pword;
-    if (pmask == 0xFu) { *w = pix; return; }
-    uint32_t keep = 0;
-    for (uint32_t b = 0; b < 4u; b++) keep |= ((pmask >> b) & 1u) ? 0u : (0xFFu << (8u * b));
-    *w = (*w & keep) | pix;
+    return (uint32_t*)(pv + (FA_RPRIV_BYTES + 4u * k) * 32u);
+}
+static __device__ __forceinline__ void r_sec_write(uint8_t* pv, uint8_t* fbp, uint32_t sc)
+{
+    uint4* d = (uint4*)(fbp + (size_t)sc * 32u);
+    d[0] = make_uint4(*r_sbuf(pv, 0), *r_sbuf(pv, 1), *r_sbuf(pv, 2), *r_sbuf(pv, 3));
+    d[1] = make_uint4(*r_sbuf(pv, 4), *r_sbuf(pv, 5), *r_sbuf(pv, 6), *r_sbuf(pv, 7));
+}
+static __device__ __forceinline__ void r_sec_clear(uint8_t* pv)
+{
+#pragma unroll
+    for (uint32_t k = 0; k < 8u; k++) *r_sbuf(pv, k) = 0u;
+}
+static __device__ __forceinline__ void r_zero_sectors(uint8_t* fbp, uint32_t from, uint32_t to)   // [from, to)
+{
+    uint4* d = (uint4*)fbp;
+    for (uint32_t q = 2u * from; q < 2u * to; q++) d[q] = make_uint4(0u, 0u, 0u, 0u);
+}
+// The buffer moves on to sector t: the sector it held is written, the ones
+// skipped between become zeros.
+static __device__ void r_seek(uint32_t& sc, uint8_t* pv, uint8_t* fbp, uint32_t t)
+{
+    r_sec_write(pv, fbp, sc);
+    if (t > sc) {
+        r_zero_sectors(fbp, sc + 1u, t);
+        r_sec_clear(pv);
+    } else {                                                         // not reached by drawing order; kept exact
+        const uint4* q = (const uint4*)(fbp + (size_t)t * 32u);
+        const uint4 u0 = q[0], u1 = q[1];
+        *r_sbuf(pv, 0) = u0.x; *r_sbuf(pv, 1) = u0.y; *r_sbuf(pv, 2) = u0.z; *r_sbuf(pv, 3) = u0.w;
+        *r_sbuf(pv, 4) = u1.x; *r_sbuf(pv, 5) = u1.y; *r_sbuf(pv, 6) = u1.z; *r_sbuf(pv, 7) = u1.w;
+    }
+    sc = t;
 }
 
 // Bits 0..7 of b, each repeated over two bits.
@@ -277,9 +315,10 @@ static __device__ __forceinline__ uint32_t r_missile_mask(const uint8_t* pv, uin
 // and the object tests (tia.rs:406-507), over a span in which no register
 // changes.  Each object is a bit mask over 32 pixels at a time; the
 // collision latches are the masks' intersections, and the priority of
-// compute_pixel is the order in which the colors are laid down.  Pixels go
-// to the framebuffer four to a word; a word that the span leaves partly
-// written stays in s.pix / s.pmask for the next span.
+// compute_pixel is the order in which the colors are laid down.  Each
+// 32-pixel chunk is one framebuffer sector: its pixels go into the sector
+// buffer four to a word, and the buffer is written out when the drawing
+// moves to another sector (r_seek).
 static __device__ __noinline__ RState r_span(RState s, uint8_t* pv, uint8_t* fbp, uint32_t vis, uint32_t x0, uint32_t x1)
 {
     const uint32_t ctrlpf = rp8(pv, PB_CTRLPF);
@@ -310,6 +349,8 @@ static __device__ __noinline__ RState r_span(RState s, uint8_t* pv, uint8_t* fbp
         const uint32_t cpf = rp8(pv, PB_COLUPF);
         const uint32_t tl = cbk | (((ctrlpf & 2u) ? c0 : cpf) << 8) | (c1 << 16) | (c0 << 24);   // x < 80 (score mode)
         const uint32_t tr = cbk | (((ctrlpf & 2u) ? c1 : cpf) << 8) | (c1 << 16) | (c0 << 24);
+        const uint32_t t = vis * (FA_FB_W / 32u) + (X >> 5);            // the chunk is one framebuffer sector
+        if (t != s.sc) r_seek(s.sc, pv, fbp, t);
         for (uint32_t q = lo >> 2; q < (hi + 3u) >> 2; q++) {
             const uint32_t x = X + 4u * q;
             // Four pixels' indices as a byte-permute selector, one nibble each.
@@ -317,17 +358,13 @@ static __device__ __noinline__ RState r_span(RState s, uint8_t* pv, uint8_t* fbp
             const uint32_t w = __byte_perm(x < 80u ? tl : tr, 0u, sel);
             const uint32_t wl = lo > 4u * q ? lo - 4u * q : 0u, wh = hi < 4u * q + 4u ? hi - 4u * q : 4u;
             const uint32_t pm = ((1u << wh) - 1u) & ~((1u << wl) - 1u);
-            const uint32_t word = (vis * FA_FB_W + x) >> 2;
-            if (word != s.pword || !s.pmask) {
-                render_fb_flush(s.pix, s.pmask, s.pword, fbp);
-                s.pmask = 0;
-                s.pword = word;
-                s.pix = 0;
+            uint32_t* bp = r_sbuf(pv, q);
+            if (pm == 0xFu) {
+                *bp = w;
+            } else {
+                const uint32_t bm = r_bytes(pm);
+                *bp = (*bp & ~bm) | (w & bm);
             }
-            const uint32_t bm = r_bytes(pm);
-            s.pix = (s.pix & ~bm) | (w & bm);
-            s.pmask |= pm;
-            if (wh == 4u) { render_fb_flush(s.pix, s.pmask, s.pword, fbp); s.pmask = 0; }
         }
     }
     if (cx) {                                                        // collision latches (tia.rs:329-343)
@@ -351,6 +388,23 @@ static __device__ __forceinline__ void r_pending(RState& s, uint8_t* pv, uint8_t
     if (upto <= from || (s.tw & 0x200u)) return;
     const uint32_t vis = (s.scanline - (s.vtop & 0xFFFFu)) & 0xFFFFu;
     if (vis < FA_FB_H) s = r_span(s, pv, fbp, vis, from - 68u, upto - 68u);
+}
+
+// The framebuffer as the reference would show it now (the pixels up to the
+// beam are already drawn): the beam's row as far as drawn, with zeros after,
+// and, once after each clear point, zeros in the rows the beam has not reached.
+static __device__ __forceinline__ void r_observe(RState& s, uint8_t* pv, uint8_t* fbp)
+{
+    const uint32_t vis = (s.scanline - (s.vtop & 0xFFFFu)) & 0xFFFFu;
+    constexpr uint32_t SPR = FA_FB_W / 32u, NSEC = FA_FB_H * SPR;   // sectors per row, in all
+    if (vis < FA_FB_H) {
+        r_sec_write(pv, fbp, s.sc);
+        r_zero_sectors(fbp, s.sc + 1u, (vis + 1u) * SPR);
+        if (s.zr & R_ZPEND) r_zero_sectors(fbp, (vis + 1u) * SPR, NSEC);
+    } else if (s.zr & R_ZPEND) {
+        r_zero_sectors(fbp, (s.zr & 0xFFu) * SPR, NSEC);
+    }
+    s.zr &= ~R_ZPEND;
 }
 
 // n TIA clocks, exactly as n calls of Tia::tick (tia.rs:271-372), advanced a
@@ -382,14 +436,19 @@ static __device__ __forceinline__ void r_advance(RState& s, uint32_t n, uint32_t
         n -= seg;
         if (s.clock >= 228u) {
             r_pending(s, pv, fbp, 228u);
+            const uint32_t vis = (s.scanline - (s.vtop & 0xFFFFu)) & 0xFFFFu;
+            if (vis < FA_FB_H) {                                     // the row is complete: written whole
+                r_seek(s.sc, pv, fbp, (vis + 1u) * (FA_FB_W / 32u));
+                s.zr = (s.zr & R_ZPEND) | (vis + 1u);
+            }
             s.clock = 0;
             s.rx = 0;
             s.scanline = (s.scanline + 1u) & 0xFFFFu;
             s.tw &= ~(TW_WSYNC | TW_HMOVE);
             if (s.scanline == (s.vtop & 0xFFFFu)) {                  // framebuffer cleared (tia.rs:349-351)
-                s.pmask = 0;
-                uint4* w = (uint4*)fbp;
-                for (uint32_t q = 0; q < FA_FB_BYTES / 16u; q++) w[q] = make_uint4(0u, 0u, 0u, 0u);
+                s.sc = 0;
+                r_sec_clear(pv);
+                s.zr = R_ZPEND;
             }
             if (!(s.tw & TW_PDUMP) && s.pcnt < 256u) s.pcnt++;
             if (s.scanline >= 262u) { s.scanline = 0; s.tw |= TW_FCOMP; }
@@ -397,10 +456,12 @@ static __device__ __forceinline__ void r_advance(RState& s, uint32_t n, uint32_t
     }
 }
 
-// The pending pixels of the current line, up to the beam.
-static __device__ __noinline__ RState render_pending(RState s, uint8_t* pv, uint8_t* fbp)
+// The pending pixels of the current line, up to the beam, then the
+// framebuffer as it can be seen now.
+static __device__ __noinline__ RState render_observe(RState s, uint8_t* pv, uint8_t* fbp)
 {
     r_pending(s, pv, fbp, s.clock);
+    r_observe(s, pv, fbp);
     return s;
 }
 
@@ -475,7 +536,7 @@ static __device__ __forceinline__ void r_write(uint32_t a, uint32_t v, RState& s
     if ((R_PIXEL_REGS >> (a & 0x3Fu)) & 1u) r_pending(s, pv, fbp, s.clock);   // the pixels drawn before the write
     switch (a & 0x3Fu) {
     case 0x00:
-        if (!(s.tw & 2u) && (v & 2u)) { r_resize_commit(s, pv); s.scanline = 0; s.tw |= TW_FCOMP; }
+        if (!(s.tw & 2u) && (v & 2u)) { r_observe(s, pv, fbp); r_resize_commit(s, pv); s.scanline = 0; s.tw |= TW_FCOMP; }
         s.tw = (s.tw & ~0xFFu) | v;
         break;
     case 0x01:
@@ -608,6 +669,91 @@ static __device__ __noinline__ RRead render_io_read(uint32_t a, uint32_t owed, R
     return out;
 }
 
+// ---------------------------------------------------------------- PIA timer (pia.rs:107-166)
+// Pia::tick_n on the unpacked timer: value, prescaler, interval, underflow.
+static __device__ __forceinline__ void pia_tick_n(uint32_t& tv, uint32_t& ps, uint32_t sel, uint32_t& uf, uint32_t n)
+{
+    if (n == 0) return;
+    if (tv == 0 && uf) { tv = (0xFFu - (n - 1u)) & 0xFFu; return; }
+    uint32_t rem = n;
+    if (ps > 0) {
+        if (rem < ps) { ps -= rem; return; }
+        rem -= ps;
+        ps = 0;
+        if (tv == 0) {
+            uf = 1;
+            tv = rem ? ((0xFFu - (rem - 1u)) & 0xFFu) : 0xFFu;
+            return;
+        }
+        tv -= 1u;
+    }
+    if (rem == 0) { ps = sel; return; }
+    uint32_t full, left;
+    if ((sel & (sel - 1u)) == 0) {                    // 1, 8, 64, 1024
+        uint32_t sh = __ffs(sel) - 1u;
+        full = rem >> sh;
+        left = rem & (sel - 1u);
+    } else {
+        full = rem / sel;
+        left = rem % sel;
+    }
+    if (full >= tv) {
+        rem = (rem - ((tv * sel) & 0xFFFFu)) & 0xFFFFu;   // u16 arithmetic as in the reference
+        uf = 1;
+        tv = rem ? ((0xFFu - (rem - 1u)) & 0xFFu) : 0xFFu;
+    } else {
+        tv -= full;
+        ps = sel - left;
+    }
+}
+
+// Headless timer bookkeeping (Emu::pia_count).  The window of a timer state
+// is the run of cycles over which tick_n only counts.  With tv >= 1 it ends
+// at the decrement that brings tv to zero: ps (a prescaler of 0, just after
+// an underflow, counts as a whole interval: tick_n then decrements after sel
+// cycles) plus tv - 1 intervals.  With tv = 0, no underflow flag and a
+// prescaler left, it ends when the prescaler runs out (that decrement
+// underflows).  Any other state, an interval that is not one of 1, 8, 64,
+// 1024, or a prescaler above the interval (states only an upload makes)
+// have no window: 0, every call exact.
+static __device__ __forceinline__ uint32_t pia_span_of(uint32_t tv, uint32_t ps, uint32_t sel, uint32_t uf)
+{
+    if (sel == 0u || (sel & (sel - 1u)) != 0u || sel > 1024u || ps > sel) return 0u;
+    if (tv == 0u) return uf ? 0u : ps;
+    return (ps ? ps : sel) + ((tv - 1u) << (__ffs(sel) - 1u));
+}
+// (tv, ps) with the counted cycles (the window less tlim) applied: fewer
+// cycles than the window, so tick_n's counting branches alone apply.
+static __device__ __forceinline__ uint2 pia_now_of(uint32_t tv, uint32_t ps, uint32_t sel, uint32_t uf, uint32_t tlim)
+{
+    const uint32_t e = pia_span_of(tv, ps, sel, uf) - tlim;
+    if (e == 0u) return make_uint2(tv, ps);
+    const uint32_t p0 = ps ? ps : sel;
+    if (e < p0) return make_uint2(tv, p0 - e);
+    const uint32_t k = e - p0;
+    return make_uint2(tv - 1u - (k >> (__ffs(sel) - 1u)), sel - (k & (sel - 1u)));
+}
+// An INTIM read (pia.rs:187-190): the counted cycles settled, the underflow
+// flag cleared (tv = 0 with a prescaler left may gain a window by it).
+// Packed (tv | ps << 16, sel | uf << 16, tlim); the value read is tv & 0xFF.
+static __device__ __noinline__ uint4 pia_intim_io(uint32_t tv_ps, uint32_t sel_uf, uint32_t tlim)
+{
+    const uint32_t sel = sel_uf & 0xFFFFu;
+    const uint2 t = pia_now_of(tv_ps & 0xFFFFu, tv_ps >> 16, sel, sel_uf >> 16, tlim);
+    return make_uint4(t.x | (t.y << 16), sel, pia_span_of(t.x, t.y, sel, 0u), 0u);
+}
+// Packed (tv | ps << 16, sel | uf << 16, tlim) after settling and one exact
+// call of n cycles.
+static __device__ __noinline__ uint4 pia_sync_io(uint32_t tv_ps, uint32_t sel_uf, uint32_t tlim, uint32_t n)
+{
+    const uint32_t sel = sel_uf & 0xFFFFu;
+    uint32_t uf = sel_uf >> 16;
+    const uint2 t = pia_now_of(tv_ps & 0xFFFFu, tv_ps >> 16, sel, uf, tlim);
+    uint32_t tv = t.x, ps = t.y;
+    pia_tick_n(tv, ps, sel, uf, n);
+    return make_uint4(tv | (ps << 16), sel | (uf << 16), pia_span_of(tv, ps, sel, uf), 0u);
+}
+
 template <int BLOCK, bool RENDER = false, bool SLICED = false>
 struct Emu {
     // ---- placement
@@ -622,9 +768,12 @@ struct Emu {
                              // saturating at 511: the count is a scheduling key only
     uint32_t slices;         // SLICED (E0, 3F carts): the 1K ROM slice of window k in byte k
     uint32_t cyc_acc;         // instruction cycles not yet added to Cpu::cycles in HBM
-    // ---- PIA (src/pia.rs:26-44): timer unpacked (ticked every instruction),
-    //      ports and input pins packed (touched only by I/O accesses)
-    uint32_t tv, ps, sel, uf;
+    // ---- PIA (src/pia.rs:26-44): timer unpacked, ports and input pins packed
+    //      (touched only by I/O accesses)
+    uint32_t tp;             // timer value | prescaler << 16 (the R_TIMER row word)
+    uint32_t su;             // interval (1, 8, 64, 1024) | underflow flag << 16
+    uint32_t tlim;           // headless: cycles the timer may still count before an exact tick
+                             // (tp lags by pia_span() - tlim counted cycles; see pia_count)
     uint32_t ports;          // pa_out | pa_ddr<<8 | pb_out<<16 | pb_ddr<<24
     uint32_t pins;           // pa_in | pb_in<<8 | inpt4<<16 | inpt5<<17
     uint32_t pads;           // paddle0 | paddle1<<8
@@ -722,38 +871,59 @@ struct Emu {
     // ------------------------------------------------------------ PIA timer (pia.rs:107-166)
     __device__ __forceinline__ void pia_tick(uint32_t n)
     {
-        if (n == 0) return;
-        if (tv == 0 && uf) { tv = (0xFFu - (n - 1u)) & 0xFFu; return; }
-        uint32_t rem = n;
-        if (ps > 0) {
-            if (rem < ps) { ps -= rem; return; }
-            rem -= ps;
-            ps = 0;
-            if (tv == 0) {
-                uf = 1;
-                tv = rem ? ((0xFFu - (rem - 1u)) & 0xFFu) : 0xFFu;
-                return;
-            }
-            tv -= 1u;
+        uint32_t tv = tp & 0xFFFFu, ps = tp >> 16, uf = su >> 16;
+        pia_tick_n(tv, ps, su & 0xFFFFu, uf, n);
+        tp = tv | (ps << 16);
+        su = (su & 0xFFFFu) | (uf << 16);
+    }
+
+    // Headless consoles tick the timer once per instruction, with the
+    // instruction's cycles (atari.rs:497-552).  Until a call makes the
+    // decrement that brings the value to zero, or is made with the value at
+    // zero, Pia::tick_n only counts, and consecutive calls add up: tick_n(a)
+    // then tick_n(b) leaves what tick_n(a + b) leaves.  So an instruction
+    // only takes its cycles off tlim, the cycles left before such a call;
+    // the call that reaches it runs exactly through pia_tick, and the
+    // counted cycles are folded into tp (pia_settle) before INTIM is
+    // read, a PIA register is written or the state is stored.
+    __device__ __forceinline__ uint32_t pia_span() const { return pia_span_of(tp & 0xFFFFu, tp >> 16, su & 0xFFFFu, su >> 16); }
+    __device__ __forceinline__ uint2 pia_now() const { return pia_now_of(tp & 0xFFFFu, tp >> 16, su & 0xFFFFu, su >> 16, tlim); }
+    // Fold the counted cycles in, run one exact call of n cycles (none for
+    // n = 0), and open the next window: one out-of-line copy.
+    __device__ __forceinline__ void pia_sync(uint32_t n)
+    {
+        const uint4 r = pia_sync_io(tp, su, tlim, n);
+        tp = r.x;
+        su = r.y;
+        tlim = r.z;
+    }
+    __device__ __forceinline__ void pia_settle() { pia_sync(0u); }
+    // An INTIM read: the counted cycles settled, the underflow flag cleared.
+    __device__ __forceinline__ void pia_intim()
+    {
+        const uint4 r = pia_intim_io(tp, su, tlim);
+        tp = r.x; su = r.y; tlim = r.z;
+    }
+    __device__ __forceinline__ void pia_count(uint32_t n)
+    {
+        if (n < tlim) { tlim -= n; return; }
+        // The call reaches the end of the window.  tick_n then underflows: uf
+        // set, prescaler 0, and the o cycles past the window counted one per
+        // cycle from $FF ($FF itself when o is 0).  That holds whatever the
+        // state at the call when o > 0.  When o is 0 it needs a window that
+        // began at tv = 0, or tv >= 2 at the call (with tv 1 and a prescaler
+        // left, the call only empties the prescaler), which tlim > sel
+        // guarantees.  Anything else runs exactly.
+        const uint32_t sel = su & 0xFFFFu;
+        if (tlim != 0u && (n > tlim || tlim > sel || (tp & 0xFFFFu) == 0u)) {
+            const uint32_t o = n - tlim;
+            const uint32_t tv = o ? (0u - o) & 0xFFu : 0xFFu;
+            tp = tv;
+            su = sel | 0x10000u;
+            tlim = tv << (__ffs(sel) - 1u);
+            return;
         }
-        if (rem == 0) { ps = sel; return; }
-        uint32_t full, left;
-        if ((sel & (sel - 1u)) == 0) {                    // 1, 8, 64, 1024
-            uint32_t sh = __ffs(sel) - 1u;
-            full = rem >> sh;
-            left = rem & (sel - 1u);
-        } else {
-            full = rem / sel;
-            left = rem % sel;
-        }
-        if (full >= tv) {
-            rem = (rem - ((tv * sel) & 0xFFFFu)) & 0xFFFFu;   // u16 arithmetic as in the reference
-            uf = 1;
-            tv = rem ? ((0xFFu - (rem - 1u)) & 0xFFu) : 0xFFu;
-        } else {
-            tv -= full;
-            ps = sel - left;
-        }
+        pia_sync(n);
     }
 
     // ------------------------------------------------------------ bus
@@ -779,9 +949,11 @@ struct Emu {
             done = j + 1u;
             return r.v;
         } else {
-            uint32_t r = io_read(a, pcnt, pins, pads, ports, tv | (uf << 16), (const uint8_t*)column(), G->stride * 4u);
-            if (r & 0x100u) uf = 0;                                 // INTIM read clears the flag
-            return r & 0xFFu;
+            if ((a & 0x87u) == 0x84u) {                             // INTIM: settles and clears the flag
+                pia_intim();
+                return tp & 0xFFu;
+            }
+            return io_read(a, pcnt, pins, pads, ports, su, (const uint8_t*)column(), G->stride * 4u);
         }
     }
     __device__ __forceinline__ void io_write(uint32_t a, uint32_t v, uint32_t j)  // TIA or PIA register write
@@ -797,8 +969,10 @@ struct Emu {
             }
             done = j + 1u;
         } else if (a & 0x200u) {
-            uint4 r = pia_write_io(a, v, ports, tv, ps, sel | (uf << 16));
-            ports = r.x; tv = r.y; ps = r.z; sel = r.w & 0xFFFFu; uf = r.w >> 16;
+            pia_settle();
+            uint4 r = pia_write_io(a, v, ports, tp & 0xFFFFu, tp >> 16, su);
+            ports = r.x; tp = r.y | (r.z << 16); su = r.w;
+            tlim = pia_span();
         } else {
             uint2 r = tia_write_io(a, v, clock, tw, scanline | (pcnt << 16), (uint8_t*)column(), G->stride * 4u);
             tw = r.x; scanline = r.y & 0xFFFFu; pcnt = r.y >> 16;
@@ -844,7 +1018,7 @@ struct Emu {
             if constexpr (SLICED) e0_hot(a); else bsw(a);
         } else if ((a & 0x287u) == 0x284u) {
             if constexpr (RENDER) (void)io(a, j);
-            else uf = 0;
+            else pia_intim();
         }
     }
     __device__ __forceinline__ uint32_t zp_read(uint32_t z, uint32_t j) { return (z & 0x80u) ? ldp(z & 0x7Fu) : io(z, j); }
@@ -1200,21 +1374,21 @@ struct Emu {
     uint32_t lag;             // CPU cycles of earlier instructions not yet given to the TIA and PIA
     uint32_t vtop;            // visible_top | vblank_top << 16
     uint8_t* fbp;             // this instance's framebuffer, 160 x 192 palette indices
-    uint32_t pix, pmask, pword;   // the framebuffer word being assembled: pixels, their mask, its index
+    uint32_t sc, zr;          // framebuffer sector in the sector buffer; rows written since the clear point | R_ZPEND
     uint32_t rx;              // the current line's pixels are drawn up to this TIA clock
 
     __device__ __forceinline__ RState rpack() const
     {
         RState r;
         r.clock = clock; r.scanline = scanline; r.tw = tw; r.pcnt = pcnt; r.vtop = vtop;
-        r.pix = pix; r.pmask = pmask; r.pword = pword; r.tv = tv; r.ps = ps; r.sel = sel; r.uf = uf;
+        r.sc = sc; r.zr = zr; r.tv = tp & 0xFFFFu; r.ps = tp >> 16; r.sel = su & 0xFFFFu; r.uf = su >> 16;
         r.rx = rx;
         return r;
     }
     __device__ __forceinline__ void runpack(const RState& r)
     {
         clock = r.clock; scanline = r.scanline; tw = r.tw; pcnt = r.pcnt; vtop = r.vtop;
-        pix = r.pix; pmask = r.pmask; pword = r.pword; tv = r.tv; ps = r.ps; sel = r.sel; uf = r.uf;
+        sc = r.sc; zr = r.zr; tp = r.tv | (r.ps << 16); su = r.sel | (r.uf << 16);
         rx = r.rx;
     }
     // The TIA and the PIA up to cycle j of the current instruction.  They are
@@ -1244,19 +1418,43 @@ struct Emu {
     }
     __device__ __forceinline__ void pia_tick1()                      // pia.rs:80-103
     {
-        if (tv == 0 && uf) { tv = 0xFFu; return; }
-        ps = (ps - 1u) & 0xFFFFu;
-        if (ps == 0) {
-            ps = uf ? 1u : sel;
-            if (tv == 0) { uf = 1; tv = 0xFFu; } else tv -= 1u;
+        uint32_t tv = tp & 0xFFFFu, ps = tp >> 16, uf = su >> 16;
+        if (tv == 0 && uf) {
+            tv = 0xFFu;
+        } else {
+            ps = (ps - 1u) & 0xFFFFu;
+            if (ps == 0) {
+                ps = uf ? 1u : (su & 0xFFFFu);
+                if (tv == 0) { uf = 1; tv = 0xFFu; } else tv -= 1u;
+            }
         }
+        tp = tv | (ps << 16);
+        su = (su & 0xFFFFu) | (uf << 16);
     }
-    __device__ __forceinline__ void fb_flush()
+    // The owed cycles, the pixels up to the beam, and the framebuffer as it
+    // can be seen now (the end of a frame or of a call).
+    __device__ __forceinline__ void fb_observe()
     {
         settle();
-        runpack(render_pending(rpack(), pv, fbp));
-        render_fb_flush(pix, pmask, pword, fbp);
-        pmask = 0;
+        runpack(render_observe(rpack(), pv, fbp));
+    }
+    // The sector buffer at the start of a call: the sector where the beam's
+    // row has been drawn to, as the last call left it in the framebuffer.
+    __device__ __forceinline__ void fb_resume()
+    {
+        const uint32_t vis = (scanline - (vtop & 0xFFFFu)) & 0xFFFFu;
+        zr = vis < FA_FB_H ? vis : FA_FB_H;
+        if (vis < FA_FB_H) {
+            const uint32_t x = (rx > 68u ? rx : 68u) - 68u;
+            sc = vis * (FA_FB_W / 32u) + ((x >> 5) < 4u ? (x >> 5) : 4u);
+            const uint4* q = (const uint4*)(fbp + (size_t)sc * 32u);
+            const uint4 u0 = q[0], u1 = q[1];
+            *r_sbuf(pv, 0) = u0.x; *r_sbuf(pv, 1) = u0.y; *r_sbuf(pv, 2) = u0.z; *r_sbuf(pv, 3) = u0.w;
+            *r_sbuf(pv, 4) = u1.x; *r_sbuf(pv, 5) = u1.y; *r_sbuf(pv, 6) = u1.z; *r_sbuf(pv, 7) = u1.w;
+        } else {
+            sc = 0;
+            r_sec_clear(pv);
+        }
     }
 
     // HeadlessAtari::set_action (src/atari.rs:571-582).
@@ -1277,9 +1475,9 @@ struct Emu {
         const uint32_t p0 = col[R_PIA0 * stride];                  // pa_out pa_ddr pa_in pb_out
         const uint32_t p1 = col[R_PIA1 * stride];                  // pb_ddr pb_in uf pdump
         ports = (p0 & 0xFFFFu) | ((p0 >> 24) << 16) | ((p1 & 0xFFu) << 24);
-        uf = (p1 >> 16) & 0xFF;
-        w = col[R_TIMER * stride]; tv = w & 0xFFFF; ps = w >> 16;
-        w = col[R_SELPC * stride]; sel = w & 0xFFFF; pcnt = w >> 16;
+        tp = col[R_TIMER * stride];
+        w = col[R_SELPC * stride]; su = (w & 0xFFFFu) | (((p1 >> 16) & 0xFFu) << 16); pcnt = w >> 16;
+        tlim = RENDER ? 0u : pia_span();
         w = col[R_TIA0 * stride];  clock = w & 0xFFFF; scanline = w >> 16;
         w = col[R_TIA1 * stride];                                   // wsync fcomp vsync vblank
         tw = ((w >> 16) & 0xFFFFu) | ((w & 1u) << 16) | (((w >> 8) & 1u) << 17) | (((p1 >> 24) & 1u) << 18);
@@ -1293,9 +1491,10 @@ struct Emu {
         col[R_AXYS * stride] = a | (x << 8) | (y << 16) | (sp << 24);
         col[R_PC * stride] = pc | (p << 16) | ((bank & 7u) << 24);
         col[R_PIA0 * stride] = (ports & 0xFFFFu) | ((pins & 0xFFu) << 16) | (((ports >> 16) & 0xFFu) << 24);
-        col[R_PIA1 * stride] = (ports >> 24) | (((pins >> 8) & 0xFFu) << 8) | (uf << 16) | (((tw >> 18) & 1u) << 24);
-        col[R_TIMER * stride] = tv | (ps << 16);
-        col[R_SELPC * stride] = sel | (pcnt << 16);
+        col[R_PIA1 * stride] = (ports >> 24) | (((pins >> 8) & 0xFFu) << 8) | ((su >> 16) << 16) | (((tw >> 18) & 1u) << 24);
+        const uint2 t = RENDER ? make_uint2(tp & 0xFFFFu, tp >> 16) : pia_now();
+        col[R_TIMER * stride] = t.x | (t.y << 16);
+        col[R_SELPC * stride] = (su & 0xFFFFu) | (pcnt << 16);
         col[R_TIA0 * stride] = clock | (scanline << 16);
         uint32_t t1 = ((tw >> 16) & 1u) | (((tw >> 17) & 1u) << 8) | ((tw & 0xFFFFu) << 16);
         if constexpr (SLICED) t1 |= fa_mapper_tia1(fa_mapper_from_slices(hot_lo, slices));

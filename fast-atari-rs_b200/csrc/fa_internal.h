@@ -34,6 +34,7 @@ struct FaGroup {
     uint32_t unit_begin;         // first work unit of this group (set by fa_launch_run)
     uint32_t rom_off;            // offset of the ROM in the shared-memory library (set by fa_launch_run)
     uint32_t rom_owner;          // 1 if this group stages the ROM (set by fa_launch_run)
+    uint32_t tag;                // the caller's number for the group (a pool's group index), in unit traces
 };
 
 // The kernel build a set of groups needs (FA_MAPS_*).
@@ -56,7 +57,24 @@ struct FaLaunch {
     unsigned long long* instr;   // guest-instruction counter, or null
     unsigned long long* rounds;  // scheduler rounds x 32 (lane slots offered), or null
     uint64_t wait_ns;            // bound of the ROM staging wait (set by fa_launch_run)
+    unsigned long long* trace;   // per work unit: start ns, end ns, smid << 32 | warp << 16 | tag, or null
+    uint32_t trace_cap;          // units the trace holds
+    const uint32_t* first_wave;  // warp-granular persistent form: the unit of each warp's first round
+                                 // (index warp * grid + cta; ~0 for none), or null for warp * grid + cta
 };
+
+// The launch shape fa_launch_run would use for L (warp-granular form only):
+// grid CTAs of `warps` warps, `per_sm` CTAs resident per SM.  Returns false
+// for the CTA-granular form.
+bool fa_launch_warp_shape(const FaLaunch& L, int block, bool persistent, int sms, uint32_t* grid, uint32_t* warps,
+                          int* per_sm);
+
+// The first-wave plan of a persistent warp-granular launch with one CTA per
+// SM: units [0, min(nunits, grid * warps)) placed on warp slots so that the
+// summed cost per SM sub-partition (warp w of a CTA issues from scheduler
+// w % 4) is as even as longest-processing-time-first makes it.  unit_cost is
+// non-increasing; table gets grid * warps entries (index warp * grid + cta).
+void fa_plan_first_wave(const float* unit_cost, uint32_t nunits, uint32_t grid, uint32_t warps, uint32_t* table);
 
 // The bound in nanoseconds that launches give their ROM staging wait
 // (fa_set_wait_limit_ns; 2 s by default).

@@ -95,7 +95,10 @@ __global__ void __launch_bounds__(WARPS * 32) fa_run_warps(const __grid_constant
         // units land on different SMs; after that the device queue.
         uint32_t u = 0;
         if (lane == 0) {
-            if (L.queue) u = round == 0 ? warp * gridDim.x + blockIdx.x : gridDim.x * WARPS + atomicAdd(L.queue, 1u);
+            if (L.queue) {
+                const uint32_t slot = warp * gridDim.x + blockIdx.x;
+                u = round != 0 ? gridDim.x * WARPS + atomicAdd(L.queue, 1u) : L.first_wave ? L.first_wave[slot] : slot;
+            }
             else u = round == 0 ? blockIdx.x * WARPS + warp : 0xFFFFFFFFu;
         }
         u = __shfl_sync(FULL, u, 0);
@@ -105,7 +108,16 @@ __global__ void __launch_bounds__(WARPS * 32) fa_run_warps(const __grid_constant
         const FaGroup& G = L.g[g];
         const uint32_t first = (u - G.unit_begin) * 32u;
         const uint32_t count = G.n - first < 32u ? G.n - first : 32u;
+        const uint64_t t0 = L.trace ? globaltimer_ns() : 0ull;
         run_unit<32, MAPS>(G, first, count, smem + G.rom_off, priv, lane, L.instr, L.rounds);
+        if (L.trace && lane == 0 && u < L.trace_cap) {
+            uint32_t smid;
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+            unsigned long long* rec = L.trace + 3ull * u;
+            rec[0] = t0;
+            rec[1] = globaltimer_ns();
+            rec[2] = ((unsigned long long)smid << 32) | (warp << 16) | G.tag;
+        }
     }
 }
 
@@ -119,8 +131,11 @@ __global__ void fa_broadcast(uint32_t* state, uint32_t stride, uint32_t n, const
 }  // namespace fa
 
 // ------------------------------------------------------------------ host launchers
+#include <algorithm>
 #include <map>
+#include <numeric>
 #include <mutex>
+#include <vector>
 
 namespace {
 std::mutex g_cfg_mu;
@@ -221,8 +236,23 @@ cudaError_t launch_warps(const FaLaunch& L, bool persistent, int sms, cudaStream
         grid = L.nunits < cap ? L.nunits : cap;
     }
     if (grid == 0) return cudaSuccess;
-    fa::fa_run_warps<WARPS, SL><<<grid, WARPS * 32, smem, s>>>(L);
+    FaLaunch Lw = L;
+    if (!persistent || per_sm != 1) Lw.first_wave = nullptr;            // a plan assumes one CTA per SM
+    fa::fa_run_warps<WARPS, SL><<<grid, WARPS * 32, smem, s>>>(Lw);
     return cudaGetLastError();
+}
+
+template <int WARPS, int SL>
+void warps_shape(const FaLaunch& L, bool persistent, int sms, uint32_t* grid, int* per_sm)
+{
+    const size_t smem = (size_t)L.romlib_bytes + (size_t)WARPS * FA_SMEM_WORDS * 32u * 4u;
+    *per_sm = warps_per_sm_for<WARPS, SL>(smem);
+    uint32_t g = (L.nunits + WARPS - 1) / WARPS;
+    if (persistent) {
+        const uint32_t cap = (uint32_t)(*per_sm * sms);
+        g = L.nunits < cap ? L.nunits : cap;
+    }
+    *grid = g;
 }
 
 template <int SL>
@@ -265,27 +295,38 @@ static void plan_units(FaLaunch& L, uint32_t unit)
     L.nunits = units;
 }
 
+// The warp-granular layout of a launch: the ROM library, 32-instance work
+// units and the warps per CTA.  False when the library leaves no room for
+// block / 32 warp slabs (the launch is CTA-granular).
+static bool warp_layout(FaLaunch& L, int block, bool persistent, int* warps)
+{
+    const uint32_t lib = plan_romlib(L);
+    L.romlib_bytes = lib;
+    const uint32_t slab = FA_SMEM_WORDS * 32u * 4u;
+    const int fit = (int)((FA_SMEM_PER_CTA_MAX - (int)lib) / (int)slab);
+    if (fit < block / 32) return false;
+    int w = block / 32;
+    if (persistent) {
+        // As many warps per CTA as shared memory allows (one CTA per SM), or
+        // fewer when a cap is set (the register budget per thread grows as
+        // 65536 / (32 x warps)).
+        const int cap = L.cta_warps ? (int)L.cta_warps : 32;
+        static const int sizes[] = { 32, 28, 24, 16, 8, 4, 2 };
+        for (int x : sizes)
+            if (x <= fit && x <= cap) { w = x; break; }
+    }
+    plan_units(L, 32u);
+    *warps = w;
+    return true;
+}
+
 cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int sms, cudaStream_t s)
 {
     FaLaunch L = L_in;
     L.wait_ns = fa_wait_limit_ns();
     const int maps = fa_maps_of(L.g, L.ngroups);                       // which cores the carts need
-    const uint32_t lib = plan_romlib(L);
-    L.romlib_bytes = lib;
-    const uint32_t slab = FA_SMEM_WORDS * 32u * 4u;
-    const int fit = (int)((FA_SMEM_PER_CTA_MAX - (int)lib) / (int)slab);
-    if (fit >= block / 32) {
-        int warps = block / 32;
-        if (persistent) {
-            // As many warps per CTA as shared memory allows (one CTA per SM),
-            // or fewer when a cap is set (the register budget per thread grows
-            // as 65536 / (32 x warps)).
-            const int cap = L.cta_warps ? (int)L.cta_warps : 32;
-            static const int sizes[] = { 32, 28, 24, 16, 8, 4, 2 };
-            for (int w : sizes)
-                if (w <= fit && w <= cap) { warps = w; break; }
-        }
-        plan_units(L, 32u);
+    int warps = 0;
+    if (warp_layout(L, block, persistent, &warps)) {
         return maps == FA_MAPS_4K   ? launch_warps_n<FA_MAPS_4K>(warps, L, persistent, sms, s)
              : maps == FA_MAPS_BOTH ? launch_warps_n<FA_MAPS_BOTH>(warps, L, persistent, sms, s)
                                     : launch_warps_n<FA_MAPS_SLICED>(warps, L, persistent, sms, s);
@@ -299,6 +340,59 @@ cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int 
     case 256: return launch_block_m<256>(maps, L, persistent, sms, s);
     case 512: return launch_block_m<512>(maps, L, persistent, sms, s);
     default: return cudaErrorInvalidValue;
+    }
+}
+
+bool fa_launch_warp_shape(const FaLaunch& L_in, int block, bool persistent, int sms, uint32_t* grid, uint32_t* warps,
+                          int* per_sm)
+{
+    FaLaunch L = L_in;
+    const int maps = fa_maps_of(L.g, L.ngroups);
+    int w = 0;
+    if (!warp_layout(L, block, persistent, &w)) return false;
+    *warps = (uint32_t)w;
+#define FA_SHAPE(WW)                                                                                        \
+    case WW:                                                                                                \
+        if (maps == FA_MAPS_4K) warps_shape<WW, FA_MAPS_4K>(L, persistent, sms, grid, per_sm);              \
+        else if (maps == FA_MAPS_BOTH) warps_shape<WW, FA_MAPS_BOTH>(L, persistent, sms, grid, per_sm);     \
+        else warps_shape<WW, FA_MAPS_SLICED>(L, persistent, sms, grid, per_sm);                            \
+        return true;
+    switch (w) {
+    FA_SHAPE(2) FA_SHAPE(4) FA_SHAPE(8) FA_SHAPE(16) FA_SHAPE(24) FA_SHAPE(28) FA_SHAPE(32)
+    default: return false;
+    }
+#undef FA_SHAPE
+}
+
+void fa_plan_first_wave(const float* unit_cost, uint32_t nunits, uint32_t grid, uint32_t warps, uint32_t* table)
+{
+    const uint32_t slots = grid * warps, parts = grid * 4u, per_part = warps / 4u;
+    std::fill(table, table + slots, 0xFFFFFFFFu);
+    const uint32_t first = nunits < slots ? nunits : slots;
+    // The first wave is units 0..first-1 (the device queue continues after
+    // them), placed heaviest first, each on the least loaded sub-partition
+    // that has a free slot: a (load, sub-partition) min-heap.
+    std::vector<uint32_t> order(first);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return unit_cost[a] > unit_cost[b]; });
+    std::vector<std::pair<double, uint32_t>> heap;
+    heap.reserve(parts);
+    for (uint32_t q = 0; q < parts; q++) heap.emplace_back(0.0, q);
+    auto cmp = [](const std::pair<double, uint32_t>& a, const std::pair<double, uint32_t>& b) { return a > b; };
+    std::make_heap(heap.begin(), heap.end(), cmp);
+    std::vector<uint32_t> used(parts, 0);
+    for (uint32_t u : order) {
+        if (heap.empty()) break;
+        std::pop_heap(heap.begin(), heap.end(), cmp);
+        auto [load, q] = heap.back();
+        heap.pop_back();
+        const uint32_t cta = q / 4u, sub = q % 4u;
+        const uint32_t warp = sub + 4u * used[q]++;                  // warp w issues from scheduler w % 4
+        table[warp * grid + cta] = u;
+        if (used[q] < per_part) {
+            heap.emplace_back(load + unit_cost[u], q);
+            std::push_heap(heap.begin(), heap.end(), cmp);
+        }
     }
 }
 

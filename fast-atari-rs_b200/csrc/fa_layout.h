@@ -128,6 +128,7 @@ enum : uint32_t {
     RB_PTOP    = 190,          // resizer: pending_top (u16, 2-byte aligned)
     FA_RPRIV_BYTES = 192,
     FA_RPRIV_WORDS = FA_RPRIV_BYTES / 4,
+    FA_RSLAB_WORDS = FA_RPRIV_WORDS + 8,               // + the framebuffer sector buffer (shared memory only)
     FA_RROW_EXTRA = FA_ROWS,                           // rows holding RB_* words
     RR_VTOP  = FA_ROWS + (FA_RPRIV_WORDS - FA_PRIV_WORDS),   // visible_top | vblank_top << 16
     RR_FLAGS = RR_VTOP + 1,    // hmove_pending | input_latch_enabled << 1 | inpt4_latch << 2 | inpt5_latch << 3

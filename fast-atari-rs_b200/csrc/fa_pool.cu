@@ -33,6 +33,14 @@ struct fa_pool {
     uint32_t queue_cap = 0;
     unsigned long long* d_ctr = nullptr;   // [0] instructions, [1] lane slots
     unsigned long long last_instr = 0, last_slots = 0;
+    unsigned long long* d_trace = nullptr;  // caller's per-unit trace buffer (fa_pool_set_trace), or null
+    uint32_t trace_cap = 0;
+    // First-wave placement of the persistent launch (fa_pool_set_balance):
+    // one device table per (grid, warps, unit costs), written once and kept
+    // until the pool is destroyed, so a launch queued on any stream, or held
+    // by a graph, reads the table it was given.
+    bool balance = true;
+    std::vector<std::pair<std::vector<float>, uint32_t*>> plans;
 };
 
 struct fa_graph {
@@ -79,6 +87,7 @@ extern "C" void fa_pool_destroy(fa_pool* p)
     cudaFree(p->d_err);
     cudaFree(p->d_queue);
     cudaFree(p->d_ctr);
+    for (auto& pl : p->plans) cudaFree(pl.second);
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;
 }
@@ -162,6 +171,7 @@ static int build_launch(fa_pool* p, const uint8_t* const* d_actions, uint32_t k,
         fa_handle* h = p->groups[gi];
         const uint8_t* acts = d_actions ? d_actions[gi] + call * (size_t)k * h->n : nullptr;
         FaGroup g = fa_handle_group(h, acts, k, d_obs ? d_obs[gi] : nullptr);
+        g.tag = (uint32_t)gi;
         g.unit_begin = units;
         units += (uint32_t)((h->n + p->block - 1) / p->block);
         rom_max = std::max(rom_max, h->nbanks * 4096u);
@@ -173,6 +183,51 @@ static int build_launch(fa_pool* p, const uint8_t* const* d_actions, uint32_t k,
     L.err = p->d_err;
     L.instr = p->d_ctr;
     L.rounds = p->d_ctr + 1;
+    L.trace = p->d_trace;
+    L.trace_cap = p->trace_cap;
+    return FA_OK;
+}
+
+// The first wave of a persistent warp-granular launch with one CTA per SM,
+// placed by fa_plan_first_wave: a unit costs its cart's weight (relative cost
+// of one instance-frame) times its instances times k.  A new table is
+// computed and uploaded (synchronously, never inside a stream capture) the
+// first time a shape and cost list appears; past kMaxPlans distinct ones the
+// launch runs without a plan.
+static int ensure_plan(fa_pool* p, FaLaunch& L, uint32_t k)
+{
+    constexpr size_t kMaxPlans = 16;
+    L.first_wave = nullptr;
+    if (!p->balance || !p->persistent) return FA_OK;
+    uint32_t grid = 0, warps = 0;
+    int per_sm = 0;
+    if (!fa_launch_warp_shape(L, p->block, true, p->sms, &grid, &warps, &per_sm) || per_sm != 1 || warps % 4u != 0u)
+        return FA_OK;
+    std::vector<float> key;
+    key.reserve(2 + L.nunits);
+    key.push_back((float)grid);
+    key.push_back((float)warps);
+    for (uint32_t g = 0; g < L.ngroups; g++) {
+        const uint32_t units = (L.g[g].n + 31u) / 32u;
+        for (uint32_t u = 0; u < units; u++) {
+            const uint32_t inst = std::min(32u, L.g[g].n - 32u * u);
+            key.push_back(p->weight[L.g[g].tag] * (float)inst * (float)k);
+        }
+    }
+    for (auto& pl : p->plans)
+        if (pl.first == key) { L.first_wave = pl.second; return FA_OK; }
+    if (p->plans.size() >= kMaxPlans) return FA_OK;
+    std::vector<uint32_t> table((size_t)grid * warps);
+    fa_plan_first_wave(key.data() + 2, (uint32_t)(key.size() - 2), grid, warps, table.data());
+    uint32_t* d = nullptr;
+    FA_CUDA(cudaMalloc(&d, table.size() * sizeof(uint32_t)));
+    const cudaError_t e = cudaMemcpy(d, table.data(), table.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        FA_CUDA(e);
+    }
+    p->plans.emplace_back(std::move(key), d);
+    L.first_wave = d;
     return FA_OK;
 }
 
@@ -185,6 +240,8 @@ static int pool_enqueue(fa_pool* p, const uint8_t* const* d_actions, int k, uint
     if (rc) return rc;
     FaLaunch L;
     build_launch(p, d_actions, (uint32_t)k, d_obs, 0, L);
+    rc = ensure_plan(p, L, (uint32_t)k);
+    if (rc) return rc;
     if (p->persistent) {
         L.queue = p->d_queue;
         FA_CUDA(cudaMemsetAsync(p->d_queue, 0, sizeof(uint32_t), s));
@@ -310,6 +367,23 @@ extern "C" int fa_pool_synchronize(fa_pool* p)
     return pool_finish(p);
 }
 
+extern "C" int fa_pool_set_balance(fa_pool* p, int on)
+{
+    if (!p) return fa_fail(FA_ERR_INVALID, "null pool");
+    p->balance = on != 0;
+    return FA_OK;
+}
+
+extern "C" int fa_pool_set_trace(fa_pool* p, unsigned long long* d_trace, uint32_t cap)
+{
+    if (!p) return fa_fail(FA_ERR_INVALID, "null pool");
+    if (!d_trace != !cap) return fa_fail(FA_ERR_INVALID, "trace buffer and capacity go together");
+    if ((uintptr_t)d_trace & 7u) return fa_fail(FA_ERR_INVALID, "trace buffer must be 8-byte aligned");
+    p->d_trace = d_trace;
+    p->trace_cap = cap;
+    return FA_OK;
+}
+
 extern "C" int fa_pool_reset_counters(fa_pool* p)
 {
     CHECK_P(p);
@@ -334,6 +408,9 @@ extern "C" int fa_pool_graph_create(fa_pool* p, const uint8_t* const* d_actions,
     FaLaunch L;
     build_launch(p, d_actions, (uint32_t)k, d_obs, 0, L);
     FA_CUDA(fa_launch_prepare(L, p->block, p->persistent));
+    rc = ensure_plan(p, L, (uint32_t)k);                                 // uploaded before the capture
+    if (rc) return rc;
+    const uint32_t* plan = L.first_wave;
     fa_graph* g = new (std::nothrow) fa_graph();
     if (!g) return fa_fail(FA_ERR_CAPACITY, "out of host memory");
     g->pool = p;
@@ -344,6 +421,7 @@ extern "C" int fa_pool_graph_create(fa_pool* p, const uint8_t* const* d_actions,
     cudaError_t le = cudaMemsetAsync(p->d_queue, 0, (size_t)calls * sizeof(uint32_t), p->stream);
     for (int c = 0; c < calls && le == cudaSuccess; c++) {
         build_launch(p, d_actions, (uint32_t)k, d_obs, (size_t)c, L);
+        L.first_wave = plan;
         if (p->persistent) L.queue = p->d_queue + c;
         le = fa_launch_run(L, p->block, p->persistent, p->sms, p->stream);
     }

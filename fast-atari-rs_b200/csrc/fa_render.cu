@@ -95,7 +95,10 @@ struct RRunner {
             e.done = 0u - e.lag;
             n = e.step();
             if (n == 0) {
-                if ((int32_t)e.done >= 0) e.lag = 0;                 // the owed cycles went with an access
+                // The reference's opcode fetch was a bus access (one cycle of
+                // TIA and PIA) before it stopped (src/cpu.rs:1139-1141): the
+                // TIA and PIA are owed up to the end of that cycle.
+                e.lag = 1u - e.done;
                 e.fold_cycles();
                 e.set_status(FA_STATUS_ILLEGAL_OPCODE);
                 active = false;
@@ -118,7 +121,7 @@ struct RRunner {
             const bool cap = fcyc > FA_FRAME_CYCLE_CAP;
             if (cap || e.vsync_on()) {
                 if (cap) e.set_status(FA_STATUS_CYCLE_CAP);
-                e.settle();                                          // before the next frame's action moves the pins
+                e.fb_observe();                                      // before the next frame's action moves the pins
                 e.fold_cycles();
                 e.row(R_FRAME) += 1u;
                 f++;
@@ -154,7 +157,7 @@ __global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLa
     __shared__ FaGroup sg;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t rom_bytes = L.nbanks * 4096u;
-    uint32_t* slab = (uint32_t*)(smem + rom_bytes) + warp * (FA_RPRIV_WORDS * 32u);
+    uint32_t* slab = (uint32_t*)(smem + rom_bytes) + warp * (FA_RSLAB_WORDS * 32u);
     if (threadIdx.x == 0) {
         mbar_init(&bar, 1);
         FaGroup g;
@@ -203,9 +206,8 @@ __global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLa
     e.scanline = 0;
     e.done = 0;
     e.lag = 0;
-    e.pix = 0;
-    e.pmask = 0;
-    e.pword = 0;
+    e.sc = 0;
+    e.zr = 0;
     e.vtop = 0;
     e.rx = 0;
     e.fbp = L.fb + (size_t)(valid ? i : 0u) * FA_FB_BYTES;
@@ -220,6 +222,7 @@ __global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLa
         e.load_hot(col, S);
         e.vtop = col[(size_t)RR_VTOP * S];
         e.rx = e.clock;
+        e.fb_resume();
         const uint32_t fl = col[(size_t)RR_FLAGS * S];
         e.tw |= ((fl & 1u) ? TW_HMOVE : 0u) | ((fl & 2u) ? TW_LATCH : 0u) | ((fl & 4u) ? TW_L4 : 0u) |
                 ((fl & 8u) ? TW_L5 : 0u);
@@ -227,7 +230,7 @@ __global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLa
     }
     const uint32_t rounds = run_lanes(r, L.sched);
     if (valid) {
-        e.fb_flush();
+        e.fb_observe();
         e.fold_cycles();
         // A console that halted before the call's last frame took the later
         // frames' set_action too; the last one is what its inputs hold.
@@ -340,13 +343,13 @@ cudaError_t launch_render(const FaRenderLaunch& L, cudaStream_t s)
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    const size_t smem = (size_t)L.nbanks * 4096u + (size_t)WARPS * FA_RPRIV_WORDS * 32u * 4u;
+    const size_t smem = (size_t)L.nbanks * 4096u + (size_t)WARPS * FA_RSLAB_WORDS * 32u * 4u;
     {
         std::lock_guard<std::mutex> lk(g_rmu);
         auto key = std::make_pair(dev, WARPS * 2 + (SLICED ? 1 : 0));
         if (g_rcfg.find(key) == g_rcfg.end()) {
             e = cudaFuncSetAttribute(fa::fa_render_run<WARPS, SLICED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     32768 + WARPS * FA_RPRIV_WORDS * 32 * 4);
+                                     32768 + WARPS * FA_RSLAB_WORDS * 32 * 4);
             if (e != cudaSuccess) return e;
             g_rcfg[key] = true;
         }

@@ -142,7 +142,7 @@ struct Runner {
             e.cyc_acc += n;
             e.tia_tick(n);
         }
-        e.pia_tick(n);
+        e.pia_count(n);
         fcyc += n;
         if (phase == 0u) {
             if (fcyc > FA_VSYNC_BUDGET) {

@@ -336,6 +336,21 @@ int  fa_pool_step_plain_async(fa_pool* p, const uint8_t* const* d_actions, int k
 int  fa_pool_synchronize(fa_pool* p);
 /* Zero the instruction / lane-slot counters (read after a synchronize). */
 int  fa_pool_reset_counters(fa_pool* p);
+/* Diagnostics (no counterpart in the reference): with a device buffer of
+ * cap x 3 unsigned 64-bit words set, every batched launch of the pool
+ * records, for each work unit (32 instances of one cart, in launch order:
+ * carts by decreasing queue weight), its start and end in device
+ * nanoseconds (%globaltimer) and smid << 32 | warp << 16 | group.  NULL
+ * (with cap 0) stops the records. */
+int  fa_pool_set_trace(fa_pool* p, unsigned long long* d_trace, uint32_t cap);
+/* Placement of the persistent launch's first wave (on by default; no
+ * counterpart in the reference): with one CTA per SM, the work units are
+ * spread over the SMs' four warp schedulers so that each scheduler's summed
+ * cost (the cart's weight from fa_pool_set_group, per instance-frame) is as
+ * even as longest-processing-time-first makes it; 0 places unit
+ * warp * grid + cta as the queue order gives them.  Results do not depend
+ * on it. */
+int  fa_pool_set_balance(fa_pool* p, int on);
 unsigned long long fa_pool_last_instructions(const fa_pool* p);
 unsigned long long fa_pool_last_lane_slots(const fa_pool* p);
 /* The pool's own stream (a cudaStream_t). */

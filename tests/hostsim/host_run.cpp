@@ -51,3 +51,33 @@ extern "C" long long hs_run(const uint8_t* rom, size_t len, fa_state* st, size_t
     for (size_t i = 0; i < n; i++) fa_unpack_column(rows.data() + i, n, scheme, st[i]);
     return (long long)instr;
 }
+
+// The timer bookkeeping of the headless core: one console counts calls
+// lazily (Emu::pia_count), the other runs every call exactly (Emu::pia_tick,
+// Pia::tick_n).  After call c, settle[c] is 1: a settle (Emu::pia_settle),
+// 2: a settle then an INTIM read (Emu::pia_intim: settles, clears the
+// underflow flag), 3: an INTIM read alone.  Both then report (value,
+// prescaler, select, underflow) as the state would be stored:
+// out[8 * c + 0..3] lazy, out[8 * c + 4..7] exact.
+extern "C" void hs_timer(const uint32_t* start, const uint32_t* ns, const uint8_t* settle, int m, uint32_t* out)
+{
+    fa::Emu<1> lz, ex;
+    memset(&lz, 0, sizeof(lz));
+    memset(&ex, 0, sizeof(ex));
+    lz.tp = ex.tp = start[0] | (start[1] << 16);
+    lz.su = ex.su = start[2] | (start[3] << 16);
+    lz.tlim = lz.pia_span();
+    for (int c = 0; c < m; c++) {
+        lz.pia_count(ns[c]);
+        ex.pia_tick(ns[c]);
+        if (settle[c] == 1 || settle[c] == 2) lz.pia_settle();
+        if (settle[c] >= 2) {
+            lz.pia_intim();
+            ex.su &= 0xFFFFu;
+        }
+        const uint2 t = lz.pia_now();
+        uint32_t* o = out + 8 * (size_t)c;
+        o[0] = t.x; o[1] = t.y; o[2] = lz.su & 0xFFFFu; o[3] = lz.su >> 16;
+        o[4] = ex.tp & 0xFFFFu; o[5] = ex.tp >> 16; o[6] = ex.su & 0xFFFFu; o[7] = ex.su >> 16;
+    }
+}

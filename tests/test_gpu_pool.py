@@ -111,3 +111,72 @@ def test_pool_rejects_too_many_carts(mixed):
             pool.add_cart(mixed[0].rom, 1)
         with pytest.raises(fa.FaError):
             pool.add_cart(mixed[0].rom, 1)
+
+
+def test_unit_trace_records_every_unit():
+    """fa_pool_set_trace: one record per 32-instance unit of a batched launch,
+    each cart's units tagged with its group, end after start, on a real SM."""
+    import torch
+    mixed = carts.mixed_carts()
+    counts = [300, 70]
+    with fa.AtariPool() as pool:
+        for c, n in zip(mixed[:2], counts):
+            pool.add_cart(c.rom, n)
+        nu = sum((n + 31) // 32 for n in counts)
+        d = torch.zeros(nu * 3, dtype=torch.int64, device="cuda")
+        pool.set_trace(d.data_ptr(), nu)
+        pool.step([carts.actions(seed=1, n=n, frames=2) for n in counts], 2, obs=False)
+        pool.set_trace()
+        tr = d.cpu().numpy().view(np.uint64).reshape(nu, 3)
+        pool.step([carts.actions(seed=2, n=n, frames=1) for n in counts], 1, obs=False)   # no longer traced
+        assert np.array_equal(d.cpu().numpy().view(np.uint64).reshape(nu, 3), tr)
+    assert (tr[:, 1] > tr[:, 0]).all() and (tr[:, 0] > 0).all()
+    tags = (tr[:, 2] & np.uint64(0xFFFF)).astype(int)
+    assert sorted(np.bincount(tags).tolist()) == sorted([(n + 31) // 32 for n in counts])
+    assert ((tr[:, 2] >> np.uint64(32)) < 1024).all()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_first_wave_placement_runs_every_unit_once(mixed, graph):
+    """fa_pool_set_balance: with 4 warps per CTA the persistent launch has
+    4 x (SMs) first-wave slots; 596 units exceed them, so the planned first
+    wave and the device queue after it share the units.  Every unit runs
+    exactly once, and the states equal those of the launch without the plan
+    and, on a sample of instances, the oracle."""
+    import torch
+    counts = [9000, 6000, 3000, 1000]
+    k = 1
+    acts = [carts.actions(seed=40 + i, n=n, frames=k) for i, n in enumerate(counts)]
+    nu = sum((n + 31) // 32 for n in counts)
+    states = {}
+    for balance in (True, False):
+        with fa.AtariPool() as pool:
+            for c, n in zip(mixed, counts):
+                pool.add_cart(c.rom, n)
+            for g, w in enumerate([1.0, 2.5, 4.0, 7.0]):
+                pool.set_group(g, "pc", w)
+            pool.set_launch(128, True, 4)
+            pool.set_balance(balance)
+            d = torch.zeros(nu * 3, dtype=torch.int64, device="cuda")
+            pool.set_trace(d.data_ptr(), nu)
+            if graph:
+                da = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in acts]
+                gr = pool.graph([t.data_ptr() for t in da], k, 1)
+                gr.launch()
+                torch.cuda.synchronize()
+                gr.close()
+            else:
+                pool.step(acts, k, obs=False)
+            tr = d.cpu().numpy().view(np.uint64).reshape(nu, 3)
+            assert (tr[:, 0] > 0).all() and (tr[:, 1] > tr[:, 0]).all(), f"balance={balance}: a unit did not run"
+            tags = (tr[:, 2] & np.uint64(0xFFFF)).astype(int)
+            assert np.bincount(tags).tolist() == [(n + 31) // 32 for n in counts]
+            states[balance] = [pool.group(g).download_states() for g in range(len(counts))]
+    assert nu > 4 * torch.cuda.get_device_properties(0).multi_processor_count
+    rng = np.random.default_rng(3)
+    for g, (c, n) in enumerate(zip(mixed, counts)):
+        assert_states_equal(states[True][g], states[False][g], f"group {g}: balance on vs off")
+        idx = np.sort(rng.choice(n, 64, replace=False))
+        ref = oracle_states(c.rom, len(idx))
+        oracle.run_batch(c.rom, ref, acts[g][:, idx], k)
+        assert_states_equal(states[True][g][idx], ref, f"group {g}: oracle sample")

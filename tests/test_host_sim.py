@@ -38,6 +38,8 @@ def sim():
     L.hs_run.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
                          ctypes.c_int]
     L.fa_rom_set_scheme.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    L.hs_timer.restype = None
+    L.hs_timer.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
     return L
 
 
@@ -137,3 +139,40 @@ def test_device_core_every_opcode_first(sim):
         got, ref = run_both(sim, rom, st, carts.actions(seed=5, n=n, frames=2), 2)
         assert_same(got, ref, f"every opcode first, {size}-byte ROM")
         assert (ref["run_status"] & 1).sum() >= 105          # the illegal opcodes halt at once
+
+
+def _timer_run(L, start, ns, settle):
+    ns = np.ascontiguousarray(ns, dtype=np.uint32)
+    settle = np.ascontiguousarray(settle, dtype=np.uint8)
+    st = np.ascontiguousarray(start, dtype=np.uint32)
+    out = np.zeros((len(ns), 8), np.uint32)
+    L.hs_timer(st.ctypes.data, ns.ctypes.data, settle.ctypes.data, len(ns), out.ctypes.data)
+    return out[:, :4], out[:, 4:]
+
+
+def test_lazy_timer_counting_equals_per_call_ticks(sim):
+    """The headless core counts instruction cycles off the timer lazily and
+    settles them on INTIM reads, PIA writes and state stores; after every
+    call, and after INTIM reads that clear the underflow flag, its state as
+    stored must equal
+    Pia::tick_n run on every call
+    (src/pia.rs:107-166), across underflows, the post-underflow wrap, every
+    interval, prescalers of 0 and above the interval, and calls of 0 to 80
+    cycles (instructions and WSYNC skips) and a few of up to 700."""
+    rng = np.random.default_rng(2600)
+    starts = [(tv, ps, sel, uf) for sel in (1, 8, 64, 1024) for tv in (0, 1, 2, 3, 200, 255)
+              for ps in (0, 1, 2, sel, sel + 3) for uf in (0, 1)]
+    starts += [(int(rng.integers(0, 256)), int(rng.integers(0, 1100)), int(rng.choice([1, 8, 64, 1024])),
+                int(rng.integers(0, 2))) for _ in range(1500)]
+    starts += [(5, 3, 3, 0), (300, 2, 8, 0)]                      # states only an upload makes
+    for start in starts:
+        m = 3000 if start[2] >= 64 else 1200
+        ns = np.where(rng.random(m) < 0.05, rng.integers(0, 81, m), rng.integers(1, 8, m))
+        ns = np.where(rng.random(m) < 0.003, rng.integers(81, 700, m), ns)
+        settle = np.where(rng.random(m) < 0.03, rng.integers(1, 4, m), 0)
+        lazy, exact = _timer_run(sim, start, ns, settle)
+        bad = np.nonzero((lazy != exact).any(axis=1))[0]
+        assert len(bad) == 0, (f"start {start}: call {bad[0]} (n={ns[bad[0]]}) lazy {lazy[bad[0]]} "
+                               f"exact {exact[bad[0]]}")
+        if start[2] == 1 and start[0] >= 1:
+            assert exact[:, 3].any()                               # the run went through underflows
