@@ -482,7 +482,7 @@ class AtariPool:
 
     def set_balance(self, on: bool = True) -> None:
         """Spread the persistent launch's first wave over the warp schedulers
-        by cart weight (on by default)."""
+        by cart weight (off by default)."""
         _check(lib().fa_pool_set_balance(self._p, 1 if on else 0))
 
     def set_trace(self, d_trace: int = 0, cap: int = 0) -> None:

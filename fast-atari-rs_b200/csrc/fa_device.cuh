@@ -742,6 +742,21 @@ static __device__ __noinline__ uint4 pia_intim_io(uint32_t tv_ps, uint32_t sel_u
     const uint2 t = pia_now_of(tv_ps & 0xFFFFu, tv_ps >> 16, sel, sel_uf >> 16, tlim);
     return make_uint4(t.x | (t.y << 16), sel, pia_span_of(t.x, t.y, sel, 0u), 0u);
 }
+// Pia::write of an I/O register by the headless core (src/pia.rs:202-228):
+// (ports, tv | ps << 16, sel | uf << 16, tlim) after it.  A port write
+// leaves the timer and its counting alone; a timer write replaces value,
+// prescaler, interval and flag, so the cycles counted so far no longer
+// matter.
+static __device__ __noinline__ uint4 pia_store_io(uint32_t a, uint32_t v, uint32_t ports, uint32_t tp, uint32_t su,
+                                                  uint32_t tlim)
+{
+    if (a & 0x10u) {
+        const uint32_t sel = 1u << ((0xA630u >> (4u * (a & 3u))) & 0xFu);   // 1, 8, 64, 1024
+        return make_uint4(ports, v | (sel << 16), sel, pia_span_of(v, sel, sel, 0u));
+    }
+    const uint32_t sh = 8u * (a & 3u);                                 // pa_out pa_ddr pb_out pb_ddr
+    return make_uint4((ports & ~(0xFFu << sh)) | (v << sh), tp, su, tlim);
+}
 // Packed (tv | ps << 16, sel | uf << 16, tlim) after settling and one exact
 // call of n cycles.
 static __device__ __noinline__ uint4 pia_sync_io(uint32_t tv_ps, uint32_t sel_uf, uint32_t tlim, uint32_t n)
@@ -969,10 +984,8 @@ struct Emu {
             }
             done = j + 1u;
         } else if (a & 0x200u) {
-            pia_settle();
-            uint4 r = pia_write_io(a, v, ports, tp & 0xFFFFu, tp >> 16, su);
-            ports = r.x; tp = r.y | (r.z << 16); su = r.w;
-            tlim = pia_span();
+            const uint4 r = pia_store_io(a, v, ports, tp, su, tlim);
+            ports = r.x; tp = r.y; su = r.z; tlim = r.w;
         } else {
             uint2 r = tia_write_io(a, v, clock, tw, scanline | (pcnt << 16), (uint8_t*)column(), G->stride * 4u);
             tw = r.x; scanline = r.y & 0xFFFFu; pcnt = r.y >> 16;
@@ -1030,7 +1043,9 @@ struct Emu {
     __device__ __forceinline__ uint32_t pull(uint32_t j)
     {
         sp = (sp + 1u) & 0xFFu;
-        return (sp & 0x80u) ? ldp(sp & 0x7Fu) : io(0x100u | sp, j);
+        if (sp & 0x80u) return ldp(sp & 0x7Fu);
+        if constexpr (RENDER) return io(0x100u | sp, j);
+        else return io_read(0x100u | sp, pcnt, pins, pads, ports, su, (const uint8_t*)column(), G->stride * 4u);  // TIA
     }
     // Read-modify-write's two writes, on cycles j and j+1; a RAM target only
     // needs the second.
@@ -1038,8 +1053,8 @@ struct Emu {
     {
         uint32_t a = ea & 0x1FFFu;
         if ((a & 0x1280u) == 0x080u) { stp(a & 0x7Fu, newv); return; }
-        write(ea, oldv, j);
-        write(ea, newv, j + 1u);
+#pragma unroll 1
+        for (uint32_t m = 0; m < 2u; m++) write(ea, m ? newv : oldv, j + m);
     }
 
     // ------------------------------------------------------------ ALU (cpu.rs:153-241)
@@ -1126,35 +1141,33 @@ struct Emu {
     __device__ __forceinline__ uint32_t group1(uint32_t pc0, uint32_t aaa, uint32_t bbb, uint32_t b1, uint32_t b2)
     {
         const bool st = aaa == 4u;
-        uint32_t ea, cyc, v;
+        uint32_t ea, cyc, v, base = 0;
+        bool indexed = false;                                       // (zp),Y, abs,Y, abs,X: a page may be crossed
         switch (bbb) {
-        case 0: {                                                   // (zp,X)
-            const uint32_t z = (b1 + x) & 0xFFu;
-            const uint32_t lo = zp_read(z, 3);
-            ea = (zp_read((z + 1u) & 0xFFu, 4) << 8) | lo;
-            cyc = 6;
+        case 0: case 4: {
+            // (zp,X): the pointer at zp b1 + X, read on cycles 3-4; (zp),Y: at
+            // zp b1, on cycles 2-3.  One zero-page read loop for both.
+            const uint32_t z = bbb == 0u ? (b1 + x) & 0xFFu : b1, j0 = bbb == 0u ? 3u : 2u;
+            uint32_t ptr = 0;
+#pragma unroll 1
+            for (uint32_t m = 0; m < 2u; m++) ptr |= zp_read((z + m) & 0xFFu, j0 + m) << (8u * m);
+            if (bbb == 0u) { ea = ptr; cyc = 6; }
+            else { base = ptr; ea = (ptr + y) & 0xFFFFu; cyc = 5; indexed = true; }
             break;
         }
         case 1: ea = b1; cyc = 3; break;                            // zp
         case 2: v = b1; cyc = 2; pc = (pc0 + 2u) & 0xFFFFu; goto operate;   // #imm ($89 is illegal)
         case 3: ea = (b2 << 8) | b1; cyc = 4; break;                // abs
-        case 4: {                                                   // (zp),Y
-            const uint32_t lo = zp_read(b1, 2);
-            const uint32_t base = (zp_read((b1 + 1u) & 0xFFu, 3) << 8) | lo;
-            ea = (base + y) & 0xFFFFu;
-            cyc = 5;
-            if (st || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu), 4); cyc = 6; }
-            break;
-        }
         case 5: ea = (b1 + x) & 0xFFu; cyc = 4; break;             // zp,X
-        default: {                                                  // abs,Y / abs,X
-            const uint32_t base = (b2 << 8) | b1;
+        default:                                                    // abs,Y / abs,X
+            base = (b2 << 8) | b1;
             ea = (base + (bbb == 6u ? y : x)) & 0xFFFFu;
             cyc = 4;
-            if (st || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu), 3); cyc = 5; }
+            indexed = true;
             break;
         }
-        }
+        // The fix-up read at the unfixed address (every store, or a page crossed).
+        if (indexed && (st || ((base ^ ea) & 0xFF00u))) { dummy((base & 0xFF00u) | (ea & 0xFFu), cyc - 1u); cyc++; }
         pc = (pc0 + ((bbb == 3u || bbb >= 6u) ? 3u : 2u)) & 0xFFFFu;
         if (st) { write(ea, a, cyc - 1u); return cyc; }
         v = read(ea, cyc - 1u);
@@ -1199,16 +1212,12 @@ struct Emu {
         default: {                                                  // abs,X (abs,Y for LDX)
             pc = (pc0 + 3u) & 0xFFFFu;
             const uint32_t base = (b2 << 8) | b1;
-            if (aaa == 5u) {
-                ea = (base + y) & 0xFFFFu; cyc = 4;
-                if ((base ^ ea) & 0xFF00u) { dummy((base & 0xFF00u) | (ea & 0xFFu), 3); cyc = 5; }
-                x = read(ea, cyc - 1u); nz(x); return cyc;
-            }
-            ea = (base + x) & 0xFFFFu;
-            dummy((base & 0xFF00u) | (ea & 0xFFu), 3);
-            const uint32_t v = read(ea, 4);
-            rmw_store(ea, v, shift_op(aaa, v), 5);
-            return 7;
+            ea = (base + (aaa == 5u ? y : x)) & 0xFFFFu;
+            cyc = 4;
+            // LDX reads the unfixed address only when a page is crossed; the
+            // read-modify-write forms always do, and take 7 cycles.
+            if (aaa != 5u || ((base ^ ea) & 0xFF00u)) { dummy((base & 0xFF00u) | (ea & 0xFFu), 3); cyc = 5; }
+            break;
         }
         }
         if (aaa == 4u) { write(ea, x, cyc - 1u); return cyc; }
@@ -1219,8 +1228,14 @@ struct Emu {
     }
 
     // cc = 00: control flow, stack, flags, BIT/STY/LDY/CPY/CPX.
+    // Bus-access sites are shared between the instructions of a group (one
+    // read and one write site for the memory forms, one push loop, one pull
+    // loop, one read loop for the new pc's bytes): every site is inlined code,
+    // and the interpreter's size decides how well it stays in the
+    // instruction cache.
     __device__ __forceinline__ uint32_t group0(uint32_t pc0, uint32_t aaa, uint32_t bbb, uint32_t b1, uint32_t b2)
     {
+        uint32_t ea, cyc, vb, vn, vs, vj, vv;
         switch (bbb) {
         case 4: {                                                   // branches
             pc = (pc0 + 2u) & 0xFFFFu;
@@ -1228,10 +1243,10 @@ struct Emu {
             if (((p >> pos) & 1u) != (aaa & 1u)) return 2;
             dummy(pc, 2);
             const uint32_t npc = (pc + (uint32_t)(int32_t)(int8_t)(uint8_t)b1) & 0xFFFFu;
-            uint32_t cyc = 3;
-            if ((pc ^ npc) & 0xFF00u) { dummy((pc & 0xFF00u) | (npc & 0xFFu), 3); cyc = 4; }
+            uint32_t bc = 3;
+            if ((pc ^ npc) & 0xFF00u) { dummy((pc & 0xFF00u) | (npc & 0xFFu), 3); bc = 4; }
             pc = npc;
-            return cyc;
+            return bc;
         }
         case 6:                                                     // flags, TYA
             pc = (pc0 + 1u) & 0xFFFFu;
@@ -1249,44 +1264,53 @@ struct Emu {
         case 2:                                                     // stack, DEY TAY INY INX
             pc = (pc0 + 1u) & 0xFFFFu;
             switch (aaa) {
-            case 0: push(p | F_B | F_U, 2); return 3;               // PHP
-            case 1: p = pull(3) & ~(F_B | F_U); return 4;           // PLP
-            case 2: push(a, 2); return 3;                           // PHA
-            case 3: a = pull(3); nz(a); return 4;                   // PLA
             case 4: y = (y - 1u) & 0xFFu; nz(y); return 2;          // DEY
             case 5: y = a; nz(y); return 2;                         // TAY
             case 6: y = (y + 1u) & 0xFFu; nz(y); return 2;          // INY
-            default: x = (x + 1u) & 0xFFu; nz(x); return 2;         // INX
+            case 7: x = (x + 1u) & 0xFFu; nz(x); return 2;          // INX
+            default: break;
             }
+            if (aaa & 1u) {                                         // PLP, PLA
+                const uint32_t v = pull(3);
+                if (aaa == 1u) p = v & ~(F_B | F_U);
+                else { a = v; nz(a); }
+                return 4;
+            }
+            push(aaa == 0u ? (p | F_B | F_U) : a, 2);               // PHP, PHA
+            return 3;
         case 0:
+            if (aaa < 2u) {                                         // BRK (b1 is the padding byte), JSR
+                const bool brk = aaa == 0u;
+                pc = (pc0 + 2u) & 0xFFFFu;
+                // BRK pushes pch, pcl, p on cycles 2-4; JSR pushes pch, pcl on
+                // cycles 3-4, before it reads the high byte.
+                const uint32_t n = brk ? 3u : 2u, j0 = brk ? 2u : 3u;
+                const uint32_t w = brk ? (pc << 8) | p | F_B | F_U : pc;
+#pragma unroll 1
+                for (uint32_t k = 0; k < n; k++) push((w >> (8u * (n - 1u - k))) & 0xFFu, j0 + k);
+                if (brk) p |= F_I;
+                // BRK: the vector at $FFFE-$FFFF on cycles 5-6; JSR: the high
+                // byte at pc on cycle 5.
+                vb = brk ? 0xFFFEu : pc; vn = brk ? 2u : 1u; vs = brk ? 0u : 8u; vj = 5u; vv = brk ? 0u : b1;
+                cyc = brk ? 7u : 6u;
+                goto vector;
+            }
+            if (aaa < 4u) {                                         // RTI (p, pcl, pch), RTS (pcl, pch)
+                const bool rti = aaa == 2u;
+                const uint32_t n = rti ? 3u : 2u;
+                uint32_t w = 0;
+#pragma unroll 1
+                for (uint32_t k = 0; k < n; k++) w |= pull(3u + k) << (8u * k);
+                if (rti) {
+                    p = w & 0xFFu & ~(F_B | F_U);
+                    pc = w >> 8;
+                } else {
+                    dummy(w, 5);
+                    pc = (w + 1u) & 0xFFFFu;
+                }
+                return 6;
+            }
             switch (aaa) {
-            case 0: {                                               // BRK (b1 is the padding byte)
-                pc = (pc0 + 2u) & 0xFFFFu;
-                push(pc >> 8, 2); push(pc & 0xFFu, 3); push(p | F_B | F_U, 4);
-                p |= F_I;
-                const uint32_t lo = read(0xFFFEu, 5);
-                pc = (read(0xFFFFu, 6) << 8) | lo;
-                return 7;
-            }
-            case 1: {                                               // JSR: pushes before the high byte
-                pc = (pc0 + 2u) & 0xFFFFu;
-                push(pc >> 8, 3); push(pc & 0xFFu, 4);
-                pc = (read(pc, 5) << 8) | b1;
-                return 6;
-            }
-            case 2: {                                               // RTI
-                p = pull(3) & ~(F_B | F_U);
-                const uint32_t lo = pull(4);
-                pc = (pull(5) << 8) | lo;
-                return 6;
-            }
-            case 3: {                                               // RTS
-                const uint32_t lo = pull(3);
-                const uint32_t ra = (pull(4) << 8) | lo;
-                dummy(ra, 5);
-                pc = (ra + 1u) & 0xFFFFu;
-                return 6;
-            }
             case 5: y = b1; nz(y); break;                           // LDY #
             case 6: cmp(y, b1); break;                              // CPY #
             default: cmp(x, b1); break;                             // CPX #
@@ -1297,28 +1321,34 @@ struct Emu {
             pc = (pc0 + 3u) & 0xFFFFu;
             if (aaa == 2u) { pc = (b2 << 8) | b1; return 3; }       // JMP
             if (aaa == 3u) {                                        // JMP (ind), page-wrap bug
-                const uint32_t ptr = (b2 << 8) | b1;
-                const uint32_t tlo = read(ptr, 3);
-                pc = (read((ptr & 0xFF00u) | ((ptr + 1u) & 0xFFu), 4) << 8) | tlo;
-                return 5;
+                vb = (b2 << 8) | b1; vn = 2u; vs = 0u; vj = 3u; vv = 0u; cyc = 5u;
+                goto vector;
             }
-            return mem0(aaa, (b2 << 8) | b1, 4);
+            ea = (b2 << 8) | b1; cyc = 4;
+            break;
         case 1:                                                     // zp: BIT STY LDY CPY CPX
             pc = (pc0 + 2u) & 0xFFFFu;
-            return mem0(aaa, b1, 3);
+            ea = b1; cyc = 3;
+            break;
         case 5:                                                     // zp,X: STY LDY
             pc = (pc0 + 2u) & 0xFFFFu;
-            return mem0(aaa, (b1 + x) & 0xFFu, 4);
+            ea = (b1 + x) & 0xFFu; cyc = 4;
+            break;
         default: {                                                  // abs,X: LDY
             pc = (pc0 + 3u) & 0xFFFFu;
             const uint32_t base = (b2 << 8) | b1;
-            const uint32_t ea = (base + x) & 0xFFFFu;
-            uint32_t cyc = 4;
+            ea = (base + x) & 0xFFFFu;
+            cyc = 4;
             if ((base ^ ea) & 0xFF00u) { dummy((base & 0xFF00u) | (ea & 0xFFu), 3); cyc = 5; }
-            y = read(ea, cyc - 1u); nz(y);
-            return cyc;
+            break;
         }
         }
+        return mem0(aaa, ea, cyc);
+    vector:                                                         // vn bytes from vb on, within its page
+#pragma unroll 1
+        for (uint32_t m = 0; m < vn; m++) vv |= read((vb & 0xFF00u) | ((vb + m) & 0xFFu), vj + m) << (vs + 8u * m);
+        pc = vv;
+        return cyc;
     }
     __device__ __forceinline__ uint32_t mem0(uint32_t aaa, uint32_t ea, uint32_t cyc)
     {
@@ -1352,11 +1382,23 @@ struct Emu {
             b1 = q[1];
             b2 = q[2];
         } else {
-            op = read(pc0, 0);
-            if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }
-            b1 = read((pc0 + 1u) & 0xFFFFu, 1);
-            const uint32_t bb = (op >> 2) & 7u;
-            if (bb == 3u || bb == 7u || (bb == 6u && (op & 3u) == 1u)) b2 = read((pc0 + 2u) & 0xFFFFu, 2);
+            // The opcode, then its operand bytes, through one bus-read site.
+            uint32_t n = 2u, w = 0u;
+            op = 0u;
+#pragma unroll 1
+            for (uint32_t k = 0; k < n; k++) {
+                const uint32_t v = read((pc0 + k) & 0xFFFFu, k);
+                if (k == 0u) {
+                    op = v;
+                    if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }
+                    const uint32_t bb = (op >> 2) & 7u;
+                    if (bb == 3u || bb == 7u || (bb == 6u && (op & 3u) == 1u)) n = 3u;
+                } else {
+                    w |= v << (8u * (k - 1u));
+                }
+            }
+            b1 = w & 0xFFu;
+            b2 = w >> 8;
         }
         const uint32_t aaa = op >> 5, bbb = (op >> 2) & 7u, cc = op & 3u;
         if (cc == 1u) return group1(pc0, aaa, bbb, b1, b2);

@@ -39,7 +39,7 @@ struct fa_pool {
     // one device table per (grid, warps, unit costs), written once and kept
     // until the pool is destroyed, so a launch queued on any stream, or held
     // by a graph, reads the table it was given.
-    bool balance = true;
+    bool balance = false;
     std::vector<std::pair<std::vector<float>, uint32_t*>> plans;
 };
 

@@ -343,9 +343,9 @@ int  fa_pool_reset_counters(fa_pool* p);
  * nanoseconds (%globaltimer) and smid << 32 | warp << 16 | group.  NULL
  * (with cap 0) stops the records. */
 int  fa_pool_set_trace(fa_pool* p, unsigned long long* d_trace, uint32_t cap);
-/* Placement of the persistent launch's first wave (on by default; no
- * counterpart in the reference): with one CTA per SM, the work units are
- * spread over the SMs' four warp schedulers so that each scheduler's summed
+/* Placement of the persistent launch's first wave (off by default; no
+ * counterpart in the reference): with one CTA per SM, 1 spreads the work
+ * units over the SMs' four warp schedulers so that each scheduler's summed
  * cost (the cart's weight from fa_pool_set_group, per instance-frame) is as
  * even as longest-processing-time-first makes it; 0 places unit
  * warp * grid + cta as the queue order gives them.  Results do not depend
