@@ -58,11 +58,11 @@ UNIT = "frames/s"
 # a warp run identical instances (fully converged), from the ncu capture in
 # profiles/fa_run_warps_converged_plain.md.  Used to express guest-instruction
 # throughput in warp-issue slots for the roofline.
-I_CONV = 187.6
+I_CONV = 165.5
 # DRAM bytes moved per instance-frame by fa_run on this workload, from the ncu
-# capture in profiles/fa_run_warps_mixed_batch_full.md (28.2 MB per 4-frame
+# capture in profiles/fa_run_warps_mixed_batch_full.md (29.6 MB per 4-frame
 # call of 135,500 instances).
-DRAM_BYTES_PER_INSTANCE_FRAME = 52.0
+DRAM_BYTES_PER_INSTANCE_FRAME = 54.6
 # The rendering kernel (fa_render_run<8>) per rendered console-frame, from
 # the ncu capture in profiles/fa_render_run_render_cart.md: SASS
 # thread-instructions and DRAM bytes (framebuffer writes included).
