@@ -66,8 +66,8 @@ DRAM_BYTES_PER_INSTANCE_FRAME = 54.6
 # The rendering kernel (fa_render_run<8>) per rendered console-frame, from
 # the ncu capture in profiles/fa_render_run_render_cart.md: SASS
 # thread-instructions and DRAM bytes (framebuffer writes included).
-RENDER_THREAD_INST_PER_FRAME = 3.863e6   # smsp__thread_inst_executed / console-frames
-RENDER_DRAM_BYTES_PER_FRAME = 107_750    # (dram read + write) / console-frames
+RENDER_THREAD_INST_PER_FRAME = 3.263e6   # smsp__thread_inst_executed / console-frames
+RENDER_DRAM_BYTES_PER_FRAME = 60_400     # (dram read + write) / console-frames
 
 
 def load_pkg():
