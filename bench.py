@@ -66,8 +66,8 @@ DRAM_BYTES_PER_INSTANCE_FRAME = 54.6
 # The rendering kernel (fa_render_run<8>) per rendered console-frame, from
 # the ncu capture in profiles/fa_render_run_render_cart.md: SASS
 # thread-instructions and DRAM bytes (framebuffer writes included).
-RENDER_THREAD_INST_PER_FRAME = 3.263e6   # smsp__thread_inst_executed / console-frames
-RENDER_DRAM_BYTES_PER_FRAME = 60_400     # (dram read + write) / console-frames
+RENDER_THREAD_INST_PER_FRAME = 2.936e6   # smsp__thread_inst_executed / console-frames
+RENDER_DRAM_BYTES_PER_FRAME = 61_600     # (dram read + write) / console-frames
 
 
 def load_pkg():
@@ -790,8 +790,8 @@ def run_gpu_arm(args, fa, carts, rank, world, local_rank):
 
 
 RENDER_DESC = ("rendering console (pixel-accurate TIA, 160x192 palette-index framebuffer per console): "
-               "render_4k_fixed cart, 113664 consoles (one wave: 148 SMs x 24 warps x 32), K=4 frames per call")
-RENDER_N, RENDER_K = 113_664, 4
+               "render_4k_fixed cart, 75776 consoles (one wave: 148 SMs x 16 warps x 32), K=4 frames per call")
+RENDER_N, RENDER_K = 75_776, 4
 
 
 def render_cpu_baseline(carts, seconds_target):
@@ -872,7 +872,7 @@ def run_render_arm(args, fa, carts, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic",
-        "config": {"workload": RENDER_DESC.replace("113664 consoles (one wave: 148 SMs x 24 warps x 32)", f"{n} consoles"),
+        "config": {"workload": RENDER_DESC.replace("75776 consoles (one wave: 148 SMs x 16 warps x 32)", f"{n} consoles"),
                    "instances": n, "frames_per_call": k,
                    "framebuffer_bytes_per_frame": 160 * 192,
                    "l2": "flushed (256 MB write) before every timed call",
@@ -953,8 +953,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=20000, help="saturation requests of the serve workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     ap.add_argument("--render-instances", type=int, default=RENDER_N, help="consoles of the render workload")
-    ap.add_argument("--render-cta-warps", type=int, default=8, choices=[4, 8, 16],
-                    help="warps per CTA of the render kernel (80 registers: 8 -> 24 warps/SM, 16 -> 16)")
+    ap.add_argument("--render-cta-warps", type=int, default=16, choices=[4, 8, 16],
+                    help="warps per CTA of the render kernel (128 registers: 16 warps/SM either way)")
     ap.add_argument("--block", type=int, default=128)
     ap.add_argument("--tuning", default=None, help="JSON file of per-cart tuning records (skips the autotuner)")
     ap.add_argument("--no-autotune", action="store_true", help="default policy and weights instead of the autotuner")

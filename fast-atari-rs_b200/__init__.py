@@ -696,7 +696,7 @@ class AtariRender:
     of one ROM: each frame also renders a 160 x 192 framebuffer of NTSC
     palette indices (Atari::framebuffer), kept on the device."""
 
-    def __init__(self, rom: bytes, n: int, cta_warps: int = 8, sched="pc"):
+    def __init__(self, rom: bytes, n: int, cta_warps: int = 16, sched="pc"):
         r = np.frombuffer(bytes(rom), dtype=np.uint8).copy()
         h = _vp()
         _check(lib().fa_render_create(_u8(r), len(r), int(n), ctypes.byref(h)))

@@ -146,11 +146,14 @@ struct RRunner {
     }
 };
 
-// 80 registers: 24 resident warps per SM (three 256-thread CTAs), the
-// occupancy that the shared-memory slabs allow; ptxas would otherwise take
-// 128 for the pixel code and hold the SM to 16 warps.
+// 128 registers: the pixel code and the bus run with almost no spills, and
+// 16 warps are resident per SM (one 512-thread CTA at 16 warps, the default,
+// or two 256-thread CTAs at 8).  Held to 80 registers for 24 resident warps,
+// the spills cost more than the extra warps gain: 2.15 against 3.92 M
+// frames/s on the render cart (113,664 consoles, one B200).  Uncapped,
+// ptxas takes 148, which a 16-warp CTA cannot launch with.
 template <int WARPS, bool SLICED>
-__global__ void __maxnreg__(80) fa_render_run(const __grid_constant__ FaRenderLaunch L)
+__global__ void __maxnreg__(128) fa_render_run(const __grid_constant__ FaRenderLaunch L)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t bar;
@@ -325,7 +328,7 @@ struct fa_render {
     uint32_t* d_err = nullptr;
     unsigned long long* d_ctr = nullptr;
     cudaStream_t stream = nullptr;
-    int warps = 8;
+    int warps = 16;
     int sched = FA_SCHED_PC;
     bool reset_done = false;
     unsigned long long last_instr = 0, last_slots = 0;

@@ -579,7 +579,7 @@ typedef struct fa_render fa_render;
 int  fa_render_create(const uint8_t* rom, size_t rom_len, size_t n, fa_render** out);
 void fa_render_destroy(fa_render* r);
 size_t fa_render_num_envs(const fa_render* r);
-/* CTA size in warps (4, 8 or 16) and warp policy (FA_SCHED_*). */
+/* CTA size in warps (4, 8 or 16; 16 by default) and warp policy (FA_SCHED_*). */
 int  fa_render_set_launch(fa_render* r, int cta_warps, int sched);
 /* Every console becomes Atari::new(rom) followed by one run_frame() without
  * an action.  fb_out (n * 160 * 192 bytes) and ram_out (n * 128) may be NULL. */
