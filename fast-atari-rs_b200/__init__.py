@@ -450,21 +450,33 @@ class AtariPool:
         _check(lib().fa_pool_set_launch(self._p, int(block), 1 if persistent else 0))
         _check(lib().fa_pool_set_cta_warps(self._p, int(cta_warps)))
 
-    def _host_step(self, fn, actions, k, obs):
+    def _host_step(self, fn, actions, k, obs, out=None):
         acts = [np.ascontiguousarray(a, dtype=np.uint8).reshape(-1) for a in actions]
         for a, (_, n) in zip(acts, self.groups):
             if a.size != k * n:
                 raise ValueError("actions size mismatch")
-        outs = [np.empty((n, 128), np.uint8) for _, n in self.groups] if obs else None
+        if out is not None:
+            if len(out) != len(self.groups):
+                raise ValueError("one output array per cart")
+            for o, (_, n) in zip(out, self.groups):
+                if not (isinstance(o, np.ndarray) and o.dtype == np.uint8 and o.size == n * 128
+                        and o.flags.c_contiguous and o.flags.writeable):
+                    raise ValueError("each output must be a writable C-contiguous uint8 array of n*128 bytes")
+            outs, obs = list(out), True
+        else:
+            outs = [np.empty((n, 128), np.uint8) for _, n in self.groups] if obs else None
         _check(fn(self._p, _ptrs([a.ctypes.data for a in acts]), int(k),
                   _ptrs([o.ctypes.data for o in outs]) if obs else None))
         return outs
 
-    def step(self, actions, k: int, obs: bool = True):
-        return self._host_step(lib().fa_pool_step, actions, k, obs)
+    def step(self, actions, k: int, obs: bool = True, out=None):
+        """One batched call from host buffers; returns each cart's RAM after
+        the last frame.  `out`: the caller's (n, 128) uint8 arrays to fill,
+        one per cart, instead of new ones."""
+        return self._host_step(lib().fa_pool_step, actions, k, obs, out)
 
-    def step_plain(self, actions, k: int, obs: bool = True):
-        return self._host_step(lib().fa_pool_step_plain, actions, k, obs)
+    def step_plain(self, actions, k: int, obs: bool = True, out=None):
+        return self._host_step(lib().fa_pool_step_plain, actions, k, obs, out)
 
     def step_async(self, d_actions, k: int, d_obs=None, stream: int = 0) -> None:
         _check(lib().fa_pool_step_async(self._p, _ptrs(d_actions), int(k),

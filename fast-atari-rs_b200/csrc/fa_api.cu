@@ -16,6 +16,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/fast_atari.h"
@@ -389,6 +390,13 @@ extern "C" int fa_create(const uint8_t* rom, size_t rom_len, size_t n, fa_handle
     TRY(cudaMemset(h->d_err, 0, 2 * sizeof(uint32_t)));
     TRY(cudaMalloc(&h->d_instr, 2 * sizeof(unsigned long long)));
     TRY(cudaMallocHost(&h->h_obs, n * 128));
+    // The same pinned buffer as the kernels see it: host-buffer calls have
+    // the kernel write observations there as its units finish, with no copy
+    // after the launch.  Without a mapping they copy from d_obs instead.
+    if (cudaHostGetDevicePointer((void**)&h->h_obs_dev, h->h_obs, 0) != cudaSuccess) {
+        h->h_obs_dev = nullptr;
+        (void)cudaGetLastError();
+    }
     // Every instance starts zeroed and marked not-reset (stepping it is a no-op).
     {
         std::vector<uint32_t> st(h->stride, FA_STATUS_NOT_RESET);
@@ -518,6 +526,31 @@ extern "C" int fa_reset(fa_handle* h, uint8_t* obs_out)
     return FA_OK;
 }
 
+void fa_host_copy(void* dst, const void* src, size_t bytes)
+{
+    constexpr size_t kPerThread = 2u << 20;                           // below this one thread copies
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t parts = std::min(std::min<size_t>(hw, 8), bytes / kPerThread);
+    if (parts <= 1) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t per = (bytes + parts - 1) / parts;
+    std::vector<std::thread> th;
+    size_t covered = per;                                              // this thread copies [0, per)
+    try {
+        for (size_t off = per; off < bytes; off += per) {
+            const size_t len = std::min(per, bytes - off);
+            th.emplace_back([=] { memcpy((uint8_t*)dst + off, (const uint8_t*)src + off, len); });
+            covered = off + len;
+        }
+    } catch (...) {                                                    // no thread: the rest here
+    }
+    memcpy(dst, src, per);
+    if (covered < bytes) memcpy((uint8_t*)dst + covered, (const uint8_t*)src + covered, bytes - covered);
+    for (auto& t : th) t.join();
+}
+
 static int step_host(fa_handle* h, const uint8_t* actions, int k, uint8_t* obs_out)
 {
     CHECK_H(h);
@@ -528,12 +561,14 @@ static int step_host(fa_handle* h, const uint8_t* actions, int k, uint8_t* obs_o
     memcpy(h->h_actions, actions, bytes);
     FA_CUDA(cudaMemcpyAsync(h->d_actions, h->h_actions, bytes, cudaMemcpyHostToDevice, h->stream));
     FA_CUDA(cudaMemsetAsync(h->d_instr, 0, 2 * sizeof(unsigned long long), h->stream));
-    rc = enqueue_run(h, fa_handle_group(h, h->d_actions, (uint32_t)k, obs_out ? h->d_obs : nullptr), h->stream);
+    uint8_t* obs_dst = obs_out ? (h->h_obs_dev ? h->h_obs_dev : h->d_obs) : nullptr;
+    rc = enqueue_run(h, fa_handle_group(h, h->d_actions, (uint32_t)k, obs_dst), h->stream);
     if (rc) return rc;
-    if (obs_out) FA_CUDA(cudaMemcpyAsync(h->h_obs, h->d_obs, h->n * 128, cudaMemcpyDeviceToHost, h->stream));
+    if (obs_out && !h->h_obs_dev)
+        FA_CUDA(cudaMemcpyAsync(h->h_obs, h->d_obs, h->n * 128, cudaMemcpyDeviceToHost, h->stream));
     rc = finish(h);
     if (rc) return rc;
-    if (obs_out) memcpy(obs_out, h->h_obs, h->n * 128);
+    if (obs_out) fa_host_copy(obs_out, h->h_obs, h->n * 128);
     return FA_OK;
 }
 

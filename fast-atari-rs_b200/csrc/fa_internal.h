@@ -139,6 +139,9 @@ cudaError_t fa_launch_broadcast(uint32_t* state, uint32_t stride, uint32_t n, co
                                 cudaStream_t s);
 
 int fa_fail(int code, const char* fmt, ...);
+// memcpy of a host-buffer call's outputs into the caller's memory, split over
+// up to 8 threads when it is large (first-touch page faults included).
+void fa_host_copy(void* dst, const void* src, size_t bytes);
 
 #define FA_CUDA(call)                                                                          \
     do {                                                                                       \
@@ -171,6 +174,7 @@ struct fa_handle {
     uint8_t* h_actions = nullptr;      // pinned staging
     size_t h_actions_cap = 0;
     uint8_t* h_obs = nullptr;          // pinned, n*128
+    uint8_t* h_obs_dev = nullptr;      // h_obs as the device addresses it (mapped), or null
     cudaStream_t stream = nullptr;
     int block = 128;
     int sched = FA_SCHED_PC;

@@ -317,20 +317,21 @@ static int pool_step_host(fa_pool* p, const uint8_t* const* actions, int k, uint
         memcpy(h->h_actions, actions[gi], bytes);
         FA_CUDA(cudaMemcpyAsync(h->d_actions, h->h_actions, bytes, cudaMemcpyHostToDevice, p->stream));
         d_act[gi] = h->d_actions;
-        d_obs[gi] = (obs && obs[gi]) ? h->d_obs : nullptr;
+        // Observations go straight into the pinned buffer where it is mapped.
+        d_obs[gi] = (obs && obs[gi]) ? (h->h_obs_dev ? h->h_obs_dev : h->d_obs) : nullptr;
     }
     FA_CUDA(cudaMemsetAsync(p->d_ctr, 0, 2 * sizeof(unsigned long long), p->stream));
     int rc = plain ? pool_enqueue_plain(p, d_act.data(), k, d_obs.data(), p->stream)
                    : pool_enqueue(p, d_act.data(), k, d_obs.data(), p->stream);
     if (rc) return rc;
     for (size_t gi = 0; gi < G; gi++)
-        if (d_obs[gi])
+        if (d_obs[gi] && !p->groups[gi]->h_obs_dev)
             FA_CUDA(cudaMemcpyAsync(p->groups[gi]->h_obs, d_obs[gi], p->groups[gi]->n * 128,
                                     cudaMemcpyDeviceToHost, p->stream));
     rc = pool_finish(p);
     if (rc) return rc;
     for (size_t gi = 0; gi < G; gi++)
-        if (d_obs[gi]) memcpy(obs[gi], p->groups[gi]->h_obs, p->groups[gi]->n * 128);
+        if (d_obs[gi]) fa_host_copy(obs[gi], p->groups[gi]->h_obs, p->groups[gi]->n * 128);
     return FA_OK;
 }
 

@@ -13,5 +13,5 @@ enum { cudaStreamNonBlocking = 1 };
 STUB(cudaDeviceGetAttribute) STUB(cudaDeviceSynchronize) STUB(cudaFree) STUB(cudaFreeHost) STUB(cudaGetDevice)
 STUB(cudaGetDeviceCount) STUB(cudaGetLastError) STUB(cudaMalloc) STUB(cudaMallocHost) STUB(cudaMemcpy)
 STUB(cudaMemcpyAsync) STUB(cudaMemset) STUB(cudaMemsetAsync) STUB(cudaSetDevice) STUB(cudaStreamCreateWithFlags)
-STUB(cudaStreamDestroy) STUB(cudaStreamSynchronize) STUB(cudaMemcpy2D)
+STUB(cudaStreamDestroy) STUB(cudaStreamSynchronize) STUB(cudaMemcpy2D) STUB(cudaHostGetDevicePointer)
 static inline const char* cudaGetErrorString(cudaError_t) { return "host simulation"; }

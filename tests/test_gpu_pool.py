@@ -180,3 +180,28 @@ def test_first_wave_placement_runs_every_unit_once(mixed, graph):
         ref = oracle_states(c.rom, len(idx))
         oracle.run_batch(c.rom, ref, acts[g][:, idx], k)
         assert_states_equal(states[True][g][idx], ref, f"group {g}: oracle sample")
+
+
+def test_host_step_fills_caller_arrays(mixed):
+    """pool.step(out=...): the observations of a host-buffer call land in the
+    caller's arrays, call after call, equal to the oracle's.  Host-buffer
+    calls have the kernel write observations into mapped pinned memory and
+    copy them out on several threads when they are large: one cart here has
+    40,000 instances (5 MB of observations)."""
+    counts = [40000, 300]
+    k = 2
+    carts_ = [mixed[0], mixed[1]]
+    refs = [oracle_states(c.rom, n) for c, n in zip(carts_, counts)]
+    outs = [np.full((n, 128), 0xAB, np.uint8) for n in counts]
+    with fa.AtariPool() as pool:
+        for c, n in zip(carts_, counts):
+            pool.add_cart(c.rom, n)
+        for call in range(2):
+            acts = [carts.actions(seed=70 + 10 * call + i, n=n, frames=k) for i, n in enumerate(counts)]
+            got = pool.step(acts, k, out=outs)
+            assert all(g is o for g, o in zip(got, outs))
+            for gi, (c, ref) in enumerate(zip(carts_, refs)):
+                o, _ = oracle.run_batch(c.rom, ref, acts[gi], k)
+                assert np.array_equal(outs[gi], o), f"call {call} group {gi}"
+        with pytest.raises(ValueError):
+            pool.step(acts, k, out=[outs[0]])
