@@ -309,8 +309,10 @@ static bool warp_layout(FaLaunch& L, int block, bool persistent, int* warps)
     if (persistent) {
         // As many warps per CTA as shared memory allows (one CTA per SM), or
         // fewer when a cap is set (the register budget per thread grows as
-        // 65536 / (32 x warps)).
-        const int cap = L.cta_warps ? (int)L.cta_warps : 32;
+        // 65536 / (32 x warps)).  A launch of sliced carts alone defaults to
+        // 24: at 32 warps its core is held to 64 registers and spills in the
+        // interpreter loop (three E0/3F carts: 2.31 against 2.13 M frames/s).
+        const int cap = L.cta_warps ? (int)L.cta_warps : fa_maps_of(L.g, L.ngroups) == FA_MAPS_SLICED ? 24 : 32;
         static const int sizes[] = { 32, 28, 24, 16, 8, 4, 2 };
         for (int x : sizes)
             if (x <= fit && x <= cap) { w = x; break; }
