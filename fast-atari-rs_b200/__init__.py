@@ -737,14 +737,26 @@ class AtariRender:
         _check(lib().fa_render_reset(self._r, fb.ctypes.data, ram.ctypes.data))
         return fb, ram
 
-    def step_multi(self, actions, k: int, fb: bool = True):
+    def step_multi(self, actions, k: int, fb: bool = True, out=None):
+        """k frames; returns (framebuffers (n, 192, 160) or None, RAM (n, 128)).
+        `out`: the caller's (framebuffers, RAM) uint8 arrays to fill instead of
+        new ones (framebuffers may be None when fb is False)."""
         a = np.ascontiguousarray(actions, dtype=np.uint8).reshape(-1)
         if a.size != k * self.n:
             raise ValueError(f"expected {k}*{self.n} actions, got {a.size}")
-        out = np.empty((self.n, FB_H, FB_W), np.uint8) if fb else None
-        ram = np.empty((self.n, 128), np.uint8)
-        _check(lib().fa_render_step_multi(self._r, _u8(a), int(k), out.ctypes.data if fb else None, ram.ctypes.data))
-        return out, ram
+        if out is not None:
+            fbo, ram = out
+            fbo = fbo if fb else None
+            wanted = [(ram, self.n * 128)] + ([(fbo, self.n * FB_H * FB_W)] if fb else [])
+            for arr, size in wanted:
+                if not (isinstance(arr, np.ndarray) and arr.dtype == np.uint8 and arr.size == size
+                        and arr.flags.c_contiguous and arr.flags.writeable):
+                    raise ValueError("outputs must be writable C-contiguous uint8 arrays of the right size")
+        else:
+            fbo = np.empty((self.n, FB_H, FB_W), np.uint8) if fb else None
+            ram = np.empty((self.n, 128), np.uint8)
+        _check(lib().fa_render_step_multi(self._r, _u8(a), int(k), fbo.ctypes.data if fb else None, ram.ctypes.data))
+        return fbo, ram
 
     def step_multi_async(self, d_actions: int, k: int, d_obs: int = 0, stream: int = 0) -> None:
         _check(lib().fa_render_step_multi_async(self._r, _vp(d_actions), int(k), _vp(d_obs or None), _vp(stream or None)))

@@ -131,3 +131,23 @@ def test_rgba_output_matches_oracle_render():
         assert np.array_equal(d.cpu().numpy().reshape(part.shape), part)
         with pytest.raises(fa.FaError):
             g.rgba(30, 8)
+
+
+def test_render_fills_caller_arrays():
+    """AtariRender.step_multi(out=...): framebuffers and RAM land in the
+    caller's arrays, call after call, equal to the oracle's."""
+    rom = carts.render_cart().rom
+    n, k = 24, 2
+    consoles = oracle.render_reset(rom, n)
+    fb_out = np.full((n, 192, 160), 0xAB, np.uint8)
+    ram_out = np.full((n, 128), 0xCD, np.uint8)
+    with fa.AtariRender(rom, n) as g:
+        g.reset()
+        for c in range(2):
+            acts = carts.actions(seed=90 + c, n=n, frames=k)
+            fb, ram = g.step_multi(acts, k, out=(fb_out, ram_out))
+            assert fb is fb_out and ram is ram_out
+            oracle.render_steps(consoles, acts)
+            check(fb_out, ram_out, g.states(), consoles, f"caller arrays, call {c}")
+        with pytest.raises(ValueError):
+            g.step_multi(acts, k, out=(fb_out[:1], ram_out))
