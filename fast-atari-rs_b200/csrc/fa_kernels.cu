@@ -366,38 +366,6 @@ bool fa_launch_warp_shape(const FaLaunch& L_in, int block, bool persistent, int 
 #undef FA_SHAPE
 }
 
-void fa_plan_first_wave(const float* unit_cost, uint32_t nunits, uint32_t grid, uint32_t warps, uint32_t* table)
-{
-    const uint32_t slots = grid * warps, parts = grid * 4u, per_part = warps / 4u;
-    std::fill(table, table + slots, 0xFFFFFFFFu);
-    const uint32_t first = nunits < slots ? nunits : slots;
-    // The first wave is units 0..first-1 (the device queue continues after
-    // them), placed heaviest first, each on the least loaded sub-partition
-    // that has a free slot: a (load, sub-partition) min-heap.
-    std::vector<uint32_t> order(first);
-    std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return unit_cost[a] > unit_cost[b]; });
-    std::vector<std::pair<double, uint32_t>> heap;
-    heap.reserve(parts);
-    for (uint32_t q = 0; q < parts; q++) heap.emplace_back(0.0, q);
-    auto cmp = [](const std::pair<double, uint32_t>& a, const std::pair<double, uint32_t>& b) { return a > b; };
-    std::make_heap(heap.begin(), heap.end(), cmp);
-    std::vector<uint32_t> used(parts, 0);
-    for (uint32_t u : order) {
-        if (heap.empty()) break;
-        std::pop_heap(heap.begin(), heap.end(), cmp);
-        auto [load, q] = heap.back();
-        heap.pop_back();
-        const uint32_t cta = q / 4u, sub = q % 4u;
-        const uint32_t warp = sub + 4u * used[q]++;                  // warp w issues from scheduler w % 4
-        table[warp * grid + cta] = u;
-        if (used[q] < per_part) {
-            heap.emplace_back(load + unit_cost[u], q);
-            std::push_heap(heap.begin(), heap.end(), cmp);
-        }
-    }
-}
-
 cudaError_t fa_launch_prepare(const FaLaunch& L, int block, bool persistent)
 {
     return fa_launch_run(L, block, persistent, 0, nullptr);

@@ -81,3 +81,9 @@ extern "C" void hs_timer(const uint32_t* start, const uint32_t* ns, const uint8_
         o[4] = ex.tp & 0xFFFFu; o[5] = ex.tp >> 16; o[6] = ex.su & 0xFFFFu; o[7] = ex.su >> 16;
     }
 }
+
+// The persistent launch's first-wave placement (fa_pool_set_balance).
+extern "C" void hs_plan(const float* cost, uint32_t nunits, uint32_t grid, uint32_t warps, uint32_t* table)
+{
+    fa_plan_first_wave(cost, nunits, grid, warps, table);
+}

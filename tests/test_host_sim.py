@@ -38,6 +38,8 @@ def sim():
     L.hs_run.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
                          ctypes.c_int]
     L.fa_rom_set_scheme.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    L.hs_plan.restype = None
+    L.hs_plan.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]
     L.hs_timer.restype = None
     L.hs_timer.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
     return L
@@ -176,3 +178,43 @@ def test_lazy_timer_counting_equals_per_call_ticks(sim):
                                f"exact {exact[bad[0]]}")
         if start[2] == 1 and start[0] >= 1:
             assert exact[:, 3].any()                               # the run went through underflows
+
+
+@pytest.mark.parametrize("grid,warps,nunits", [(148, 32, 4236), (10, 8, 100), (5, 4, 7), (148, 28, 4144), (20, 32, 300)])
+def test_first_wave_plan(sim, grid, warps, nunits):
+    """fa_plan_first_wave (fa_pool_set_balance): slot warp * grid + cta gets
+    units 0 .. min(units, slots) - 1 exactly once (the device queue hands out
+    the rest), every unit on a warp of its (SM, scheduler) sub-partition
+    (warp % 4), at most warps / 4 per sub-partition, placed longest first on
+    the least-loaded one."""
+    rng = np.random.default_rng(grid * warps + nunits)
+    cost = np.concatenate([rng.choice([1.0, 1.1, 1.8, 17.0], nunits, p=[0.7, 0.2, 0.07, 0.03])]).astype(np.float32)
+    table = np.zeros(grid * warps, np.uint32)
+    sim.hs_plan(cost.ctypes.data, nunits, grid, warps, table.ctypes.data)
+    slots = grid * warps
+    first = min(nunits, slots)
+    used = table[table != 0xFFFFFFFF]
+    assert sorted(used.tolist()) == list(range(first))
+    parts = grid * 4
+    load = np.zeros(parts)
+    count = np.zeros(parts, int)
+    for slot, u in enumerate(table):
+        if u == 0xFFFFFFFF:
+            continue
+        warp, cta = divmod(slot, grid)
+        q = cta * 4 + warp % 4
+        load[q] += cost[u]
+        count[q] += 1
+    assert count.max() <= warps // 4
+    if nunits <= slots and count.max() < warps // 4:
+        # capacity never bound: longest-first keeps every load within one unit of the lightest
+        assert load.max() - load.min() <= cost.max() + 1e-4
+    elif (grid, warps, nunits) == (20, 32, 300):
+        raise AssertionError("the unconstrained case must exercise the balance check")
+    heaviest = np.argsort(-cost[:first], kind="stable")[:min(parts, first)]
+    qs = {}
+    for slot, u in enumerate(table):
+        if u != 0xFFFFFFFF:
+            warp, cta = divmod(slot, grid)
+            qs[int(u)] = cta * 4 + warp % 4
+    assert len({qs[int(u)] for u in heaviest}) == len(heaviest)
