@@ -87,3 +87,6 @@ extern "C" void hs_plan(const float* cost, uint32_t nunits, uint32_t grid, uint3
 {
     fa_plan_first_wave(cost, nunits, grid, warps, table);
 }
+
+// The threaded copy of host-buffer calls' outputs into the caller's memory.
+extern "C" void hs_host_copy(void* dst, const void* src, size_t bytes) { fa_host_copy(dst, src, bytes); }

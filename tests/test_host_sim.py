@@ -38,6 +38,8 @@ def sim():
     L.hs_run.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
                          ctypes.c_int]
     L.fa_rom_set_scheme.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    L.hs_host_copy.restype = None
+    L.hs_host_copy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
     L.hs_plan.restype = None
     L.hs_plan.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]
     L.hs_timer.restype = None
@@ -218,3 +220,16 @@ def test_first_wave_plan(sim, grid, warps, nunits):
             warp, cta = divmod(slot, grid)
             qs[int(u)] = cta * 4 + warp % 4
     assert len({qs[int(u)] for u in heaviest}) == len(heaviest)
+
+
+@pytest.mark.parametrize("nbytes", [0, 1, 4097, (2 << 20) - 1, 2 << 20, (5 << 20) + 3, (17 << 20) + 12345])
+def test_host_copy(sim, nbytes):
+    """fa_host_copy, the copy of a host-buffer call's outputs into the
+    caller's memory: one thread below 2 MB, up to 8 above, every byte in
+    place, nothing written past the end."""
+    rng = np.random.default_rng(nbytes)
+    src = rng.integers(0, 256, nbytes, dtype=np.uint8)
+    dst = np.full(nbytes + 64, 0x5A, np.uint8)
+    sim.hs_host_copy(dst.ctypes.data, src.ctypes.data, nbytes)
+    assert np.array_equal(dst[:nbytes], src)
+    assert (dst[nbytes:] == 0x5A).all()
