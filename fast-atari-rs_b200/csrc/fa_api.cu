@@ -527,6 +527,43 @@ extern "C" int fa_reset(fa_handle* h, uint8_t* obs_out)
     return FA_OK;
 }
 
+// Atari::new (src/atari.rs:240-247) as one rendering state column (FA_RROWS
+// words): the headless power-on column with the rendering Tia's defaults
+// (src/tia.rs:192-238), then the two bus reads of Cpu::reset
+// (src/cpu.rs:125-134), which each tick three TIA clocks (in horizontal blank
+// of scanline 0: nothing renders) and one PIA clock.
+void fa_render_power_on_column(const uint8_t* image, uint32_t nbanks, int scheme, uint32_t hot_lo, uint32_t* col)
+{
+    memset(col, 0, FA_RROWS * sizeof(uint32_t));
+    fa_power_on_column(image, nbanks, scheme, hot_lo, col);
+    fa_state s;
+    fa_unpack_column(col, 1, scheme, s);
+    s.paddle0 = 128;
+    s.paddle1 = 128;
+    s.tia_clock = 6;
+    // Pia::tick twice from its default (timer 0, prescaler 1, select 1).
+    uint32_t tv = s.timer_value, ps = s.timer_prescaler, sel = s.timer_prescaler_select, uf = s.timer_underflow;
+    for (int c = 0; c < 2; c++) {
+        if (tv == 0 && uf) { tv = 0xFF; continue; }
+        ps = (ps - 1u) & 0xFFFFu;
+        if (ps == 0) {
+            ps = uf ? 1u : sel;
+            if (tv == 0) { uf = 1; tv = 0xFF; } else tv -= 1u;
+        }
+    }
+    s.timer_value = (uint16_t)tv;
+    s.timer_prescaler = (uint16_t)ps;
+    s.timer_underflow = (uint8_t)uf;
+    fa_pack_column(s, col, 1);
+    // Rendering rows: pending_top 32 (RB_PTOP in the RB_* words), visible_top 32,
+    // vblank_top 262, input latches 0x80.
+    uint8_t rb[FA_RPRIV_BYTES - FA_PRIV_BYTES] = {};
+    rb[RB_PTOP - FA_PRIV_BYTES] = 32;
+    for (uint32_t w = 0; w < (FA_RPRIV_WORDS - FA_PRIV_WORDS); w++) memcpy(&col[FA_RROW_EXTRA + w], rb + 4 * w, 4);
+    col[RR_VTOP] = 32u | (262u << 16);
+    col[RR_FLAGS] = 4u | 8u;
+}
+
 // First-wave placement of a persistent launch (fa_pool_set_balance); host
 // code, kept here so the host tests can run it.
 void fa_plan_first_wave(const float* unit_cost, uint32_t nunits, uint32_t grid, uint32_t warps, uint32_t* table)

@@ -193,3 +193,5 @@ void fa_pack_column(const fa_state& s, uint32_t* col, size_t stride);
 void fa_unpack_column(const uint32_t* col, size_t stride, int scheme, fa_state& s);
 // Power-on state of HeadlessAtari::new (src/atari.rs:562-569) for a bank image.
 void fa_power_on_column(const uint8_t* bank_image, uint32_t nbanks, int scheme, uint32_t hot_lo, uint32_t* col);
+// The rendering console's power-on column: FA_RROWS words.
+void fa_render_power_on_column(const uint8_t* image, uint32_t nbanks, int scheme, uint32_t hot_lo, uint32_t* col);

@@ -34,7 +34,7 @@
 
 #include "../../include/fast_atari.h"
 #include "fa_internal.h"
-#include "fa_run.cuh"
+#include "fa_render.cuh"
 
 struct FaRenderLaunch {
     const uint8_t* rom;
@@ -52,99 +52,6 @@ struct FaRenderLaunch {
 };
 
 namespace fa {
-
-// One rendering console per lane: HeadlessAtari's frame loop with the
-// rendering console's per-cycle run_one_cycle (src/atari.rs:284-318).
-template <bool SLICED>
-struct RRunner {
-    Emu<32, true, SLICED> e;
-    uint32_t f, phase, fcyc;
-    bool active;
-
-    // set_action, then run_frame, which does nothing for a halted console
-    // (src/atari.rs:250-270, 284-306): a halted console's inputs still take
-    // the frame's action.
-    __device__ __forceinline__ bool begin_frame()
-    {
-        const FaGroup* G = e.G;
-        if (G->actions) e.apply_action(G->actions[(size_t)f * G->act_stride + e.i]);
-        if (e.row(R_STATUS) & FA_STATUS_HALT_MASK) return false;
-        e.tw &= ~TW_FCOMP;
-        e.bank &= 7u;
-        fcyc = 0;
-        phase = e.vsync_on() ? 0u : 1u;
-        return true;
-    }
-    // One run_one_cycle: a WSYNC cycle (tick_components) or an instruction,
-    // then the frame-end checks of run_frame.
-    __device__ __forceinline__ bool one()
-    {
-        uint32_t n;
-        if (e.wsync()) e.settle();                                   // the wait starts where the beam is
-        if (e.wsync()) {
-            // The cycles of a WSYNC wait up to the end of the line, cut where
-            // a per-cycle frame check would first fire: nothing else changes
-            // from one cycle of the wait to the next.
-            n = (228u - e.clock + 2u) / 3u;
-            uint32_t lim;
-            if (phase == 0u) lim = e.vsync_on() ? FA_VSYNC_BUDGET + 1u - fcyc : 1u;
-            else lim = FA_FRAME_CYCLE_CAP + 1u - fcyc;
-            n = n < lim ? n : lim;
-            e.rcycles(n);
-        } else {
-            e.done = 0u - e.lag;
-            n = e.step();
-            if (n == 0) {
-                // The reference's opcode fetch was a bus access (one cycle of
-                // TIA and PIA) before it stopped (src/cpu.rs:1139-1141): the
-                // TIA and PIA are owed up to the end of that cycle.
-                e.lag = 1u - e.done;
-                e.fold_cycles();
-                e.set_status(FA_STATUS_ILLEGAL_OPCODE);
-                active = false;
-                return false;
-            }
-            e.lag = n - e.done;
-            e.instr++;
-            e.cyc_acc += n;
-        }
-        fcyc += n;
-        if (phase == 0u) {
-            if (fcyc > FA_VSYNC_BUDGET) {
-                e.fold_cycles();
-                e.set_status(FA_STATUS_VSYNC_BUDGET);
-                active = false;
-                return false;
-            }
-            if (!e.vsync_on()) phase = 1u;
-        } else {
-            const bool cap = fcyc > FA_FRAME_CYCLE_CAP;
-            if (cap || e.vsync_on()) {
-                if (cap) e.set_status(FA_STATUS_CYCLE_CAP);
-                e.fb_observe();                                      // before the next frame's action moves the pins
-                e.fold_cycles();
-                e.row(R_FRAME) += 1u;
-                f++;
-                if (f >= e.G->k || !begin_frame()) { active = false; return false; }
-                return false;
-            }
-        }
-        return e.wsync();
-    }
-    __device__ __forceinline__ uint32_t key(uint32_t sched) const
-    {
-        const uint32_t fc = f < 0x7Fu ? f : 0x7Fu;
-        const uint32_t mid = sched == FA_SCHED_LINE ? (e.scanline < 0x1FFu ? e.scanline : 0x1FFu) : (e.bank >> 3);
-        return (fc << 25) | (mid << 16) | e.pc;
-    }
-    // A WSYNC wait is consumed without going back to the warp scheduler.
-    __device__ __forceinline__ void iterate()
-    {
-#pragma unroll 1
-        while (one() && active) {
-        }
-    }
-};
 
 // 128 registers: the pixel code and the bus run with almost no spills, and
 // 16 warps are resident per SM (one 512-thread CTA at 16 warps, the default,
@@ -190,74 +97,12 @@ __global__ void __maxnreg__(128) fa_render_run(const __grid_constant__ FaRenderL
     const bool valid = i < L.n;
 
     RRunner<SLICED> r;
-    r.f = 0;
-    r.phase = 0;
-    r.fcyc = 0;
-    r.active = false;
-    Emu<32, true, SLICED>& e = r.e;
-    e.pv = (uint8_t*)(slab + lane);
-    e.G = &sg;
-    e.i = i;
-    e.rom = smem;
-    e.hot_lo = L.hot_lo;
-    e.nbanks = L.nbanks;
-    e.instr = 0;
-    e.cyc_acc = 0;
-    e.pc = 0;
-    e.bank = 0;
-    e.slices = 0;
-    e.scanline = 0;
-    e.done = 0;
-    e.lag = 0;
-    e.sc = 0;
-    e.zr = 0;
-    e.vtop = 0;
-    e.rx = 0;
-    e.fbp = L.fb + (size_t)(valid ? i : 0u) * FA_FB_BYTES;
     uint32_t* col = L.state + i;
-    const uint32_t S = L.stride;
-    if (valid) {
-        uint32_t* w = slab + lane;
-#pragma unroll 4
-        for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) w[k * 32u] = col[(size_t)k * S];
-        for (uint32_t k = FA_PRIV_WORDS; k < FA_RPRIV_WORDS; k++)
-            w[k * 32u] = col[(size_t)(FA_RROW_EXTRA + (k - FA_PRIV_WORDS)) * S];
-        e.load_hot(col, S);
-        e.vtop = col[(size_t)RR_VTOP * S];
-        e.rx = e.clock;
-        e.fb_resume();
-        const uint32_t fl = col[(size_t)RR_FLAGS * S];
-        e.tw |= ((fl & 1u) ? TW_HMOVE : 0u) | ((fl & 2u) ? TW_LATCH : 0u) | ((fl & 4u) ? TW_L4 : 0u) |
-                ((fl & 8u) ? TW_L5 : 0u);
-        if (L.k > 0) r.active = r.begin_frame();
-    }
+    render_begin(r, slab + lane, &sg, i, valid, smem, L.fb + (size_t)(valid ? i : 0u) * FA_FB_BYTES, col, L.stride);
     const uint32_t rounds = run_lanes(r, L.sched);
-    if (valid) {
-        e.fb_observe();
-        e.fold_cycles();
-        // A console that halted before the call's last frame took the later
-        // frames' set_action too; the last one is what its inputs hold.
-        if (L.actions && r.f + 1u < L.k && (e.row(R_STATUS) & FA_STATUS_HALT_MASK))
-            e.apply_action(L.actions[(size_t)(L.k - 1u) * L.n + i]);
-        uint32_t* w = slab + lane;
-#pragma unroll 4
-        for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) col[(size_t)k * S] = w[k * 32u];
-        for (uint32_t k = FA_PRIV_WORDS; k < FA_RPRIV_WORDS; k++)
-            col[(size_t)(FA_RROW_EXTRA + (k - FA_PRIV_WORDS)) * S] = w[k * 32u];
-        e.store_hot(col, S);
-        col[(size_t)RR_VTOP * S] = e.vtop;
-        col[(size_t)RR_FLAGS * S] = ((e.tw & TW_HMOVE) ? 1u : 0u) | ((e.tw & TW_LATCH) ? 2u : 0u) |
-                                    ((e.tw & TW_L4) ? 4u : 0u) | ((e.tw & TW_L5) ? 8u : 0u);
-        if (L.obs) {
-            uint4* o = (uint4*)(L.obs + (size_t)i * 128u);
-#pragma unroll
-            for (uint32_t q = 0; q < 8u; q++)
-                o[q] = make_uint4(w[(4u * q) * 32u], w[(4u * q + 1u) * 32u], w[(4u * q + 2u) * 32u],
-                                  w[(4u * q + 3u) * 32u]);
-        }
-    }
+    if (valid) render_end(r, slab + lane, col, L.stride, L.obs ? L.obs + (size_t)i * 128u : nullptr);
     if (L.instr) {
-        uint32_t c = valid ? e.instr : 0u;
+        uint32_t c = valid ? r.e.instr : 0u;
         for (int d = 16; d > 0; d >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, d);
         if (lane == 0 && c) atomicAdd(L.instr, (unsigned long long)c);
     }
@@ -465,40 +310,11 @@ int copy_d2h(fa_render* r, uint8_t* dst, const uint8_t* src, size_t bytes)
     return FA_OK;
 }
 
-// Atari::new (src/atari.rs:240-247) as one state column: the headless power-on
-// column with the rendering Tia's defaults (src/tia.rs:192-238), then the two
-// bus reads of Cpu::reset (src/cpu.rs:125-134), which each tick three TIA
-// clocks (in horizontal blank of scanline 0: nothing renders) and one PIA clock.
+// Atari::new (src/atari.rs:240-247) as one state column.
 void render_power_on(const fa_render* r, std::vector<uint32_t>& col)
 {
     col.assign(FA_RROWS, 0u);
-    fa_power_on_column(r->image.data(), r->nbanks, r->scheme, r->hot_lo, col.data());
-    fa_state s;
-    fa_unpack_column(col.data(), 1, r->scheme, s);
-    s.paddle0 = 128;
-    s.paddle1 = 128;
-    s.tia_clock = 6;
-    // Pia::tick twice from its default (timer 0, prescaler 1, select 1).
-    uint32_t tv = s.timer_value, ps = s.timer_prescaler, sel = s.timer_prescaler_select, uf = s.timer_underflow;
-    for (int c = 0; c < 2; c++) {
-        if (tv == 0 && uf) { tv = 0xFF; continue; }
-        ps = (ps - 1u) & 0xFFFFu;
-        if (ps == 0) {
-            ps = uf ? 1u : sel;
-            if (tv == 0) { uf = 1; tv = 0xFF; } else tv -= 1u;
-        }
-    }
-    s.timer_value = (uint16_t)tv;
-    s.timer_prescaler = (uint16_t)ps;
-    s.timer_underflow = (uint8_t)uf;
-    fa_pack_column(s, col.data(), 1);
-    // Rendering rows: pending_top 32 (RB_PTOP in the RB_* words), visible_top 32,
-    // vblank_top 262, input latches 0x80.
-    uint8_t rb[FA_RPRIV_BYTES - FA_PRIV_BYTES] = {};
-    rb[RB_PTOP - FA_PRIV_BYTES] = 32;
-    for (uint32_t w = 0; w < (FA_RPRIV_WORDS - FA_PRIV_WORDS); w++) memcpy(&col[FA_RROW_EXTRA + w], rb + 4 * w, 4);
-    col[RR_VTOP] = 32u | (262u << 16);
-    col[RR_FLAGS] = 4u | 8u;
+    fa_render_power_on_column(r->image.data(), r->nbanks, r->scheme, r->hot_lo, col.data());
 }
 
 int enqueue(fa_render* r, const uint8_t* d_actions, int k, uint8_t* d_obs, cudaStream_t s)

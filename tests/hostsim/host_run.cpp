@@ -6,6 +6,7 @@
 #include "shim.h"
 #include "../../fast-atari-rs_b200/csrc/fa_api.cu"
 #include "../../fast-atari-rs_b200/csrc/fa_run.cuh"
+#include "../../fast-atari-rs_b200/csrc/fa_render.cuh"
 
 template <bool SL>
 static void run_one(const FaGroup& G, uint32_t i, uint8_t* rom, unsigned long long* instr)
@@ -90,3 +91,56 @@ extern "C" void hs_plan(const float* cost, uint32_t nunits, uint32_t grid, uint3
 
 // The threaded copy of host-buffer calls' outputs into the caller's memory.
 extern "C" void hs_host_copy(void* dst, const void* src, size_t bytes) { fa_host_copy(dst, src, bytes); }
+
+// The rendering console (fa_render.cu's per-console code, fa_render.cuh) on
+// the host, one console at a time, the way fa_render_reset and
+// fa_render_step_multi drive it: power-on column, one frame without an
+// action (frame numbers then restart at 0), then `calls` calls of k frames
+// with actions[call][frame][console].  Returns the framebuffers (n x 30,720),
+// the states and the RAM after the last call; -1 for a bad ROM.
+template <bool SL>
+static void render_one(FaGroup& G, uint32_t i, const uint8_t* rom, uint8_t* fb, uint8_t* obs)
+{
+    uint32_t slab[FA_RSLAB_WORDS * 32];
+    memset(slab, 0, sizeof(slab));
+    fa::RRunner<SL> r;
+    uint32_t* col = G.state + i;
+    fa::render_begin(r, slab, &G, i, true, rom, fb + (size_t)i * FA_FB_BYTES, col, G.stride);
+    while (r.active) r.iterate();
+    fa::render_end(r, slab, col, G.stride, obs ? obs + (size_t)i * 128u : nullptr);
+}
+
+extern "C" long long hs_render(const uint8_t* rom, size_t len, size_t n, const uint8_t* actions, int calls, int k,
+                               uint8_t* fb, fa_state* st, uint8_t* ram)
+{
+    std::vector<uint8_t> img;
+    int scheme = 0;
+    uint32_t nbanks = 0, hot_lo = 0;
+    if (fa_make_bank_image(rom, len, img, scheme, &nbanks, &hot_lo)) return -1;
+    std::vector<uint8_t> simg(img.size() + 64, 0);
+    memcpy(simg.data(), img.data(), img.size());
+    std::vector<uint32_t> col(FA_RROWS);
+    fa_render_power_on_column(img.data(), nbanks, scheme, hot_lo, col.data());
+    std::vector<uint32_t> rows((size_t)FA_RROWS * n);
+    for (uint32_t w = 0; w < FA_RROWS; w++)
+        for (size_t i = 0; i < n; i++) rows[(size_t)w * n + i] = col[w];
+    memset(fb, 0, n * (size_t)FA_FB_BYTES);
+    FaGroup G;
+    memset(&G, 0, sizeof(G));
+    G.rom = simg.data(); G.state = rows.data(); G.stride = (uint32_t)n; G.n = (uint32_t)n;
+    G.act_stride = (uint32_t)n; G.nbanks = nbanks; G.hot_lo = hot_lo;
+    const bool sliced = fa_map_kind(hot_lo) != 0;
+    long long instr = 0;
+    for (int c = -1; c < calls; c++) {
+        G.actions = c < 0 ? nullptr : actions + (size_t)c * k * n;
+        G.k = c < 0 ? 1u : (uint32_t)k;
+        for (uint32_t i = 0; i < n; i++) {
+            if (sliced) render_one<true>(G, i, simg.data(), fb, ram);
+            else render_one<false>(G, i, simg.data(), fb, ram);
+        }
+        if (c < 0)
+            for (size_t i = 0; i < n; i++) rows[(size_t)R_FRAME * n + i] = 0;
+    }
+    for (size_t i = 0; i < n; i++) fa_unpack_column(rows.data() + i, n, scheme, st[i]);
+    return instr;
+}

@@ -38,6 +38,9 @@ def sim():
     L.hs_run.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
                          ctypes.c_int]
     L.fa_rom_set_scheme.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    L.hs_render.restype = ctypes.c_longlong
+    L.hs_render.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_int,
+                            ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.hs_host_copy.restype = None
     L.hs_host_copy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
     L.hs_plan.restype = None
@@ -233,3 +236,39 @@ def test_host_copy(sim, nbytes):
     sim.hs_host_copy(dst.ctypes.data, src.ctypes.data, nbytes)
     assert np.array_equal(dst[:nbytes], src)
     assert (dst[nbytes:] == 0x5A).all()
+
+
+@pytest.mark.parametrize("name", ["render", "divergence", "mixed_32k", "e0", "3f16"])
+def test_rendering_console_device_code_matches_oracle(sim, name):
+    """The rendering console's device code (fa_render.cuh over fa_device.cuh
+    with RENDER) compiled for the host, driven as fa_render_reset and
+    fa_render_step_multi drive it, against the rendering oracle (the
+    reference's Atari + Tia restated): framebuffers, RAM, registers, cycles,
+    beam, timer and every TIA register after two calls of 3 frames."""
+    from fa_pkg import fa
+    from test_gpu_render import check
+    c, code = {"render": (carts.render_cart(), None), "divergence": (carts.divergence_cart(), None),
+               "mixed_32k": (carts.mixed_carts()[3], None), "e0": (carts.e0_cart(), 4),
+               "3f16": (carts.f3_cart(16384), 5)}[name]
+    rom = c.rom
+    r = np.frombuffer(rom, np.uint8).copy()
+    if code is not None:
+        sim.fa_rom_set_scheme(r.ctypes.data, len(r), code)
+        oracle.set_rom_scheme(rom, code)
+    try:
+        n, calls, k = 6, 2, 3
+        acts = np.stack([carts.actions(seed=70 + i, n=n, frames=k) for i in range(calls)])
+        fb = np.zeros((n, 192, 160), np.uint8)
+        ram = np.zeros((n, 128), np.uint8)
+        st = np.zeros(n, fa.STATE_DTYPE)
+        a = np.ascontiguousarray(acts, dtype=np.uint8)
+        assert sim.hs_render(r.ctypes.data, len(r), n, a.ctypes.data, calls, k, fb.ctypes.data, st.ctypes.data,
+                             ram.ctypes.data) >= 0
+        consoles = oracle.render_reset(rom, n)
+        for i in range(calls):
+            oracle.render_steps(consoles, acts[i])
+        check(fb, ram, st, consoles, f"{name} on the host")
+    finally:
+        if code is not None:
+            sim.fa_rom_set_scheme(r.ctypes.data, len(r), -1)
+            oracle.set_rom_scheme(rom, "auto")
