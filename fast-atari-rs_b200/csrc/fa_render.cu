@@ -97,12 +97,74 @@ __global__ void __maxnreg__(128) fa_render_run(const __grid_constant__ FaRenderL
     const bool valid = i < L.n;
 
     RRunner<SLICED> r;
+    r.f = 0;
+    r.phase = 0;
+    r.fcyc = 0;
+    r.active = false;
+    Emu<32, true, SLICED>& e = r.e;
+    e.pv = (uint8_t*)(slab + lane);
+    e.G = &sg;
+    e.i = i;
+    e.rom = smem;
+    e.hot_lo = L.hot_lo;
+    e.nbanks = L.nbanks;
+    e.instr = 0;
+    e.cyc_acc = 0;
+    e.pc = 0;
+    e.bank = 0;
+    e.slices = 0;
+    e.scanline = 0;
+    e.done = 0;
+    e.lag = 0;
+    e.sc = 0;
+    e.zr = 0;
+    e.vtop = 0;
+    e.rx = 0;
+    e.fbp = L.fb + (size_t)(valid ? i : 0u) * FA_FB_BYTES;
     uint32_t* col = L.state + i;
-    render_begin(r, slab + lane, &sg, i, valid, smem, L.fb + (size_t)(valid ? i : 0u) * FA_FB_BYTES, col, L.stride);
+    const uint32_t S = L.stride;
+    if (valid) {
+        uint32_t* w = slab + lane;
+#pragma unroll 4
+        for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) w[k * 32u] = col[(size_t)k * S];
+        for (uint32_t k = FA_PRIV_WORDS; k < FA_RPRIV_WORDS; k++)
+            w[k * 32u] = col[(size_t)(FA_RROW_EXTRA + (k - FA_PRIV_WORDS)) * S];
+        e.load_hot(col, S);
+        e.vtop = col[(size_t)RR_VTOP * S];
+        e.rx = e.clock;
+        e.fb_resume();
+        const uint32_t fl = col[(size_t)RR_FLAGS * S];
+        e.tw |= ((fl & 1u) ? TW_HMOVE : 0u) | ((fl & 2u) ? TW_LATCH : 0u) | ((fl & 4u) ? TW_L4 : 0u) |
+                ((fl & 8u) ? TW_L5 : 0u);
+        if (L.k > 0) r.active = r.begin_frame();
+    }
     const uint32_t rounds = run_lanes(r, L.sched);
-    if (valid) render_end(r, slab + lane, col, L.stride, L.obs ? L.obs + (size_t)i * 128u : nullptr);
+    if (valid) {
+        e.fb_observe();
+        e.fold_cycles();
+        // A console that halted before the call's last frame took the later
+        // frames' set_action too; the last one is what its inputs hold.
+        if (L.actions && r.f + 1u < L.k && (e.row(R_STATUS) & FA_STATUS_HALT_MASK))
+            e.apply_action(L.actions[(size_t)(L.k - 1u) * L.n + i]);
+        uint32_t* w = slab + lane;
+#pragma unroll 4
+        for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) col[(size_t)k * S] = w[k * 32u];
+        for (uint32_t k = FA_PRIV_WORDS; k < FA_RPRIV_WORDS; k++)
+            col[(size_t)(FA_RROW_EXTRA + (k - FA_PRIV_WORDS)) * S] = w[k * 32u];
+        e.store_hot(col, S);
+        col[(size_t)RR_VTOP * S] = e.vtop;
+        col[(size_t)RR_FLAGS * S] = ((e.tw & TW_HMOVE) ? 1u : 0u) | ((e.tw & TW_LATCH) ? 2u : 0u) |
+                                    ((e.tw & TW_L4) ? 4u : 0u) | ((e.tw & TW_L5) ? 8u : 0u);
+        if (L.obs) {
+            uint4* o = (uint4*)(L.obs + (size_t)i * 128u);
+#pragma unroll
+            for (uint32_t q = 0; q < 8u; q++)
+                o[q] = make_uint4(w[(4u * q) * 32u], w[(4u * q + 1u) * 32u], w[(4u * q + 2u) * 32u],
+                                  w[(4u * q + 3u) * 32u]);
+        }
+    }
     if (L.instr) {
-        uint32_t c = valid ? r.e.instr : 0u;
+        uint32_t c = valid ? e.instr : 0u;
         for (int d = 16; d > 0; d >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, d);
         if (lane == 0 && c) atomicAdd(L.instr, (unsigned long long)c);
     }

@@ -1,6 +1,8 @@
-// fa_render.cuh — one rendering console per lane: the frame loop and the
-// per-console start and end of a launch, shared by the rendering kernel
-// (fa_render.cu) and the host tests that run the same code on the CPU.
+// fa_render.cuh — one rendering console per lane: the frame loop, shared by
+// the rendering kernel (fa_render.cu) and the host tests that run the same
+// code on the CPU.  The kernel's start and end of a launch (the console's
+// rows in and out of HBM) stay in the kernel body: moved into helpers here,
+// the same steps ran 8 % slower on the render cart.
 #pragma once
 
 #include "fa_run.cuh"
@@ -99,79 +101,5 @@ struct RRunner {
         }
     }
 };
-
-// A console's start of a launch: its private bytes (RAM and the rendering
-// registers) from the HBM rows into its slab words w (32-lane interleave),
-// its packed state, the beam where the last call left it, its framebuffer
-// sector, the TIA latches, then the first frame's set_action.
-template <bool SLICED>
-__device__ __forceinline__ void render_begin(RRunner<SLICED>& r, uint32_t* w, const FaGroup* G, uint32_t i, bool valid,
-                                             const uint8_t* rom, uint8_t* fbp, uint32_t* col, uint32_t S)
-{
-    r.f = 0;
-    r.phase = 0;
-    r.fcyc = 0;
-    r.active = false;
-    Emu<32, true, SLICED>& e = r.e;
-    e.pv = (uint8_t*)w;
-    e.G = G;
-    e.i = i;
-    e.rom = rom;
-    e.hot_lo = G->hot_lo;
-    e.nbanks = G->nbanks;
-    e.instr = 0;
-    e.cyc_acc = 0;
-    e.pc = 0;
-    e.bank = 0;
-    e.slices = 0;
-    e.scanline = 0;
-    e.done = 0;
-    e.lag = 0;
-    e.sc = 0;
-    e.zr = 0;
-    e.vtop = 0;
-    e.rx = 0;
-    e.fbp = fbp;
-    if (!valid) return;
-#pragma unroll 4
-    for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) w[k * 32u] = col[(size_t)k * S];
-    for (uint32_t k = FA_PRIV_WORDS; k < FA_RPRIV_WORDS; k++) w[k * 32u] = col[(size_t)(FA_RROW_EXTRA + (k - FA_PRIV_WORDS)) * S];
-    e.load_hot(col, S);
-    e.vtop = col[(size_t)RR_VTOP * S];
-    e.rx = e.clock;
-    e.fb_resume();
-    const uint32_t fl = col[(size_t)RR_FLAGS * S];
-    e.tw |= ((fl & 1u) ? TW_HMOVE : 0u) | ((fl & 2u) ? TW_LATCH : 0u) | ((fl & 4u) ? TW_L4 : 0u) | ((fl & 8u) ? TW_L5 : 0u);
-    if (G->k > 0) r.active = r.begin_frame();
-}
-
-// A console's end of a launch: the framebuffer as it can be seen, the owed
-// cycles, then everything back to its HBM rows, and its RAM to obs (128
-// bytes, 16-byte aligned) when obs is not null.
-template <bool SLICED>
-__device__ __forceinline__ void render_end(RRunner<SLICED>& r, uint32_t* w, uint32_t* col, uint32_t S, uint8_t* obs)
-{
-    Emu<32, true, SLICED>& e = r.e;
-    const FaGroup* G = e.G;
-    e.fb_observe();
-    e.fold_cycles();
-    // A console that halted before the call's last frame took the later
-    // frames' set_action too; the last one is what its inputs hold.
-    if (G->actions && r.f + 1u < G->k && (e.row(R_STATUS) & FA_STATUS_HALT_MASK))
-        e.apply_action(G->actions[(size_t)(G->k - 1u) * G->act_stride + e.i]);
-#pragma unroll 4
-    for (uint32_t k = 0; k < FA_PRIV_WORDS; k++) col[(size_t)k * S] = w[k * 32u];
-    for (uint32_t k = FA_PRIV_WORDS; k < FA_RPRIV_WORDS; k++) col[(size_t)(FA_RROW_EXTRA + (k - FA_PRIV_WORDS)) * S] = w[k * 32u];
-    e.store_hot(col, S);
-    col[(size_t)RR_VTOP * S] = e.vtop;
-    col[(size_t)RR_FLAGS * S] = ((e.tw & TW_HMOVE) ? 1u : 0u) | ((e.tw & TW_LATCH) ? 2u : 0u) |
-                                ((e.tw & TW_L4) ? 4u : 0u) | ((e.tw & TW_L5) ? 8u : 0u);
-    if (obs) {
-        uint4* o = (uint4*)obs;
-#pragma unroll
-        for (uint32_t q = 0; q < 8u; q++)
-            o[q] = make_uint4(w[(4u * q) * 32u], w[(4u * q + 1u) * 32u], w[(4u * q + 2u) * 32u], w[(4u * q + 3u) * 32u]);
-    }
-}
 
 }  // namespace fa

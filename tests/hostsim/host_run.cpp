@@ -92,22 +92,74 @@ extern "C" void hs_plan(const float* cost, uint32_t nunits, uint32_t grid, uint3
 // The threaded copy of host-buffer calls' outputs into the caller's memory.
 extern "C" void hs_host_copy(void* dst, const void* src, size_t bytes) { fa_host_copy(dst, src, bytes); }
 
-// The rendering console (fa_render.cu's per-console code, fa_render.cuh) on
-// the host, one console at a time, the way fa_render_reset and
+// The rendering console (RRunner, fa_render.cuh, over the device console)
+// on the host, one console at a time, the way fa_render_reset and
 // fa_render_step_multi drive it: power-on column, one frame without an
 // action (frame numbers then restart at 0), then `calls` calls of k frames
 // with actions[call][frame][console].  Returns the framebuffers (n x 30,720),
 // the states and the RAM after the last call; -1 for a bad ROM.
+//
+// render_one restates fa_render_run's start and end of a launch for one
+// console (the kernel keeps those steps in its own body): private words and
+// packed state in from the rows, the beam and framebuffer resumed, the TIA
+// latches from the flags row, the first frame's set_action; at the end the
+// visible framebuffer, the owed cycles, a halted console's last action, the
+// rows written back and the RAM to obs.
 template <bool SL>
 static void render_one(FaGroup& G, uint32_t i, const uint8_t* rom, uint8_t* fb, uint8_t* obs)
 {
-    uint32_t slab[FA_RSLAB_WORDS * 32];
-    memset(slab, 0, sizeof(slab));
-    fa::RRunner<SL> r;
+    using namespace fa;
+    uint32_t w[FA_RSLAB_WORDS * 32];
+    memset(w, 0, sizeof(w));
+    RRunner<SL> r;
+    r.f = 0;
+    r.phase = 0;
+    r.fcyc = 0;
+    r.active = false;
+    Emu<32, true, SL>& e = r.e;
+    e.pv = (uint8_t*)w;
+    e.G = &G;
+    e.i = i;
+    e.rom = rom;
+    e.hot_lo = G.hot_lo;
+    e.nbanks = G.nbanks;
+    e.instr = 0;
+    e.cyc_acc = 0;
+    e.pc = 0;
+    e.bank = 0;
+    e.slices = 0;
+    e.scanline = 0;
+    e.done = 0;
+    e.lag = 0;
+    e.sc = 0;
+    e.zr = 0;
+    e.vtop = 0;
+    e.rx = 0;
+    e.fbp = fb + (size_t)i * FA_FB_BYTES;
     uint32_t* col = G.state + i;
-    fa::render_begin(r, slab, &G, i, true, rom, fb + (size_t)i * FA_FB_BYTES, col, G.stride);
+    const uint32_t S = G.stride;
+    for (uint32_t q = 0; q < FA_PRIV_WORDS; q++) w[q * 32u] = col[(size_t)q * S];
+    for (uint32_t q = FA_PRIV_WORDS; q < FA_RPRIV_WORDS; q++) w[q * 32u] = col[(size_t)(FA_RROW_EXTRA + (q - FA_PRIV_WORDS)) * S];
+    e.load_hot(col, S);
+    e.vtop = col[(size_t)RR_VTOP * S];
+    e.rx = e.clock;
+    e.fb_resume();
+    const uint32_t fl = col[(size_t)RR_FLAGS * S];
+    e.tw |= ((fl & 1u) ? TW_HMOVE : 0u) | ((fl & 2u) ? TW_LATCH : 0u) | ((fl & 4u) ? TW_L4 : 0u) | ((fl & 8u) ? TW_L5 : 0u);
+    if (G.k > 0) r.active = r.begin_frame();
     while (r.active) r.iterate();
-    fa::render_end(r, slab, col, G.stride, obs ? obs + (size_t)i * 128u : nullptr);
+    e.fb_observe();
+    e.fold_cycles();
+    if (G.actions && r.f + 1u < G.k && (e.row(R_STATUS) & FA_STATUS_HALT_MASK))
+        e.apply_action(G.actions[(size_t)(G.k - 1u) * G.act_stride + i]);
+    for (uint32_t q = 0; q < FA_PRIV_WORDS; q++) col[(size_t)q * S] = w[q * 32u];
+    for (uint32_t q = FA_PRIV_WORDS; q < FA_RPRIV_WORDS; q++) col[(size_t)(FA_RROW_EXTRA + (q - FA_PRIV_WORDS)) * S] = w[q * 32u];
+    e.store_hot(col, S);
+    col[(size_t)RR_VTOP * S] = e.vtop;
+    col[(size_t)RR_FLAGS * S] = ((e.tw & TW_HMOVE) ? 1u : 0u) | ((e.tw & TW_LATCH) ? 2u : 0u) | ((e.tw & TW_L4) ? 4u : 0u) |
+                                ((e.tw & TW_L5) ? 8u : 0u);
+    if (obs)
+        for (uint32_t q = 0; q < 32u; q++) memcpy(obs + (size_t)i * 128u + 4u * q, &w[q * 32u], 4);
 }
 
 extern "C" long long hs_render(const uint8_t* rom, size_t len, size_t n, const uint8_t* actions, int calls, int k,

@@ -240,9 +240,10 @@ def test_host_copy(sim, nbytes):
 
 @pytest.mark.parametrize("name", ["render", "divergence", "mixed_32k", "e0", "3f16"])
 def test_rendering_console_device_code_matches_oracle(sim, name):
-    """The rendering console's device code (fa_render.cuh over fa_device.cuh
-    with RENDER) compiled for the host, driven as fa_render_reset and
-    fa_render_step_multi drive it, against the rendering oracle (the
+    """The rendering console's device code (fa_render.cuh's frame loop over
+    fa_device.cuh with RENDER) compiled for the host, driven as
+    fa_render_reset and fa_render_step_multi drive it (the kernel's start and
+    end of a launch restated in host_run.cpp), against the rendering oracle (the
     reference's Atari + Tia restated): framebuffers, RAM, registers, cycles,
     beam, timer and every TIA register after two calls of 3 frames."""
     from fa_pkg import fa
