@@ -55,8 +55,11 @@ STATE_DTYPE = np.dtype([
     ("bank", "u1"), ("scheme", "u1"), ("_pad_end", "u1", (2,)),
     ("mapper", "u1", (2,)), ("_pad_ext", "u1"),
     ("cycles", "<u8"), ("frame_no", "<u4"), ("run_status", "<u4"),
+    ("dpc_counter", "<u2", (8,)), ("dpc_top", "u1", (8,)), ("dpc_bottom", "u1", (8,)),
+    ("dpc_flags", "u1"), ("dpc_music", "u1"), ("dpc_random", "u1"), ("_pad_dpc", "u1"),
+    ("dpc_osc", "<u4"),
 ])
-assert STATE_DTYPE.itemsize == 240
+assert STATE_DTYPE.itemsize == 280
 
 # Symbols declared in include/fast_atari.h, with ctypes signatures.
 _vp, _u8p, _sz, _i, _u32 = ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint8), ctypes.c_size_t, ctypes.c_int, ctypes.c_uint32
@@ -218,7 +221,7 @@ def wait_limit_ns() -> int:
     return int(lib().fa_wait_limit_ns_get())
 
 
-SCHEME_NAMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "auto": -1}
+SCHEME_NAMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "dpc": 6, "auto": -1}
 
 
 def _scheme_code(scheme) -> int:

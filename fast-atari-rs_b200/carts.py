@@ -906,6 +906,143 @@ def f3_cart(size: int = 16384, seed: int = 7, lines: int = 64) -> Cart:
     return Cart(CartSpec(f"3f_{size // 1024}k", size, seed, wsync_density=1.0), rom, labels, scheme="3f")
 
 
+DPC_BANKID = 0xFE80
+
+
+def dpc_cart(seed: int = 8, lines: int = 48, dump_tail: bool = False) -> Cart:
+    """Activision DPC cart (Pitfall II's scheme): two 4K program banks, then
+    2K of display data; 10,240 bytes, or 10,495 with the 255-byte tail some
+    dumps of the cart carry.  Both banks hold the same code at the same
+    addresses (only the bank-id byte at $FE80 and the ROM data differ), so a
+    switch anywhere keeps running.  Each frame loads all 8 fetchers' top,
+    bottom and counter registers from RAM-mixed values, fetchers 5-7 turning
+    into music channels by a RAM bit.  Each visible line reads a RAM-chosen
+    fetcher's display data, masked data, flag and a no-value function, the
+    random number and the music amplitude, mixes them into RAM, and switches
+    the program bank through $1FF8/$1FF9 by a RAM bit.  Every 8th line resets
+    the random number generator, rewrites fetcher 0's counter through a
+    read-modify-write, and makes a page-crossing indexed read whose phantom
+    read lands on a DPC read register ($1008)."""
+    rng = Rng(seed * 0x9E3779B1 + 0xDC)
+    tops = [rng.range(0x20, 0xF0) for _ in range(8)]
+    his = [0x07] * 5 + [0x17] * 3                      # bit 4: music mode for fetchers 5-7
+
+    def bank(b: int) -> bytes:
+        a = Asm(0xF000)
+        a.org(0xF100)
+        _reset_code(a)
+        _frame_head(a, lines)
+        a.ins("LDX", "imm", 7)
+        a.label("setup")
+        a.ins("LDA", "zp", MIX); a.ins("ADC", "absx", "tops"); a.ins("STA", "absx", 0x1040)     # top
+        a.ins("LSR", "acc"); a.ins("STA", "absx", 0x1048)                                       # bottom
+        a.ins("EOR", "zp", 0x83); a.ins("STA", "absx", 0x1050)                                  # counter low
+        a.ins("LDA", "zp", MIX); a.ins("AND", "absx", "his"); a.ins("STA", "absx", 0x1058)      # counter high
+        a.ins("DEX"); a.ins("BPL", "rel", "setup")
+        a.label("line")
+        a.ins("STA", "zp", WSYNC)
+        a.ins("LDA", "zp", MIX); a.ins("ADC", "zp", LINE_CTR); a.ins("AND", "imm", 7); a.ins("TAX")
+        for base, op, acc in ((0x1008, "EOR", MIX), (0x1010, "ADC", 0x84), (0x1038, "EOR", 0x85),
+                              (0x1018, "ADC", 0x86)):
+            a.ins("LDA", "absx", base); a.ins(op, "zp", acc); a.ins("STA", "zp", acc)
+        for addr, acc in ((0x1000, 0x87), (0x1004, 0x88), (0x1007, 0x88), (0x1002, 0x89)):
+            a.ins("LDA", "abs", addr); a.ins("ADC", "zp", acc); a.ins("STA", "zp", acc)
+        a.ins("LDA", "zp", MIX); a.ins("LSR", "acc"); a.ins("AND", "imm", 1); a.ins("TAX")
+        a.ins("LDA", "absx", 0xFFF8)                                                            # bank 0 / 1
+        a.ins("LDA", "abs", DPC_BANKID); a.ins("ADC", "zp", 0x8A); a.ins("STA", "zp", 0x8A)
+        a.ins("LDA", "zp", LINE_CTR); a.ins("AND", "imm", 7); a.ins("BNE", "rel", "skip")
+        a.ins("STA", "abs", 0x1070)                                                             # random reset
+        a.ins("INC", "abs", 0x1050)                                                             # counter 0 low, twice
+        a.ins("LDX", "imm", 0x10); a.ins("LDA", "absx", 0x10F8)                                 # phantom at $1008
+        a.ins("ADC", "zp", 0x8B); a.ins("STA", "zp", 0x8B)
+        a.label("skip")
+        _frame_tail(a)
+        a.label("tops")
+        a.raw(bytes(tops))
+        a.label("his")
+        a.raw(bytes(his))
+        a.org(DPC_BANKID)
+        a.raw(bytes([0xB0 + b]))
+        a.org(0xFFF8)
+        a.raw(bytes([rng.below(256), rng.below(256)]))                                         # hotspot rows: data
+        a.org(0xFFFC)
+        a.raw(bytes([0x00, 0xF1, 0x00, 0xF1]))
+        img, labels, end = a.assemble(4096)
+        assert labels["reset"] == 0xF100 and labels["his"] + 8 <= DPC_BANKID
+        img = bytearray(img)
+        for i in list(range(0x000, 0x100)) + list(range(labels["his"] + 8 - 0xF000, DPC_BANKID - 0xF000)):
+            img[i] = rng.below(256)                                                             # ROM data
+        return bytes(img), labels
+
+    (b0, labels), (b1, _) = bank(0), bank(1)
+    display = bytes(rng.below(256) for _ in range(2048))
+    rom = b0 + b1 + display + (bytes(rng.below(256) for _ in range(255)) if dump_tail else b"")
+    assert len(rom) == (10495 if dump_tail else 10240)
+    name = "dpc_10k_tail" if dump_tail else "dpc_10k"
+    return Cart(CartSpec(name, len(rom), seed, wsync_density=1.0), rom, labels, scheme=None)
+
+
+def dpc_display_byte(i: int) -> int:
+    """Display data of dpc_script_cart: byte i of the 2K block."""
+    return (i * 37 + 11) & 0xFF
+
+
+def dpc_script() -> List[tuple]:
+    """The DPC accesses dpc_script_cart makes, in order: ("w", addr, value),
+    ("r", addr) (its value goes to the next RAM byte from $80 on) and
+    ("nop", count).  It walks fetcher 0's counter through top and bottom,
+    fetcher 3's across the 11-bit wrap, the random number generator before
+    and after a reset, the no-value functions, and two music channels
+    sampled after gaps of 1 to 300 CPU cycles, one switched off again."""
+    s: List[tuple] = []
+    s += [("w", 0x1040, 0x30), ("w", 0x1048, 0x2A), ("w", 0x1050, 0x32), ("w", 0x1058, 0x00)]
+    s += [("r", 0x1000 + f * 8) for f in (1, 7, 2, 1, 7, 2, 1, 7, 1, 2, 7, 1, 2, 7, 1, 1)]
+    s += [("w", 0x1053, 0x01), ("w", 0x105B, 0x00)]
+    s += [("r", 0x100B), ("r", 0x103B), ("r", 0x100B), ("r", 0x1013)]
+    s += [("r", 0x1000), ("r", 0x1001), ("r", 0x1003), ("r", 0x1000), ("w", 0x1070, 0x00), ("r", 0x1002), ("r", 0x1001)]
+    s += [("r", 0x101A), ("r", 0x1022), ("r", 0x102A), ("r", 0x1032), ("r", 0x103A)]
+    s += [("w", 0x1045, 0x04), ("w", 0x104D, 0x01), ("w", 0x1055, 0x03), ("w", 0x105D, 0x10),
+          ("w", 0x1046, 0x02), ("w", 0x104E, 0x00), ("w", 0x1056, 0x00), ("w", 0x105E, 0x10)]
+    for gap in (0, 20, 30, 31, 60, 1, 90, 150, 17, 45):
+        s += [("nop", gap), ("r", 0x1004), ("r", 0x103D), ("r", 0x100E)]
+    s += [("w", 0x105E, 0x00), ("r", 0x100E), ("r", 0x100E), ("r", 0x103E), ("r", 0x1007), ("r", 0x100D)]
+    return s
+
+
+def dpc_script_cart() -> Cart:
+    """A 10,240-byte DPC cart that runs dpc_script() once, straight-line, in
+    its second frame.  The reset frame only raises VSYNC; the second clears
+    it, runs the script (each read stored to $80, $81, ...), raises VSYNC
+    again; later frames only toggle VSYNC.  Both banks are the same image."""
+    a = Asm(0xF000)
+    a.org(0xF100)
+    a.label("reset")
+    a.ins("SEI"); a.ins("CLD"); a.ins("LDX", "imm", 0xFF); a.ins("TXS")
+    a.ins("LDA", "imm", 0x02); a.ins("STA", "zp", VSYNC)
+    a.ins("LDA", "imm", 0x00); a.ins("STA", "zp", VSYNC)
+    slot = 0x80
+    for step in dpc_script():
+        if step[0] == "w":
+            a.ins("LDA", "imm", step[2]); a.ins("STA", "abs", step[1])
+        elif step[0] == "r":
+            a.ins("LDA", "abs", step[1]); a.ins("STA", "zp", slot)
+            slot += 1
+        else:
+            for _ in range(step[1]):
+                a.ins("NOP")
+    assert slot <= 0x100
+    a.label("again")
+    a.ins("LDA", "imm", 0x02); a.ins("STA", "zp", VSYNC)
+    a.ins("LDA", "imm", 0x00); a.ins("STA", "zp", VSYNC)
+    a.ins("JMP", "abs", "again")
+    a.org(0xFFFC)
+    a.raw(bytes([0x00, 0xF1, 0x00, 0xF1]))
+    img, labels, _ = a.assemble(4096)
+    rom = img + img + bytes(dpc_display_byte(i) for i in range(2048))
+    assert len(rom) == 10240
+    return Cart(CartSpec("dpc_script", len(rom), 0, wsync_density=0.0), rom, labels, scheme=None)
+
+
 # ------------------------------------------------------- phantom-access carts
 # The reference CPU makes a bus access on every cycle (src/cpu.rs:245-1146),
 # including reads whose value it throws away: the fix-up read of an indexed

@@ -119,6 +119,16 @@ void fa_pack_column(const fa_state& s, uint32_t* col, size_t stride)
     col[R_TIA2 * stride] = b4(!!s.inpt4, !!s.inpt5, s.paddle0, s.paddle1);
     col[R_FRAME * stride] = s.frame_no;
     col[R_STATUS * stride] = s.run_status;
+    for (uint32_t r = 0; r < 4; r++)
+        col[(R_DPC_CNT + r) * stride] = (uint32_t)(s.dpc_counter[2 * r] & 0x7FFu) |
+                                        ((uint32_t)(s.dpc_counter[2 * r + 1] & 0x7FFu) << 16);
+    for (uint32_t r = 0; r < 2; r++) {
+        col[(R_DPC_TOP + r) * stride] = b4(s.dpc_top[4 * r], s.dpc_top[4 * r + 1], s.dpc_top[4 * r + 2], s.dpc_top[4 * r + 3]);
+        col[(R_DPC_BOT + r) * stride] =
+            b4(s.dpc_bottom[4 * r], s.dpc_bottom[4 * r + 1], s.dpc_bottom[4 * r + 2], s.dpc_bottom[4 * r + 3]);
+    }
+    col[R_DPC_MISC * stride] = (uint32_t)s.dpc_flags | ((uint32_t)(s.dpc_music & 7u) << 8) | ((uint32_t)s.dpc_random << 16);
+    col[R_DPC_OSC * stride] = s.dpc_osc;
 }
 
 void fa_unpack_column(const uint32_t* col, size_t stride, int scheme, fa_state& s)
@@ -162,6 +172,19 @@ void fa_unpack_column(const uint32_t* col, size_t stride, int scheme, fa_state& 
     s.frame_no = col[R_FRAME * stride];
     s.run_status = col[R_STATUS * stride];
     s.scheme = (uint8_t)scheme;
+    for (uint32_t r = 0; r < 4; r++) {
+        w = col[(R_DPC_CNT + r) * stride];
+        s.dpc_counter[2 * r] = (uint16_t)(w & 0xFFFFu);
+        s.dpc_counter[2 * r + 1] = (uint16_t)(w >> 16);
+    }
+    for (uint32_t r = 0; r < 2; r++)
+        for (uint32_t b = 0; b < 4; b++) {
+            s.dpc_top[4 * r + b] = (uint8_t)(col[(R_DPC_TOP + r) * stride] >> (8 * b));
+            s.dpc_bottom[4 * r + b] = (uint8_t)(col[(R_DPC_BOT + r) * stride] >> (8 * b));
+        }
+    w = col[R_DPC_MISC * stride];
+    s.dpc_flags = (uint8_t)w; s.dpc_music = (uint8_t)(w >> 8); s.dpc_random = (uint8_t)(w >> 16);
+    s.dpc_osc = col[R_DPC_OSC * stride];
 }
 
 void fa_power_on_column(const uint8_t* img, uint32_t nbanks, int scheme, uint32_t hot_lo, uint32_t* col)
@@ -172,9 +195,12 @@ void fa_power_on_column(const uint8_t* img, uint32_t nbanks, int scheme, uint32_
     memset(&s, 0, sizeof(s));
     if (fa_map_kind(hot_lo)) {
         // Sliced carts: E0 windows 4, 5, 6, 7 (the image's last 4K, as the
-        // reference powers on in its last bank); 3F bank 0.  The vector is in
-        // window 3 ($1C00-$1FFF), whose slice is byte 3.
-        const uint32_t m = fa_map_kind(hot_lo) == FA_MAP_E0 ? (4u | 5u << 4 | 6u << 8) : 0u;
+        // reference powers on in its last bank); 3F bank 0; DPC program bank
+        // 1 (the last), with its random number generator at 1.  The vector is
+        // in window 3 ($1C00-$1FFF), whose slice is byte 3.
+        const uint32_t kind = fa_map_kind(hot_lo);
+        const uint32_t m = kind == FA_MAP_E0 ? (4u | 5u << 4 | 6u << 8) : kind == FA_MAP_DPC ? 1u : 0u;
+        if (kind == FA_MAP_DPC) s.dpc_random = 1;
         const uint32_t vec = (fa_slices_from_mapper(hot_lo, m) >> 24) * 1024u + 0x3FCu;
         s.mapper[0] = (uint8_t)m;
         s.mapper[1] = (uint8_t)(m >> 8);
@@ -195,6 +221,8 @@ void fa_power_on_column(const uint8_t* img, uint32_t nbanks, int scheme, uint32_
 }
 
 // ------------------------------------------------------------------ ROM schemes
+static int dpc_len(size_t len) { return len == 10240 || len == 10495; }
+
 static int rom_len_ok(size_t len)          // lengths HeadlessBus::new accepts (src/atari.rs:410-449)
 {
     if (len == 0) return 0;
@@ -206,10 +234,20 @@ static int rom_len_ok(size_t len)          // lengths HeadlessBus::new accepts (
     }
 }
 
+// The scheme for a ROM length with nothing registered: DPC for its two dump
+// lengths (which the reference's size rule cannot construct), else the
+// reference's size rule; -1 for a length neither can build.
+static int auto_scheme(size_t len)
+{
+    if (dpc_len(len)) return FA_SCHEME_DPC;
+    return rom_len_ok(len) ? fa_detect_scheme(len) : -1;
+}
+
 static int scheme_len_ok(int scheme, size_t len)
 {
     switch (scheme) {
     case FA_SCHEME_E0: return len == 8192;
+    case FA_SCHEME_DPC: return dpc_len(len);
     case FA_SCHEME_3F: return len >= 2048 && len <= 32768 && len % 2048 == 0;
     case FA_SCHEME_FIXED: case FA_SCHEME_F8: case FA_SCHEME_F6: case FA_SCHEME_F4:
         return rom_len_ok(len) && fa_detect_scheme(len) == scheme;
@@ -256,9 +294,9 @@ extern "C" int fa_rom_scheme(const uint8_t* rom, size_t rom_len)
     if (!rom || rom_len == 0) return fa_fail(FA_ERR_BAD_ROM, "empty ROM");
     const int reg = registered_scheme(rom, rom_len);
     if (reg != FA_SCHEME_AUTO) return reg;
-    if (!rom_len_ok(rom_len))
-        return fa_fail(FA_ERR_BAD_ROM, "ROM length %zu cannot be constructed (reference panics)", rom_len);
-    return fa_detect_scheme(rom_len);
+    const int s = auto_scheme(rom_len);
+    if (s < 0) return fa_fail(FA_ERR_BAD_ROM, "ROM length %zu cannot be constructed (reference panics)", rom_len);
+    return s;
 }
 
 extern "C" int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len)
@@ -270,7 +308,8 @@ extern "C" int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len)
     // accesses to the hotspots of the scheme the size rule gives.
     static const uint8_t abs_ops[] = { 0xAD, 0xAE, 0xAC, 0x8D, 0x8E, 0x8C, 0x2C, 0xCD,
                                        0xBD, 0xB9, 0xBE, 0xBC, 0x9D, 0x99 };
-    const int by_size = rom_len_ok(rom_len) ? fa_detect_scheme(rom_len) : -1;
+    const int by_size = auto_scheme(rom_len);
+    if (by_size == FA_SCHEME_DPC) return by_size;
     const uint32_t hlo = by_size > 0 ? fa_hot_lo(by_size) : 0x2000u, hn = by_size > 0 ? fa_nbanks(by_size) : 0u;
     size_t e0 = 0, own = 0, st3f = 0;
     for (size_t i = 0; i + 2 < rom_len; i++) {
@@ -298,20 +337,27 @@ extern "C" int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len)
 // The shared-memory image of a ROM, in 4 KiB units: Fixed carts mirror into
 // one 4K window (HeadlessBus::load_bank, src/atari.rs:433-449); 4K-bank carts
 // use their first nbanks * 4 KiB; sliced carts (E0, 3F) the whole ROM,
-// zero-padded to a 4K multiple.  The scheme is the registered one for these
-// bytes, else the reference's size rule.
+// zero-padded to a 4K multiple; DPC carts their 10K, padded to 12K.  The
+// scheme is the registered one for these bytes, else DPC for its lengths,
+// else the reference's size rule.
 int fa_make_bank_image(const uint8_t* rom, size_t len, std::vector<uint8_t>& img, int& scheme, uint32_t* nbanks,
                        uint32_t* hot_lo)
 {
     if (!rom || len == 0) return fa_fail(FA_ERR_BAD_ROM, "empty ROM");
     scheme = registered_scheme(rom, len);
     if (scheme == FA_SCHEME_AUTO) {
-        if (!rom_len_ok(len))
-            return fa_fail(FA_ERR_BAD_ROM, "ROM length %zu cannot be constructed (reference panics)", len);
-        scheme = fa_detect_scheme(len);
+        scheme = auto_scheme(len);
+        if (scheme < 0) return fa_fail(FA_ERR_BAD_ROM, "ROM length %zu cannot be constructed (reference panics)", len);
     }
     uint32_t nb, hl;
-    if (scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_3F) {
+    if (scheme == FA_SCHEME_DPC) {
+        // 8K of program, then the 2K of display data; the 255 bytes some
+        // dumps carry after them are not used.
+        nb = 3;
+        hl = FA_MAP_DPC << 8;
+        img.assign((size_t)nb * 4096, 0);
+        memcpy(img.data(), rom, 10240);
+    } else if (scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_3F) {
         nb = (uint32_t)((len + 4095) / 4096);
         hl = scheme == FA_SCHEME_E0 ? (FA_MAP_E0 << 8) : ((FA_MAP_3F << 8) | (uint32_t)(len / 2048));
         img.assign((size_t)nb * 4096, 0);
@@ -697,6 +743,9 @@ extern "C" int fa_set_states(fa_handle* h, const fa_state* in)
             h->hot_lo, fa_slices_from_mapper(h->hot_lo, (uint32_t)s.mapper[0] | ((uint32_t)s.mapper[1] << 8)));
         s.mapper[0] = (uint8_t)m;
         s.mapper[1] = (uint8_t)(m >> 8);
+        // The DPC registers end the struct; other schemes do not take them.
+        if (fa_map_kind(h->hot_lo) != FA_MAP_DPC)
+            memset(&s.dpc_counter, 0, sizeof(fa_state) - offsetof(fa_state, dpc_counter));
         fa_pack_column(s, buf.data() + i, h->stride);
     }
     FA_CUDA(cudaStreamSynchronize(h->stream));

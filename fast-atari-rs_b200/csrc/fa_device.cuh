@@ -669,6 +669,90 @@ static __device__ __noinline__ RRead render_io_read(uint32_t a, uint32_t owed, R
     return out;
 }
 
+// ---------------------------------------------------------------- DPC (Pitfall II)
+// The DPC chip of FA_SCHEME_DPC carts (no counterpart in the reference),
+// with the semantics the oracle's DPC section fixes: 8 data fetchers (11-bit
+// counter, top, bottom, flag), an 8-bit random number generator and 3 music
+// channels clocked at 20 kHz of Cpu::cycles.  The registers stay in their
+// HBM rows (R_DPC_*) and are changed there in place, one access at a time:
+// a read of $1000-$103F (wr 0; returns the value) or a write of v to
+// $1040-$107F (wr 1).  cyc_acc: the instruction cycles not yet added to the
+// rows' Cpu::cycles (none of the accessing instruction's).  `disp` is the
+// 2K of display data.  One out-of-line copy for every access site.
+static __device__ __forceinline__ uint32_t dpc_byte(uint32_t w, uint32_t k) { return (w >> ((k & 3u) * 8u)) & 0xFFu; }
+
+static __device__ __noinline__ uint32_t dpc_io(uint32_t a, uint32_t v, uint32_t wr, uint32_t* col, uint32_t S,
+                                               const uint8_t* disp, uint32_t cyc_acc)
+{
+    const uint32_t misc = col[(size_t)R_DPC_MISC * S];
+    uint32_t flags = misc & 0xFFu, music = (misc >> 8) & 7u, rnd = (misc >> 16) & 0xFFu;
+    // The music channels up to the instruction's start: one clock of the
+    // oscillator counts a channel's low byte down, the clock after 0 reloads
+    // top; the flag is set while the low byte is above bottom.
+    const unsigned long long t =
+        (((unsigned long long)col[(size_t)R_CYC_HI * S] << 32) | col[(size_t)R_CYC_LO * S]) + cyc_acc;
+    const uint32_t now = (uint32_t)((t / 3579545ull) * 60000ull + ((t % 3579545ull) * 60000ull) / 3579545ull);
+    const uint32_t clocks = now - col[(size_t)R_DPC_OSC * S];
+    col[(size_t)R_DPC_OSC * S] = now;
+    if (clocks && music) {
+#pragma unroll 1
+        for (uint32_t f = 5u; f < 8u; f++) {
+            if (!((music >> (f - 5u)) & 1u)) continue;
+            uint32_t& cw = col[(size_t)(R_DPC_CNT + (f >> 1)) * S];
+            const uint32_t sh = (f & 1u) * 16u, cnt = (cw >> sh) & 0x7FFu;
+            const uint32_t top = dpc_byte(col[(size_t)(R_DPC_TOP + (f >> 2)) * S], f);
+            const uint32_t bot = dpc_byte(col[(size_t)(R_DPC_BOT + (f >> 2)) * S], f);
+            uint32_t low = cnt & 0xFFu;
+            low = clocks <= low ? low - clocks : top - (clocks - low - 1u) % (top + 1u);
+            cw = (cw & ~(0xFFFFu << sh)) | (((cnt & 0x700u) | low) << sh);
+            flags = low > bot ? flags | (1u << f) : flags & ~(1u << f);
+        }
+    }
+    const uint32_t k = a & 7u, f = (a >> 3) & 7u, sh = (k & 1u) * 16u;
+    uint32_t& cw = col[(size_t)(R_DPC_CNT + (k >> 1)) * S];
+    uint32_t& tw = col[(size_t)(R_DPC_TOP + (k >> 2)) * S];
+    uint32_t& bw = col[(size_t)(R_DPC_BOT + (k >> 2)) * S];
+    uint32_t cnt = (cw >> sh) & 0x7FFu, out = 0u;
+    if (!wr) {
+        const bool mus = k >= 5u && ((music >> (k - 5u)) & 1u);
+        // The generator shifts left, taking in the XNOR of bits 7, 5, 4, 3.
+        rnd = ((rnd << 1) | (~((rnd >> 7) ^ (rnd >> 5) ^ (rnd >> 4) ^ (rnd >> 3)) & 1u)) & 0xFFu;
+        if (!mus) {
+            const uint32_t low = cnt & 0xFFu;
+            if (low == dpc_byte(tw, k)) flags |= 1u << k;
+            else if (low == dpc_byte(bw, k)) flags &= ~(1u << k);
+        }
+        const uint32_t flag = ((flags >> k) & 1u) ? 0xFFu : 0u, data = disp[2047u - cnt];
+        switch (f) {
+        case 0:
+            if (k < 4u) out = rnd;
+            else
+                for (uint32_t m = 0; m < 3u; m++) out += (((music & (flags >> 5)) >> m) & 1u) ? 4u + m : 0u;
+            break;
+        case 1: out = data; break;
+        case 2: out = data & flag; break;
+        case 7: out = flag; break;
+        default: break;
+        }
+        if (!mus) cw = (cw & ~(0xFFFFu << sh)) | (((cnt - 1u) & 0x7FFu) << sh);
+    } else {
+        const uint32_t bs = (k & 3u) * 8u;
+        switch (f) {
+        case 0: tw = (tw & ~(0xFFu << bs)) | (v << bs); flags &= ~(1u << k); break;
+        case 1: bw = (bw & ~(0xFFu << bs)) | (v << bs); break;
+        case 2: cw = (cw & ~(0xFFFFu << sh)) | (((cnt & 0x700u) | v) << sh); break;
+        case 3:
+            cw = (cw & ~(0xFFFFu << sh)) | ((((v & 7u) << 8) | (cnt & 0xFFu)) << sh);
+            if (k >= 5u) music = (music & ~(1u << (k - 5u))) | (((v >> 4) & 1u) << (k - 5u));
+            break;
+        case 6: rnd = 1u; break;
+        default: break;
+        }
+    }
+    col[(size_t)R_DPC_MISC * S] = flags | (music << 8) | (rnd << 16);
+    return out;
+}
+
 // ---------------------------------------------------------------- PIA timer (pia.rs:107-166)
 // Pia::tick_n on the unpacked timer: value, prescaler, interval, underflow.
 static __device__ __forceinline__ void pia_tick_n(uint32_t& tv, uint32_t& ps, uint32_t sel, uint32_t& uf, uint32_t n)
@@ -769,8 +853,12 @@ static __device__ __noinline__ uint4 pia_sync_io(uint32_t tv_ps, uint32_t sel_uf
     return make_uint4(tv | (ps << 16), sel | (uf << 16), pia_span_of(tv, ps, sel, uf), 0u);
 }
 
-template <int BLOCK, bool RENDER = false, bool SLICED = false>
+// SLICED: the core of E0 and 3F carts (and, with DPC, of DPC carts alone).
+// The DPC core is its own build so that the E0 / 3F core carries none of the
+// DPC register decode on its bus paths.
+template <int BLOCK, bool RENDER = false, bool SLICED = false, bool DPC = false>
 struct Emu {
+    static_assert(!DPC || (SLICED && !RENDER), "the DPC core is a headless sliced core");
     // ---- placement
     uint8_t* pv;             // this thread's RAM (shared memory, interleaved by thread)
     const FaGroup* G;        // the instance's group (HBM state rows, stride)
@@ -842,14 +930,27 @@ struct Emu {
     }
     __device__ __forceinline__ void sbump() { bank = bank < (511u << 3) ? bank + 8u : bank; }
     // E0: any access to $1FE0-$1FF7 maps slice (a & 7) into window (a - $1FE0) >> 3.
+    // DPC core: any access to $1FF8 / $1FF9 maps program bank 0 / 1 (slices 4b..4b+3).
     __device__ __forceinline__ void e0_hot(uint32_t a13)
     {
-        const uint32_t d = a13 - 0x1FE0u;
-        if (d < 24u && fa_map_kind(hot_lo) == FA_MAP_E0) {
-            const uint32_t sh = (d >> 3) * 8u;
-            slices = (slices & ~(0xFFu << sh)) | ((a13 & 7u) << sh);
-            sbump();
+        if constexpr (DPC) {
+            if ((a13 | 1u) == 0x1FF9u) {
+                slices = (a13 & 1u) * 0x04040404u + 0x03020100u;
+                sbump();
+            }
+        } else {
+            const uint32_t d = a13 - 0x1FE0u;
+            if (d < 24u && fa_map_kind(hot_lo) == FA_MAP_E0) {
+                const uint32_t sh = (d >> 3) * 8u;
+                slices = (slices & ~(0xFFu << sh)) | ((a13 & 7u) << sh);
+                sbump();
+            }
         }
+    }
+    // DPC core: reads of $1000-$103F and writes of $1040-$107F reach the registers.
+    __device__ __forceinline__ uint32_t dpc(uint32_t a13, uint32_t v, uint32_t wr)
+    {
+        return dpc_io(a13, v, wr, column(), G->stride, rom + 8192u, cyc_acc);
     }
     // 3F: a write of v to $0000-$003F maps 2K bank v mod n at $1000-$17FF.
     __device__ __forceinline__ void f3_write(uint32_t a13, uint32_t v)
@@ -1004,6 +1105,9 @@ struct Emu {
         uint32_t a = addr & 0x1FFFu;
         if (a & 0x1000u) {
             if constexpr (SLICED) {
+                if constexpr (DPC) {
+                    if (a < 0x1040u) return dpc(a, 0u, 0u);
+                }
                 e0_hot(a);
                 return rom[srom(a)];
             } else {
@@ -1017,7 +1121,14 @@ struct Emu {
     {
         uint32_t a = addr & 0x1FFFu;
         if (a & 0x1000u) {
-            if constexpr (SLICED) e0_hot(a); else bsw(a);
+            if constexpr (SLICED) {
+                if constexpr (DPC) {
+                    if (a - 0x1040u < 0x40u) (void)dpc(a, v, 1u);
+                }
+                e0_hot(a);
+            } else {
+                bsw(a);
+            }
             return;
         }
         if ((a & 0x280u) == 0x080u) { stp(a & 0x7Fu, v); return; }
@@ -1028,7 +1139,14 @@ struct Emu {
     {
         uint32_t a = addr & 0x1FFFu;
         if (a & 0x1000u) {
-            if constexpr (SLICED) e0_hot(a); else bsw(a);
+            if constexpr (SLICED) {
+                if constexpr (DPC) {
+                    if (a < 0x1040u) (void)dpc(a, 0u, 0u);
+                }
+                e0_hot(a);
+            } else {
+                bsw(a);
+            }
         } else if ((a & 0x287u) == 0x284u) {
             if constexpr (RENDER) (void)io(a, j);
             else pia_intim();
@@ -1372,10 +1490,11 @@ struct Emu {
         const uint32_t a0 = pc0 & 0x1FFFu;
         uint32_t op, b1, b2 = 0;
         // Fast path: the three bytes at pc0 lie in the current bank (SLICED:
-        // in one window) and clear of every hotspot, so reading them has no
-        // side effect.
-        if (SLICED ? (a0 >= 0x1000u && (a0 & 0x3FFu) <= 0x3FDu && (a0 + 2u < 0x1FE0u || a0 > 0x1FF7u))
-                   : (a0 >= 0x1000u && a0 + 2u < hot_lo)) {
+        // in one window) and clear of every hotspot (and, DPC, of its read
+        // registers at $1000-$103F), so reading them has no side effect.
+        if (DPC      ? (a0 >= 0x1040u && (a0 & 0x3FFu) <= 0x3FDu && (a0 + 2u < 0x1FF8u || a0 > 0x1FF9u))
+            : SLICED ? (a0 >= 0x1000u && (a0 & 0x3FFu) <= 0x3FDu && (a0 + 2u < 0x1FE0u || a0 > 0x1FF7u))
+                     : (a0 >= 0x1000u && a0 + 2u < hot_lo)) {
             const uint8_t* q = SLICED ? rom + srom(a0) : rom + ((bank & 7u) << 12) + (a0 & 0xFFFu);
             op = q[0];
             if (!((c_legal[op >> 5] >> (op & 31u)) & 1u)) { pc = (pc0 + 1u) & 0xFFFFu; return 0; }

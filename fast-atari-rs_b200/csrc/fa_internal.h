@@ -40,9 +40,13 @@ struct FaGroup {
 // The kernel build a set of groups needs (FA_MAPS_*).
 static inline int fa_maps_of(const FaGroup* g, uint32_t ngroups)
 {
-    bool sl = false, std4k = false;
-    for (uint32_t i = 0; i < ngroups; i++) (fa_map_kind(g[i].hot_lo) ? sl : std4k) = true;
-    return sl ? (std4k ? FA_MAPS_BOTH : FA_MAPS_SLICED) : FA_MAPS_4K;
+    bool sl = false, dpc = false, std4k = false;
+    for (uint32_t i = 0; i < ngroups; i++) {
+        const uint32_t kind = fa_map_kind(g[i].hot_lo);
+        (kind == FA_MAP_DPC ? dpc : kind ? sl : std4k) = true;
+    }
+    if ((int)sl + (int)dpc + (int)std4k > 1) return FA_MAPS_BOTH;
+    return dpc ? FA_MAPS_DPC : sl ? FA_MAPS_SLICED : FA_MAPS_4K;
 }
 
 struct FaLaunch {

@@ -191,6 +191,7 @@ static cudaError_t launch_block_m(int maps, const FaLaunch& L, bool persistent, 
 {
     return maps == FA_MAPS_4K   ? launch_block<BLOCK, FA_MAPS_4K>(L, persistent, sms, s)
          : maps == FA_MAPS_BOTH ? launch_block<BLOCK, FA_MAPS_BOTH>(L, persistent, sms, s)
+         : maps == FA_MAPS_DPC  ? launch_block<BLOCK, FA_MAPS_DPC>(L, persistent, sms, s)
                                 : launch_block<BLOCK, FA_MAPS_SLICED>(L, persistent, sms, s);
 }
 
@@ -312,7 +313,8 @@ static bool warp_layout(FaLaunch& L, int block, bool persistent, int* warps)
         // 65536 / (32 x warps)).  A launch of sliced carts alone defaults to
         // 24: at 32 warps its core is held to 64 registers and spills in the
         // interpreter loop (three E0/3F carts: 2.31 against 2.13 M frames/s).
-        const int cap = L.cta_warps ? (int)L.cta_warps : fa_maps_of(L.g, L.ngroups) == FA_MAPS_SLICED ? 24 : 32;
+        const int m = fa_maps_of(L.g, L.ngroups);
+        const int cap = L.cta_warps ? (int)L.cta_warps : (m == FA_MAPS_SLICED || m == FA_MAPS_DPC) ? 24 : 32;
         static const int sizes[] = { 32, 28, 24, 16, 8, 4, 2 };
         for (int x : sizes)
             if (x <= fit && x <= cap) { w = x; break; }
@@ -331,6 +333,7 @@ cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int 
     if (warp_layout(L, block, persistent, &warps)) {
         return maps == FA_MAPS_4K   ? launch_warps_n<FA_MAPS_4K>(warps, L, persistent, sms, s)
              : maps == FA_MAPS_BOTH ? launch_warps_n<FA_MAPS_BOTH>(warps, L, persistent, sms, s)
+             : maps == FA_MAPS_DPC  ? launch_warps_n<FA_MAPS_DPC>(warps, L, persistent, sms, s)
                                     : launch_warps_n<FA_MAPS_SLICED>(warps, L, persistent, sms, s);
     }
     // ROM library too large for shared memory: CTA-granular units that
@@ -357,6 +360,7 @@ bool fa_launch_warp_shape(const FaLaunch& L_in, int block, bool persistent, int 
     case WW:                                                                                                \
         if (maps == FA_MAPS_4K) warps_shape<WW, FA_MAPS_4K>(L, persistent, sms, grid, per_sm);              \
         else if (maps == FA_MAPS_BOTH) warps_shape<WW, FA_MAPS_BOTH>(L, persistent, sms, grid, per_sm);     \
+        else if (maps == FA_MAPS_DPC) warps_shape<WW, FA_MAPS_DPC>(L, persistent, sms, grid, per_sm);       \
         else warps_shape<WW, FA_MAPS_SLICED>(L, persistent, sms, grid, per_sm);                            \
         return true;
     switch (w) {

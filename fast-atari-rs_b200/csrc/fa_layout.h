@@ -50,7 +50,14 @@ enum : uint32_t {
     R_TIA2   = FA_PRIV_WORDS + 10,  // inpt4 | inpt5<<8 | paddle0<<16 | paddle1<<24
     R_FRAME  = FA_PRIV_WORDS + 11,  // frame_no
     R_STATUS = FA_PRIV_WORDS + 12,  // run_status
-    FA_ROWS  = FA_PRIV_WORDS + 13,
+    // DPC registers (FA_SCHEME_DPC carts only; the device touches them only
+    // on a DPC register access, in place in HBM).
+    R_DPC_CNT = FA_PRIV_WORDS + 13, // 4 rows: counter 2r | counter 2r+1 << 16
+    R_DPC_TOP = FA_PRIV_WORDS + 17, // 2 rows: top 4r..4r+3, one per byte
+    R_DPC_BOT = FA_PRIV_WORDS + 19, // 2 rows: bottom 4r..4r+3
+    R_DPC_MISC = FA_PRIV_WORDS + 21,// flags | music << 8 | random << 16
+    R_DPC_OSC = FA_PRIV_WORDS + 22, // oscillator clock count at the last update
+    FA_ROWS  = FA_PRIV_WORDS + 23,
 };
 
 // Bank-switch decode: a read or write of (addr & 0x1FFF) - hot_lo < nbanks
@@ -77,19 +84,21 @@ static inline int fa_detect_scheme(size_t len)        // BankScheme::detect, src
 #define FA_HD
 #endif
 
-// Sliced carts (E0, 3F) map 1K slices of the ROM image into the four 1K
+// Sliced carts (E0, 3F, DPC) map 1K slices of the ROM image into the four 1K
 // windows of $1000-$1FFF; `slices` holds the slice of window k in byte k.
 // Their hot_lo is FA_MAP_* << 8 (3F: | the number of 2K banks), below 0x1000,
 // so no ROM address passes the 4K-bank hotspot decode or the 4K-bank fetch
 // path.  The bank state a caller sees is 16 bits (fa_state::mapper): E0 =
-// window 0 | window 1 << 4 | window 2 << 8; 3F = the 2K bank at $1000.
-enum : uint32_t { FA_MAP_E0 = 1u, FA_MAP_3F = 2u };
+// window 0 | window 1 << 4 | window 2 << 8; 3F = the 2K bank at $1000; DPC =
+// the 4K program bank (slices 4b..4b+3).  A DPC image holds the 8K of
+// program, then the 2K of display data at byte 8192.
+enum : uint32_t { FA_MAP_E0 = 1u, FA_MAP_3F = 2u, FA_MAP_DPC = 3u };
 
 FA_HD static inline uint32_t fa_map_kind(uint32_t hot_lo) { return hot_lo < 0x1000u ? hot_lo >> 8 : 0u; }
 
 // Kernel builds by the cores they hold (see run_unit): 4K-bank carts only,
-// both kinds, sliced carts only.
-enum : int { FA_MAPS_4K = 0, FA_MAPS_BOTH = 1, FA_MAPS_SLICED = 2 };
+// several kinds, E0 / 3F carts only, DPC carts only.
+enum : int { FA_MAPS_4K = 0, FA_MAPS_BOTH = 1, FA_MAPS_SLICED = 2, FA_MAPS_DPC = 3 };
 
 FA_HD static inline uint32_t fa_slices_from_mapper(uint32_t hot_lo, uint32_t m)
 {
@@ -99,6 +108,7 @@ FA_HD static inline uint32_t fa_slices_from_mapper(uint32_t hot_lo, uint32_t m)
         const uint32_t n = hot_lo & 0xFFu, b = (m & 0xFFu) % n, l = n - 1u;
         return (2u * b) | ((2u * b + 1u) << 8) | ((2u * l) << 16) | ((2u * l + 1u) << 24);
     }
+    if (fa_map_kind(hot_lo) == FA_MAP_DPC) return (m & 1u) * 0x04040404u + 0x03020100u;
     return 0u;
 }
 
@@ -107,6 +117,7 @@ FA_HD static inline uint32_t fa_mapper_from_slices(uint32_t hot_lo, uint32_t sli
     if (fa_map_kind(hot_lo) == FA_MAP_E0)
         return (slices & 7u) | (((slices >> 8) & 7u) << 4) | (((slices >> 16) & 7u) << 8);
     if (fa_map_kind(hot_lo) == FA_MAP_3F) return (slices & 0xFFu) >> 1;
+    if (fa_map_kind(hot_lo) == FA_MAP_DPC) return (slices & 0xFFu) >> 2;
     return 0u;
 }
 

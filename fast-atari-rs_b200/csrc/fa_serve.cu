@@ -7,7 +7,7 @@
 // a frame count k and k*n actions) and wait for their observations.
 //
 // Memory.  Instance state lives in blocks of FA_SERVE_BLOCK_COLS SoA columns
-// (one block = FA_ROWS rows x 256 words = 58,368 bytes), carved from device
+// (one block = FA_ROWS rows x 256 words = 68,608 bytes), carved from device
 // slabs.  A session owns a list of blocks, so it grows by appending blocks,
 // never by moving state.  New instances are admitted — their blocks allocated
 // and set to the cart's post-reset snapshot — when a request names more

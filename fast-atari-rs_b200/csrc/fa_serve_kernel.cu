@@ -131,11 +131,17 @@ cudaError_t launch_serve(const FaServeLaunch& L, cudaStream_t s)
 cudaError_t fa_launch_serve(const FaServeLaunch& L, int block, cudaStream_t s)
 {
     if (L.nbanks < 1 || L.nbanks > 8) return cudaErrorInvalidValue;
-    const bool sl = fa_map_kind(L.hot_lo) != 0;                        // one cart per launch: E0 / 3F or not
+    const uint32_t kind = fa_map_kind(L.hot_lo);                       // one cart per launch
     switch (block) {
-    case 128: return sl ? launch_serve<4, FA_MAPS_SLICED>(L, s) : launch_serve<4, FA_MAPS_4K>(L, s);
-    case 256: return sl ? launch_serve<8, FA_MAPS_SLICED>(L, s) : launch_serve<8, FA_MAPS_4K>(L, s);
-    case 512: return sl ? launch_serve<16, FA_MAPS_SLICED>(L, s) : launch_serve<16, FA_MAPS_4K>(L, s);
+    case 128:
+        return kind == FA_MAP_DPC ? launch_serve<4, FA_MAPS_DPC>(L, s)
+             : kind               ? launch_serve<4, FA_MAPS_SLICED>(L, s) : launch_serve<4, FA_MAPS_4K>(L, s);
+    case 256:
+        return kind == FA_MAP_DPC ? launch_serve<8, FA_MAPS_DPC>(L, s)
+             : kind               ? launch_serve<8, FA_MAPS_SLICED>(L, s) : launch_serve<8, FA_MAPS_4K>(L, s);
+    case 512:
+        return kind == FA_MAP_DPC ? launch_serve<16, FA_MAPS_DPC>(L, s)
+             : kind               ? launch_serve<16, FA_MAPS_SLICED>(L, s) : launch_serve<16, FA_MAPS_4K>(L, s);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -54,8 +54,8 @@ extern "C" {
 #define FA_SCHEME_F6    2
 #define FA_SCHEME_F4    3
 /* Schemes the reference does not have (its BankScheme::detect picks by size
- * alone, so these carts run as F8 there and crash or misbehave).  They are
- * never picked by size: register them per ROM with fa_rom_set_scheme. */
+ * alone, so these carts run as F8 there and crash or misbehave).  E0 and 3F
+ * are never picked by size: register them per ROM with fa_rom_set_scheme. */
 #define FA_SCHEME_E0    4   /* Parker Brothers, 8K: four 1K windows; any access to
                                $1FE0-$1FE7 / $1FE8-$1FEF / $1FF0-$1FF7 maps 1K slice
                                (addr & 7) into window 0 / 1 / 2; window 3 holds
@@ -64,6 +64,16 @@ extern "C" {
                                switchable 2K bank, $1800-$1FFF the last 2K; a write
                                of v to $0000-$003F selects bank v mod (len / 2K) and
                                also reaches the TIA.  Power-on bank: 0. */
+#define FA_SCHEME_DPC   6   /* Activision's DPC (Pitfall II): 8K of program in two 4K
+                               banks ($1FF8 / $1FF9 select bank 0 / 1, any access;
+                               power-on bank 1), 2K of display data read through 8
+                               data fetchers, an 8-bit random number generator and 3
+                               music channels.  Reads of $1000-$103F and writes of
+                               $1040-$107F reach the DPC registers (fa_state's dpc_*
+                               fields).  Unlike E0 and 3F, picked by size: 10240
+                               bytes (program + display data) or 10495 (with the 255
+                               bytes that dumps of the cart carry after them, ignored),
+                               lengths the reference cannot construct. */
 #define FA_SCHEME_AUTO  (-1)
 
 #define FA_RAM_BYTES 128
@@ -104,18 +114,30 @@ typedef struct fa_state {
     uint8_t  bank, scheme;
     uint8_t  _pad_end[2];
     /* ---- extension beyond the reference layout ---- */
-    /* E0 and 3F bank state, 16 bits little-endian: E0 = slice of window 0 |
-     * window 1 << 4 | window 2 << 8; 3F = the 2K bank at $1000.  0 for the
-     * reference's schemes, whose bank is `bank`. */
+    /* E0, 3F and DPC bank state, 16 bits little-endian: E0 = slice of window
+     * 0 | window 1 << 4 | window 2 << 8; 3F = the 2K bank at $1000; DPC = the
+     * 4K program bank.  0 for the reference's schemes, whose bank is `bank`. */
     uint8_t  mapper[2];
     uint8_t  _pad_ext;
     uint64_t cycles;      /* Cpu::cycles: executed instruction cycles, never reset */
     uint32_t frame_no;    /* frames run since the last reset (episode counter) */
     uint32_t run_status;  /* FA_STATUS_* bits */
+    /* DPC registers (FA_SCHEME_DPC; 0 for every other scheme, whose
+     * fa_set_states does not take them).  Fetcher k has
+     * an 11-bit counter, top and bottom registers and a flag (bit k of
+     * dpc_flags: the flag reads $FF).  dpc_music bit m: fetcher 5 + m is a
+     * music channel.  dpc_osc: the music oscillator's clock count when the
+     * fetchers were last brought up to date (it counts 20,000 per second of
+     * Cpu::cycles at 3,579,545 / 3 cycles per second). */
+    uint16_t dpc_counter[8];
+    uint8_t  dpc_top[8];
+    uint8_t  dpc_bottom[8];
+    uint8_t  dpc_flags, dpc_music, dpc_random, _pad_dpc;
+    uint32_t dpc_osc;
 } fa_state;
 
 #define FA_STATE_REF_BYTES 221   /* prefix shared with the reference AtariStateGpu */
-#define FA_STATE_BYTES     240
+#define FA_STATE_BYTES     280
 
 #ifdef __cplusplus
 #define FA_STATIC_ASSERT(c, m) static_assert(c, m)
@@ -131,6 +153,8 @@ FA_STATIC_ASSERT(offsetof(fa_state, pos_p0) == 176, "pos offset");
 FA_STATIC_ASSERT(offsetof(fa_state, bank) == 217, "bank offset");
 FA_STATIC_ASSERT(offsetof(fa_state, cycles) == 224, "cycles offset");
 FA_STATIC_ASSERT(offsetof(fa_state, run_status) == 236, "status offset");
+FA_STATIC_ASSERT(offsetof(fa_state, dpc_counter) == 240, "dpc offset");
+FA_STATIC_ASSERT(offsetof(fa_state, dpc_osc) == 276, "dpc oscillator offset");
 
 /* Opaque handle: one ROM, n instances, resident in HBM (`BatchAtariGpu`). */
 typedef struct fa_handle fa_handle;
@@ -167,13 +191,15 @@ uint64_t fa_wait_limit_ns_get(void);
  * entry point that is later given the same bytes (fa_create, fa_pool_add_cart,
  * fa_server_create, fa_render_create, fa_autotune) uses it instead of the
  * size rule.  FA_SCHEME_AUTO removes the record.  The length must suit the
- * scheme: E0 exactly 8192; 3F a multiple of 2048 up to 32768; the reference's
+ * scheme: E0 exactly 8192; 3F a multiple of 2048 up to 32768; DPC 10240 or
+ * 10495; the reference's
  * schemes the lengths fa_create accepts for them.  FA_ERR_BAD_ROM otherwise.
  */
 int fa_rom_set_scheme(const uint8_t* rom, size_t rom_len, int scheme);
 
 /* The scheme the entry points will use for these bytes (a registered one,
- * else the size rule), or FA_ERR_BAD_ROM for a length that cannot be built. */
+ * else DPC for 10240 or 10495 bytes, else the size rule), or FA_ERR_BAD_ROM
+ * for a length that cannot be built. */
 int fa_rom_scheme(const uint8_t* rom, size_t rom_len);
 
 /* A guess from the ROM's code, for a caller deciding what to register; never
@@ -184,8 +210,8 @@ int fa_rom_scheme(const uint8_t* rom, size_t rom_len);
  * accesses, over eight times the size-rule ones, and a reset vector in
  * $1C00-$1FFF is E0; at least three $3F stores, over eight times the size-rule
  * accesses, and a reset vector in $1800-$1FFF make a 2K-multiple image 3F;
- * anything else gets the size rule.  On random bytes it picks E0 or 3F for a
- * few percent of 8K images. */
+ * a DPC length is DPC; anything else gets the size rule.  On random bytes it
+ * picks E0 or 3F for a few percent of 8K images. */
 int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len);
 
 /*
@@ -575,7 +601,8 @@ int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_loadgen_res
 #define FA_FB_WIDTH  160
 #define FA_FB_HEIGHT 192
 typedef struct fa_render fa_render;
-/* n rendering consoles of one ROM on the current device (lengths as fa_create). */
+/* n rendering consoles of one ROM on the current device (lengths as fa_create;
+ * DPC carts, FA_ERR_BAD_ROM: they run on the headless console only). */
 int  fa_render_create(const uint8_t* rom, size_t rom_len, size_t n, fa_render** out);
 void fa_render_destroy(fa_render* r);
 size_t fa_render_num_envs(const fa_render* r);
@@ -618,7 +645,7 @@ uint32_t fa_palette_rgba(uint8_t index);
  * allocates nothing.
  *   d_rom_image  nbanks * 4096 bytes, 16-byte aligned (Fixed carts as their
  *                mirrored 4 KiB window, banked carts as-is)
- *   scheme       FA_SCHEME_FIXED, _F8, _F6 or _F4 (E0 and 3F are not taken here)
+ *   scheme       FA_SCHEME_FIXED, _F8, _F6 or _F4 (E0, 3F and DPC are not taken here)
  *   d_state      the FA SoA state rows (fa_device_state layout), stride >= n,
  *                of instances created for the same scheme (rows of another
  *                scheme keep bank numbers this one does not have, and step

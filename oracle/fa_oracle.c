@@ -386,6 +386,42 @@ static void orc_pia_write(orc_pia* p, uint16_t addr, uint8_t v)    /* pia.rs:202
     }
 }
 
+/* ------------------------------------------------- DPC (Pitfall II's cartridge chip)
+ * The reference has no DPC cart (its size rule cannot construct one).  This is
+ * the chip as its published descriptions give it (Activision's US patent
+ * 4,644,495 and the community's cartridge documentation), with the choices
+ * they leave open fixed here and in the device core alike:
+ *   - a read of $1000-$103F: fetcher k = a & 7, function f = (a >> 3) & 7.
+ *     The music channels are first brought up to the instruction's start
+ *     (Cpu::cycles), the random number generator steps, and a fetcher that is
+ *     not a music channel updates its flag (set when the counter's low byte
+ *     equals top, else cleared when it equals bottom).  f 0 reads the random
+ *     number (k < 4) or the music amplitude (k >= 4); f 1 the display byte at
+ *     the counter; f 2 that byte ANDed with the flag; f 7 the flag; the rest
+ *     0.  Then the counter counts down (11 bits), unless the fetcher is a
+ *     music channel.
+ *   - a write of $1040-$107F (same k and f): music brought up to date, then
+ *     f 0 top (and the flag cleared), f 1 bottom, f 2 counter low byte, f 3
+ *     counter bits 8-10 (and, for fetchers 5-7, music mode from bit 4), f 6
+ *     the random number reset to 1; the rest nothing.
+ *   - display data: the 2K after the 8K of program, addressed downward from
+ *     its end (counter c reads byte 2047 - c), as dumps of the cart hold it.
+ *   - music: the oscillator counts 20,000 clocks per second of CPU cycles
+ *     (3,579,545 / 3 per second), exactly: clock(t) = floor(t * 60000 /
+ *     3579545).  Each clock counts a music channel's low byte down by one;
+ *     the clock after 0 reloads top.  After an update that counted clocks,
+ *     a channel's flag is set while its low byte is above bottom.  The
+ *     amplitude is 4, 5 and 6 for channels 5, 6 and 7 whose flag is set,
+ *     summed.
+ *   - the random number generator shifts left, taking in the XNOR of bits 7,
+ *     5, 4 and 3; power-on value 1. */
+typedef struct orc_dpc {
+    uint16_t counter[8];
+    uint8_t  top[8], bottom[8];
+    uint8_t  flags, music, random;
+    uint32_t osc;
+} orc_dpc;
+
 /* ------------------------------------------------- HeadlessBus + HeadlessAtari */
 struct orc_atari {
     orc_cpu  cpu;
@@ -396,7 +432,8 @@ struct orc_atari {
     size_t   rom_len;
     int      bank;
     int      scheme;
-    int      slice[4];            /* E0 / 3F: the 1K ROM slice in each 1K window of $1000-$1FFF */
+    int      slice[4];            /* E0 / 3F / DPC: the 1K ROM slice in each 1K window of $1000-$1FFF */
+    orc_dpc  dpc;                 /* DPC registers (FA_SCHEME_DPC) */
     uint32_t frame_no;
     uint32_t run_status;
     uint64_t instructions;
@@ -438,9 +475,12 @@ static uint64_t orc_rom_hash(const uint8_t* rom, size_t len)
     return h;
 }
 
+static int orc_dpc_len(size_t len) { return len == 10240 || len == 10495; }
+
 static int orc_scheme_len_ok(int scheme, size_t len)
 {
     if (scheme == FA_SCHEME_E0) return len == 8192;
+    if (scheme == FA_SCHEME_DPC) return orc_dpc_len(len);
     if (scheme == FA_SCHEME_3F) return len >= 2048 && len <= 32768 && len % 2048 == 0;
     return orc_rom_len_ok(len) && orc_detect(len) == scheme;
 }
@@ -469,16 +509,17 @@ static int orc_scheme_for(const uint8_t* rom, size_t len)
     const uint64_t h = orc_rom_hash(rom, len);
     for (int i = 0; i < g_orc_nreg; i++)
         if (g_orc_reg[i].h == h && g_orc_reg[i].len == len) return g_orc_reg[i].scheme;
+    if (orc_dpc_len(len)) return FA_SCHEME_DPC;
     return orc_rom_len_ok(len) ? orc_detect(len) : -1;
 }
 
-static int orc_sliced(int scheme) { return scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_3F; }
+static int orc_sliced(int scheme) { return scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_3F || scheme == FA_SCHEME_DPC; }
 
 /* Power-on windows of the sliced schemes: E0 slices 4, 5, 6, 7; 3F 2K bank 0
  * under the last 2K. */
 static void orc_power_on_slices(int scheme, size_t len, int* slice)
 {
-    if (scheme == FA_SCHEME_E0) { slice[0] = 4; slice[1] = 5; slice[2] = 6; slice[3] = 7; return; }
+    if (scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_DPC) { slice[0] = 4; slice[1] = 5; slice[2] = 6; slice[3] = 7; return; }
     const int l = (int)(len / 2048) - 1;
     slice[0] = 0; slice[1] = 1; slice[2] = 2 * l; slice[3] = 2 * l + 1;
 }
@@ -487,6 +528,7 @@ static unsigned orc_mapper_of(int scheme, const int* slice)
 {
     if (scheme == FA_SCHEME_E0) return (unsigned)(slice[0] | slice[1] << 4 | slice[2] << 8);
     if (scheme == FA_SCHEME_3F) return (unsigned)(slice[0] / 2);
+    if (scheme == FA_SCHEME_DPC) return (unsigned)(slice[0] / 4);
     return 0;
 }
 
@@ -495,6 +537,7 @@ static void orc_slices_of(int scheme, size_t len, unsigned m, int* slice)
     orc_power_on_slices(scheme, len, slice);
     if (scheme == FA_SCHEME_E0) { slice[0] = m & 7; slice[1] = (m >> 4) & 7; slice[2] = (m >> 8) & 7; }
     else if (scheme == FA_SCHEME_3F) { const int b = (int)((m & 0xFF) % (len / 2048)); slice[0] = 2 * b; slice[1] = 2 * b + 1; }
+    else if (scheme == FA_SCHEME_DPC) for (int w = 0; w < 4; w++) slice[w] = 4 * (int)(m & 1) + w;
 }
 
 static void orc_load_window(orc_atari* e, int w)
@@ -536,6 +579,13 @@ static inline void orc_check_bankswitch(orc_atari* e, uint16_t addr) /* atari.rs
             orc_load_window(e, w);
         }
         return;
+    case FA_SCHEME_DPC:                      /* $1FF8 / $1FF9: program bank 0 / 1 */
+        if (a == 0x1FF8 || a == 0x1FF9)
+            for (int w = 0; w < 4; w++) {
+                e->slice[w] = 4 * (a - 0x1FF8) + w;
+                orc_load_window(e, w);
+            }
+        return;
     default: return;
     }
     if (nb != e->bank) {
@@ -544,9 +594,97 @@ static inline void orc_check_bankswitch(orc_atari* e, uint16_t addr) /* atari.rs
     }
 }
 
+/* The oscillator's clock count at CPU cycle t: floor(t * 60000 / 3579545)
+ * without overflowing 64 bits, modulo 2^32. */
+static uint32_t orc_dpc_clock_at(uint64_t t)
+{
+    return (uint32_t)((t / 3579545u) * 60000u + ((t % 3579545u) * 60000u) / 3579545u);
+}
+
+/* A music channel's low byte after k oscillator clocks. */
+static uint32_t orc_dpc_count_down(uint32_t low, uint32_t top, uint32_t k)
+{
+    if (k <= low) return low - k;
+    k -= low + 1;                                    /* the clock that leaves 0 reloads top */
+    return top - k % (top + 1);
+}
+
+static void orc_dpc_update(orc_atari* e)
+{
+    orc_dpc* d = &e->dpc;
+    const uint32_t now = orc_dpc_clock_at(e->cpu.cycles);
+    const uint32_t k = now - d->osc;
+    d->osc = now;
+    if (k == 0) return;
+    for (int m = 0; m < 3; m++) {
+        if (!((d->music >> m) & 1)) continue;
+        const int f = 5 + m;
+        const uint32_t low = orc_dpc_count_down(d->counter[f] & 0xFFu, d->top[f], k);
+        d->counter[f] = (uint16_t)((d->counter[f] & 0x700u) | low);
+        if (low > d->bottom[f]) d->flags |= (uint8_t)(1u << f);
+        else d->flags &= (uint8_t)~(1u << f);
+    }
+}
+
+static uint8_t orc_dpc_next_random(uint8_t r)
+{
+    const unsigned x = (unsigned)(r >> 7) ^ (unsigned)(r >> 5) ^ (unsigned)(r >> 4) ^ (unsigned)(r >> 3);
+    return (uint8_t)((r << 1) | (~x & 1u));
+}
+
+static uint8_t orc_dpc_read(orc_atari* e, uint16_t a)
+{
+    orc_dpc* d = &e->dpc;
+    const int k = a & 7, f = (a >> 3) & 7;
+    const int music = k >= 5 && ((d->music >> (k - 5)) & 1);
+    orc_dpc_update(e);
+    d->random = orc_dpc_next_random(d->random);
+    if (!music) {
+        const unsigned low = d->counter[k] & 0xFFu;
+        if (low == d->top[k]) d->flags |= (uint8_t)(1u << k);
+        else if (low == d->bottom[k]) d->flags &= (uint8_t)~(1u << k);
+    }
+    const uint8_t flag = ((d->flags >> k) & 1) ? 0xFF : 0x00;
+    const uint8_t data = e->rom[8192 + 2047 - d->counter[k]];
+    uint8_t v = 0;
+    switch (f) {
+    case 0:
+        if (k < 4) v = d->random;
+        else
+            for (int m = 0; m < 3; m++)
+                if (((d->music >> m) & 1) && ((d->flags >> (5 + m)) & 1)) v = (uint8_t)(v + 4 + m);
+        break;
+    case 1: v = data; break;
+    case 2: v = data & flag; break;
+    case 7: v = flag; break;
+    default: break;
+    }
+    if (!music) d->counter[k] = (uint16_t)((d->counter[k] - 1u) & 0x7FFu);
+    return v;
+}
+
+static void orc_dpc_write(orc_atari* e, uint16_t a, uint8_t v)
+{
+    orc_dpc* d = &e->dpc;
+    const int k = a & 7, f = (a >> 3) & 7;
+    orc_dpc_update(e);
+    switch (f) {
+    case 0: d->top[k] = v; d->flags &= (uint8_t)~(1u << k); break;
+    case 1: d->bottom[k] = v; break;
+    case 2: d->counter[k] = (uint16_t)((d->counter[k] & 0x700u) | v); break;
+    case 3:
+        d->counter[k] = (uint16_t)(((v & 7u) << 8) | (d->counter[k] & 0xFFu));
+        if (k >= 5) d->music = (uint8_t)((d->music & ~(1u << (k - 5))) | (((v >> 4) & 1u) << (k - 5)));
+        break;
+    case 6: d->random = 1; break;
+    default: break;
+    }
+}
+
 static inline uint8_t orc_bus_read(orc_atari* e, uint16_t addr)   /* atari.rs:497-520 */
 {
     uint16_t a = addr & 0x1FFF;
+    if (e->scheme == FA_SCHEME_DPC && (a & 0x1FC0) == 0x1000) return orc_dpc_read(e, a);
     if ((a & 0x1080) != 0 && (a & 0x1280) != 0x0280) {
         if ((a & 0x1000) && e->scheme != FA_SCHEME_FIXED) orc_check_bankswitch(e, addr);
         return e->mem[a];
@@ -560,6 +698,7 @@ static inline void orc_bus_write(orc_atari* e, uint16_t addr, uint8_t v) /* atar
 {
     uint16_t a = addr & 0x1FFF;
     if (a & 0x1000) {
+        if (e->scheme == FA_SCHEME_DPC && (a & 0x1FC0) == 0x1040) orc_dpc_write(e, a, v);
         if (e->scheme != FA_SCHEME_FIXED) orc_check_bankswitch(e, addr);
         return;
     }
@@ -644,9 +783,13 @@ orc_atari* orc_create(const uint8_t* rom, size_t rom_len)          /* atari.rs:4
     case FA_SCHEME_FIXED: e->bank = 0; break;
     case FA_SCHEME_F8: e->bank = 1; break;
     case FA_SCHEME_F6: e->bank = 3; break;
-    case FA_SCHEME_E0: case FA_SCHEME_3F: e->bank = 0; orc_power_on_slices(scheme, rom_len, e->slice); break;
+    case FA_SCHEME_E0: case FA_SCHEME_3F: case FA_SCHEME_DPC:
+        e->bank = 0;
+        orc_power_on_slices(scheme, rom_len, e->slice);
+        break;
     default: e->bank = 7; break;
     }
+    if (scheme == FA_SCHEME_DPC) e->dpc.random = 1;
     orc_tia_default(&e->tia);
     orc_pia_default(&e->pia);
     e->cpu.sp = 0xFD;                                              /* Cpu::default, cpu.rs:107-119 */
@@ -771,6 +914,11 @@ void orc_get_state(const orc_atari* e, fa_state* s)                /* cuda_env.r
     s->cycles = e->cpu.cycles;
     s->frame_no = e->frame_no;
     s->run_status = e->run_status;
+    memcpy(s->dpc_counter, e->dpc.counter, sizeof(s->dpc_counter));
+    memcpy(s->dpc_top, e->dpc.top, 8);
+    memcpy(s->dpc_bottom, e->dpc.bottom, 8);
+    s->dpc_flags = e->dpc.flags; s->dpc_music = e->dpc.music; s->dpc_random = e->dpc.random;
+    s->dpc_osc = e->dpc.osc;
 }
 
 void orc_set_state(orc_atari* e, const fa_state* s)
@@ -803,6 +951,15 @@ void orc_set_state(orc_atari* e, const fa_state* s)
     t->pf0 = s->pf0; t->pf1 = s->pf1; t->pf2 = s->pf2;
     e->frame_no = s->frame_no;
     e->run_status = s->run_status;
+    memset(&e->dpc, 0, sizeof(e->dpc));                /* other schemes: the DPC fields are not taken */
+    if (e->scheme == FA_SCHEME_DPC) {
+        memcpy(e->dpc.counter, s->dpc_counter, sizeof(e->dpc.counter));
+        for (int k = 0; k < 8; k++) e->dpc.counter[k] &= 0x7FFu;
+        memcpy(e->dpc.top, s->dpc_top, 8);
+        memcpy(e->dpc.bottom, s->dpc_bottom, 8);
+        e->dpc.flags = s->dpc_flags; e->dpc.music = s->dpc_music & 7u; e->dpc.random = s->dpc_random;
+        e->dpc.osc = s->dpc_osc;
+    }
     /* The bank index is clamped to the scheme's range when the flat array is
      * rebuilt; the scheme itself always follows the ROM. */
     int nb = s->bank;
@@ -1340,7 +1497,7 @@ static void orc_rbus_write(orc_ratari* e, uint16_t addr, uint8_t v) /* atari.rs:
 orc_ratari* orc_rcreate(const uint8_t* rom, size_t rom_len)        /* atari.rs:120-136, 240-247 */
 {
     const int scheme = orc_scheme_for(rom, rom_len);
-    if (scheme < 0) return NULL;
+    if (scheme < 0 || scheme == FA_SCHEME_DPC) return NULL;        /* DPC carts run headless only */
     orc_ratari* e = (orc_ratari*)calloc(1, sizeof(orc_ratari));
     if (!e) return NULL;
     e->rom = (uint8_t*)malloc(rom_len);

@@ -19,7 +19,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_build" / "libfa_oracle.so"
 
-STATE_BYTES = 240
+STATE_BYTES = 280
 
 # fa_state (include/fast_atari.h), restated for the checker.
 _fields = [
@@ -48,11 +48,14 @@ _fields = [
     ("bank", "u1"), ("scheme", "u1"), ("_pad_end", "u1", (2,)),
     ("mapper", "u1", (2,)), ("_pad_ext", "u1"),
     ("cycles", "<u8"), ("frame_no", "<u4"), ("run_status", "<u4"),
+    ("dpc_counter", "<u2", (8,)), ("dpc_top", "u1", (8,)), ("dpc_bottom", "u1", (8,)),
+    ("dpc_flags", "u1"), ("dpc_music", "u1"), ("dpc_random", "u1"), ("_pad_dpc", "u1"),
+    ("dpc_osc", "<u4"),
 ]
 STATE_DTYPE = np.dtype(_fields, align=False)
 assert STATE_DTYPE.itemsize == STATE_BYTES, STATE_DTYPE.itemsize
 
-PAD_FIELDS = ("_pad0", "_pad1", "_pad2", "_pad3", "_pad4", "_pad5", "_pad_end", "_pad_ext")
+PAD_FIELDS = ("_pad0", "_pad1", "_pad2", "_pad3", "_pad4", "_pad5", "_pad_end", "_pad_ext", "_pad_dpc")
 COMPARED_FIELDS = tuple(n for n in STATE_DTYPE.names if n not in PAD_FIELDS)
 
 
@@ -281,7 +284,7 @@ def render_steps(consoles, actions: np.ndarray, nthreads: int | None = None, out
     return (np.stack([c.framebuffer() for c in consoles]), np.stack([c.ram() for c in consoles]))
 
 
-SCHEMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "auto": -1}
+SCHEMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "dpc": 6, "auto": -1}
 
 
 def set_rom_scheme(rom: bytes, scheme) -> None:

@@ -8,11 +8,11 @@
 #include "../../fast-atari-rs_b200/csrc/fa_run.cuh"
 #include "../../fast-atari-rs_b200/csrc/fa_render.cuh"
 
-template <bool SL>
+template <bool SL, bool DPC = false>
 static void run_one(const FaGroup& G, uint32_t i, uint8_t* rom, unsigned long long* instr)
 {
     uint32_t priv[FA_SMEM_WORDS];
-    fa::Runner<1, SL> r;
+    fa::Runner<1, SL, DPC> r;
     r.f = 0; r.phase = 0; r.fcyc = 0; r.active = false;
     r.e.pv = (uint8_t*)priv;
     r.e.G = &G; r.e.i = i; r.e.rom = rom; r.e.hot_lo = G.hot_lo; r.e.nbanks = G.nbanks;
@@ -46,7 +46,8 @@ extern "C" long long hs_run(const uint8_t* rom, size_t len, fa_state* st, size_t
     G.actions = actions; G.act_stride = (uint32_t)n; G.nbanks = nbanks; G.hot_lo = hot_lo; G.k = (uint32_t)k;
     unsigned long long instr = 0;
     for (uint32_t i = 0; i < n; i++) {
-        if (fa_map_kind(hot_lo)) run_one<true>(G, i, simg.data(), &instr);
+        if (fa_map_kind(hot_lo) == FA_MAP_DPC) run_one<true, true>(G, i, simg.data(), &instr);   // as run_unit
+        else if (fa_map_kind(hot_lo)) run_one<true>(G, i, simg.data(), &instr);
         else run_one<false>(G, i, simg.data(), &instr);
     }
     for (size_t i = 0; i < n; i++) fa_unpack_column(rows.data() + i, n, scheme, st[i]);

@@ -40,7 +40,7 @@ def test_library_loads_and_reports_version():
 
 def test_state_dtype_matches_oracle_and_header():
     assert fa.STATE_DTYPE == oracle.STATE_DTYPE
-    assert oracle.lib().orc_state_size() == 240
+    assert oracle.lib().orc_state_size() == 280
     off = {n: fa.STATE_DTYPE.fields[n][1] for n in fa.STATE_DTYPE.names}
     # offsets pinned by FA_STATIC_ASSERT in include/fast_atari.h
     assert (off["ram"], off["timer_value"], off["tia_clock"], off["paddle_counter"],

@@ -1,11 +1,13 @@
-"""GPU parity of the E0 and 3F bank-switching schemes (registered per ROM).
+"""GPU parity of the E0 and 3F bank-switching schemes (registered per ROM) and
+of DPC carts (Pitfall II's scheme, picked by length).
 
-The reference has neither scheme (it crashes on E0 carts), so the oracle's
-restatement, pinned by the hand-checked programs of test_mappers.py, is the
-checker here: full state (including the slice map) and RAM after every call,
-through the handle's persistent and plain forms, every warp policy, a pool
-that mixes sliced and 4K-bank carts in one launch, state upload, and the
-rendering console."""
+The reference has none of these (it crashes on E0 and DPC carts), so the
+oracle's restatement, pinned by the hand-checked programs of test_mappers.py,
+is the checker here: full state (including the slice map and the DPC
+registers) and RAM after every call, through the handle's persistent and
+plain forms, every warp policy, a pool that mixes sliced and 4K-bank carts in
+one launch, state upload, the server and the rendering console (which takes
+E0 and 3F, and refuses DPC)."""
 import numpy as np
 import pytest
 
@@ -35,10 +37,15 @@ def sliced():
         oracle.set_rom_scheme(c.rom, "auto")
 
 
-@pytest.mark.parametrize("name", ["e0", "3f16", "3f6"])
+@pytest.fixture(scope="module")
+def dpc():
+    return {"dpc": carts.dpc_cart(), "dpc_tail": carts.dpc_cart(dump_tail=True)}
+
+
+@pytest.mark.parametrize("name", ["e0", "3f16", "3f6", "dpc", "dpc_tail"])
 @pytest.mark.parametrize("sched", ["pc", "lane", "line", "match"])
-def test_sliced_carts_match_oracle(sliced, name, sched):
-    rom = sliced[name].rom
+def test_sliced_carts_match_oracle(sliced, dpc, name, sched):
+    rom = (dpc[name] if name.startswith("dpc") else sliced[name]).rom
     n, k, chunk = 150, 12, 4
     acts = carts.actions(seed=21, n=n, frames=k)
     ref = oracle_states(rom, n)
@@ -53,8 +60,11 @@ def test_sliced_carts_match_oracle(sliced, name, sched):
             assert np.array_equal(obs, o_obs), f"{name}/{sched} frames {f0}..{f0 + chunk}"
             assert_states_equal(g.download_states(), ref, f"{name}/{sched} after {f0 + chunk}")
     maps = {int(m[0]) | int(m[1]) << 8 for m in ref["mapper"]}
-    assert int(ref["scheme"][0]) in (4, 5)
+    assert int(ref["scheme"][0]) in (4, 5, 6)
     assert len(maps) >= 1
+    if name.startswith("dpc"):                              # the cart reaches every DPC mechanism
+        assert len(maps) == 2 and ref["dpc_music"].any() and (ref["dpc_music"] == 0).any()
+        assert len({bytes(r) for r in ref["dpc_counter"]}) > n // 2
 
 
 @pytest.mark.parametrize("block,persistent", [(256, False), (128, True)])
@@ -73,10 +83,11 @@ def test_sliced_launch_shapes_and_per_frame(sliced, block, persistent):
         assert_states_equal(g.download_states(), ref, f"block {block} persistent {persistent}")
 
 
-def test_pool_mixes_sliced_and_4k_bank_carts(sliced):
+def test_pool_mixes_sliced_and_4k_bank_carts(sliced, dpc):
     mixed = carts.mixed_carts()
-    roms = [mixed[0].rom, sliced["e0"].rom, mixed[2].rom, sliced["3f16"].rom, sliced["3f6"].rom, mixed[3].rom]
-    counts = [300, 200, 90, 130, 64, 33]
+    roms = [mixed[0].rom, sliced["e0"].rom, mixed[2].rom, sliced["3f16"].rom, sliced["3f6"].rom, mixed[3].rom,
+            dpc["dpc"].rom]
+    counts = [300, 200, 90, 130, 64, 33, 77]
     k = 5
     acts = [carts.actions(seed=50 + i, n=n, frames=k) for i, n in enumerate(counts)]
     with fa.AtariPool() as pool:
@@ -108,6 +119,75 @@ def test_sliced_state_upload_round_trip(sliced):
         assert_states_equal(g.download_states(), ref, "continued")
 
 
+def test_dpc_state_upload_round_trip(dpc):
+    """DPC registers set by hand (counters, tops, bottoms, flags, music
+    channels, random number, oscillator count) go up and come back unchanged,
+    and running on from them matches the oracle started from the same
+    states."""
+    rom = dpc["dpc"].rom
+    n = 96
+    ref = oracle_states(rom, n)
+    oracle.run_batch(rom, ref, carts.actions(seed=5, n=n, frames=3), 3)
+    rng = np.random.default_rng(7)
+    ref["dpc_counter"] = rng.integers(0, 2048, (n, 8))
+    ref["dpc_top"] = rng.integers(0, 256, (n, 8))
+    ref["dpc_bottom"] = rng.integers(0, 256, (n, 8))
+    ref["dpc_flags"] = rng.integers(0, 256, n)
+    ref["dpc_music"] = rng.integers(0, 8, n)
+    ref["dpc_random"] = rng.integers(0, 256, n)
+    ref["dpc_osc"] = rng.integers(0, 2**32, n, dtype=np.uint64)
+    ref["mapper"][:, 0] = np.arange(n) % 2
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.upload_states(ref)
+        assert_states_equal(g.download_states(), ref, "round trip")
+        acts = carts.actions(seed=6, n=n, frames=4)
+        obs = g.step_multi(acts, 4)
+        o_obs, _ = oracle.run_batch(rom, ref, acts, 4)
+        assert np.array_equal(obs, o_obs)
+        assert_states_equal(g.download_states(), ref, "continued")
+
+
+def test_dpc_script_cart_matches_oracle():
+    """The scripted DPC cart whose oracle run the step-by-step model of
+    test_mappers.py predicts: every fetcher function, the 11-bit wrap, the
+    random number generator around a reset and two music channels."""
+    rom = carts.dpc_script_cart().rom
+    n = 64
+    ref = oracle_states(rom, n)
+    acts = carts.actions(seed=8, n=n, frames=3)
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.reset()
+        obs = g.step_multi(acts, 3)
+        o_obs, _ = oracle.run_batch(rom, ref, acts, 3)
+        assert np.array_equal(obs, o_obs)
+        assert_states_equal(g.download_states(), ref, "dpc script")
+
+
+def test_dpc_fields_not_taken_by_other_schemes():
+    rom = carts.plain_cart().rom
+    n = 40
+    ref = oracle_states(rom, n)
+    up = ref.copy()
+    up["dpc_counter"] = 0x155
+    up["dpc_bottom"] = 3
+    up["dpc_flags"] = 0xFF
+    up["dpc_osc"] = 99
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.upload_states(up)
+        got = g.download_states()
+        assert_states_equal(got, ref, "DPC fields dropped")
+        acts = carts.actions(seed=9, n=n, frames=2)
+        g.step_multi(acts, 2)
+        oracle.run_batch(rom, ref, acts, 2)
+        assert_states_equal(g.download_states(), ref, "run on")
+
+
+def test_rendering_console_refuses_dpc(dpc):
+    with pytest.raises(fa.FaError) as ei:
+        fa.AtariRender(dpc["dpc"].rom, 4)
+    assert ei.value.code == fa.FA_ERR_BAD_ROM
+
+
 @pytest.mark.parametrize("name", ["e0", "3f16"])
 def test_sliced_rendering_console_matches_oracle(sliced, name):
     rom = sliced[name].rom
@@ -126,8 +206,8 @@ def test_sliced_rendering_console_matches_oracle(sliced, name):
                 assert int(st[i]["mapper"][0]) | int(st[i]["mapper"][1]) << 8 == con.mapper(), f"{name} mapper {i}"
 
 
-def test_sliced_carts_in_the_server(sliced):
-    roms = [sliced["e0"].rom, carts.mixed_carts()[1].rom, sliced["3f6"].rom]
+def test_sliced_carts_in_the_server(sliced, dpc):
+    roms = [sliced["e0"].rom, carts.mixed_carts()[1].rom, dpc["dpc"].rom]
     reqs = [(0, 70, 3), (1, 40, 2), (2, 33, 4), (0, 70, 2)]
     with fa.AtariServer(roms) as srv:
         sids = {c: srv.open(c) for c in (0, 1, 2)}
@@ -141,25 +221,26 @@ def test_sliced_carts_in_the_server(sliced):
         assert_states_equal(states[c], ref[c], f"cart {c}")
 
 
-@pytest.mark.parametrize("name", ["e0_8k", "3f_16k", "3f_6k"])
-def test_sliced_carts_match_committed_golden_vectors(sliced, name):
+@pytest.mark.parametrize("name", ["e0_8k", "3f_16k", "3f_6k", "dpc_10k"])
+def test_sliced_carts_match_committed_golden_vectors(sliced, dpc, name):
     """The frozen oracle vectors of tests/golden/ (RAM at checkpoint frames and
     the full final state, mapper field included), without running the oracle."""
     import hashlib
     import json
     from pathlib import Path
+    from make_golden import state_sha
     want = json.loads((Path(__file__).parent / "golden" / "oracle_vectors.json").read_text())[name]
-    rom = {"e0_8k": sliced["e0"], "3f_16k": sliced["3f16"], "3f_6k": sliced["3f6"]}[name].rom
+    rom = {"e0_8k": sliced["e0"], "3f_16k": sliced["3f16"], "3f_6k": sliced["3f6"], "dpc_10k": dpc["dpc"]}[name].rom
     assert hashlib.sha256(rom).hexdigest() == want["rom_sha256"]
     n, frames = want["n"], want["frames"]
     acts = carts.actions(seed=want["action_seed"], n=n, frames=frames)
     with fa.BatchAtariGpu(rom, n) as g:
         g.reset()
-        assert hashlib.sha256(g.download_states()[:1].tobytes()).hexdigest() == want["reset_state_sha256"]
+        assert state_sha(g.download_states()[:1]) == want["reset_state_sha256"]
         done = 0
         for f_end in sorted(int(x) for x in want["ram_sha256_at"]):
             obs = g.step_multi(acts[done:f_end], f_end - done)
             done = f_end
             assert hashlib.sha256(obs.tobytes()).hexdigest() == want["ram_sha256_at"][str(f_end)], f_end
         st = g.download_states()
-    assert hashlib.sha256(st.tobytes()).hexdigest() == want["final_state_sha256"]
+    assert state_sha(st) == want["final_state_sha256"]

@@ -317,6 +317,7 @@ def test_matches_committed_golden_vectors(name):
     """The CUDA path reproduces the frozen oracle vectors (tests/golden/) without
     running the oracle: RAM at checkpoint frames and the full final state."""
     import hashlib
+    from make_golden import state_sha
     want = _golden()[name]
     rom = cart(name)
     assert hashlib.sha256(rom).hexdigest() == want["rom_sha256"]
@@ -324,11 +325,11 @@ def test_matches_committed_golden_vectors(name):
     acts = carts.actions(seed=want["action_seed"], n=n, frames=frames)
     with fa.BatchAtariGpu(rom, n) as g:
         g.reset()
-        assert hashlib.sha256(g.download_states()[:1].tobytes()).hexdigest() == want["reset_state_sha256"]
+        assert state_sha(g.download_states()[:1]) == want["reset_state_sha256"]
         done = 0
         for f_end in sorted(int(x) for x in want["ram_sha256_at"]):
             obs = g.step_multi(acts[done:f_end], f_end - done)
             done = f_end
             assert hashlib.sha256(obs.tobytes()).hexdigest() == want["ram_sha256_at"][str(f_end)], f_end
         st = g.download_states()
-    assert hashlib.sha256(st.tobytes()).hexdigest() == want["final_state_sha256"]
+    assert state_sha(st) == want["final_state_sha256"]

@@ -17,7 +17,7 @@ from test_gpu_parity import assert_states_equal
 
 pytestmark = pytest.mark.gpu
 
-BLOCK_BYTES = 57 * 256 * 4      # one state block of the server (FA_ROWS x 256 words)
+BLOCK_BYTES = 67 * 256 * 4      # one state block of the server (FA_ROWS x 256 words)
 
 
 @pytest.fixture(scope="module", autouse=True)

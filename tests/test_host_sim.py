@@ -80,14 +80,18 @@ def test_device_core_matches_oracle_on_carts(sim, c):
     assert_same(got, ref, c.spec.name)
 
 
-@pytest.mark.parametrize("name", ["e0", "3f16", "3f6"])
+@pytest.mark.parametrize("name", ["e0", "3f16", "3f6", "dpc", "dpc_tail", "dpc_script"])
 def test_device_core_matches_oracle_on_sliced_carts(sim, name):
-    c, code = {"e0": (carts.e0_cart(), 4), "3f16": (carts.f3_cart(16384), 5), "3f6": (carts.f3_cart(6144), 5)}[name]
+    """E0 and 3F registered per ROM; DPC picked by its lengths (10,240 and
+    10,495 bytes) on both sides."""
+    c, code = {"e0": (carts.e0_cart(), 4), "3f16": (carts.f3_cart(16384), 5), "3f6": (carts.f3_cart(6144), 5),
+               "dpc": (carts.dpc_cart(), -1), "dpc_tail": (carts.dpc_cart(dump_tail=True), -1),
+               "dpc_script": (carts.dpc_script_cart(), -1)}[name]
     r = np.frombuffer(c.rom, np.uint8).copy()
     sim.fa_rom_set_scheme(r.ctypes.data, len(r), code)
     oracle.set_rom_scheme(c.rom, code)
     try:
-        n, k = 40, 4
+        n, k = 40, 12 if code < 0 else 4
         start = np.array([oracle.reset_state(c.rom)] * n, dtype=oracle.STATE_DTYPE)
         got, ref = run_both(sim, c.rom, start, carts.actions(seed=2, n=n, frames=k), k)
         assert_same(got, ref, name)

@@ -1,4 +1,4 @@
-"""Bank-switching schemes the reference lacks (E0, 3F), checked without a GPU.
+"""Bank-switching schemes the reference lacks (E0, 3F, DPC), checked without a GPU.
 
 The reference picks a scheme from the ROM length alone (BankScheme::detect,
 src/atari.rs:96-105), so an 8K Parker Brothers E0 cart runs as F8 there and
@@ -6,7 +6,11 @@ crashes (montezuma_revenge and tutankham in bench_all_fast_atari.json).  The
 library and the oracle take a scheme registered per ROM image instead.
 These tests pin the oracle's E0 and 3F restatement on small hand-written
 programs whose expected RAM is worked out from the ROM bytes, then check the
-registry and the content guess through the C ABI (host code only)."""
+registry and the content guess through the C ABI (host code only).  DPC
+carts (Pitfall II, 10,240 or 10,495 bytes, which the reference's size rule
+cannot construct: pitfall2 in bench_all_fast_atari.json) are picked by
+length; the oracle's DPC is pinned against a second, step-by-step model of
+the chip on a scripted cart."""
 import numpy as np
 import pytest
 
@@ -197,3 +201,155 @@ def test_registry_is_safe_across_threads():
     for rom in roms:
         fa.set_rom_scheme(rom, "auto")
         assert fa.rom_scheme(rom) == 1
+
+
+# ------------------------------------------------------------------ DPC
+class DpcModel:
+    """Pitfall II's DPC chip, restated a second time and step by step, as the
+    check of the oracle's DPC: the music channels are clocked one oscillator
+    clock at a time (the oracle and the device count many clocks in closed
+    form), and the rules are written out again from their description:
+    - reads of $1000-$103F: fetcher a & 7, function (a >> 3) & 7; music
+      first brought up to the instruction's start cycle t (oscillator clock
+      t * 60000 // 3579545), the random number generator stepped, a fetcher
+      that is no music channel sets its flag at counter low byte == top, else
+      clears it at == bottom; functions 0 (random number for fetchers 0-3,
+      else the music amplitude 4/5/6 per sounding channel 5/6/7), 1 (display
+      byte 2047 - counter), 2 (display byte AND flag), 7 (flag), else 0; then
+      the counter (11 bits) counts down unless the fetcher is a music channel;
+    - writes of $1040-$107F: music brought up to date; 0 top (flag cleared),
+      1 bottom, 2 counter low, 3 counter high three bits (+ music mode from
+      bit 4 for fetchers 5-7), 6 random number := 1;
+    - a music clock counts the low byte down, the clock after 0 reloads top;
+      after clocks were counted, a channel's flag is set while low > bottom."""
+
+    def __init__(self, display):
+        self.display = display
+        self.counter = [0] * 8
+        self.top = [0] * 8
+        self.bottom = [0] * 8
+        self.flag = [0] * 8
+        self.music = [0] * 3
+        self.random = 1
+        self.osc = 0
+
+    def update(self, t):
+        now = (t * 60000 // 3579545) & 0xFFFFFFFF
+        clocks = (now - self.osc) & 0xFFFFFFFF
+        self.osc = now
+        if not clocks:
+            return
+        for m in range(3):
+            if not self.music[m]:
+                continue
+            f = 5 + m
+            low = self.counter[f] & 0xFF
+            for _ in range(clocks):
+                low = self.top[f] if low == 0 else low - 1
+            self.counter[f] = (self.counter[f] & 0x700) | low
+            self.flag[f] = 1 if low > self.bottom[f] else 0
+
+    def read(self, a, t):
+        k, fn = a & 7, (a >> 3) & 7
+        music = k >= 5 and self.music[k - 5]
+        self.update(t)
+        r = self.random
+        feedback = 1 - (((r >> 7) ^ (r >> 5) ^ (r >> 4) ^ (r >> 3)) & 1)
+        self.random = ((r << 1) | feedback) & 0xFF
+        if not music:
+            low = self.counter[k] & 0xFF
+            if low == self.top[k]:
+                self.flag[k] = 1
+            elif low == self.bottom[k]:
+                self.flag[k] = 0
+        data = self.display[2047 - self.counter[k]]
+        flag = 0xFF if self.flag[k] else 0
+        if fn == 0:
+            v = self.random if k < 4 else sum(4 + m for m in range(3) if self.music[m] and self.flag[5 + m])
+        else:
+            v = {1: data, 2: data & flag, 7: flag}.get(fn, 0)
+        if not music:
+            self.counter[k] = (self.counter[k] - 1) & 0x7FF
+        return v
+
+    def write(self, a, v, t):
+        k, fn = a & 7, (a >> 3) & 7
+        self.update(t)
+        if fn == 0:
+            self.top[k] = v
+            self.flag[k] = 0
+        elif fn == 1:
+            self.bottom[k] = v
+        elif fn == 2:
+            self.counter[k] = (self.counter[k] & 0x700) | v
+        elif fn == 3:
+            self.counter[k] = ((v & 7) << 8) | (self.counter[k] & 0xFF)
+            if k >= 5:
+                self.music[k - 5] = (v >> 4) & 1
+        elif fn == 6:
+            self.random = 1
+
+
+def test_oracle_dpc_matches_a_step_by_step_model():
+    """dpc_script_cart runs carts.dpc_script() straight-line in its second
+    frame; the model replays the same accesses at the same instruction start
+    cycles (LDA # 2, STA abs 4, LDA abs 4, STA zp 3, NOP 2) and must predict
+    every value read and every DPC register the oracle ends with."""
+    c = carts.dpc_script_cart()
+    st = np.array([oracle.reset_state(c.rom)], dtype=oracle.STATE_DTYPE)
+    assert int(st["scheme"][0]) == 6 and int(st["mapper"][0][0]) == 1 and int(st["dpc_random"][0]) == 1
+    t = int(st["cycles"][0]) + 2 + 3                       # the frame's LDA #0 / STA VSYNC
+    oracle.run_batch(c.rom, st, np.zeros((1, 1), np.uint8), 1)
+    m = DpcModel([carts.dpc_display_byte(i) for i in range(2048)])
+    want = []
+    for step in carts.dpc_script():
+        if step[0] == "w":
+            t += 2
+            m.write(step[1], step[2], t)
+            t += 4
+        elif step[0] == "r":
+            want.append(m.read(step[1], t))
+            t += 4 + 3
+        else:
+            t += 2 * step[1]
+    got = [int(x) for x in st["ram"][0][:len(want)]]
+    assert got == want
+    assert [int(x) for x in st["dpc_counter"][0]] == m.counter
+    assert [int(x) for x in st["dpc_top"][0]] == m.top
+    assert [int(x) for x in st["dpc_bottom"][0]] == m.bottom
+    assert int(st["dpc_flags"][0]) == sum(f << k for k, f in enumerate(m.flag))
+    assert int(st["dpc_music"][0]) == sum(b << i for i, b in enumerate(m.music))
+    assert int(st["dpc_random"][0]) == m.random and int(st["dpc_osc"][0]) == m.osc
+    # The script reached what it is for: a flag set and cleared, the 11-bit
+    # wrap, a sounding amplitude of each channel alone and together.
+    assert 0xFF in got and 0 in got and {4, 5, 9} <= set(got)
+
+
+def test_oracle_dpc_schemes_by_length():
+    c = carts.dpc_cart()
+    assert int(oracle.reset_state(c.rom)["scheme"]) == 6
+    assert int(oracle.reset_state(carts.dpc_cart(dump_tail=True).rom)["scheme"]) == 6
+    assert fa.rom_scheme(c.rom) == 6 and fa.rom_scheme(carts.dpc_cart(dump_tail=True).rom) == 6
+    assert fa.guess_rom_scheme(c.rom) == 6
+    for n in (10239, 10241, 10494, 10496):
+        with pytest.raises(fa.FaError):
+            fa.rom_scheme(bytes(n))
+    st = oracle.reset_state(carts.plain_cart().rom)                # other schemes keep the DPC fields at 0
+    assert not st["dpc_counter"].any() and int(st["dpc_random"]) == 0 and int(st["dpc_osc"]) == 0
+
+
+def test_oracle_ignores_dpc_fields_of_other_schemes():
+    """A state of another scheme carrying nonzero DPC fields runs as if they
+    were 0, and comes back with them 0 (fa_set_states does the same)."""
+    rom = carts.plain_cart().rom
+    a = np.array([oracle.reset_state(rom)] * 4, dtype=oracle.STATE_DTYPE)
+    b = a.copy()
+    b["dpc_counter"] = 0x3FF
+    b["dpc_top"] = 7
+    b["dpc_music"] = 7
+    b["dpc_random"] = 9
+    b["dpc_osc"] = 12345
+    acts = carts.actions(seed=3, n=4, frames=3)
+    oracle.run_batch(rom, a, acts, 3)
+    oracle.run_batch(rom, b, acts, 3)
+    assert a.tobytes() == b.tobytes()
