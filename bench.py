@@ -1,7 +1,7 @@
 """Benchmark of the batched Atari 2600 core on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mixed|divergence|plain|scale|serve|render|mappers|micro]
+                    [--workload mixed|divergence|plain|scale|serve|render|mappers|dpc|micro]
 
 Default workload (the batched configuration the headline metric is quoted
 on): four seeded synthetic carts — 2K Fixed, 8K F8, 16K F6, 32K F4 with
@@ -113,6 +113,11 @@ def workload(name: str, carts):
         # Schemes the reference lacks, registered per ROM (fa_rom_set_scheme).
         return ("sliced-bank carts: 8K E0 / 16K 3F / 6K 3F, 40000/40000/20000 instances, K=4 frames per call",
                 [(carts.e0_cart(), 40_000), (carts.f3_cart(16384), 40_000), (carts.f3_cart(6144), 20_000)], 4, 0)
+    if name == "dpc":
+        # Pitfall II's scheme, picked by ROM length (10,240 and 10,495 bytes).
+        return ("DPC carts (fetchers, random numbers, music channels): 10240- and 10495-byte images, "
+                "40000/40000 instances, K=4 frames per call",
+                [(carts.dpc_cart(), 40_000), (carts.dpc_cart(dump_tail=True), 40_000)], 4, 0)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -952,7 +957,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed",
                     choices=["mixed", "divergence", "plain", "scale", "converged", "serve", "render", "mappers",
-                             "micro"])
+                             "dpc", "micro"])
     ap.add_argument("--serve-requests", type=int, default=20000, help="saturation requests of the serve workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     ap.add_argument("--render-instances", type=int, default=RENDER_N, help="consoles of the render workload")

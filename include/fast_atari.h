@@ -460,7 +460,7 @@ int fa_autotune(const uint8_t* rom, size_t rom_len, size_t n, fa_tuning* best,
  * if n exceeds the instances the session holds, the new ones are admitted
  * first, each starting from the cart's post-reset snapshot (BatchAtariGpu::
  * reset, src/cuda_env.rs:131-142).  Admission is charged against a budget of
- * state bytes (whole 256-instance blocks of 58,368 bytes); when the budget is
+ * state bytes (whole 256-instance blocks of 68,608 bytes); when the budget is
  * spent, admissions wait in FIFO order until a session is closed.  A
  * session's requests run one at a time in submission order; requests of
  * different sessions are batched into shared launches whenever they are
