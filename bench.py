@@ -1,7 +1,7 @@
 """Benchmark of the batched Atari 2600 core on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mixed|divergence|plain|scale|serve|render|mappers|dpc|micro]
+                    [--workload mixed|divergence|plain|scale|serve|render|mappers|dpc|fe|micro]
 
 Default workload (the batched configuration the headline metric is quoted
 on): four seeded synthetic carts — 2K Fixed, 8K F8, 16K F6, 32K F4 with
@@ -118,6 +118,10 @@ def workload(name: str, carts):
         return ("DPC carts (fetchers, random numbers, music channels): 10240- and 10495-byte images, "
                 "40000/40000 instances, K=4 frames per call",
                 [(carts.dpc_cart(), 40_000), (carts.dpc_cart(dump_tail=True), 40_000)], 4, 0)
+    if name == "fe":
+        # Activision FE, registered per ROM (fa_rom_set_scheme).
+        return ("FE cart (bank chosen by the access after one to $01FE): 8K, 80000 instances, K=4 frames per call",
+                [(carts.fe_cart(), 80_000)], 4, 0)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -957,7 +961,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixed",
                     choices=["mixed", "divergence", "plain", "scale", "converged", "serve", "render", "mappers",
-                             "dpc", "micro"])
+                             "dpc", "fe", "micro"])
     ap.add_argument("--serve-requests", type=int, default=20000, help="saturation requests of the serve workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     ap.add_argument("--render-instances", type=int, default=RENDER_N, help="consoles of the render workload")

@@ -221,7 +221,7 @@ def wait_limit_ns() -> int:
     return int(lib().fa_wait_limit_ns_get())
 
 
-SCHEME_NAMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "dpc": 6, "auto": -1}
+SCHEME_NAMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "dpc": 6, "fe": 7, "auto": -1}
 
 
 def _scheme_code(scheme) -> int:

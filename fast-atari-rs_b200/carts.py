@@ -906,6 +906,97 @@ def f3_cart(size: int = 16384, seed: int = 7, lines: int = 64) -> Cart:
     return Cart(CartSpec(f"3f_{size // 1024}k", size, seed, wsync_density=1.0), rom, labels, scheme="3f")
 
 
+FE_BANKID = 0xFE80
+FE_SUB = 0xFA00                                      # the subroutine, at $1A00 of both banks
+FE_TABLE = 0xFB00                                    # 256 bytes of bank-specific data
+
+
+def fe_cart(seed: int = 9, lines: int = 40) -> Cart:
+    """Activision FE cart, 8K: two 4K banks with the same code at the same
+    addresses (only the bank-id byte at $FE80 and a data table at $FB00
+    differ), so a switch at any access keeps running.  Each visible line arms
+    the cart through every kind of access to $01FE and lets the next access
+    pick the bank:
+      - JSR with S = $FF (the low return byte lands on $01FE; the target's
+        high byte, $DA or $FA as a RAM bit chooses, selects bank 1 or 0), and
+        RTS with S = $FD (pulls from $01FE; the high return byte selects);
+      - JSR with S = $FE (its stack read at $01FE arms, the push of the high
+        byte there selects and re-arms, the low byte's push selects), and the
+        matching RTS with S = $FC (the high byte pulled from $01FE arms, the
+        read at the return address selects);
+      - PLA with S = $FE (its stack read arms, the pulled byte selects);
+      - PHA and PLA at $01FE, LDA $01FE and LDA $01F0,X with X = $0E (the
+        next opcode fetch selects), and INC $01FE on every 4th line (the
+        read arms, the write of the original value selects by RAM data and
+        re-arms, the final write does too).
+    In the RTS with S = $FC and the PLA with S = $FE, a phantom access (the
+    read of the return address, the stack read) decides the bank: the cart
+    runs differently when they are left out.
+    The subroutine mixes the bank-id byte and a bank-specific table byte into
+    RAM."""
+    rng = Rng(seed * 0x9E3779B1 + 0xFE)
+    a = Asm(0xF000)
+    a.org(0xF100)
+    _reset_code(a)
+    _frame_head(a, lines)
+    a.label("line")
+    a.ins("STA", "zp", WSYNC)
+    a.ins("LDX", "imm", 0xFF); a.ins("TXS")
+    for i, (via, stack) in enumerate((("bit0", 0xFF), ("bit1", 0xFE))):
+        a.ins("LDX", "imm", stack); a.ins("TXS")
+        a.ins("LDA", "zp", MIX); a.ins("ADC", "zp", LINE_CTR); a.ins("STA", "zp", MIX)
+        a.ins("AND", "imm", 1 if via == "bit0" else 2)
+        a.ins("BEQ", "rel", f"f_{via}")
+        a.ins("JSR", "abs", FE_SUB - 0x2000)                # $DA00: bank 1
+        # The opcode after each JSR has bit 5 opposite to the JSR's high byte:
+        # returning with S = $FC, the read of the return address ($DA / $FA)
+        # selects the bank, not this fetch.
+        a.ins("LDY", "imm", 0)                              # $A0
+        a.ins("JMP", "abs", f"after_{via}")
+        a.label(f"f_{via}")
+        a.ins("JSR", "abs", FE_SUB)                         # $FA00: bank 0
+        a.ins("CLC")                                        # $18
+        a.label(f"after_{via}")
+        a.ins("LDA", "abs", FE_BANKID); a.ins("ADC", "zp", 0x8A + i); a.ins("STA", "zp", 0x8A + i)
+    # PLA with S = $FE: its stack read at $01FE arms, the pull of $01FF
+    # (written from RAM just before) selects.
+    a.ins("LDA", "zp", MIX); a.ins("EOR", "zp", 0x84); a.ins("STA", "zp", 0xFF)
+    a.ins("LDX", "imm", 0xFE); a.ins("TXS"); a.ins("PLA")
+    a.ins("LDA", "abs", FE_BANKID); a.ins("ADC", "zp", 0x8C); a.ins("STA", "zp", 0x8C)
+    a.ins("LDX", "imm", 0xFE); a.ins("TXS")
+    a.ins("LDA", "zp", MIX); a.ins("PHA")                   # writes $01FE
+    a.ins("LDA", "abs", FE_BANKID); a.ins("ADC", "zp", 0x83); a.ins("STA", "zp", 0x83)
+    a.ins("PLA")                                            # pulls $01FE
+    a.ins("EOR", "abs", FE_BANKID); a.ins("STA", "zp", 0x86)
+    a.ins("LDA", "abs", 0x01FE); a.ins("ADC", "zp", 0x87); a.ins("STA", "zp", 0x87)
+    a.ins("LDX", "imm", 0x0E); a.ins("LDA", "absx", 0x01F0)
+    a.ins("LDA", "abs", FE_BANKID); a.ins("ADC", "zp", 0x88); a.ins("STA", "zp", 0x88)
+    a.ins("LDA", "zp", LINE_CTR); a.ins("AND", "imm", 3); a.ins("BNE", "rel", "noinc")
+    a.ins("INC", "abs", 0x01FE)
+    a.ins("LDA", "abs", FE_BANKID); a.ins("ADC", "zp", 0x89); a.ins("STA", "zp", 0x89)
+    a.label("noinc")
+    a.ins("LDX", "imm", 0xFF); a.ins("TXS")
+    _frame_tail(a)
+    a.org(FE_SUB)
+    a.ins("LDA", "abs", FE_BANKID); a.ins("ADC", "zp", 0x84); a.ins("STA", "zp", 0x84)
+    a.ins("LDX", "zp", MIX); a.ins("LDA", "absx", FE_TABLE); a.ins("EOR", "zp", 0x85); a.ins("STA", "zp", 0x85)
+    a.ins("RTS")
+    a.org(FE_TABLE)
+    a.org(0xFFFC)
+    a.raw(bytes([0x00, 0xF1, 0x00, 0xF1]))
+    img, labels, _ = a.assemble(4096)
+    assert labels["reset"] == 0xF100 and labels["noinc"] < FE_SUB
+    banks = []
+    for b in range(2):
+        bank = bytearray(img)
+        for i in range(256):
+            bank[FE_TABLE - 0xF000 + i] = rng.below(256)
+        bank[FE_BANKID - 0xF000] = 0xC0 + b
+        banks.append(bytes(bank))
+    rom = banks[0] + banks[1]
+    return Cart(CartSpec("fe_8k", 8192, seed, wsync_density=1.0), rom, labels, scheme="fe")
+
+
 DPC_BANKID = 0xFE80
 
 

@@ -196,10 +196,11 @@ void fa_power_on_column(const uint8_t* img, uint32_t nbanks, int scheme, uint32_
     if (fa_map_kind(hot_lo)) {
         // Sliced carts: E0 windows 4, 5, 6, 7 (the image's last 4K, as the
         // reference powers on in its last bank); 3F bank 0; DPC program bank
-        // 1 (the last), with its random number generator at 1.  The vector is
-        // in window 3 ($1C00-$1FFF), whose slice is byte 3.
+        // 1 (the last), with its random number generator at 1; FE bank 1, not
+        // armed.  The vector is in window 3 ($1C00-$1FFF), whose slice is
+        // byte 3.
         const uint32_t kind = fa_map_kind(hot_lo);
-        const uint32_t m = kind == FA_MAP_E0 ? (4u | 5u << 4 | 6u << 8) : kind == FA_MAP_DPC ? 1u : 0u;
+        const uint32_t m = kind == FA_MAP_E0 ? (4u | 5u << 4 | 6u << 8) : (kind == FA_MAP_DPC || kind == FA_MAP_FE) ? 1u : 0u;
         if (kind == FA_MAP_DPC) s.dpc_random = 1;
         const uint32_t vec = (fa_slices_from_mapper(hot_lo, m) >> 24) * 1024u + 0x3FCu;
         s.mapper[0] = (uint8_t)m;
@@ -246,7 +247,7 @@ static int auto_scheme(size_t len)
 static int scheme_len_ok(int scheme, size_t len)
 {
     switch (scheme) {
-    case FA_SCHEME_E0: return len == 8192;
+    case FA_SCHEME_E0: case FA_SCHEME_FE: return len == 8192;
     case FA_SCHEME_DPC: return dpc_len(len);
     case FA_SCHEME_3F: return len >= 2048 && len <= 32768 && len % 2048 == 0;
     case FA_SCHEME_FIXED: case FA_SCHEME_F8: case FA_SCHEME_F6: case FA_SCHEME_F4:
@@ -357,9 +358,11 @@ int fa_make_bank_image(const uint8_t* rom, size_t len, std::vector<uint8_t>& img
         hl = FA_MAP_DPC << 8;
         img.assign((size_t)nb * 4096, 0);
         memcpy(img.data(), rom, 10240);
-    } else if (scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_3F) {
+    } else if (scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_3F || scheme == FA_SCHEME_FE) {
         nb = (uint32_t)((len + 4095) / 4096);
-        hl = scheme == FA_SCHEME_E0 ? (FA_MAP_E0 << 8) : ((FA_MAP_3F << 8) | (uint32_t)(len / 2048));
+        hl = scheme == FA_SCHEME_E0   ? (FA_MAP_E0 << 8)
+           : scheme == FA_SCHEME_FE   ? (FA_MAP_FE << 8)
+                                      : ((FA_MAP_3F << 8) | (uint32_t)(len / 2048));
         img.assign((size_t)nb * 4096, 0);
         memcpy(img.data(), rom, len);
     } else {

@@ -853,12 +853,15 @@ static __device__ __noinline__ uint4 pia_sync_io(uint32_t tv_ps, uint32_t sel_uf
     return make_uint4(tv | (ps << 16), sel | (uf << 16), pia_span_of(tv, ps, sel, uf), 0u);
 }
 
-// SLICED: the core of E0 and 3F carts (and, with DPC, of DPC carts alone).
-// The DPC core is its own build so that the E0 / 3F core carries none of the
-// DPC register decode on its bus paths.
-template <int BLOCK, bool RENDER = false, bool SLICED = false, bool DPC = false>
+// SLICED: the core of E0 and 3F carts (with DPC, of DPC carts alone; with
+// FE, of FE carts alone).  The DPC and FE cores are their own builds so that
+// the E0 / 3F core carries none of their bus decode.  The FE core issues
+// every bus access the reference CPU makes, phantom ones included: any of
+// them can select an FE cart's bank.
+template <int BLOCK, bool RENDER = false, bool SLICED = false, bool DPC = false, bool FE = false>
 struct Emu {
     static_assert(!DPC || (SLICED && !RENDER), "the DPC core is a headless sliced core");
+    static_assert(!FE || (SLICED && !RENDER && !DPC), "the FE core is a headless sliced core");
     // ---- placement
     uint8_t* pv;             // this thread's RAM (shared memory, interleaved by thread)
     const FaGroup* G;        // the instance's group (HBM state rows, stride)
@@ -946,6 +949,17 @@ struct Emu {
                 sbump();
             }
         }
+    }
+    // FE core: the access after one to $01FE selects the 4K bank by bit 5 of
+    // its data (set: bank 0, clear: bank 1); bit 7 of `slices` marks that the
+    // last access was to $01FE.  v is the byte the access read or wrote.
+    __device__ __forceinline__ void fe_note(uint32_t a13, uint32_t v)
+    {
+        if (slices & 0x80u) {
+            slices = ((v & 0x20u) ? 0u : 0x04040404u) + 0x03020100u;
+            sbump();
+        }
+        if (a13 == 0x01FEu) slices |= 0x80u;
     }
     // DPC core: reads of $1000-$103F and writes of $1040-$107F reach the registers.
     __device__ __forceinline__ uint32_t dpc(uint32_t a13, uint32_t v, uint32_t wr)
@@ -1109,17 +1123,28 @@ struct Emu {
                     if (a < 0x1040u) return dpc(a, 0u, 0u);
                 }
                 e0_hot(a);
+                if constexpr (FE) {
+                    const uint32_t v = rom[srom(a)];
+                    fe_note(a, v);
+                    return v;
+                }
                 return rom[srom(a)];
             } else {
                 bsw(a);
                 return rom[((bank & 7u) << 12) | (a & 0xFFFu)];
             }
         }
+        if constexpr (FE) {
+            const uint32_t v = read_low(a, j);
+            fe_note(a, v);
+            return v;
+        }
         return read_low(a, j);
     }
     __device__ __forceinline__ void write(uint32_t addr, uint32_t v, uint32_t j)
     {
         uint32_t a = addr & 0x1FFFu;
+        if constexpr (FE) fe_note(a, v);
         if (a & 0x1000u) {
             if constexpr (SLICED) {
                 if constexpr (DPC) {
@@ -1134,9 +1159,14 @@ struct Emu {
         if ((a & 0x280u) == 0x080u) { stp(a & 0x7Fu, v); return; }
         io_write(a, v, j);
     }
-    // A phantom read: only its side effects (hotspot, INTIM) matter.
+    // A phantom read: only its side effects (hotspot, INTIM) matter; in the FE
+    // core its value too.
     __device__ __forceinline__ void dummy(uint32_t addr, uint32_t j)
     {
+        if constexpr (FE) {
+            (void)read(addr, j);
+            return;
+        }
         uint32_t a = addr & 0x1FFFu;
         if (a & 0x1000u) {
             if constexpr (SLICED) {
@@ -1152,15 +1182,31 @@ struct Emu {
             else pia_intim();
         }
     }
-    __device__ __forceinline__ uint32_t zp_read(uint32_t z, uint32_t j) { return (z & 0x80u) ? ldp(z & 0x7Fu) : io(z, j); }
+    __device__ __forceinline__ uint32_t zp_read(uint32_t z, uint32_t j)
+    {
+        if constexpr (FE) {
+            const uint32_t v = (z & 0x80u) ? ldp(z & 0x7Fu) : io(z, j);
+            fe_note(z, v);
+            return v;
+        }
+        return (z & 0x80u) ? ldp(z & 0x7Fu) : io(z, j);
+    }
     __device__ __forceinline__ void push(uint32_t v, uint32_t j)
     {
+        if constexpr (FE) fe_note(0x100u | sp, v);
         if (sp & 0x80u) stp(sp & 0x7Fu, v); else io_write(0x100u | sp, v, j);
         sp = (sp - 1u) & 0xFFu;
     }
     __device__ __forceinline__ uint32_t pull(uint32_t j)
     {
         sp = (sp + 1u) & 0xFFu;
+        if constexpr (FE) {
+            const uint32_t v = (sp & 0x80u) ? ldp(sp & 0x7Fu)
+                                            : io_read(0x100u | sp, pcnt, pins, pads, ports, su, (const uint8_t*)column(),
+                                                      G->stride * 4u);
+            fe_note(0x100u | sp, v);
+            return v;
+        }
         if (sp & 0x80u) return ldp(sp & 0x7Fu);
         if constexpr (RENDER) return io(0x100u | sp, j);
         else return io_read(0x100u | sp, pcnt, pins, pads, ports, su, (const uint8_t*)column(), G->stride * 4u);  // TIA
@@ -1170,7 +1216,9 @@ struct Emu {
     __device__ __forceinline__ void rmw_store(uint32_t ea, uint32_t oldv, uint32_t newv, uint32_t j)
     {
         uint32_t a = ea & 0x1FFFu;
-        if ((a & 0x1280u) == 0x080u) { stp(a & 0x7Fu, newv); return; }
+        if constexpr (!FE) {                                          // FE: the first write is an access too
+            if ((a & 0x1280u) == 0x080u) { stp(a & 0x7Fu, newv); return; }
+        }
 #pragma unroll 1
         for (uint32_t m = 0; m < 2u; m++) write(ea, m ? newv : oldv, j + m);
     }
@@ -1266,6 +1314,9 @@ struct Emu {
             // (zp,X): the pointer at zp b1 + X, read on cycles 3-4; (zp),Y: at
             // zp b1, on cycles 2-3.  One zero-page read loop for both.
             const uint32_t z = bbb == 0u ? (b1 + x) & 0xFFu : b1, j0 = bbb == 0u ? 3u : 2u;
+            if constexpr (FE) {
+                if (bbb == 0u) dummy(b1, 2);                        // the base, before X is added
+            }
             uint32_t ptr = 0;
 #pragma unroll 1
             for (uint32_t m = 0; m < 2u; m++) ptr |= zp_read((z + m) & 0xFFu, j0 + m) << (8u * m);
@@ -1276,7 +1327,10 @@ struct Emu {
         case 1: ea = b1; cyc = 3; break;                            // zp
         case 2: v = b1; cyc = 2; pc = (pc0 + 2u) & 0xFFFFu; goto operate;   // #imm ($89 is illegal)
         case 3: ea = (b2 << 8) | b1; cyc = 4; break;                // abs
-        case 5: ea = (b1 + x) & 0xFFu; cyc = 4; break;             // zp,X
+        case 5:                                                     // zp,X
+            ea = (b1 + x) & 0xFFu; cyc = 4;
+            if constexpr (FE) dummy(b1, 2);                         // the base, before X is added
+            break;
         default:                                                    // abs,Y / abs,X
             base = (b2 << 8) | b1;
             ea = (base + (bbb == 6u ? y : x)) & 0xFFFFu;
@@ -1326,7 +1380,9 @@ struct Emu {
         case 1: ea = b1; cyc = 3; pc = (pc0 + 2u) & 0xFFFFu; break; // zp
         case 3: ea = (b2 << 8) | b1; cyc = 4; pc = (pc0 + 3u) & 0xFFFFu; break;
         case 5:                                                     // zp,X (zp,Y for STX/LDX)
-            ea = (b1 + ((aaa == 4u || aaa == 5u) ? y : x)) & 0xFFu; cyc = 4; pc = (pc0 + 2u) & 0xFFFFu; break;
+            ea = (b1 + ((aaa == 4u || aaa == 5u) ? y : x)) & 0xFFu; cyc = 4; pc = (pc0 + 2u) & 0xFFFFu;
+            if constexpr (FE) dummy(b1, 2);                         // the base, before the index is added
+            break;
         default: {                                                  // abs,X (abs,Y for LDX)
             pc = (pc0 + 3u) & 0xFFFFu;
             const uint32_t base = (b2 << 8) | b1;
@@ -1389,6 +1445,7 @@ struct Emu {
             default: break;
             }
             if (aaa & 1u) {                                         // PLP, PLA
+                if constexpr (FE) dummy(0x100u | sp, 2);            // the stack, before the pull
                 const uint32_t v = pull(3);
                 if (aaa == 1u) p = v & ~(F_B | F_U);
                 else { a = v; nz(a); }
@@ -1404,6 +1461,9 @@ struct Emu {
                 // cycles 3-4, before it reads the high byte.
                 const uint32_t n = brk ? 3u : 2u, j0 = brk ? 2u : 3u;
                 const uint32_t w = brk ? (pc << 8) | p | F_B | F_U : pc;
+                if constexpr (FE) {
+                    if (!brk) dummy(0x100u | sp, 2);                // JSR reads the stack before its pushes
+                }
 #pragma unroll 1
                 for (uint32_t k = 0; k < n; k++) push((w >> (8u * (n - 1u - k))) & 0xFFu, j0 + k);
                 if (brk) p |= F_I;
@@ -1416,6 +1476,7 @@ struct Emu {
             if (aaa < 4u) {                                         // RTI (p, pcl, pch), RTS (pcl, pch)
                 const bool rti = aaa == 2u;
                 const uint32_t n = rti ? 3u : 2u;
+                if constexpr (FE) dummy(0x100u | sp, 2);                // the stack, before the pulls
                 uint32_t w = 0;
 #pragma unroll 1
                 for (uint32_t k = 0; k < n; k++) w |= pull(3u + k) << (8u * k);
@@ -1451,6 +1512,7 @@ struct Emu {
         case 5:                                                     // zp,X: STY LDY
             pc = (pc0 + 2u) & 0xFFFFu;
             ea = (b1 + x) & 0xFFu; cyc = 4;
+            if constexpr (FE) dummy(b1, 2);                         // the base, before X is added
             break;
         default: {                                                  // abs,X: LDY
             pc = (pc0 + 3u) & 0xFFFFu;
@@ -1493,6 +1555,7 @@ struct Emu {
         // in one window) and clear of every hotspot (and, DPC, of its read
         // registers at $1000-$103F), so reading them has no side effect.
         if (DPC      ? (a0 >= 0x1040u && (a0 & 0x3FFu) <= 0x3FDu && (a0 + 2u < 0x1FF8u || a0 > 0x1FF9u))
+            : FE     ? (a0 >= 0x1000u && (a0 & 0x3FFu) <= 0x3FDu && !(slices & 0x80u))     // not armed by $01FE
             : SLICED ? (a0 >= 0x1000u && (a0 & 0x3FFu) <= 0x3FDu && (a0 + 2u < 0x1FE0u || a0 > 0x1FF7u))
                      : (a0 >= 0x1000u && a0 + 2u < hot_lo)) {
             const uint8_t* q = SLICED ? rom + srom(a0) : rom + ((bank & 7u) << 12) + (a0 & 0xFFFu);

@@ -40,13 +40,13 @@ struct FaGroup {
 // The kernel build a set of groups needs (FA_MAPS_*).
 static inline int fa_maps_of(const FaGroup* g, uint32_t ngroups)
 {
-    bool sl = false, dpc = false, std4k = false;
+    bool sl = false, dpc = false, fe = false, std4k = false;
     for (uint32_t i = 0; i < ngroups; i++) {
         const uint32_t kind = fa_map_kind(g[i].hot_lo);
-        (kind == FA_MAP_DPC ? dpc : kind ? sl : std4k) = true;
+        (kind == FA_MAP_DPC ? dpc : kind == FA_MAP_FE ? fe : kind ? sl : std4k) = true;
     }
-    if ((int)sl + (int)dpc + (int)std4k > 1) return FA_MAPS_BOTH;
-    return dpc ? FA_MAPS_DPC : sl ? FA_MAPS_SLICED : FA_MAPS_4K;
+    if ((int)sl + (int)dpc + (int)fe + (int)std4k > 1) return FA_MAPS_BOTH;
+    return dpc ? FA_MAPS_DPC : fe ? FA_MAPS_FE : sl ? FA_MAPS_SLICED : FA_MAPS_4K;
 }
 
 struct FaLaunch {

@@ -192,6 +192,7 @@ static cudaError_t launch_block_m(int maps, const FaLaunch& L, bool persistent, 
     return maps == FA_MAPS_4K   ? launch_block<BLOCK, FA_MAPS_4K>(L, persistent, sms, s)
          : maps == FA_MAPS_BOTH ? launch_block<BLOCK, FA_MAPS_BOTH>(L, persistent, sms, s)
          : maps == FA_MAPS_DPC  ? launch_block<BLOCK, FA_MAPS_DPC>(L, persistent, sms, s)
+         : maps == FA_MAPS_FE   ? launch_block<BLOCK, FA_MAPS_FE>(L, persistent, sms, s)
                                 : launch_block<BLOCK, FA_MAPS_SLICED>(L, persistent, sms, s);
 }
 
@@ -314,7 +315,7 @@ static bool warp_layout(FaLaunch& L, int block, bool persistent, int* warps)
         // 24: at 32 warps its core is held to 64 registers and spills in the
         // interpreter loop (three E0/3F carts: 2.31 against 2.13 M frames/s).
         const int m = fa_maps_of(L.g, L.ngroups);
-        const int cap = L.cta_warps ? (int)L.cta_warps : (m == FA_MAPS_SLICED || m == FA_MAPS_DPC) ? 24 : 32;
+        const int cap = L.cta_warps ? (int)L.cta_warps : (m == FA_MAPS_4K || m == FA_MAPS_BOTH) ? 32 : 24;
         static const int sizes[] = { 32, 28, 24, 16, 8, 4, 2 };
         for (int x : sizes)
             if (x <= fit && x <= cap) { w = x; break; }
@@ -334,6 +335,7 @@ cudaError_t fa_launch_run(const FaLaunch& L_in, int block, bool persistent, int 
         return maps == FA_MAPS_4K   ? launch_warps_n<FA_MAPS_4K>(warps, L, persistent, sms, s)
              : maps == FA_MAPS_BOTH ? launch_warps_n<FA_MAPS_BOTH>(warps, L, persistent, sms, s)
              : maps == FA_MAPS_DPC  ? launch_warps_n<FA_MAPS_DPC>(warps, L, persistent, sms, s)
+             : maps == FA_MAPS_FE   ? launch_warps_n<FA_MAPS_FE>(warps, L, persistent, sms, s)
                                     : launch_warps_n<FA_MAPS_SLICED>(warps, L, persistent, sms, s);
     }
     // ROM library too large for shared memory: CTA-granular units that
@@ -361,6 +363,7 @@ bool fa_launch_warp_shape(const FaLaunch& L_in, int block, bool persistent, int 
         if (maps == FA_MAPS_4K) warps_shape<WW, FA_MAPS_4K>(L, persistent, sms, grid, per_sm);              \
         else if (maps == FA_MAPS_BOTH) warps_shape<WW, FA_MAPS_BOTH>(L, persistent, sms, grid, per_sm);     \
         else if (maps == FA_MAPS_DPC) warps_shape<WW, FA_MAPS_DPC>(L, persistent, sms, grid, per_sm);       \
+        else if (maps == FA_MAPS_FE) warps_shape<WW, FA_MAPS_FE>(L, persistent, sms, grid, per_sm);         \
         else warps_shape<WW, FA_MAPS_SLICED>(L, persistent, sms, grid, per_sm);                            \
         return true;
     switch (w) {

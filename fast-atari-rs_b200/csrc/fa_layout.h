@@ -91,14 +91,16 @@ static inline int fa_detect_scheme(size_t len)        // BankScheme::detect, src
 // path.  The bank state a caller sees is 16 bits (fa_state::mapper): E0 =
 // window 0 | window 1 << 4 | window 2 << 8; 3F = the 2K bank at $1000; DPC =
 // the 4K program bank (slices 4b..4b+3).  A DPC image holds the 8K of
-// program, then the 2K of display data at byte 8192.
-enum : uint32_t { FA_MAP_E0 = 1u, FA_MAP_3F = 2u, FA_MAP_DPC = 3u };
+// program, then the 2K of display data at byte 8192.  FE = the 4K bank |
+// 0x100 while the last bus access was to $01FE (bit 7 of `slices` on the
+// device, which the slice decode ignores).
+enum : uint32_t { FA_MAP_E0 = 1u, FA_MAP_3F = 2u, FA_MAP_DPC = 3u, FA_MAP_FE = 4u };
 
 FA_HD static inline uint32_t fa_map_kind(uint32_t hot_lo) { return hot_lo < 0x1000u ? hot_lo >> 8 : 0u; }
 
 // Kernel builds by the cores they hold (see run_unit): 4K-bank carts only,
-// several kinds, E0 / 3F carts only, DPC carts only.
-enum : int { FA_MAPS_4K = 0, FA_MAPS_BOTH = 1, FA_MAPS_SLICED = 2, FA_MAPS_DPC = 3 };
+// several kinds, E0 / 3F carts only, DPC carts only, FE carts only.
+enum : int { FA_MAPS_4K = 0, FA_MAPS_BOTH = 1, FA_MAPS_SLICED = 2, FA_MAPS_DPC = 3, FA_MAPS_FE = 4 };
 
 FA_HD static inline uint32_t fa_slices_from_mapper(uint32_t hot_lo, uint32_t m)
 {
@@ -109,6 +111,7 @@ FA_HD static inline uint32_t fa_slices_from_mapper(uint32_t hot_lo, uint32_t m)
         return (2u * b) | ((2u * b + 1u) << 8) | ((2u * l) << 16) | ((2u * l + 1u) << 24);
     }
     if (fa_map_kind(hot_lo) == FA_MAP_DPC) return (m & 1u) * 0x04040404u + 0x03020100u;
+    if (fa_map_kind(hot_lo) == FA_MAP_FE) return ((m & 1u) * 0x04040404u + 0x03020100u) | (((m >> 8) & 1u) << 7);
     return 0u;
 }
 
@@ -118,6 +121,7 @@ FA_HD static inline uint32_t fa_mapper_from_slices(uint32_t hot_lo, uint32_t sli
         return (slices & 7u) | (((slices >> 8) & 7u) << 4) | (((slices >> 16) & 7u) << 8);
     if (fa_map_kind(hot_lo) == FA_MAP_3F) return (slices & 0xFFu) >> 1;
     if (fa_map_kind(hot_lo) == FA_MAP_DPC) return (slices & 0xFFu) >> 2;
+    if (fa_map_kind(hot_lo) == FA_MAP_FE) return ((slices & 0x7Fu) >> 2) | (((slices >> 7) & 1u) << 8);
     return 0u;
 }
 

@@ -446,9 +446,9 @@ extern "C" int fa_render_create(const uint8_t* rom, size_t rom_len, size_t n, fa
     if (!r) return fa_fail(FA_ERR_CAPACITY, "out of host memory");
     int rc = fa_make_bank_image(rom, rom_len, r->image, r->scheme, &r->nbanks, &r->hot_lo);
     if (rc) { delete r; return rc; }
-    if (r->scheme == FA_SCHEME_DPC) {
+    if (r->scheme == FA_SCHEME_DPC || r->scheme == FA_SCHEME_FE) {
         delete r;
-        return fa_fail(FA_ERR_BAD_ROM, "DPC carts run on the headless console only");
+        return fa_fail(FA_ERR_BAD_ROM, "DPC and FE carts run on the headless console only");
     }
     cudaGetDevice(&r->device);
     r->n = n;

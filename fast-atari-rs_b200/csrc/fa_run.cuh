@@ -100,9 +100,9 @@ static __device__ bool stage_rom(uint8_t* dst, const uint8_t* src, uint32_t byte
 }
 
 // ------------------------------------------------------------------ per-unit runner
-template <int BLOCK, bool SLICED = false, bool DPC = false>
+template <int BLOCK, bool SLICED = false, bool DPC = false, bool FE = false>
 struct Runner {
-    Emu<BLOCK, false, SLICED, DPC> e;
+    Emu<BLOCK, false, SLICED, DPC, FE> e;
     uint32_t f, phase, fcyc;
     bool active;
 
@@ -272,12 +272,12 @@ __device__ __forceinline__ uint32_t run_lanes(RUNNER& r, uint32_t sched)
 
 // Run one work unit: instances [first, first + count) of group G, one per
 // thread; t is the thread's slot in a private-byte slab of BLOCK slots.
-template <int BLOCK, bool SLICED, bool DPC = false>
+template <int BLOCK, bool SLICED, bool DPC = false, bool FE = false>
 __device__ __forceinline__ void run_unit_as(const FaGroup& G, uint32_t first, uint32_t count, const uint8_t* rom_s,
                                             uint32_t* priv, uint32_t t, unsigned long long* instr_out,
                                             unsigned long long* rounds_out)
 {
-    Runner<BLOCK, SLICED, DPC> r;
+    Runner<BLOCK, SLICED, DPC, FE> r;
     r.f = 0;
     r.phase = 0;
     r.fcyc = 0;
@@ -327,12 +327,12 @@ __device__ __forceinline__ void run_unit_as(const FaGroup& G, uint32_t first, ui
     if (rounds_out && (t & 31u) == 0 && rounds) atomicAdd(rounds_out, 32ull * rounds);
 }
 
-// Kernels come in four builds, picked by the host from the carts of a
+// Kernels come in five builds, picked by the host from the carts of a
 // launch: FA_MAPS_4K (only the reference's schemes) holds the 4K-bank core
 // alone, FA_MAPS_SLICED (only E0 and 3F carts) the SLICED core alone,
-// FA_MAPS_DPC (only DPC carts) the DPC core alone, and FA_MAPS_BOTH runs
-// each unit on its cart's core (hot_lo below 0x1000: sliced, FA_MAP_DPC:
-// the DPC core).  A build's register budget is the largest of the cores it
+// FA_MAPS_DPC (only DPC carts) the DPC core alone, FA_MAPS_FE (only FE
+// carts) the FE core alone, and FA_MAPS_BOTH runs each unit on its cart's
+// core (hot_lo below 0x1000: sliced; FA_MAP_DPC / FA_MAP_FE: those cores).  A build's register budget is the largest of the cores it
 // holds, so the single-core builds keep their own.
 template <int BLOCK, int MAPS>
 __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint32_t count, const uint8_t* rom_s,
@@ -345,9 +345,13 @@ __device__ __forceinline__ void run_unit(const FaGroup& G, uint32_t first, uint3
         run_unit_as<BLOCK, true>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
     } else if constexpr (MAPS == FA_MAPS_DPC) {
         run_unit_as<BLOCK, true, true>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
+    } else if constexpr (MAPS == FA_MAPS_FE) {
+        run_unit_as<BLOCK, true, false, true>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
     } else {
         const uint32_t kind = fa_map_kind(G.hot_lo);
         if (kind == FA_MAP_DPC) run_unit_as<BLOCK, true, true>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
+        else if (kind == FA_MAP_FE)
+            run_unit_as<BLOCK, true, false, true>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
         else if (kind) run_unit_as<BLOCK, true>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
         else run_unit_as<BLOCK, false>(G, first, count, rom_s, priv, t, instr_out, rounds_out);
     }

@@ -135,12 +135,15 @@ cudaError_t fa_launch_serve(const FaServeLaunch& L, int block, cudaStream_t s)
     switch (block) {
     case 128:
         return kind == FA_MAP_DPC ? launch_serve<4, FA_MAPS_DPC>(L, s)
+             : kind == FA_MAP_FE  ? launch_serve<4, FA_MAPS_FE>(L, s)
              : kind               ? launch_serve<4, FA_MAPS_SLICED>(L, s) : launch_serve<4, FA_MAPS_4K>(L, s);
     case 256:
         return kind == FA_MAP_DPC ? launch_serve<8, FA_MAPS_DPC>(L, s)
+             : kind == FA_MAP_FE  ? launch_serve<8, FA_MAPS_FE>(L, s)
              : kind               ? launch_serve<8, FA_MAPS_SLICED>(L, s) : launch_serve<8, FA_MAPS_4K>(L, s);
     case 512:
         return kind == FA_MAP_DPC ? launch_serve<16, FA_MAPS_DPC>(L, s)
+             : kind == FA_MAP_FE  ? launch_serve<16, FA_MAPS_FE>(L, s)
              : kind               ? launch_serve<16, FA_MAPS_SLICED>(L, s) : launch_serve<16, FA_MAPS_4K>(L, s);
     default: return cudaErrorInvalidValue;
     }

@@ -74,6 +74,12 @@ extern "C" {
                                bytes (program + display data) or 10495 (with the 255
                                bytes that dumps of the cart carry after them, ignored),
                                lengths the reference cannot construct. */
+#define FA_SCHEME_FE    7   /* Activision FE, 8K: two 4K banks at $1000-$1FFF.  Every
+                               bus access (phantom ones included) to $01FE arms the
+                               cart; the next access then selects the bank by bit 5
+                               of its data (set: bank 0, clear: bank 1), as JSR and
+                               RTS with the stack at $01FE/$01FF do on these carts.
+                               Power-on bank: 1.  Registered per ROM, like E0. */
 #define FA_SCHEME_AUTO  (-1)
 
 #define FA_RAM_BYTES 128
@@ -114,9 +120,10 @@ typedef struct fa_state {
     uint8_t  bank, scheme;
     uint8_t  _pad_end[2];
     /* ---- extension beyond the reference layout ---- */
-    /* E0, 3F and DPC bank state, 16 bits little-endian: E0 = slice of window
-     * 0 | window 1 << 4 | window 2 << 8; 3F = the 2K bank at $1000; DPC = the
-     * 4K program bank.  0 for the reference's schemes, whose bank is `bank`. */
+    /* E0, 3F, DPC and FE bank state, 16 bits little-endian: E0 = slice of
+     * window 0 | window 1 << 4 | window 2 << 8; 3F = the 2K bank at $1000; DPC
+     * = the 4K program bank; FE = the 4K bank | 0x100 while the last access
+     * was to $01FE.  0 for the reference's schemes, whose bank is `bank`. */
     uint8_t  mapper[2];
     uint8_t  _pad_ext;
     uint64_t cycles;      /* Cpu::cycles: executed instruction cycles, never reset */
@@ -191,8 +198,8 @@ uint64_t fa_wait_limit_ns_get(void);
  * entry point that is later given the same bytes (fa_create, fa_pool_add_cart,
  * fa_server_create, fa_render_create, fa_autotune) uses it instead of the
  * size rule.  FA_SCHEME_AUTO removes the record.  The length must suit the
- * scheme: E0 exactly 8192; 3F a multiple of 2048 up to 32768; DPC 10240 or
- * 10495; the reference's
+ * scheme: E0 and FE exactly 8192; 3F a multiple of 2048 up to 32768; DPC
+ * 10240 or 10495; the reference's
  * schemes the lengths fa_create accepts for them.  FA_ERR_BAD_ROM otherwise.
  */
 int fa_rom_set_scheme(const uint8_t* rom, size_t rom_len, int scheme);
@@ -602,7 +609,7 @@ int fa_server_loadgen(fa_server* s, const fa_loadgen_config* cfg, fa_loadgen_res
 #define FA_FB_HEIGHT 192
 typedef struct fa_render fa_render;
 /* n rendering consoles of one ROM on the current device (lengths as fa_create;
- * DPC carts, FA_ERR_BAD_ROM: they run on the headless console only). */
+ * DPC and FE carts, FA_ERR_BAD_ROM: they run on the headless console only). */
 int  fa_render_create(const uint8_t* rom, size_t rom_len, size_t n, fa_render** out);
 void fa_render_destroy(fa_render* r);
 size_t fa_render_num_envs(const fa_render* r);
@@ -645,7 +652,7 @@ uint32_t fa_palette_rgba(uint8_t index);
  * allocates nothing.
  *   d_rom_image  nbanks * 4096 bytes, 16-byte aligned (Fixed carts as their
  *                mirrored 4 KiB window, banked carts as-is)
- *   scheme       FA_SCHEME_FIXED, _F8, _F6 or _F4 (E0, 3F and DPC are not taken here)
+ *   scheme       FA_SCHEME_FIXED, _F8, _F6 or _F4 (E0, 3F, DPC and FE are not taken here)
  *   d_state      the FA SoA state rows (fa_device_state layout), stride >= n,
  *                of instances created for the same scheme (rows of another
  *                scheme keep bank numbers this one does not have, and step

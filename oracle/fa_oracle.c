@@ -434,6 +434,7 @@ struct orc_atari {
     int      scheme;
     int      slice[4];            /* E0 / 3F / DPC: the 1K ROM slice in each 1K window of $1000-$1FFF */
     orc_dpc  dpc;                 /* DPC registers (FA_SCHEME_DPC) */
+    int      fe_pend;             /* FE: the last bus access was to $01FE */
     uint32_t frame_no;
     uint32_t run_status;
     uint64_t instructions;
@@ -479,7 +480,7 @@ static int orc_dpc_len(size_t len) { return len == 10240 || len == 10495; }
 
 static int orc_scheme_len_ok(int scheme, size_t len)
 {
-    if (scheme == FA_SCHEME_E0) return len == 8192;
+    if (scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_FE) return len == 8192;
     if (scheme == FA_SCHEME_DPC) return orc_dpc_len(len);
     if (scheme == FA_SCHEME_3F) return len >= 2048 && len <= 32768 && len % 2048 == 0;
     return orc_rom_len_ok(len) && orc_detect(len) == scheme;
@@ -513,13 +514,19 @@ static int orc_scheme_for(const uint8_t* rom, size_t len)
     return orc_rom_len_ok(len) ? orc_detect(len) : -1;
 }
 
-static int orc_sliced(int scheme) { return scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_3F || scheme == FA_SCHEME_DPC; }
+static int orc_sliced(int scheme)
+{
+    return scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_3F || scheme == FA_SCHEME_DPC || scheme == FA_SCHEME_FE;
+}
 
 /* Power-on windows of the sliced schemes: E0 slices 4, 5, 6, 7; 3F 2K bank 0
  * under the last 2K. */
 static void orc_power_on_slices(int scheme, size_t len, int* slice)
 {
-    if (scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_DPC) { slice[0] = 4; slice[1] = 5; slice[2] = 6; slice[3] = 7; return; }
+    if (scheme == FA_SCHEME_E0 || scheme == FA_SCHEME_DPC || scheme == FA_SCHEME_FE) {
+        slice[0] = 4; slice[1] = 5; slice[2] = 6; slice[3] = 7;
+        return;
+    }
     const int l = (int)(len / 2048) - 1;
     slice[0] = 0; slice[1] = 1; slice[2] = 2 * l; slice[3] = 2 * l + 1;
 }
@@ -528,7 +535,7 @@ static unsigned orc_mapper_of(int scheme, const int* slice)
 {
     if (scheme == FA_SCHEME_E0) return (unsigned)(slice[0] | slice[1] << 4 | slice[2] << 8);
     if (scheme == FA_SCHEME_3F) return (unsigned)(slice[0] / 2);
-    if (scheme == FA_SCHEME_DPC) return (unsigned)(slice[0] / 4);
+    if (scheme == FA_SCHEME_DPC || scheme == FA_SCHEME_FE) return (unsigned)(slice[0] / 4);
     return 0;
 }
 
@@ -537,7 +544,7 @@ static void orc_slices_of(int scheme, size_t len, unsigned m, int* slice)
     orc_power_on_slices(scheme, len, slice);
     if (scheme == FA_SCHEME_E0) { slice[0] = m & 7; slice[1] = (m >> 4) & 7; slice[2] = (m >> 8) & 7; }
     else if (scheme == FA_SCHEME_3F) { const int b = (int)((m & 0xFF) % (len / 2048)); slice[0] = 2 * b; slice[1] = 2 * b + 1; }
-    else if (scheme == FA_SCHEME_DPC) for (int w = 0; w < 4; w++) slice[w] = 4 * (int)(m & 1) + w;
+    else if (scheme == FA_SCHEME_DPC || scheme == FA_SCHEME_FE) for (int w = 0; w < 4; w++) slice[w] = 4 * (int)(m & 1) + w;
 }
 
 static void orc_load_window(orc_atari* e, int w)
@@ -681,7 +688,33 @@ static void orc_dpc_write(orc_atari* e, uint16_t a, uint8_t v)
     }
 }
 
-static inline uint8_t orc_bus_read(orc_atari* e, uint16_t addr)   /* atari.rs:497-520 */
+/* FE (Activision): an access after one to $01FE selects the 4K bank by bit 5
+ * of its data (set: bank 0, clear: bank 1); the access itself is served from
+ * the mapping before the switch.  The reference has no FE cart: this is the
+ * published behaviour of these carts, for every access the reference CPU
+ * makes (phantom ones included). */
+static inline void orc_fe_note(orc_atari* e, uint16_t a13, uint8_t v)
+{
+    if (e->fe_pend) {
+        const int b = (v & 0x20) ? 0 : 1;
+        for (int w = 0; w < 4; w++) {
+            e->slice[w] = 4 * b + w;
+            orc_load_window(e, w);
+        }
+    }
+    e->fe_pend = a13 == 0x01FE;
+}
+
+static inline uint8_t orc_bus_read_value(orc_atari* e, uint16_t addr);
+
+static inline uint8_t orc_bus_read(orc_atari* e, uint16_t addr)
+{
+    const uint8_t v = orc_bus_read_value(e, addr);
+    if (e->scheme == FA_SCHEME_FE) orc_fe_note(e, (uint16_t)(addr & 0x1FFF), v);
+    return v;
+}
+
+static inline uint8_t orc_bus_read_value(orc_atari* e, uint16_t addr) /* atari.rs:497-520 */
 {
     uint16_t a = addr & 0x1FFF;
     if (e->scheme == FA_SCHEME_DPC && (a & 0x1FC0) == 0x1000) return orc_dpc_read(e, a);
@@ -697,6 +730,7 @@ static inline uint8_t orc_bus_read(orc_atari* e, uint16_t addr)   /* atari.rs:49
 static inline void orc_bus_write(orc_atari* e, uint16_t addr, uint8_t v) /* atari.rs:523-552 */
 {
     uint16_t a = addr & 0x1FFF;
+    if (e->scheme == FA_SCHEME_FE) orc_fe_note(e, a, v);
     if (a & 0x1000) {
         if (e->scheme == FA_SCHEME_DPC && (a & 0x1FC0) == 0x1040) orc_dpc_write(e, a, v);
         if (e->scheme != FA_SCHEME_FIXED) orc_check_bankswitch(e, addr);
@@ -783,7 +817,7 @@ orc_atari* orc_create(const uint8_t* rom, size_t rom_len)          /* atari.rs:4
     case FA_SCHEME_FIXED: e->bank = 0; break;
     case FA_SCHEME_F8: e->bank = 1; break;
     case FA_SCHEME_F6: e->bank = 3; break;
-    case FA_SCHEME_E0: case FA_SCHEME_3F: case FA_SCHEME_DPC:
+    case FA_SCHEME_E0: case FA_SCHEME_3F: case FA_SCHEME_DPC: case FA_SCHEME_FE:
         e->bank = 0;
         orc_power_on_slices(scheme, rom_len, e->slice);
         break;
@@ -909,7 +943,7 @@ void orc_get_state(const orc_atari* e, fa_state* s)                /* cuda_env.r
     s->ctrlpf = t->ctrlpf; s->refp0 = t->refp0; s->refp1 = t->refp1;
     s->pf0 = t->pf0; s->pf1 = t->pf1; s->pf2 = t->pf2;
     s->bank = (uint8_t)e->bank; s->scheme = (uint8_t)e->scheme;
-    const unsigned m = orc_mapper_of(e->scheme, e->slice);
+    const unsigned m = orc_mapper_of(e->scheme, e->slice) | (e->scheme == FA_SCHEME_FE && e->fe_pend ? 0x100u : 0u);
     s->mapper[0] = (uint8_t)m; s->mapper[1] = (uint8_t)(m >> 8);
     s->cycles = e->cpu.cycles;
     s->frame_no = e->frame_no;
@@ -968,6 +1002,7 @@ void orc_set_state(orc_atari* e, const fa_state* s)
     e->bank = nb;
     if (orc_sliced(e->scheme))
         orc_slices_of(e->scheme, e->rom_len, (unsigned)s->mapper[0] | ((unsigned)s->mapper[1] << 8), e->slice);
+    e->fe_pend = e->scheme == FA_SCHEME_FE && (s->mapper[1] & 1);
     orc_load_bank(e, nb);
     orc_sync_ram_to_mem(e);
 }
@@ -1497,7 +1532,7 @@ static void orc_rbus_write(orc_ratari* e, uint16_t addr, uint8_t v) /* atari.rs:
 orc_ratari* orc_rcreate(const uint8_t* rom, size_t rom_len)        /* atari.rs:120-136, 240-247 */
 {
     const int scheme = orc_scheme_for(rom, rom_len);
-    if (scheme < 0 || scheme == FA_SCHEME_DPC) return NULL;        /* DPC carts run headless only */
+    if (scheme < 0 || scheme == FA_SCHEME_DPC || scheme == FA_SCHEME_FE) return NULL;   /* headless only */
     orc_ratari* e = (orc_ratari*)calloc(1, sizeof(orc_ratari));
     if (!e) return NULL;
     e->rom = (uint8_t*)malloc(rom_len);

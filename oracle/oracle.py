@@ -284,7 +284,7 @@ def render_steps(consoles, actions: np.ndarray, nthreads: int | None = None, out
     return (np.stack([c.framebuffer() for c in consoles]), np.stack([c.ram() for c in consoles]))
 
 
-SCHEMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "dpc": 6, "auto": -1}
+SCHEMES = {"fixed": 0, "f8": 1, "f6": 2, "f4": 3, "e0": 4, "3f": 5, "dpc": 6, "fe": 7, "auto": -1}
 
 
 def set_rom_scheme(rom: bytes, scheme) -> None:

@@ -34,6 +34,8 @@ CASES = {
     "3f_6k": (lambda: carts.f3_cart(6144), 16, 30, 110),
     # DPC, picked by its length.
     "dpc_10k": (carts.dpc_cart, 16, 30, 111),
+    # FE, registered per ROM.
+    "fe_8k": (carts.fe_cart, 16, 30, 112),
 }
 CHECKPOINTS = (1, 10, 30)
 

@@ -8,11 +8,11 @@
 #include "../../fast-atari-rs_b200/csrc/fa_run.cuh"
 #include "../../fast-atari-rs_b200/csrc/fa_render.cuh"
 
-template <bool SL, bool DPC = false>
+template <bool SL, bool DPC = false, bool FE = false>
 static void run_one(const FaGroup& G, uint32_t i, uint8_t* rom, unsigned long long* instr)
 {
     uint32_t priv[FA_SMEM_WORDS];
-    fa::Runner<1, SL, DPC> r;
+    fa::Runner<1, SL, DPC, FE> r;
     r.f = 0; r.phase = 0; r.fcyc = 0; r.active = false;
     r.e.pv = (uint8_t*)priv;
     r.e.G = &G; r.e.i = i; r.e.rom = rom; r.e.hot_lo = G.hot_lo; r.e.nbanks = G.nbanks;
@@ -47,6 +47,7 @@ extern "C" long long hs_run(const uint8_t* rom, size_t len, fa_state* st, size_t
     unsigned long long instr = 0;
     for (uint32_t i = 0; i < n; i++) {
         if (fa_map_kind(hot_lo) == FA_MAP_DPC) run_one<true, true>(G, i, simg.data(), &instr);   // as run_unit
+        else if (fa_map_kind(hot_lo) == FA_MAP_FE) run_one<true, false, true>(G, i, simg.data(), &instr);
         else if (fa_map_kind(hot_lo)) run_one<true>(G, i, simg.data(), &instr);
         else run_one<false>(G, i, simg.data(), &instr);
     }

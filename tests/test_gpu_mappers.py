@@ -27,7 +27,8 @@ def need_gpu():
 
 @pytest.fixture(scope="module")
 def sliced():
-    out = {"e0": (carts.e0_cart(), "e0"), "3f16": (carts.f3_cart(16384), "3f"), "3f6": (carts.f3_cart(6144), "3f")}
+    out = {"e0": (carts.e0_cart(), "e0"), "3f16": (carts.f3_cart(16384), "3f"), "3f6": (carts.f3_cart(6144), "3f"),
+           "fe": (carts.fe_cart(), "fe")}
     for c, sch in out.values():
         fa.set_rom_scheme(c.rom, sch)
         oracle.set_rom_scheme(c.rom, sch)
@@ -42,7 +43,7 @@ def dpc():
     return {"dpc": carts.dpc_cart(), "dpc_tail": carts.dpc_cart(dump_tail=True)}
 
 
-@pytest.mark.parametrize("name", ["e0", "3f16", "3f6", "dpc", "dpc_tail"])
+@pytest.mark.parametrize("name", ["e0", "3f16", "3f6", "dpc", "dpc_tail", "fe"])
 @pytest.mark.parametrize("sched", ["pc", "lane", "line", "match"])
 def test_sliced_carts_match_oracle(sliced, dpc, name, sched):
     rom = (dpc[name] if name.startswith("dpc") else sliced[name]).rom
@@ -60,7 +61,7 @@ def test_sliced_carts_match_oracle(sliced, dpc, name, sched):
             assert np.array_equal(obs, o_obs), f"{name}/{sched} frames {f0}..{f0 + chunk}"
             assert_states_equal(g.download_states(), ref, f"{name}/{sched} after {f0 + chunk}")
     maps = {int(m[0]) | int(m[1]) << 8 for m in ref["mapper"]}
-    assert int(ref["scheme"][0]) in (4, 5, 6)
+    assert int(ref["scheme"][0]) in (4, 5, 6, 7)
     assert len(maps) >= 1
     if name.startswith("dpc"):                              # the cart reaches every DPC mechanism
         assert len(maps) == 2 and ref["dpc_music"].any() and (ref["dpc_music"] == 0).any()
@@ -86,8 +87,8 @@ def test_sliced_launch_shapes_and_per_frame(sliced, block, persistent):
 def test_pool_mixes_sliced_and_4k_bank_carts(sliced, dpc):
     mixed = carts.mixed_carts()
     roms = [mixed[0].rom, sliced["e0"].rom, mixed[2].rom, sliced["3f16"].rom, sliced["3f6"].rom, mixed[3].rom,
-            dpc["dpc"].rom]
-    counts = [300, 200, 90, 130, 64, 33, 77]
+            dpc["dpc"].rom, sliced["fe"].rom]
+    counts = [300, 200, 90, 130, 64, 33, 77, 45]
     k = 5
     acts = [carts.actions(seed=50 + i, n=n, frames=k) for i, n in enumerate(counts)]
     with fa.AtariPool() as pool:
@@ -182,9 +183,32 @@ def test_dpc_fields_not_taken_by_other_schemes():
         assert_states_equal(g.download_states(), ref, "run on")
 
 
-def test_rendering_console_refuses_dpc(dpc):
+def test_fe_state_upload_round_trip(sliced):
+    """FE bank state set by hand, armed (the last access was to $01FE) or
+    not, goes up and comes back unchanged, and running on matches the oracle
+    started from the same states: an armed console's first opcode fetch picks
+    its bank."""
+    rom = sliced["fe"].rom
+    n = 64
+    ref = oracle_states(rom, n)
+    oracle.run_batch(rom, ref, carts.actions(seed=11, n=n, frames=2), 2)
+    ref["mapper"][:, 0] = np.arange(n) % 2
+    ref["mapper"][:, 1] = (np.arange(n) // 2) % 2
+    with fa.BatchAtariGpu(rom, n) as g:
+        g.upload_states(ref)
+        assert_states_equal(g.download_states(), ref, "round trip")
+        acts = carts.actions(seed=12, n=n, frames=3)
+        obs = g.step_multi(acts, 3)
+        o_obs, _ = oracle.run_batch(rom, ref, acts, 3)
+        assert np.array_equal(obs, o_obs)
+        assert_states_equal(g.download_states(), ref, "continued")
+
+
+@pytest.mark.parametrize("name", ["dpc", "fe"])
+def test_rendering_console_refuses_dpc_and_fe(sliced, dpc, name):
+    rom = dpc["dpc"].rom if name == "dpc" else sliced["fe"].rom
     with pytest.raises(fa.FaError) as ei:
-        fa.AtariRender(dpc["dpc"].rom, 4)
+        fa.AtariRender(rom, 4)
     assert ei.value.code == fa.FA_ERR_BAD_ROM
 
 
@@ -221,7 +245,7 @@ def test_sliced_carts_in_the_server(sliced, dpc):
         assert_states_equal(states[c], ref[c], f"cart {c}")
 
 
-@pytest.mark.parametrize("name", ["e0_8k", "3f_16k", "3f_6k", "dpc_10k"])
+@pytest.mark.parametrize("name", ["e0_8k", "3f_16k", "3f_6k", "dpc_10k", "fe_8k"])
 def test_sliced_carts_match_committed_golden_vectors(sliced, dpc, name):
     """The frozen oracle vectors of tests/golden/ (RAM at checkpoint frames and
     the full final state, mapper field included), without running the oracle."""
@@ -230,7 +254,8 @@ def test_sliced_carts_match_committed_golden_vectors(sliced, dpc, name):
     from pathlib import Path
     from make_golden import state_sha
     want = json.loads((Path(__file__).parent / "golden" / "oracle_vectors.json").read_text())[name]
-    rom = {"e0_8k": sliced["e0"], "3f_16k": sliced["3f16"], "3f_6k": sliced["3f6"], "dpc_10k": dpc["dpc"]}[name].rom
+    rom = {"e0_8k": sliced["e0"], "3f_16k": sliced["3f16"], "3f_6k": sliced["3f6"], "dpc_10k": dpc["dpc"],
+           "fe_8k": sliced["fe"]}[name].rom
     assert hashlib.sha256(rom).hexdigest() == want["rom_sha256"]
     n, frames = want["n"], want["frames"]
     acts = carts.actions(seed=want["action_seed"], n=n, frames=frames)

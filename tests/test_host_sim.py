@@ -80,13 +80,13 @@ def test_device_core_matches_oracle_on_carts(sim, c):
     assert_same(got, ref, c.spec.name)
 
 
-@pytest.mark.parametrize("name", ["e0", "3f16", "3f6", "dpc", "dpc_tail", "dpc_script"])
+@pytest.mark.parametrize("name", ["e0", "3f16", "3f6", "dpc", "dpc_tail", "dpc_script", "fe"])
 def test_device_core_matches_oracle_on_sliced_carts(sim, name):
-    """E0 and 3F registered per ROM; DPC picked by its lengths (10,240 and
-    10,495 bytes) on both sides."""
+    """E0, 3F and FE registered per ROM; DPC picked by its lengths (10,240
+    and 10,495 bytes) on both sides."""
     c, code = {"e0": (carts.e0_cart(), 4), "3f16": (carts.f3_cart(16384), 5), "3f6": (carts.f3_cart(6144), 5),
                "dpc": (carts.dpc_cart(), -1), "dpc_tail": (carts.dpc_cart(dump_tail=True), -1),
-               "dpc_script": (carts.dpc_script_cart(), -1)}[name]
+               "dpc_script": (carts.dpc_script_cart(), -1), "fe": (carts.fe_cart(), 7)}[name]
     r = np.frombuffer(c.rom, np.uint8).copy()
     sim.fa_rom_set_scheme(r.ctypes.data, len(r), code)
     oracle.set_rom_scheme(c.rom, code)
@@ -127,6 +127,51 @@ def test_device_core_on_random_roms_and_states(sim, size):
         st["run_status"] = 0
         got, ref = run_both(sim, rom, st, carts.actions(seed=t, n=n, frames=3), 3)
         assert_same(got, ref, f"random {size}-byte ROM {t}")
+
+
+@pytest.mark.parametrize("scheme,code", [("fe", 7), ("dpc", 6)])
+def test_extra_cores_on_random_roms_and_states(sim, scheme, code):
+    """The FE and DPC cores on random images from random CPU states and RAM,
+    some started armed (FE) or with random DPC registers: random stack
+    pointers put JSR, RTS, RTI, PHA, PLA, BRK and indexed or indirect
+    accesses on $01FE, and every phantom access the reference CPU makes
+    (zero-page bases, stack reads, old-value writes, fix-ups) must reach the
+    FE decode in the oracle's order; random reads and writes hit the DPC
+    registers in every function."""
+    rng = np.random.default_rng(code)
+    size = 8192 if scheme == "fe" else 10240
+    for t in range(8):
+        rom = bytearray(rng.integers(0, 256, size, dtype=np.uint8).tobytes())
+        for b in range(2):
+            rom[b * 4096 + 4092:b * 4096 + 4094] = bytes([0x00, 0xF0])
+        rom = bytes(rom)
+        r = np.frombuffer(rom, np.uint8).copy()
+        if scheme == "fe":
+            sim.fa_rom_set_scheme(r.ctypes.data, len(r), code)
+            oracle.set_rom_scheme(rom, code)
+        try:
+            n = 96
+            st = np.array([oracle.reset_state(rom)] * n, dtype=oracle.STATE_DTYPE)
+            st["a"], st["x"], st["y"] = rng.integers(0, 256, n), rng.integers(0, 256, n), rng.integers(0, 256, n)
+            st["sp"], st["status"] = rng.integers(0xF8, 0x100, n), rng.integers(0, 256, n) & 0xCF
+            st["pc"] = 0xF000 + rng.integers(0, 0x1000, n)
+            st["ram"] = rng.integers(0, 256, (n, 128))
+            st["mapper"][:, 0] = rng.integers(0, 2, n)
+            st["mapper"][:, 1] = rng.integers(0, 2, n) if scheme == "fe" else 0
+            if scheme == "dpc":
+                st["dpc_counter"] = rng.integers(0, 2048, (n, 8))
+                st["dpc_top"] = rng.integers(0, 256, (n, 8))
+                st["dpc_bottom"] = rng.integers(0, 256, (n, 8))
+                st["dpc_flags"] = rng.integers(0, 256, n)
+                st["dpc_music"] = rng.integers(0, 8, n)
+                st["dpc_random"] = rng.integers(0, 256, n)
+            st["run_status"] = 0
+            got, ref = run_both(sim, rom, st, carts.actions(seed=t, n=n, frames=3), 3)
+            assert_same(got, ref, f"random {scheme} image {t}")
+        finally:
+            if scheme == "fe":
+                sim.fa_rom_set_scheme(r.ctypes.data, len(r), -1)
+                oracle.set_rom_scheme(rom, "auto")
 
 
 def test_device_core_every_opcode_first(sim):

@@ -353,3 +353,66 @@ def test_oracle_ignores_dpc_fields_of_other_schemes():
     oracle.run_batch(rom, a, acts, 3)
     oracle.run_batch(rom, b, acts, 3)
     assert a.tobytes() == b.tobytes()
+
+
+# ------------------------------------------------------------------ FE
+def test_oracle_fe_bank_follows_the_access_after_01fe():
+    """An 8K FE image whose two banks hold the same code and differ only in a
+    marker byte at $1E80 ($B0 in bank 0, $B1 in bank 1).  Each step's
+    expected bank is worked out from the access order of the reference CPU
+    (src/cpu.rs): power-on bank 1; JSR $FA00 / $DA00 with S = $FF (the low
+    return byte is pushed to $01FE, the target's high byte selects: $FA has
+    bit 5 set, bank 0; $DA clear, bank 1) and RTS with S = $FD (the high
+    return byte $F1 selects bank 0); LDA $01FE then CLC (the opcode $18
+    selects bank 1); PLA with S = $FE (its stack read arms, the pulled byte
+    selects: $20 bank 0, $00 bank 1)."""
+    a = carts.Asm(0xF000)
+    a.org(0xF100)
+    a.label("reset")
+    a.ins("LDX", "imm", 0xFF); a.ins("TXS")
+    a.ins("LDA", "abs", 0xFE80); a.ins("STA", "zp", 0x80)          # bank 1 (power-on)
+    a.ins("JSR", "abs", 0xFA00); a.ins("STA", "zp", 0x81)          # sub ran in bank 0
+    a.ins("LDA", "abs", 0xFE80); a.ins("STA", "zp", 0x82)          # back in bank 0
+    a.ins("JSR", "abs", 0xDA00); a.ins("STA", "zp", 0x83)          # sub ran in bank 1
+    a.ins("LDA", "abs", 0xFE80); a.ins("STA", "zp", 0x84)          # RTS: $F1 -> bank 0
+    a.ins("LDA", "abs", 0x01FE); a.ins("CLC")                      # $18 -> bank 1
+    a.ins("LDA", "abs", 0xFE80); a.ins("STA", "zp", 0x85)
+    a.ins("LDA", "imm", 0x20); a.ins("STA", "zp", 0xFF)
+    a.ins("LDX", "imm", 0xFE); a.ins("TXS"); a.ins("PLA")          # pulls $20 -> bank 0
+    a.ins("LDA", "abs", 0xFE80); a.ins("STA", "zp", 0x86)
+    a.ins("LDA", "imm", 0x00); a.ins("STA", "zp", 0xFF)
+    a.ins("LDX", "imm", 0xFE); a.ins("TXS"); a.ins("PLA")          # pulls $00 -> bank 1
+    a.ins("LDA", "abs", 0xFE80); a.ins("STA", "zp", 0x87)
+    a.ins("LDX", "imm", 0xFF); a.ins("TXS")
+    a.label("spin")
+    a.ins("LDA", "imm", 0x02); a.ins("STA", "zp", carts.VSYNC)
+    a.ins("JMP", "abs", "spin")
+    a.org(0xFA00)
+    a.ins("LDA", "abs", 0xFE80); a.ins("RTS")
+    a.org(0xFFFC)
+    a.raw(bytes([0x00, 0xF1, 0x00, 0xF1]))
+    img, _, _ = a.assemble(4096)
+    banks = [bytearray(img), bytearray(img)]
+    banks[0][0xE80], banks[1][0xE80] = 0xB0, 0xB1
+    rom = bytes(banks[0] + banks[1])
+    oracle.set_rom_scheme(rom, "fe")
+    try:
+        st = oracle.reset_state(rom)
+        assert int(st["scheme"]) == 7
+        assert [int(x) for x in st["ram"][0:8]] == [0xB1, 0xB0, 0xB0, 0xB1, 0xB0, 0xB1, 0xB0, 0xB1]
+        with oracle.phantoms_off():                                 # PLA's stack read is a phantom access
+            st = oracle.reset_state(rom)
+        assert [int(x) for x in st["ram"][6:8]] != [0xB0, 0xB1]
+    finally:
+        oracle.set_rom_scheme(rom, "auto")
+
+
+def test_fe_registry_lengths():
+    c = carts.fe_cart()
+    fa.set_rom_scheme(c.rom, "fe")
+    try:
+        assert fa.rom_scheme(c.rom) == 7
+    finally:
+        fa.set_rom_scheme(c.rom, "auto")
+    with pytest.raises(fa.FaError):
+        fa.set_rom_scheme(bytes(4096), "fe")
