@@ -312,10 +312,14 @@ extern "C" int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len)
     const int by_size = auto_scheme(rom_len);
     if (by_size == FA_SCHEME_DPC) return by_size;
     const uint32_t hlo = by_size > 0 ? fa_hot_lo(by_size) : 0x2000u, hn = by_size > 0 ? fa_nbanks(by_size) : 0u;
-    size_t e0 = 0, own = 0, st3f = 0;
+    size_t e0 = 0, own = 0, st3f = 0, jsr_d = 0, jsr_f = 0;
     for (size_t i = 0; i + 2 < rom_len; i++) {
         const uint8_t op = rom[i];
         if ((op == 0x85 || op == 0x86 || op == 0x84) && rom[i + 1] == 0x3F) st3f++;
+        if (op == 0x20) {                                   // JSR: FE carts call across banks by $Dxxx / $Fxxx
+            jsr_d += (rom[i + 2] & 0xF0u) == 0xD0u;
+            jsr_f += (rom[i + 2] & 0xF0u) == 0xF0u;
+        }
         if (std::find(std::begin(abs_ops), std::end(abs_ops), op) == std::end(abs_ops)) continue;
         const uint32_t a = (uint32_t)rom[i + 1] | ((uint32_t)rom[i + 2] << 8);
         if (!(a & 0x1000u)) continue;
@@ -330,6 +334,12 @@ extern "C" int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len)
     if (rom_len == 8192 && e0 >= 3 && e0 > 8 * own && (vec_hi & 0x1Cu) == 0x1Cu) return FA_SCHEME_E0;
     if (st3f >= 3 && st3f > 8 * own && (vec_hi & 0x18u) == 0x18u && scheme_len_ok(FA_SCHEME_3F, rom_len))
         return FA_SCHEME_3F;
+    // FE: no access to the F8 hotspots (an F8 cart cannot switch without
+    // them), calls into both $Dxxx and $Fxxx, and a reset vector in one of
+    // those two ranges.
+    const uint32_t vec_top = rom_len >= 4 ? rom[rom_len - 3] & 0xF0u : 0u;
+    if (rom_len == 8192 && own == 0 && jsr_d >= 6 && jsr_f >= 6 && (vec_top == 0xD0u || vec_top == 0xF0u))
+        return FA_SCHEME_FE;
     if (by_size < 0)
         return fa_fail(FA_ERR_BAD_ROM, "ROM length %zu cannot be constructed (reference panics)", rom_len);
     return by_size;

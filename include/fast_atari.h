@@ -217,8 +217,11 @@ int fa_rom_scheme(const uint8_t* rom, size_t rom_len);
  * accesses, over eight times the size-rule ones, and a reset vector in
  * $1C00-$1FFF is E0; at least three $3F stores, over eight times the size-rule
  * accesses, and a reset vector in $1800-$1FFF make a 2K-multiple image 3F;
- * a DPC length is DPC; anything else gets the size rule.  On random bytes it
- * picks E0 or 3F for a few percent of 8K images. */
+ * an 8K image with no access to the F8 hotspots, at least six JSRs into
+ * $Dxxx and six into $Fxxx (FE carts call across their banks that way) and
+ * a reset vector in one of those ranges is FE; a DPC length is DPC; anything
+ * else gets the size rule.  On random bytes it picks E0, 3F or FE for a few
+ * percent of 8K images. */
 int fa_rom_guess_scheme(const uint8_t* rom, size_t rom_len);
 
 /*

@@ -416,3 +416,24 @@ def test_fe_registry_lengths():
         fa.set_rom_scheme(c.rom, "auto")
     with pytest.raises(fa.FaError):
         fa.set_rom_scheme(bytes(4096), "fe")
+
+
+def test_guess_fe_from_cross_bank_calls():
+    """Six JSRs into $Dxxx and six into $Fxxx, no F8 hotspot access and a
+    reset vector at $F100: FE.  One LDA $FFF8 (an F8 bank switch) makes it the
+    size rule's F8 again, and so do fewer calls."""
+    def image(calls, hotspot):
+        rom = bytearray(8192)
+        at = 0x100
+        for hi in (0xD1, 0xF1):
+            for _ in range(calls):
+                rom[at:at + 3] = bytes([0x20, 0x00, hi])
+                at += 3
+        if hotspot:
+            rom[at:at + 3] = bytes([0xAD, 0xF8, 0xFF])
+        for b in range(2):
+            rom[b * 4096 + 0xFFC:b * 4096 + 0xFFE] = bytes([0x00, 0xF1])
+        return bytes(rom)
+    assert fa.guess_rom_scheme(image(6, False)) == 7
+    assert fa.guess_rom_scheme(image(6, True)) == 1
+    assert fa.guess_rom_scheme(image(5, False)) == 1
