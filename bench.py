@@ -64,7 +64,7 @@ I_CONV = 165.5
 # capture in profiles/fa_run_warps_mixed_batch_full.md (29.6 MB per 4-frame
 # call of 135,500 instances).
 DRAM_BYTES_PER_INSTANCE_FRAME = 54.6
-# The rendering kernel (fa_render_run<8>) per rendered console-frame, from
+# The rendering kernel (fa_render_run) per rendered console-frame, from
 # the ncu capture in profiles/fa_render_run_render_cart.md: SASS
 # thread-instructions and DRAM bytes (framebuffer writes included).
 RENDER_THREAD_INST_PER_FRAME = 2.936e6   # smsp__thread_inst_executed / console-frames
