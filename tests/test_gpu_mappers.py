@@ -231,17 +231,18 @@ def test_sliced_rendering_console_matches_oracle(sliced, name):
 
 
 def test_sliced_carts_in_the_server(sliced, dpc):
-    roms = [sliced["e0"].rom, carts.mixed_carts()[1].rom, dpc["dpc"].rom]
-    reqs = [(0, 70, 3), (1, 40, 2), (2, 33, 4), (0, 70, 2)]
+    roms = [sliced["e0"].rom, carts.mixed_carts()[1].rom, dpc["dpc"].rom, sliced["fe"].rom]
+    sizes = {0: 70, 1: 40, 2: 33, 3: 50}
+    reqs = [(0, 70, 3), (1, 40, 2), (2, 33, 4), (3, 50, 3), (0, 70, 2), (3, 50, 2)]
     with fa.AtariServer(roms) as srv:
-        sids = {c: srv.open(c) for c in (0, 1, 2)}
+        sids = {c: srv.open(c) for c in sizes}
         got = [srv.step(sids[c], carts.actions(seed=90 + i, n=n, frames=k), n, k)[0] for i, (c, n, k) in enumerate(reqs)]
-        states = {c: srv.states(sids[c]) for c in (0, 1, 2)}
-    ref = {c: oracle_states(roms[c], 70 if c == 0 else (40 if c == 1 else 33)) for c in (0, 1, 2)}
+        states = {c: srv.states(sids[c]) for c in sizes}
+    ref = {c: oracle_states(roms[c], sizes[c]) for c in sizes}
     for i, (c, n, k) in enumerate(reqs):
         o, _ = oracle.run_batch(roms[c], ref[c], carts.actions(seed=90 + i, n=n, frames=k), k)
         assert np.array_equal(got[i], o), f"request {i}"
-    for c in (0, 1, 2):
+    for c in sizes:
         assert_states_equal(states[c], ref[c], f"cart {c}")
 
 
