@@ -1083,8 +1083,9 @@ def dpc_script() -> List[tuple]:
     ("r", addr) (its value goes to the next RAM byte from $80 on) and
     ("nop", count).  It walks fetcher 0's counter through top and bottom,
     fetcher 3's across the 11-bit wrap, the random number generator before
-    and after a reset, the no-value functions, and two music channels
-    sampled after gaps of 1 to 300 CPU cycles, one switched off again."""
+    and after a reset, the no-value functions, and music channels sampled
+    after gaps of 1 to 300 CPU cycles: one switched off again, one whose low
+    byte starts above top with bottom above top, one with top 0."""
     s: List[tuple] = []
     s += [("w", 0x1040, 0x30), ("w", 0x1048, 0x2A), ("w", 0x1050, 0x32), ("w", 0x1058, 0x00)]
     s += [("r", 0x1000 + f * 8) for f in (1, 7, 2, 1, 7, 2, 1, 7, 1, 2, 7, 1, 2, 7, 1, 1)]
@@ -1097,6 +1098,11 @@ def dpc_script() -> List[tuple]:
     for gap in (0, 20, 30, 31, 60, 1, 90, 150, 17, 45):
         s += [("nop", gap), ("r", 0x1004), ("r", 0x103D), ("r", 0x100E)]
     s += [("w", 0x105E, 0x00), ("r", 0x100E), ("r", 0x100E), ("r", 0x103E), ("r", 0x1007), ("r", 0x100D)]
+    # Fetcher 7 as a music channel whose low byte starts above top, with
+    # bottom above top; then fetcher 5's top set to 0.
+    s += [("w", 0x1047, 0x03), ("w", 0x104F, 0x05), ("w", 0x1057, 0x0C), ("w", 0x105F, 0x10), ("w", 0x1045, 0x00)]
+    for gap in (40, 7, 250, 300, 3):
+        s += [("nop", gap), ("r", 0x1007), ("r", 0x103F), ("r", 0x100F), ("r", 0x103D)]
     return s
 
 
