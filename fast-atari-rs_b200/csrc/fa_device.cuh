@@ -950,6 +950,19 @@ struct Emu {
             }
         }
     }
+    // The bank state (fa_state::mapper) to and from `slices`, for this core's
+    // schemes only (fa_slices_from_mapper / fa_mapper_from_slices decode all
+    // of them; a core carries only its own).
+    __device__ __forceinline__ uint32_t slices_of(uint32_t m) const
+    {
+        if constexpr (DPC || FE) return fa_slices_4k_bank(m, FE);
+        else return fa_slices_e0_3f(hot_lo, m);
+    }
+    __device__ __forceinline__ uint32_t mapper_of(uint32_t s) const
+    {
+        if constexpr (DPC || FE) return fa_mapper_4k_bank(s, FE);
+        else return fa_mapper_e0_3f(hot_lo, s);
+    }
     // FE core: the access after one to $01FE selects the 4K bank by bit 5 of
     // its data (set: bank 0, clear: bank 1); bit 7 of `slices` marks that the
     // last access was to $01FE.  v is the byte the access read or wrote.
@@ -1705,7 +1718,7 @@ struct Emu {
         w = col[R_TIA0 * stride];  clock = w & 0xFFFF; scanline = w >> 16;
         w = col[R_TIA1 * stride];                                   // wsync fcomp vsync vblank
         tw = ((w >> 16) & 0xFFFFu) | ((w & 1u) << 16) | (((w >> 8) & 1u) << 17) | (((p1 >> 24) & 1u) << 18);
-        if constexpr (SLICED) slices = fa_slices_from_mapper(hot_lo, fa_tia1_mapper(w));
+        if constexpr (SLICED) slices = slices_of(fa_tia1_mapper(w));
         w = col[R_TIA2 * stride];                                   // inpt4 inpt5 pad0 pad1
         pins = ((p0 >> 16) & 0xFFu) | (((p1 >> 8) & 0xFFu) << 8) | ((w & 1u) << 16) | (((w >> 8) & 1u) << 17);
         pads = w >> 16;
@@ -1721,7 +1734,7 @@ struct Emu {
         col[R_SELPC * stride] = (su & 0xFFFFu) | (pcnt << 16);
         col[R_TIA0 * stride] = clock | (scanline << 16);
         uint32_t t1 = ((tw >> 16) & 1u) | (((tw >> 17) & 1u) << 8) | ((tw & 0xFFFFu) << 16);
-        if constexpr (SLICED) t1 |= fa_mapper_tia1(fa_mapper_from_slices(hot_lo, slices));
+        if constexpr (SLICED) t1 |= fa_mapper_tia1(mapper_of(slices));
         col[R_TIA1 * stride] = t1;
         col[R_TIA2 * stride] = ((pins >> 16) & 1u) | (((pins >> 17) & 1u) << 8) | (pads << 16);
     }

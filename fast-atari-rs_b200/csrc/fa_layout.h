@@ -102,7 +102,9 @@ FA_HD static inline uint32_t fa_map_kind(uint32_t hot_lo) { return hot_lo < 0x10
 // several kinds, E0 / 3F carts only, DPC carts only, FE carts only.
 enum : int { FA_MAPS_4K = 0, FA_MAPS_BOTH = 1, FA_MAPS_SLICED = 2, FA_MAPS_DPC = 3, FA_MAPS_FE = 4 };
 
-FA_HD static inline uint32_t fa_slices_from_mapper(uint32_t hot_lo, uint32_t m)
+// E0 and 3F; the 4K-bank pair of DPC and FE (bank b: slices 4b..4b+3, FE's
+// armed flag in bit 7); any scheme.  Each device core calls only its own.
+FA_HD static inline uint32_t fa_slices_e0_3f(uint32_t hot_lo, uint32_t m)
 {
     if (fa_map_kind(hot_lo) == FA_MAP_E0)
         return (m & 7u) | (((m >> 4) & 7u) << 8) | (((m >> 8) & 7u) << 16) | (7u << 24);
@@ -110,19 +112,35 @@ FA_HD static inline uint32_t fa_slices_from_mapper(uint32_t hot_lo, uint32_t m)
         const uint32_t n = hot_lo & 0xFFu, b = (m & 0xFFu) % n, l = n - 1u;
         return (2u * b) | ((2u * b + 1u) << 8) | ((2u * l) << 16) | ((2u * l + 1u) << 24);
     }
-    if (fa_map_kind(hot_lo) == FA_MAP_DPC) return (m & 1u) * 0x04040404u + 0x03020100u;
-    if (fa_map_kind(hot_lo) == FA_MAP_FE) return ((m & 1u) * 0x04040404u + 0x03020100u) | (((m >> 8) & 1u) << 7);
     return 0u;
 }
+FA_HD static inline uint32_t fa_slices_4k_bank(uint32_t m, bool fe)
+{
+    return ((m & 1u) * 0x04040404u + 0x03020100u) | (fe ? ((m >> 8) & 1u) << 7 : 0u);
+}
+FA_HD static inline uint32_t fa_slices_from_mapper(uint32_t hot_lo, uint32_t m)
+{
+    if (fa_map_kind(hot_lo) == FA_MAP_DPC || fa_map_kind(hot_lo) == FA_MAP_FE)
+        return fa_slices_4k_bank(m, fa_map_kind(hot_lo) == FA_MAP_FE);
+    return fa_slices_e0_3f(hot_lo, m);
+}
 
-FA_HD static inline uint32_t fa_mapper_from_slices(uint32_t hot_lo, uint32_t slices)
+FA_HD static inline uint32_t fa_mapper_e0_3f(uint32_t hot_lo, uint32_t slices)
 {
     if (fa_map_kind(hot_lo) == FA_MAP_E0)
         return (slices & 7u) | (((slices >> 8) & 7u) << 4) | (((slices >> 16) & 7u) << 8);
     if (fa_map_kind(hot_lo) == FA_MAP_3F) return (slices & 0xFFu) >> 1;
-    if (fa_map_kind(hot_lo) == FA_MAP_DPC) return (slices & 0xFFu) >> 2;
-    if (fa_map_kind(hot_lo) == FA_MAP_FE) return ((slices & 0x7Fu) >> 2) | (((slices >> 7) & 1u) << 8);
     return 0u;
+}
+FA_HD static inline uint32_t fa_mapper_4k_bank(uint32_t slices, bool fe)
+{
+    return ((slices & 0x7Fu) >> 2) | (fe ? ((slices >> 7) & 1u) << 8 : 0u);
+}
+FA_HD static inline uint32_t fa_mapper_from_slices(uint32_t hot_lo, uint32_t slices)
+{
+    if (fa_map_kind(hot_lo) == FA_MAP_DPC || fa_map_kind(hot_lo) == FA_MAP_FE)
+        return fa_mapper_4k_bank(slices, fa_map_kind(hot_lo) == FA_MAP_FE);
+    return fa_mapper_e0_3f(hot_lo, slices);
 }
 
 // The bank state's 14 stored bits ride in R_TIA1's flag bytes, above the
