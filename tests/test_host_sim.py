@@ -133,8 +133,9 @@ def test_device_core_on_random_roms_and_states(sim, size):
 def test_extra_cores_on_random_roms_and_states(sim, scheme, code):
     """The FE and DPC cores on random images from random CPU states and RAM,
     some started armed (FE) or with random DPC registers: random stack
-    pointers put JSR, RTS, RTI, PHA, PLA, BRK and indexed or indirect
-    accesses on $01FE, and every phantom access the reference CPU makes
+    pointers ($F8-$FF and, wrapping, $00-$07) put JSR, RTS, RTI, PHA, PLA,
+    BRK and indexed or indirect accesses on $01FE, and every phantom access
+    the reference CPU makes
     (zero-page bases, stack reads, old-value writes, fix-ups) must reach the
     FE decode in the oracle's order; random reads and writes hit the DPC
     registers in every function."""
@@ -153,7 +154,10 @@ def test_extra_cores_on_random_roms_and_states(sim, scheme, code):
             n = 96
             st = np.array([oracle.reset_state(rom)] * n, dtype=oracle.STATE_DTYPE)
             st["a"], st["x"], st["y"] = rng.integers(0, 256, n), rng.integers(0, 256, n), rng.integers(0, 256, n)
-            st["sp"], st["status"] = rng.integers(0xF8, 0x100, n), rng.integers(0, 256, n) & 0xCF
+            # Stacks at $01F8-$01FF put $01FE in reach; at $0100-$0107 they
+            # wrap and push into the TIA's mirror.
+            st["sp"] = (rng.integers(0xF8, 0x108, n) & 0xFF)
+            st["status"] = rng.integers(0, 256, n) & 0xCF
             st["pc"] = 0xF000 + rng.integers(0, 0x1000, n)
             st["ram"] = rng.integers(0, 256, (n, 128))
             st["mapper"][:, 0] = rng.integers(0, 2, n)
